@@ -1,0 +1,250 @@
+/* ptx_rt.h — C ABI of the B200 transport loop for PathTracerGLSL scenes.
+ *
+ * This library replaces the WebGL executor of a CompiledRenderer
+ * (reference: src/engine/RenderExecutor.ts:27-230, driven by src/engine/Engine.ts:83-438).
+ * The host compiles a SceneDescription + RenderStrategy into a packed scene (the
+ * counterpart of CompiledScene.sceneData, src/compiler/types.ts:1154-1164, executed by
+ * src/app/sceneData.ts:27) and a program description (the estimator/measurement knobs of
+ * ProgramDescription, src/compiler/plan/types.ts:39-112), then renders frames and reads
+ * exports exactly where the reference calls Engine.renderFrame / Engine.readExport.
+ *
+ * Conventions (mirroring the reference's engine contract):
+ *   - every entry point returns an int status: 0 = OK, negative = error class (PTR_E_*);
+ *     ptr_last_error(ctx) returns the message of the last failure on that context;
+ *   - the host owns every array it passes; upload copies them (registerDataTexture);
+ *   - calls on one context are not re-entrant (one host thread per context, like the
+ *     reference's single JS main thread); rendering is asynchronous on the context's
+ *     stream and ptr_sync / ptr_read_export synchronise.
+ *   - images are row-major with row 0 at the BOTTOM (gl_FragCoord convention), RGB.
+ */
+#ifndef PTX_RT_H
+#define PTX_RT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTR_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------- */
+#define PTR_OK 0
+#define PTR_E_INVALID -1     /* bad argument / malformed scene (Validator-class error)  */
+#define PTR_E_CUDA -2        /* CUDA runtime/driver error                                */
+#define PTR_E_NOMEM -3       /* device allocation failed                                 */
+#define PTR_E_TIMEOUT -4     /* ptr_sync timed out (work still in flight)                */
+#define PTR_E_DEVICE -5      /* a kernel reported an error flag (budget / bounds guard)  */
+#define PTR_E_UNSUPPORTED -6 /* feature not available in this build                      */
+
+/* ---- shapes (one region = one scene object, reference region index order) --------- */
+/* Shape occupants: src/components/geometry/{plane,sphere,quad,box}, meshes
+ * src/components/intersection/mesh, instanced batches src/components/intersection/instancing. */
+#define PTR_SHAPE_PLANE 0     /* p: normal.xyz, offset            (plane.glsl)            */
+#define PTR_SHAPE_SPHERE 1    /* p: center.xyz, radius            (sphere.glsl)           */
+#define PTR_SHAPE_QUAD 2      /* p: corner, edge1, edge2, normal  (quad.glsl)  thin       */
+#define PTR_SHAPE_BOX 3       /* p: center.xyz, halfSize.xyz      (box.glsl)              */
+#define PTR_SHAPE_MESH 4      /* ref = mesh index; thin (v0 meshes are open surfaces)     */
+#define PTR_SHAPE_INSTANCES 5 /* ref = batch index (placements of one prototype)          */
+
+typedef struct ptr_region {
+    int32_t shape;     /* PTR_SHAPE_*                                                    */
+    int32_t material;  /* material_of(region); -1 = none                                 */
+    int32_t thin;      /* 1 = zero-thickness owner (scene_region_thin)                   */
+    int32_t ref;       /* mesh / batch index for PTR_SHAPE_MESH / PTR_SHAPE_INSTANCES     */
+    float ior;         /* ior_of(region)                                                 */
+    float p[15];       /* shape parameters, layout per PTR_SHAPE_*                       */
+} ptr_region;          /* 80 bytes */
+
+/* ---- materials (src/components/materials, volume_scattering, transport/volume) ---- */
+#define PTR_MAT_LAMBERT 0
+#define PTR_MAT_DIELECTRIC 1
+#define PTR_MAT_GGX 2
+#define PTR_MAT_MIRROR 3
+#define PTR_MAT_NONE 4 /* null interface: a medium boundary with no optical surface */
+
+#define PTR_MATF_EMISSIVE 1
+#define PTR_MATF_MEDIUM 2       /* material_has_medium                               */
+#define PTR_MATF_SCATTERING 4   /* medium with sigma_s > 0 (HG phase)                */
+
+typedef struct ptr_material {
+    int32_t model;          /* PTR_MAT_*                                                  */
+    int32_t flags;          /* PTR_MATF_*                                                 */
+    int32_t pad0, pad1;
+    float albedo[4];        /* lambert albedo (rgb)                                       */
+    float emission[4];      /* emitted radiance (rgb)                                     */
+    float transmittance[4]; /* dielectric interface tint                                  */
+    float f0[4];            /* ggx / mirror normal-incidence reflectance                  */
+    float sigma_a[4];       /* medium absorption (rgb)                                    */
+    float sigma_s[4];       /* medium scattering (rgb)                                    */
+    float alpha;            /* ggx alpha = max(1e-3, roughness^2)  (ggx.glsl:7-9)          */
+    float phase_g;          /* HG asymmetry                                               */
+    float pad2, pad3;
+} ptr_material;             /* 128 bytes */
+
+/* ---- lights (src/components/lights/{quad,sphere,point}) ---------------------------- */
+#define PTR_LIGHT_QUAD 0   /* p: corner(3) edge1(3) edge2(3) normal(3) area(1) */
+#define PTR_LIGHT_SPHERE 1 /* p: center(3) radius(1)                            */
+#define PTR_LIGHT_POINT 2  /* p: position(3)     radiance = intensity (W/sr)    */
+
+typedef struct ptr_light {
+    int32_t kind;
+    int32_t region;        /* the hittable region desugared from this light, -1 for delta */
+    float select_pdf;      /* selection probability among finite lights (power CDF)       */
+    float select_cdf;      /* cumulative probability up to and including this light       */
+    float radiance[4];
+    float p[16];
+} ptr_light;               /* 96 bytes */
+
+/* ---- environment (src/components/env; features/environment.ts) --------------------- */
+#define PTR_ENV_NONE 0
+#define PTR_ENV_CONSTANT 1
+#define PTR_ENV_IMAGE 2 /* equirect table + 2-level CDF (importance.ts, sampler_cdf.glsl) */
+
+typedef struct ptr_env {
+    int32_t kind;
+    int32_t sample_as_light;  /* joins NEE/MIS                                          */
+    int32_t width, height;    /* equirect table size                                    */
+    float color[4];           /* constant radiance                                      */
+    float intensity;          /* live multiplier (u_envIntensity)                       */
+    float select_prob;        /* P(sample env) in two-stage NEE (u_envSelectProb)       */
+    float rotation;           /* azimuth rotation, radians (u_envRotation)              */
+    float pad;
+    const float* radiance;    /* width*height*4 RGBA32F, row 0 = v=0 (+Y pole)          */
+    const float* marginal;    /* height+1 cumulative (CDF over rows)                    */
+    const float* conditional; /* height*(width+1) cumulative (CDF within each row)      */
+} ptr_env;
+
+/* ---- triangle meshes, BVH / CWBVH (src/components/accel, intersection/mesh) --------- */
+typedef struct ptr_mesh_desc {
+    int32_t n_vertices, n_triangles;
+    const float* positions;    /* 3*V, object-local                                       */
+    const uint32_t* indices;   /* 3*T                                                     */
+    const float* tri_alpha;    /* optional per-triangle GGX alpha (T), NULL = material's  */
+} ptr_mesh_desc;
+
+typedef struct ptr_batch_desc {
+    int32_t prototype_shape;   /* PTR_SHAPE_SPHERE or PTR_SHAPE_MESH                     */
+    int32_t prototype_ref;     /* mesh index for mesh prototypes                          */
+    int32_t n_instances;
+    int32_t pad;
+    float proto[4];            /* sphere prototype: center.xyz, radius                   */
+    const float* placements;   /* 8*N: quaternion xyzw (world->local rigid), ts = (t_rigid.xyz, s) */
+} ptr_batch_desc;
+
+typedef struct ptr_scene_desc {
+    int32_t abi_version;       /* PTR_ABI_VERSION                                         */
+    int32_t n_regions;
+    const ptr_region* regions;
+    int32_t n_materials;
+    const ptr_material* materials;
+    int32_t n_lights;
+    const ptr_light* lights;
+    int32_t ambient_material;  /* material_of(-1); -1 = vacuum                             */
+    ptr_env env;
+    int32_t n_meshes;
+    const ptr_mesh_desc* meshes;
+    int32_t n_batches;
+    const ptr_batch_desc* batches;
+} ptr_scene_desc;
+
+/* ---- program (strategy) ---------------------------------------------------------- */
+#define PTR_DIRECT_NONE 0
+#define PTR_DIRECT_NEE 1
+#define PTR_DIRECT_MIS 2
+#define PTR_ACCEL_BVH 0   /* binary SAH BVH (bvh.ts)                   */
+#define PTR_ACCEL_CWBVH 1 /* compressed wide BVH (cwbvh.ts)            */
+
+typedef struct ptr_program_desc {
+    int32_t abi_version;
+    int32_t max_bounces;        /* measurement.maxBounces                             */
+    int32_t max_null_crossings; /* measurement.maxNullCrossings (default 32)          */
+    int32_t direct;             /* estimator.directLighting                           */
+    int32_t rr_start;           /* russianRoulette.startDepth, -1 = off               */
+    float rr_max_survival;      /* russianRoulette.maxSurvival (0.95)                 */
+    int32_t scattering;         /* measurement.scattering: 1 full, 0 ignored           */
+    int32_t accel;              /* PTR_ACCEL_*  (meshTraversal / instanceAccel)        */
+    int32_t equiangular;        /* mediumLightSampling 'equiangular'                  */
+    int32_t pad[7];
+} ptr_program_desc;
+
+/* The per-frame builtins + camera uniforms (Engine.ts:231-258, camera.ts:69-160). */
+typedef struct ptr_camera {
+    float position[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float tan_fov;              /* tan(fov/2) */
+    float aspect;               /* width/height */
+} ptr_camera;
+
+typedef struct ptr_frame {
+    int32_t width, height;      /* engine.imageSize                                   */
+    int32_t first_sample;       /* engine.sampleCount of the first sample             */
+    int32_t spp;                /* samples per pixel rendered by this call            */
+    uint32_t reset_salt;        /* engine.resetSalt                                   */
+    int32_t pixel_offset[2];    /* engine.pixelOffset (tiled renders)                 */
+    int32_t accumulate;         /* 0 = clear the film first, 1 = add to it            */
+    ptr_camera camera;
+} ptr_frame;
+
+typedef struct ptr_counters {
+    uint64_t paths;             /* camera paths traced                                */
+    uint64_t closest_queries;   /* closest-hit ray queries                            */
+    uint64_t shadow_queries;    /* shadow (any-hit / transmittance) queries           */
+    uint64_t nodes_visited;     /* BVH nodes popped (when counting is enabled)         */
+    uint64_t prims_tested;      /* primitive / triangle tests (when counting enabled)  */
+    uint32_t error_flags;       /* device-side guard flags (stack / budget)            */
+    uint32_t pad;
+} ptr_counters;
+
+typedef struct ptr_ctx ptr_ctx;
+typedef struct ptr_scene ptr_scene;
+typedef struct ptr_program ptr_program;
+
+/* Context: one CUDA device + stream.  (Engine constructor, Engine.ts:83) */
+int ptr_create(int device_ordinal, ptr_ctx** out);
+int ptr_destroy(ptr_ctx* ctx);
+const char* ptr_last_error(const ptr_ctx* ctx);
+int ptr_abi_version(void);
+
+/* Scene data upload, once per scene (Engine.registerDataTexture, Engine.ts:438;
+ * sceneData.ts:27).  Builds the BVH/CWBVH of every mesh on the host and copies all
+ * arrays to device memory. */
+int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* desc, ptr_scene** out);
+int ptr_free_scene(ptr_scene* scene);
+
+/* Program per scene x strategy (Engine.loadRenderer, Engine.ts:147). */
+int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* desc, ptr_program** out);
+int ptr_free_program(ptr_program* prog);
+
+/* Render frame.spp samples per pixel into the program's film, asynchronously
+ * (Engine.renderFrame, Engine.ts:190-204; one call may fold many frames). */
+int ptr_render(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame);
+
+/* Wait for the context's stream, at most timeout_ms (<0 = no limit). */
+int ptr_sync(ptr_ctx* ctx, int timeout_ms);
+
+/* Read an export into host memory (Engine.readExport, Engine.ts:351).
+ * name: "radiance" (mean, 3 floats/pixel), "variance" (per-pixel sample variance of
+ * the mean's samples, 3 floats/pixel), "samples" (1 float/pixel: sample count).
+ * n = number of floats in dst. */
+int ptr_read_export(ptr_program* prog, const char* name, float* dst, size_t n);
+
+/* Same, but the destination is device memory (no synchronisation). */
+int ptr_read_export_device(ptr_program* prog, const char* name, float* dst_device, size_t n);
+
+/* Device work counters of the last ptr_render on this program (synchronises). */
+int ptr_get_counters(ptr_program* prog, ptr_counters* out);
+
+/* Record the per-launch kernel timings of the next ptr_render (CUDA events on the
+ * context's stream).  ms_out[k] = total ms of kernel class k over that render:
+ * 0 generate, 1 closest-hit, 2 shade, 3 shadow, 4 film. */
+int ptr_profile_next(ptr_program* prog, int enable);
+int ptr_get_profile(ptr_program* prog, float* ms_out, int n, int* launches_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PTX_RT_H */

@@ -1,0 +1,73 @@
+"""Python binding of the CPU restatement (``oracle/pt_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY: used by ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / reference arm of ``bench.py`` as the checker, never by the product.
+It consumes the same packed scene (``include/ptx_rt.h`` layout) the CUDA engine uploads.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "liboracle.so")
+SOURCES = [os.path.join(HERE, "pt_oracle.cpp")]
+
+
+def build(force=False):
+    """Compile the restatement with g++ (OpenMP, -O3, binary32 without FMA contraction)."""
+    os.makedirs(BUILD, exist_ok=True)
+    header = os.path.join(HERE, "..", "include", "ptx_rt.h")
+    newest = max(os.path.getmtime(p) for p in SOURCES + [header])
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+        return LIB
+    cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+           *SOURCES, "-o", LIB]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+        _lib.oracle_render.restype = ctypes.c_int
+        _lib.oracle_render.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_void_p, ctypes.c_int]
+    return _lib
+
+
+def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=None,
+           threads=0, keep_samples=False, pixel_offset=(0, 0)):
+    """Render with the oracle.  Returns dict(mean, var, sum, sumsq, samples?, counts)."""
+    from pathtracerglsl_b200 import abi
+    desc = packed.desc()
+    fr = abi.Frame()
+    fr.width, fr.height = width, height
+    fr.first_sample, fr.spp = first_sample, spp
+    fr.reset_salt = salt
+    fr.pixel_offset = (ctypes.c_int32 * 2)(*pixel_offset)
+    fr.camera = renderer.camera(params or {}, width, height)
+    s = np.zeros((height, width, 3), np.float64)
+    q = np.zeros((height, width, 3), np.float64)
+    samples = np.zeros((spp, height, width, 3), np.float32) if keep_samples else None
+    counts = (ctypes.c_uint64 * 2)()
+    rc = lib().oracle_render(ctypes.addressof(desc), ctypes.addressof(renderer.program), ctypes.addressof(fr),
+                             s.ctypes.data, q.ctypes.data,
+                             samples.ctypes.data if samples is not None else None,
+                             ctypes.addressof(counts), threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_render failed: {rc}")
+    mean = s / spp
+    var = np.maximum(q / spp - mean * mean, 0.0) * (spp / max(spp - 1, 1))
+    out = {"mean": mean, "var": var, "sum": s, "sumsq": q,
+           "closest_queries": counts[0], "shadow_queries": counts[1]}
+    if samples is not None:
+        out["samples"] = samples
+    return out

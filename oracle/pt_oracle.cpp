@@ -1,0 +1,909 @@
+// pt_oracle.cpp — CPU restatement of PathTracerGLSL's generated transport loop.
+//
+// TEST INFRASTRUCTURE ONLY (the oracle): linked by tests/, __graft_entry__.smoke() and
+// bench.py's cpu_baseline / reference arm as the checker; the product never links it.
+//
+// This is a scalar, data-driven restatement of the program the reference's Generate
+// stage emits for a scene x strategy (the unrolled arms of
+// src/compiler/generate/features/*.ts become loops over the packed scene of
+// include/ptx_rt.h).  Every function names the reference file:line it follows.  The
+// arithmetic is binary32 in the GLSL operation order; it is pinned against the
+// reference's own programs compiled on the host (oracle/_ref) and the witness values.
+//
+// Parallelism: OpenMP over pixels (the reference's only parallel axis, one fragment
+// per pixel).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <omp.h>
+
+#include "../include/ptx_rt.h"
+
+namespace {
+
+// ---------------------------------------------------------------- vector helpers
+struct v3 {
+    float x, y, z;
+    v3() : x(0), y(0), z(0) {}
+    v3(float a, float b, float c) : x(a), y(b), z(c) {}
+    explicit v3(float s) : x(s), y(s), z(s) {}
+    float& operator[](int i) { return (&x)[i]; }
+    float operator[](int i) const { return (&x)[i]; }
+};
+inline v3 operator+(v3 a, v3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline v3 operator-(v3 a, v3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline v3 operator*(v3 a, v3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline v3 operator/(v3 a, v3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline v3 operator*(v3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline v3 operator*(float s, v3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+inline v3 operator/(v3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+inline v3 operator-(v3 a) { return v3(-a.x, -a.y, -a.z); }
+inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline v3 cross(v3 a, v3 b) { return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+inline float length(v3 a) { return std::sqrt(dot(a, a)); }
+inline v3 normalize(v3 a) { return a * (1.0f / length(a)); }
+inline float fminf_(float a, float b) { return b < a ? b : a; }
+inline float fmaxf_(float a, float b) { return a < b ? b : a; }
+inline v3 vmin(v3 a, v3 b) { return v3(fminf_(a.x, b.x), fminf_(a.y, b.y), fminf_(a.z, b.z)); }
+inline v3 vmax(v3 a, v3 b) { return v3(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z)); }
+inline v3 vexp(v3 a) { return v3(std::exp(a.x), std::exp(a.y), std::exp(a.z)); }
+inline v3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
+inline float clampf(float x, float lo, float hi) { return fminf_(fmaxf_(x, lo), hi); }
+inline float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
+constexpr float PI = 3.14159265359f;       // math.glsl PI
+constexpr float TWO_PI = 6.28318530718f;   // math.glsl TWO_PI
+constexpr float MAX_DIST = 1000.0f;        // math.glsl MAX_DIST
+constexpr float EPS_INTERFACE = 0.001f;    // math.glsl EPS_INTERFACE
+constexpr float MARCH_CLEARANCE = 0.001f;  // math.glsl MARCH_CLEARANCE
+constexpr float SHADOW_BACKOFF = 0.002f;   // math.glsl:39 SHADOW_BACKOFF
+constexpr float FP_UNCERTAINTY_REL = 3.0517578125e-5f;
+constexpr float FP_UNCERTAINTY_ABS = 1.52587890625e-5f;
+
+constexpr uint32_t LOBE_REFLECTION = 1u, LOBE_TRANSMISSION = 2u, LOBE_DELTA = 4u, LOBE_MEDIUM = 8u;
+constexpr uint32_t LIGHT_DELTA = 1u;
+
+// spectrum helpers (components/color/spectrum.glsl:1-24), N = 3
+inline float spectrum_average(v3 s) { float sum = s[0]; sum += s[1]; sum += s[2]; return sum * (1.0f / 3.0f); }
+inline float spectrum_max(v3 s) { float m = s[2]; m = fmaxf_(s[1], m); m = fmaxf_(s[0], m); return m; }
+inline bool spectrum_is_black(v3 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f; }
+inline int spectrum_sample_channel(float u) { int c = (int)(u * 3.0f); return c < 2 ? c : 2; }
+
+// ---------------------------------------------------------------- RNG (pcg4d.glsl:12-40)
+struct Rng {
+    uint32_t base, dim;
+    static void pcg4d(uint32_t v[4]) {
+        for (int i = 0; i < 4; ++i) v[i] = v[i] * 1664525u + 1013904223u;
+        v[0] += v[1] * v[3]; v[1] += v[2] * v[0]; v[2] += v[0] * v[1]; v[3] += v[1] * v[2];
+        for (int i = 0; i < 4; ++i) v[i] ^= v[i] >> 16u;
+        v[0] += v[1] * v[3]; v[1] += v[2] * v[0]; v[2] += v[0] * v[1]; v[3] += v[1] * v[2];
+    }
+    void init(uint32_t px, uint32_t py, uint32_t sample_count, uint32_t salt) {
+        uint32_t v[4] = {px, py, sample_count, salt};
+        pcg4d(v);
+        base = v[0];
+        dim = 0;
+    }
+    float next() {
+        uint32_t v[4] = {base, dim++, 0u, 0u};
+        pcg4d(v);
+        return (float)(v[0] >> 8) * (1.0f / 16777216.0f);
+    }
+};
+
+// ---------------------------------------------------------------- core structs (structs.glsl)
+struct Frame { v3 t, b, n; };
+struct Ray { v3 o, d; };
+struct Hit {
+    float t; v3 p; Frame frame; v3 ng;
+    int region_from, region_to, region_owner, element;
+    float eps;
+};
+struct LightSample { v3 wi; float distance; v3 radiance; float pdf; uint32_t flags; int light_id; };
+struct ISample { v3 wi; v3 weight; float pdf; uint32_t flags; };
+
+// fp_uncertainty (math.glsl:54-56)
+inline float fp_uncertainty(v3 p) {
+    return fmaxf_(FP_UNCERTAINTY_ABS, FP_UNCERTAINTY_REL * fmaxf_(std::fabs(p.x), fmaxf_(std::fabs(p.y), std::fabs(p.z))));
+}
+// ambient_frame (components/ambient/euclidean/euclidean.glsl:6-33)
+inline Frame ambient_frame(v3 n) {
+    v3 nn = normalize(n);
+    v3 t = std::fabs(nn.x) < 0.9f ? v3(1, 0, 0) : v3(0, 1, 0);
+    t = normalize(t - dot(t, nn) * nn);
+    return Frame{t, cross(nn, t), nn};
+}
+// build_basis (math.glsl)
+inline void build_basis(v3 n, v3& t, v3& b) {
+    v3 up = std::fabs(n.y) < 0.999f ? v3(0, 1, 0) : v3(1, 0, 0);
+    t = normalize(cross(up, n));
+    b = cross(n, t);
+}
+// dielectric_fresnel (math.glsl:95-102)
+inline float dielectric_fresnel(float cos_i, float eta) {
+    float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+    if (sin2_t >= 1.0f) return 1.0f;
+    float cos_t = std::sqrt(1.0f - sin2_t);
+    float r_par = (cos_i - eta * cos_t) / (cos_i + eta * cos_t);
+    float r_perp = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
+    return 0.5f * (r_par * r_par + r_perp * r_perp);
+}
+// schlick_fresnel (math.glsl:83-85)
+inline v3 schlick_fresnel(v3 f0, float c) { return f0 + (v3(1.0f) - f0) * std::pow(1.0f - c, 5.0f); }
+// ray_spawn (glsl/core/ray.glsl:29-32)
+inline Ray ray_spawn(const Hit& h, v3 wi) {
+    float side = dot(wi, h.ng) >= 0.0f ? 1.0f : -1.0f;
+    return Ray{h.p + (h.ng * side) * h.eps, wi};
+}
+
+// ---------------------------------------------------------------- shapes (components/geometry)
+// sphere_intersect (geometry/sphere/sphere.glsl:28-46) — robust Haines form
+inline bool sphere_intersect(const Ray& r, v3 c, float rad, float& t) {
+    v3 oc = r.o - c;
+    float b = dot(oc, r.d);
+    v3 perp = oc - b * r.d;
+    float disc = rad * rad - dot(perp, perp);
+    if (disc < 0.0f) return false;
+    float cc = dot(oc, oc) - rad * rad;
+    float q = (b >= 0.0f) ? -b - std::sqrt(disc) : -b + std::sqrt(disc);
+    if (q == 0.0f) return false;
+    float ta = q, tb = cc / q;
+    t = (cc < 0.0f) ? fmaxf_(ta, tb) : fminf_(ta, tb);
+    return t > 0.0f;
+}
+inline float sphere_sdf(v3 p, v3 c, float rad) { return length(p - c) - rad; }
+// plane_intersect (geometry/plane/plane.glsl)
+inline bool plane_intersect(const Ray& r, v3 n, float off, float& t) {
+    float denom = dot(r.d, n);
+    if (std::fabs(denom) < 1e-8f) return false;
+    t = -(dot(r.o, n) + off) / denom;
+    return t > 0.0f;
+}
+inline float plane_sdf(v3 p, v3 n, float off) { return dot(p, n) + off; }
+// quad_intersect (geometry/quad/quad.glsl:9-22)
+inline bool quad_intersect(const Ray& r, v3 corner, v3 e1, v3 e2, v3 n, float& t) {
+    float denom = dot(r.d, n);
+    if (std::fabs(denom) < 1e-8f) return false;
+    t = dot(corner - r.o, n) / denom;
+    if (t <= 0.0f) return false;
+    v3 local = r.o + r.d * t - corner;
+    float e11 = dot(e1, e1), e22 = dot(e2, e2), e12 = dot(e1, e2);
+    float d1 = dot(local, e1), d2 = dot(local, e2);
+    float det = e11 * e22 - e12 * e12;
+    float u = (d1 * e22 - d2 * e12) / det;
+    float v = (d2 * e11 - d1 * e12) / det;
+    return u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f;
+}
+// box_intersect / box_sdf / box_normal (geometry/box/box.glsl)
+inline bool box_intersect(const Ray& r, v3 c, v3 h, float& t) {
+    v3 inv = v3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    v3 t0 = (c - h - r.o) * inv;
+    v3 t1 = (c + h - r.o) * inv;
+    v3 tsm = vmin(t0, t1), tbg = vmax(t0, t1);
+    float tn = fmaxf_(fmaxf_(tsm.x, tsm.y), tsm.z);
+    float tf = fminf_(fminf_(tbg.x, tbg.y), tbg.z);
+    if (tf < tn) return false;
+    t = (tn < 0.0f) ? tf : tn;
+    return t > 0.0f;
+}
+inline float box_sdf(v3 p, v3 c, v3 h) {
+    v3 d = v3(std::fabs(p.x - c.x), std::fabs(p.y - c.y), std::fabs(p.z - c.z)) - h;
+    return length(vmax(d, v3(0.0f))) + fminf_(fmaxf_(d.x, fmaxf_(d.y, d.z)), 0.0f);
+}
+inline v3 box_normal(v3 p, v3 c, v3 h) {
+    v3 q = (p - c) / h;
+    v3 a(std::fabs(q.x), std::fabs(q.y), std::fabs(q.z));
+    if (a.x >= a.y && a.x >= a.z) return v3(signf(q.x), 0, 0);
+    if (a.y >= a.z) return v3(0, signf(q.y), 0);
+    return v3(0, 0, signf(q.z));
+}
+
+// ---------------------------------------------------------------- scene
+struct Scene {
+    const ptr_scene_desc* d;
+    const ptr_program_desc* prog;
+    std::vector<int> light_of_region;  // region -> light index (light_of), -1 none
+    bool env_samplable, env_select_live;
+    bool has_media;
+
+    explicit Scene(const ptr_scene_desc* sd, const ptr_program_desc* pd) : d(sd), prog(pd) {
+        light_of_region.assign(sd->n_regions, -1);
+        for (int i = 0; i < sd->n_lights; ++i)
+            if (sd->lights[i].region >= 0) light_of_region[sd->lights[i].region] = i;
+        env_samplable = sd->env.kind != PTR_ENV_NONE && sd->env.sample_as_light;
+        env_select_live = env_samplable && sd->n_lights > 0;
+        has_media = sd->ambient_material >= 0 && (sd->materials[sd->ambient_material].flags & PTR_MATF_MEDIUM);
+        for (int i = 0; i < sd->n_materials; ++i)
+            if (sd->materials[i].flags & PTR_MATF_MEDIUM) has_media = true;
+    }
+    const ptr_material* mat(int m) const { return (m >= 0 && m < d->n_materials) ? &d->materials[m] : nullptr; }
+    // material_of (generated, features/intersection.ts): region -> material; -1 = ambient
+    int material_of(int region) const {
+        if (region < 0) return d->ambient_material;
+        return d->regions[region].material;
+    }
+    float ior_of(int region) const { return region < 0 ? 1.0f : d->regions[region].ior; }
+    bool material_is_emissive(int m) const { auto* p = mat(m); return p && (p->flags & PTR_MATF_EMISSIVE); }
+    bool is_null_interface(int m) const { auto* p = mat(m); return p && p->model == PTR_MAT_NONE; }
+    bool material_has_medium(int m) const { auto* p = mat(m); return p && (p->flags & PTR_MATF_MEDIUM); }
+    bool material_has_nondelta_lobes(int m) const {
+        auto* p = mat(m);
+        return p && (p->model == PTR_MAT_LAMBERT || p->model == PTR_MAT_GGX);
+    }
+
+    // primitive_intersect (features/intersection.ts:801-824, primitiveHitFill :695-715)
+    bool primitive_intersect(const Ray& r, Hit& hit) const {
+        bool found = false;
+        for (int i = 0; i < d->n_regions; ++i) {
+            const ptr_region& g = d->regions[i];
+            float t;
+            v3 n;
+            bool ok = false;
+            switch (g.shape) {
+                case PTR_SHAPE_PLANE: ok = plane_intersect(r, ld3(g.p), g.p[3], t); break;
+                case PTR_SHAPE_SPHERE: ok = sphere_intersect(r, ld3(g.p), g.p[3], t); break;
+                case PTR_SHAPE_QUAD: ok = quad_intersect(r, ld3(g.p), ld3(g.p + 3), ld3(g.p + 6), ld3(g.p + 9), t); break;
+                case PTR_SHAPE_BOX: ok = box_intersect(r, ld3(g.p), ld3(g.p + 3), t); break;
+                default: break;
+            }
+            if (!(ok && t < hit.t)) continue;
+            hit.t = t;
+            found = true;
+            hit.p = r.o + r.d * t;
+            hit.eps = fp_uncertainty(hit.p);
+            switch (g.shape) {
+                case PTR_SHAPE_PLANE: n = ld3(g.p); break;
+                case PTR_SHAPE_SPHERE: n = normalize(hit.p - ld3(g.p)); break;
+                case PTR_SHAPE_QUAD: n = ld3(g.p + 9); break;
+                default: n = box_normal(hit.p, ld3(g.p), ld3(g.p + 3)); break;
+            }
+            hit.frame = ambient_frame(n);
+            hit.ng = hit.frame.n;
+            hit.region_owner = i;
+            hit.element = 0;
+        }
+        return found;
+    }
+    bool scene_intersect_any(const Ray& r, float maxDist) const {
+        for (int i = 0; i < d->n_regions; ++i) {
+            const ptr_region& g = d->regions[i];
+            float t;
+            bool ok = false;
+            switch (g.shape) {
+                case PTR_SHAPE_PLANE: ok = plane_intersect(r, ld3(g.p), g.p[3], t); break;
+                case PTR_SHAPE_SPHERE: ok = sphere_intersect(r, ld3(g.p), g.p[3], t); break;
+                case PTR_SHAPE_QUAD: ok = quad_intersect(r, ld3(g.p), ld3(g.p + 3), ld3(g.p + 6), ld3(g.p + 9), t); break;
+                case PTR_SHAPE_BOX: ok = box_intersect(r, ld3(g.p), ld3(g.p + 3), t); break;
+                default: break;
+            }
+            if (ok && t < maxDist) return true;
+        }
+        return false;
+    }
+    // scene_region_at (features/intersection.ts:1121-1225): innermost-wins point classification
+    int scene_region_at(v3 p) const {
+        int region = -1;
+        float best = -1.0e20f;
+        for (int i = 0; i < d->n_regions; ++i) {
+            const ptr_region& g = d->regions[i];
+            float dd;
+            switch (g.shape) {
+                case PTR_SHAPE_PLANE: dd = plane_sdf(p, ld3(g.p), g.p[3]); break;
+                case PTR_SHAPE_SPHERE: dd = sphere_sdf(p, ld3(g.p), g.p[3]); break;
+                case PTR_SHAPE_BOX: dd = box_sdf(p, ld3(g.p), ld3(g.p + 3)); break;
+                default: dd = 1.0e20f; break;   // thin owners never claim containment
+            }
+            if (dd < 0.0f && dd > best) { best = dd; region = i; }
+        }
+        return region;
+    }
+    // scene_intersect (features/intersection.ts:1665-1713 generateSceneIntersect)
+    bool scene_intersect(const Ray& r, Hit& hit) const {
+        hit.t = MAX_DIST;
+        hit.eps = MARCH_CLEARANCE;
+        bool found = primitive_intersect(r, hit);
+        if (found) {
+            int outside = scene_region_at(hit.p + hit.ng * EPS_INTERFACE);
+            if (dot(r.d, hit.ng) < 0.0f) {
+                hit.region_from = outside;
+                hit.region_to = hit.region_owner;
+            } else {
+                hit.region_from = d->regions[hit.region_owner].thin
+                    ? scene_region_at(hit.p + hit.ng * (-EPS_INTERFACE))
+                    : hit.region_owner;
+                hit.region_to = outside;
+                hit.frame = ambient_frame(-hit.frame.n);
+                hit.ng = -hit.ng;
+            }
+        }
+        return found;
+    }
+};
+
+// ---------------------------------------------------------------- materials
+// lambert (materials/lambert/lambert.glsl:7-37)
+inline v3 lambert_eval(v3 wi, v3 wo, const Hit& h, const ptr_material& m) {
+    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return v3(0.0f);
+    return ld3(m.albedo) * (1.0f / PI);
+}
+inline ISample lambert_sample(v3 wo, const Hit& h, const ptr_material& m, float, float u0, float u1) {
+    const Frame& f = h.frame;
+    v3 n = dot(wo, f.n) < 0.0f ? -f.n : f.n;
+    float cos_theta = std::sqrt(u1);
+    float sin_theta = std::sqrt(fmaxf_(0.0f, 1.0f - u1));
+    float phi = TWO_PI * u0;
+    ISample s;
+    s.wi = normalize(f.t * (sin_theta * std::cos(phi)) + f.b * (sin_theta * std::sin(phi)) + n * cos_theta);
+    s.weight = ld3(m.albedo);
+    s.pdf = cos_theta * (1.0f / PI);
+    s.flags = LOBE_REFLECTION;
+    return s;
+}
+inline float lambert_pdf(v3 wi, v3 wo, const Hit& h) {
+    float c = dot(wi, h.frame.n) * signf(dot(wo, h.frame.n));
+    return fmaxf_(0.0f, c) * (1.0f / PI);
+}
+// microfacet (glsl/core/microfacet.glsl:22-54)
+inline v3 mf_to_local(const Frame& f, v3 v) { return v3(dot(v, f.t), dot(v, f.b), dot(v, f.n)); }
+inline v3 mf_from_local(const Frame& f, v3 v) { return normalize(f.t * v.x + f.b * v.y + f.n * v.z); }
+inline float mf_D(v3 h, float a) { float t = h.z * h.z * (a * a - 1.0f) + 1.0f; return a * a / (PI * t * t); }
+inline float mf_G1(v3 v, float a) { float c = std::fabs(v.z); return 2.0f * c / (c + std::sqrt(a * a + (1.0f - a * a) * c * c)); }
+inline v3 mf_sample_vndf(v3 wol, float a, float u0, float u1) {
+    v3 vh = normalize(v3(a * wol.x, a * wol.y, wol.z));
+    float lensq = vh.x * vh.x + vh.y * vh.y;
+    v3 T1 = lensq > 0.0f ? v3(-vh.y, vh.x, 0.0f) * (1.0f / std::sqrt(lensq)) : v3(1, 0, 0);
+    v3 T2 = cross(vh, T1);
+    float rr = std::sqrt(u0);
+    float phi = TWO_PI * u1;
+    float t1 = rr * std::cos(phi);
+    float t2 = rr * std::sin(phi);
+    float s_ = 0.5f * (1.0f + vh.z);
+    t2 = (1.0f - s_) * std::sqrt(fmaxf_(0.0f, 1.0f - t1 * t1)) + s_ * t2;
+    v3 nh = t1 * T1 + t2 * T2 + std::sqrt(fmaxf_(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
+    return normalize(v3(a * nh.x, a * nh.y, fmaxf_(1e-6f, nh.z)));
+}
+// ggx conductor (materials/ggx/ggx.glsl:16-64)
+inline v3 ggx_eval(v3 wi, v3 wo, const Hit& h, const ptr_material& m, float a) {
+    v3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+    if (wil.z * wol.z <= 0.0f) return v3(0.0f);
+    v3 hh = normalize(wil + wol);
+    v3 F = schlick_fresnel(ld3(m.f0), std::fabs(dot(wol, hh)));
+    return F * (mf_D(hh, a) * mf_G1(wil, a) * mf_G1(wol, a) / (4.0f * std::fabs(wil.z) * std::fabs(wol.z)));
+}
+inline ISample ggx_sample(v3 wo, const Hit& h, const ptr_material& m, float a, float u0, float u1) {
+    v3 wol = mf_to_local(h.frame, wo);
+    float side = wol.z < 0.0f ? -1.0f : 1.0f;
+    wol = wol * side;
+    v3 hh = mf_sample_vndf(wol, a, u0, u1);
+    v3 i = -wol;
+    v3 wil = i - 2.0f * dot(hh, i) * hh;   // reflect(-wol, h)
+    ISample s;
+    if (wil.z <= 0.0f) { s.wi = wo; s.weight = v3(0.0f); s.pdf = 0.0f; s.flags = LOBE_REFLECTION; return s; }
+    v3 F = schlick_fresnel(ld3(m.f0), std::fabs(dot(wol, hh)));
+    s.weight = F * mf_G1(wil, a);
+    s.pdf = mf_G1(wol, a) * mf_D(hh, a) / (4.0f * std::fabs(wol.z));
+    s.flags = LOBE_REFLECTION;
+    s.wi = mf_from_local(h.frame, wil * side);
+    return s;
+}
+inline float ggx_pdf(v3 wi, v3 wo, const Hit& h, float a) {
+    v3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+    if (wil.z * wol.z <= 0.0f) return 0.0f;
+    v3 hh = normalize(wil + wol);
+    return mf_G1(wol, a) * mf_D(hh, a) / (4.0f * std::fabs(wol.z));
+}
+
+// ---------------------------------------------------------------- media (transport/volume/analytic)
+struct MediumSample { bool scattered; float t; v3 weight; v3 exit_p, exit_dir; };
+// medium_sample_analytic (transport/volume/analytic/analytic.glsl:9-43)
+inline MediumSample medium_sample_analytic(const ptr_material& m, const Ray& r, float t_max, float x0, float x1) {
+    v3 sigma_t = ld3(m.sigma_a) + ld3(m.sigma_s);
+    int c = spectrum_sample_channel(x0);
+    float sc = sigma_t[c];
+    float t = sc == 0.0f ? t_max : -std::log(1.0f - x1) / sc;
+    MediumSample ms;
+    if (t < t_max) {
+        v3 tr = vexp(-sigma_t * t);
+        float pdf = spectrum_average(sigma_t * tr);
+        ms.scattered = true;
+        ms.t = t;
+        ms.exit_p = r.o + r.d * t;
+        ms.exit_dir = r.d;
+        ms.weight = ld3(m.sigma_s) * tr / fmaxf_(pdf, 1e-20f);
+    } else {
+        v3 tr = vexp(-sigma_t * t_max);
+        float pdf = spectrum_average(tr);
+        ms.scattered = false;
+        ms.t = t_max;
+        ms.weight = tr / fmaxf_(pdf, 1e-20f);
+    }
+    return ms;
+}
+// hg (volume_scattering/hg/hg.glsl:11-42) — forward convention
+inline float hg_eval(v3 wi, v3 wo, float g) {
+    float c = dot(wi, -wo);
+    float d = 1.0f + g * g - 2.0f * g * c;
+    return (1.0f - g * g) / (4.0f * PI * d * std::sqrt(fmaxf_(d, 1e-8f)));
+}
+inline ISample hg_sample(v3 wo, float g, float x0, float x1) {
+    float cos_theta;
+    if (std::fabs(g) < 1e-3f) cos_theta = 1.0f - 2.0f * x0;
+    else {
+        float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * x0);
+        cos_theta = (1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    float sin_theta = std::sqrt(fmaxf_(0.0f, 1.0f - cos_theta * cos_theta));
+    float phi = TWO_PI * x1;
+    v3 t, b;
+    build_basis(-wo, t, b);
+    ISample s;
+    s.wi = normalize(t * (sin_theta * std::cos(phi)) + b * (sin_theta * std::sin(phi)) + (-wo) * cos_theta);
+    s.weight = v3(1.0f);
+    s.pdf = spectrum_average(v3(hg_eval(s.wi, wo, g)));
+    s.flags = LOBE_MEDIUM;
+    return s;
+}
+
+// ---------------------------------------------------------------- the renderer
+struct Counters { uint64_t closest = 0, shadow = 0; };
+
+struct Tracer {
+    const Scene& S;
+    const ptr_scene_desc& d;
+    const ptr_program_desc& P;
+    Rng rng;
+    Counters cnt;
+    Tracer(const Scene& s) : S(s), d(*s.d), P(*s.prog) {}
+
+    bool intersect(const Ray& r, Hit& h) { cnt.closest++; return S.scene_intersect(r, h); }
+
+    // ---- environment (features/environment.ts:109-252; constant env T3 sampler)
+    v3 environment_radiance(v3) const {
+        if (d.env.kind == PTR_ENV_CONSTANT) return ld3(d.env.color) * d.env.intensity;
+        return v3(0.0f);
+    }
+    LightSample environment_sample(float x0, float x1) const {
+        LightSample ls;
+        float z = 1.0f - 2.0f * x0;
+        float r = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
+        float phi = TWO_PI * x1;
+        ls.wi = v3(r * std::cos(phi), z, r * std::sin(phi));
+        ls.distance = MAX_DIST;
+        ls.radiance = ld3(d.env.color) * d.env.intensity;
+        ls.pdf = 1.0f / (4.0f * PI);
+        ls.flags = 0u;
+        ls.light_id = -1;
+        return ls;
+    }
+    float environment_pdf(v3) const { return 1.0f / (4.0f * PI); }
+
+    // ---- lights (lights/quad/quad.glsl:14-41, sphere/sphere.glsl:21-71, point/point.glsl:11-23)
+    LightSample light_sample_one(const ptr_light& l, v3 p, float x0, float x1) const {
+        LightSample ls;
+        ls.radiance = ld3(l.radiance);
+        ls.flags = 0u;
+        ls.light_id = -1;
+        if (l.kind == PTR_LIGHT_QUAD) {
+            v3 corner = ld3(l.p), e1 = ld3(l.p + 3), e2 = ld3(l.p + 6), nrm = ld3(l.p + 9);
+            float area = l.p[12];
+            v3 q = corner + x0 * e1 + x1 * e2;
+            v3 dd = q - p;
+            float d2 = dot(dd, dd);
+            ls.wi = dd * (1.0f / std::sqrt(d2));
+            ls.distance = std::sqrt(d2);
+            float cos_l = dot(nrm, -ls.wi);
+            if (cos_l <= 0.0f) { ls.pdf = 0.0f; return ls; }
+            ls.pdf = d2 / (area * cos_l);
+            return ls;
+        }
+        if (l.kind == PTR_LIGHT_SPHERE) {
+            v3 c = ld3(l.p);
+            float r = l.p[3];
+            v3 to_c = c - p;
+            float dc2 = dot(to_c, to_c);
+            if (dc2 <= r * r) { ls.wi = v3(0, 1, 0); ls.distance = 1.0f; ls.pdf = 0.0f; return ls; }
+            float sin2_max = r * r / dc2;
+            float omc_max = sin2_max / (1.0f + std::sqrt(fmaxf_(0.0f, 1.0f - sin2_max)));
+            float w_t = x0 * omc_max;
+            float cos_t = 1.0f - w_t;
+            float sin_t = std::sqrt(fmaxf_(0.0f, w_t * (2.0f - w_t)));
+            float phi = TWO_PI * x1;
+            v3 w = to_c * (1.0f / std::sqrt(dc2));
+            v3 t, b;
+            build_basis(w, t, b);
+            ls.wi = normalize(t * (sin_t * std::cos(phi)) + b * (sin_t * std::sin(phi)) + w * cos_t);
+            ls.pdf = 1.0f / (TWO_PI * omc_max);
+            float proj = dot(to_c, ls.wi);
+            v3 perp = to_c - proj * ls.wi;
+            float disc = fmaxf_(0.0f, r * r - dot(perp, perp));
+            ls.distance = (dc2 - r * r) / (proj + std::sqrt(disc));
+            return ls;
+        }
+        // point (delta): radiance = I / d^2 folded in, pdf 1 (point.glsl:11-23)
+        v3 pos = ld3(l.p);
+        v3 dd = pos - p;
+        float d2 = dot(dd, dd);
+        ls.wi = dd * (1.0f / std::sqrt(d2));
+        ls.distance = std::sqrt(d2);
+        ls.radiance = ld3(l.radiance) / d2;
+        ls.pdf = 1.0f;
+        ls.flags = LIGHT_DELTA;
+        return ls;
+    }
+    float light_pdf_one(const ptr_light& l, v3 p, v3 light_p, v3 wi) const {
+        if (l.kind == PTR_LIGHT_QUAD) {
+            float cos_l = dot(ld3(l.p + 9), -wi);
+            if (cos_l <= 0.0f) return 0.0f;
+            v3 dd = light_p - p;
+            return dot(dd, dd) / (l.p[12] * cos_l);
+        }
+        if (l.kind == PTR_LIGHT_SPHERE) {
+            v3 to_c = ld3(l.p) - p;
+            float dc2 = dot(to_c, to_c);
+            float r = l.p[3];
+            if (dc2 <= r * r) return 0.0f;
+            float sin2_max = r * r / dc2;
+            float omc = sin2_max / (1.0f + std::sqrt(fmaxf_(0.0f, 1.0f - sin2_max)));
+            return 1.0f / (TWO_PI * omc);
+        }
+        return 0.0f;
+    }
+    // lighting_sample_finite: power CDF + cdf_rescale (features/lighting.ts:546-637)
+    LightSample lighting_sample_finite(v3 p, float x0, float x1) const {
+        LightSample ls;
+        if (d.n_lights == 1) {
+            ls = light_sample_one(d.lights[0], p, x0, x1);
+            ls.light_id = 0;
+            return ls;
+        }
+        int id = d.n_lights - 1;
+        for (int i = 0; i < d.n_lights - 1; ++i)
+            if (x0 < d.lights[i].select_cdf) { id = i; break; }
+        float lo = id == 0 ? 0.0f : d.lights[id - 1].select_cdf;
+        float sel = d.lights[id].select_pdf;
+        float xr = (x0 - lo) / sel;
+        ls = light_sample_one(d.lights[id], p, clampf(xr, 0.0f, 0.9999999f), x1);
+        ls.light_id = id;
+        ls.pdf *= sel;
+        return ls;
+    }
+    // lighting_sample: two-stage env-vs-finite (features/lighting.ts generateLightSampling)
+    LightSample lighting_sample(v3 p, float x0, float x1) const {
+        if (d.n_lights == 0) {
+            if (S.env_samplable) return environment_sample(x0, x1);
+            LightSample ls; ls.pdf = 0.0f; return ls;
+        }
+        if (!S.env_select_live) return lighting_sample_finite(p, x0, x1);
+        float pe = d.env.select_prob;
+        if (x0 < pe) {
+            LightSample ls = environment_sample(clampf(x0 / pe, 0.0f, 0.9999999f), x1);
+            ls.pdf *= pe;
+            return ls;
+        }
+        float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
+        LightSample ls = lighting_sample_finite(p, fx, x1);
+        ls.pdf *= (1.0f - pe);
+        return ls;
+    }
+    // lighting_pdf (features/lighting.ts:639-693)
+    float lighting_pdf(v3 qp, v3 wi, int lid, const Hit& lh) const {
+        const ptr_light& l = d.lights[lid];
+        float sel = d.n_lights == 1 ? 1.0f : l.select_pdf;
+        float pe = S.env_select_live ? (1.0f - d.env.select_prob) : 1.0f;
+        return sel * pe * light_pdf_one(l, qp, lh.p, wi);
+    }
+
+    // ---- material dispatch (features/materials.ts:902-954)
+    float alpha_of(const ptr_material& m) const { return m.alpha; }
+    ISample surface_sample(const ptr_material& m, v3 wo, const Hit& h, float uc, float u0, float u1) const {
+        if (m.model == PTR_MAT_LAMBERT) return lambert_sample(wo, h, m, uc, u0, u1);
+        if (m.model == PTR_MAT_GGX) return ggx_sample(wo, h, m, alpha_of(m), u0, u1);
+        // dielectric (materials/dielectric/dielectric.glsl:14-52)
+        float n_i = S.ior_of(h.region_from), n_t = S.ior_of(h.region_to);
+        float eta = n_i / n_t;
+        v3 n = h.frame.n;
+        float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
+        float F = dielectric_fresnel(cos_i, eta);
+        ISample s;
+        if (uc < F) {
+            s.wi = normalize(2.0f * cos_i * n - wo);
+            s.weight = v3(1.0f);
+            s.pdf = 0.0f;
+            s.flags = LOBE_REFLECTION | LOBE_DELTA;
+        } else {
+            float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+            float cos_t = std::sqrt(fmaxf_(0.0f, 1.0f - sin2_t));
+            s.wi = normalize(-eta * wo + (eta * cos_i - cos_t) * n);
+            float radiance_scale = (n_i * n_i) / (n_t * n_t);
+            s.weight = ld3(m.transmittance) * radiance_scale;
+            s.pdf = 0.0f;
+            s.flags = LOBE_TRANSMISSION | LOBE_DELTA;
+        }
+        return s;
+    }
+    v3 surface_eval(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
+        if (m.model == PTR_MAT_LAMBERT) return lambert_eval(wi, wo, h, m);
+        if (m.model == PTR_MAT_GGX) return ggx_eval(wi, wo, h, m, alpha_of(m));
+        return v3(0.0f);
+    }
+    float surface_pdf(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
+        if (m.model == PTR_MAT_LAMBERT) return lambert_pdf(wi, wo, h);
+        if (m.model == PTR_MAT_GGX) return ggx_pdf(wi, wo, h, alpha_of(m));
+        return 0.0f;
+    }
+
+    // ---- media dispatch (features/materials.ts:675-866)
+    // a medium scatters when it has sigma_s and measurement.scattering is 'full'
+    bool scatter_live(int med) const { return P.scattering && (d.materials[med].flags & PTR_MATF_SCATTERING); }
+    // medium_transmittance (analytic.glsl:49-51): Beer-Lambert over sigma_t; under
+    // scattering 'ignored' the medium is absorbing-only (sigma_t = sigma_a)
+    v3 medium_transmittance(int med, float len) const {
+        const ptr_material& m = d.materials[med];
+        v3 st = scatter_live(med) ? ld3(m.sigma_a) + ld3(m.sigma_s) : ld3(m.sigma_a);
+        return vexp(-st * len);
+    }
+    v3 medium_survival(int med) const {
+        const ptr_material& m = d.materials[med];
+        v3 sa = ld3(m.sigma_a), ss = ld3(m.sigma_s);
+        return ss / vmax(ss + sa, v3(1e-9f));
+    }
+
+    // shadow_transmittance: opaque (transport/shadow/opaque/opaque.glsl:16-19) or the
+    // media segment walker (transport/shadow/media/media.glsl:29-62)
+    v3 shadow_transmittance(Ray sr, v3 light_p, int crossings_left) {
+        cnt.shadow++;
+        if (!S.has_media) {
+            float maxDist = length(light_p - sr.o) - SHADOW_BACKOFF;
+            return S.scene_intersect_any(sr, maxDist) ? v3(0.0f) : v3(1.0f);
+        }
+        v3 T(1.0f);
+        int medium = S.scene_region_at(sr.o);
+        Ray seg = sr;
+        for (int crossed = 0; crossed <= crossings_left; crossed++) {
+            float remaining = length(light_p - seg.o) - SHADOW_BACKOFF;
+            if (remaining <= 0.0f) return T;
+            Hit h;
+            bool hit_boundary = S.scene_intersect(seg, h) && h.t < remaining;
+            float seg_len = hit_boundary ? h.t : remaining;
+            int med_mat = S.material_of(medium);
+            if (S.material_has_medium(med_mat)) T = T * medium_transmittance(med_mat, seg_len);
+            if (!hit_boundary) return T;
+            if (!S.is_null_interface(S.material_of(h.region_owner))) return v3(0.0f);
+            medium = h.region_to;
+            seg = ray_spawn(h, seg.d);
+            seg.d = normalize(light_p - seg.o);
+        }
+        return v3(0.0f);
+    }
+
+    static float power_heuristic(float pf, float pg) {
+        float f2 = pf * pf;
+        if (f2 >= 1.0e38f) return 1.0f;
+        return f2 / fmaxf_(1e-20f, f2 + pg * pg);
+    }
+
+    // ---- the walk (transport/integrators/pt/pt.ts:299-464, as emitted for media scenes)
+    v3 transport_trace(Ray ray) {
+        const bool nee = P.direct != PTR_DIRECT_NONE;
+        const bool mis = P.direct == PTR_DIRECT_MIS;
+        const bool media = S.has_media;
+        const int N = P.max_bounces;
+        // path_state_init (pt.ts:147-176)
+        v3 throughput(1.0f), radiance(0.0f);
+        bool prev_was_delta = true;
+        float prev_bsdf_pdf = 0.0f;
+        v3 prev_qp = ray.o;
+        float eta_scale = 1.0f;
+        int current_medium = media ? S.scene_region_at(ray.o) : -1;
+        int null_crossings = 0;
+        Ray r = ray;
+
+        auto roulette = [&](int bounce) -> bool {   // pt.ts:204-222
+            if (P.rr_start < 0) return true;
+            if (bounce < P.rr_start) return true;
+            float p_survive = fminf_(P.rr_max_survival, spectrum_max(throughput) * eta_scale);
+            if (p_survive <= 0.0f) return false;
+            if (rng.next() > p_survive) return false;
+            throughput = throughput / p_survive;
+            return true;
+        };
+        auto roulette_interior = [&](int bounce, v3 survival) -> bool {   // pt.ts:230-283
+            if (P.rr_start < 0) return true;
+            if (bounce < P.rr_start) return true;
+            float p_survive = spectrum_max(survival);
+            if (p_survive <= 0.0f) return false;
+            if (rng.next() > p_survive) return false;
+            throughput = throughput / p_survive;
+            return true;
+        };
+        auto w_emitter = [&](const Hit& hit) -> float {   // combiner.ts:27-46
+            if (!nee) return 1.0f;
+            int lid = hit.region_to >= 0 ? S.light_of_region[hit.region_to] : -1;
+            if (lid < 0 || prev_was_delta) return 1.0f;
+            if (!mis) return 0.0f;
+            return power_heuristic(prev_bsdf_pdf, lighting_pdf(prev_qp, r.d, lid, hit));
+        };
+        auto w_env = [&]() -> float {   // combiner.ts:49-65
+            if (!(S.env_samplable && nee)) return 1.0f;
+            if (prev_was_delta) return 1.0f;
+            if (!mis) return 0.0f;
+            float pe = S.env_select_live ? d.env.select_prob : 1.0f;
+            return power_heuristic(prev_bsdf_pdf, pe * environment_pdf(r.d));
+        };
+        int shadow_left_base = P.max_null_crossings;
+
+        for (int bounce = 0; bounce <= N; bounce++) {
+            Hit hit;
+            bool boundary = intersect(r, hit);
+            if (media) {
+                // the volumetric call site (pt.ts walk): one segment, random2() drawn for
+                // every medium arm, scattering or absorbing-only (features/materials.ts:675-746)
+                int med_mat = S.material_of(current_medium);
+                if (S.material_has_medium(med_mat)) {
+                    float x0 = rng.next(), x1 = rng.next();
+                    float t_max = boundary ? hit.t : MAX_DIST;
+                    const ptr_material& mm = d.materials[med_mat];
+                    if (!scatter_live(med_mat)) {
+                        // absorbing-only arm (deterministic): weight = exp(-sigma_a t_max)
+                        throughput = throughput * vexp(-ld3(mm.sigma_a) * t_max);
+                    } else {
+                        MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
+                        throughput = throughput * ms.weight;
+                        if (ms.scattered) {
+                            if (bounce == N) break;
+                            v3 p_evt = ms.exit_p;
+                            v3 wo_med = -ms.exit_dir;
+                            // light_sample_direct_medium (techniques/light/light_medium.glsl:7-18)
+                            if (nee) {
+                                float y0 = rng.next(), y1 = rng.next();
+                                LightSample ls = lighting_sample(p_evt, y0, y1);
+                                if (ls.pdf > 0.0f) {
+                                    v3 light_p = p_evt + ls.wi * ls.distance;
+                                    v3 vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings);
+                                    if (!spectrum_is_black(vis)) {
+                                        float w = 1.0f;
+                                        if (mis && !(ls.flags & LIGHT_DELTA))
+                                            w = power_heuristic(ls.pdf, hg_eval(ls.wi, wo_med, mm.phase_g));
+                                        radiance = radiance + throughput * ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
+                                    }
+                                }
+                            }
+                            // kernel_sample_phase (techniques/kernel/kernel_phase.glsl:7-15)
+                            float z0 = rng.next(), z1 = rng.next();
+                            ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
+                            throughput = throughput * ps.weight;
+                            prev_was_delta = false;
+                            prev_bsdf_pdf = ps.pdf;
+                            prev_qp = p_evt;
+                            r = Ray{p_evt, ps.wi};
+                            if (!roulette_interior(bounce, medium_survival(med_mat))) break;
+                            continue;
+                        }
+                    }
+                }
+            }
+            if (!boundary) {   // kernel_score_miss (kernel.glsl:11-14)
+                radiance = radiance + throughput * w_env() * environment_radiance(r.d);
+                break;
+            }
+            if (media && hit.region_from != current_medium) current_medium = hit.region_from;
+            int mat = S.material_of(hit.region_owner);
+            if (media && S.is_null_interface(mat)) {   // pt.ts:404-417 null pass-through
+                current_medium = hit.region_to;
+                r = ray_spawn(hit, r.d);
+                null_crossings++;
+                if (null_crossings > P.max_null_crossings) break;
+                bounce--;
+                continue;
+            }
+            v3 wo = -r.d;
+            // kernel_score_emitter_hit (kernel.glsl:16-25)
+            int mat_emit = S.material_of(hit.region_to);
+            if (S.material_is_emissive(mat_emit))
+                radiance = radiance + throughput * w_emitter(hit) * ld3(d.materials[mat_emit].emission);
+            if (bounce == N) break;
+            const ptr_material& m = d.materials[mat];
+            // light_sample_direct (techniques/light/light.glsl:8-28)
+            if (nee && S.material_has_nondelta_lobes(mat)) {
+                float y0 = rng.next(), y1 = rng.next();
+                LightSample ls = lighting_sample(hit.p, y0, y1);
+                if (ls.pdf > 0.0f) {
+                    v3 light_p = hit.p + ls.wi * ls.distance;
+                    Ray sr = ray_spawn(hit, ls.wi);
+                    sr.d = normalize(light_p - sr.o);
+                    v3 vis = shadow_transmittance(sr, light_p, shadow_left_base - null_crossings);
+                    if (!spectrum_is_black(vis)) {
+                        v3 f = surface_eval(m, ls.wi, wo, hit);
+                        float cos_i = std::fabs(dot(ls.wi, hit.frame.n));
+                        float w = 1.0f;
+                        if (mis && !(ls.flags & LIGHT_DELTA)) w = power_heuristic(ls.pdf, surface_pdf(m, ls.wi, wo, hit));
+                        radiance = radiance + throughput * ls.radiance * f * cos_i * vis * w / ls.pdf;
+                    }
+                }
+            }
+            // kernel_sample_continuation (kernel.glsl:27-34)
+            float uc = rng.next();
+            float u0 = rng.next(), u1 = rng.next();
+            ISample bs = surface_sample(m, wo, hit, uc, u0, u1);
+            if (spectrum_is_black(bs.weight)) break;
+            throughput = throughput * bs.weight;
+            prev_was_delta = (bs.flags & LOBE_DELTA) != 0u;
+            prev_bsdf_pdf = bs.pdf;
+            prev_qp = hit.p;
+            if (bs.flags & LOBE_TRANSMISSION) {
+                if (media) current_medium = hit.region_to;
+                float rr = S.ior_of(hit.region_to) / S.ior_of(hit.region_from);   // pt.ts:447-455
+                eta_scale *= rr * rr;
+            }
+            if (!roulette(bounce)) break;
+            r = ray_spawn(hit, bs.wi);
+        }
+        return radiance;
+    }
+};
+
+// camera_generateRay (camera/pinhole/pinhole.glsl:4-18) + pixel_sample (pixel/box/box.glsl:5)
+inline Ray camera_ray(const ptr_camera& c, int W, int H, float fx, float fy) {
+    float ndcx = (2.0f * fx / (float)W) - 1.0f;
+    float ndcy = (2.0f * fy / (float)H) - 1.0f;
+    ndcx *= c.aspect;
+    v3 dir = normalize(ld3(c.forward) + ndcx * c.tan_fov * ld3(c.right) + ndcy * c.tan_fov * ld3(c.up));
+    return Ray{ld3(c.position), dir};
+}
+
+}  // namespace
+
+extern "C" {
+
+// Render frame->spp samples for every pixel; accumulate per-pixel sum / sum of squares
+// (float64, 3 per pixel, row 0 = bottom).  Returns counters through out_counts[2]
+// (closest-hit queries, shadow queries) when non-null.
+int oracle_render(const ptr_scene_desc* sd, const ptr_program_desc* pd, const ptr_frame* fr,
+                  double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
+    if (!sd || !pd || !fr) return -1;
+    Scene S(sd, pd);
+    const int W = fr->width, H = fr->height;
+    uint64_t closest = 0, shadow = 0;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel reduction(+ : closest, shadow)
+    {
+        Tracer T(S);
+#pragma omp for schedule(dynamic, 1)
+        for (int y = 0; y < H; ++y) {
+            for (int x = 0; x < W; ++x) {
+                size_t pix = (size_t)y * W + x;
+                for (int k = 0; k < fr->spp; ++k) {
+                    uint32_t px = (uint32_t)(x + fr->pixel_offset[0]);
+                    uint32_t py = (uint32_t)(y + fr->pixel_offset[1]);
+                    T.rng.init(px, py, (uint32_t)(fr->first_sample + k), fr->reset_salt);
+                    // main(): pixel = gl_FragCoord + offset; film = pixel + (xi - 0.5)
+                    float pxf = (float)x + 0.5f + (float)fr->pixel_offset[0];
+                    float pyf = (float)y + 0.5f + (float)fr->pixel_offset[1];
+                    float a0 = T.rng.next(), a1 = T.rng.next();
+                    float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+                    T.rng.next(); T.rng.next();   // xiLens (pinhole ignores it)
+                    Ray r = camera_ray(fr->camera, W, H, fx, fy);
+                    v3 L = T.transport_trace(r);
+                    if (samples_out) {
+                        float* o = samples_out + 3 * ((size_t)k * W * H + pix);
+                        o[0] = L.x; o[1] = L.y; o[2] = L.z;
+                    }
+                    if (sum) {
+                        for (int c = 0; c < 3; ++c) {
+                            sum[3 * pix + c] += (double)L[c];
+                            sumsq[3 * pix + c] += (double)L[c] * (double)L[c];
+                        }
+                    }
+                }
+            }
+        }
+        closest += T.cnt.closest;
+        shadow += T.cnt.shadow;
+    }
+    if (out_counts) { out_counts[0] = closest; out_counts[1] = shadow; }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+"""ctypes mirror of ``include/ptx_rt.h`` (the C ABI of the transport loop).
+
+Every structure here has the exact layout of its C counterpart; ``tests/`` checks
+the sizes against the header.  Both the CUDA engine and the oracle bindings build
+their descriptors from these types, so the two consume byte-identical scenes.
+"""
+import ctypes as C
+
+ABI_VERSION = 1
+
+PTR_OK = 0
+PTR_E_INVALID = -1
+PTR_E_CUDA = -2
+PTR_E_NOMEM = -3
+PTR_E_TIMEOUT = -4
+PTR_E_DEVICE = -5
+PTR_E_UNSUPPORTED = -6
+
+SHAPE_PLANE, SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_MESH, SHAPE_INSTANCES = range(6)
+MAT_LAMBERT, MAT_DIELECTRIC, MAT_GGX, MAT_MIRROR, MAT_NONE = range(5)
+MATF_EMISSIVE, MATF_MEDIUM, MATF_SCATTERING = 1, 2, 4
+LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT = range(3)
+ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)
+DIRECT_NONE, DIRECT_NEE, DIRECT_MIS = range(3)
+ACCEL_BVH, ACCEL_CWBVH = range(2)
+
+F4 = C.c_float * 4
+
+
+class Region(C.Structure):
+    _fields_ = [("shape", C.c_int32), ("material", C.c_int32), ("thin", C.c_int32),
+                ("ref", C.c_int32), ("ior", C.c_float), ("p", C.c_float * 15)]
+
+
+class Material(C.Structure):
+    _fields_ = [("model", C.c_int32), ("flags", C.c_int32), ("pad0", C.c_int32), ("pad1", C.c_int32),
+                ("albedo", F4), ("emission", F4), ("transmittance", F4), ("f0", F4),
+                ("sigma_a", F4), ("sigma_s", F4), ("alpha", C.c_float), ("phase_g", C.c_float),
+                ("pad2", C.c_float), ("pad3", C.c_float)]
+
+
+class Light(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("region", C.c_int32), ("select_pdf", C.c_float),
+                ("select_cdf", C.c_float), ("radiance", F4), ("p", C.c_float * 16)]
+
+
+class Env(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("sample_as_light", C.c_int32), ("width", C.c_int32),
+                ("height", C.c_int32), ("color", F4), ("intensity", C.c_float),
+                ("select_prob", C.c_float), ("rotation", C.c_float), ("pad", C.c_float),
+                ("radiance", C.POINTER(C.c_float)), ("marginal", C.POINTER(C.c_float)),
+                ("conditional", C.POINTER(C.c_float))]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_vertices", C.c_int32), ("n_triangles", C.c_int32),
+                ("positions", C.POINTER(C.c_float)), ("indices", C.POINTER(C.c_uint32)),
+                ("tri_alpha", C.POINTER(C.c_float))]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("prototype_shape", C.c_int32), ("prototype_ref", C.c_int32),
+                ("n_instances", C.c_int32), ("pad", C.c_int32), ("proto", F4),
+                ("placements", C.POINTER(C.c_float))]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("n_regions", C.c_int32), ("regions", C.POINTER(Region)),
+                ("n_materials", C.c_int32), ("materials", C.POINTER(Material)),
+                ("n_lights", C.c_int32), ("lights", C.POINTER(Light)),
+                ("ambient_material", C.c_int32), ("env", Env),
+                ("n_meshes", C.c_int32), ("meshes", C.POINTER(MeshDesc)),
+                ("n_batches", C.c_int32), ("batches", C.POINTER(BatchDesc))]
+
+
+class ProgramDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_int32), ("max_bounces", C.c_int32),
+                ("max_null_crossings", C.c_int32), ("direct", C.c_int32), ("rr_start", C.c_int32),
+                ("rr_max_survival", C.c_float), ("scattering", C.c_int32), ("accel", C.c_int32),
+                ("equiangular", C.c_int32), ("pad", C.c_int32 * 7)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3),
+                ("up", C.c_float * 3), ("tan_fov", C.c_float), ("aspect", C.c_float)]
+
+
+class Frame(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("first_sample", C.c_int32),
+                ("spp", C.c_int32), ("reset_salt", C.c_uint32), ("pixel_offset", C.c_int32 * 2),
+                ("accumulate", C.c_int32), ("camera", Camera)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("closest_queries", C.c_uint64), ("shadow_queries", C.c_uint64),
+                ("nodes_visited", C.c_uint64), ("prims_tested", C.c_uint64),
+                ("error_flags", C.c_uint32), ("pad", C.c_uint32)]
+
+
+# Sizes the header documents (checked by the CPU tests).
+EXPECTED_SIZES = {"Region": 80, "Material": 128, "Light": 96}

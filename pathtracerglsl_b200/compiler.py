@@ -1,0 +1,672 @@
+"""SceneDescription + RenderStrategy -> CompiledRenderer + packed scene data.
+
+Host mirror of the reference's Compiler for the transport-loop path
+(``src/compiler/Compiler.ts:14-72``: Analyze -> Validate -> Plan -> Generate).  The
+"Generate" stage here emits no shader text: it packs the plan into the flat tables of
+``include/ptx_rt.h`` that the CUDA kernels read (the unrolled arms the GLSL emitter bakes
+as literals become table rows), plus a ``ptr_program_desc`` with the estimator knobs.
+
+Inputs use the reference's own JSON shapes (``src/compiler/types.ts:21-721``): objects
+``{type, parameters, material}``, materials ``{model, albedo, emission, ior, roughness,
+f0, medium}``, lights ``{kind, emission, ...}``, ``environment``, ``ambientMedium``,
+strategies ``{id, measurement, estimator, view}``.  Errors are collected in a
+DiagnosticBag and raised together (``src/errors/DiagnosticBag.ts:310`` throwIfErrors).
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+# ----------------------------------------------------------------------------- diagnostics
+
+
+class Diagnostic:
+    def __init__(self, severity, code, message):
+        self.severity, self.code, self.message = severity, code, message
+
+    def __repr__(self):
+        return f"{self.severity}[{self.code}]: {self.message}"
+
+
+class CompileError(Exception):
+    """All errors of one compile, like ``DiagnosticBag.throwIfErrors``."""
+
+    def __init__(self, diagnostics):
+        self.diagnostics = diagnostics
+        super().__init__("; ".join(f"[{d.code}] {d.message}" for d in diagnostics))
+
+
+class DiagnosticBag:
+    def __init__(self):
+        self.items = []
+
+    def error(self, code, message):
+        self.items.append(Diagnostic("error", code, message))
+
+    def warning(self, code, message):
+        self.items.append(Diagnostic("warning", code, message))
+
+    @property
+    def errors(self):
+        return [d for d in self.items if d.severity == "error"]
+
+    @property
+    def warnings(self):
+        return [d for d in self.items if d.severity == "warning"]
+
+    def throw_if_errors(self):
+        if self.errors:
+            raise CompileError(self.errors)
+
+
+# ----------------------------------------------------------------------------- values
+
+def is_param(v):
+    return isinstance(v, dict) and "param" in v
+
+
+def resolve(v, params, default=None):
+    """``Value<T>`` -> concrete value: constants as is, ``{param}`` from ``params`` or
+    its default (contracts §2.8 in the reference's types.ts:257-275)."""
+    if v is None:
+        return default
+    if is_param(v):
+        return params.get(v["param"], v.get("default", default))
+    return v
+
+
+def rgb(v, params, default):
+    """A SpectrumProperty as RGB: scalars broadcast (types.ts SpectrumProperty)."""
+    v = resolve(v, params, default)
+    if v is None:
+        v = default
+    if isinstance(v, (int, float)):
+        return [float(v)] * 3
+    if isinstance(v, dict):
+        raise ValueError(f"unsupported spectrum value {v!r}")
+    return [float(x) for x in v]
+
+
+def _f32(x):
+    return float(np.float32(x))
+
+
+def _norm3(v):
+    n = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    return [v[0] / n, v[1] / n, v[2] / n]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def camera_basis(position, target):
+    """``cameraBasis`` (src/components/camera/basis.ts:49-55), float64 like the TS."""
+    fwd = _norm3([target[i] - position[i] for i in range(3)])
+    up_ref = [0.0, 0.0, 1.0] if abs(fwd[1]) > 0.999999 else [0.0, 1.0, 0.0]
+    right = _norm3(_cross(fwd, up_ref))
+    up = _cross(right, fwd)
+    return fwd, right, up
+
+
+# ----------------------------------------------------------------------------- registries
+# The occupant registries this build implements (one row per occupant, like the
+# reference's MATERIAL_MODELS / LIGHT_KINDS / PRIMITIVES registries).
+MATERIAL_MODELS = {"lambert": abi.MAT_LAMBERT, "dielectric": abi.MAT_DIELECTRIC,
+                   "ggx": abi.MAT_GGX, "none": abi.MAT_NONE}
+PRIMITIVES = {"plane": abi.SHAPE_PLANE, "sphere": abi.SHAPE_SPHERE, "quad": abi.SHAPE_QUAD,
+              "box": abi.SHAPE_BOX}
+LIGHT_KINDS = {"quad": abi.LIGHT_QUAD, "sphere": abi.LIGHT_SPHERE, "point": abi.LIGHT_POINT}
+DIRECT = {"none": abi.DIRECT_NONE, "nee": abi.DIRECT_NEE, "mis": abi.DIRECT_MIS}
+ACCELS = {"bvh": abi.ACCEL_BVH, "tlas": abi.ACCEL_BVH, "cwbvh": abi.ACCEL_CWBVH}
+THIN_SHAPES = {"quad"}
+
+
+# ----------------------------------------------------------------------------- outputs
+
+@dataclass
+class PackedScene:
+    """The scene-data plan, executed: every table the device reads, host-owned."""
+    regions: np.ndarray
+    materials: np.ndarray
+    lights: np.ndarray
+    ambient_material: int
+    env: dict
+    meshes: list = field(default_factory=list)
+    batches: list = field(default_factory=list)
+    region_names: list = field(default_factory=list)
+    material_names: list = field(default_factory=list)
+
+    def desc(self):
+        """A ``ptr_scene_desc`` pointing into this object's arrays (keep self alive)."""
+        d = abi.SceneDesc()
+        d.abi_version = abi.ABI_VERSION
+        d.n_regions = len(self.regions)
+        d.regions = self.regions.ctypes.data_as(abi.C.POINTER(abi.Region))
+        d.n_materials = len(self.materials)
+        d.materials = self.materials.ctypes.data_as(abi.C.POINTER(abi.Material))
+        d.n_lights = len(self.lights)
+        d.lights = self.lights.ctypes.data_as(abi.C.POINTER(abi.Light)) if len(self.lights) else None
+        d.ambient_material = self.ambient_material
+        e = self.env
+        d.env.kind = e["kind"]
+        d.env.sample_as_light = int(e.get("sample_as_light", 0))
+        d.env.color = abi.F4(*(list(e.get("color", [0, 0, 0])) + [0.0]))
+        d.env.intensity = e.get("intensity", 1.0)
+        d.env.select_prob = e.get("select_prob", 1.0)
+        d.env.rotation = e.get("rotation", 0.0)
+        if e["kind"] == abi.ENV_IMAGE:
+            d.env.width, d.env.height = e["width"], e["height"]
+            d.env.radiance = e["radiance"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+            d.env.marginal = e["marginal"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+            d.env.conditional = e["conditional"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+        if self.meshes:
+            self._mesh_arr = (abi.MeshDesc * len(self.meshes))()
+            for i, m in enumerate(self.meshes):
+                md = self._mesh_arr[i]
+                md.n_vertices = len(m["positions"]) // 3
+                md.n_triangles = len(m["indices"]) // 3
+                md.positions = m["positions"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+                md.indices = m["indices"].ctypes.data_as(abi.C.POINTER(abi.C.c_uint32))
+                ta = m.get("tri_alpha")
+                md.tri_alpha = ta.ctypes.data_as(abi.C.POINTER(abi.C.c_float)) if ta is not None else None
+            d.n_meshes = len(self.meshes)
+            d.meshes = self._mesh_arr
+        if self.batches:
+            self._batch_arr = (abi.BatchDesc * len(self.batches))()
+            for i, b in enumerate(self.batches):
+                bd = self._batch_arr[i]
+                bd.prototype_shape = b["prototype_shape"]
+                bd.prototype_ref = b.get("prototype_ref", -1)
+                bd.n_instances = len(b["placements"]) // 8
+                bd.proto = abi.F4(*b.get("proto", [0, 0, 0, 0]))
+                bd.placements = b["placements"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+            d.n_batches = len(self.batches)
+            d.batches = self._batch_arr
+        return d
+
+
+@dataclass
+class CompiledRenderer:
+    """The CompiledRenderer contract (src/compiler/types.ts:1084-1136) for this engine:
+    the program description replaces ``shaders``/``pipeline``; ``uniforms`` are the
+    host-side compute closures (camera basis, tan(fov/2), aspect)."""
+    id: str
+    program: abi.ProgramDesc
+    strategy: dict
+    parameters: dict
+    export_targets: dict
+
+    def camera(self, params, width, height):
+        """Evaluate the camera uniforms (features/camera.ts:69-160) into a ``ptr_camera``."""
+        p = {k: v["default"] for k, v in self.parameters.items()}
+        p.update(params or {})
+        pos, tgt, fov = p["camera.position"], p["camera.target"], p["camera.fov"]
+        fwd, right, up = camera_basis(pos, tgt)
+        cam = abi.Camera()
+        cam.position = (abi.C.c_float * 3)(*pos)
+        cam.forward = (abi.C.c_float * 3)(*fwd)
+        cam.right = (abi.C.c_float * 3)(*right)
+        cam.up = (abi.C.c_float * 3)(*up)
+        cam.tan_fov = math.tan(fov / 2.0)
+        cam.aspect = width / height if height else 1.0
+        return cam
+
+
+@dataclass
+class CompiledScene:
+    renderers: list
+    scene_data: PackedScene
+    warnings: list
+
+
+# ----------------------------------------------------------------------------- compiler
+
+class Compiler:
+    """``Compiler.compile`` / ``compileScene`` (src/compiler/Compiler.ts:14-72)."""
+
+    def compile(self, scene, strategy, params=None):
+        out = self.compile_scene(scene, [strategy], params)
+        return out.renderers[0], out.scene_data
+
+    def compile_scene(self, scene, strategies, params=None):
+        params = dict(params or {})
+        bag = DiagnosticBag()
+        for st in strategies:
+            self._validate(scene, st, bag)
+        bag.throw_if_errors()
+        data = self._pack(scene, strategies, params, bag)
+        bag.throw_if_errors()
+        renderers = [self._program(scene, st, data) for st in strategies]
+        return CompiledScene(renderers, data, bag.warnings)
+
+    # -- Validate (src/compiler/analyze/Validator.ts:50) ------------------------------
+    def _validate(self, scene, st, bag):
+        mats = scene.get("materials", {})
+        for i, o in enumerate(scene.get("objects", [])):
+            kind = o.get("kind")
+            if kind == "mesh":
+                if "positions" not in o or "indices" not in o:
+                    bag.error("invalid-mesh", f"object {i}: mesh needs positions and indices")
+            elif kind == "instanced":
+                proto = o.get("prototype", {})
+                if proto.get("kind") != "mesh" and proto.get("type") != "sphere":
+                    bag.error("unsupported", f"object {i}: instanced prototype must be a mesh or a sphere")
+            elif o.get("type") not in PRIMITIVES:
+                bag.error("unknown-primitive", f"object {i}: unknown primitive type {o.get('type')!r} "
+                          f"(available: {', '.join(PRIMITIVES)})")
+            mname = o.get("material") if kind != "instanced" else o.get("prototype", {}).get("material")
+            if mname not in mats:
+                bag.error("unknown-material", f"object {i}: unknown material {mname!r}")
+        for name, m in mats.items():
+            if m.get("model") not in MATERIAL_MODELS:
+                bag.error("unknown-model", f"material {name!r}: unknown model {m.get('model')!r} "
+                          f"(available: {', '.join(MATERIAL_MODELS)})")
+        for i, l in enumerate(scene.get("lights", [])):
+            if l.get("kind") not in LIGHT_KINDS:
+                bag.error("unknown-light", f"light {i}: unknown kind {l.get('kind')!r}")
+        env = scene.get("environment", {"type": "none"})
+        if env.get("type") not in ("none", "constant", "image", "procedural"):
+            bag.error("unknown-environment", f"unknown environment type {env.get('type')!r}")
+        am = scene.get("ambientMedium")
+        if am is not None and am not in mats:
+            bag.error("unknown-material", f"ambientMedium {am!r} is not a material")
+        meas = st.get("measurement", {})
+        est = st.get("estimator", {})
+        mb = meas.get("maxBounces")
+        if not isinstance(mb, int) or mb < 0:
+            bag.error("invalid-setting", f"strategy {st.get('id')}: maxBounces must be a non-negative integer")
+        if est.get("directLighting", "none") not in DIRECT:
+            bag.error("invalid-setting", f"strategy {st.get('id')}: directLighting {est.get('directLighting')!r}")
+        rr = est.get("russianRoulette")
+        if rr is not None:
+            ms = rr.get("maxSurvival", 0.95)
+            if not (0.0 < ms <= 1.0):
+                bag.error("invalid-setting", "russianRoulette.maxSurvival must be in (0, 1]")
+        if meas.get("color", "rgb") != "rgb":
+            bag.error("unsupported", "measurement.color 'spectral' is not available in this build")
+        vs = est.get("volumeSampling", "analytic")
+        if vs not in ("analytic", None):
+            bag.error("unsupported", f"volumeSampling {vs!r} is not available in this build")
+        if est.get("mediumLightSampling", "vertex") == "equiangular":
+            # Validator.ts:506-540: equiangular is pinned to delta lights and plain NEE.
+            if est.get("directLighting") != "nee":
+                bag.error("invalid-setting", "mediumLightSampling 'equiangular' requires directLighting 'nee'")
+            if any(l.get("kind") != "point" for l in scene.get("lights", [])):
+                bag.error("invalid-setting", "mediumLightSampling 'equiangular' supports delta (point) lights only")
+            bag.error("unsupported", "mediumLightSampling 'equiangular' is not available in this build")
+        for key in ("meshTraversal", "instanceAccel"):
+            v = est.get(key)
+            if v is not None and v not in ACCELS:
+                bag.error("invalid-setting", f"{key} {v!r} (available: {', '.join(ACCELS)})")
+
+    # -- Plan + pack (src/compiler/plan/Planner.ts:72, app/sceneData.ts:27) -----------
+    def _pack(self, scene, strategies, params, bag):
+        mats_src = scene.get("materials", {})
+        mat_names = list(mats_src.keys())
+        mat_index = {n: i for i, n in enumerate(mat_names)}
+        materials = []
+        for n in mat_names:
+            materials.append(self._material(mats_src[n], params))
+
+        regions, region_names, lights = [], [], []
+        meshes, batches = [], []
+        for i, o in enumerate(scene.get("objects", [])):
+            kind = o.get("kind")
+            if kind == "mesh":
+                r = abi.Region()
+                r.shape = abi.SHAPE_MESH
+                r.material = mat_index[o["material"]]
+                r.thin = 0 if o.get("closed") else 1
+                r.ref = len(meshes)
+                meshes.append(self._mesh(o))
+                r.ior = self._ior(mats_src[o["material"]], params)
+            elif kind == "instanced":
+                r = abi.Region()
+                r.shape = abi.SHAPE_INSTANCES
+                proto = o["prototype"]
+                r.material = mat_index[proto["material"]]
+                r.ref = len(batches)
+                r.ior = self._ior(mats_src[proto["material"]], params)
+                b = {"placements": self._placements(o["placements"])}
+                if proto.get("kind") == "mesh":
+                    b["prototype_shape"] = abi.SHAPE_MESH
+                    b["prototype_ref"] = len(meshes)
+                    meshes.append(self._mesh(proto))
+                    r.thin = 1
+                else:
+                    pp = proto["parameters"]
+                    b["prototype_shape"] = abi.SHAPE_SPHERE
+                    b["proto"] = list(pp.get("center", [0, 0, 0])) + [pp["radius"]]
+                    r.thin = 0
+                batches.append(b)
+            else:
+                r = self._primitive(o, params)
+                r.material = mat_index[o["material"]]
+                r.ior = self._ior(mats_src[o["material"]], params)
+            regions.append(r)
+            region_names.append(o.get("name") or f"object_{i}")
+
+        # Light roster (plan/dataTenants.ts lightRosterOf): authored lights, then emissive
+        # analytic objects in scene order.  Authored area lights desugar into a hittable
+        # region with a synthesized emissive material (impl-plan-area-lights A3).
+        for li, l in enumerate(scene.get("lights", [])):
+            kind = l["kind"]
+            e = rgb(l.get("emission"), params, [1.0, 1.0, 1.0])
+            rec = abi.Light()
+            rec.kind = LIGHT_KINDS[kind]
+            rec.radiance = abi.F4(*(e + [0.0]))
+            rec.region = -1
+            if kind == "quad":
+                corner, e1, e2 = l["corner"], l["edge1"], l["edge2"]
+                c = _cross(e1, e2)
+                area = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
+                nrm = [c[0] / area, c[1] / area, c[2] / area]
+                vals = list(corner) + list(e1) + list(e2) + nrm + [area]
+                rec.p = (abi.C.c_float * 16)(*vals)
+                materials.append(self._light_material(e))
+                reg = abi.Region()
+                reg.shape = abi.SHAPE_QUAD
+                reg.thin = 1
+                reg.material = len(materials) - 1
+                reg.ior = 1.0
+                reg.p = (abi.C.c_float * 15)(*(list(corner) + list(e1) + list(e2) + nrm))
+                rec.region = len(regions)
+                regions.append(reg)
+                region_names.append(f"light_{li}")
+            elif kind == "sphere":
+                center = l.get("position", l.get("center"))
+                rad = l["radius"]
+                rec.p = (abi.C.c_float * 16)(*(list(center) + [rad]))
+                materials.append(self._light_material(e))
+                reg = abi.Region()
+                reg.shape = abi.SHAPE_SPHERE
+                reg.thin = 0
+                reg.material = len(materials) - 1
+                reg.ior = 1.0
+                reg.p = (abi.C.c_float * 15)(*(list(center) + [rad]))
+                rec.region = len(regions)
+                regions.append(reg)
+                region_names.append(f"light_{li}")
+            else:   # point: delta, registry entry only
+                rec.p = (abi.C.c_float * 16)(*list(l["position"]))
+            lights.append((rec, kind, e))
+        for i, o in enumerate(scene.get("objects", [])):
+            if o.get("kind") is not None:
+                continue
+            m = mats_src[o["material"]]
+            if m.get("sampleAsLight") is False or m.get("model") != "lambert":
+                continue
+            e = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
+            if max(e) <= 0.0 or o["type"] not in ("sphere", "quad"):
+                continue
+            rec = abi.Light()
+            rec.region = i
+            rec.radiance = abi.F4(*(e + [0.0]))
+            reg = regions[i]
+            if o["type"] == "sphere":
+                rec.kind = abi.LIGHT_SPHERE
+                rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:4])))
+            else:
+                rec.kind = abi.LIGHT_QUAD
+                e1, e2 = list(reg.p[3:6]), list(reg.p[6:9])
+                c = _cross(e1, e2)
+                area = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
+                rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:12]) + [area]))
+            lights.append((rec, o["type"], e))
+
+        # Selection CDF (features/lighting.ts computeSelectPdf; power per kind from the
+        # descriptors: quad pi*A*Le, sphere pi*4*pi*r^2*Le, point 4*pi*I).
+        sel_mode = "power"
+        for st in strategies:
+            sel_mode = st.get("estimator", {}).get("lightSelection", "power")
+        weights = []
+        for rec, kind, e in lights:
+            mean = (e[0] + e[1] + e[2]) / 3.0
+            if sel_mode == "uniform":
+                w = 1.0
+            elif rec.kind == abi.LIGHT_QUAD:
+                w = max(1e-8, math.pi * rec.p[12] * mean)
+            elif rec.kind == abi.LIGHT_SPHERE:
+                r = rec.p[3]
+                w = max(1e-8, math.pi * 4 * math.pi * r * r * mean)
+            else:
+                w = max(1e-8, 4 * math.pi * mean)
+            weights.append(w)
+        total = sum(weights)
+        acc = 0.0
+        light_arr = np.zeros(len(lights), dtype=np.dtype((np.void, abi.C.sizeof(abi.Light))))
+        light_recs = (abi.Light * max(len(lights), 1))()
+        for i, (rec, kind, e) in enumerate(lights):
+            pdf = weights[i] / total
+            acc += pdf
+            rec.select_pdf = pdf
+            rec.select_cdf = acc
+            light_recs[i] = rec
+        light_arr = np.frombuffer(bytes(light_recs), dtype=np.uint8).reshape(max(len(lights), 1), -1)[:len(lights)].copy()
+
+        env = self._environment(scene.get("environment") or {"type": "none"}, params, scene, lights, bag)
+        am = scene.get("ambientMedium")
+        packed = PackedScene(
+            regions=_as_bytes(regions, abi.Region),
+            materials=_as_bytes([m for m in materials], abi.Material),
+            lights=light_arr,
+            ambient_material=mat_index[am] if am is not None else -1,
+            env=env, meshes=meshes, batches=batches,
+            region_names=region_names, material_names=mat_names,
+        )
+        return packed
+
+    def _primitive(self, o, params):
+        t = o["type"]
+        p = o.get("parameters", {})
+        r = abi.Region()
+        r.shape = PRIMITIVES[t]
+        r.thin = 1 if t in THIN_SHAPES else 0
+        vals = []
+        if t == "plane":
+            n = p["normal"]
+            ln = math.sqrt(sum(x * x for x in n))
+            vals = [n[0] / ln, n[1] / ln, n[2] / ln, p.get("offset", 0.0) / ln]   # canonicalPlane
+        elif t == "sphere":
+            vals = list(p.get("center", [0, 0, 0])) + [p["radius"]]
+        elif t == "quad":
+            corner, e1, e2 = p["corner"], p["edge1"], p["edge2"]
+            nrm = _norm3(_cross(e1, e2))
+            vals = list(corner) + list(e1) + list(e2) + nrm
+        elif t == "box":
+            vals = list(p.get("center", [0, 0, 0])) + list(p["halfSize"])
+        tr = o.get("transform")
+        if tr:
+            vals = self._fold_transform(t, vals, tr)
+        r.p = (abi.C.c_float * 15)(*vals)
+        return r
+
+    @staticmethod
+    def _fold_transform(t, vals, tr):
+        """Fold a constant similarity into the canonical parameters (translation and
+        uniform scale; the analytic set is similarity-closed, fable-transforms §5.1)."""
+        if tr.get("rotation") is not None:
+            raise CompileError([Diagnostic("error", "unsupported", "rotated primitives are not available in this build")])
+        pos = tr.get("position", [0, 0, 0])
+        s = float(tr.get("scale", 1.0))
+        if t == "sphere":
+            return [vals[0] * s + pos[0], vals[1] * s + pos[1], vals[2] * s + pos[2], vals[3] * s]
+        if t == "box":
+            return [vals[0] * s + pos[0], vals[1] * s + pos[1], vals[2] * s + pos[2]] + [v * s for v in vals[3:6]]
+        if t == "quad":
+            return [vals[i] * s + pos[i] for i in range(3)] + [v * s for v in vals[3:9]] + vals[9:12]
+        if t == "plane":
+            n = vals[0:3]
+            return n + [vals[3] * s - (n[0] * pos[0] + n[1] * pos[1] + n[2] * pos[2])]
+        return vals
+
+    def _material(self, m, params):
+        """MaterialProperties defaults of the generated lookup (features/materials.ts:372-423):
+        albedo 0.8, emission 0, transmittance 1, f0 0.9, roughness 0.5."""
+        rec = abi.Material()
+        model = m["model"]
+        rec.model = MATERIAL_MODELS[model]
+        alb = rgb(m.get("albedo"), params, [0.8, 0.8, 0.8])
+        emi = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
+        rec.albedo = abi.F4(*(alb + [0.0]))
+        rec.emission = abi.F4(*(emi + [0.0]))
+        rec.transmittance = abi.F4(*(rgb(m.get("transmittance"), params, [1.0, 1.0, 1.0]) + [0.0]))
+        rec.f0 = abi.F4(*(rgb(m.get("f0"), params, [0.9, 0.9, 0.9]) + [0.0]))
+        rough = float(resolve(m.get("roughness"), params, 0.5))
+        rec.alpha = max(1e-3, rough * rough)          # ggx.glsl:7-9 derived row
+        flags = 0
+        if model == "lambert" and max(emi) > 0.0:
+            flags |= abi.MATF_EMISSIVE
+        med = m.get("medium")
+        if med is not None:
+            sa = rgb(med.get("sigma_a"), params, [0.0, 0.0, 0.0])
+            ss = rgb(med.get("sigma_s"), params, [0.0, 0.0, 0.0])
+            rec.sigma_a = abi.F4(*(sa + [0.0]))
+            rec.sigma_s = abi.F4(*(ss + [0.0]))
+            rec.phase_g = float(resolve(med.get("phase_g", med.get("g")), params, 0.0))
+            flags |= abi.MATF_MEDIUM
+            if max(ss) > 0.0:
+                flags |= abi.MATF_SCATTERING
+        rec.flags = flags
+        return rec
+
+    @staticmethod
+    def _light_material(e):
+        rec = abi.Material()
+        rec.model = abi.MAT_LAMBERT
+        rec.albedo = abi.F4(0.0, 0.0, 0.0, 0.0)
+        rec.emission = abi.F4(*(list(e) + [0.0]))
+        rec.transmittance = abi.F4(1.0, 1.0, 1.0, 0.0)
+        rec.f0 = abi.F4(0.9, 0.9, 0.9, 0.0)
+        rec.alpha = 0.25
+        rec.flags = abi.MATF_EMISSIVE
+        return rec
+
+    @staticmethod
+    def _ior(m, params):
+        if m.get("model") == "dielectric":
+            return float(resolve(m.get("ior"), params, 1.5))
+        return 1.0
+
+    @staticmethod
+    def _mesh(o):
+        pos = np.ascontiguousarray(np.asarray(o["positions"], np.float32).reshape(-1))
+        idx = np.ascontiguousarray(np.asarray(o["indices"], np.uint32).reshape(-1))
+        out = {"positions": pos, "indices": idx}
+        if o.get("triangleAlpha") is not None:
+            out["tri_alpha"] = np.ascontiguousarray(np.asarray(o["triangleAlpha"], np.float32))
+        return out
+
+    @staticmethod
+    def _placements(pl):
+        """Placement records (intersection/instancing/placement.glsl:19-41): the world ->
+        rigid-frame quaternion q (xyzw) and ts = (t_rigid, s) with t_rigid = -R^T t."""
+        recs = []
+        for tr in pl:
+            pos = tr.get("position", [0, 0, 0])
+            s = float(tr.get("scale", 1.0))
+            rot = tr.get("rotation")
+            if rot is None:
+                qx, qy, qz, qw = 0.0, 0.0, 0.0, 1.0
+            elif isinstance(rot, dict):
+                ax = _norm3(rot["axis"])
+                h = rot["angle"] / 2.0
+                qx, qy, qz, qw = ax[0] * math.sin(h), ax[1] * math.sin(h), ax[2] * math.sin(h), math.cos(h)
+            else:
+                qx, qy, qz, qw = rot
+            # inverse rotation (conjugate) maps world to the rigid frame
+            iq = (-qx, -qy, -qz, qw)
+            t_r = _qrot(iq, [-pos[0], -pos[1], -pos[2]])
+            recs.extend([iq[0], iq[1], iq[2], iq[3], t_r[0], t_r[1], t_r[2], s])
+        return np.asarray(recs, np.float32)
+
+    def _environment(self, env, params, scene, lights, bag):
+        t = env.get("type", "none")
+        if t == "none":
+            return {"kind": abi.ENV_NONE}
+        intensity = float(resolve(env.get("intensity"), params, 1.0))
+        if t == "constant":
+            col = rgb(env.get("color"), params, [1.0, 1.0, 1.0])
+            sal = bool(env.get("sampleAsLight", False))
+            out = {"kind": abi.ENV_CONSTANT, "color": col, "intensity": intensity,
+                   "sample_as_light": sal, "rotation": 0.0}
+            out["select_prob"] = self._env_select_prob(sum(col) / 3.0, intensity, scene, lights)
+            return out
+        bag.error("unsupported", f"environment {t!r} needs the image table path (pack_environment)")
+        return {"kind": abi.ENV_NONE}
+
+    @staticmethod
+    def _env_select_prob(mean_l, intensity, scene, lights):
+        """envSelectionProbability (features/lighting.ts:488-525), 'power' selection."""
+        r = 1.0
+        for o in scene.get("objects", []):
+            p = o.get("parameters", {})
+            center = 0.0
+            extent = 0.0
+            for k in ("center", "corner"):
+                if k in p:
+                    center = max(center, math.hypot(*p[k]))
+            for k in ("radius", "halfSize", "offset"):
+                if k in p:
+                    v = p[k]
+                    extent += max(v) if isinstance(v, (list, tuple)) else float(v)
+            r = max(r, center + extent)
+        phi_env = 4 * math.pi * math.pi * r * r * mean_l * intensity
+        phi_fin = 0.0
+        for rec, kind, e in lights:
+            mean = (e[0] + e[1] + e[2]) / 3.0
+            if rec.kind == abi.LIGHT_QUAD:
+                phi_fin += max(1e-8, math.pi * rec.p[12] * mean)
+            elif rec.kind == abi.LIGHT_SPHERE:
+                phi_fin += max(1e-8, math.pi * 4 * math.pi * rec.p[3] ** 2 * mean)
+            else:
+                phi_fin += max(1e-8, 4 * math.pi * mean)
+        return min(0.99, max(0.01, phi_env / max(phi_env + phi_fin, 1e-20)))
+
+    # -- Generate: the program description (flags of plan/types.ts:39-112) -------------
+    def _program(self, scene, st, data):
+        meas = st.get("measurement", {})
+        est = st.get("estimator", {})
+        prog = abi.ProgramDesc()
+        prog.abi_version = abi.ABI_VERSION
+        prog.max_bounces = int(meas["maxBounces"])
+        prog.max_null_crossings = int(meas.get("maxNullCrossings", 32))
+        prog.direct = DIRECT[est.get("directLighting", "none")]
+        rr = est.get("russianRoulette")
+        prog.rr_start = int(rr.get("startDepth", 0)) if rr else -1
+        prog.rr_max_survival = float(rr.get("maxSurvival", 0.95)) if rr else 1.0
+        prog.scattering = 0 if meas.get("scattering") == "ignored" else 1
+        prog.accel = ACCELS[est.get("meshTraversal") or est.get("instanceAccel") or "bvh"]
+        prog.equiangular = 1 if est.get("mediumLightSampling") == "equiangular" else 0
+        cam = meas.get("camera", {})
+        fov = cam.get("fov", 0.8)
+        fov_default = fov.get("default", 0.8) if is_param(fov) else fov
+        parameters = {
+            "camera.position": {"type": "vec3", "default": list(cam.get("position", [0, 0, 8]))},
+            "camera.target": {"type": "vec3", "default": list(cam.get("target", [0, 0, 0]))},
+            "camera.fov": {"type": "float", "default": fov_default},
+        }
+        rid = f"{st.get('id', 'strategy')}-{scene.get('id', 'scene')}"
+        exports = {"radiance": {"format": "float"}, "variance": {"format": "float"}}
+        return CompiledRenderer(rid, prog, st, parameters, exports)
+
+
+def _qrot(q, v):
+    """Rotate v by unit quaternion q = (x, y, z, w): v + 2 q.xyz x (q.xyz x v + w v)."""
+    qv = q[:3]
+    c1 = _cross(qv, v)
+    t = [c1[i] + q[3] * v[i] for i in range(3)]
+    c2 = _cross(qv, t)
+    return [v[i] + 2.0 * c2[i] for i in range(3)]
+
+
+def _as_bytes(recs, ctype):
+    n = len(recs)
+    arr = (ctype * max(n, 1))()
+    for i, r in enumerate(recs):
+        arr[i] = r
+    buf = np.frombuffer(bytes(arr), dtype=np.uint8).reshape(max(n, 1), -1)[:n].copy()
+    return buf
