@@ -1,0 +1,319 @@
+"""Benchmark of the transport loop on B200 (one JSON line on rank 0).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cornell]
+
+A step renders the whole workload once (every pixel x every sample) from the
+device-resident scene.  The Cornell workload is the configuration of the plain Cornell
+box: 256x256, 64 spp, max depth 8, roulette from depth 3, MIS, RGB binary32.
+
+* value: samples/s of the whole job (all ranks' samples / max-over-ranks device time of
+  K steps, CUDA events on the library's stream; the L2 is flushed between steps by
+  writing a 256 MiB buffer on that stream, untimed).
+* e2e: the same metric through the public API per step (CudaEngine.render_frame with the
+  frame uniforms uploaded from host memory + read_export of the radiance to host memory),
+  wall clock around each step, max over ranks.
+* roofline: the dominant kernel class of an instrumented render of the same workload
+  (CUDA events around each launch), algorithmic bytes per launch / its mean duration,
+  against the measured HBM copy bandwidth.
+* cpu_baseline: the oracle (the CPU restatement) on the host cores, bounded sample.
+
+Multi-GPU: replicas (each rank renders its own sample range of the same image; no data
+path collective; the barrier and the max-over-ranks timing use torch.distributed).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "samples/s on 1 B200: batched wavefront and adjoint vs plain, at matched RMSE"
+
+
+def workload(name):
+    from pathtracerglsl_b200 import scenes
+    if name == "cornell":
+        sc, st = scenes.cornell()
+        w, h, spp = scenes.CORNELL_SIZE
+        cfg = {"workload": "cornell-c1: 5 Lambert quads + Lambert sphere + dielectric sphere (IOR 1.5), "
+                           "0.5x0.5 quad light Le=15, pinhole fov 40deg, MIS, RR from depth 3",
+               "width": w, "height": h, "spp": spp, "max_depth": 8, "color": "rgb"}
+        return sc, st, w, h, spp, cfg
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------- helpers
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(sc, st, w, h, spp, seconds=10.0):
+    """Oracle (CPU restatement) on all host threads: repeat sample passes until ~seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from pathtracerglsl_b200.compiler import Compiler
+    oracle.build()
+    r, pk = Compiler().compile(sc, st)
+    threads = os.cpu_count() or 1
+    chunk = max(1, min(spp, 8))
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        oracle.render(pk, r, w, h, chunk, first_sample=done, salt=1, threads=threads)
+        done += chunk
+        el = time.perf_counter() - t0
+        if el >= seconds or done >= 4 * spp:
+            break
+    value = w * h * done / el
+    return {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{w}x{h} x {done} spp of the same workload ({el:.1f} s of host time)"}
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 0, 1, None
+    import torch
+    import torch.distributed as dist
+    import datetime
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return dist.get_rank(), local, world, dist
+
+
+def reduce_max(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------------- arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from pathtracerglsl_b200.compiler import Compiler
+    sc, st, w, h, spp, cfg = workload(args.workload)
+    oracle.build()
+    r, pk = Compiler().compile(sc, st)
+    threads = os.cpu_count() or 1
+    for i in range(args.warmup):
+        oracle.render(pk, r, w, h, spp, first_sample=i * spp, salt=1, threads=threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        oracle.render(pk, r, w, h, spp, first_sample=(args.warmup + i) * spp, salt=1, threads=threads)
+    el = time.perf_counter() - t0
+    value = w * h * spp * args.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
+                             "sample": f"the whole workload per step ({w}x{h} x {spp} spp), OpenMP over pixels"},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def algorithmic_bytes(kernel, c):
+    """Bytes the algorithm must move per render for one kernel class (path state in HBM;
+    the scene tables are a few KB and cache-resident by design, so not counted)."""
+    paths, closest, shadow = c["paths"], c["closest_queries"], c["shadow_queries"]
+    alive = max(closest - paths, 0)
+    if kernel == "closest":
+        return closest * (4 + 32 + 32)                      # queue, ray, hit record
+    if kernel == "shade":
+        return closest * (4 + 136 + 16) + alive * (104 + 4) + shadow * (64 + 4)
+    if kernel == "shadow":
+        return shadow * (4 + 64 + 32)
+    if kernel == "generate":
+        return paths * (104 + 4 + 16)
+    if kernel == "film":
+        return paths * 16 + 0
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from pathtracerglsl_b200.compiler import Compiler
+    from pathtracerglsl_b200.engine import CudaEngine
+
+    sc, st, w, h, spp, cfg = workload(args.workload)
+    renderer, packed = Compiler().compile(sc, st)
+    eng = CudaEngine(local)
+    eng.register_scene(packed)
+    eng.load_renderer(renderer)
+    eng.pin_reset_salt(1 + rank)      # each replica renders its own sample stream
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def step():
+        eng.reset()
+        eng.render_frame(w, h, spp)
+
+    for _ in range(args.warmup):
+        step()
+    eng.sync()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, device time with events on the library's stream
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(dist)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(float(k))                 # untimed L2 flush (256 MiB > 126 MB L2)
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+    eng.sync()
+    torch.cuda.synchronize()
+    barrier(dist)
+    clk = clocks.stop()
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    dev_ms = reduce_max(dist, dev_ms)
+    samples_total = w * h * spp * args.steps * world
+    value = samples_total / (dev_ms / 1000.0)
+
+    # ---- end to end through the public API (host uniforms in, host image out)
+    img = None
+    barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.reset()
+        eng.render_frame(w, h, spp)
+        img = eng.read_export("radiance", out=img)
+    el = reduce_max(dist, time.perf_counter() - t0)
+    e2e = {"value": samples_total / el, "unit": "samples/s",
+           "h2d_bytes_per_step": 160, "d2h_bytes_per_step": int(img.nbytes)}
+
+    # ---- instrumented pass: per-kernel-class device time (not part of the timed region)
+    eng.reset()
+    prof = eng.profile_render(w, h, spp)
+    cnt = eng.counters()
+    kernel, (kms, klaunch) = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = measured_peaks()
+    launch_ms = kms / max(klaunch, 1)
+    bytes_per_launch = algorithmic_bytes(kernel, cnt) / max(klaunch, 1)
+    achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9
+    total_prof_ms = sum(v[0] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": "k_" + kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
+                "share": {k: v[0] / total_prof_ms for k, v in prof.items()}}
+    launches = sum(v[1] for v in prof.values()) + 1   # + the frame-parameter kernel
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(cfg, l2="flushed between steps (256 MiB write, untimed)",
+                               parallelism=f"replicas x{world}"),
+                "e2e": e2e, "roofline": roofline, "gpu_launches": launches * args.steps,
+                "clocks": clk,
+                "rays": {"closest_per_sample": cnt["closest_queries"] / cnt["paths"],
+                         "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
+                         "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cornell")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -223,6 +223,15 @@ int ptr_free_program(ptr_program* prog);
  * (Engine.renderFrame, Engine.ts:190-204; one call may fold many frames). */
 int ptr_render(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame);
 
+/* Test hook: render like ptr_render (film included) and also copy every sample's radiance
+ * to host_out, laid out [sample][row][column][rgb] (n >= width*height*spp*3 floats).
+ * The per-sample values are what the reference's accumulation folds in (accumulation.ts:14-51). */
+int ptr_render_samples(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, float* host_out, size_t n);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work
+ * (timing events, cache flushes) with the library's launches. */
+int ptr_get_stream(ptr_ctx* ctx, void** stream);
+
 /* Wait for the context's stream, at most timeout_ms (<0 = no limit). */
 int ptr_sync(ptr_ctx* ctx, int timeout_ms);
 
@@ -238,11 +247,12 @@ int ptr_read_export_device(ptr_program* prog, const char* name, float* dst_devic
 /* Device work counters of the last ptr_render on this program (synchronises). */
 int ptr_get_counters(ptr_program* prog, ptr_counters* out);
 
-/* Record the per-launch kernel timings of the next ptr_render (CUDA events on the
- * context's stream).  ms_out[k] = total ms of kernel class k over that render:
- * 0 generate, 1 closest-hit, 2 shade, 3 shadow, 4 film. */
+/* Instrument the next ptr_render: it runs without the CUDA graph and records a pair of
+ * CUDA events around every kernel launch on the context's stream.  ptr_get_profile then
+ * returns, per kernel class k (0 generate, 1 closest-hit, 2 shade, 3 shadow, 4 film),
+ * the summed device time ms_out[k] and the number of launches launches_out[k]. */
 int ptr_profile_next(ptr_program* prog, int enable);
-int ptr_get_profile(ptr_program* prog, float* ms_out, int n, int* launches_out);
+int ptr_get_profile(ptr_program* prog, float* ms_out, int* launches_out, int n);
 
 #ifdef __cplusplus
 }

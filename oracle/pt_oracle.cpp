@@ -764,8 +764,8 @@ struct Tracer {
                                     v3 vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings);
                                     if (!spectrum_is_black(vis)) {
                                         float w = 1.0f;
-                                        if (mis && !(ls.flags & LIGHT_DELTA))
-                                            w = power_heuristic(ls.pdf, hg_eval(ls.wi, wo_med, mm.phase_g));
+                                        if (mis && !(ls.flags & LIGHT_DELTA))   // hg_pdf = spectrum_average(hg_eval)
+                                            w = power_heuristic(ls.pdf, spectrum_average(v3(hg_eval(ls.wi, wo_med, mm.phase_g))));
                                         radiance = radiance + throughput * ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
                                     }
                                 }

@@ -1,0 +1,154 @@
+// common.cuh — device math shared by every occupant of the transport loop.
+//
+// binary32 throughout; the library is compiled with -fmad=false so products and sums
+// round exactly as written (the reference's GLSL operation order), which keeps the device
+// results comparable sample-for-sample with the CPU restatement.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../../include/ptx_rt.h"
+
+namespace ptx {
+
+struct f3 {
+    float x, y, z;
+    __host__ __device__ f3() : x(0.f), y(0.f), z(0.f) {}
+    __host__ __device__ f3(float a, float b, float c) : x(a), y(b), z(c) {}
+    __host__ __device__ explicit f3(float s) : x(s), y(s), z(s) {}
+    __device__ float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, f3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ f3 operator/(f3 a, f3 b) { return f3(a.x / b.x, a.y / b.y, a.z / b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ f3 operator*(float s, f3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ f3 operator-(f3 a) { return f3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return f3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+__device__ __forceinline__ float length(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 normalize(f3 a) { return a * (1.0f / length(a)); }
+// GLSL min/max: min(x, y) = y < x ? y : x
+__device__ __forceinline__ float gmin(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float gmax(float a, float b) { return a < b ? b : a; }
+__device__ __forceinline__ f3 vmin(f3 a, f3 b) { return f3(gmin(a.x, b.x), gmin(a.y, b.y), gmin(a.z, b.z)); }
+__device__ __forceinline__ f3 vmax(f3 a, f3 b) { return f3(gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z)); }
+__device__ __forceinline__ f3 vexp(f3 a) { return f3(expf(a.x), expf(a.y), expf(a.z)); }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
+__device__ __forceinline__ float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+__device__ __forceinline__ f3 ld3(const float* p) { return f3(p[0], p[1], p[2]); }
+__device__ __forceinline__ f3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// Scalar constants of the reference's core math (glsl/core/math.glsl).
+constexpr float kPi = 3.14159265359f;
+constexpr float kTwoPi = 6.28318530718f;
+constexpr float kMaxDist = 1000.0f;           // MAX_DIST: the far clip
+constexpr float kEpsInterface = 0.001f;       // EPS_INTERFACE: classification probe depth
+constexpr float kMarchClearance = 0.001f;     // MARCH_CLEARANCE: conservative Hit.eps seed
+constexpr float kShadowBackoff = 0.002f;      // SHADOW_BACKOFF (math.glsl:39)
+constexpr float kFpRel = 3.0517578125e-5f;    // 256 ulps relative
+constexpr float kFpAbs = 1.52587890625e-5f;   // 2^-16 absolute floor
+
+constexpr uint32_t kLobeReflection = 1u, kLobeTransmission = 2u, kLobeDelta = 4u, kLobeMedium = 8u;
+constexpr uint32_t kLightDelta = 1u;
+
+// Spectrum helpers over the three RGB transport channels (components/color/spectrum.glsl).
+__device__ __forceinline__ float spectrum_average(f3 s) { float a = s.x; a += s.y; a += s.z; return a * (1.0f / 3.0f); }
+__device__ __forceinline__ float spectrum_max(f3 s) { float m = s.z; m = gmax(s.y, m); m = gmax(s.x, m); return m; }
+__device__ __forceinline__ bool spectrum_is_black(f3 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f; }
+__device__ __forceinline__ int spectrum_sample_channel(float u) { int c = (int)(u * 3.0f); return c < 2 ? c : 2; }
+
+// ---- counter-based sampler: the pcg4d hash of Jarzynski & Olano ("Hash Functions for
+// GPU Rendering", JCGT 2020), keyed per (pixel, sample, reset salt) with a dimension
+// counter; the 24 high bits give an exactly representable float in [0, 1).
+// (components/sampler/pcg4d/pcg4d.glsl:12-40)
+__device__ __forceinline__ uint4 pcg4d(uint4 v) {
+    v.x = v.x * 1664525u + 1013904223u;
+    v.y = v.y * 1664525u + 1013904223u;
+    v.z = v.z * 1664525u + 1013904223u;
+    v.w = v.w * 1664525u + 1013904223u;
+    v.x += v.y * v.w; v.y += v.z * v.x; v.z += v.x * v.y; v.w += v.y * v.z;
+    v.x ^= v.x >> 16u; v.y ^= v.y >> 16u; v.z ^= v.z >> 16u; v.w ^= v.w >> 16u;
+    v.x += v.y * v.w; v.y += v.z * v.x; v.z += v.x * v.y; v.w += v.y * v.z;
+    return v;
+}
+struct Rng {
+    uint32_t base, dim;
+    __device__ __forceinline__ void init(uint32_t px, uint32_t py, uint32_t sample, uint32_t salt) {
+        base = pcg4d(make_uint4(px, py, sample, salt)).x;
+        dim = 0u;
+    }
+    __device__ __forceinline__ float next() {
+        uint32_t u = pcg4d(make_uint4(base, dim, 0u, 0u)).x;
+        dim += 1u;
+        return (float)(u >> 8) * (1.0f / 16777216.0f);
+    }
+};
+
+// ---- frames, Fresnel, spawn ---------------------------------------------------------
+struct Frame { f3 t, b, n; };
+
+// Positional error bound of a floating-point-accurate hit point (math.glsl:54-56).
+__device__ __forceinline__ float fp_uncertainty(f3 p) {
+    return gmax(kFpAbs, kFpRel * gmax(fabsf(p.x), gmax(fabsf(p.y), fabsf(p.z))));
+}
+// Shading frame from a normal (the Euclidean ambient_frame, euclidean.glsl:6-33).
+__device__ __forceinline__ Frame ambient_frame(f3 n) {
+    f3 nn = normalize(n);
+    f3 t = fabsf(nn.x) < 0.9f ? f3(1.f, 0.f, 0.f) : f3(0.f, 1.f, 0.f);
+    t = normalize(t - dot(t, nn) * nn);
+    Frame f;
+    f.t = t; f.b = cross(nn, t); f.n = nn;
+    return f;
+}
+// Orthonormal completion used by samplers (math.glsl build_basis).
+__device__ __forceinline__ void build_basis(f3 n, f3& t, f3& b) {
+    f3 up = fabsf(n.y) < 0.999f ? f3(0.f, 1.f, 0.f) : f3(1.f, 0.f, 0.f);
+    t = normalize(cross(up, n));
+    b = cross(n, t);
+}
+// Exact unpolarised dielectric Fresnel, eta = n_i / n_t (math.glsl:95-102).
+__device__ __forceinline__ float dielectric_fresnel(float cos_i, float eta) {
+    float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+    if (sin2_t >= 1.0f) return 1.0f;
+    float cos_t = sqrtf(1.0f - sin2_t);
+    float r_par = (cos_i - eta * cos_t) / (cos_i + eta * cos_t);
+    float r_perp = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
+    return 0.5f * (r_par * r_par + r_perp * r_perp);
+}
+__device__ __forceinline__ f3 schlick_fresnel(f3 f0, float c) {
+    return f0 + (f3(1.0f) - f0) * powf(1.0f - c, 5.0f);
+}
+__device__ __forceinline__ float power_heuristic(float pf, float pg) {
+    float f2 = pf * pf;
+    if (f2 >= 1.0e38f) return 1.0f;
+    return f2 / gmax(1e-20f, f2 + pg * pg);
+}
+
+struct Ray { f3 o, d; };
+
+// The hit record every arm fills (structs.glsl Hit), minus the wavelengths.
+struct Hit {
+    float t;
+    f3 p;
+    Frame frame;
+    f3 ng;
+    int region_from, region_to, region_owner, element;
+    float eps;
+    float alpha;   // per-triangle GGX alpha when the mesh carries one, else < 0
+};
+
+// Escape to wi's side of the true surface by the hit's own uncertainty (ray.glsl:29-32).
+__device__ __forceinline__ Ray ray_spawn(const Hit& h, f3 wi) {
+    float side = dot(wi, h.ng) >= 0.0f ? 1.0f : -1.0f;
+    Ray r;
+    r.o = h.p + (h.ng * side) * h.eps;
+    r.d = wi;
+    return r;
+}
+
+}  // namespace ptx

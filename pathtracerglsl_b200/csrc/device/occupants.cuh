@@ -1,0 +1,306 @@
+// occupants.cuh — materials, lights, environment and media of the transport loop.
+//
+// One function family per occupant, selected by the material/light record's kind (the
+// device counterpart of the reference's generated dispatch over its registries,
+// src/compiler/generate/features/materials.ts:902-954 and lighting.ts:546-693).
+#pragma once
+#include "scene.cuh"
+
+namespace ptx {
+
+struct ISample { f3 wi; f3 weight; float pdf; uint32_t flags; };
+struct LightSample { f3 wi; float distance; f3 radiance; float pdf; uint32_t flags; int light_id; };
+
+// ---- Lambert (materials/lambert/lambert.glsl:7-37) --------------------------------------
+__device__ __forceinline__ f3 lambert_eval(f3 wi, f3 wo, const Hit& h, const ptr_material& m) {
+    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return f3(0.0f);
+    return ld3(m.albedo) * (1.0f / kPi);
+}
+__device__ __forceinline__ ISample lambert_sample(f3 wo, const Hit& h, const ptr_material& m, float u0, float u1) {
+    f3 n = dot(wo, h.frame.n) < 0.0f ? -h.frame.n : h.frame.n;
+    float cos_theta = sqrtf(u1);
+    float sin_theta = sqrtf(gmax(0.0f, 1.0f - u1));
+    float phi = kTwoPi * u0;
+    float sp, cp;
+    sp = sinf(phi);
+    cp = cosf(phi);
+    ISample s;
+    s.wi = normalize(h.frame.t * (sin_theta * cp) + h.frame.b * (sin_theta * sp) + n * cos_theta);
+    s.weight = ld3(m.albedo);
+    s.pdf = cos_theta * (1.0f / kPi);
+    s.flags = kLobeReflection;
+    return s;
+}
+__device__ __forceinline__ float lambert_pdf(f3 wi, f3 wo, const Hit& h) {
+    float c = dot(wi, h.frame.n) * signf(dot(wo, h.frame.n));
+    return gmax(0.0f, c) * (1.0f / kPi);
+}
+
+// ---- GGX conductor + microfacet machinery (glsl/core/microfacet.glsl:22-54,
+// materials/ggx/ggx.glsl:16-64): Trowbridge-Reitz D, separable Smith G1, Heitz 2018
+// visible-normal sampling, Schlick Fresnel. ----------------------------------------------
+__device__ __forceinline__ f3 mf_to_local(const Frame& f, f3 v) { return f3(dot(v, f.t), dot(v, f.b), dot(v, f.n)); }
+__device__ __forceinline__ f3 mf_from_local(const Frame& f, f3 v) { return normalize(f.t * v.x + f.b * v.y + f.n * v.z); }
+__device__ __forceinline__ float mf_D(f3 h, float a) {
+    float t = h.z * h.z * (a * a - 1.0f) + 1.0f;
+    return a * a / (kPi * t * t);
+}
+__device__ __forceinline__ float mf_G1(f3 v, float a) {
+    float c = fabsf(v.z);
+    return 2.0f * c / (c + sqrtf(a * a + (1.0f - a * a) * c * c));
+}
+__device__ __forceinline__ f3 mf_sample_vndf(f3 wol, float a, float u0, float u1) {
+    f3 vh = normalize(f3(a * wol.x, a * wol.y, wol.z));
+    float lensq = vh.x * vh.x + vh.y * vh.y;
+    f3 T1 = lensq > 0.0f ? f3(-vh.y, vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : f3(1.f, 0.f, 0.f);
+    f3 T2 = cross(vh, T1);
+    float rr = sqrtf(u0);
+    float phi = kTwoPi * u1;
+    float t1 = rr * cosf(phi);
+    float t2 = rr * sinf(phi);
+    float s_ = 0.5f * (1.0f + vh.z);
+    t2 = (1.0f - s_) * sqrtf(gmax(0.0f, 1.0f - t1 * t1)) + s_ * t2;
+    f3 nh = t1 * T1 + t2 * T2 + sqrtf(gmax(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
+    return normalize(f3(a * nh.x, a * nh.y, gmax(1e-6f, nh.z)));
+}
+__device__ __forceinline__ f3 ggx_eval(f3 wi, f3 wo, const Hit& h, f3 f0, float a) {
+    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+    if (wil.z * wol.z <= 0.0f) return f3(0.0f);
+    f3 hh = normalize(wil + wol);
+    f3 F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
+    return F * (mf_D(hh, a) * mf_G1(wil, a) * mf_G1(wol, a) / (4.0f * fabsf(wil.z) * fabsf(wol.z)));
+}
+__device__ __forceinline__ ISample ggx_sample(f3 wo, const Hit& h, f3 f0, float a, float u0, float u1) {
+    f3 wol = mf_to_local(h.frame, wo);
+    float side = wol.z < 0.0f ? -1.0f : 1.0f;
+    wol = wol * side;
+    f3 hh = mf_sample_vndf(wol, a, u0, u1);
+    f3 i = -wol;
+    f3 wil = i - 2.0f * dot(hh, i) * hh;
+    ISample s;
+    if (wil.z <= 0.0f) { s.wi = wo; s.weight = f3(0.0f); s.pdf = 0.0f; s.flags = kLobeReflection; return s; }
+    f3 F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
+    s.weight = F * mf_G1(wil, a);
+    s.pdf = mf_G1(wol, a) * mf_D(hh, a) / (4.0f * fabsf(wol.z));
+    s.flags = kLobeReflection;
+    s.wi = mf_from_local(h.frame, wil * side);
+    return s;
+}
+__device__ __forceinline__ float ggx_pdf(f3 wi, f3 wo, const Hit& h, float a) {
+    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+    if (wil.z * wol.z <= 0.0f) return 0.0f;
+    f3 hh = normalize(wil + wol);
+    return mf_G1(wol, a) * mf_D(hh, a) / (4.0f * fabsf(wol.z));
+}
+
+// ---- smooth dielectric with the eta^2 radiance factor (dielectric.glsl:14-52) ----------
+__device__ __forceinline__ ISample dielectric_sample(f3 wo, const Hit& h, const ptr_material& m,
+                                                     float n_i, float n_t, float uc) {
+    float eta = n_i / n_t;
+    f3 n = h.frame.n;
+    float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
+    float F = dielectric_fresnel(cos_i, eta);
+    ISample s;
+    if (uc < F) {
+        s.wi = normalize(2.0f * cos_i * n - wo);
+        s.weight = f3(1.0f);
+        s.pdf = 0.0f;
+        s.flags = kLobeReflection | kLobeDelta;
+    } else {
+        float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+        float cos_t = sqrtf(gmax(0.0f, 1.0f - sin2_t));
+        s.wi = normalize(-eta * wo + (eta * cos_i - cos_t) * n);
+        float radiance_scale = (n_i * n_i) / (n_t * n_t);
+        s.weight = ld3(m.transmittance) * radiance_scale;
+        s.pdf = 0.0f;
+        s.flags = kLobeTransmission | kLobeDelta;
+    }
+    return s;
+}
+
+// ---- HG phase, forward convention (volume_scattering/hg/hg.glsl:11-42) -----------------
+__device__ __forceinline__ float hg_eval(f3 wi, f3 wo, float g) {
+    float c = dot(wi, -wo);
+    float d = 1.0f + g * g - 2.0f * g * c;
+    return (1.0f - g * g) / (4.0f * kPi * d * sqrtf(gmax(d, 1e-8f)));
+}
+__device__ __forceinline__ ISample hg_sample(f3 wo, float g, float x0, float x1) {
+    float cos_theta;
+    if (fabsf(g) < 1e-3f) {
+        cos_theta = 1.0f - 2.0f * x0;
+    } else {
+        float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * x0);
+        cos_theta = (1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    float sin_theta = sqrtf(gmax(0.0f, 1.0f - cos_theta * cos_theta));
+    float phi = kTwoPi * x1;
+    f3 t, b;
+    build_basis(-wo, t, b);
+    ISample s;
+    s.wi = normalize(t * (sin_theta * cosf(phi)) + b * (sin_theta * sinf(phi)) + (-wo) * cos_theta);
+    s.weight = f3(1.0f);
+    float e = hg_eval(s.wi, wo, g);
+    s.pdf = spectrum_average(f3(e));
+    s.flags = kLobeMedium;
+    return s;
+}
+
+// ---- environment (features/environment.ts; constant env as a uniform-sphere light) ------
+__device__ __forceinline__ f3 env_radiance(const DevScene& S, f3) {
+    if (S.env_kind == PTR_ENV_CONSTANT) return ld3(S.env_color) * S.env_intensity;
+    return f3(0.0f);
+}
+__device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, float x1) {
+    LightSample ls;
+    float z = 1.0f - 2.0f * x0;
+    float r = sqrtf(gmax(0.0f, 1.0f - z * z));
+    float phi = kTwoPi * x1;
+    ls.wi = f3(r * cosf(phi), z, r * sinf(phi));
+    ls.distance = kMaxDist;
+    ls.radiance = ld3(S.env_color) * S.env_intensity;
+    ls.pdf = 1.0f / (4.0f * kPi);
+    ls.flags = 0u;
+    ls.light_id = -1;
+    return ls;
+}
+__device__ __forceinline__ float env_pdf(const DevScene&, f3) { return 1.0f / (4.0f * kPi); }
+
+// ---- lights: quad (area -> solid angle), sphere (visible cone), point (delta) -----------
+// (lights/quad/quad.glsl:14-41, lights/sphere/sphere.glsl:21-71, lights/point/point.glsl)
+__device__ __forceinline__ float sphere_omc_max(float r, float dc2) {
+    float sin2_max = r * r / dc2;
+    return sin2_max / (1.0f + sqrtf(gmax(0.0f, 1.0f - sin2_max)));
+}
+__device__ LightSample light_sample_one(const ptr_light& l, f3 p, float x0, float x1) {
+    LightSample ls;
+    ls.radiance = ld3(l.radiance);
+    ls.flags = 0u;
+    ls.light_id = -1;
+    if (l.kind == PTR_LIGHT_QUAD) {
+        f3 q = ld3(l.p) + x0 * ld3(l.p + 3) + x1 * ld3(l.p + 6);
+        f3 dd = q - p;
+        float d2 = dot(dd, dd);
+        ls.wi = dd * (1.0f / sqrtf(d2));
+        ls.distance = sqrtf(d2);
+        float cos_l = dot(ld3(l.p + 9), -ls.wi);
+        if (cos_l <= 0.0f) { ls.pdf = 0.0f; return ls; }
+        ls.pdf = d2 / (l.p[12] * cos_l);
+        return ls;
+    }
+    if (l.kind == PTR_LIGHT_SPHERE) {
+        f3 to_c = ld3(l.p) - p;
+        float r = l.p[3];
+        float dc2 = dot(to_c, to_c);
+        if (dc2 <= r * r) { ls.wi = f3(0.f, 1.f, 0.f); ls.distance = 1.0f; ls.pdf = 0.0f; return ls; }
+        float omc = sphere_omc_max(r, dc2);
+        float w_t = x0 * omc;
+        float cos_t = 1.0f - w_t;
+        float sin_t = sqrtf(gmax(0.0f, w_t * (2.0f - w_t)));
+        float phi = kTwoPi * x1;
+        f3 w = to_c * (1.0f / sqrtf(dc2));
+        f3 t, b;
+        build_basis(w, t, b);
+        ls.wi = normalize(t * (sin_t * cosf(phi)) + b * (sin_t * sinf(phi)) + w * cos_t);
+        ls.pdf = 1.0f / (kTwoPi * omc);
+        float proj = dot(to_c, ls.wi);
+        f3 perp = to_c - proj * ls.wi;
+        float disc = gmax(0.0f, r * r - dot(perp, perp));
+        ls.distance = (dc2 - r * r) / (proj + sqrtf(disc));
+        return ls;
+    }
+    f3 dd = ld3(l.p) - p;
+    float d2 = dot(dd, dd);
+    ls.wi = dd * (1.0f / sqrtf(d2));
+    ls.distance = sqrtf(d2);
+    ls.radiance = ld3(l.radiance) / d2;
+    ls.pdf = 1.0f;
+    ls.flags = kLightDelta;
+    return ls;
+}
+__device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 light_p, f3 wi) {
+    if (l.kind == PTR_LIGHT_QUAD) {
+        float cos_l = dot(ld3(l.p + 9), -wi);
+        if (cos_l <= 0.0f) return 0.0f;
+        f3 dd = light_p - p;
+        return dot(dd, dd) / (l.p[12] * cos_l);
+    }
+    if (l.kind == PTR_LIGHT_SPHERE) {
+        f3 to_c = ld3(l.p) - p;
+        float dc2 = dot(to_c, to_c);
+        float r = l.p[3];
+        if (dc2 <= r * r) return 0.0f;
+        return 1.0f / (kTwoPi * sphere_omc_max(r, dc2));
+    }
+    return 0.0f;
+}
+// Finite-light selection by the power CDF with the rescaled coordinate (lighting.ts:546-637).
+__device__ LightSample lighting_sample_finite(const DevScene& S, f3 p, float x0, float x1) {
+    if (S.n_lights == 1) {
+        LightSample ls = light_sample_one(S.lights[0], p, x0, x1);
+        ls.light_id = 0;
+        return ls;
+    }
+    int id = S.n_lights - 1;
+    for (int i = 0; i < S.n_lights - 1; ++i)
+        if (x0 < S.lights[i].select_cdf) { id = i; break; }
+    float lo = id == 0 ? 0.0f : S.lights[id - 1].select_cdf;
+    float sel = S.lights[id].select_pdf;
+    float xr = (x0 - lo) / sel;
+    LightSample ls = light_sample_one(S.lights[id], p, clampf(xr, 0.0f, 0.9999999f), x1);
+    ls.light_id = id;
+    ls.pdf *= sel;
+    return ls;
+}
+// Two-stage env-vs-finite draw (lighting.ts generateLightSampling).
+__device__ LightSample lighting_sample(const DevScene& S, f3 p, float x0, float x1) {
+    if (S.n_lights == 0) {
+        if (S.env_samplable) return env_sample(S, x0, x1);
+        LightSample ls;
+        ls.pdf = 0.0f;
+        return ls;
+    }
+    if (!S.env_select_live) return lighting_sample_finite(S, p, x0, x1);
+    float pe = S.env_select_prob;
+    if (x0 < pe) {
+        LightSample ls = env_sample(S, clampf(x0 / pe, 0.0f, 0.9999999f), x1);
+        ls.pdf *= pe;
+        return ls;
+    }
+    float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
+    LightSample ls = lighting_sample_finite(S, p, fx, x1);
+    ls.pdf *= (1.0f - pe);
+    return ls;
+}
+__device__ __forceinline__ float lighting_pdf(const DevScene& S, f3 qp, f3 wi, int lid, f3 light_p) {
+    const ptr_light& l = S.lights[lid];
+    float sel = S.n_lights == 1 ? 1.0f : l.select_pdf;
+    float pe = S.env_select_live ? (1.0f - S.env_select_prob) : 1.0f;
+    return sel * pe * light_pdf_one(l, qp, light_p, wi);
+}
+
+// ---- homogeneous media: chromatic channel-MIS free flight (analytic.glsl:9-51) ---------
+struct MediumSample { bool scattered; f3 weight; f3 exit_p, exit_dir; };
+__device__ __forceinline__ MediumSample medium_sample_analytic(const ptr_material& m, const Ray& r, float t_max,
+                                                               float x0, float x1) {
+    f3 sigma_t = ld3(m.sigma_a) + ld3(m.sigma_s);
+    int c = spectrum_sample_channel(x0);
+    float sc = sigma_t[c];
+    float t = sc == 0.0f ? t_max : -logf(1.0f - x1) / sc;
+    MediumSample ms;
+    if (t < t_max) {
+        f3 tr = vexp(-sigma_t * t);
+        float pdf = spectrum_average(sigma_t * tr);
+        ms.scattered = true;
+        ms.exit_p = r.o + r.d * t;
+        ms.exit_dir = r.d;
+        ms.weight = ld3(m.sigma_s) * tr / gmax(pdf, 1e-20f);
+    } else {
+        f3 tr = vexp(-sigma_t * t_max);
+        float pdf = spectrum_average(tr);
+        ms.scattered = false;
+        ms.weight = tr / gmax(pdf, 1e-20f);
+    }
+    return ms;
+}
+
+}  // namespace ptx

@@ -1,0 +1,139 @@
+// scene.cuh — the device-resident scene and its geometry queries.
+//
+// Analytic regions (plane, sphere, quad, box) are closed-form arms evaluated in region
+// order, exactly the reference's unrolled primitive dispatch
+// (src/compiler/generate/features/intersection.ts:801-824); meshes and instanced batches
+// are walked through their acceleration structures (bvh.cuh).  Region classification
+// (scene_region_at, intersection.ts:1121-1225) is the innermost-wins point query.
+#pragma once
+#include "common.cuh"
+
+namespace ptx {
+
+// Mesh BLAS on the device: binary BVH (2 x float4 per node, bvh.ts:344-383 layout) and/or
+// the compressed wide BVH (5 x uint4 = 80 B per node, cwbvh.ts:18-31 layout).
+struct DevMesh {
+    const float4* tri;        // 3 float4 per triangle: v0.xyz | e1.xyz | e2.xyz (w unused)
+    const float4* bvh;        // 2 float4 per node (min.xyz, A) (max.xyz, B)
+    const uint4* cwbvh;       // 5 uint4 per node
+    const uint32_t* cw_items; // CWBVH leaf item -> triangle index
+    const float* tri_alpha;   // optional per-triangle GGX alpha
+    int n_tris, n_nodes, n_cw_nodes, pad;
+};
+
+struct DevBatch {
+    const float4* place;      // 2 float4 per instance: q (world -> rigid), ts = (t_rigid, s)
+    const float4* tlas;       // binary BVH over instance world boxes (2 float4 per node)
+    int n_inst, proto_shape, proto_mesh, n_tlas;
+    float4 proto;             // sphere prototype: center, radius
+};
+
+struct DevScene {
+    const ptr_region* regions;
+    const ptr_material* materials;
+    const ptr_light* lights;
+    const int* light_of_region;
+    const DevMesh* meshes;
+    const DevBatch* batches;
+    int n_regions, n_materials, n_lights, ambient_material;
+    int has_media, has_accel, n_meshes, n_batches;
+    // environment
+    int env_kind, env_samplable, env_select_live, env_w;
+    int env_h, pad0, pad1, pad2;
+    float env_color[4];
+    float env_intensity, env_select_prob, env_rotation, pad3;
+    const float4* env_map;    // W*H RGBA
+    const float* env_marg;    // H+1 cumulative
+    const float* env_cond;    // H*(W+1) cumulative
+};
+
+// ---- closed-form arms (components/geometry/*/*.glsl) ------------------------------------
+// Sphere: the robust Haines–Günther–Akenine-Möller roots, inside-test root selection
+// (sphere.glsl:28-46).
+__device__ __forceinline__ bool sphere_intersect(const Ray& r, f3 c, float rad, float& t) {
+    f3 oc = r.o - c;
+    float b = dot(oc, r.d);
+    f3 perp = oc - b * r.d;
+    float disc = rad * rad - dot(perp, perp);
+    if (disc < 0.0f) return false;
+    float cc = dot(oc, oc) - rad * rad;
+    float q = (b >= 0.0f) ? -b - sqrtf(disc) : -b + sqrtf(disc);
+    if (q == 0.0f) return false;
+    float ta = q, tb = cc / q;
+    t = (cc < 0.0f) ? gmax(ta, tb) : gmin(ta, tb);
+    return t > 0.0f;
+}
+__device__ __forceinline__ bool plane_intersect(const Ray& r, f3 n, float off, float& t) {
+    float denom = dot(r.d, n);
+    if (fabsf(denom) < 1e-8f) return false;
+    t = -(dot(r.o, n) + off) / denom;
+    return t > 0.0f;
+}
+// Quad: plane root + inside test through the 2x2 Gram system (quad.glsl:9-22).
+__device__ __forceinline__ bool quad_intersect(const Ray& r, f3 corner, f3 e1, f3 e2, f3 n, float& t) {
+    float denom = dot(r.d, n);
+    if (fabsf(denom) < 1e-8f) return false;
+    t = dot(corner - r.o, n) / denom;
+    if (t <= 0.0f) return false;
+    f3 local = r.o + r.d * t - corner;
+    float e11 = dot(e1, e1), e22 = dot(e2, e2), e12 = dot(e1, e2);
+    float d1 = dot(local, e1), d2 = dot(local, e2);
+    float det = e11 * e22 - e12 * e12;
+    float u = (d1 * e22 - d2 * e12) / det;
+    float v = (d2 * e11 - d1 * e12) / det;
+    return u >= 0.0f && u <= 1.0f && v >= 0.0f && v <= 1.0f;
+}
+// Box: slab method with inside-test root selection (box.glsl).
+__device__ __forceinline__ bool box_intersect(const Ray& r, f3 c, f3 h, float& t) {
+    f3 inv = f3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    f3 t0 = (c - h - r.o) * inv;
+    f3 t1 = (c + h - r.o) * inv;
+    f3 tsm = vmin(t0, t1), tbg = vmax(t0, t1);
+    float tn = gmax(gmax(tsm.x, tsm.y), tsm.z);
+    float tf = gmin(gmin(tbg.x, tbg.y), tbg.z);
+    if (tf < tn) return false;
+    t = (tn < 0.0f) ? tf : tn;
+    return t > 0.0f;
+}
+__device__ __forceinline__ float box_sdf(f3 p, f3 c, f3 h) {
+    f3 d = f3(fabsf(p.x - c.x), fabsf(p.y - c.y), fabsf(p.z - c.z)) - h;
+    return length(vmax(d, f3(0.0f))) + gmin(gmax(d.x, gmax(d.y, d.z)), 0.0f);
+}
+__device__ __forceinline__ f3 box_normal(f3 p, f3 c, f3 h) {
+    f3 q = (p - c) / h;
+    f3 a(fabsf(q.x), fabsf(q.y), fabsf(q.z));
+    if (a.x >= a.y && a.x >= a.z) return f3(signf(q.x), 0.f, 0.f);
+    if (a.y >= a.z) return f3(0.f, signf(q.y), 0.f);
+    return f3(0.f, 0.f, signf(q.z));
+}
+
+// One analytic arm: root of region g along r (false when the shape is not analytic).
+__device__ __forceinline__ bool analytic_root(const ptr_region& g, const Ray& r, float& t) {
+    switch (g.shape) {
+        case PTR_SHAPE_PLANE: return plane_intersect(r, ld3(g.p), g.p[3], t);
+        case PTR_SHAPE_SPHERE: return sphere_intersect(r, ld3(g.p), g.p[3], t);
+        case PTR_SHAPE_QUAD: return quad_intersect(r, ld3(g.p), ld3(g.p + 3), ld3(g.p + 6), ld3(g.p + 9), t);
+        case PTR_SHAPE_BOX: return box_intersect(r, ld3(g.p), ld3(g.p + 3), t);
+        default: return false;
+    }
+}
+// Signed distance of an analytic solid (thin owners and meshes never claim containment).
+__device__ __forceinline__ float analytic_sdf(const ptr_region& g, f3 p) {
+    switch (g.shape) {
+        case PTR_SHAPE_PLANE: return dot(p, ld3(g.p)) + g.p[3];
+        case PTR_SHAPE_SPHERE: return length(p - ld3(g.p)) - g.p[3];
+        case PTR_SHAPE_BOX: return box_sdf(p, ld3(g.p), ld3(g.p + 3));
+        default: return 1.0e20f;
+    }
+}
+// Outward normal of an analytic arm at its hit point.
+__device__ __forceinline__ f3 analytic_normal(const ptr_region& g, f3 p) {
+    switch (g.shape) {
+        case PTR_SHAPE_PLANE: return ld3(g.p);
+        case PTR_SHAPE_SPHERE: return normalize(p - ld3(g.p));
+        case PTR_SHAPE_QUAD: return ld3(g.p + 9);
+        default: return box_normal(p, ld3(g.p), ld3(g.p + 3));
+    }
+}
+
+}  // namespace ptx

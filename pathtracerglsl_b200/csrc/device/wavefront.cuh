@@ -1,0 +1,580 @@
+// wavefront.cuh — the transport loop as a wavefront of kernels over a path pool.
+//
+// The reference runs the whole walk (transport/integrators/pt/pt.ts:299-464) as one
+// fragment per pixel.  Here each path lives in struct-of-arrays state in HBM and the walk
+// is split at its two traversals:
+//
+//   k_generate  camera rays + path_state_init for one wave of (pixel, sample) paths
+//   k_closest   nearest hit of every live path (the scene_intersect traversal)
+//   k_shade     one walk iteration: medium segment, null pass-through, emitter scoring,
+//               NEE sampling (emits a shadow query), BSDF continuation, roulette, spawn;
+//               live paths are compacted into the next queue with warp ballots
+//   k_shadow    visibility / transmittance of the queued shadow queries, folded into
+//               the owning path's radiance
+//   k_film      per-pixel FP64 sum and sum of squares over the wave's samples
+//
+// Every path draws its random numbers in exactly the order of the reference's walk
+// (the sampler is counter-based, so a path's stream does not depend on scheduling), and
+// its radiance is accumulated in the same order: emission, then the vertex's NEE term,
+// then the next vertex's emission.
+#pragma once
+#include "occupants.cuh"
+#include "bvh.cuh"
+
+namespace ptx {
+
+// Path pool (indexed by path slot).
+struct PathPool {
+    float4* ray_o;     // origin.xyz, prev_bsdf_pdf
+    float4* ray_d;     // direction.xyz, eta_scale
+    float4* thr;       // throughput.xyz, -
+    float4* rad;       // radiance.xyz, -
+    float4* prev_q;    // stored light-query point (prev_query.p)
+    int4* st;          // bounce, current_medium, null_crossings, prev_was_delta
+    uint2* rng;        // sampler base, dimension
+    float4* hit;       // t, u, v, - ; (region, element, prim) in hit_i
+    int4* hit_i;       // region_owner, element, prim, -
+    // shadow queries (one per path and iteration at most)
+    float4* sh_o;      // origin.xyz, max distance (opaque form)
+    float4* sh_d;      // direction.xyz, crossings left (as int)
+    float4* sh_lp;     // light point.xyz, MIS weight
+    float4* sh_c;      // contribution prefix throughput*Le*f*cos (xyz), pdf
+    int* q[2];         // live-path queues (ping-pong)
+    int* shq;          // shadow queue
+    unsigned int* cnt; // [0],[1] queue counts, [2] shadow count, [3] error flags
+    unsigned long long* stats; // [0] closest queries, [1] shadow queries, [2] paths
+    long long* wave;   // [0] first global path index of the wave, [1] wave size
+};
+
+struct FrameParams {
+    int width, height, spp, first_sample;
+    uint32_t salt;
+    int px_off, py_off;
+    long long total;   // width*height*spp
+    int capacity;
+    ptr_camera cam;
+};
+
+struct ProgParams {
+    int max_bounces, direct, rr_start, max_null;
+    float rr_max_survival;
+    int scattering;
+};
+
+constexpr unsigned kErrStack = 1u;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated append: one atomic per warp, slots in lane order.
+__device__ __forceinline__ int warp_append(unsigned* counter, bool pred) {
+    unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0u) return -1;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return pred ? (int)(base + __popc(mask & lanemask_lt())) : -1;
+}
+
+// ---- scene queries -------------------------------------------------------------------
+// Nearest hit over every arm; returns region (or -1), element, primitive and t.
+struct HitRec { float t, u, v; int region, element, prim; };
+
+__device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r) {
+    HitRec h;
+    h.t = kMaxDist;
+    h.u = h.v = 0.f;
+    h.region = -1;
+    h.element = 0;
+    h.prim = -1;
+    for (int i = 0; i < S.n_regions; ++i) {
+        const ptr_region& g = S.regions[i];
+        if (g.shape >= PTR_SHAPE_MESH) {
+            accel_closest(S, g, i, r, h);
+            continue;
+        }
+        float t;
+        if (analytic_root(g, r, t) && t < h.t) {
+            h.t = t;
+            h.region = i;
+            h.element = 0;
+            h.prim = -1;
+        }
+    }
+    return h;
+}
+
+__device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float max_dist) {
+    for (int i = 0; i < S.n_regions; ++i) {
+        const ptr_region& g = S.regions[i];
+        if (g.shape >= PTR_SHAPE_MESH) {
+            if (accel_any(S, g, r, max_dist)) return true;
+            continue;
+        }
+        float t;
+        if (analytic_root(g, r, t) && t < max_dist) return true;
+    }
+    return false;
+}
+
+// Innermost-wins point classification (features/intersection.ts:1121-1225).
+__device__ __forceinline__ int scene_region_at(const DevScene& S, f3 p) {
+    int region = -1;
+    float best = -1.0e20f;
+    for (int i = 0; i < S.n_regions; ++i) {
+        const ptr_region& g = S.regions[i];
+        float d = g.shape == PTR_SHAPE_INSTANCES ? accel_region_sdf(S, g, p) : analytic_sdf(g, p);
+        if (d < 0.0f && d > best) { best = d; region = i; }
+    }
+    return region;
+}
+
+// Complete the hit record: point, uncertainty, frame, and the region classification of
+// scene_intersect (intersection.ts:1665-1713).
+__device__ __forceinline__ void fill_hit(const DevScene& S, const Ray& r, const HitRec& hr, Hit& h) {
+    h.t = hr.t;
+    h.p = r.o + r.d * hr.t;
+    h.region_owner = hr.region;
+    h.element = hr.element;
+    h.alpha = -1.0f;
+    const ptr_region& g = S.regions[hr.region];
+    f3 n;
+    if (g.shape >= PTR_SHAPE_MESH) {
+        n = accel_hit_normal(S, g, hr, r, h);
+    } else {
+        n = analytic_normal(g, h.p);
+        h.eps = fp_uncertainty(h.p);
+    }
+    h.frame = ambient_frame(n);
+    h.ng = h.frame.n;
+    int outside = scene_region_at(S, h.p + h.ng * kEpsInterface);
+    if (dot(r.d, h.ng) < 0.0f) {
+        h.region_from = outside;
+        h.region_to = hr.region;
+    } else {
+        h.region_from = g.thin ? scene_region_at(S, h.p + h.ng * (-kEpsInterface)) : hr.region;
+        h.region_to = outside;
+        h.frame = ambient_frame(-h.frame.n);
+        h.ng = -h.ng;
+    }
+}
+
+__device__ __forceinline__ int material_of(const DevScene& S, int region) {
+    return region < 0 ? S.ambient_material : S.regions[region].material;
+}
+__device__ __forceinline__ float ior_of(const DevScene& S, int region) {
+    return region < 0 ? 1.0f : S.regions[region].ior;
+}
+__device__ __forceinline__ bool mat_has_medium(const DevScene& S, int m) {
+    return m >= 0 && (S.materials[m].flags & PTR_MATF_MEDIUM);
+}
+__device__ __forceinline__ bool scatter_live(const DevScene& S, const ProgParams& P, int m) {
+    return P.scattering && (S.materials[m].flags & PTR_MATF_SCATTERING);
+}
+__device__ __forceinline__ f3 medium_transmittance(const DevScene& S, const ProgParams& P, int m, float len) {
+    const ptr_material& mm = S.materials[m];
+    f3 st = scatter_live(S, P, m) ? ld3(mm.sigma_a) + ld3(mm.sigma_s) : ld3(mm.sigma_a);
+    return vexp(-st * len);
+}
+
+// ---- kernels ---------------------------------------------------------------------------
+
+// Camera rays for one wave (accumulation.ts:14-26 cameraSample; pinhole.glsl:4-18).
+__global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp) {
+    const FrameParams F = *fp;
+    long long base = pool.wave[0];
+    long long n = F.total - base;
+    if (n > F.capacity) n = F.capacity;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        pool.cnt[0] = (unsigned)n;
+        pool.wave[1] = n;
+        pool.stats[2] += (unsigned long long)n;
+    }
+    const long long npix = (long long)F.width * F.height;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long g = base + i;
+        int pix = (int)(g % npix);
+        int sample = (int)(g / npix);
+        int x = pix % F.width, y = pix / F.width;
+        Rng rng;
+        rng.init((uint32_t)(x + F.px_off), (uint32_t)(y + F.py_off), (uint32_t)(F.first_sample + sample), F.salt);
+        float pxf = (float)x + 0.5f + (float)F.px_off;
+        float pyf = (float)y + 0.5f + (float)F.py_off;
+        float a0 = rng.next();
+        float a1 = rng.next();
+        float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+        rng.next();   // the lens draw (a pinhole has no aperture)
+        rng.next();
+        float ndcx = (2.0f * fx / (float)F.width) - 1.0f;
+        float ndcy = (2.0f * fy / (float)F.height) - 1.0f;
+        ndcx *= F.cam.aspect;
+        f3 dir = normalize(ld3(F.cam.forward) + ndcx * F.cam.tan_fov * ld3(F.cam.right) +
+                           ndcy * F.cam.tan_fov * ld3(F.cam.up));
+        f3 o = ld3(F.cam.position);
+        int medium = S.has_media ? scene_region_at(S, o) : -1;
+        pool.ray_o[i] = f4(o, 0.0f);
+        pool.ray_d[i] = f4(dir, 1.0f);
+        pool.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        pool.rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pool.prev_q[i] = f4(o, 0.0f);
+        pool.st[i] = make_int4(0, medium, 0, 1);
+        pool.rng[i] = make_uint2(rng.base, rng.dim);
+        pool.q[0][i] = (int)i;
+    }
+}
+
+// Nearest hit of every live path.
+__global__ void k_closest(DevScene S, PathPool pool, int in) {
+    unsigned n = pool.cnt[in];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        pool.cnt[in ^ 1] = 0u;
+        pool.cnt[2] = 0u;
+        pool.stats[0] += n;
+    }
+    const int* q = pool.q[in];
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int i = q[k];
+        Ray r;
+        r.o = xyz(pool.ray_o[i]);
+        r.d = xyz(pool.ray_d[i]);
+        HitRec h = scene_closest(S, r);
+        pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
+        pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
+    }
+}
+
+// One walk iteration for every live path.
+template <int DIRECT, bool MEDIA>
+__global__ void k_shade(DevScene S, PathPool pool, ProgParams P, int in) {
+    const unsigned n = pool.cnt[in];
+    const int* q = pool.q[in];
+    int* qout = pool.q[in ^ 1];
+    const bool nee = DIRECT != PTR_DIRECT_NONE;
+    const bool mis = DIRECT == PTR_DIRECT_MIS;
+    const unsigned stride = gridDim.x * blockDim.x;
+    const unsigned n_round = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n_round + 0u; k += stride) {
+        bool alive = false, shadow = false;
+        int i = -1;
+        if (k < n) {
+            i = q[k];
+            float4 ro = pool.ray_o[i], rd = pool.ray_d[i];
+            Ray r;
+            r.o = xyz(ro);
+            r.d = xyz(rd);
+            float prev_bsdf_pdf = ro.w;
+            float eta_scale = rd.w;
+            f3 thr = xyz(pool.thr[i]);
+            f3 rad = xyz(pool.rad[i]);
+            f3 prev_qp = xyz(pool.prev_q[i]);
+            int4 st = pool.st[i];
+            int bounce = st.x, cur_med = st.y, nulls = st.z;
+            bool prev_delta = st.w != 0;
+            uint2 rs = pool.rng[i];
+            Rng rng;
+            rng.base = rs.x;
+            rng.dim = rs.y;
+            float4 hf = pool.hit[i];
+            int4 hi = pool.hit_i[i];
+            HitRec hr;
+            hr.t = hf.x; hr.u = hf.y; hr.v = hf.z;
+            hr.region = hi.x; hr.element = hi.y; hr.prim = hi.z;
+            const bool boundary = hr.region >= 0;
+            const int N = P.max_bounces;
+            Hit hit;
+            if (boundary) fill_hit(S, r, hr, hit);
+            bool done = false, handled = false;
+
+            // -- the volumetric call site: one segment (features/materials.ts:675-746)
+            if (MEDIA) {
+                int med_mat = material_of(S, cur_med);
+                if (mat_has_medium(S, med_mat)) {
+                    float x0 = rng.next();
+                    float x1 = rng.next();
+                    float t_max = boundary ? hr.t : kMaxDist;
+                    const ptr_material& mm = S.materials[med_mat];
+                    if (!scatter_live(S, P, med_mat)) {
+                        thr = thr * vexp(-ld3(mm.sigma_a) * t_max);
+                    } else {
+                        MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
+                        thr = thr * ms.weight;
+                        if (ms.scattered) {
+                            handled = true;
+                            if (bounce == N) {
+                                done = true;
+                            } else {
+                                f3 p_evt = ms.exit_p;
+                                f3 wo_med = -ms.exit_dir;
+                                if (nee) {   // light_sample_direct_medium (light_medium.glsl:7-18)
+                                    float y0 = rng.next();
+                                    float y1 = rng.next();
+                                    LightSample ls = lighting_sample(S, p_evt, y0, y1);
+                                    if (ls.pdf > 0.0f) {
+                                        f3 light_p = p_evt + ls.wi * ls.distance;
+                                        float ph = hg_eval(ls.wi, wo_med, mm.phase_g);
+                                        float w = 1.0f;
+                                        if (mis && !(ls.flags & kLightDelta)) w = power_heuristic(ls.pdf, spectrum_average(f3(ph)));
+                                        pool.sh_o[i] = f4(p_evt, 0.0f);
+                                        pool.sh_d[i] = f4(ls.wi, __int_as_float(P.max_null - nulls));
+                                        pool.sh_lp[i] = f4(light_p, w);
+                                        pool.sh_c[i] = f4(thr * ls.radiance * f3(ph), ls.pdf);
+                                        shadow = true;
+                                    }
+                                }
+                                float z0 = rng.next();
+                                float z1 = rng.next();
+                                ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
+                                thr = thr * ps.weight;
+                                prev_delta = false;
+                                prev_bsdf_pdf = ps.pdf;
+                                prev_qp = p_evt;
+                                r.o = p_evt;
+                                r.d = ps.wi;
+                                // roulette_interior (pt.ts:230-283)
+                                bool survive = true;
+                                if (P.rr_start >= 0 && bounce >= P.rr_start) {
+                                    f3 ss = ld3(mm.sigma_s), sa = ld3(mm.sigma_a);
+                                    f3 surv = ss / vmax(ss + sa, f3(1e-9f));
+                                    float p_survive = spectrum_max(surv);
+                                    if (p_survive <= 0.0f) survive = false;
+                                    else if (rng.next() > p_survive) survive = false;
+                                    else thr = thr / p_survive;
+                                }
+                                if (survive) { bounce += 1; alive = true; }
+                                else done = true;
+                            }
+                        }
+                    }
+                }
+            }
+            if (!handled) {
+                if (!boundary) {   // kernel_score_miss (kernel.glsl:11-14)
+                    float w = 1.0f;
+                    if (nee && S.env_samplable && !prev_delta) {
+                        if (!mis) w = 0.0f;
+                        else {
+                            float pe = S.env_select_live ? S.env_select_prob : 1.0f;
+                            w = power_heuristic(prev_bsdf_pdf, pe * env_pdf(S, r.d));
+                        }
+                    }
+                    rad = rad + thr * w * env_radiance(S, r.d);
+                    done = true;
+                } else {
+                    if (MEDIA && hit.region_from != cur_med) cur_med = hit.region_from;
+                    int mat = material_of(S, hit.region_owner);
+                    const ptr_material& m = S.materials[mat];
+                    if (MEDIA && m.model == PTR_MAT_NONE) {   // null pass-through (pt.ts:404-417)
+                        cur_med = hit.region_to;
+                        Ray nr = ray_spawn(hit, r.d);
+                        r = nr;
+                        nulls += 1;
+                        if (nulls > P.max_null) done = true;
+                        else alive = true;
+                    } else {
+                        f3 wo = -r.d;
+                        // kernel_score_emitter_hit (kernel.glsl:16-25; combiner.ts:27-46)
+                        int mat_emit = material_of(S, hit.region_to);
+                        if (mat_emit >= 0 && (S.materials[mat_emit].flags & PTR_MATF_EMISSIVE)) {
+                            float w = 1.0f;
+                            if (nee) {
+                                int lid = hit.region_to >= 0 ? S.light_of_region[hit.region_to] : -1;
+                                if (lid >= 0 && !prev_delta) {
+                                    if (!mis) w = 0.0f;
+                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p));
+                                }
+                            }
+                            rad = rad + thr * w * ld3(S.materials[mat_emit].emission);
+                        }
+                        if (bounce == N) {
+                            done = true;
+                        } else {
+                            const float alpha = hit.alpha >= 0.0f ? hit.alpha : m.alpha;
+                            const bool nondelta = m.model == PTR_MAT_LAMBERT || m.model == PTR_MAT_GGX;
+                            // light_sample_direct (light.glsl:8-28)
+                            if (nee && nondelta) {
+                                float y0 = rng.next();
+                                float y1 = rng.next();
+                                LightSample ls = lighting_sample(S, hit.p, y0, y1);
+                                if (ls.pdf > 0.0f) {
+                                    f3 light_p = hit.p + ls.wi * ls.distance;
+                                    Ray sr = ray_spawn(hit, ls.wi);
+                                    sr.d = normalize(light_p - sr.o);
+                                    f3 f = m.model == PTR_MAT_LAMBERT ? lambert_eval(ls.wi, wo, hit, m)
+                                                                      : ggx_eval(ls.wi, wo, hit, ld3(m.f0), alpha);
+                                    float cos_i = fabsf(dot(ls.wi, hit.frame.n));
+                                    float w = 1.0f;
+                                    if (mis && !(ls.flags & kLightDelta)) {
+                                        float bp = m.model == PTR_MAT_LAMBERT ? lambert_pdf(ls.wi, wo, hit)
+                                                                              : ggx_pdf(ls.wi, wo, hit, alpha);
+                                        w = power_heuristic(ls.pdf, bp);
+                                    }
+                                    float maxd = length(light_p - sr.o) - kShadowBackoff;
+                                    pool.sh_o[i] = f4(sr.o, maxd);
+                                    pool.sh_d[i] = f4(sr.d, __int_as_float(P.max_null - nulls));
+                                    pool.sh_lp[i] = f4(light_p, w);
+                                    pool.sh_c[i] = f4(thr * ls.radiance * f * cos_i, ls.pdf);
+                                    shadow = true;
+                                }
+                            }
+                            // kernel_sample_continuation (kernel.glsl:27-34)
+                            float uc = rng.next();
+                            float u0 = rng.next();
+                            float u1 = rng.next();
+                            ISample bs;
+                            if (m.model == PTR_MAT_LAMBERT) bs = lambert_sample(wo, hit, m, u0, u1);
+                            else if (m.model == PTR_MAT_GGX) bs = ggx_sample(wo, hit, ld3(m.f0), alpha, u0, u1);
+                            else bs = dielectric_sample(wo, hit, m, ior_of(S, hit.region_from), ior_of(S, hit.region_to), uc);
+                            if (spectrum_is_black(bs.weight)) {
+                                done = true;
+                            } else {
+                                thr = thr * bs.weight;
+                                prev_delta = (bs.flags & kLobeDelta) != 0u;
+                                prev_bsdf_pdf = bs.pdf;
+                                prev_qp = hit.p;
+                                if (bs.flags & kLobeTransmission) {
+                                    if (MEDIA) cur_med = hit.region_to;
+                                    float rr = ior_of(S, hit.region_to) / ior_of(S, hit.region_from);
+                                    eta_scale *= rr * rr;
+                                }
+                                // roulette (pt.ts:204-222)
+                                bool survive = true;
+                                if (P.rr_start >= 0 && bounce >= P.rr_start) {
+                                    float p_survive = gmin(P.rr_max_survival, spectrum_max(thr) * eta_scale);
+                                    if (p_survive <= 0.0f) survive = false;
+                                    else if (rng.next() > p_survive) survive = false;
+                                    else thr = thr / p_survive;
+                                }
+                                if (survive) {
+                                    r = ray_spawn(hit, bs.wi);
+                                    bounce += 1;
+                                    alive = true;
+                                } else {
+                                    done = true;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            (void)done;
+            pool.rad[i] = f4(rad, 0.0f);
+            if (alive) {
+                pool.ray_o[i] = f4(r.o, prev_bsdf_pdf);
+                pool.ray_d[i] = f4(r.d, eta_scale);
+                pool.thr[i] = f4(thr, 0.0f);
+                pool.prev_q[i] = f4(prev_qp, 0.0f);
+                pool.st[i] = make_int4(bounce, cur_med, nulls, prev_delta ? 1 : 0);
+                pool.rng[i] = make_uint2(rng.base, rng.dim);
+            }
+        }
+        int slot = warp_append(&pool.cnt[in ^ 1], alive);
+        if (alive) qout[slot] = i;
+        int sslot = warp_append(&pool.cnt[2], shadow);
+        if (shadow) pool.shq[sslot] = i;
+    }
+}
+
+// Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
+// segment walker (shadow/media/media.glsl:29-62); the surviving fraction scales the
+// stored contribution prefix into the path's radiance.
+template <bool MEDIA>
+__global__ void k_shadow(DevScene S, PathPool pool, ProgParams P) {
+    const unsigned n = pool.cnt[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int i = pool.shq[k];
+        float4 so = pool.sh_o[i], sd = pool.sh_d[i], lp = pool.sh_lp[i], c = pool.sh_c[i];
+        Ray sr;
+        sr.o = xyz(so);
+        sr.d = xyz(sd);
+        f3 vis;
+        if (!MEDIA) {
+            vis = scene_any(S, sr, so.w) ? f3(0.0f) : f3(1.0f);
+        } else {
+            f3 light_p = xyz(lp);
+            int crossings_left = __float_as_int(sd.w);
+            f3 T(1.0f);
+            int medium = scene_region_at(S, sr.o);
+            Ray seg = sr;
+            bool finished = false;
+            for (int crossed = 0; crossed <= crossings_left; crossed++) {
+                float remaining = length(light_p - seg.o) - kShadowBackoff;
+                if (remaining <= 0.0f) { finished = true; break; }
+                HitRec hr = scene_closest(S, seg);
+                bool hit_boundary = hr.region >= 0 && hr.t < remaining;
+                float seg_len = hit_boundary ? hr.t : remaining;
+                int med_mat = material_of(S, medium);
+                if (mat_has_medium(S, med_mat)) T = T * medium_transmittance(S, P, med_mat, seg_len);
+                if (!hit_boundary) { finished = true; break; }
+                Hit h;
+                fill_hit(S, seg, hr, h);
+                int om = material_of(S, h.region_owner);
+                if (!(om >= 0 && S.materials[om].model == PTR_MAT_NONE)) { T = f3(0.0f); finished = true; break; }
+                medium = h.region_to;
+                seg = ray_spawn(h, seg.d);
+                seg.d = normalize(light_p - seg.o);
+            }
+            vis = finished ? T : f3(0.0f);
+        }
+        if (!spectrum_is_black(vis)) {
+            float w = lp.w;
+            f3 add = xyz(c) * vis * w / c.w;
+            float4 rr = pool.rad[i];
+            pool.rad[i] = make_float4(rr.x + add.x, rr.y + add.y, rr.z + add.z, 0.f);
+        }
+    }
+}
+
+// Fold the wave's per-path radiance into the film, per pixel in sample order; then
+// advance the wave cursor.
+__global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double* sumsq, float* samples_out) {
+    const FrameParams F = *fp;
+    const long long base = pool.wave[0];
+    const long long n = pool.wave[1];
+    const long long npix = (long long)F.width * F.height;
+    const long long nslot = n < npix ? n : npix;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nslot; j += (long long)gridDim.x * blockDim.x) {
+        int pix = (int)((base + j) % npix);
+        double s0 = sum[3 * pix + 0], s1 = sum[3 * pix + 1], s2 = sum[3 * pix + 2];
+        double q0 = sumsq[3 * pix + 0], q1 = sumsq[3 * pix + 1], q2 = sumsq[3 * pix + 2];
+        for (long long i = j; i < n; i += npix) {
+            float4 L = pool.rad[i];
+            s0 += (double)L.x; s1 += (double)L.y; s2 += (double)L.z;
+            q0 += (double)L.x * (double)L.x; q1 += (double)L.y * (double)L.y; q2 += (double)L.z * (double)L.z;
+            if (samples_out) {
+                long long g = base + i;
+                samples_out[3 * g + 0] = L.x; samples_out[3 * g + 1] = L.y; samples_out[3 * g + 2] = L.z;
+            }
+        }
+        sum[3 * pix + 0] = s0; sum[3 * pix + 1] = s1; sum[3 * pix + 2] = s2;
+        sumsq[3 * pix + 0] = q0; sumsq[3 * pix + 1] = q1; sumsq[3 * pix + 2] = q2;
+    }
+}
+
+__global__ void k_set_frame(FrameParams* dst, FrameParams F) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dst = F;
+}
+
+__global__ void k_advance(PathPool pool) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) pool.wave[0] += pool.wave[1];
+}
+
+// Mean / variance exports from the FP64 film.
+__global__ void k_export(const double* sum, const double* sumsq, double nsamples, int npix, int what, float* out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npix * 3; j += gridDim.x * blockDim.x) {
+        double m = sum[j] / nsamples;
+        if (what == 0) out[j] = (float)m;
+        else {
+            double v = sumsq[j] / nsamples - m * m;
+            if (v < 0.0) v = 0.0;
+            out[j] = (float)(nsamples > 1.0 ? v * nsamples / (nsamples - 1.0) : 0.0);
+        }
+    }
+}
+
+}  // namespace ptx

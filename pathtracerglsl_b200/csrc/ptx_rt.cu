@@ -1,0 +1,578 @@
+// ptx_rt.cu — the C ABI of include/ptx_rt.h: context, scene upload, programs, frames.
+//
+// One context = one CUDA device + one stream.  A program owns its film (FP64 per-pixel
+// sum and sum of squares) and its path pool; ptr_render renders frame.spp samples per
+// pixel as waves of at most `capacity` paths, each wave a CUDA graph of
+//   k_generate, (k_closest, k_shade, k_shadow) x iterations, k_film, k_advance
+// captured once per (program, scene, image size) and replayed for every wave and frame.
+// Frame-varying values (sample index, salt, camera) live in a device-side FrameParams
+// block refreshed by one cudaMemcpyAsync before the replays, so the graph stays valid.
+#include <cuda_runtime.h>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "device/wavefront.cuh"
+
+using namespace ptx;
+
+struct ptr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+struct ptr_scene {
+    ptr_ctx* ctx = nullptr;
+    DevScene dev{};
+    std::vector<void*> allocs;
+    int has_media = 0;
+    int max_stack_depth = 0;
+};
+
+struct ptr_program {
+    ptr_ctx* ctx = nullptr;
+    ptr_program_desc desc{};
+    // film
+    int fw = 0, fh = 0;
+    double* sum = nullptr;
+    double* sumsq = nullptr;
+    double nsamples = 0.0;
+    float* export_buf = nullptr;
+    // path pool
+    int capacity = 0;
+    std::vector<void*> pool_allocs;
+    PathPool pool{};
+    FrameParams* fp_dev = nullptr;
+    // graph cache
+    cudaGraphExec_t graph = nullptr;
+    const ptr_scene* graph_scene = nullptr;
+    int graph_w = 0, graph_h = 0, graph_iters = 0;
+    float* graph_samples = nullptr;
+    // counters / profiling
+    ptr_counters last{};
+    int profile_next = 0;
+    float prof_ms[5] = {0, 0, 0, 0, 0};
+    int prof_launches[5] = {0, 0, 0, 0, 0};
+};
+
+namespace {
+
+int fail(ptr_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+int cuda_fail(ptr_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, PTR_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(ctx, call)                                              \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+template <typename T>
+int dev_copy(ptr_ctx* ctx, std::vector<void*>& allocs, const T* host, size_t n, const T** out) {
+    *out = nullptr;
+    if (n == 0) return PTR_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) return fail(ctx, PTR_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(p);
+    CK(ctx, cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice));
+    *out = (const T*)p;
+    return PTR_OK;
+}
+
+int launch_grid(int n_sm) { return n_sm * 8; }   // 8 resident blocks of 256 threads per SM
+
+void free_pool(ptr_program* p) {
+    for (void* a : p->pool_allocs) cudaFree(a);
+    p->pool_allocs.clear();
+    p->pool = PathPool{};
+    p->capacity = 0;
+    if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+}
+
+int alloc_pool(ptr_program* p, int capacity) {
+    free_pool(p);
+    ptr_ctx* ctx = p->ctx;
+    auto get = [&](size_t bytes, void** out) -> int {
+        cudaError_t e = cudaMalloc(out, bytes);
+        if (e != cudaSuccess) return fail(ctx, PTR_E_NOMEM, std::string("path pool cudaMalloc: ") + cudaGetErrorString(e));
+        p->pool_allocs.push_back(*out);
+        return PTR_OK;
+    };
+    size_t c = (size_t)capacity;
+    PathPool& q = p->pool;
+    int rc = PTR_OK;
+    if ((rc = get(c * 16, (void**)&q.ray_o)) || (rc = get(c * 16, (void**)&q.ray_d)) ||
+        (rc = get(c * 16, (void**)&q.thr)) || (rc = get(c * 16, (void**)&q.rad)) ||
+        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.st)) ||
+        (rc = get(c * 8, (void**)&q.rng)) || (rc = get(c * 16, (void**)&q.hit)) ||
+        (rc = get(c * 16, (void**)&q.hit_i)) || (rc = get(c * 16, (void**)&q.sh_o)) ||
+        (rc = get(c * 16, (void**)&q.sh_d)) || (rc = get(c * 16, (void**)&q.sh_lp)) ||
+        (rc = get(c * 16, (void**)&q.sh_c)) || (rc = get(c * 4, (void**)&q.q[0])) ||
+        (rc = get(c * 4, (void**)&q.q[1])) || (rc = get(c * 4, (void**)&q.shq)) ||
+        (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
+        (rc = get(64, (void**)&q.wave))) {
+        free_pool(p);
+        return rc;
+    }
+    p->capacity = capacity;
+    return PTR_OK;
+}
+
+// Number of walk iterations a wave needs: maxBounces + 1 vertex evaluations, plus one per
+// null-interface crossing a path may make (crossings do not consume a bounce).
+int wave_iterations(const ptr_program* p, const ptr_scene* s) {
+    int it = p->desc.max_bounces + 1;
+    if (s->has_media) it += p->desc.max_null_crossings;
+    return it;
+}
+
+// Event pairs around each launch of an instrumented render (kernel class, start, end).
+struct ProfRec { int cls; cudaEvent_t a, b; };
+
+void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
+                 std::vector<ProfRec>* prof = nullptr) {
+    auto mark = [&](int cls) -> ProfRec* {
+        if (!prof) return nullptr;
+        ProfRec r{cls, nullptr, nullptr};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, st);
+        prof->push_back(r);
+        return &prof->back();
+    };
+    auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
+    const DevScene& S = s->dev;
+    const PathPool& pool = p->pool;
+    ProgParams P;
+    P.max_bounces = p->desc.max_bounces;
+    P.direct = p->desc.direct;
+    P.rr_start = p->desc.rr_start;
+    P.max_null = p->desc.max_null_crossings;
+    P.rr_max_survival = p->desc.rr_max_survival;
+    P.scattering = p->desc.scattering;
+    const int grid = launch_grid(n_sm), block = 256;
+    ProfRec* r = mark(0);
+    k_generate<<<grid, block, 0, st>>>(S, pool, p->fp_dev);
+    done(r);
+    for (int it = 0; it < iters; ++it) {
+        int in = it & 1;
+        r = mark(1);
+        k_closest<<<grid, block, 0, st>>>(S, pool, in);
+        done(r);
+        const bool media = s->has_media != 0;
+        r = mark(2);
+        switch (P.direct * 2 + (media ? 1 : 0)) {
+            case 0: k_shade<PTR_DIRECT_NONE, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            case 1: k_shade<PTR_DIRECT_NONE, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            case 2: k_shade<PTR_DIRECT_NEE, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            case 3: k_shade<PTR_DIRECT_NEE, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            case 4: k_shade<PTR_DIRECT_MIS, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            default: k_shade<PTR_DIRECT_MIS, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
+        }
+        done(r);
+        if (P.direct != PTR_DIRECT_NONE) {
+            r = mark(3);
+            if (media) k_shadow<true><<<grid, block, 0, st>>>(S, pool, P);
+            else k_shadow<false><<<grid, block, 0, st>>>(S, pool, P);
+            done(r);
+        }
+    }
+    r = mark(4);
+    k_film<<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples);
+    k_advance<<<1, 32, 0, st>>>(pool);
+    done(r);
+}
+
+int device_sms(int dev) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+// Acceleration structures of meshes and instanced batches (built on the host, uploaded once).
+int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
+    (void)s;
+    if (d->n_meshes > 0 || d->n_batches > 0) return fail(ctx, PTR_E_UNSUPPORTED, "meshes and instanced batches are not available in this build");
+    return PTR_OK;
+}
+
+int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples_dev) {
+    ptr_ctx* ctx = p->ctx;
+    if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return fail(ctx, PTR_E_INVALID, "frame: width, height and spp must be positive");
+    if (s->ctx != ctx) return fail(ctx, PTR_E_INVALID, "scene belongs to another context");
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t npix = (size_t)f->width * f->height;
+    if (p->fw != f->width || p->fh != f->height || !p->sum) {
+        if (p->sum) cudaFree(p->sum);
+        if (p->sumsq) cudaFree(p->sumsq);
+        if (p->export_buf) cudaFree(p->export_buf);
+        p->sum = p->sumsq = nullptr;
+        p->export_buf = nullptr;
+        if (cudaMalloc(&p->sum, npix * 3 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&p->sumsq, npix * 3 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&p->export_buf, npix * 3 * sizeof(float)) != cudaSuccess)
+            return fail(ctx, PTR_E_NOMEM, "film allocation failed");
+        p->fw = f->width;
+        p->fh = f->height;
+        p->nsamples = 0.0;
+        CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
+        CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
+    } else if (!f->accumulate) {
+        p->nsamples = 0.0;
+        CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
+        CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
+    }
+    const long long total = (long long)npix * f->spp;
+    // capacity: whole sample passes when a pass fits the pool, else a chunk of pixels
+    long long cap_max = 1ll << 21;
+    if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::atoll(env);
+    if (cap_max < 1024) cap_max = 1024;
+    long long cap;
+    if ((long long)npix <= cap_max) cap = (cap_max / (long long)npix) * (long long)npix;
+    else cap = cap_max;
+    if (cap > total) cap = total;
+    if (p->capacity < cap) {
+        int rc = alloc_pool(p, (int)cap);
+        if (rc) return rc;
+    }
+    if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
+    // The frame's parameters travel as a kernel argument into a device block: no host
+    // synchronisation, and the captured graph (which reads the block) stays valid.
+    FrameParams F;
+    F.width = f->width;
+    F.height = f->height;
+    F.spp = f->spp;
+    F.first_sample = f->first_sample;
+    F.salt = f->reset_salt;
+    F.px_off = f->pixel_offset[0];
+    F.py_off = f->pixel_offset[1];
+    F.total = total;
+    F.capacity = (int)cap;
+    F.cam = f->camera;
+    k_set_frame<<<1, 1, 0, st>>>(p->fp_dev, F);
+    CK(ctx, cudaGetLastError());
+    CK(ctx, cudaMemsetAsync(p->pool.wave, 0, 64, st));
+    CK(ctx, cudaMemsetAsync(p->pool.stats, 0, 64, st));
+    CK(ctx, cudaMemsetAsync(p->pool.cnt, 0, 64, st));
+    const int iters = wave_iterations(p, s);
+    const long long waves = (total + cap - 1) / cap;
+    const int n_sm = device_sms(ctx->device);
+    const bool profiling = p->profile_next != 0;
+    const bool use_graph = std::getenv("PTR_NO_GRAPH") == nullptr && !profiling;
+    if (use_graph) {
+        if (!p->graph || p->graph_scene != s || p->graph_w != f->width || p->graph_h != f->height ||
+            p->graph_iters != iters || p->graph_samples != samples_dev) {
+            if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+            cudaGraph_t g = nullptr;
+            CK(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            launch_wave(p, s, st, iters, samples_dev, n_sm);
+            cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (ce != cudaSuccess) return cuda_fail(ctx, ce, "graph capture");
+            ce = cudaGraphInstantiate(&p->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return cuda_fail(ctx, ce, "graph instantiate");
+            p->graph_scene = s;
+            p->graph_w = f->width;
+            p->graph_h = f->height;
+            p->graph_iters = iters;
+            p->graph_samples = samples_dev;
+        }
+        for (long long w = 0; w < waves; ++w) CK(ctx, cudaGraphLaunch(p->graph, st));
+    } else if (profiling) {
+        std::vector<ProfRec> prof;
+        prof.reserve((size_t)waves * (iters * 3 + 2));
+        for (long long w = 0; w < waves; ++w) launch_wave(p, s, st, iters, samples_dev, n_sm, &prof);
+        CK(ctx, cudaGetLastError());
+        CK(ctx, cudaStreamSynchronize(st));
+        for (int k = 0; k < 5; ++k) { p->prof_ms[k] = 0.f; p->prof_launches[k] = 0; }
+        for (ProfRec& r : prof) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            p->prof_ms[r.cls] += ms;
+            p->prof_launches[r.cls] += 1;
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        p->profile_next = 0;
+    } else {
+        for (long long w = 0; w < waves; ++w) launch_wave(p, s, st, iters, samples_dev, n_sm);
+        CK(ctx, cudaGetLastError());
+    }
+    p->nsamples += (double)f->spp;
+    return PTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptr_abi_version(void) { return PTR_ABI_VERSION; }
+
+int ptr_create(int device_ordinal, ptr_ctx** out) {
+    if (!out) return PTR_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return PTR_E_CUDA;
+    if (device_ordinal < 0 || device_ordinal >= n) return PTR_E_INVALID;
+    ptr_ctx* c = new ptr_ctx();
+    c->device = device_ordinal;
+    if (cudaSetDevice(device_ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PTR_E_CUDA;
+    }
+    *out = c;
+    return PTR_OK;
+}
+
+int ptr_destroy(ptr_ctx* ctx) {
+    if (!ctx) return PTR_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return PTR_OK;
+}
+
+const char* ptr_last_error(const ptr_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
+    if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
+    *out = nullptr;
+    if (d->abi_version != PTR_ABI_VERSION) return fail(ctx, PTR_E_INVALID, "scene: ABI version mismatch");
+    if (d->n_regions < 0 || d->n_materials <= 0 || d->n_lights < 0) return fail(ctx, PTR_E_INVALID, "scene: bad table sizes");
+    for (int i = 0; i < d->n_regions; ++i) {
+        const ptr_region& g = d->regions[i];
+        if (g.shape < 0 || g.shape > PTR_SHAPE_INSTANCES) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has an unknown shape");
+        if (g.material < 0 || g.material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has a material out of range");
+        if (g.shape == PTR_SHAPE_MESH && (g.ref < 0 || g.ref >= d->n_meshes)) return fail(ctx, PTR_E_INVALID, "scene: mesh region references a missing mesh");
+        if (g.shape == PTR_SHAPE_INSTANCES && (g.ref < 0 || g.ref >= d->n_batches)) return fail(ctx, PTR_E_INVALID, "scene: instanced region references a missing batch");
+        for (int k = 0; k < 15; ++k)
+            if (!std::isfinite(g.p[k])) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has a non-finite parameter");
+    }
+    for (int i = 0; i < d->n_lights; ++i) {
+        const ptr_light& l = d->lights[i];
+        if (l.region >= d->n_regions) return fail(ctx, PTR_E_INVALID, "scene: light region out of range");
+        if (!(l.select_pdf > 0.0f) || !std::isfinite(l.select_pdf)) return fail(ctx, PTR_E_INVALID, "scene: light selection pdf must be positive");
+    }
+    if (d->ambient_material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: ambient material out of range");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PTR_E_CUDA, "cudaSetDevice");
+    ptr_scene* s = new ptr_scene();
+    s->ctx = ctx;
+    DevScene& S = s->dev;
+    int rc = PTR_OK;
+    std::vector<int> lor(d->n_regions > 0 ? d->n_regions : 1, -1);
+    for (int i = 0; i < d->n_lights; ++i)
+        if (d->lights[i].region >= 0) lor[d->lights[i].region] = i;
+    if ((rc = dev_copy(ctx, s->allocs, d->regions, (size_t)d->n_regions, &S.regions)) ||
+        (rc = dev_copy(ctx, s->allocs, d->materials, (size_t)d->n_materials, &S.materials)) ||
+        (rc = dev_copy(ctx, s->allocs, d->lights, (size_t)d->n_lights, &S.lights)) ||
+        (rc = dev_copy(ctx, s->allocs, lor.data(), lor.size(), &S.light_of_region))) {
+        ptr_free_scene(s);
+        return rc;
+    }
+    S.n_regions = d->n_regions;
+    S.n_materials = d->n_materials;
+    S.n_lights = d->n_lights;
+    S.ambient_material = d->ambient_material;
+    bool media = d->ambient_material >= 0 && (d->materials[d->ambient_material].flags & PTR_MATF_MEDIUM);
+    for (int i = 0; i < d->n_materials; ++i)
+        if (d->materials[i].flags & PTR_MATF_MEDIUM) media = true;
+    S.has_media = media ? 1 : 0;
+    s->has_media = S.has_media;
+    S.env_kind = d->env.kind;
+    S.env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
+    S.env_select_live = S.env_samplable && d->n_lights > 0;
+    for (int k = 0; k < 4; ++k) S.env_color[k] = d->env.color[k];
+    S.env_intensity = d->env.intensity;
+    S.env_select_prob = d->env.select_prob;
+    S.env_rotation = d->env.rotation;
+    if (d->env.kind == PTR_ENV_IMAGE) {
+        S.env_w = d->env.width;
+        S.env_h = d->env.height;
+        const float* m = nullptr;
+        if ((rc = dev_copy(ctx, s->allocs, (const float4*)d->env.radiance, (size_t)S.env_w * S.env_h, &S.env_map)) ||
+            (rc = dev_copy(ctx, s->allocs, d->env.marginal, (size_t)S.env_h + 1, &S.env_marg)) ||
+            (rc = dev_copy(ctx, s->allocs, d->env.conditional, (size_t)S.env_h * (S.env_w + 1), &m))) {
+            ptr_free_scene(s);
+            return rc;
+        }
+        S.env_cond = m;
+    }
+    rc = upload_accels(ctx, s, d);
+    if (rc) {
+        ptr_free_scene(s);
+        return rc;
+    }
+    *out = s;
+    return PTR_OK;
+}
+
+int ptr_free_scene(ptr_scene* s) {
+    if (!s) return PTR_E_INVALID;
+    if (s->ctx) {
+        cudaSetDevice(s->ctx->device);
+        cudaStreamSynchronize(s->ctx->stream);
+    }
+    for (void* a : s->allocs) cudaFree(a);
+    delete s;
+    return PTR_OK;
+}
+
+int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* d, ptr_program** out) {
+    if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
+    *out = nullptr;
+    if (d->abi_version != PTR_ABI_VERSION) return fail(ctx, PTR_E_INVALID, "program: ABI version mismatch");
+    if (d->max_bounces < 0 || d->max_bounces > 4096) return fail(ctx, PTR_E_INVALID, "program: maxBounces out of range");
+    if (d->direct < PTR_DIRECT_NONE || d->direct > PTR_DIRECT_MIS) return fail(ctx, PTR_E_INVALID, "program: unknown directLighting");
+    if (d->rr_start >= 0 && !(d->rr_max_survival > 0.0f && d->rr_max_survival <= 1.0f))
+        return fail(ctx, PTR_E_INVALID, "program: russianRoulette.maxSurvival must be in (0, 1]");
+    if (d->max_null_crossings < 0 || d->max_null_crossings > 4096) return fail(ctx, PTR_E_INVALID, "program: maxNullCrossings out of range");
+    if (d->equiangular) return fail(ctx, PTR_E_UNSUPPORTED, "program: equiangular medium NEE is not available in this build");
+    ptr_program* p = new ptr_program();
+    p->ctx = ctx;
+    p->desc = *d;
+    *out = p;
+    return PTR_OK;
+}
+
+int ptr_free_program(ptr_program* p) {
+    if (!p) return PTR_E_INVALID;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    free_pool(p);
+    if (p->sum) cudaFree(p->sum);
+    if (p->sumsq) cudaFree(p->sumsq);
+    if (p->export_buf) cudaFree(p->export_buf);
+    if (p->fp_dev) cudaFree(p->fp_dev);
+    delete p;
+    return PTR_OK;
+}
+
+int ptr_render(ptr_program* p, ptr_scene* s, const ptr_frame* f) {
+    if (!p || !s || !f) return PTR_E_INVALID;
+    return render_impl(p, s, f, nullptr);
+}
+
+int ptr_render_samples(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* host_out, size_t n) {
+    if (!p || !s || !f || !host_out) return PTR_E_INVALID;
+    ptr_ctx* ctx = p->ctx;
+    size_t need = (size_t)f->width * f->height * f->spp * 3;
+    if (n < need) return fail(ctx, PTR_E_INVALID, "ptr_render_samples: destination too small");
+    float* dev = nullptr;
+    CK(ctx, cudaSetDevice(ctx->device));
+    if (cudaMalloc(&dev, need * sizeof(float)) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, "samples buffer");
+    int rc = render_impl(p, s, f, dev);
+    if (rc == PTR_OK) {
+        cudaError_t e = cudaMemcpyAsync(host_out, dev, need * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "samples readback");
+    }
+    if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+    cudaFree(dev);
+    return rc;
+}
+
+int ptr_get_stream(ptr_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return PTR_E_INVALID;
+    *stream = (void*)ctx->stream;
+    return PTR_OK;
+}
+
+int ptr_sync(ptr_ctx* ctx, int timeout_ms) {
+    if (!ctx) return PTR_E_INVALID;
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) return PTR_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "stream");
+        if (timeout_ms >= 0) {
+            auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+            if (ms >= timeout_ms) return fail(ctx, PTR_E_TIMEOUT, "ptr_sync: timed out with work in flight");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
+static int export_impl(ptr_program* p, const char* name, float* dst, size_t n, bool device_dst) {
+    ptr_ctx* ctx = p->ctx;
+    if (!name || !dst) return fail(ctx, PTR_E_INVALID, "export: null argument");
+    const size_t npix = (size_t)p->fw * p->fh;
+    if (!p->sum) return fail(ctx, PTR_E_INVALID, "export: nothing rendered yet");
+    CK(ctx, cudaSetDevice(ctx->device));
+    if (std::strcmp(name, "samples") == 0) {
+        if (n < npix) return fail(ctx, PTR_E_INVALID, "export: destination too small");
+        std::vector<float> v(npix, (float)p->nsamples);
+        if (device_dst) CK(ctx, cudaMemcpyAsync(dst, v.data(), npix * 4, cudaMemcpyHostToDevice, ctx->stream));
+        else std::memcpy(dst, v.data(), npix * 4);
+        if (device_dst) CK(ctx, cudaStreamSynchronize(ctx->stream));
+        return PTR_OK;
+    }
+    int what;
+    if (std::strcmp(name, "radiance") == 0) what = 0;
+    else if (std::strcmp(name, "variance") == 0) what = 1;
+    else return fail(ctx, PTR_E_INVALID, std::string("export: unknown export '") + name + "'");
+    if (n < npix * 3) return fail(ctx, PTR_E_INVALID, "export: destination too small");
+    float* target = device_dst ? dst : p->export_buf;
+    k_export<<<256, 256, 0, ctx->stream>>>(p->sum, p->sumsq, p->nsamples > 0 ? p->nsamples : 1.0, (int)npix, what, target);
+    CK(ctx, cudaGetLastError());
+    if (!device_dst) {
+        CK(ctx, cudaMemcpyAsync(dst, p->export_buf, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return PTR_OK;
+}
+
+int ptr_read_export(ptr_program* p, const char* name, float* dst, size_t n) {
+    if (!p) return PTR_E_INVALID;
+    return export_impl(p, name, dst, n, false);
+}
+
+int ptr_read_export_device(ptr_program* p, const char* name, float* dst, size_t n) {
+    if (!p) return PTR_E_INVALID;
+    return export_impl(p, name, dst, n, true);
+}
+
+int ptr_get_counters(ptr_program* p, ptr_counters* out) {
+    if (!p || !out) return PTR_E_INVALID;
+    ptr_ctx* ctx = p->ctx;
+    std::memset(out, 0, sizeof(*out));
+    if (!p->pool.stats) return PTR_OK;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned long long st[3] = {0, 0, 0};
+    unsigned cnt[4] = {0, 0, 0, 0};
+    CK(ctx, cudaMemcpy(st, p->pool.stats, sizeof(st), cudaMemcpyDeviceToHost));
+    CK(ctx, cudaMemcpy(cnt, p->pool.cnt, sizeof(cnt), cudaMemcpyDeviceToHost));
+    out->closest_queries = st[0];
+    out->shadow_queries = st[1];
+    out->paths = st[2];
+    out->error_flags = cnt[3];
+    return PTR_OK;
+}
+
+int ptr_profile_next(ptr_program* p, int enable) {
+    if (!p) return PTR_E_INVALID;
+    p->profile_next = enable;
+    return PTR_OK;
+}
+
+int ptr_get_profile(ptr_program* p, float* ms_out, int* launches_out, int n) {
+    if (!p) return PTR_E_INVALID;
+    for (int i = 0; i < n && i < 5; ++i) {
+        if (ms_out) ms_out[i] = p->prof_ms[i];
+        if (launches_out) launches_out[i] = p->prof_launches[i];
+    }
+    return PTR_OK;
+}
+
+}  // extern "C"

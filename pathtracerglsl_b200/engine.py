@@ -1,0 +1,203 @@
+"""CudaEngine — the executor a CompiledRenderer runs on, over the C ABI.
+
+Mirrors the reference's Engine surface (``src/engine/Engine.ts:83-438``):
+
+* ``register_scene``  ~ ``registerDataTexture`` for the whole scene-data plan (:438)
+* ``load_renderer`` / ``select_renderer`` (:147-186)
+* ``render_frame``    ~ ``renderFrame`` (:190-204): sampleCount advances per sample,
+  resetSalt decorrelates accumulation resets; ``spp`` folds several frames per call
+* ``read_export``     ~ ``readExport`` (:351): linear HDR radiance / variance
+* ``reset`` / ``pin_reset_salt`` ~ accumulation reset and the witness salt pin
+
+Errors from the library raise ``EngineError`` carrying ``ptr_last_error``.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._native import load
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, message):
+        self.code = code
+        super().__init__(f"ptx_rt error {code}: {message}")
+
+
+class CudaEngine:
+    def __init__(self, device=0):
+        self.lib = load()
+        self.ctx = C.c_void_p()
+        rc = self.lib.ptr_create(device, C.byref(self.ctx))
+        if rc != abi.PTR_OK:
+            raise EngineError(rc, f"cannot create a context on CUDA device {device}")
+        self.scene = None
+        self._scene_data = None
+        self.programs = {}
+        self.renderers = {}
+        self.current = None
+        self.sample_count = 0
+        self.reset_salt = 0
+        self._pinned_salt = None
+        self.width = self.height = 0
+        self.params = {}
+
+    # -- errors ---------------------------------------------------------------------
+    def _check(self, rc):
+        if rc != abi.PTR_OK:
+            msg = self.lib.ptr_last_error(self.ctx)
+            raise EngineError(rc, msg.decode() if msg else "")
+        return rc
+
+    # -- scene data --------------------------------------------------------------------
+    def register_scene(self, packed):
+        """Upload a packed scene (host arrays are copied; the host keeps ownership)."""
+        if self.scene is not None:
+            self.lib.ptr_free_scene(self.scene)
+            self.scene = None
+        desc = packed.desc()
+        h = C.c_void_p()
+        self._check(self.lib.ptr_upload_scene(self.ctx, C.byref(desc), C.byref(h)))
+        self.scene = h
+        self._scene_data = packed
+        self.reset()
+
+    # -- renderers ----------------------------------------------------------------------
+    def load_renderer(self, renderer):
+        h = C.c_void_p()
+        self._check(self.lib.ptr_compile(self.ctx, C.byref(renderer.program), C.byref(h)))
+        if renderer.id in self.programs:
+            self.lib.ptr_free_program(self.programs[renderer.id])
+        self.programs[renderer.id] = h
+        self.renderers[renderer.id] = renderer
+        if self.current is None:
+            self.current = renderer.id
+        return renderer.id
+
+    def select_renderer(self, rid):
+        if rid not in self.programs:
+            raise KeyError(f"renderer {rid!r} not loaded")
+        self.current = rid
+        self.reset()
+
+    def set_parameter(self, path, value):
+        """Live parameter (camera.* re-evaluates the camera uniforms; a triggersReset
+        parameter resets accumulation)."""
+        self.params[path] = value
+        self.reset()
+
+    # -- accumulation ---------------------------------------------------------------------
+    def pin_reset_salt(self, salt):
+        self._pinned_salt = salt
+        self.reset_salt = salt
+
+    def reset(self):
+        self.sample_count = 0
+        if self._pinned_salt is None:
+            self.reset_salt += 1
+        else:
+            self.reset_salt = self._pinned_salt
+
+    def _frame(self, width, height, spp, accumulate):
+        r = self.renderers[self.current]
+        fr = abi.Frame()
+        fr.width, fr.height = width, height
+        fr.first_sample = self.sample_count
+        fr.spp = spp
+        fr.reset_salt = self.reset_salt & 0xFFFFFFFF
+        fr.accumulate = 1 if accumulate else 0
+        fr.camera = r.camera(self.params, width, height)
+        return fr
+
+    def render_frame(self, width, height, spp=1, sync=False):
+        """Render ``spp`` more samples per pixel into the current renderer's film."""
+        if self.scene is None or self.current is None:
+            raise EngineError(abi.PTR_E_INVALID, "no scene registered or no renderer loaded")
+        if (width, height) != (self.width, self.height):
+            self.width, self.height = width, height
+            self.reset()
+        fr = self._frame(width, height, spp, accumulate=self.sample_count > 0)
+        self._check(self.lib.ptr_render(self.programs[self.current], self.scene, C.byref(fr)))
+        self.sample_count += spp
+        if sync:
+            self.sync()
+        return self.sample_count
+
+    def render_samples(self, width, height, spp):
+        """Render and also return every sample's radiance, shape (spp, H, W, 3)."""
+        self.width, self.height = width, height
+        fr = self._frame(width, height, spp, accumulate=self.sample_count > 0)
+        out = np.zeros((spp, height, width, 3), np.float32)
+        self._check(self.lib.ptr_render_samples(self.programs[self.current], self.scene, C.byref(fr),
+                                                out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        self.sample_count += spp
+        return out
+
+    def stream_handle(self):
+        """The context's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
+        h = C.c_void_p()
+        self._check(self.lib.ptr_get_stream(self.ctx, C.byref(h)))
+        return h.value or 0
+
+    def sync(self, timeout_ms=-1):
+        self._check(self.lib.ptr_sync(self.ctx, timeout_ms))
+
+    def read_export(self, name="radiance", out=None):
+        """Linear HDR export as (H, W, 3) float32, row 0 = bottom (gl_FragCoord order)."""
+        if out is None:
+            out = np.empty((self.height, self.width, 3), np.float32)
+        self._check(self.lib.ptr_read_export(self.programs[self.current], name.encode(),
+                                             out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film")
+
+    def profile_render(self, width, height, spp):
+        """Render once with CUDA events around every launch; per kernel class returns
+        (summed device ms, launch count)."""
+        self._check(self.lib.ptr_profile_next(self.programs[self.current], 1))
+        self.render_frame(width, height, spp, sync=True)
+        ms = (C.c_float * 5)()
+        n = (C.c_int * 5)()
+        self._check(self.lib.ptr_get_profile(self.programs[self.current], ms, n, 5))
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def counters(self):
+        c = abi.Counters()
+        self._check(self.lib.ptr_get_counters(self.programs[self.current], C.byref(c)))
+        return {"paths": c.paths, "closest_queries": c.closest_queries, "shadow_queries": c.shadow_queries,
+                "error_flags": c.error_flags}
+
+    def close(self):
+        for h in self.programs.values():
+            self.lib.ptr_free_program(h)
+        self.programs.clear()
+        if self.scene is not None:
+            self.lib.ptr_free_scene(self.scene)
+            self.scene = None
+        if self.ctx:
+            self.lib.ptr_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render(scene, strategy, width, height, spp, params=None, salt=0, device=0, engine=None):
+    """Compile, upload and render one scene x strategy; returns (mean, variance, engine)."""
+    from .compiler import Compiler
+    renderer, packed = Compiler().compile(scene, strategy, params)
+    eng = engine or CudaEngine(device)
+    eng.register_scene(packed)
+    eng.load_renderer(renderer)
+    eng.select_renderer(renderer.id)
+    eng.params = dict(params or {})
+    eng.pin_reset_salt(salt)
+    eng.render_frame(width, height, spp)
+    mean = eng.read_export("radiance")
+    var = eng.read_export("variance")
+    return mean, var, eng
