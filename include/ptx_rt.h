@@ -232,6 +232,26 @@ int ptr_render_samples(ptr_program* prog, ptr_scene* scene, const ptr_frame* fra
  * (timing events, cache flushes) with the library's launches. */
 int ptr_get_stream(ptr_ctx* ctx, void** stream);
 
+/* Allocation-free rendering.  No counterpart in the reference (its WebGL engine owns all
+ * GPU memory); added for callers that cannot allocate device memory themselves: hosts
+ * that give the whole GPU to their own memory pool, plugin hosts that forbid driver
+ * allocations in their frame loop, or loops that cannot take the device-wide stall an
+ * allocation may cause.  It renders frame->spp samples per pixel of an ANALYTIC scene
+ * (no meshes, no instanced batches, no image environment) given as host tables like
+ * ptr_upload_scene, on `stream` (a cudaStream_t, NULL = the legacy default stream), and
+ * accumulates into the caller's device film buffers sum_dev / sumsq_dev (3 doubles per
+ * pixel each; cleared first unless frame->accumulate).  It calls no cudaMalloc, cudaFree
+ * or other allocating routine: the scene tables and the path pool live in one fixed
+ * array inside the library, about 15 MB on every GPU that loads the library, held until
+ * the process exits, for at most 65536 paths in flight (larger frames run in waves) and
+ * at most 256 regions, materials and lights (more returns PTR_E_INVALID).
+ * The first call on each device looks the array's device address up (with that device
+ * current); make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU race.  The current device must be set by the
+ * caller.  Returns a PTR_E_* status (messages go to stderr; there is no context). */
+int ptr_render_noalloc(const ptr_scene_desc* scene, const ptr_program_desc* prog, const ptr_frame* frame,
+                       double* sum_dev, double* sumsq_dev, void* stream);
+
 /* Wait for the context's stream, at most timeout_ms (<0 = no limit). */
 int ptr_sync(ptr_ctx* ctx, int timeout_ms);
 

@@ -23,6 +23,8 @@ SIGNATURES = {
     "ptr_render": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame)]),
     "ptr_render_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame), C.POINTER(C.c_float), C.c_size_t]),
     "ptr_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ptr_render_noalloc": (C.c_int, [C.POINTER(abi.SceneDesc), C.POINTER(abi.ProgramDesc), C.POINTER(abi.Frame),
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "ptr_sync": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_read_export": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_float), C.c_size_t]),
     "ptr_read_export_device": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),

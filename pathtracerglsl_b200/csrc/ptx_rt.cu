@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <chrono>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -576,3 +577,187 @@ int ptr_get_profile(ptr_program* p, float* ms_out, int* launches_out, int n) {
 }
 
 }  // extern "C"
+
+// =====================================================================================
+// Allocation-free rendering (ptr_render_noalloc).
+//
+// Some callers cannot allocate device memory: an application that hands every byte of
+// the GPU to its own memory pool, a plugin host that forbids driver allocations inside
+// its frame loop, or a real-time loop that cannot afford the device-wide synchronisation
+// cudaMalloc/cudaFree may imply.  For them this entry point renders analytic scenes with
+// no allocation at all: the scene tables and the path pool live in one file-scope
+// __device__ array of fixed size, and the caller passes its own film buffers.
+//
+// Limits: at most kNoAllocMaxPaths paths in flight (frames of any size are processed in
+// waves) and at most kNoAllocMaxTable regions, materials and lights.  The array costs
+// about 15 MB on every GPU that loads this library, held until the process exits.
+// Every call shares the array: calls that overlap on the GPU (on different streams, or
+// from different host threads) race and corrupt each other's paths.
+// =====================================================================================
+namespace {
+
+constexpr int kNoAllocMaxPaths = 1 << 16;
+constexpr int kNoAllocMaxTable = 256;
+
+// Byte layout of the array: small blocks first, then the path pool.
+constexpr size_t kNaCnt = 0;                                            // 16 x u32
+constexpr size_t kNaStats = 64;                                         // 8 x u64
+constexpr size_t kNaWave = 128;                                         // 8 x i64
+constexpr size_t kNaFrame = 256;                                        // FrameParams
+constexpr size_t kNaRegions = 1024;
+constexpr size_t kNaMaterials = kNaRegions + sizeof(ptr_region) * kNoAllocMaxTable;
+constexpr size_t kNaLights = kNaMaterials + sizeof(ptr_material) * kNoAllocMaxTable;
+constexpr size_t kNaLightOf = kNaLights + sizeof(ptr_light) * kNoAllocMaxTable;
+constexpr size_t kNaPool = (kNaLightOf + sizeof(int) * kNoAllocMaxTable + 255) / 256 * 256;
+constexpr size_t kNaPathBytes = 13 * 16 + 8 + 3 * 4;                    // per path, see na_pool()
+constexpr size_t kNaBytes = kNaPool + kNaPathBytes * (size_t)kNoAllocMaxPaths;
+static_assert(sizeof(FrameParams) <= kNaRegions - kNaFrame, "FrameParams block too small");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_na_mutex;
+unsigned char* g_na_addr[kMaxDevices] = {nullptr};
+
+// Device address of the array on the current device, looked up once per device.  The
+// array's host-side name is only a stand-in; kernels must be given this address.
+int na_address(int dev, unsigned char** out, const char** why) {
+    if (dev < 0 || dev >= kMaxDevices) { *why = "device ordinal out of range"; return PTR_E_INVALID; }
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            *why = cudaGetErrorString(e);
+            return PTR_E_CUDA;
+        }
+        g_na_addr[dev] = (unsigned char*)p;
+    }
+    *out = g_na_addr[dev];
+    return PTR_OK;
+}
+
+PathPool na_pool(unsigned char* base) {
+    PathPool q{};
+    size_t c = kNoAllocMaxPaths;
+    unsigned char* p = base + kNaPool;
+    auto take = [&](size_t bytes) { unsigned char* r = p; p += bytes * c; return (void*)r; };
+    q.ray_o = (float4*)take(16); q.ray_d = (float4*)take(16); q.thr = (float4*)take(16);
+    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.st = (int4*)take(16);
+    q.hit = (float4*)take(16); q.hit_i = (int4*)take(16); q.sh_o = (float4*)take(16);
+    q.sh_d = (float4*)take(16); q.sh_lp = (float4*)take(16); q.sh_c = (float4*)take(16);
+    q.rng = (uint2*)take(8); q.q[0] = (int*)take(4); q.q[1] = (int*)take(4); q.shq = (int*)take(4);
+    q.cnt = (unsigned*)(base + kNaCnt);
+    q.stats = (unsigned long long*)(base + kNaStats);
+    q.wave = (long long*)(base + kNaWave);
+    return q;
+}
+
+}  // namespace
+
+extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_desc* pd, const ptr_frame* f,
+                                  double* sum_dev, double* sumsq_dev, void* stream) {
+    if (!d || !pd || !f || !sum_dev || !sumsq_dev) return PTR_E_INVALID;
+    if (d->abi_version != PTR_ABI_VERSION || pd->abi_version != PTR_ABI_VERSION) return PTR_E_INVALID;
+    if (d->n_regions < 0 || d->n_regions > kNoAllocMaxTable || d->n_materials <= 0 || d->n_materials > kNoAllocMaxTable ||
+        d->n_lights < 0 || d->n_lights > kNoAllocMaxTable) {
+        std::fprintf(stderr, "ptr_render_noalloc: scene tables exceed the fixed maximum of %d regions, materials and lights\n",
+                     kNoAllocMaxTable);
+        return PTR_E_INVALID;
+    }
+    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE) {
+        std::fprintf(stderr, "ptr_render_noalloc: only analytic scenes with a constant or no environment are supported\n");
+        return PTR_E_UNSUPPORTED;
+    }
+    if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return PTR_E_INVALID;
+    if (pd->max_bounces < 0 || pd->max_bounces > 4096 || pd->direct < 0 || pd->direct > 2 || pd->equiangular) return PTR_E_INVALID;
+    for (int i = 0; i < d->n_regions; ++i)
+        if (d->regions[i].shape > PTR_SHAPE_BOX || d->regions[i].material < 0 || d->regions[i].material >= d->n_materials)
+            return PTR_E_INVALID;
+    if (d->ambient_material >= d->n_materials) return PTR_E_INVALID;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PTR_E_CUDA;
+    unsigned char* base = nullptr;
+    const char* why = "";
+    int rc = na_address(dev, &base, &why);
+    if (rc) {
+        std::fprintf(stderr, "ptr_render_noalloc: cudaGetSymbolAddress failed: %s\n", why);
+        return rc;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // scene tables into the array (host arrays on the caller's side; no staging allocation)
+    int lor[kNoAllocMaxTable];
+    for (int i = 0; i < kNoAllocMaxTable; ++i) lor[i] = -1;
+    for (int i = 0; i < d->n_lights; ++i)
+        if (d->lights[i].region >= 0 && d->lights[i].region < d->n_regions) lor[d->lights[i].region] = i;
+    if (d->n_regions && cudaMemcpyAsync(base + kNaRegions, d->regions, sizeof(ptr_region) * d->n_regions, cudaMemcpyHostToDevice, st) != cudaSuccess) return PTR_E_CUDA;
+    if (cudaMemcpyAsync(base + kNaMaterials, d->materials, sizeof(ptr_material) * d->n_materials, cudaMemcpyHostToDevice, st) != cudaSuccess) return PTR_E_CUDA;
+    if (d->n_lights && cudaMemcpyAsync(base + kNaLights, d->lights, sizeof(ptr_light) * d->n_lights, cudaMemcpyHostToDevice, st) != cudaSuccess) return PTR_E_CUDA;
+    if (cudaMemcpyAsync(base + kNaLightOf, lor, sizeof(int) * kNoAllocMaxTable, cudaMemcpyHostToDevice, st) != cudaSuccess) return PTR_E_CUDA;
+    // the previous call's counters, statistics and wave cursor must not leak in
+    if (cudaMemsetAsync(base, 0, kNaFrame, st) != cudaSuccess) return PTR_E_CUDA;
+    const size_t npix = (size_t)f->width * f->height;
+    if (!f->accumulate) {
+        if (cudaMemsetAsync(sum_dev, 0, npix * 3 * sizeof(double), st) != cudaSuccess) return PTR_E_CUDA;
+        if (cudaMemsetAsync(sumsq_dev, 0, npix * 3 * sizeof(double), st) != cudaSuccess) return PTR_E_CUDA;
+    }
+    DevScene S{};
+    S.regions = (const ptr_region*)(base + kNaRegions);
+    S.materials = (const ptr_material*)(base + kNaMaterials);
+    S.lights = (const ptr_light*)(base + kNaLights);
+    S.light_of_region = (const int*)(base + kNaLightOf);
+    S.n_regions = d->n_regions;
+    S.n_materials = d->n_materials;
+    S.n_lights = d->n_lights;
+    S.ambient_material = d->ambient_material;
+    bool media = d->ambient_material >= 0 && (d->materials[d->ambient_material].flags & PTR_MATF_MEDIUM);
+    for (int i = 0; i < d->n_materials; ++i)
+        if (d->materials[i].flags & PTR_MATF_MEDIUM) media = true;
+    S.has_media = media ? 1 : 0;
+    S.env_kind = d->env.kind;
+    S.env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
+    S.env_select_live = S.env_samplable && d->n_lights > 0;
+    for (int k = 0; k < 4; ++k) S.env_color[k] = d->env.color[k];
+    S.env_intensity = d->env.intensity;
+    S.env_select_prob = d->env.select_prob;
+    S.env_rotation = d->env.rotation;
+
+    const long long total = (long long)npix * f->spp;
+    long long cap = (long long)npix <= kNoAllocMaxPaths ? (kNoAllocMaxPaths / (long long)npix) * (long long)npix
+                                                        : (long long)kNoAllocMaxPaths;
+    if (cap > total) cap = total;
+    FrameParams F;
+    F.width = f->width;
+    F.height = f->height;
+    F.spp = f->spp;
+    F.first_sample = f->first_sample;
+    F.salt = f->reset_salt;
+    F.px_off = f->pixel_offset[0];
+    F.py_off = f->pixel_offset[1];
+    F.total = total;
+    F.capacity = (int)cap;
+    F.cam = f->camera;
+    FrameParams* fp = (FrameParams*)(base + kNaFrame);
+    k_set_frame<<<1, 1, 0, st>>>(fp, F);
+
+    // the same wave sequence as ptr_render, launched directly
+    ptr_program prog;
+    prog.desc = *pd;
+    prog.pool = na_pool(base);
+    prog.fp_dev = fp;
+    prog.sum = sum_dev;
+    prog.sumsq = sumsq_dev;
+    ptr_scene scene;
+    scene.dev = S;
+    scene.has_media = S.has_media;
+    const int iters = wave_iterations(&prog, &scene);
+    const long long waves = (total + cap - 1) / cap;
+    const int n_sm = device_sms(dev);
+    for (long long w = 0; w < waves; ++w) launch_wave(&prog, &scene, st, iters, nullptr, n_sm);
+    // keep the stack objects from releasing anything they do not own
+    prog.pool = PathPool{};
+    prog.fp_dev = nullptr;
+    prog.sum = prog.sumsq = nullptr;
+    if (cudaGetLastError() != cudaSuccess) return PTR_E_CUDA;
+    return PTR_OK;
+}
