@@ -376,6 +376,7 @@ class Compiler:
                 rec.region = len(regions)
                 regions.append(reg)
                 region_names.append(f"light_{li}")
+                geom = area
             elif kind == "sphere":
                 center = l.get("position", l.get("center"))
                 rad = l["radius"]
@@ -390,9 +391,11 @@ class Compiler:
                 rec.region = len(regions)
                 regions.append(reg)
                 region_names.append(f"light_{li}")
+                geom = float(rad)
             else:   # point: delta, registry entry only
                 rec.p = (abi.C.c_float * 16)(*list(l["position"]))
-            lights.append((rec, kind, e))
+                geom = None
+            lights.append((rec, kind, e, geom))
         for i, o in enumerate(scene.get("objects", [])):
             if o.get("kind") is not None:
                 continue
@@ -406,40 +409,31 @@ class Compiler:
             rec.region = i
             rec.radiance = abi.F4(*(e + [0.0]))
             reg = regions[i]
+            pp = o.get("parameters", {})
             if o["type"] == "sphere":
                 rec.kind = abi.LIGHT_SPHERE
                 rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:4])))
+                geom = float(pp["radius"]) * float((o.get("transform") or {}).get("scale", 1.0))
             else:
                 rec.kind = abi.LIGHT_QUAD
-                e1, e2 = list(reg.p[3:6]), list(reg.p[6:9])
-                c = _cross(e1, e2)
+                c = _cross(pp["edge1"], pp["edge2"])
                 area = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
                 rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:12]) + [area]))
-            lights.append((rec, o["type"], e))
+                geom = area
+            lights.append((rec, o["type"], e, geom))
 
         # Selection CDF (features/lighting.ts computeSelectPdf; power per kind from the
         # descriptors: quad pi*A*Le, sphere pi*4*pi*r^2*Le, point 4*pi*I).
         sel_mode = "power"
         for st in strategies:
             sel_mode = st.get("estimator", {}).get("lightSelection", "power")
-        weights = []
-        for rec, kind, e in lights:
-            mean = (e[0] + e[1] + e[2]) / 3.0
-            if sel_mode == "uniform":
-                w = 1.0
-            elif rec.kind == abi.LIGHT_QUAD:
-                w = max(1e-8, math.pi * rec.p[12] * mean)
-            elif rec.kind == abi.LIGHT_SPHERE:
-                r = rec.p[3]
-                w = max(1e-8, math.pi * 4 * math.pi * r * r * mean)
-            else:
-                w = max(1e-8, 4 * math.pi * mean)
-            weights.append(w)
+        weights = [1.0 if sel_mode == "uniform" else _light_power(rec.kind, e, geom)
+                   for rec, kind, e, geom in lights]
         total = sum(weights)
         acc = 0.0
         light_arr = np.zeros(len(lights), dtype=np.dtype((np.void, abi.C.sizeof(abi.Light))))
         light_recs = (abi.Light * max(len(lights), 1))()
-        for i, (rec, kind, e) in enumerate(lights):
+        for i, (rec, kind, e, geom) in enumerate(lights):
             pdf = weights[i] / total
             acc += pdf
             rec.select_pdf = pdf
@@ -615,15 +609,7 @@ class Compiler:
                     extent += max(v) if isinstance(v, (list, tuple)) else float(v)
             r = max(r, center + extent)
         phi_env = 4 * math.pi * math.pi * r * r * mean_l * intensity
-        phi_fin = 0.0
-        for rec, kind, e in lights:
-            mean = (e[0] + e[1] + e[2]) / 3.0
-            if rec.kind == abi.LIGHT_QUAD:
-                phi_fin += max(1e-8, math.pi * rec.p[12] * mean)
-            elif rec.kind == abi.LIGHT_SPHERE:
-                phi_fin += max(1e-8, math.pi * 4 * math.pi * rec.p[3] ** 2 * mean)
-            else:
-                phi_fin += max(1e-8, 4 * math.pi * mean)
+        phi_fin = sum(_light_power(rec.kind, e, geom) for rec, kind, e, geom in lights)
         return min(0.99, max(0.01, phi_env / max(phi_env + phi_fin, 1e-20)))
 
     # -- Generate: the program description (flags of plan/types.ts:39-112) -------------
@@ -652,6 +638,18 @@ class Compiler:
         rid = f"{st.get('id', 'strategy')}-{scene.get('id', 'scene')}"
         exports = {"radiance": {"format": "float"}, "variance": {"format": "float"}}
         return CompiledRenderer(rid, prog, st, parameters, exports)
+
+
+def _light_power(kind, e, geom):
+    """Emitted power for the selection CDF, from the authored float64 values like the
+    kind descriptors (lights/quad/quad.ts:46 pi*A*Le, sphere.ts:24 pi*4*pi*r^2*Le,
+    point.ts:24 4*pi*I; radiantScalar = channel mean)."""
+    mean = (e[0] + e[1] + e[2]) / 3.0
+    if kind == abi.LIGHT_QUAD:
+        return max(1e-8, math.pi * geom * mean)
+    if kind == abi.LIGHT_SPHERE:
+        return max(1e-8, math.pi * 4 * math.pi * geom * geom * mean)
+    return max(1e-8, 4 * math.pi * mean)
 
 
 def _qrot(q, v):

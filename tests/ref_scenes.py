@@ -157,6 +157,65 @@ ORB = {
     "environment": {"type": "constant", "color": [0.03, 0.035, 0.05], "intensity": 1.0},
 }
 
+ORB_NEE = {"id": "pt-nee",
+           "measurement": {"camera": {"type": "pinhole", "fov": 0.8, "position": [0, 1.3, 3.4], "target": [0, 0.7, 0]},
+                           "maxBounces": 12},
+           "estimator": {"directLighting": "nee", "russianRoulette": {"startDepth": 3}, "accumulation": {"type": "average"}},
+           "view": {"tonemap": {"type": "reinhard"}}}
+
+# ggxScenes.ts:16-75 (veach-mis: GGX plates under three sphere lights)
+VEACH = {
+    "id": "veach-mis", "ambientSpace": {"type": "euclidean"},
+    "objects": [
+        {"type": "quad", "parameters": {"corner": [-1.8, 1.113, -0.54], "edge1": [0.0, -0.125, 0.38], "edge2": [3.6, 0.0, 0.0]}, "material": "plate1"},
+        {"type": "quad", "parameters": {"corner": [-1.8, 0.769, 0.156], "edge1": [0.0, -0.099, 0.388], "edge2": [3.6, 0.0, 0.0]}, "material": "plate2"},
+        {"type": "quad", "parameters": {"corner": [-1.8, 0.457, 0.853], "edge1": [0.0, -0.074, 0.393], "edge2": [3.6, 0.0, 0.0]}, "material": "plate3"},
+        {"type": "quad", "parameters": {"corner": [-1.8, 0.173, 1.551], "edge1": [0.0, -0.047, 0.397], "edge2": [3.6, 0.0, 0.0]}, "material": "plate4"},
+        {"type": "plane", "parameters": {"normal": [0, 1, 0], "offset": 0.35}, "material": "floor"},
+    ],
+    "materials": {
+        "plate1": {"model": "ggx", "f0": [0.95, 0.93, 0.88], "roughness": 0.1},
+        "plate2": {"model": "ggx", "f0": [0.95, 0.93, 0.88], "roughness": 0.22},
+        "plate3": {"model": "ggx", "f0": [0.95, 0.93, 0.88], "roughness": 0.38},
+        "plate4": {"model": "ggx", "f0": [0.95, 0.93, 0.88], "roughness": 0.6},
+        "floor": {"model": "lambert", "albedo": [0.18, 0.18, 0.2]},
+    },
+    "lights": [
+        {"kind": "sphere", "position": [-1.15, 2.3, -1.9], "radius": 0.035, "emission": [150, 127.5, 105]},
+        {"kind": "sphere", "position": [0.0, 2.3, -1.9], "radius": 0.14, "emission": [8.46, 9.4, 7.99]},
+        {"kind": "sphere", "position": [1.15, 2.3, -1.9], "radius": 0.5, "emission": [0.592, 0.666, 0.74]},
+    ],
+    "environment": {"type": "constant", "color": [0.015, 0.015, 0.02], "intensity": 1.0},
+}
+VEACH_MIS = {"id": "pt-mis",
+             "measurement": {"camera": {"type": "pinhole", "fov": 0.8, "position": [0, 1.3, 5.5], "target": [0, 0.55, 0]},
+                             "maxBounces": 6},
+             "estimator": {"directLighting": "mis", "russianRoulette": {"startDepth": 3}, "accumulation": {"type": "average"}},
+             "view": {"tonemap": {"type": "reinhard"}}}
+
+# twoLightScene.ts:17-80 (point lights under the power CDF)
+TWO_LIGHT = {
+    "id": "two-light", "ambientSpace": {"type": "euclidean"},
+    "objects": [
+        {"type": "plane", "parameters": {"normal": [0, 1, 0], "offset": 0.0}, "material": "floor"},
+        {"type": "plane", "parameters": {"normal": [0, 0, 1], "offset": 3.0}, "material": "floor"},
+        {"type": "sphere", "parameters": {"center": [-0.75, 0.5, 0], "radius": 0.5}, "material": "ivory"},
+        {"type": "sphere", "parameters": {"center": [0.75, 0.5, 0], "radius": 0.5}, "material": "ivory"},
+    ],
+    "materials": {"floor": {"model": "lambert", "albedo": [0.6, 0.6, 0.6]},
+                  "ivory": {"model": "lambert", "albedo": [0.82, 0.78, 0.68]}},
+    "lights": [{"kind": "point", "position": [-2.5, 3.0, 1.5], "emission": [26, 14.3, 6.5]},
+               {"kind": "point", "position": [2.5, 2.5, 1.5], "emission": [4.9, 7.7, 14]}],
+    "environment": {"type": "none"},
+}
+TWO_LIGHT_POWER = {"id": "power",
+                   "measurement": {"camera": {"type": "pinhole", "fov": 0.9, "position": [0, 1.2, 4], "target": [0, 0.5, 0]},
+                                   "maxBounces": 6},
+                   "estimator": {"directLighting": "nee", "russianRoulette": None, "lightSelection": "power",
+                                 "accumulation": {"type": "average"}},
+                   "view": {"tonemap": {"type": "reinhard"}}}
+HAZE_NEE["measurement"]["camera"].update({"position": [0, 1.2, 5], "target": [0, 1.2, -1]})
+
 # (scene, strategy, snapshot program, camera parameters of that program)
 CASES = {
     "cornell_area_glass_pt_mis": (CORNELL_AREA_GLASS, CORNELL_AREA_MIS),
@@ -169,4 +228,8 @@ CASES = {
     "slab_witness": (SLAB, SLAB_STRATEGY),
     "fog_area_pt_mis": (FOG_AREA, FOG_AREA_MIS),
     "fog_area_pt_nee": (FOG_AREA, FOG_AREA_NEE),
+    "veach_mis": (VEACH, VEACH_MIS),
+    "orb_pt_nee": (ORB, ORB_NEE),
+    "two_light_power": (TWO_LIGHT, TWO_LIGHT_POWER),
+    "haze_pt_nee": (HAZE, HAZE_NEE),
 }
