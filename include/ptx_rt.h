@@ -112,8 +112,8 @@ typedef struct ptr_env {
     float rotation;           /* azimuth rotation, radians (u_envRotation)              */
     float pad;
     const float* radiance;    /* width*height*4 RGBA32F, row 0 = v=0 (+Y pole)          */
-    const float* marginal;    /* height+1 cumulative (CDF over rows)                    */
-    const float* conditional; /* height*(width+1) cumulative (CDF within each row)      */
+    const float* marginal;    /* height floats: cumulative CDF over rows                 */
+    const float* conditional; /* height*width floats: cumulative CDF within each row     */
 } ptr_env;
 
 /* ---- triangle meshes, BVH / CWBVH (src/components/accel, intersection/mesh) --------- */
@@ -227,6 +227,24 @@ int ptr_render(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame);
  * to host_out, laid out [sample][row][column][rgb] (n >= width*height*spp*3 floats).
  * The per-sample values are what the reference's accumulation folds in (accumulation.ts:14-51). */
 int ptr_render_samples(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, float* host_out, size_t n);
+
+/* Nearest-hit queries on an uploaded scene: rays are n x (origin.xyz, direction.xyz);
+ * per ray returns the region (-1 = miss), the instance element, the ORIGINAL triangle
+ * index of a mesh hit (-1 otherwise) and t (1000 = MAX_DIST on a miss).  accel selects
+ * the mesh BLAS walk (PTR_ACCEL_BVH / PTR_ACCEL_CWBVH).  The scene_intersect traversal
+ * of the reference (features/intersection.ts:1665-1713) without the region probe. */
+int ptr_trace_closest(ptr_ctx* ctx, ptr_scene* scene, int accel, const float* rays, int n,
+                      int* region, int* element, int* prim, float* t);
+
+/* Host builders on their own (no GPU): the binary SAH BVH of the reference's
+ * buildBVHNodesFlat (src/components/accel/bvh/bvh.ts:344-383; 8 floats per node) and the
+ * compressed wide BVH of buildCWBVH (src/components/accel/cwbvh/cwbvh.ts:80-372; 20 u32
+ * per node) over n boxes of 6 doubles (min.xyz, max.xyz).  order_out[i] = item index of
+ * leaf slot i.  Pass nodes_out = NULL to query node_count first. */
+int ptr_build_bvh(const double* boxes, int n, int leaf_size, int always_split,
+                  float* nodes_out, int nodes_cap, uint32_t* order_out, int* node_count, int* max_depth);
+int ptr_build_cwbvh(const double* boxes, int n, double c_prim,
+                    uint32_t* nodes_out, int nodes_cap, uint32_t* order_out, int* node_count, int* max_depth);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that order their own work
  * (timing events, cache flushes) with the library's launches. */

@@ -40,6 +40,16 @@ def lib():
         _lib = ctypes.CDLL(LIB)
         _lib.oracle_render.restype = ctypes.c_int
         _lib.oracle_render.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_void_p, ctypes.c_int]
+        _lib.oracle_render_tile.restype = ctypes.c_int
+        _lib.oracle_render_tile.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        _lib.oracle_session_create.restype = ctypes.c_void_p
+        _lib.oracle_session_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib.oracle_session_free.argtypes = [ctypes.c_void_p]
+        _lib.oracle_session_render_tile.restype = ctypes.c_int
+        _lib.oracle_session_render_tile.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        _lib.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.oracle_mesh_brute.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     return _lib
 
 
@@ -71,3 +81,84 @@ def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=
     if samples is not None:
         out["samples"] = samples
     return out
+
+
+def render_tile(packed, renderer, width, height, tile, spp, first_sample=0, salt=0, params=None, threads=0):
+    """Render the tile (x0, y0, tw, th) of a width x height image; returns (mean, counts)."""
+    from pathtracerglsl_b200 import abi
+    x0, y0, tw, th = tile
+    desc = packed.desc()
+    fr = abi.Frame()
+    fr.width, fr.height = width, height
+    fr.first_sample, fr.spp = first_sample, spp
+    fr.reset_salt = salt
+    fr.camera = renderer.camera(params or {}, width, height)
+    s = np.zeros((th, tw, 3), np.float64)
+    q = np.zeros((th, tw, 3), np.float64)
+    counts = (ctypes.c_uint64 * 2)()
+    rc = lib().oracle_render_tile(ctypes.addressof(desc), ctypes.addressof(renderer.program), ctypes.addressof(fr),
+                                  x0, y0, tw, th, s.ctypes.data, q.ctypes.data, None, ctypes.addressof(counts), threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_render_tile failed: {rc}")
+    return s / spp, (counts[0], counts[1])
+
+
+class Session:
+    """A scene prepared once (the oracle's mesh acceleration built), rendered many times."""
+
+    def __init__(self, packed, renderer):
+        self.packed, self.renderer = packed, renderer
+        self._desc = packed.desc()
+        self._h = lib().oracle_session_create(ctypes.addressof(self._desc), ctypes.addressof(renderer.program))
+
+    def render_tile(self, width, height, tile, spp, first_sample=0, salt=0, params=None, threads=0):
+        from pathtracerglsl_b200 import abi
+        x0, y0, tw, th = tile
+        fr = abi.Frame()
+        fr.width, fr.height = width, height
+        fr.first_sample, fr.spp = first_sample, spp
+        fr.reset_salt = salt
+        fr.camera = self.renderer.camera(params or {}, width, height)
+        s = np.zeros((th, tw, 3), np.float64)
+        q = np.zeros((th, tw, 3), np.float64)
+        counts = (ctypes.c_uint64 * 2)()
+        rc = lib().oracle_session_render_tile(self._h, ctypes.addressof(fr), x0, y0, tw, th, s.ctypes.data, q.ctypes.data,
+                                              None, ctypes.addressof(counts), threads)
+        if rc != 0:
+            raise RuntimeError(f"oracle_session_render_tile failed: {rc}")
+        return s / spp, (counts[0], counts[1])
+
+    def close(self):
+        if self._h:
+            lib().oracle_session_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def trace_closest(packed, renderer, rays):
+    """Nearest hit per ray (rays: n x 6 float32 origin, direction) -> (region, prim, t)."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = len(rays)
+    region = np.zeros(n, np.int32)
+    prim = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    desc = packed.desc()
+    lib().oracle_trace_closest(ctypes.addressof(desc), ctypes.addressof(renderer.program), rays.ctypes.data, n,
+                               region.ctypes.data, prim.ctypes.data, t.ctypes.data)
+    return region, prim, t
+
+
+def mesh_brute(packed, mesh_index, rays):
+    """Brute-force nearest triangle of one packed mesh -> (prim, t)."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = len(rays)
+    prim = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    desc = packed.desc()
+    lib().oracle_mesh_brute(ctypes.addressof(desc.meshes[mesh_index]), rays.ctypes.data, n, prim.ctypes.data, t.ctypes.data)
+    return prim, t

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <limits>
 #include <omp.h>
 
 #include "../include/ptx_rt.h"
@@ -100,6 +101,8 @@ struct Hit {
     float t; v3 p; Frame frame; v3 ng;
     int region_from, region_to, region_owner, element;
     float eps;
+    float alpha = -1.0f;   // per-triangle GGX alpha of a mesh hit, < 0 = the material's
+    int prim = -1;         // original triangle index of a mesh hit
 };
 struct LightSample { v3 wi; float distance; v3 radiance; float pdf; uint32_t flags; int light_id; };
 struct ISample { v3 wi; v3 weight; float pdf; uint32_t flags; };
@@ -200,6 +203,190 @@ inline v3 box_normal(v3 p, v3 c, v3 h) {
     return v3(0, 0, signf(q.z));
 }
 
+// ---------------------------------------------------------------- meshes
+// Triangle leaf: Moller-Trumbore of the reference's mesh_tri_test
+// (src/components/intersection/mesh/mesh.glsl:41-59); e1, e2 from the float32 positions.
+inline bool tri_test(v3 ro, v3 rd, v3 a, v3 e1, v3 e2, float& t) {
+    v3 gnorm = cross(e1, e2);
+    float det = -dot(rd, gnorm);
+    if (std::fabs(det) < 1e-12f) return false;
+    float invdet = 1.0f / det;
+    v3 ao = ro - a;
+    v3 dao = cross(ao, rd);
+    float u = dot(e2, dao) * invdet;
+    float v = -dot(e1, dao) * invdet;
+    t = dot(ao, gnorm) * invdet;
+    float w = 1.0f - u - v;
+    const float E = 1e-6f;
+    return u >= -E && v >= -E && w >= -E;
+}
+
+// The oracle's own mesh acceleration: a median-split BVH over triangle boxes (4 triangles
+// per leaf).  Its shape is irrelevant to the result: the nearest hit over a triangle set is
+// the minimum of the same per-triangle t values whatever the tree.
+struct OMesh {
+    std::vector<v3> a, e1, e2;
+    std::vector<float> alpha;
+    struct Node { float mn[3], mx[3]; int left, right, start, count; };
+    std::vector<Node> nodes;
+    std::vector<int> idx;
+    float root_mn[3], root_mx[3];
+
+    void build(const ptr_mesh_desc& md) {
+        const int T = md.n_triangles;
+        a.resize(T); e1.resize(T); e2.resize(T); alpha.assign(T, -1.0f);
+        std::vector<float> bmn(3 * (size_t)T), bmx(3 * (size_t)T), cen(3 * (size_t)T);
+        for (int t = 0; t < T; ++t) {
+            const float* p0 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t];
+            const float* p1 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 1];
+            const float* p2 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 2];
+            a[t] = v3(p0[0], p0[1], p0[2]);
+            e1[t] = v3(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]);
+            e2[t] = v3(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]);
+            if (md.tri_alpha) alpha[t] = md.tri_alpha[t];
+            for (int k = 0; k < 3; ++k) {
+                bmn[3 * (size_t)t + k] = std::min(p0[k], std::min(p1[k], p2[k]));
+                bmx[3 * (size_t)t + k] = std::max(p0[k], std::max(p1[k], p2[k]));
+                cen[3 * (size_t)t + k] = 0.5f * (bmn[3 * (size_t)t + k] + bmx[3 * (size_t)t + k]);
+            }
+        }
+        idx.resize(T);
+        for (int i = 0; i < T; ++i) idx[i] = i;
+        nodes.clear();
+        nodes.reserve(2 * (size_t)T);
+        build_rec(0, T, bmn, bmx, cen);
+        for (int k = 0; k < 3; ++k) { root_mn[k] = nodes[0].mn[k]; root_mx[k] = nodes[0].mx[k]; }
+    }
+    int build_rec(int s0, int s1, const std::vector<float>& bmn, const std::vector<float>& bmx, const std::vector<float>& cen) {
+        Node nd;
+        for (int k = 0; k < 3; ++k) { nd.mn[k] = 1e30f; nd.mx[k] = -1e30f; }
+        for (int i = s0; i < s1; ++i)
+            for (int k = 0; k < 3; ++k) {
+                nd.mn[k] = std::min(nd.mn[k], bmn[3 * (size_t)idx[i] + k]);
+                nd.mx[k] = std::max(nd.mx[k], bmx[3 * (size_t)idx[i] + k]);
+            }
+        int me = (int)nodes.size();
+        nodes.push_back(nd);
+        if (s1 - s0 <= 4) {
+            nodes[me].left = nodes[me].right = -1;
+            nodes[me].start = s0;
+            nodes[me].count = s1 - s0;
+            return me;
+        }
+        int axis = 0;
+        float ext = -1.0f;
+        for (int k = 0; k < 3; ++k) if (nd.mx[k] - nd.mn[k] > ext) { ext = nd.mx[k] - nd.mn[k]; axis = k; }
+        int mid = (s0 + s1) / 2;
+        std::nth_element(idx.begin() + s0, idx.begin() + mid, idx.begin() + s1,
+                         [&](int x, int y) { return cen[3 * (size_t)x + axis] < cen[3 * (size_t)y + axis]; });
+        int l = build_rec(s0, mid, bmn, bmx, cen);
+        int r = build_rec(mid, s1, bmn, bmx, cen);
+        nodes[me].left = l;
+        nodes[me].right = r;
+        nodes[me].start = nodes[me].count = 0;
+        return me;
+    }
+    // entry distance of the ray into the node box, or +inf when it misses within tmax
+    // (conservative: only prunes and orders, never decides a hit)
+    static float box_entry(const Node& n, v3 ro, v3 inv, float tmax) {
+        float tn = 0.0f, tf = tmax;
+        for (int k = 0; k < 3; ++k) {
+            float t0 = (n.mn[k] - ro[k]) * inv[k], t1 = (n.mx[k] - ro[k]) * inv[k];
+            if (t0 != t0 || t1 != t1) continue;   // ray on the slab plane with a zero direction: no constraint
+            tn = std::max(tn, std::min(t0, t1));
+            tf = std::min(tf, std::max(t0, t1));
+        }
+        return tn <= tf * 1.0001f + 1e-6f ? tn : std::numeric_limits<float>::infinity();
+    }
+    static bool box_hit(const Node& n, v3 ro, v3 inv, float tmax) {
+        return box_entry(n, ro, inv, tmax) != std::numeric_limits<float>::infinity();
+    }
+    // nearest triangle with t in (0, tmax); returns the triangle index or -1
+    int nearest(v3 ro, v3 rd, float& tmax) const {
+        v3 inv(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+        int best = -1;
+        int stack[128];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const Node& n = nodes[stack[--sp]];
+            if (!box_hit(n, ro, inv, tmax)) continue;
+            if (n.left < 0) {
+                for (int i = n.start; i < n.start + n.count; ++i) {
+                    int t_i = idx[i];
+                    float t;
+                    if (tri_test(ro, rd, a[t_i], e1[t_i], e2[t_i], t) && t > 0.0f && (t < tmax || (t == tmax && best >= 0 && t_i < best))) {
+                        tmax = t;
+                        best = t_i;
+                    }
+                }
+            } else {
+                // front to back: push the farther child first
+                float tl = box_entry(nodes[n.left], ro, inv, tmax), tr = box_entry(nodes[n.right], ro, inv, tmax);
+                bool hl = tl != std::numeric_limits<float>::infinity(), hr = tr != std::numeric_limits<float>::infinity();
+                if (hl && hr) {
+                    if (tl <= tr) { stack[sp++] = n.right; stack[sp++] = n.left; }
+                    else { stack[sp++] = n.left; stack[sp++] = n.right; }
+                } else if (hl) stack[sp++] = n.left;
+                else if (hr) stack[sp++] = n.right;
+            }
+        }
+        return best;
+    }
+    bool any(v3 ro, v3 rd, float max_dist) const {
+        float tm = max_dist;
+        v3 inv(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+        int stack[128];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const Node& n = nodes[stack[--sp]];
+            if (!box_hit(n, ro, inv, tm)) continue;
+            if (n.left < 0) {
+                for (int i = n.start; i < n.start + n.count; ++i) {
+                    int t_i = idx[i];
+                    float t;
+                    if (tri_test(ro, rd, a[t_i], e1[t_i], e2[t_i], t) && t > 0.0f && t < max_dist) return true;
+                }
+            } else {
+                stack[sp++] = n.left;
+                stack[sp++] = n.right;
+            }
+        }
+        return false;
+    }
+};
+
+// Placement algebra (intersection/instancing/placement.glsl:19-41).
+inline v3 qrot(const float* q, v3 v) {
+    v3 qv(q[0], q[1], q[2]);
+    return v + 2.0f * cross(qv, cross(qv, v) + q[3] * v);
+}
+inline v3 placement_normal(const float* q, v3 n) {
+    float c[4] = {-q[0], -q[1], -q[2], q[3]};
+    return qrot(c, n);
+}
+
+struct OBatch {
+    int shape, mesh;
+    std::vector<float> place;    // 8 per instance (q, ts)
+    std::vector<float> sphere;   // 4 per instance: world centre, world radius (sphere batches)
+    std::vector<float> wbox;     // 6 per instance: world box of a mesh instance (culling only)
+};
+
+// Ray vs world box (culling only: conservative, never decides a hit).
+inline bool ray_box_cull(const float* b, v3 ro, v3 rd, float tmax) {
+    float tn = 0.0f, tf = tmax;
+    for (int k = 0; k < 3; ++k) {
+        float inv = 1.0f / rd[k];
+        float t0 = (b[k] - ro[k]) * inv, t1 = (b[3 + k] - ro[k]) * inv;
+        if (t0 != t0 || t1 != t1) continue;
+        tn = std::max(tn, std::min(t0, t1));
+        tf = std::min(tf, std::max(t0, t1));
+    }
+    return tn <= tf * 1.0001f + 1e-5f;
+}
+
 // ---------------------------------------------------------------- scene
 struct Scene {
     const ptr_scene_desc* d;
@@ -208,7 +395,58 @@ struct Scene {
     bool env_samplable, env_select_live;
     bool has_media;
 
+    std::vector<OMesh> meshes;
+    std::vector<OBatch> batches;
+
     explicit Scene(const ptr_scene_desc* sd, const ptr_program_desc* pd) : d(sd), prog(pd) {
+        meshes.resize(sd->n_meshes > 0 ? sd->n_meshes : 0);
+        for (int i = 0; i < sd->n_meshes; ++i) meshes[i].build(sd->meshes[i]);
+        batches.resize(sd->n_batches > 0 ? sd->n_batches : 0);
+        for (int i = 0; i < sd->n_batches; ++i) {
+            const ptr_batch_desc& bd = sd->batches[i];
+            OBatch& b = batches[i];
+            b.shape = bd.prototype_shape;
+            b.mesh = bd.prototype_ref;
+            b.place.assign(bd.placements, bd.placements + 8 * (size_t)bd.n_instances);
+            if (b.shape == PTR_SHAPE_MESH) {
+                const OMesh& m = meshes[b.mesh];
+                for (int k = 0; k < bd.n_instances; ++k) {
+                    const float* pl = bd.placements + 8 * (size_t)k;
+                    float bx[6] = {1e30f, 1e30f, 1e30f, -1e30f, -1e30f, -1e30f};
+                    for (int c = 0; c < 8; ++c) {
+                        double lx = (c & 1) ? m.root_mx[0] : m.root_mn[0];
+                        double ly = (c & 2) ? m.root_mx[1] : m.root_mn[1];
+                        double lz = (c & 4) ? m.root_mx[2] : m.root_mn[2];
+                        double sc = pl[7];
+                        double vx = sc * lx - pl[4], vy = sc * ly - pl[5], vz = sc * lz - pl[6];
+                        double cx = -pl[0], cy = -pl[1], cz = -pl[2], w = pl[3];
+                        double c1x = cy * vz - cz * vy + w * vx, c1y = cz * vx - cx * vz + w * vy, c1z = cx * vy - cy * vx + w * vz;
+                        double c2x = cy * c1z - cz * c1y, c2y = cz * c1x - cx * c1z, c2z = cx * c1y - cy * c1x;
+                        double wp[3] = {vx + 2.0 * c2x, vy + 2.0 * c2y, vz + 2.0 * c2z};
+                        for (int a = 0; a < 3; ++a) {
+                            bx[a] = std::min(bx[a], (float)wp[a] - 1e-4f * (1.0f + std::fabs((float)wp[a])));
+                            bx[3 + a] = std::max(bx[3 + a], (float)wp[a] + 1e-4f * (1.0f + std::fabs((float)wp[a])));
+                        }
+                    }
+                    b.wbox.insert(b.wbox.end(), bx, bx + 6);
+                }
+            }
+            if (b.shape == PTR_SHAPE_SPHERE) {
+                for (int k = 0; k < bd.n_instances; ++k) {
+                    const float* pl = bd.placements + 8 * (size_t)k;
+                    // world centre = rotate(conj(q), s*c - t_rigid) in double, then float
+                    double sc = pl[7];
+                    double vx = sc * bd.proto[0] - pl[4], vy = sc * bd.proto[1] - pl[5], vz = sc * bd.proto[2] - pl[6];
+                    double cx = -pl[0], cy = -pl[1], cz = -pl[2], w = pl[3];
+                    double c1x = cy * vz - cz * vy + w * vx, c1y = cz * vx - cx * vz + w * vy, c1z = cx * vy - cy * vx + w * vz;
+                    double c2x = cy * c1z - cz * c1y, c2y = cz * c1x - cx * c1z, c2z = cx * c1y - cy * c1x;
+                    b.sphere.push_back((float)(vx + 2.0 * c2x));
+                    b.sphere.push_back((float)(vy + 2.0 * c2y));
+                    b.sphere.push_back((float)(vz + 2.0 * c2z));
+                    b.sphere.push_back((float)(sc * bd.proto[3]));
+                }
+            }
+        }
         light_of_region.assign(sd->n_regions, -1);
         for (int i = 0; i < sd->n_lights; ++i)
             if (sd->lights[i].region >= 0) light_of_region[sd->lights[i].region] = i;
@@ -233,11 +471,76 @@ struct Scene {
         return p && (p->model == PTR_MAT_LAMBERT || p->model == PTR_MAT_GGX);
     }
 
-    // primitive_intersect (features/intersection.ts:801-824, primitiveHitFill :695-715)
+    // primitive_intersect (features/intersection.ts:801-824, primitiveHitFill :695-715),
+    // mesh arms (generateMeshDispatch :890-915) and instance leaves (instanceLeafItem :981-1066)
     bool primitive_intersect(const Ray& r, Hit& hit) const {
         bool found = false;
         for (int i = 0; i < d->n_regions; ++i) {
             const ptr_region& g = d->regions[i];
+            if (g.shape == PTR_SHAPE_MESH) {
+                const OMesh& m = meshes[g.ref];
+                float t = hit.t;
+                int tri = m.nearest(r.o, r.d, t);
+                if (tri >= 0) {
+                    hit.t = t;
+                    found = true;
+                    hit.p = r.o + r.d * t;
+                    hit.eps = fp_uncertainty(hit.p);
+                    v3 gl = cross(m.e1[tri], m.e2[tri]);
+                    hit.frame = ambient_frame(normalize(gl));
+                    hit.ng = normalize(gl);
+                    hit.region_owner = i;
+                    hit.element = 0;
+                    hit.alpha = m.alpha[tri];
+                    hit.prim = tri;
+                }
+                continue;
+            }
+            if (g.shape == PTR_SHAPE_INSTANCES) {
+                const OBatch& b = batches[g.ref];
+                const int N = (int)b.place.size() / 8;
+                for (int k = 0; k < N; ++k) {
+                    if (b.shape == PTR_SHAPE_SPHERE) {
+                        const float* sp = &b.sphere[4 * (size_t)k];
+                        float t;
+                        if (sphere_intersect(r, v3(sp[0], sp[1], sp[2]), sp[3], t) && t < hit.t) {
+                            hit.t = t;
+                            found = true;
+                            hit.p = r.o + r.d * t;
+                            hit.eps = fp_uncertainty(hit.p);
+                            hit.frame = ambient_frame(normalize(hit.p - v3(sp[0], sp[1], sp[2])));
+                            hit.ng = hit.frame.n;
+                            hit.region_owner = i;
+                            hit.element = k;
+                            hit.alpha = -1.0f;
+                            hit.prim = -1;
+                        }
+                        continue;
+                    }
+                    if (!ray_box_cull(&b.wbox[6 * (size_t)k], r.o, r.d, hit.t)) continue;
+                    const float* q = &b.place[8 * (size_t)k];
+                    const float s = q[7];
+                    v3 ro = (qrot(q, r.o) + v3(q[4], q[5], q[6])) / s;
+                    v3 rd = qrot(q, r.d) / s;
+                    const OMesh& m = meshes[b.mesh];
+                    float t = hit.t;
+                    int tri = m.nearest(ro, rd, t);
+                    if (tri >= 0) {
+                        hit.t = t;
+                        found = true;
+                        hit.p = r.o + r.d * t;
+                        hit.eps = fp_uncertainty(hit.p);
+                        v3 gl = cross(m.e1[tri], m.e2[tri]);
+                        hit.frame = ambient_frame(normalize(placement_normal(q, gl)));
+                        hit.ng = normalize(placement_normal(q, gl));
+                        hit.region_owner = i;
+                        hit.element = k;
+                        hit.alpha = m.alpha[tri];
+                        hit.prim = tri;
+                    }
+                }
+                continue;
+            }
             float t;
             v3 n;
             bool ok = false;
@@ -263,12 +566,36 @@ struct Scene {
             hit.ng = hit.frame.n;
             hit.region_owner = i;
             hit.element = 0;
+            hit.alpha = -1.0f;
+            hit.prim = -1;
         }
         return found;
     }
     bool scene_intersect_any(const Ray& r, float maxDist) const {
         for (int i = 0; i < d->n_regions; ++i) {
             const ptr_region& g = d->regions[i];
+            if (g.shape == PTR_SHAPE_MESH) {
+                if (meshes[g.ref].any(r.o, r.d, maxDist)) return true;
+                continue;
+            }
+            if (g.shape == PTR_SHAPE_INSTANCES) {
+                const OBatch& b = batches[g.ref];
+                const int N = (int)b.place.size() / 8;
+                for (int k = 0; k < N; ++k) {
+                    if (b.shape == PTR_SHAPE_SPHERE) {
+                        const float* sp = &b.sphere[4 * (size_t)k];
+                        float t;
+                        if (sphere_intersect(r, v3(sp[0], sp[1], sp[2]), sp[3], t) && t < maxDist) return true;
+                        continue;
+                    }
+                    if (!ray_box_cull(&b.wbox[6 * (size_t)k], r.o, r.d, maxDist)) continue;
+                    const float* q = &b.place[8 * (size_t)k];
+                    v3 ro = (qrot(q, r.o) + v3(q[4], q[5], q[6])) / q[7];
+                    v3 rd = qrot(q, r.d) / q[7];
+                    if (meshes[b.mesh].any(ro, rd, maxDist)) return true;
+                }
+                continue;
+            }
             float t;
             bool ok = false;
             switch (g.shape) {
@@ -289,6 +616,16 @@ struct Scene {
         for (int i = 0; i < d->n_regions; ++i) {
             const ptr_region& g = d->regions[i];
             float dd;
+            if (g.shape == PTR_SHAPE_INSTANCES) {
+                // instanced sphere batch: every containing instance competes (innermost wins)
+                const OBatch& b = batches[g.ref];
+                if (b.shape != PTR_SHAPE_SPHERE) continue;
+                for (size_t k = 0; k + 3 < b.sphere.size(); k += 4) {
+                    float ds = sphere_sdf(p, v3(b.sphere[k], b.sphere[k + 1], b.sphere[k + 2]), b.sphere[k + 3]);
+                    if (ds < 0.0f && ds > best) { best = ds; region = i; }
+                }
+                continue;
+            }
             switch (g.shape) {
                 case PTR_SHAPE_PLANE: dd = plane_sdf(p, ld3(g.p), g.p[3]); break;
                 case PTR_SHAPE_SPHERE: dd = sphere_sdf(p, ld3(g.p), g.p[3]); break;
@@ -459,13 +796,98 @@ struct Tracer {
 
     bool intersect(const Ray& r, Hit& h) { cnt.closest++; return S.scene_intersect(r, h); }
 
-    // ---- environment (features/environment.ts:109-252; constant env T3 sampler)
-    v3 environment_radiance(v3) const {
+    // ---- environment (features/environment.ts:109-252): constant env (T3 uniform sphere)
+    // or an equirect table read through equirect_uv (env/equirect/equirect_map.glsl:15-21,
+    // bilinear, wrap u, clamp v) and sampled by env/sampler_cdf.glsl:13-84.
+    void equirect_uv(v3 dir, float& u, float& v) const {
+        v3 n = normalize(dir);
+        float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : std::atan2(n.z, n.x)) + d.env.rotation;
+        float theta = std::atan2(std::sqrt(n.x * n.x + n.z * n.z), n.y);
+        u = phi * (1.0f / TWO_PI) + 0.5f;
+        u = u - std::floor(u);
+        v = theta * (1.0f / PI);
+    }
+    v3 env_texel(int i, int j) const {
+        const float* p = d.env.radiance + 4 * ((size_t)j * d.env.width + i);
+        return v3(p[0], p[1], p[2]);
+    }
+    v3 environment_radiance(v3 dir) const {
         if (d.env.kind == PTR_ENV_CONSTANT) return ld3(d.env.color) * d.env.intensity;
-        return v3(0.0f);
+        if (d.env.kind != PTR_ENV_IMAGE) return v3(0.0f);
+        const int W = d.env.width, H = d.env.height;
+        float u, v;
+        equirect_uv(dir, u, v);
+        float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
+        float fx0 = std::floor(x), fy0 = std::floor(y);
+        float ax = x - fx0, ay = y - fy0;
+        int i0 = (int)fx0, j0 = (int)fy0, i1 = i0 + 1, j1 = j0 + 1;
+        i0 = ((i0 % W) + W) % W;
+        i1 = ((i1 % W) + W) % W;
+        j0 = std::min(std::max(j0, 0), H - 1);
+        j1 = std::min(std::max(j1, 0), H - 1);
+        v3 top = env_texel(i0, j0) * (1.0f - ax) + env_texel(i1, j0) * ax;
+        v3 bot = env_texel(i0, j1) * (1.0f - ax) + env_texel(i1, j1) * ax;
+        return (top * (1.0f - ay) + bot * ay) * d.env.intensity;
+    }
+    float marg(int j) const { return d.env.marginal[j]; }
+    float cond(int j, int i) const { return d.env.conditional[(size_t)j * d.env.width + i]; }
+    float uniform_fraction() const { return marg(d.env.height - 1) > 0.0f ? 0.0625f : 1.0f; }
+    float table_pdf(v3 dir) const {
+        const int W = d.env.width, H = d.env.height;
+        float u, v;
+        equirect_uv(dir, u, v);
+        int i = std::min(std::max((int)(u * (float)W), 0), W - 1);
+        int j = std::min(std::max((int)(v * (float)H), 0), H - 1);
+        float dm = marg(j) - (j > 0 ? marg(j - 1) : 0.0f);
+        float dc = cond(j, i) - (i > 0 ? cond(j, i - 1) : 0.0f);
+        float theta = PI * ((float)j + 0.5f) / (float)H;
+        float domega = (TWO_PI / (float)W) * 2.0f * std::sin(theta) * std::sin(0.5f * PI / (float)H);
+        return (dc * dm) / domega;
+    }
+    v3 sample_table(float x0, float x1) const {
+        const int W = d.env.width, H = d.env.height;
+        int lo = 0, hi = H - 1;
+        while (lo < hi) { int mid = (lo + hi) >> 1; if (x0 >= marg(mid)) lo = mid + 1; else hi = mid; }
+        int j = lo;
+        float mlo = j > 0 ? marg(j - 1) : 0.0f;
+        float dm = marg(j) - mlo;
+        float vf = dm > 0.0f ? clampf((x0 - mlo) / dm, 0.0f, 0.9999999f) : 0.5f;
+        lo = 0; hi = W - 1;
+        while (lo < hi) { int mid = (lo + hi) >> 1; if (x1 >= cond(j, mid)) lo = mid + 1; else hi = mid; }
+        int i = lo;
+        float clo = i > 0 ? cond(j, i - 1) : 0.0f;
+        float dc = cond(j, i) - clo;
+        float uf = dc > 0.0f ? clampf((x1 - clo) / dc, 0.0f, 0.9999999f) : 0.5f;
+        float phi = (((float)i + uf) / (float)W - 0.5f) * TWO_PI - d.env.rotation;
+        bool north = 2 * j < H;
+        float row = north ? (float)j : (float)(H - j - 1);
+        float a = std::sin(0.5f * PI * row / (float)H);
+        float b = std::sin(0.5f * PI * (row + 1.0f) / (float)H);
+        float tt = north ? vf : 1.0f - vf;
+        float h = (a * a) * (1.0f - tt) + (b * b) * tt;
+        float y = (north ? 1.0f : -1.0f) * (1.0f - 2.0f * h);
+        float rr = 2.0f * std::sqrt(h * (1.0f - h));
+        return v3(rr * std::cos(phi), y, rr * std::sin(phi));
     }
     LightSample environment_sample(float x0, float x1) const {
         LightSample ls;
+        if (d.env.kind == PTR_ENV_IMAGE) {
+            float a = uniform_fraction();
+            if (x0 < a) {
+                float y = 1.0f - 2.0f * (x0 / a);
+                float r = std::sqrt(fmaxf_(0.0f, 1.0f - y * y));
+                float phi = TWO_PI * x1;
+                ls.wi = v3(r * std::cos(phi), y, r * std::sin(phi));
+            } else {
+                ls.wi = sample_table((x0 - a) / (1.0f - a), x1);
+            }
+            ls.distance = MAX_DIST;
+            ls.radiance = environment_radiance(ls.wi);
+            ls.pdf = environment_pdf(ls.wi);
+            ls.flags = 0u;
+            ls.light_id = -1;
+            return ls;
+        }
         float z = 1.0f - 2.0f * x0;
         float r = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
         float phi = TWO_PI * x1;
@@ -477,7 +899,11 @@ struct Tracer {
         ls.light_id = -1;
         return ls;
     }
-    float environment_pdf(v3) const { return 1.0f / (4.0f * PI); }
+    float environment_pdf(v3 dir) const {
+        if (d.env.kind != PTR_ENV_IMAGE) return 1.0f / (4.0f * PI);
+        float a = uniform_fraction();
+        return (1.0f - a) * table_pdf(dir) + a / (4.0f * PI);
+    }
 
     // ---- lights (lights/quad/quad.glsl:14-41, sphere/sphere.glsl:21-71, point/point.glsl:11-23)
     LightSample light_sample_one(const ptr_light& l, v3 p, float x0, float x1) const {
@@ -596,7 +1022,8 @@ struct Tracer {
     }
 
     // ---- material dispatch (features/materials.ts:902-954)
-    float alpha_of(const ptr_material& m) const { return m.alpha; }
+    float hit_alpha = -1.0f;   // the current vertex's per-triangle alpha (mesh hits)
+    float alpha_of(const ptr_material& m) const { return hit_alpha >= 0.0f ? hit_alpha : m.alpha; }
     ISample surface_sample(const ptr_material& m, v3 wo, const Hit& h, float uc, float u0, float u1) const {
         if (m.model == PTR_MAT_LAMBERT) return lambert_sample(wo, h, m, uc, u0, u1);
         if (m.model == PTR_MAT_GGX) return ggx_sample(wo, h, m, alpha_of(m), u0, u1);
@@ -799,6 +1226,7 @@ struct Tracer {
                 continue;
             }
             v3 wo = -r.d;
+            hit_alpha = hit.alpha;
             // kernel_score_emitter_hit (kernel.glsl:16-25)
             int mat_emit = S.material_of(hit.region_to);
             if (S.material_is_emissive(mat_emit))
@@ -860,10 +1288,59 @@ extern "C" {
 // Render frame->spp samples for every pixel; accumulate per-pixel sum / sum of squares
 // (float64, 3 per pixel, row 0 = bottom).  Returns counters through out_counts[2]
 // (closest-hit queries, shadow queries) when non-null.
+int oracle_render_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, const ptr_frame* fr,
+                       int x0, int y0, int tw, int th,
+                       double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads);
+
 int oracle_render(const ptr_scene_desc* sd, const ptr_program_desc* pd, const ptr_frame* fr,
                   double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
+    if (!fr) return -1;
+    return oracle_render_tile(sd, pd, fr, 0, 0, fr->width, fr->height, sum, sumsq, samples_out, out_counts, threads);
+}
+
+// Render the tile [x0, x0+tw) x [y0, y0+th) of the frame's image (the camera sees the
+// whole frame->width x frame->height image); outputs are indexed within the tile.
+static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
+                             double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads);
+
+int oracle_render_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, const ptr_frame* fr,
+                       int x0, int y0, int tw, int th,
+                       double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
     if (!sd || !pd || !fr) return -1;
     Scene S(sd, pd);
+    return render_tile_scene(S, fr, x0, y0, tw, th, sum, sumsq, samples_out, out_counts, threads);
+}
+
+// A prepared scene (its mesh acceleration built once): the descriptor and program are
+// copied; the arrays they point to must stay alive while the session is used.
+struct OracleSession {
+    ptr_scene_desc desc;
+    ptr_program_desc prog;
+    Scene* scene;
+};
+
+void* oracle_session_create(const ptr_scene_desc* sd, const ptr_program_desc* pd) {
+    OracleSession* s = new OracleSession();
+    s->desc = *sd;
+    s->prog = *pd;
+    s->scene = new Scene(&s->desc, &s->prog);
+    return s;
+}
+
+void oracle_session_free(void* h) {
+    OracleSession* s = (OracleSession*)h;
+    delete s->scene;
+    delete s;
+}
+
+int oracle_session_render_tile(void* h, const ptr_frame* fr, int x0, int y0, int tw, int th,
+                               double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
+    OracleSession* s = (OracleSession*)h;
+    return render_tile_scene(*s->scene, fr, x0, y0, tw, th, sum, sumsq, samples_out, out_counts, threads);
+}
+
+static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
+                             double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
     const int W = fr->width, H = fr->height;
     uint64_t closest = 0, shadow = 0;
     if (threads > 0) omp_set_num_threads(threads);
@@ -871,9 +1348,11 @@ int oracle_render(const ptr_scene_desc* sd, const ptr_program_desc* pd, const pt
     {
         Tracer T(S);
 #pragma omp for schedule(dynamic, 1)
-        for (int y = 0; y < H; ++y) {
-            for (int x = 0; x < W; ++x) {
-                size_t pix = (size_t)y * W + x;
+        for (int ty = 0; ty < th; ++ty) {
+            const int y = y0 + ty;
+            for (int tx = 0; tx < tw; ++tx) {
+                const int x = x0 + tx;
+                size_t pix = (size_t)ty * tw + tx;
                 for (int k = 0; k < fr->spp; ++k) {
                     uint32_t px = (uint32_t)(x + fr->pixel_offset[0]);
                     uint32_t py = (uint32_t)(y + fr->pixel_offset[1]);
@@ -887,7 +1366,7 @@ int oracle_render(const ptr_scene_desc* sd, const ptr_program_desc* pd, const pt
                     Ray r = camera_ray(fr->camera, W, H, fx, fy);
                     v3 L = T.transport_trace(r);
                     if (samples_out) {
-                        float* o = samples_out + 3 * ((size_t)k * W * H + pix);
+                        float* o = samples_out + 3 * ((size_t)k * tw * th + pix);
                         o[0] = L.x; o[1] = L.y; o[2] = L.z;
                     }
                     if (sum) {
@@ -903,6 +1382,45 @@ int oracle_render(const ptr_scene_desc* sd, const ptr_program_desc* pd, const pt
         shadow += T.cnt.shadow;
     }
     if (out_counts) { out_counts[0] = closest; out_counts[1] = shadow; }
+    return 0;
+}
+
+
+// Nearest-hit queries with the oracle's own acceleration: per ray (o.xyz, d.xyz) the
+// region (-1 = miss), the original triangle index (-1 if not a mesh hit) and t.
+int oracle_trace_closest(const ptr_scene_desc* sd, const ptr_program_desc* pd, const float* rays, int n,
+                         int* region, int* prim, float* t_out) {
+    Scene S(sd, pd);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int k = 0; k < n; ++k) {
+        Ray r{v3(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]), v3(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5])};
+        Hit h;
+        h.t = MAX_DIST;
+        h.eps = MARCH_CLEARANCE;
+        bool f = S.primitive_intersect(r, h);
+        region[k] = f ? h.region_owner : -1;
+        prim[k] = f ? h.prim : -1;
+        t_out[k] = h.t;
+    }
+    return 0;
+}
+
+// Brute-force nearest triangle of one mesh (every triangle, the same leaf test).
+int oracle_mesh_brute(const ptr_mesh_desc* md, const float* rays, int n, int* prim, float* t_out) {
+    OMesh m;
+    m.build(*md);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int k = 0; k < n; ++k) {
+        v3 ro(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]), rd(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
+        float tmax = MAX_DIST;
+        int best = -1;
+        for (int i = 0; i < md->n_triangles; ++i) {
+            float t;
+            if (tri_test(ro, rd, m.a[i], m.e1[i], m.e2[i], t) && t > 0.0f && t < tmax) { tmax = t; best = i; }
+        }
+        prim[k] = best;
+        t_out[k] = tmax;
+    }
     return 0;
 }
 

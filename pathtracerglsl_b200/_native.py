@@ -23,6 +23,12 @@ SIGNATURES = {
     "ptr_render": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame)]),
     "ptr_render_samples": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame), C.POINTER(C.c_float), C.c_size_t]),
     "ptr_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ptr_trace_closest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ptr_build_bvh": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ptr_build_cwbvh": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "ptr_render_noalloc": (C.c_int, [C.POINTER(abi.SceneDesc), C.POINTER(abi.ProgramDesc), C.POINTER(abi.Frame),
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "ptr_sync": (C.c_int, [C.c_void_p, C.c_int]),

@@ -589,8 +589,28 @@ class Compiler:
                    "sample_as_light": sal, "rotation": 0.0}
             out["select_prob"] = self._env_select_prob(sum(col) / 3.0, intensity, scene, lights)
             return out
-        bag.error("unsupported", f"environment {t!r} needs the image table path (pack_environment)")
-        return {"kind": abi.ENV_NONE}
+        # tabulated environments: an equirect RGB table (image, or a procedural recipe already
+        # baked into one) + the importance CDFs; joins NEE/MIS by default (sampleAsLight true)
+        table = env.get("table")
+        if table is None:
+            bag.error("invalid-environment", f"environment {t!r} needs a 'table' (H x W x 3 float32 equirect radiance)")
+            return {"kind": abi.ENV_NONE}
+        table = np.ascontiguousarray(np.asarray(table, np.float32))
+        if table.ndim != 3 or table.shape[2] != 3 or not np.isfinite(table).all() or (table < 0).any():
+            bag.error("invalid-environment", "environment table must be H x W x 3, finite and nonnegative")
+            return {"kind": abi.ENV_NONE}
+        H, W = table.shape[:2]
+        cond, marg, total = build_env_importance(table)
+        rgba = np.zeros((H, W, 4), np.float32)
+        rgba[:, :, :3] = table
+        sal = bool(env.get("sampleAsLight", True))
+        out = {"kind": abi.ENV_IMAGE, "width": W, "height": H, "radiance": rgba.reshape(-1),
+               "marginal": marg, "conditional": cond.reshape(-1), "intensity": intensity,
+               "sample_as_light": sal, "rotation": float(resolve(env.get("rotation"), params, 0.0)),
+               "total_weight": total}
+        mean_l = (total * math.pi) / (2 * W * H)      # equirect: integral L dOmega / 4 pi
+        out["select_prob"] = self._env_select_prob(mean_l, intensity, scene, lights)
+        return out
 
     @staticmethod
     def _env_select_prob(mean_l, intensity, scene, lights):
@@ -638,6 +658,36 @@ class Compiler:
         rid = f"{st.get('id', 'strategy')}-{scene.get('id', 'scene')}"
         exports = {"radiance": {"format": "float"}, "variance": {"format": "float"}}
         return CompiledRenderer(rid, prog, st, parameters, exports)
+
+
+def build_env_importance(table):
+    """The environment importance table of the reference (src/components/env/importance.ts:16):
+    Rec. 709 luminance per texel (float32 store), a 3x3 tent blur that wraps in u and clamps
+    in v (float32 store), then per row the sin(theta)-weighted conditional CDF and over rows
+    the marginal CDF, accumulated in float64 in index order and stored as float32.
+    Returns (conditional H x W, marginal H, total weight)."""
+    H, W = table.shape[:2]
+    t = table.astype(np.float64)
+    Y = (0.2126 * t[:, :, 0] + 0.7152 * t[:, :, 1] + 0.0722 * t[:, :, 2]).astype(np.float32)
+    Yd = Y.astype(np.float64)
+    acc = np.zeros((H, W), np.float64)
+    for dj in (-1, 0, 1):
+        rows = np.clip(np.arange(H) + dj, 0, H - 1)
+        for di in (-1, 0, 1):
+            cols = (np.arange(W) + di + W) % W
+            w = (2 if dj == 0 else 1) * (2 if di == 0 else 1)
+            acc = acc + w * Yd[rows][:, cols]
+    Y = (acc / 16.0).astype(np.float32)
+    sin_t = np.sin(np.pi * (np.arange(H) + 0.5) / H)
+    wY = np.maximum(0.0, Y.astype(np.float64)) * sin_t[:, None]
+    csum = np.cumsum(wY, axis=1)                   # sequential, like the reference's loop
+    row_sum = csum[:, -1].copy()
+    with np.errstate(invalid="ignore", divide="ignore"):
+        cond = np.where(row_sum[:, None] > 0, csum / row_sum[:, None], 0.0).astype(np.float32)
+    total = float(np.cumsum(row_sum)[-1]) if H else 0.0
+    macc = np.cumsum(row_sum)
+    marg = (macc / total if total > 0 else np.zeros(H)).astype(np.float32)
+    return np.ascontiguousarray(cond), np.ascontiguousarray(marg), total
 
 
 def _light_power(kind, e, geom):

@@ -1,17 +1,346 @@
-// bvh.cuh — acceleration-structure arms of the scene queries (meshes, instanced batches).
+// bvh.cuh — acceleration-structure arms of the scene queries: triangle meshes (binary BVH
+// or compressed wide BVH BLAS) and instanced batches (binary TLAS over placements).
+//
+// Triangle leaf: Moller-Trumbore as the reference's mesh_tri_test
+//   (src/components/intersection/mesh/mesh.glsl:41-59), flat geometric normal.
+// Binary walk: the stack-DFS of mesh_nearest_bvh (mesh.glsl:162-191) with the padded slab
+//   test bvh_aabb_hit (accel/bvh/bvh.glsl:28-36), near child first by the split axis.
+// Wide walk: the octant-ordered CWBVH walk (intersection/index.ts:99-158): per-node ray
+//   transform, one-FMA quantized slabs, find-MSB child order, node groups on a small stack.
+//   Nodes are fetched as five 128-bit loads.
+// Placements (intersection/instancing/placement.glsl:19-41): world -> rigid frame by the
+//   stored quaternion q and ts = (t_rigid, s); mesh prototypes are intersected in their
+//   local frame with the t-preserving (un-normalised) direction.
 #pragma once
 #include "scene.cuh"
 
 namespace ptx {
 
-struct HitRec;
+constexpr float kBvhTfarPad = 1.00000024f;   // BVH_TFAR_PAD (Ize 2013 far-plane pad)
+constexpr int kBvhStack = 64;                // BVH_STACK_DEPTH
+constexpr int kCwStack = 24;                 // CWBVH_STACK_DEPTH
+constexpr unsigned kErrBvhStack = 1u;        // a binary walk dropped a subtree (stack full)
+constexpr unsigned kErrCwStack = 2u;         // a wide walk dropped a node group
+constexpr unsigned kErrCwGuard = 4u;         // a wide walk hit its iteration guard
 
-__device__ __forceinline__ void accel_closest(const DevScene&, const ptr_region&, int, const Ray&, HitRec&) {}
-__device__ __forceinline__ bool accel_any(const DevScene&, const ptr_region&, const Ray&, float) { return false; }
-__device__ __forceinline__ float accel_region_sdf(const DevScene&, const ptr_region&, f3) { return 1.0e20f; }
-__device__ __forceinline__ f3 accel_hit_normal(const DevScene&, const ptr_region&, const HitRec&, const Ray&, Hit& h) {
-    h.eps = kMarchClearance;
-    return f3(0.f, 1.f, 0.f);
+struct HitRec { float t, u, v; int region, element, prim; };
+
+__device__ __forceinline__ void flag_error(const DevScene& S, unsigned bit) {
+    if (S.err_flags) atomicOr(S.err_flags, bit);
+}
+
+// ---- placement algebra ------------------------------------------------------------------
+__device__ __forceinline__ f3 qrot(float4 q, f3 v) {
+    f3 qv(q.x, q.y, q.z);
+    return v + 2.0f * cross(qv, cross(qv, v) + q.w * v);
+}
+__device__ __forceinline__ f3 placement_rigid(float4 q, float4 ts, f3 p) { return qrot(q, p) + f3(ts.x, ts.y, ts.z); }
+__device__ __forceinline__ f3 placement_normal(float4 q, f3 n) { return qrot(make_float4(-q.x, -q.y, -q.z, q.w), n); }
+
+// ---- triangle leaf --------------------------------------------------------------------
+__device__ __forceinline__ bool tri_test(f3 ro, f3 rd, f3 a, f3 e1, f3 e2, float& t) {
+    f3 gnorm = cross(e1, e2);
+    float det = -dot(rd, gnorm);
+    if (fabsf(det) < 1e-12f) return false;
+    float invdet = 1.0f / det;
+    f3 ao = ro - a;
+    f3 dao = cross(ao, rd);
+    float u = dot(e2, dao) * invdet;
+    float v = -dot(e1, dao) * invdet;
+    t = dot(ao, gnorm) * invdet;
+    float w = 1.0f - u - v;
+    const float E = 1e-6f;
+    return u >= -E && v >= -E && w >= -E;
+}
+__device__ __forceinline__ void load_tri(const float4* tri, int i, f3& a, f3& e1, f3& e2) {
+    float4 t0 = __ldg(tri + 3 * i), t1 = __ldg(tri + 3 * i + 1), t2 = __ldg(tri + 3 * i + 2);
+    a = xyz(t0); e1 = xyz(t1); e2 = xyz(t2);
+}
+
+// ---- binary BVH walk --------------------------------------------------------------------
+__device__ __forceinline__ bool aabb_hit(float4 n0, float4 n1, f3 ro, f3 inv, float tmax) {
+    float tx0 = (n0.x - ro.x) * inv.x, tx1 = (n1.x - ro.x) * inv.x;
+    float ty0 = (n0.y - ro.y) * inv.y, ty1 = (n1.y - ro.y) * inv.y;
+    float tz0 = (n0.z - ro.z) * inv.z, tz1 = (n1.z - ro.z) * inv.z;
+    float tn = gmax(gmax(gmin(tx0, tx1), gmin(ty0, ty1)), gmin(tz0, tz1));
+    float tf = gmin(gmin(gmax(tx0, tx1), gmax(ty0, ty1)), gmax(tz0, tz1)) * kBvhTfarPad;
+    float tenter = gmax(tn, 0.0f);
+    return tf >= tenter && tenter < tmax;
+}
+
+// Leaf(off, cnt) -> for nearest walks updates the caller's tmax itself; returns true to
+// stop the walk (any-hit found).
+template <class Leaf>
+__device__ __forceinline__ bool walk_binary(const DevScene& S, const float4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf) {
+    f3 inv(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+    int stack[kBvhStack];
+    int ptr = 0;
+    stack[0] = 0;
+    while (ptr >= 0) {
+        int ni = stack[ptr];
+        ptr--;
+        float4 n0 = __ldg(nodes + 2 * ni), n1 = __ldg(nodes + 2 * ni + 1);
+        if (!aabb_hit(n0, n1, ro, inv, tmax)) continue;
+        if (n0.w >= 0.0f) {
+            if (leaf((int)n1.w, (int)n0.w)) return true;
+        } else {
+            int axis = (int)(-n0.w - 1.0f);
+            int L = ni + 1, R = (int)n1.w;
+            bool nf = (axis == 0 ? rd.x : (axis == 1 ? rd.y : rd.z)) >= 0.0f;
+            if (ptr + 2 < kBvhStack) {
+                stack[++ptr] = nf ? R : L;
+                stack[++ptr] = nf ? L : R;
+            } else {
+                flag_error(S, kErrBvhStack);
+            }
+        }
+    }
+    return false;
+}
+
+// ---- compressed wide BVH walk ---------------------------------------------------------------
+__device__ __forceinline__ int find_msb24(unsigned v) { return 31 - __clz(v); }
+__device__ __forceinline__ float clamp_dir(float d) { return fabsf(d) < 1e-20f ? (d < 0.0f ? -1e-20f : 1e-20f) : d; }
+
+// Leaf(item) for one leaf item index (wide-order); returns true to stop.
+template <class Leaf>
+__device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf) {
+    f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
+    unsigned octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
+    f3 inv(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
+    uint2 stack[kCwStack];
+    int ptr = -1;
+    unsigned g_base = 0u, g_hits = 1u << (octinv & 7u), g_imask = 1u;
+    for (int guard = 0; guard < 65536; guard++) {
+        if (g_hits == 0u) {
+            if (ptr < 0) return false;
+            g_base = stack[ptr].x;
+            g_hits = stack[ptr].y & 0xFFu;
+            g_imask = stack[ptr].y >> 8;
+            ptr--;
+            continue;
+        }
+        int bit = find_msb24(g_hits);
+        g_hits &= ~(1u << (unsigned)bit);
+        unsigned slot = ((unsigned)bit ^ octinv) & 7u;
+        unsigned child = g_base + __popc(g_imask & ((1u << slot) - 1u));
+        if (g_hits != 0u) {
+            if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
+            else flag_error(S, kErrCwStack);
+        }
+        const uint4* nd = nodes + 5 * (size_t)child;
+        uint4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
+        f3 p(__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z));
+        f3 dq = f3(__uint_as_float((n0.w & 0xFFu) << 23), __uint_as_float(((n0.w >> 8) & 0xFFu) << 23),
+                   __uint_as_float(((n0.w >> 16) & 0xFFu) << 23)) * inv;
+        unsigned imask = (n0.w >> 24) & 0xFFu;
+        f3 oq = (p - ro) * inv;
+        unsigned hits = 0u, leaf_bits = 0u;
+#pragma unroll
+        for (unsigned sl = 0u; sl < 8u; sl++) {
+            const unsigned sh = 8u * (sl & 3u);
+            unsigned m = ((sl < 4u ? n1.z : n1.w) >> sh) & 0xFFu;
+            if (m == 0u) continue;
+            float qlx = (float)(((sl < 4u ? n2.x : n2.y) >> sh) & 0xFFu);
+            float qly = (float)(((sl < 4u ? n2.z : n2.w) >> sh) & 0xFFu);
+            float qlz = (float)(((sl < 4u ? n3.x : n3.y) >> sh) & 0xFFu);
+            float qhx = (float)(((sl < 4u ? n3.z : n3.w) >> sh) & 0xFFu);
+            float qhy = (float)(((sl < 4u ? n4.x : n4.y) >> sh) & 0xFFu);
+            float qhz = (float)(((sl < 4u ? n4.z : n4.w) >> sh) & 0xFFu);
+            float lox = __fmaf_rn(qlx, dq.x, oq.x), hix = __fmaf_rn(qhx, dq.x, oq.x);
+            float loy = __fmaf_rn(qly, dq.y, oq.y), hiy = __fmaf_rn(qhy, dq.y, oq.y);
+            float loz = __fmaf_rn(qlz, dq.z, oq.z), hiz = __fmaf_rn(qhz, dq.z, oq.z);
+            float tn = gmax(gmax(gmin(lox, hix), gmin(loy, hiy)), gmax(gmin(loz, hiz), 0.0f));
+            float tf = gmin(gmin(gmax(lox, hix), gmax(loy, hiy)), gmin(gmax(loz, hiz), tmax)) * kBvhTfarPad;
+            if (tf < tn) continue;
+            if ((m & 0xE0u) == 0x20u && (m & 0x1Fu) >= 24u) hits |= 1u << ((((m & 0x1Fu) - 24u) ^ octinv) & 7u);
+            else leaf_bits |= (m >> 5) << (m & 0x1Fu);
+        }
+        while (leaf_bits != 0u) {
+            int lb = find_msb24(leaf_bits);
+            leaf_bits &= ~(1u << (unsigned)lb);
+            if (leaf((int)n1.y + lb)) return true;
+        }
+        if (hits != 0u) { g_base = n1.x; g_hits = hits; g_imask = imask; }
+        else g_hits = 0u;
+    }
+    flag_error(S, kErrCwGuard);
+    return false;
+}
+
+// ---- one mesh BLAS in a given frame (ro/rd already in the mesh's local frame) --------------
+__device__ __forceinline__ bool mesh_nearest(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float& tmax, int& prim) {
+    bool found = false;
+    if (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) {
+        const float4* tri = m.tri_w;
+        walk_wide(S, m.cwbvh, ro, rd, tmax, [&](int i) {
+            f3 a, e1, e2;
+            load_tri(tri, i, a, e1, e2);
+            float t;
+            if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
+            return false;
+        });
+    } else {
+        const float4* tri = m.tri;
+        walk_binary(S, m.bvh, ro, rd, tmax, [&](int off, int cnt) {
+            for (int i = off; i < off + cnt; ++i) {
+                f3 a, e1, e2;
+                load_tri(tri, i, a, e1, e2);
+                float t;
+                if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
+            }
+            return false;
+        });
+    }
+    return found;
+}
+__device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float max_dist) {
+    if (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) {
+        const float4* tri = m.tri_w;
+        return walk_wide(S, m.cwbvh, ro, rd, max_dist, [&](int i) {
+            f3 a, e1, e2;
+            load_tri(tri, i, a, e1, e2);
+            float t;
+            return tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < max_dist;
+        });
+    }
+    const float4* tri = m.tri;
+    return walk_binary(S, m.bvh, ro, rd, max_dist, [&](int off, int cnt) {
+        for (int i = off; i < off + cnt; ++i) {
+            f3 a, e1, e2;
+            load_tri(tri, i, a, e1, e2);
+            float t;
+            if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < max_dist) return true;
+        }
+        return false;
+    });
+}
+
+// ---- region arms ------------------------------------------------------------------------
+__device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_region& g, int region, const Ray& r, HitRec& h) {
+    if (g.shape == PTR_SHAPE_MESH) {
+        const DevMesh& m = S.meshes[g.ref];
+        int prim = -1;
+        float t = h.t;
+        if (mesh_nearest(S, m, r.o, r.d, t, prim)) {
+            h.t = t;
+            h.region = region;
+            h.element = 0;
+            h.prim = prim;
+        }
+        return;
+    }
+    const DevBatch& b = S.batches[g.ref];
+    float t_near = h.t;
+    walk_binary(S, b.tlas, r.o, r.d, t_near, [&](int off, int cnt) {
+        for (int i = off; i < off + cnt; ++i) {
+            if (b.proto_shape == PTR_SHAPE_SPHERE) {
+                float4 rec = __ldg(b.place + 2 * i);
+                float t;
+                if (sphere_intersect(r, xyz(rec), rec.w, t) && t < t_near) {
+                    t_near = t; h.t = t; h.region = region; h.element = i; h.prim = -1;
+                }
+            } else {
+                float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
+                float s = ts.w;
+                f3 ro = placement_rigid(q, ts, r.o) / s;
+                f3 rd = qrot(q, r.d) / s;
+                int prim = -1;
+                float t = t_near;
+                if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim)) {
+                    t_near = t; h.t = t; h.region = region; h.element = i; h.prim = prim;
+                }
+            }
+        }
+        return false;
+    });
+}
+
+__device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g, const Ray& r, float max_dist) {
+    if (g.shape == PTR_SHAPE_MESH) return mesh_any(S, S.meshes[g.ref], r.o, r.d, max_dist);
+    const DevBatch& b = S.batches[g.ref];
+    return walk_binary(S, b.tlas, r.o, r.d, max_dist, [&](int off, int cnt) {
+        for (int i = off; i < off + cnt; ++i) {
+            if (b.proto_shape == PTR_SHAPE_SPHERE) {
+                float4 rec = __ldg(b.place + 2 * i);
+                float t;
+                if (sphere_intersect(r, xyz(rec), rec.w, t) && t < max_dist) return true;
+            } else {
+                float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
+                float s = ts.w;
+                f3 ro = placement_rigid(q, ts, r.o) / s;
+                f3 rd = qrot(q, r.d) / s;
+                if (mesh_any(S, S.meshes[b.proto_mesh], ro, rd, max_dist)) return true;
+            }
+        }
+        return false;
+    });
+}
+
+// Containment of an instanced SPHERE batch (the TLAS point descent of scene_region_at):
+// the least-negative signed distance among the instances that contain p, else 1e20.
+// Mesh batches are thin (no containment).
+__device__ __forceinline__ float accel_region_sdf(const DevScene& S, const ptr_region& g, f3 p) {
+    const DevBatch& b = S.batches[g.ref];
+    if (b.proto_shape != PTR_SHAPE_SPHERE) return 1.0e20f;
+    float best = -1.0e20f;
+    bool any = false;
+    int stack[kBvhStack];
+    int ptr = 0;
+    stack[0] = 0;
+    while (ptr >= 0) {
+        int ni = stack[ptr];
+        ptr--;
+        float4 n0 = __ldg(b.tlas + 2 * ni), n1 = __ldg(b.tlas + 2 * ni + 1);
+        if (!(p.x >= n0.x && p.y >= n0.y && p.z >= n0.z && p.x <= n1.x && p.y <= n1.y && p.z <= n1.z)) continue;
+        if (n0.w >= 0.0f) {
+            int off = (int)n1.w, cnt = (int)n0.w;
+            for (int i = off; i < off + cnt; ++i) {
+                float4 rec = __ldg(b.place + 2 * i);
+                float ds = length(p - xyz(rec)) - rec.w;
+                if (ds < 0.0f && ds > best) { best = ds; any = true; }
+            }
+        } else {
+            int L = ni + 1, R = (int)n1.w;
+            if (ptr + 2 < kBvhStack) { stack[++ptr] = L; stack[++ptr] = R; }
+            else flag_error(S, kErrBvhStack);
+        }
+    }
+    return any ? best : 1.0e20f;
+}
+
+// Hit normals of an acceleration-structure hit (world space): shading normal (returned)
+// and the geometric normal (h.ng), plus eps and the per-triangle alpha.
+__device__ __forceinline__ f3 accel_hit_normal(const DevScene& S, const ptr_region& g, const HitRec& hr, const Ray&, Hit& h, f3& ng) {
+    h.eps = fp_uncertainty(h.p);
+    if (g.shape == PTR_SHAPE_INSTANCES) {
+        const DevBatch& b = S.batches[g.ref];
+        if (b.proto_shape == PTR_SHAPE_SPHERE) {
+            float4 rec = __ldg(b.place + 2 * hr.element);
+            f3 n = normalize(h.p - xyz(rec));
+            ng = n;   // a primitive's normal is its true surface normal (set from frame.n)
+            return n;
+        }
+        const DevMesh& m = S.meshes[b.proto_mesh];
+        float4 q = __ldg(b.place + 2 * hr.element);
+        const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
+        f3 a, e1, e2;
+        load_tri(tri, hr.prim, a, e1, e2);
+        f3 gl = cross(e1, e2);
+        float al = __ldg(&tri[3 * hr.prim + 1].w);
+        if (al >= 0.0f) h.alpha = al;
+        ng = normalize(placement_normal(q, gl));
+        return normalize(placement_normal(q, gl));
+    }
+    const DevMesh& m = S.meshes[g.ref];
+    const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
+    f3 a, e1, e2;
+    load_tri(tri, hr.prim, a, e1, e2);
+    f3 gl = cross(e1, e2);
+    float al = __ldg(&tri[3 * hr.prim + 1].w);
+    if (al >= 0.0f) h.alpha = al;
+    ng = normalize(gl);
+    return normalize(gl);
 }
 
 }  // namespace ptx

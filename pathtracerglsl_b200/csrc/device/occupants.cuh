@@ -145,13 +145,122 @@ __device__ __forceinline__ ISample hg_sample(f3 wo, float g, float x0, float x1)
     return s;
 }
 
-// ---- environment (features/environment.ts; constant env as a uniform-sphere light) ------
-__device__ __forceinline__ f3 env_radiance(const DevScene& S, f3) {
+// ---- environment (features/environment.ts) ----------------------------------------------
+// constant: closed-form radiance, uniform-sphere NEE (T3).  image: an equirect RGB table
+// read through equirect_uv (env/equirect/equirect_map.glsl:15-21) with bilinear
+// filtering (wrap in u, clamp in v), importance-sampled by the 2-level CDF of
+// env/sampler_cdf.glsl:13-84 mixed with 1/16 uniform-sphere probability.
+__device__ __forceinline__ float2 equirect_uv(const DevScene& S, f3 dir) {
+    f3 n = normalize(dir);
+    float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : atan2f(n.z, n.x)) + S.env_rotation;
+    float theta = atan2f(sqrtf(n.x * n.x + n.z * n.z), n.y);
+    float u = phi * (1.0f / kTwoPi) + 0.5f;
+    u = u - floorf(u);
+    return make_float2(u, theta * (1.0f / kPi));
+}
+__device__ __forceinline__ f3 env_map_bilinear(const DevScene& S, float2 uv) {
+    const int W = S.env_w, H = S.env_h;
+    float x = uv.x * (float)W - 0.5f, y = uv.y * (float)H - 0.5f;
+    float fx0 = floorf(x), fy0 = floorf(y);
+    float ax = x - fx0, ay = y - fy0;
+    int i0 = (int)fx0, j0 = (int)fy0;
+    int i1 = i0 + 1, j1 = j0 + 1;
+    i0 = ((i0 % W) + W) % W;
+    i1 = ((i1 % W) + W) % W;
+    j0 = j0 < 0 ? 0 : (j0 >= H ? H - 1 : j0);
+    j1 = j1 < 0 ? 0 : (j1 >= H ? H - 1 : j1);
+    float4 c00 = __ldg(S.env_map + (size_t)j0 * W + i0), c10 = __ldg(S.env_map + (size_t)j0 * W + i1);
+    float4 c01 = __ldg(S.env_map + (size_t)j1 * W + i0), c11 = __ldg(S.env_map + (size_t)j1 * W + i1);
+    f3 top = xyz(c00) * (1.0f - ax) + xyz(c10) * ax;
+    f3 bot = xyz(c01) * (1.0f - ax) + xyz(c11) * ax;
+    return top * (1.0f - ay) + bot * ay;
+}
+__device__ __forceinline__ f3 env_radiance(const DevScene& S, f3 dir) {
     if (S.env_kind == PTR_ENV_CONSTANT) return ld3(S.env_color) * S.env_intensity;
+    if (S.env_kind == PTR_ENV_IMAGE) return env_map_bilinear(S, equirect_uv(S, dir)) * S.env_intensity;
     return f3(0.0f);
+}
+__device__ __forceinline__ float env_marg(const DevScene& S, int j) { return __ldg(S.env_marg + j); }
+__device__ __forceinline__ float env_cond(const DevScene& S, int j, int i) { return __ldg(S.env_cond + (size_t)j * S.env_w + i); }
+__device__ __forceinline__ float env_texel_domega(int j, int W, int H) {
+    float theta = kPi * ((float)j + 0.5f) / (float)H;
+    return (kTwoPi / (float)W) * 2.0f * sinf(theta) * sinf(0.5f * kPi / (float)H);
+}
+__device__ __forceinline__ float env_uniform_fraction(const DevScene& S) {
+    return env_marg(S, S.env_h - 1) > 0.0f ? 0.0625f : 1.0f;
+}
+__device__ __forceinline__ float env_table_pdf(const DevScene& S, f3 dir) {
+    const int W = S.env_w, H = S.env_h;
+    float2 uv = equirect_uv(S, dir);
+    int i = (int)(uv.x * (float)W);
+    int j = (int)(uv.y * (float)H);
+    i = i < 0 ? 0 : (i > W - 1 ? W - 1 : i);
+    j = j < 0 ? 0 : (j > H - 1 ? H - 1 : j);
+    float d_marg = env_marg(S, j) - (j > 0 ? env_marg(S, j - 1) : 0.0f);
+    float d_cond = env_cond(S, j, i) - (i > 0 ? env_cond(S, j, i - 1) : 0.0f);
+    return (d_cond * d_marg) / env_texel_domega(j, W, H);
+}
+__device__ __forceinline__ f3 env_chart_sample(const DevScene& S, int ci, int cj, float ux, float uy) {
+    const int W = S.env_w, H = S.env_h;
+    float phi = (((float)ci + ux) / (float)W - 0.5f) * kTwoPi - S.env_rotation;
+    bool north = 2 * cj < H;
+    float row = north ? (float)cj : (float)(H - cj - 1);
+    float a = sinf(0.5f * kPi * row / (float)H);
+    float b = sinf(0.5f * kPi * (row + 1.0f) / (float)H);
+    float t = north ? uy : 1.0f - uy;
+    float h = (a * a) * (1.0f - t) + (b * b) * t;
+    float y = (north ? 1.0f : -1.0f) * (1.0f - 2.0f * h);
+    float r = 2.0f * sqrtf(h * (1.0f - h));
+    return f3(r * cosf(phi), y, r * sinf(phi));
+}
+__device__ __forceinline__ f3 env_sample_table(const DevScene& S, float x0, float x1) {
+    const int W = S.env_w, H = S.env_h;
+    const float kFracMax = 0.9999999f;
+    int lo = 0, hi = H - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (x0 >= env_marg(S, mid)) lo = mid + 1; else hi = mid;
+    }
+    int j = lo;
+    float m_lo = j > 0 ? env_marg(S, j - 1) : 0.0f;
+    float d_marg = env_marg(S, j) - m_lo;
+    float v_frac = d_marg > 0.0f ? clampf((x0 - m_lo) / d_marg, 0.0f, kFracMax) : 0.5f;
+    lo = 0;
+    hi = W - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (x1 >= env_cond(S, j, mid)) lo = mid + 1; else hi = mid;
+    }
+    int i = lo;
+    float c_lo = i > 0 ? env_cond(S, j, i - 1) : 0.0f;
+    float d_cond = env_cond(S, j, i) - c_lo;
+    float u_frac = d_cond > 0.0f ? clampf((x1 - c_lo) / d_cond, 0.0f, kFracMax) : 0.5f;
+    return env_chart_sample(S, i, j, u_frac, v_frac);
+}
+__device__ __forceinline__ float env_pdf(const DevScene& S, f3 dir) {
+    if (S.env_kind != PTR_ENV_IMAGE) return 1.0f / (4.0f * kPi);
+    float a = env_uniform_fraction(S);
+    return (1.0f - a) * env_table_pdf(S, dir) + a / (4.0f * kPi);
 }
 __device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, float x1) {
     LightSample ls;
+    if (S.env_kind == PTR_ENV_IMAGE) {
+        float a = env_uniform_fraction(S);
+        if (x0 < a) {
+            float y = 1.0f - 2.0f * (x0 / a);
+            float r = sqrtf(gmax(0.0f, 1.0f - y * y));
+            float phi = kTwoPi * x1;
+            ls.wi = f3(r * cosf(phi), y, r * sinf(phi));
+        } else {
+            ls.wi = env_sample_table(S, (x0 - a) / (1.0f - a), x1);
+        }
+        ls.distance = kMaxDist;
+        ls.radiance = env_radiance(S, ls.wi);
+        ls.pdf = env_pdf(S, ls.wi);
+        ls.flags = 0u;
+        ls.light_id = -1;
+        return ls;
+    }
     float z = 1.0f - 2.0f * x0;
     float r = sqrtf(gmax(0.0f, 1.0f - z * z));
     float phi = kTwoPi * x1;
@@ -163,7 +272,6 @@ __device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, f
     ls.light_id = -1;
     return ls;
 }
-__device__ __forceinline__ float env_pdf(const DevScene&, f3) { return 1.0f / (4.0f * kPi); }
 
 // ---- lights: quad (area -> solid angle), sphere (visible cone), point (delta) -----------
 // (lights/quad/quad.glsl:14-41, lights/sphere/sphere.glsl:21-71, lights/point/point.glsl)

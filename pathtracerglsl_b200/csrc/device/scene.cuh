@@ -10,22 +10,25 @@
 
 namespace ptx {
 
-// Mesh BLAS on the device: binary BVH (2 x float4 per node, bvh.ts:344-383 layout) and/or
-// the compressed wide BVH (5 x uint4 = 80 B per node, cwbvh.ts:18-31 layout).
+// Mesh BLAS on the device: triangles (3 float4 each: v0 | e1, alpha | e2, in leaf order),
+// binary BVH nodes (2 float4: (min.xyz, A) (max.xyz, B), bvh.ts:344-383 layout) and the
+// compressed wide BVH (5 uint4 = 80 B per node, cwbvh.ts:18-31 layout) with its own
+// triangle order.
 struct DevMesh {
-    const float4* tri;        // 3 float4 per triangle: v0.xyz | e1.xyz | e2.xyz (w unused)
-    const float4* bvh;        // 2 float4 per node (min.xyz, A) (max.xyz, B)
-    const uint4* cwbvh;       // 5 uint4 per node
-    const uint32_t* cw_items; // CWBVH leaf item -> triangle index
-    const float* tri_alpha;   // optional per-triangle GGX alpha
+    const float4* tri;        // binary-BVH leaf order
+    const float4* tri_w;      // wide-BVH leaf order
+    const float4* bvh;
+    const uint4* cwbvh;
     int n_tris, n_nodes, n_cw_nodes, pad;
 };
 
+// Instanced batch: placements in TLAS leaf order, 2 float4 each — mesh prototypes
+// (q, ts) with ts = (t_rigid.xyz, s); sphere prototypes (world centre, world radius)
+// folded into the first float4 (the params tier).
 struct DevBatch {
-    const float4* place;      // 2 float4 per instance: q (world -> rigid), ts = (t_rigid, s)
-    const float4* tlas;       // binary BVH over instance world boxes (2 float4 per node)
+    const float4* place;
+    const float4* tlas;       // binary BVH over the instances' world boxes
     int n_inst, proto_shape, proto_mesh, n_tlas;
-    float4 proto;             // sphere prototype: center, radius
 };
 
 struct DevScene {
@@ -35,16 +38,17 @@ struct DevScene {
     const int* light_of_region;
     const DevMesh* meshes;
     const DevBatch* batches;
+    unsigned* err_flags;      // device guard flags (stack overflow, iteration guard)
     int n_regions, n_materials, n_lights, ambient_material;
-    int has_media, has_accel, n_meshes, n_batches;
+    int has_media, accel, n_meshes, n_batches;
     // environment
     int env_kind, env_samplable, env_select_live, env_w;
     int env_h, pad0, pad1, pad2;
     float env_color[4];
     float env_intensity, env_select_prob, env_rotation, pad3;
-    const float4* env_map;    // W*H RGBA
-    const float* env_marg;    // H+1 cumulative
-    const float* env_cond;    // H*(W+1) cumulative
+    const float4* env_map;    // W*H RGBA, row 0 = v = 0 (+Y pole)
+    const float* env_marg;    // H cumulative (marginal over rows)
+    const float* env_cond;    // H*W cumulative (conditional within each row)
 };
 
 // ---- closed-form arms (components/geometry/*/*.glsl) ------------------------------------

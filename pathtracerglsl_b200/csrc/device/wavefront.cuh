@@ -83,7 +83,6 @@ __device__ __forceinline__ int warp_append(unsigned* counter, bool pred) {
 
 // ---- scene queries -------------------------------------------------------------------
 // Nearest hit over every arm; returns region (or -1), element, primitive and t.
-struct HitRec { float t, u, v; int region, element, prim; };
 
 __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r) {
     HitRec h;
@@ -143,15 +142,24 @@ __device__ __forceinline__ void fill_hit(const DevScene& S, const Ray& r, const 
     h.element = hr.element;
     h.alpha = -1.0f;
     const ptr_region& g = S.regions[hr.region];
-    f3 n;
-    if (g.shape >= PTR_SHAPE_MESH) {
-        n = accel_hit_normal(S, g, hr, r, h);
+    if (g.shape == PTR_SHAPE_MESH || (g.shape == PTR_SHAPE_INSTANCES && S.batches[g.ref].proto_shape == PTR_SHAPE_MESH)) {
+        // mesh hits: frame from the (normalised) shading normal, ng the triangle's plane normal
+        f3 ngv;
+        f3 n = accel_hit_normal(S, g, hr, r, h, ngv);
+        h.frame = ambient_frame(n);
+        h.ng = ngv;
     } else {
-        n = analytic_normal(g, h.p);
-        h.eps = fp_uncertainty(h.p);
+        f3 n;
+        if (g.shape == PTR_SHAPE_INSTANCES) {
+            f3 unused;
+            n = accel_hit_normal(S, g, hr, r, h, unused);
+        } else {
+            n = analytic_normal(g, h.p);
+            h.eps = fp_uncertainty(h.p);
+        }
+        h.frame = ambient_frame(n);
+        h.ng = h.frame.n;   // a primitive's normal is its true surface normal
     }
-    h.frame = ambient_frame(n);
-    h.ng = h.frame.n;
     int outside = scene_region_at(S, h.p + h.ng * kEpsInterface);
     if (dot(r.d, h.ng) < 0.0f) {
         h.region_from = outside;
@@ -553,6 +561,28 @@ __global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double
         }
         sum[3 * pix + 0] = s0; sum[3 * pix + 1] = s1; sum[3 * pix + 2] = s2;
         sumsq[3 * pix + 0] = q0; sumsq[3 * pix + 1] = q1; sumsq[3 * pix + 2] = q2;
+    }
+}
+
+// Raw nearest-hit queries (tests and tools): per ray (o.xyz, d.xyz) the region, the
+// element (instance), the ORIGINAL triangle index (or -1) and t (kMaxDist on a miss).
+__global__ void k_trace_rays(DevScene S, const float* rays, int n, int* region, int* element, int* prim, float* t_out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        Ray r;
+        r.o = f3(rays[6 * k], rays[6 * k + 1], rays[6 * k + 2]);
+        r.d = f3(rays[6 * k + 3], rays[6 * k + 4], rays[6 * k + 5]);
+        HitRec h = scene_closest(S, r);
+        int orig = -1;
+        if (h.region >= 0 && h.prim >= 0) {
+            const ptr_region& g = S.regions[h.region];
+            const DevMesh& m = S.meshes[g.shape == PTR_SHAPE_MESH ? g.ref : S.batches[g.ref].proto_mesh];
+            const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
+            orig = __float_as_int(tri[3 * h.prim].w);
+        }
+        region[k] = h.region;
+        element[k] = h.element;
+        prim[k] = orig;
+        t_out[k] = h.t;
     }
 }
 

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "device/wavefront.cuh"
+#include "host/accel_build.h"
 
 using namespace ptx;
 
@@ -63,6 +64,8 @@ struct ptr_program {
 };
 
 namespace {
+
+inline float __int_as_float_host(int v) { float f; std::memcpy(&f, &v, 4); return f; }
 
 int fail(ptr_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -142,6 +145,8 @@ struct ProfRec { int cls; cudaEvent_t a, b; };
 
 void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
                  std::vector<ProfRec>* prof = nullptr) {
+    DevScene Sp = s->dev;
+    Sp.accel = p->desc.accel;
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
         ProfRec r{cls, nullptr, nullptr};
@@ -152,7 +157,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
         return &prof->back();
     };
     auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
-    const DevScene& S = s->dev;
+    const DevScene& S = Sp;
     const PathPool& pool = p->pool;
     ProgParams P;
     P.max_bounces = p->desc.max_bounces;
@@ -200,10 +205,146 @@ int device_sms(int dev) {
     return n > 0 ? n : 148;
 }
 
-// Acceleration structures of meshes and instanced batches (built on the host, uploaded once).
+// Acceleration structures of meshes and instanced batches, built on the host and uploaded
+// once: per mesh the binary SAH BLAS (leaf 2) and the compressed wide BVH, each with the
+// triangles re-emitted in its leaf order as (v0, e1 | alpha, e2); per batch a binary TLAS
+// (leaf 2) over the instances' world boxes with the placements in leaf order.
 int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
-    (void)s;
-    if (d->n_meshes > 0 || d->n_batches > 0) return fail(ctx, PTR_E_UNSUPPORTED, "meshes and instanced batches are not available in this build");
+    DevScene& S = s->dev;
+    std::vector<DevMesh> meshes(d->n_meshes > 0 ? d->n_meshes : 0);
+    std::vector<std::vector<double>> root_box(meshes.size());
+    for (int mi = 0; mi < d->n_meshes; ++mi) {
+        const ptr_mesh_desc& md = d->meshes[mi];
+        if (md.n_triangles <= 0 || md.n_vertices <= 0 || !md.positions || !md.indices)
+            return fail(ctx, PTR_E_INVALID, "scene: mesh " + std::to_string(mi) + " is empty");
+        const int T = md.n_triangles;
+        std::vector<double> boxes(6 * (size_t)T);
+        for (int t = 0; t < T; ++t) {
+            double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+            for (int k = 0; k < 3; ++k) {
+                uint32_t v = md.indices[3 * (size_t)t + k];
+                if (v >= (uint32_t)md.n_vertices) return fail(ctx, PTR_E_INVALID, "scene: mesh index out of range");
+                for (int a = 0; a < 3; ++a) {
+                    double x = md.positions[3 * (size_t)v + a];
+                    if (!std::isfinite(x)) return fail(ctx, PTR_E_INVALID, "scene: non-finite vertex");
+                    mn[a] = std::min(mn[a], x);
+                    mx[a] = std::max(mx[a], x);
+                }
+            }
+            for (int a = 0; a < 3; ++a) { boxes[6 * (size_t)t + a] = mn[a]; boxes[6 * (size_t)t + 3 + a] = mx[a]; }
+        }
+        auto tri_array = [&](const std::vector<uint32_t>& order) {
+            std::vector<float4> tri(3 * (size_t)T);
+            for (int i = 0; i < T; ++i) {
+                const uint32_t t = order[i];
+                const float* a = md.positions + 3 * (size_t)md.indices[3 * (size_t)t];
+                const float* b = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 1];
+                const float* c = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 2];
+                float alpha = md.tri_alpha ? md.tri_alpha[t] : -1.0f;
+                tri[3 * (size_t)i] = make_float4(a[0], a[1], a[2], __int_as_float_host((int)t));
+                tri[3 * (size_t)i + 1] = make_float4(b[0] - a[0], b[1] - a[1], b[2] - a[2], alpha);
+                tri[3 * (size_t)i + 2] = make_float4(c[0] - a[0], c[1] - a[1], c[2] - a[2], 0.0f);
+            }
+            return tri;
+        };
+        ptx_host::BinaryBvh bin = ptx_host::build_bvh(boxes.data(), T, ptx_host::kBvhLeafSize, false);
+        if (bin.max_depth >= ptx_host::kBvhStackDepth) std::fprintf(stderr, "ptx_rt: BVH depth %d reaches the walk's stack depth\n", bin.max_depth);
+        ptx_host::WideBvh wide = ptx_host::build_cwbvh(boxes.data(), T, ptx_host::kCwbvhCPrim);
+        if (wide.error) return fail(ctx, PTR_E_INVALID, "scene: CWBVH build failed (exponent range or DP invariant)");
+        std::vector<float4> tri_b = tri_array(bin.order), tri_w = tri_array(wide.order);
+        DevMesh& m = meshes[mi];
+        const float4* p4 = nullptr;
+        const uint4* u4 = nullptr;
+        int rc;
+        if ((rc = dev_copy(ctx, s->allocs, tri_b.data(), tri_b.size(), &p4))) return rc;
+        m.tri = p4;
+        if ((rc = dev_copy(ctx, s->allocs, tri_w.data(), tri_w.size(), &p4))) return rc;
+        m.tri_w = p4;
+        if ((rc = dev_copy(ctx, s->allocs, (const float4*)bin.nodes.data(), 2 * (size_t)bin.node_count, &p4))) return rc;
+        m.bvh = p4;
+        if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wide.nodes.data(), 5 * (size_t)wide.node_count, &u4))) return rc;
+        m.cwbvh = u4;
+        m.n_tris = T;
+        m.n_nodes = bin.node_count;
+        m.n_cw_nodes = wide.node_count;
+        root_box[mi] = {bin.nodes[0], bin.nodes[1], bin.nodes[2], bin.nodes[4], bin.nodes[5], bin.nodes[6]};
+        s->max_stack_depth = std::max(s->max_stack_depth, bin.max_depth);
+    }
+    std::vector<DevBatch> batches(d->n_batches > 0 ? d->n_batches : 0);
+    for (int bi = 0; bi < d->n_batches; ++bi) {
+        const ptr_batch_desc& bd = d->batches[bi];
+        const int N = bd.n_instances;
+        if (N <= 0 || !bd.placements) return fail(ctx, PTR_E_INVALID, "scene: instanced batch " + std::to_string(bi) + " is empty");
+        if (bd.prototype_shape == PTR_SHAPE_MESH && (bd.prototype_ref < 0 || bd.prototype_ref >= d->n_meshes))
+            return fail(ctx, PTR_E_INVALID, "scene: batch prototype mesh out of range");
+        if (bd.prototype_shape != PTR_SHAPE_MESH && bd.prototype_shape != PTR_SHAPE_SPHERE)
+            return fail(ctx, PTR_E_INVALID, "scene: batch prototype must be a mesh or a sphere");
+        std::vector<double> boxes(6 * (size_t)N);
+        std::vector<float4> rec(2 * (size_t)N);
+        for (int i = 0; i < N; ++i) {
+            const float* pl = bd.placements + 8 * (size_t)i;
+            const double qx = pl[0], qy = pl[1], qz = pl[2], qw = pl[3];
+            const double tx = pl[4], ty = pl[5], tz = pl[6], sc = pl[7];
+            if (!(sc > 0.0)) return fail(ctx, PTR_E_INVALID, "scene: placement scale must be positive");
+            // world = rotate(conj(q), s * local - t_rigid)
+            auto to_world = [&](double x, double y, double z, double out[3]) {
+                double vx = sc * x - tx, vy = sc * y - ty, vz = sc * z - tz;
+                const double cx = -qx, cy = -qy, cz = -qz;   // conjugate
+                double c1x = cy * vz - cz * vy + qw * vx, c1y = cz * vx - cx * vz + qw * vy, c1z = cx * vy - cy * vx + qw * vz;
+                double c2x = cy * c1z - cz * c1y, c2y = cz * c1x - cx * c1z, c2z = cx * c1y - cy * c1x;
+                out[0] = vx + 2.0 * c2x; out[1] = vy + 2.0 * c2y; out[2] = vz + 2.0 * c2z;
+            };
+            double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+            if (bd.prototype_shape == PTR_SHAPE_SPHERE) {
+                double c[3];
+                to_world(bd.proto[0], bd.proto[1], bd.proto[2], c);
+                const double r = sc * bd.proto[3];
+                for (int a = 0; a < 3; ++a) { mn[a] = c[a] - r; mx[a] = c[a] + r; }
+                rec[2 * (size_t)i] = make_float4((float)c[0], (float)c[1], (float)c[2], (float)r);
+                rec[2 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                const std::vector<double>& rb = root_box[bd.prototype_ref];
+                for (int k = 0; k < 8; ++k) {
+                    double w[3];
+                    to_world((k & 1) ? rb[3] : rb[0], (k & 2) ? rb[4] : rb[1], (k & 4) ? rb[5] : rb[2], w);
+                    for (int a = 0; a < 3; ++a) { mn[a] = std::min(mn[a], w[a]); mx[a] = std::max(mx[a], w[a]); }
+                }
+                rec[2 * (size_t)i] = make_float4(pl[0], pl[1], pl[2], pl[3]);
+                rec[2 * (size_t)i + 1] = make_float4(pl[4], pl[5], pl[6], pl[7]);
+            }
+            for (int a = 0; a < 3; ++a) { boxes[6 * (size_t)i + a] = mn[a]; boxes[6 * (size_t)i + 3 + a] = mx[a]; }
+        }
+        ptx_host::BinaryBvh tl = ptx_host::build_bvh(boxes.data(), N, ptx_host::kBvhLeafSize, false);
+        std::vector<float4> rec_leaf(2 * (size_t)N);
+        for (int i = 0; i < N; ++i) {
+            rec_leaf[2 * (size_t)i] = rec[2 * (size_t)tl.order[i]];
+            rec_leaf[2 * (size_t)i + 1] = rec[2 * (size_t)tl.order[i] + 1];
+        }
+        DevBatch& b = batches[bi];
+        const float4* p4 = nullptr;
+        int rc;
+        if ((rc = dev_copy(ctx, s->allocs, rec_leaf.data(), rec_leaf.size(), &p4))) return rc;
+        b.place = p4;
+        if ((rc = dev_copy(ctx, s->allocs, (const float4*)tl.nodes.data(), 2 * (size_t)tl.node_count, &p4))) return rc;
+        b.tlas = p4;
+        b.n_inst = N;
+        b.proto_shape = bd.prototype_shape;
+        b.proto_mesh = bd.prototype_ref;
+        b.n_tlas = tl.node_count;
+    }
+    int rc;
+    const DevMesh* dm = nullptr;
+    const DevBatch* db = nullptr;
+    if ((rc = dev_copy(ctx, s->allocs, meshes.data(), meshes.size(), &dm))) return rc;
+    if ((rc = dev_copy(ctx, s->allocs, batches.data(), batches.size(), &db))) return rc;
+    S.meshes = dm;
+    S.batches = db;
+    S.n_meshes = (int)meshes.size();
+    S.n_batches = (int)batches.size();
+    unsigned zero = 0;
+    const unsigned* ef = nullptr;
+    if ((rc = dev_copy(ctx, s->allocs, &zero, 1, &ef))) return rc;
+    S.err_flags = (unsigned*)ef;
     return PTR_OK;
 }
 
@@ -399,12 +540,16 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     S.env_select_prob = d->env.select_prob;
     S.env_rotation = d->env.rotation;
     if (d->env.kind == PTR_ENV_IMAGE) {
+        if (d->env.width <= 0 || d->env.height <= 0 || !d->env.radiance || !d->env.marginal || !d->env.conditional) {
+            ptr_free_scene(s);
+            return fail(ctx, PTR_E_INVALID, "scene: image environment without its table");
+        }
         S.env_w = d->env.width;
         S.env_h = d->env.height;
         const float* m = nullptr;
         if ((rc = dev_copy(ctx, s->allocs, (const float4*)d->env.radiance, (size_t)S.env_w * S.env_h, &S.env_map)) ||
-            (rc = dev_copy(ctx, s->allocs, d->env.marginal, (size_t)S.env_h + 1, &S.env_marg)) ||
-            (rc = dev_copy(ctx, s->allocs, d->env.conditional, (size_t)S.env_h * (S.env_w + 1), &m))) {
+            (rc = dev_copy(ctx, s->allocs, d->env.marginal, (size_t)S.env_h, &S.env_marg)) ||
+            (rc = dev_copy(ctx, s->allocs, d->env.conditional, (size_t)S.env_h * S.env_w, &m))) {
             ptr_free_scene(s);
             return rc;
         }
@@ -482,6 +627,37 @@ int ptr_render_samples(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* 
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
     cudaFree(dev);
     return rc;
+}
+
+int ptr_trace_closest(ptr_ctx* ctx, ptr_scene* s, int accel, const float* rays, int n,
+                      int* region, int* element, int* prim, float* t) {
+    if (!ctx || !s || !rays || n < 0 || !region || !element || !prim || !t) return fail(ctx, PTR_E_INVALID, "ptr_trace_closest: null argument");
+    if (n == 0) return PTR_OK;
+    CK(ctx, cudaSetDevice(ctx->device));
+    float* d_rays = nullptr;
+    int *d_reg = nullptr, *d_el = nullptr, *d_prim = nullptr;
+    float* d_t = nullptr;
+    size_t nn = (size_t)n;
+    if (cudaMalloc(&d_rays, nn * 6 * sizeof(float)) != cudaSuccess || cudaMalloc(&d_reg, nn * 4) != cudaSuccess ||
+        cudaMalloc(&d_el, nn * 4) != cudaSuccess || cudaMalloc(&d_prim, nn * 4) != cudaSuccess || cudaMalloc(&d_t, nn * 4) != cudaSuccess) {
+        cudaFree(d_rays); cudaFree(d_reg); cudaFree(d_el); cudaFree(d_prim); cudaFree(d_t);
+        return fail(ctx, PTR_E_NOMEM, "ptr_trace_closest: buffers");
+    }
+    DevScene S = s->dev;
+    S.accel = accel;
+    cudaError_t e = cudaMemcpyAsync(d_rays, rays, nn * 6 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        k_trace_rays<<<256, 128, 0, ctx->stream>>>(S, d_rays, n, d_reg, d_el, d_prim, d_t);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(region, d_reg, nn * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(element, d_el, nn * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(prim, d_prim, nn * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t, d_t, nn * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_rays); cudaFree(d_reg); cudaFree(d_el); cudaFree(d_prim); cudaFree(d_t);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ptr_trace_closest");
+    return PTR_OK;
 }
 
 int ptr_get_stream(ptr_ctx* ctx, void** stream) {

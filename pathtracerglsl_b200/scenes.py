@@ -73,3 +73,133 @@ def furnace(direct="mis", max_depth=8):
         "view": {"tonemap": {"type": "none"}},
     }
     return scene, strategy
+
+
+# ---------------------------------------------------------------------------------- meshes
+import numpy as _np
+
+
+def icosphere(level):
+    """Subdivided icosahedron on the unit sphere: 20*4^level triangles, 10*4^level+2 vertices."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = _np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                   [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], _np.float64)
+    f = _np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+                   [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8],
+                   [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], _np.int64)
+    v /= _np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        nv = len(v)
+        edges = _np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        key = _np.minimum(edges[:, 0], edges[:, 1]) * nv + _np.maximum(edges[:, 0], edges[:, 1])
+        uniq, inv = _np.unique(key, return_inverse=True)
+        a, b = uniq // nv, uniq % nv
+        mid = v[a] + v[b]
+        mid /= _np.linalg.norm(mid, axis=1, keepdims=True)
+        v = _np.concatenate([v, mid])
+        m = inv.reshape(3, -1).T + nv          # midpoints of (01, 12, 20)
+        f = _np.concatenate([_np.stack([f[:, 0], m[:, 0], m[:, 2]], 1), _np.stack([f[:, 1], m[:, 1], m[:, 0]], 1),
+                             _np.stack([f[:, 2], m[:, 2], m[:, 1]], 1), m])
+    return v, f
+
+
+def _hash3(ix, iy, iz, seed):
+    h = (ix.astype(_np.uint32) * _np.uint32(73856093)) ^ (iy.astype(_np.uint32) * _np.uint32(19349663)) \
+        ^ (iz.astype(_np.uint32) * _np.uint32(83492791)) ^ _np.uint32(seed * 2654435761 & 0xFFFFFFFF)
+    h = h ^ (h >> _np.uint32(13))
+    h = h * _np.uint32(1274126177)
+    h = h ^ (h >> _np.uint32(16))
+    return (h & _np.uint32(0xFFFFFF)).astype(_np.float64) / float(1 << 24)
+
+
+def value_noise(p, seed, freq=4.0):
+    """Seeded 3D value noise in [-1, 1]: hashed lattice values, smoothstep-trilinear."""
+    q = p * freq
+    i0 = _np.floor(q).astype(_np.int64)
+    fq = q - i0
+    w = fq * fq * (3.0 - 2.0 * fq)
+    out = _np.zeros(len(p))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                h = _hash3(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed)
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out += wx * wy * wz * h
+    return 2.0 * out - 1.0
+
+
+def sky_table(width=1024, height=512, seed=0, sun_radiance=5.0e3, sun_diameter_deg=0.5):
+    """Procedural equirect sky (row 0 = +Y pole): a zenith-to-horizon gradient, a dark
+    ground half, and a seeded sun disc of the given radiance and angular diameter."""
+    rng = _np.random.RandomState(seed)
+    j = (_np.arange(height) + 0.5) / height
+    i = (_np.arange(width) + 0.5) / width
+    theta = _np.pi * j[:, None] * _np.ones((1, width))
+    phi = (i[None, :] - 0.5) * 2.0 * _np.pi * _np.ones((height, 1))
+    d = _np.stack([_np.cos(phi) * _np.sin(theta), _np.cos(theta), _np.sin(phi) * _np.sin(theta)], -1)
+    up = _np.clip(d[..., 1], 0.0, 1.0)
+    zen = _np.array([0.25, 0.45, 0.95])
+    hor = _np.array([0.9, 0.95, 1.0])
+    sky = hor[None, None, :] * (1 - up[..., None]) ** 2 + zen[None, None, :] * (1 - (1 - up[..., None]) ** 2)
+    ground = _np.array([0.08, 0.07, 0.06])
+    table = _np.where(d[..., 1:2] >= 0.0, sky, ground[None, None, :] * _np.ones_like(sky))
+    sun_el = rng.uniform(0.35, 1.0)
+    sun_az = rng.uniform(0, 2 * _np.pi)
+    sd = _np.array([_np.cos(sun_az) * _np.cos(sun_el), _np.sin(sun_el), _np.sin(sun_az) * _np.cos(sun_el)])
+    cosang = d @ sd
+    half = _np.radians(sun_diameter_deg) / 2.0
+    table = table + (cosang >= _np.cos(half))[..., None] * sun_radiance * _np.array([1.0, 0.95, 0.85])
+    return table.astype(_np.float32), sd
+
+
+def mesh_scene(level=8, instances=16, seed=0, width=1920, height=1080, spp=256, max_depth=12,
+               env_size=(1024, 512), direct="mis", accel="cwbvh"):
+    """The mesh workload: a noise-displaced level-`level` icosphere (GGX conductor,
+    F0 (0.9, 0.6, 0.3), per-triangle alpha ~ U(0.05, 0.5)) instanced `instances` times
+    by seeded similarities over a Lambert ground plane (albedo 0.5), lit by a procedural
+    equirect sky with a sun lobe of radiance 5e3 over 0.5 degrees."""
+    rng = _np.random.RandomState(seed)
+    v, f = icosphere(level)
+    v = v * (1.0 + 0.05 * value_noise(v, seed))[:, None]
+    alpha = rng.uniform(0.05, 0.5, len(f)).astype(_np.float32)
+    placements = []
+    cells = _np.arange(instances)
+    grid = int(_np.ceil(_np.sqrt(instances)))
+    for k in cells:
+        gx, gz = k % grid, k // grid
+        s = float(rng.uniform(0.5, 1.1))
+        x = (gx - (grid - 1) / 2.0) * 2.6 + float(rng.uniform(-0.3, 0.3))
+        z = (gz - (grid - 1) / 2.0) * 2.6 + float(rng.uniform(-0.3, 0.3))
+        axis = rng.normal(size=3)
+        placements.append({"position": [x, s * 1.05, z], "scale": s,
+                           "rotation": {"axis": list(axis / _np.linalg.norm(axis)), "angle": float(rng.uniform(0, 6.28))}})
+    table, sun = sky_table(env_size[0], env_size[1], seed)
+    scene = {
+        "id": "mesh-c2",
+        "ambientSpace": {"type": "euclidean"},
+        "objects": [
+            {"type": "plane", "parameters": {"normal": [0, 1, 0], "offset": 0.0}, "material": "ground"},
+            {"kind": "instanced",
+             "prototype": {"kind": "mesh", "positions": v.astype(_np.float32).reshape(-1),
+                           "indices": f.astype(_np.uint32).reshape(-1), "material": "metal",
+                           "triangleAlpha": alpha},
+             "placements": placements},
+        ],
+        "materials": {"ground": {"model": "lambert", "albedo": [0.5, 0.5, 0.5]},
+                      "metal": {"model": "ggx", "f0": [0.9, 0.6, 0.3], "roughness": 0.5}},
+        "lights": [],
+        "environment": {"type": "image", "table": table, "intensity": 1.0, "sampleAsLight": True},
+    }
+    extent = grid * 1.3
+    strategy = {
+        "id": "pt-" + direct,
+        "measurement": {"camera": {"type": "pinhole", "fov": math.radians(45.0),
+                                   "position": [0.0, extent * 1.1, extent * 2.2], "target": [0.0, 0.6, 0.0]},
+                        "maxBounces": max_depth},
+        "estimator": {"directLighting": direct, "russianRoulette": {"startDepth": 3},
+                      "meshTraversal": accel, "accumulation": {"type": "average"}},
+        "view": {"tonemap": {"type": "none"}},
+    }
+    return scene, strategy, (width, height, spp)
