@@ -226,21 +226,29 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def algorithmic_bytes(kernel, c):
-    """Bytes the algorithm must move per render for one kernel class (path state in HBM;
-    the scene tables are a few KB and cache-resident by design, so not counted)."""
+def algorithmic_bytes(kernel, c, cw=True):
+    """Bytes the algorithm must move per render for one kernel class.  Path state: the
+    SoA records each kernel reads and writes.  Traversal: every node popped (80 B wide /
+    32 B binary BLAS node, 32 B TLAS node), every triangle tested (48 B: v0, e1, e2) and
+    every instance entered (32 B placement).  The few-KB scene tables (regions,
+    materials, lights) are cache-resident by design and not counted."""
     paths, closest, shadow = c["paths"], c["closest_queries"], c["shadow_queries"]
     alive = max(closest - paths, 0)
+    node_b = 80 if cw else 32
+
+    def trav(prefix):
+        return (c.get(prefix + "blas_nodes", 0) * node_b + c.get(prefix + "triangles", 0) * 48
+                + c.get(prefix + "tlas_nodes", 0) * 32 + c.get(prefix + "instances", 0) * 32)
     if kernel == "closest":
-        return closest * (4 + 32 + 32)                      # queue, ray, hit record
+        return closest * (4 + 32 + 32) + trav("")
     if kernel == "shade":
         return closest * (4 + 136 + 16) + alive * (104 + 4) + shadow * (64 + 4)
     if kernel == "shadow":
-        return shadow * (4 + 64 + 32)
+        return shadow * (4 + 64 + 32) + trav("shadow_")
     if kernel == "generate":
         return paths * (104 + 4 + 16)
     if kernel == "film":
-        return paths * 16 + 0
+        return paths * 16
     return 0
 
 
@@ -307,14 +315,18 @@ def run_ours(args):
     e2e = {"value": samples_total / el, "unit": "samples/s",
            "h2d_bytes_per_step": 160, "d2h_bytes_per_step": int(img.nbytes)}
 
-    # ---- instrumented pass: per-kernel-class device time (not part of the timed region)
+    # ---- instrumented passes (not part of the timed region): per-kernel-class device
+    # time with CUDA events, then the traversal tallies of the counting kernels
+    from pathtracerglsl_b200 import abi as _abi
     eng.reset()
-    prof = eng.profile_render(w, h, spp)
+    prof = eng.profile_render(w, h, spp, _abi.PROFILE_TIMING)
+    eng.reset()
+    eng.profile_render(w, h, spp, _abi.PROFILE_WORK)
     cnt = eng.counters()
     kernel, (kms, klaunch) = max(prof.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = measured_peaks()
     launch_ms = kms / max(klaunch, 1)
-    bytes_per_launch = algorithmic_bytes(kernel, cnt) / max(klaunch, 1)
+    bytes_per_launch = algorithmic_bytes(kernel, cnt, cfg.get("mesh_accel", "cwbvh") == "cwbvh") / max(klaunch, 1)
     achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9
     total_prof_ms = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": "k_" + kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -331,6 +343,9 @@ def run_ours(args):
                                parallelism=f"replicas x{world}"),
                 "e2e": e2e, "roofline": roofline, "gpu_launches": launches * args.steps,
                 "clocks": clk,
+                "traversal": {k: cnt[k] for k in ("blas_nodes", "triangles", "tlas_nodes", "instances",
+                                                   "shadow_blas_nodes", "shadow_triangles", "shadow_tlas_nodes",
+                                                   "shadow_instances")},
                 "rays": {"closest_per_sample": cnt["closest_queries"] / cnt["paths"],
                          "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
                          "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}

@@ -193,8 +193,11 @@ typedef struct ptr_counters {
     uint64_t paths;             /* camera paths traced                                */
     uint64_t closest_queries;   /* closest-hit ray queries                            */
     uint64_t shadow_queries;    /* shadow (any-hit / transmittance) queries           */
-    uint64_t nodes_visited;     /* BVH nodes popped (when counting is enabled)         */
-    uint64_t prims_tested;      /* primitive / triangle tests (when counting enabled)  */
+    uint64_t nodes_visited;     /* mesh BLAS nodes popped (counting pass only)         */
+    uint64_t prims_tested;      /* triangles tested (counting pass only)               */
+    uint64_t tlas_nodes;        /* instance TLAS nodes popped (counting pass only)     */
+    uint64_t instances;         /* instances entered (counting pass only)              */
+    uint64_t shadow_work[4];    /* the same four tallies for the shadow queries        */
     uint32_t error_flags;       /* device-side guard flags (stack / budget)            */
     uint32_t pad;
 } ptr_counters;
@@ -285,10 +288,14 @@ int ptr_read_export_device(ptr_program* prog, const char* name, float* dst_devic
 /* Device work counters of the last ptr_render on this program (synchronises). */
 int ptr_get_counters(ptr_program* prog, ptr_counters* out);
 
-/* Instrument the next ptr_render: it runs without the CUDA graph and records a pair of
- * CUDA events around every kernel launch on the context's stream.  ptr_get_profile then
- * returns, per kernel class k (0 generate, 1 closest-hit, 2 shade, 3 shadow, 4 film),
- * the summed device time ms_out[k] and the number of launches launches_out[k]. */
+/* Instrument the next ptr_render (mode bits): PTR_PROFILE_TIMING runs it without the
+ * CUDA graph with a pair of CUDA events around every kernel launch on the context's
+ * stream — ptr_get_profile then returns, per kernel class k (0 generate, 1 closest-hit,
+ * 2 shade, 3 shadow, 4 film), the summed device time ms_out[k] and the number of
+ * launches launches_out[k]; PTR_PROFILE_WORK runs the traversal kernels' counting
+ * variants, which tally nodes, triangles, TLAS nodes and instances into ptr_counters. */
+#define PTR_PROFILE_TIMING 1
+#define PTR_PROFILE_WORK 2
 int ptr_profile_next(ptr_program* prog, int enable);
 int ptr_get_profile(ptr_program* prog, float* ms_out, int* launches_out, int n);
 

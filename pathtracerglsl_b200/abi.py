@@ -93,8 +93,12 @@ class Frame(C.Structure):
 
 class Counters(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("closest_queries", C.c_uint64), ("shadow_queries", C.c_uint64),
-                ("nodes_visited", C.c_uint64), ("prims_tested", C.c_uint64),
+                ("nodes_visited", C.c_uint64), ("prims_tested", C.c_uint64), ("tlas_nodes", C.c_uint64),
+                ("instances", C.c_uint64), ("shadow_work", C.c_uint64 * 4),
                 ("error_flags", C.c_uint32), ("pad", C.c_uint32)]
+
+
+PROFILE_TIMING, PROFILE_WORK = 1, 2
 
 
 # Sizes the header documents (checked by the CPU tests).

@@ -25,6 +25,10 @@ constexpr unsigned kErrCwGuard = 4u;         // a wide walk hit its iteration gu
 
 struct HitRec { float t, u, v; int region, element, prim; };
 
+// Per-thread work tally (instrumented pass only): the timed kernels pass a null tally,
+// which the inlined walks fold away.
+struct Work { unsigned nodes, tris, tlas, inst; };
+
 __device__ __forceinline__ void flag_error(const DevScene& S, unsigned bit) {
     if (S.err_flags) atomicOr(S.err_flags, bit);
 }
@@ -71,7 +75,8 @@ __device__ __forceinline__ bool aabb_hit(float4 n0, float4 n1, f3 ro, f3 inv, fl
 // Leaf(off, cnt) -> for nearest walks updates the caller's tmax itself; returns true to
 // stop the walk (any-hit found).
 template <class Leaf>
-__device__ __forceinline__ bool walk_binary(const DevScene& S, const float4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf) {
+__device__ __forceinline__ bool walk_binary(const DevScene& S, const float4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf,
+                                            unsigned* visits = nullptr) {
     f3 inv(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
     int stack[kBvhStack];
     int ptr = 0;
@@ -79,6 +84,7 @@ __device__ __forceinline__ bool walk_binary(const DevScene& S, const float4* nod
     while (ptr >= 0) {
         int ni = stack[ptr];
         ptr--;
+        if (visits) (*visits)++;
         float4 n0 = __ldg(nodes + 2 * ni), n1 = __ldg(nodes + 2 * ni + 1);
         if (!aabb_hit(n0, n1, ro, inv, tmax)) continue;
         if (n0.w >= 0.0f) {
@@ -104,7 +110,8 @@ __device__ __forceinline__ float clamp_dir(float d) { return fabsf(d) < 1e-20f ?
 
 // Leaf(item) for one leaf item index (wide-order); returns true to stop.
 template <class Leaf>
-__device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf) {
+__device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf,
+                                          unsigned* visits = nullptr) {
     f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
     unsigned octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
     f3 inv(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
@@ -129,6 +136,7 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
             else flag_error(S, kErrCwStack);
         }
         const uint4* nd = nodes + 5 * (size_t)child;
+        if (visits) (*visits)++;
         uint4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
         f3 p(__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z));
         f3 dq = f3(__uint_as_float((n0.w & 0xFFu) << 23), __uint_as_float(((n0.w >> 8) & 0xFFu) << 23),
@@ -169,60 +177,66 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
 }
 
 // ---- one mesh BLAS in a given frame (ro/rd already in the mesh's local frame) --------------
-__device__ __forceinline__ bool mesh_nearest(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float& tmax, int& prim) {
+__device__ __forceinline__ bool mesh_nearest(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float& tmax, int& prim,
+                                             Work* w = nullptr) {
     bool found = false;
     if (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) {
         const float4* tri = m.tri_w;
         walk_wide(S, m.cwbvh, ro, rd, tmax, [&](int i) {
             f3 a, e1, e2;
+            if (w) w->tris++;
             load_tri(tri, i, a, e1, e2);
             float t;
             if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
             return false;
-        });
+        }, w ? &w->nodes : nullptr);
     } else {
         const float4* tri = m.tri;
         walk_binary(S, m.bvh, ro, rd, tmax, [&](int off, int cnt) {
             for (int i = off; i < off + cnt; ++i) {
                 f3 a, e1, e2;
+                if (w) w->tris++;
                 load_tri(tri, i, a, e1, e2);
                 float t;
                 if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
             }
             return false;
-        });
+        }, w ? &w->nodes : nullptr);
     }
     return found;
 }
-__device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float max_dist) {
+__device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float max_dist, Work* w = nullptr) {
     if (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) {
         const float4* tri = m.tri_w;
         return walk_wide(S, m.cwbvh, ro, rd, max_dist, [&](int i) {
             f3 a, e1, e2;
+            if (w) w->tris++;
             load_tri(tri, i, a, e1, e2);
             float t;
             return tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < max_dist;
-        });
+        }, w ? &w->nodes : nullptr);
     }
     const float4* tri = m.tri;
     return walk_binary(S, m.bvh, ro, rd, max_dist, [&](int off, int cnt) {
         for (int i = off; i < off + cnt; ++i) {
             f3 a, e1, e2;
+            if (w) w->tris++;
             load_tri(tri, i, a, e1, e2);
             float t;
             if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < max_dist) return true;
         }
         return false;
-    });
+    }, w ? &w->nodes : nullptr);
 }
 
 // ---- region arms ------------------------------------------------------------------------
-__device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_region& g, int region, const Ray& r, HitRec& h) {
+__device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_region& g, int region, const Ray& r, HitRec& h,
+                                              Work* w = nullptr) {
     if (g.shape == PTR_SHAPE_MESH) {
         const DevMesh& m = S.meshes[g.ref];
         int prim = -1;
         float t = h.t;
-        if (mesh_nearest(S, m, r.o, r.d, t, prim)) {
+        if (mesh_nearest(S, m, r.o, r.d, t, prim, w)) {
             h.t = t;
             h.region = region;
             h.element = 0;
@@ -243,21 +257,23 @@ __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_regio
             } else {
                 float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
                 float s = ts.w;
+                if (w) w->inst++;
                 f3 ro = placement_rigid(q, ts, r.o) / s;
                 f3 rd = qrot(q, r.d) / s;
                 int prim = -1;
                 float t = t_near;
-                if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim)) {
+                if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim, w)) {
                     t_near = t; h.t = t; h.region = region; h.element = i; h.prim = prim;
                 }
             }
         }
         return false;
-    });
+    }, w ? &w->tlas : nullptr);
 }
 
-__device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g, const Ray& r, float max_dist) {
-    if (g.shape == PTR_SHAPE_MESH) return mesh_any(S, S.meshes[g.ref], r.o, r.d, max_dist);
+__device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g, const Ray& r, float max_dist,
+                                          Work* w = nullptr) {
+    if (g.shape == PTR_SHAPE_MESH) return mesh_any(S, S.meshes[g.ref], r.o, r.d, max_dist, w);
     const DevBatch& b = S.batches[g.ref];
     return walk_binary(S, b.tlas, r.o, r.d, max_dist, [&](int off, int cnt) {
         for (int i = off; i < off + cnt; ++i) {
@@ -268,13 +284,14 @@ __device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g
             } else {
                 float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
                 float s = ts.w;
+                if (w) w->inst++;
                 f3 ro = placement_rigid(q, ts, r.o) / s;
                 f3 rd = qrot(q, r.d) / s;
-                if (mesh_any(S, S.meshes[b.proto_mesh], ro, rd, max_dist)) return true;
+                if (mesh_any(S, S.meshes[b.proto_mesh], ro, rd, max_dist, w)) return true;
             }
         }
         return false;
-    });
+    }, w ? &w->tlas : nullptr);
 }
 
 // Containment of an instanced SPHERE batch (the TLAS point descent of scene_region_at):

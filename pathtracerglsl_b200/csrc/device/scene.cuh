@@ -39,6 +39,8 @@ struct DevScene {
     const DevMesh* meshes;
     const DevBatch* batches;
     unsigned* err_flags;      // device guard flags (stack overflow, iteration guard)
+    unsigned long long* work; // instrumented pass only: [0] BLAS nodes, [1] triangles,
+                              // [2] TLAS nodes, [3] instances entered (NULL = not counted)
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
     // environment

@@ -84,7 +84,7 @@ __device__ __forceinline__ int warp_append(unsigned* counter, bool pred) {
 // ---- scene queries -------------------------------------------------------------------
 // Nearest hit over every arm; returns region (or -1), element, primitive and t.
 
-__device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r) {
+__device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r, Work* w = nullptr) {
     HitRec h;
     h.t = kMaxDist;
     h.u = h.v = 0.f;
@@ -94,7 +94,7 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r)
     for (int i = 0; i < S.n_regions; ++i) {
         const ptr_region& g = S.regions[i];
         if (g.shape >= PTR_SHAPE_MESH) {
-            accel_closest(S, g, i, r, h);
+            accel_closest(S, g, i, r, h, w);
             continue;
         }
         float t;
@@ -108,11 +108,11 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r)
     return h;
 }
 
-__device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float max_dist) {
+__device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float max_dist, Work* w = nullptr) {
     for (int i = 0; i < S.n_regions; ++i) {
         const ptr_region& g = S.regions[i];
         if (g.shape >= PTR_SHAPE_MESH) {
-            if (accel_any(S, g, r, max_dist)) return true;
+            if (accel_any(S, g, r, max_dist, w)) return true;
             continue;
         }
         float t;
@@ -236,8 +236,24 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp) {
     }
 }
 
+#ifndef PTR_TRACE_MIN_BLOCKS
+#define PTR_TRACE_MIN_BLOCKS 4
+#endif
+
+// Fold a thread's tally into S.work (one atomic per warp and counter).
+__device__ __forceinline__ void flush_work(const DevScene& S, const Work& w) {
+    unsigned v[4] = {w.nodes, w.tris, w.tlas, w.inst};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        unsigned x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(&S.work[k], (unsigned long long)x);
+    }
+}
+
 // Nearest hit of every live path.
-__global__ void k_closest(DevScene S, PathPool pool, int in) {
+template <bool COUNT>
+__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S, PathPool pool, int in) {
     unsigned n = pool.cnt[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         pool.cnt[in ^ 1] = 0u;
@@ -245,15 +261,17 @@ __global__ void k_closest(DevScene S, PathPool pool, int in) {
         pool.stats[0] += n;
     }
     const int* q = pool.q[in];
+    Work w{0u, 0u, 0u, 0u};
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int i = q[k];
         Ray r;
         r.o = xyz(pool.ray_o[i]);
         r.d = xyz(pool.ray_d[i]);
-        HitRec h = scene_closest(S, r);
+        HitRec h = scene_closest(S, r, COUNT ? &w : nullptr);
         pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
         pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
     }
+    if (COUNT) flush_work(S, w);
 }
 
 // One walk iteration for every live path.
@@ -490,10 +508,11 @@ __global__ void k_shade(DevScene S, PathPool pool, ProgParams P, int in) {
 // Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
 // segment walker (shadow/media/media.glsl:29-62); the surviving fraction scales the
 // stored contribution prefix into the path's radiance.
-template <bool MEDIA>
-__global__ void k_shadow(DevScene S, PathPool pool, ProgParams P) {
+template <bool MEDIA, bool COUNT>
+__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S, PathPool pool, ProgParams P) {
     const unsigned n = pool.cnt[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
+    Work wk{0u, 0u, 0u, 0u};
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int i = pool.shq[k];
         float4 so = pool.sh_o[i], sd = pool.sh_d[i], lp = pool.sh_lp[i], c = pool.sh_c[i];
@@ -502,7 +521,7 @@ __global__ void k_shadow(DevScene S, PathPool pool, ProgParams P) {
         sr.d = xyz(sd);
         f3 vis;
         if (!MEDIA) {
-            vis = scene_any(S, sr, so.w) ? f3(0.0f) : f3(1.0f);
+            vis = scene_any(S, sr, so.w, COUNT ? &wk : nullptr) ? f3(0.0f) : f3(1.0f);
         } else {
             f3 light_p = xyz(lp);
             int crossings_left = __float_as_int(sd.w);
@@ -513,7 +532,7 @@ __global__ void k_shadow(DevScene S, PathPool pool, ProgParams P) {
             for (int crossed = 0; crossed <= crossings_left; crossed++) {
                 float remaining = length(light_p - seg.o) - kShadowBackoff;
                 if (remaining <= 0.0f) { finished = true; break; }
-                HitRec hr = scene_closest(S, seg);
+                HitRec hr = scene_closest(S, seg, COUNT ? &wk : nullptr);
                 bool hit_boundary = hr.region >= 0 && hr.t < remaining;
                 float seg_len = hit_boundary ? hr.t : remaining;
                 int med_mat = material_of(S, medium);
@@ -536,6 +555,7 @@ __global__ void k_shadow(DevScene S, PathPool pool, ProgParams P) {
             pool.rad[i] = make_float4(rr.x + add.x, rr.y + add.y, rr.z + add.z, 0.f);
         }
     }
+    if (COUNT) flush_work(S, wk);
 }
 
 // Fold the wave's per-path radiance into the film, per pixel in sample order; then

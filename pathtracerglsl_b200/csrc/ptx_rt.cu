@@ -58,6 +58,9 @@ struct ptr_program {
     float* graph_samples = nullptr;
     // counters / profiling
     ptr_counters last{};
+    unsigned long long* work_dev = nullptr;   // counting-pass tallies (4 x u64)
+    const ptr_scene* last_scene = nullptr;
+    int work_valid = 0;
     int profile_next = 0;
     float prof_ms[5] = {0, 0, 0, 0, 0};
     int prof_launches[5] = {0, 0, 0, 0, 0};
@@ -147,6 +150,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
                  std::vector<ProfRec>* prof = nullptr) {
     DevScene Sp = s->dev;
     Sp.accel = p->desc.accel;
+    Sp.work = (p->profile_next & PTR_PROFILE_WORK) ? p->work_dev : nullptr;
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
         ProfRec r{cls, nullptr, nullptr};
@@ -173,7 +177,8 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
         r = mark(1);
-        k_closest<<<grid, block, 0, st>>>(S, pool, in);
+        if (S.work) k_closest<true><<<grid, block, 0, st>>>(S, pool, in);
+        else k_closest<false><<<grid, block, 0, st>>>(S, pool, in);
         done(r);
         const bool media = s->has_media != 0;
         r = mark(2);
@@ -188,8 +193,15 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
             r = mark(3);
-            if (media) k_shadow<true><<<grid, block, 0, st>>>(S, pool, P);
-            else k_shadow<false><<<grid, block, 0, st>>>(S, pool, P);
+            if (S.work) {
+                DevScene Sq = S;
+                Sq.work = S.work + 4;   // the shadow queries' own tallies
+                if (media) k_shadow<true, true><<<grid, block, 0, st>>>(Sq, pool, P);
+                else k_shadow<false, true><<<grid, block, 0, st>>>(Sq, pool, P);
+            } else {
+                if (media) k_shadow<true, false><<<grid, block, 0, st>>>(S, pool, P);
+                else k_shadow<false, false><<<grid, block, 0, st>>>(S, pool, P);
+            }
             done(r);
         }
     }
@@ -410,8 +422,17 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     const int iters = wave_iterations(p, s);
     const long long waves = (total + cap - 1) / cap;
     const int n_sm = device_sms(ctx->device);
-    const bool profiling = p->profile_next != 0;
-    const bool use_graph = std::getenv("PTR_NO_GRAPH") == nullptr && !profiling;
+    const bool profiling = (p->profile_next & PTR_PROFILE_TIMING) != 0;
+    const bool counting = (p->profile_next & PTR_PROFILE_WORK) != 0;
+    p->last_scene = s;
+    if (counting) {
+        if (!p->work_dev) CK(ctx, cudaMalloc(&p->work_dev, 64));
+        CK(ctx, cudaMemsetAsync(p->work_dev, 0, 64, st));
+        p->work_valid = 1;
+    } else {
+        p->work_valid = 0;
+    }
+    const bool use_graph = std::getenv("PTR_NO_GRAPH") == nullptr && !profiling && !counting;
     if (use_graph) {
         if (!p->graph || p->graph_scene != s || p->graph_w != f->width || p->graph_h != f->height ||
             p->graph_iters != iters || p->graph_samples != samples_dev) {
@@ -450,6 +471,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     } else {
         for (long long w = 0; w < waves; ++w) launch_wave(p, s, st, iters, samples_dev, n_sm);
         CK(ctx, cudaGetLastError());
+        p->profile_next = 0;
     }
     p->nsamples += (double)f->spp;
     return PTR_OK;
@@ -601,6 +623,7 @@ int ptr_free_program(ptr_program* p) {
     if (p->sumsq) cudaFree(p->sumsq);
     if (p->export_buf) cudaFree(p->export_buf);
     if (p->fp_dev) cudaFree(p->fp_dev);
+    if (p->work_dev) cudaFree(p->work_dev);
     delete p;
     return PTR_OK;
 }
@@ -734,6 +757,20 @@ int ptr_get_counters(ptr_program* p, ptr_counters* out) {
     out->shadow_queries = st[1];
     out->paths = st[2];
     out->error_flags = cnt[3];
+    if (p->last_scene && p->last_scene->dev.err_flags) {
+        unsigned ef = 0;
+        CK(ctx, cudaMemcpy(&ef, p->last_scene->dev.err_flags, 4, cudaMemcpyDeviceToHost));
+        out->error_flags |= ef;
+    }
+    if (p->work_valid && p->work_dev) {
+        unsigned long long wk[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        CK(ctx, cudaMemcpy(wk, p->work_dev, sizeof(wk), cudaMemcpyDeviceToHost));
+        out->nodes_visited = wk[0];
+        out->prims_tested = wk[1];
+        out->tlas_nodes = wk[2];
+        out->instances = wk[3];
+        for (int k = 0; k < 4; ++k) out->shadow_work[k] = wk[4 + k];
+    }
     return PTR_OK;
 }
 

@@ -153,10 +153,11 @@ class CudaEngine:
 
     KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film")
 
-    def profile_render(self, width, height, spp):
-        """Render once with CUDA events around every launch; per kernel class returns
-        (summed device ms, launch count)."""
-        self._check(self.lib.ptr_profile_next(self.programs[self.current], 1))
+    def profile_render(self, width, height, spp, mode=abi.PROFILE_TIMING):
+        """Render once instrumented: PROFILE_TIMING (CUDA events around every launch; per
+        kernel class returns (summed device ms, launch count)) and/or PROFILE_WORK (the
+        traversal tallies, read with counters())."""
+        self._check(self.lib.ptr_profile_next(self.programs[self.current], mode))
         self.render_frame(width, height, spp, sync=True)
         ms = (C.c_float * 5)()
         n = (C.c_int * 5)()
@@ -167,6 +168,9 @@ class CudaEngine:
         c = abi.Counters()
         self._check(self.lib.ptr_get_counters(self.programs[self.current], C.byref(c)))
         return {"paths": c.paths, "closest_queries": c.closest_queries, "shadow_queries": c.shadow_queries,
+                "blas_nodes": c.nodes_visited, "triangles": c.prims_tested, "tlas_nodes": c.tlas_nodes,
+                "instances": c.instances, "shadow_blas_nodes": c.shadow_work[0], "shadow_triangles": c.shadow_work[1],
+                "shadow_tlas_nodes": c.shadow_work[2], "shadow_instances": c.shadow_work[3],
                 "error_flags": c.error_flags}
 
     def close(self):
