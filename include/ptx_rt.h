@@ -226,6 +226,26 @@ int ptr_free_program(ptr_program* prog);
  * (Engine.renderFrame, Engine.ts:190-204; one call may fold many frames). */
 int ptr_render(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame);
 
+/* Batched rendering: many scenes x programs x frames of uneven size in ONE wavefront —
+ * the jobs' paths share one path pool and every wave is one CUDA graph of the
+ * generate / closest / shade / shadow / film kernels over the concatenated job space,
+ * with per-job scene, program and frame tables (paths of shallow jobs retire early;
+ * compaction keeps the queues dense).  Each job accumulates into its own program's film
+ * (read it with ptr_read_export).  All jobs must share directLighting.  Synchronises.
+ * No counterpart in the reference (one fragment draw per renderer and frame). */
+typedef struct ptr_batch_job {
+    ptr_program* prog;
+    ptr_scene* scene;
+    ptr_frame frame;
+} ptr_batch_job;
+int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs);
+/* Counters of the last batched render (paths, closest and shadow queries). */
+int ptr_get_batch_counters(ptr_ctx* ctx, ptr_counters* out);
+/* Instrument the next ptr_render_batch (PTR_PROFILE_TIMING: CUDA events around every
+ * launch, no graph) and read the per-kernel-class times like ptr_get_profile. */
+int ptr_profile_batch_next(ptr_ctx* ctx, int mode);
+int ptr_get_batch_profile(ptr_ctx* ctx, float* ms_out, int* launches_out, int n);
+
 /* Test hook: render like ptr_render (film included) and also copy every sample's radiance
  * to host_out, laid out [sample][row][column][rgb] (n >= width*height*spp*3 floats).
  * The per-sample values are what the reference's accumulation folds in (accumulation.ts:14-51). */

@@ -31,6 +31,10 @@ SIGNATURES = {
                                   C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "ptr_render_noalloc": (C.c_int, [C.POINTER(abi.SceneDesc), C.POINTER(abi.ProgramDesc), C.POINTER(abi.Frame),
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ptr_render_batch": (C.c_int, [C.c_void_p, C.POINTER(abi.BatchJob), C.c_int]),
+    "ptr_get_batch_counters": (C.c_int, [C.c_void_p, C.POINTER(abi.Counters)]),
+    "ptr_profile_batch_next": (C.c_int, [C.c_void_p, C.c_int]),
+    "ptr_get_batch_profile": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int), C.c_int]),
     "ptr_sync": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_read_export": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_float), C.c_size_t]),
     "ptr_read_export_device": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),

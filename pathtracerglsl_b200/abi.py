@@ -91,6 +91,10 @@ class Frame(C.Structure):
                 ("accumulate", C.c_int32), ("camera", Camera)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("prog", C.c_void_p), ("scene", C.c_void_p), ("frame", Frame)]
+
+
 class Counters(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("closest_queries", C.c_uint64), ("shadow_queries", C.c_uint64),
                 ("nodes_visited", C.c_uint64), ("prims_tested", C.c_uint64), ("tlas_nodes", C.c_uint64),

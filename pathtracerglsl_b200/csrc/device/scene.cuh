@@ -41,6 +41,12 @@ struct DevScene {
     unsigned* err_flags;      // device guard flags (stack overflow, iteration guard)
     unsigned long long* work; // instrumented pass only: [0] BLAS nodes, [1] triangles,
                               // [2] TLAS nodes, [3] instances entered (NULL = not counted)
+    // Region BVH over the bounded analytic regions (sphere, box, quad): the scene table
+    // walk of the reference's 'table' object dispatch.  NULL = scan every region in order.
+    const float4* region_bvh;     // 2 float4 per node, leaf items index region_items
+    const int* region_items;      // leaf order -> region index
+    const int* linear_regions;    // regions outside the BVH (planes, meshes, batches), in order
+    int n_linear, n_region_nodes, pad_r0, pad_r1;
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
     // environment

@@ -44,6 +44,7 @@ struct PathPool {
     unsigned int* cnt; // [0],[1] queue counts, [2] shadow count, [3] error flags
     unsigned long long* stats; // [0] closest queries, [1] shadow queries, [2] paths
     long long* wave;   // [0] first global path index of the wave, [1] wave size
+    int* job;          // batched renders: the job (scene x program x frame) of each path
 };
 
 struct FrameParams {
@@ -59,6 +60,23 @@ struct ProgParams {
     int max_bounces, direct, rr_start, max_null;
     float rr_max_survival;
     int scattering;
+};
+
+// Batched renders: per job its scene, program knobs, frame and film; offsets[j] is the
+// first global path index of job j (offsets[n_jobs] = total paths).
+struct BatchJob {
+    FrameParams frame;
+    double* sum;
+    double* sumsq;
+};
+struct BatchTables {
+    const DevScene* scenes;
+    const ProgParams* progs;
+    const BatchJob* jobs;
+    const long long* offsets;
+    int n_jobs;
+    long long total;
+    int capacity;
 };
 
 constexpr unsigned kErrStack = 1u;
@@ -91,7 +109,10 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
     h.region = -1;
     h.element = 0;
     h.prim = -1;
-    for (int i = 0; i < S.n_regions; ++i) {
+    const bool tabled = S.region_bvh != nullptr;
+    const int n = tabled ? S.n_linear : S.n_regions;
+    for (int k = 0; k < n; ++k) {
+        const int i = tabled ? S.linear_regions[k] : k;
         const ptr_region& g = S.regions[i];
         if (g.shape >= PTR_SHAPE_MESH) {
             accel_closest(S, g, i, r, h, w);
@@ -105,11 +126,33 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
             h.prim = -1;
         }
     }
+    if (tabled) {
+        float tb = h.t;
+        walk_binary(S, S.region_bvh, r.o, r.d, tb, [&](int off, int cnt) {
+            for (int j = off; j < off + cnt; ++j) {
+                const int i = S.region_items[j];
+                float t;
+                // strict '<', and on an exact tie the lower region index (the order of the
+                // unrolled arms) keeps the hit
+                if (analytic_root(S.regions[i], r, t) && (t < tb || (t == tb && h.region > i))) {
+                    tb = t;
+                    h.t = t;
+                    h.region = i;
+                    h.element = 0;
+                    h.prim = -1;
+                }
+            }
+            return false;
+        });
+    }
     return h;
 }
 
 __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float max_dist, Work* w = nullptr) {
-    for (int i = 0; i < S.n_regions; ++i) {
+    const bool tabled = S.region_bvh != nullptr;
+    const int n = tabled ? S.n_linear : S.n_regions;
+    for (int k = 0; k < n; ++k) {
+        const int i = tabled ? S.linear_regions[k] : k;
         const ptr_region& g = S.regions[i];
         if (g.shape >= PTR_SHAPE_MESH) {
             if (accel_any(S, g, r, max_dist, w)) return true;
@@ -118,17 +161,52 @@ __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float
         float t;
         if (analytic_root(g, r, t) && t < max_dist) return true;
     }
+    if (tabled) {
+        return walk_binary(S, S.region_bvh, r.o, r.d, max_dist, [&](int off, int cnt) {
+            for (int j = off; j < off + cnt; ++j) {
+                float t;
+                if (analytic_root(S.regions[S.region_items[j]], r, t) && t < max_dist) return true;
+            }
+            return false;
+        });
+    }
     return false;
 }
 
-// Innermost-wins point classification (features/intersection.ts:1121-1225).
+// Innermost-wins point classification (features/intersection.ts:1121-1225); with a region
+// BVH the bounded solids are found by the containment descent (bvh.ts bvhPointWalkLines).
 __device__ __forceinline__ int scene_region_at(const DevScene& S, f3 p) {
     int region = -1;
     float best = -1.0e20f;
-    for (int i = 0; i < S.n_regions; ++i) {
+    const bool tabled = S.region_bvh != nullptr;
+    const int n = tabled ? S.n_linear : S.n_regions;
+    for (int k = 0; k < n; ++k) {
+        const int i = tabled ? S.linear_regions[k] : k;
         const ptr_region& g = S.regions[i];
         float d = g.shape == PTR_SHAPE_INSTANCES ? accel_region_sdf(S, g, p) : analytic_sdf(g, p);
-        if (d < 0.0f && d > best) { best = d; region = i; }
+        if (d < 0.0f && (d > best || (d == best && i < region))) { best = d; region = i; }
+    }
+    if (tabled) {
+        int stack[kBvhStack];
+        int ptr = 0;
+        stack[0] = 0;
+        while (ptr >= 0) {
+            int ni = stack[ptr];
+            ptr--;
+            float4 n0 = __ldg(S.region_bvh + 2 * ni), n1 = __ldg(S.region_bvh + 2 * ni + 1);
+            if (!(p.x >= n0.x && p.y >= n0.y && p.z >= n0.z && p.x <= n1.x && p.y <= n1.y && p.z <= n1.z)) continue;
+            if (n0.w >= 0.0f) {
+                for (int j = (int)n1.w; j < (int)n1.w + (int)n0.w; ++j) {
+                    const int i = S.region_items[j];
+                    float d = analytic_sdf(S.regions[i], p);
+                    if (d < 0.0f && (d > best || (d == best && i < region))) { best = d; region = i; }
+                }
+            } else {
+                int L = ni + 1, R = (int)n1.w;
+                if (ptr + 2 < kBvhStack) { stack[++ptr] = L; stack[++ptr] = R; }
+                else flag_error(S, kErrBvhStack);
+            }
+        }
     }
     return region;
 }
@@ -252,8 +330,8 @@ __device__ __forceinline__ void flush_work(const DevScene& S, const Work& w) {
 }
 
 // Nearest hit of every live path.
-template <bool COUNT>
-__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S, PathPool pool, int in) {
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S0, PathPool pool, int in, BatchTables bt) {
     unsigned n = pool.cnt[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         pool.cnt[in ^ 1] = 0u;
@@ -264,6 +342,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     Work w{0u, 0u, 0u, 0u};
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int i = q[k];
+        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         Ray r;
         r.o = xyz(pool.ray_o[i]);
         r.d = xyz(pool.ray_d[i]);
@@ -271,12 +350,12 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
         pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
     }
-    if (COUNT) flush_work(S, w);
+    if (COUNT) flush_work(S0, w);
 }
 
 // One walk iteration for every live path.
-template <int DIRECT, bool MEDIA>
-__global__ void k_shade(DevScene S, PathPool pool, ProgParams P, int in) {
+template <int DIRECT, bool MEDIA, bool BATCH>
+__global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt) {
     const unsigned n = pool.cnt[in];
     const int* q = pool.q[in];
     int* qout = pool.q[in ^ 1];
@@ -289,6 +368,8 @@ __global__ void k_shade(DevScene S, PathPool pool, ProgParams P, int in) {
         int i = -1;
         if (k < n) {
             i = q[k];
+            const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
+            const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
             float4 ro = pool.ray_o[i], rd = pool.ray_d[i];
             Ray r;
             r.o = xyz(ro);
@@ -508,13 +589,15 @@ __global__ void k_shade(DevScene S, PathPool pool, ProgParams P, int in) {
 // Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
 // segment walker (shadow/media/media.glsl:29-62); the surviving fraction scales the
 // stored contribution prefix into the path's radiance.
-template <bool MEDIA, bool COUNT>
-__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S, PathPool pool, ProgParams P) {
+template <bool MEDIA, bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt) {
     const unsigned n = pool.cnt[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
     Work wk{0u, 0u, 0u, 0u};
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         int i = pool.shq[k];
+        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
+        const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
         float4 so = pool.sh_o[i], sd = pool.sh_d[i], lp = pool.sh_lp[i], c = pool.sh_c[i];
         Ray sr;
         sr.o = xyz(so);
@@ -555,7 +638,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
             pool.rad[i] = make_float4(rr.x + add.x, rr.y + add.y, rr.z + add.z, 0.f);
         }
     }
-    if (COUNT) flush_work(S, wk);
+    if (COUNT) flush_work(S0, wk);
 }
 
 // Fold the wave's per-path radiance into the film, per pixel in sample order; then
@@ -581,6 +664,86 @@ __global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double
         }
         sum[3 * pix + 0] = s0; sum[3 * pix + 1] = s1; sum[3 * pix + 2] = s2;
         sumsq[3 * pix + 0] = q0; sumsq[3 * pix + 1] = q1; sumsq[3 * pix + 2] = q2;
+    }
+}
+
+// ---- batched renders ------------------------------------------------------------------
+__device__ __forceinline__ int job_of(const BatchTables& bt, long long g) {
+    int lo = 0, hi = bt.n_jobs - 1;   // last j with offsets[j] <= g
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (bt.offsets[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Camera rays for one wave of the concatenated job space.
+__global__ void k_generate_batch(PathPool pool, BatchTables bt) {
+    long long base = pool.wave[0];
+    long long n = bt.total - base;
+    if (n > bt.capacity) n = bt.capacity;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        pool.cnt[0] = (unsigned)n;
+        pool.wave[1] = n;
+        pool.stats[2] += (unsigned long long)n;
+    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long g = base + i;
+        int j = job_of(bt, g);
+        const FrameParams& F = bt.jobs[j].frame;
+        const DevScene& S = bt.scenes[j];
+        long long local = g - bt.offsets[j];
+        const long long npix = (long long)F.width * F.height;
+        int pix = (int)(local % npix);
+        int sample = (int)(local / npix);
+        int x = pix % F.width, y = pix / F.width;
+        Rng rng;
+        rng.init((uint32_t)(x + F.px_off), (uint32_t)(y + F.py_off), (uint32_t)(F.first_sample + sample), F.salt);
+        float pxf = (float)x + 0.5f + (float)F.px_off;
+        float pyf = (float)y + 0.5f + (float)F.py_off;
+        float a0 = rng.next();
+        float a1 = rng.next();
+        float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+        rng.next();
+        rng.next();
+        float ndcx = (2.0f * fx / (float)F.width) - 1.0f;
+        float ndcy = (2.0f * fy / (float)F.height) - 1.0f;
+        ndcx *= F.cam.aspect;
+        f3 dir = normalize(ld3(F.cam.forward) + ndcx * F.cam.tan_fov * ld3(F.cam.right) +
+                           ndcy * F.cam.tan_fov * ld3(F.cam.up));
+        f3 o = ld3(F.cam.position);
+        int medium = S.has_media ? scene_region_at(S, o) : -1;
+        pool.ray_o[i] = f4(o, 0.0f);
+        pool.ray_d[i] = f4(dir, 1.0f);
+        pool.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        pool.rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        pool.prev_q[i] = f4(o, 0.0f);
+        pool.st[i] = make_int4(0, medium, 0, 1);
+        pool.rng[i] = make_uint2(rng.base, rng.dim);
+        pool.job[i] = j;
+        pool.q[0][i] = (int)i;
+    }
+}
+
+// Fold the wave's radiance into each job's film (FP64 atomics: the order of samples of
+// one pixel within a wave is not fixed, which moves the sum by float64 rounding only).
+__global__ void k_film_batch(PathPool pool, BatchTables bt) {
+    const long long base = pool.wave[0];
+    const long long n = pool.wave[1];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int j = pool.job[i];
+        const BatchJob& J = bt.jobs[j];
+        const long long npix = (long long)J.frame.width * J.frame.height;
+        long long pix = (base + i - bt.offsets[j]) % npix;
+        float4 L = pool.rad[i];
+        double* su = J.sum + 3 * pix;
+        double* sq = J.sumsq + 3 * pix;
+        atomicAdd(su + 0, (double)L.x);
+        atomicAdd(su + 1, (double)L.y);
+        atomicAdd(su + 2, (double)L.z);
+        atomicAdd(sq + 0, (double)L.x * (double)L.x);
+        atomicAdd(sq + 1, (double)L.y * (double)L.y);
+        atomicAdd(sq + 2, (double)L.z * (double)L.z);
     }
 }
 

@@ -23,10 +23,12 @@
 
 using namespace ptx;
 
+struct ptr_program;
 struct ptr_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    ptr_program* batch = nullptr;     // path pool + tables of batched renders
 };
 
 struct ptr_scene {
@@ -126,6 +128,7 @@ int alloc_pool(ptr_program* p, int capacity) {
         (rc = get(c * 16, (void**)&q.sh_d)) || (rc = get(c * 16, (void**)&q.sh_lp)) ||
         (rc = get(c * 16, (void**)&q.sh_c)) || (rc = get(c * 4, (void**)&q.q[0])) ||
         (rc = get(c * 4, (void**)&q.q[1])) || (rc = get(c * 4, (void**)&q.shq)) ||
+        (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
         (rc = get(64, (void**)&q.wave))) {
         free_pool(p);
@@ -172,23 +175,24 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     P.scattering = p->desc.scattering;
     const int grid = launch_grid(n_sm), block = 256;
     ProfRec* r = mark(0);
+    const BatchTables nob{};
     k_generate<<<grid, block, 0, st>>>(S, pool, p->fp_dev);
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
         r = mark(1);
-        if (S.work) k_closest<true><<<grid, block, 0, st>>>(S, pool, in);
-        else k_closest<false><<<grid, block, 0, st>>>(S, pool, in);
+        if (S.work) k_closest<true, false><<<grid, block, 0, st>>>(S, pool, in, nob);
+        else k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
         done(r);
         const bool media = s->has_media != 0;
         r = mark(2);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<PTR_DIRECT_NONE, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
-            case 1: k_shade<PTR_DIRECT_NONE, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
-            case 2: k_shade<PTR_DIRECT_NEE, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
-            case 3: k_shade<PTR_DIRECT_NEE, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
-            case 4: k_shade<PTR_DIRECT_MIS, false><<<grid, block, 0, st>>>(S, pool, P, in); break;
-            default: k_shade<PTR_DIRECT_MIS, true><<<grid, block, 0, st>>>(S, pool, P, in); break;
+            case 0: k_shade<PTR_DIRECT_NONE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 1: k_shade<PTR_DIRECT_NONE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 2: k_shade<PTR_DIRECT_NEE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 3: k_shade<PTR_DIRECT_NEE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 4: k_shade<PTR_DIRECT_MIS, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            default: k_shade<PTR_DIRECT_MIS, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
         }
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
@@ -196,17 +200,64 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
             if (S.work) {
                 DevScene Sq = S;
                 Sq.work = S.work + 4;   // the shadow queries' own tallies
-                if (media) k_shadow<true, true><<<grid, block, 0, st>>>(Sq, pool, P);
-                else k_shadow<false, true><<<grid, block, 0, st>>>(Sq, pool, P);
+                if (media) k_shadow<true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob);
+                else k_shadow<false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob);
             } else {
-                if (media) k_shadow<true, false><<<grid, block, 0, st>>>(S, pool, P);
-                else k_shadow<false, false><<<grid, block, 0, st>>>(S, pool, P);
+                if (media) k_shadow<true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob);
+                else k_shadow<false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob);
             }
             done(r);
         }
     }
     r = mark(4);
     k_film<<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples);
+    k_advance<<<1, 32, 0, st>>>(pool);
+    done(r);
+}
+
+// One wave of a batched render: the same kernel sequence over the concatenated job space;
+// scene, program knobs and frame come from the per-job tables.
+void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTables& bt, int direct, bool media,
+                       cudaStream_t st, int iters, int n_sm, std::vector<ProfRec>* prof = nullptr) {
+    const int grid = launch_grid(n_sm), block = 256;
+    ProgParams P0{};
+    auto mark = [&](int cls) -> ProfRec* {
+        if (!prof) return nullptr;
+        ProfRec r{cls, nullptr, nullptr};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, st);
+        prof->push_back(r);
+        return &prof->back();
+    };
+    auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
+    ProfRec* r = mark(0);
+    k_generate_batch<<<grid, block, 0, st>>>(pool, bt);
+    done(r);
+    for (int it = 0; it < iters; ++it) {
+        int in = it & 1;
+        r = mark(1);
+        k_closest<false, true><<<grid, block, 0, st>>>(S0, pool, in, bt);
+        done(r);
+        r = mark(2);
+        switch (direct * 2 + (media ? 1 : 0)) {
+            case 0: k_shade<PTR_DIRECT_NONE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 1: k_shade<PTR_DIRECT_NONE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 2: k_shade<PTR_DIRECT_NEE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 3: k_shade<PTR_DIRECT_NEE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 4: k_shade<PTR_DIRECT_MIS, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            default: k_shade<PTR_DIRECT_MIS, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+        }
+        done(r);
+        if (direct != PTR_DIRECT_NONE) {
+            r = mark(3);
+            if (media) k_shadow<true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt);
+            else k_shadow<false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt);
+            done(r);
+        }
+    }
+    r = mark(4);
+    k_film_batch<<<grid, block, 0, st>>>(pool, bt);
     k_advance<<<1, 32, 0, st>>>(pool);
     done(r);
 }
@@ -360,6 +411,95 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     return PTR_OK;
 }
 
+// Region BVH over the bounded analytic regions (spheres, boxes, quads) when there are at
+// least PTR_REGION_BVH_MIN of them (default 8): the reference's 'table' object dispatch,
+// one scene TLAS instead of one unrolled arm per object.  Planes, meshes and instanced
+// batches stay in the ordered linear list.
+int upload_region_bvh(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
+    DevScene& S = s->dev;
+    int min_items = 8;
+    if (const char* env = std::getenv("PTR_REGION_BVH_MIN")) min_items = std::atoi(env);
+    std::vector<int> bounded, linear;
+    std::vector<double> boxes;
+    for (int i = 0; i < d->n_regions; ++i) {
+        const ptr_region& g = d->regions[i];
+        const float* q = g.p;
+        double mn[3], mx[3];
+        if (g.shape == PTR_SHAPE_SPHERE) {
+            for (int a = 0; a < 3; ++a) { mn[a] = (double)q[a] - q[3]; mx[a] = (double)q[a] + q[3]; }
+        } else if (g.shape == PTR_SHAPE_BOX) {
+            for (int a = 0; a < 3; ++a) { mn[a] = (double)q[a] - q[3 + a]; mx[a] = (double)q[a] + q[3 + a]; }
+        } else if (g.shape == PTR_SHAPE_QUAD) {
+            for (int a = 0; a < 3; ++a) {
+                double c0 = q[a], c1 = c0 + q[3 + a], c2 = c0 + q[6 + a], c3 = c0 + q[3 + a] + q[6 + a];
+                mn[a] = std::min(std::min(c0, c1), std::min(c2, c3));
+                mx[a] = std::max(std::max(c0, c1), std::max(c2, c3));
+            }
+        } else {
+            linear.push_back(i);
+            continue;
+        }
+        // a float-rounding margin so the (float) node boxes never cut the geometry
+        for (int a = 0; a < 3; ++a) {
+            double m = 1e-6 * (1.0 + std::max(std::fabs(mn[a]), std::fabs(mx[a])));
+            boxes.push_back(mn[a] - m);
+        }
+        for (int a = 0; a < 3; ++a) {
+            double m = 1e-6 * (1.0 + std::max(std::fabs(mn[a]), std::fabs(mx[a])));
+            boxes.push_back(mx[a] + m);
+        }
+        bounded.push_back(i);
+    }
+    if ((int)bounded.size() < min_items) return PTR_OK;
+    // reorder to (min.xyz, max.xyz) per item
+    std::vector<double> b6(boxes.size());
+    for (size_t k = 0; k < bounded.size(); ++k)
+        for (int a = 0; a < 6; ++a) b6[6 * k + a] = boxes[6 * k + a];
+    ptx_host::BinaryBvh bvh = ptx_host::build_bvh(b6.data(), (int)bounded.size(), ptx_host::kBvhLeafSize, false);
+    std::vector<int> items(bounded.size());
+    for (size_t k = 0; k < bounded.size(); ++k) items[k] = bounded[bvh.order[k]];
+    int rc;
+    const float4* nodes = nullptr;
+    const int* it = nullptr;
+    const int* lin = nullptr;
+    if ((rc = dev_copy(ctx, s->allocs, (const float4*)bvh.nodes.data(), 2 * (size_t)bvh.node_count, &nodes))) return rc;
+    if ((rc = dev_copy(ctx, s->allocs, items.data(), items.size(), &it))) return rc;
+    if (!linear.empty() && (rc = dev_copy(ctx, s->allocs, linear.data(), linear.size(), &lin))) return rc;
+    S.region_bvh = nodes;
+    S.region_items = it;
+    S.linear_regions = lin;
+    S.n_linear = (int)linear.size();
+    S.n_region_nodes = bvh.node_count;
+    return PTR_OK;
+}
+
+// Size (and clear unless accumulating) a program's FP64 film for a frame.
+int prepare_film(ptr_program* p, const ptr_frame* f, cudaStream_t st) {
+    ptr_ctx* ctx = p->ctx;
+    const size_t npix = (size_t)f->width * f->height;
+    if (p->fw != f->width || p->fh != f->height || !p->sum) {
+        if (p->sum) cudaFree(p->sum);
+        if (p->sumsq) cudaFree(p->sumsq);
+        if (p->export_buf) cudaFree(p->export_buf);
+        p->sum = p->sumsq = nullptr;
+        p->export_buf = nullptr;
+        if (cudaMalloc(&p->sum, npix * 3 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&p->sumsq, npix * 3 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&p->export_buf, npix * 3 * sizeof(float)) != cudaSuccess)
+            return fail(ctx, PTR_E_NOMEM, "film allocation failed");
+        p->fw = f->width;
+        p->fh = f->height;
+        p->nsamples = 0.0;
+        CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
+        CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
+    } else if (!f->accumulate) {
+        p->nsamples = 0.0;
+        CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
+        CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
+    }
+    return PTR_OK;
+}
+
 int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples_dev) {
     ptr_ctx* ctx = p->ctx;
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return fail(ctx, PTR_E_INVALID, "frame: width, height and spp must be positive");
@@ -503,6 +643,7 @@ int ptr_destroy(ptr_ctx* ctx) {
     if (!ctx) return PTR_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->batch) ptr_free_program(ctx->batch);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PTR_OK;
@@ -578,6 +719,7 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         S.env_cond = m;
     }
     rc = upload_accels(ctx, s, d);
+    if (!rc) rc = upload_region_bvh(ctx, s, d);
     if (rc) {
         ptr_free_scene(s);
         return rc;
@@ -631,6 +773,167 @@ int ptr_free_program(ptr_program* p) {
 int ptr_render(ptr_program* p, ptr_scene* s, const ptr_frame* f) {
     if (!p || !s || !f) return PTR_E_INVALID;
     return render_impl(p, s, f, nullptr);
+}
+
+int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
+    if (!ctx || !jobs || n_jobs <= 0) return fail(ctx, PTR_E_INVALID, "ptr_render_batch: no jobs");
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int direct = jobs[0].prog ? jobs[0].prog->desc.direct : -1;
+    bool media = false;
+    for (int j = 0; j < n_jobs; ++j) {
+        const ptr_batch_job& J = jobs[j];
+        if (!J.prog || !J.scene || J.prog->ctx != ctx || J.scene->ctx != ctx)
+            return fail(ctx, PTR_E_INVALID, "ptr_render_batch: job " + std::to_string(j) + " has a null or foreign program/scene");
+        if (J.prog->desc.direct != direct)
+            return fail(ctx, PTR_E_INVALID, "ptr_render_batch: every job must use the same directLighting");
+        if (J.frame.width <= 0 || J.frame.height <= 0 || J.frame.spp <= 0)
+            return fail(ctx, PTR_E_INVALID, "ptr_render_batch: job " + std::to_string(j) + " has an empty frame");
+        if (J.scene->has_media) media = true;
+        for (int k = 0; k < j; ++k)
+            if (jobs[k].prog == J.prog)
+                return fail(ctx, PTR_E_INVALID, "ptr_render_batch: jobs " + std::to_string(k) + " and " + std::to_string(j) + " share a program (one film per job)");
+    }
+    std::vector<DevScene> scenes(n_jobs);
+    std::vector<ProgParams> progs(n_jobs);
+    std::vector<BatchJob> bjobs(n_jobs);
+    std::vector<long long> offsets(n_jobs + 1, 0);
+    int iters = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        const ptr_batch_job& J = jobs[j];
+        ptr_program* p = J.prog;
+        int rc = prepare_film(p, &J.frame, st);
+        if (rc) return rc;
+        scenes[j] = J.scene->dev;
+        scenes[j].accel = p->desc.accel;
+        scenes[j].work = nullptr;
+        ProgParams& P = progs[j];
+        P.max_bounces = p->desc.max_bounces;
+        P.direct = p->desc.direct;
+        P.rr_start = p->desc.rr_start;
+        P.max_null = p->desc.max_null_crossings;
+        P.rr_max_survival = p->desc.rr_max_survival;
+        P.scattering = p->desc.scattering;
+        const long long total_j = (long long)J.frame.width * J.frame.height * J.frame.spp;
+        FrameParams& F = bjobs[j].frame;
+        F.width = J.frame.width;
+        F.height = J.frame.height;
+        F.spp = J.frame.spp;
+        F.first_sample = J.frame.first_sample;
+        F.salt = J.frame.reset_salt;
+        F.px_off = J.frame.pixel_offset[0];
+        F.py_off = J.frame.pixel_offset[1];
+        F.total = total_j;
+        F.capacity = 0;
+        F.cam = J.frame.camera;
+        bjobs[j].sum = p->sum;
+        bjobs[j].sumsq = p->sumsq;
+        offsets[j + 1] = offsets[j] + total_j;
+        iters = std::max(iters, p->desc.max_bounces + 1 + (J.scene->has_media ? p->desc.max_null_crossings : 0));
+    }
+    const long long total = offsets[n_jobs];
+    if (!ctx->batch) {
+        ctx->batch = new ptr_program();
+        ctx->batch->ctx = ctx;
+    }
+    ptr_program* bp = ctx->batch;
+    long long cap_max = 1ll << 21;
+    if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
+    long long cap = std::min(total, cap_max);
+    if (bp->capacity < cap) {
+        int rc = alloc_pool(bp, (int)cap);
+        if (rc) return rc;
+    }
+    // device tables (a few KB; refreshed every call)
+    DevScene* d_scenes = nullptr;
+    ProgParams* d_progs = nullptr;
+    BatchJob* d_jobs = nullptr;
+    long long* d_off = nullptr;
+    if (cudaMalloc(&d_scenes, sizeof(DevScene) * n_jobs) != cudaSuccess || cudaMalloc(&d_progs, sizeof(ProgParams) * n_jobs) != cudaSuccess ||
+        cudaMalloc(&d_jobs, sizeof(BatchJob) * n_jobs) != cudaSuccess || cudaMalloc(&d_off, sizeof(long long) * (n_jobs + 1)) != cudaSuccess) {
+        cudaFree(d_scenes); cudaFree(d_progs); cudaFree(d_jobs); cudaFree(d_off);
+        return fail(ctx, PTR_E_NOMEM, "ptr_render_batch: tables");
+    }
+    int rc = PTR_OK;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    BatchTables bt{};
+    bt.scenes = d_scenes;
+    bt.progs = d_progs;
+    bt.jobs = d_jobs;
+    bt.offsets = d_off;
+    bt.n_jobs = n_jobs;
+    bt.total = total;
+    bt.capacity = (int)cap;
+    const long long waves = (total + cap - 1) / cap;
+    const int n_sm = device_sms(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(d_scenes, scenes.data(), sizeof(DevScene) * n_jobs, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_progs, progs.data(), sizeof(ProgParams) * n_jobs, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_jobs, bjobs.data(), sizeof(BatchJob) * n_jobs, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_off, offsets.data(), sizeof(long long) * (n_jobs + 1), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bp->pool.wave, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bp->pool.stats, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bp->pool.cnt, 0, 64, st);
+    const bool profiling = (bp->profile_next & PTR_PROFILE_TIMING) != 0;
+    bp->profile_next = 0;
+    if (profiling) {
+        // instrumented: plain launches with events around each (no graph)
+        std::vector<ProfRec> prof;
+        prof.reserve((size_t)waves * (iters * 3 + 2));
+        for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, st, iters, n_sm, &prof);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        for (int k = 0; k < 5; ++k) { bp->prof_ms[k] = 0.0f; bp->prof_launches[k] = 0; }
+        for (ProfRec& pr : prof) {
+            float ms = 0.0f;
+            if (e == cudaSuccess) cudaEventElapsedTime(&ms, pr.a, pr.b);
+            bp->prof_ms[pr.cls] += ms;
+            bp->prof_launches[pr.cls] += 1;
+            cudaEventDestroy(pr.a);
+            cudaEventDestroy(pr.b);
+        }
+    } else {
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, st, iters, n_sm);
+            e = cudaStreamEndCapture(st, &g);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+        for (long long w = 0; e == cudaSuccess && w < waves; ++w) e = cudaGraphLaunch(ge, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "ptr_render_batch");
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    cudaFree(d_scenes); cudaFree(d_progs); cudaFree(d_jobs); cudaFree(d_off);
+    if (rc) return rc;
+    for (int j = 0; j < n_jobs; ++j) jobs[j].prog->nsamples += (double)jobs[j].frame.spp;
+    bp->last_scene = nullptr;
+    return PTR_OK;
+}
+
+int ptr_profile_batch_next(ptr_ctx* ctx, int mode) {
+    if (!ctx) return PTR_E_INVALID;
+    if (!ctx->batch) {
+        ctx->batch = new ptr_program();
+        ctx->batch->ctx = ctx;
+    }
+    ctx->batch->profile_next = mode & PTR_PROFILE_TIMING;
+    return PTR_OK;
+}
+
+int ptr_get_batch_profile(ptr_ctx* ctx, float* ms_out, int* launches_out, int n) {
+    if (!ctx || !ctx->batch) return PTR_E_INVALID;
+    return ptr_get_profile(ctx->batch, ms_out, launches_out, n);
+}
+
+int ptr_get_batch_counters(ptr_ctx* ctx, ptr_counters* out) {
+    if (!ctx || !out) return PTR_E_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    if (!ctx->batch || !ctx->batch->pool.stats) return PTR_OK;
+    return ptr_get_counters(ctx->batch, out);
 }
 
 int ptr_render_samples(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* host_out, size_t n) {

@@ -42,6 +42,7 @@ class CudaEngine:
         self._pinned_salt = None
         self.width = self.height = 0
         self.params = {}
+        self._batches = []
 
     # -- errors ---------------------------------------------------------------------
     def _check(self, rc):
@@ -173,7 +174,16 @@ class CudaEngine:
                 "shadow_tlas_nodes": c.shadow_work[2], "shadow_instances": c.shadow_work[3],
                 "error_flags": c.error_flags}
 
+    def batch(self, items):
+        """A ``Batch`` of (renderer, packed scene) jobs on this engine's context."""
+        b = Batch(self, items)
+        self._batches.append(b)
+        return b
+
     def close(self):
+        for b in self._batches:
+            b.close()
+        self._batches.clear()
         for h in self.programs.values():
             self.lib.ptr_free_program(h)
         self.programs.clear()
@@ -189,6 +199,99 @@ class CudaEngine:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many (renderer, scene) jobs rendered together: ``render`` draws every job's frame
+    in ONE batched wavefront (``ptr_render_batch``: one path pool, one CUDA graph per
+    wave over all jobs); ``render_plain`` draws the same frames one job per launch
+    (``ptr_render``).  Each job keeps its own film, read with ``read_export(j)``.
+    No counterpart in the reference, which draws one renderer per frame."""
+
+    def __init__(self, engine, items):
+        self.engine = engine
+        self.lib = engine.lib
+        self.scenes, self.programs, self.renderers, self.sizes = [], [], [], []
+        self._packed = []
+        try:
+            for renderer, packed in items:
+                desc = packed.desc()
+                h = C.c_void_p()
+                engine._check(self.lib.ptr_upload_scene(engine.ctx, C.byref(desc), C.byref(h)))
+                self.scenes.append(h)
+                self._packed.append(packed)
+                p = C.c_void_p()
+                engine._check(self.lib.ptr_compile(engine.ctx, C.byref(renderer.program), C.byref(p)))
+                self.programs.append(p)
+                self.renderers.append(renderer)
+                self.sizes.append((0, 0))
+        except Exception:
+            self.close()
+            raise
+
+    def __len__(self):
+        return len(self.programs)
+
+    def _jobs(self, frames):
+        """frames: per job (width, height, spp[, first_sample[, salt[, params]]])."""
+        if len(frames) != len(self.programs):
+            raise ValueError("one frame per job")
+        arr = (abi.BatchJob * len(frames))()
+        for j, f in enumerate(frames):
+            w, h, spp = f[:3]
+            first = f[3] if len(f) > 3 else 0
+            salt = f[4] if len(f) > 4 else 0
+            params = f[5] if len(f) > 5 else {}
+            J = arr[j]
+            J.prog = self.programs[j].value
+            J.scene = self.scenes[j].value
+            J.frame.width, J.frame.height, J.frame.spp = w, h, spp
+            J.frame.first_sample = first
+            J.frame.reset_salt = salt & 0xFFFFFFFF
+            J.frame.accumulate = 1 if first > 0 else 0
+            J.frame.camera = self.renderers[j].camera(params, w, h)
+            self.sizes[j] = (w, h)
+        return arr
+
+    def render(self, frames):
+        arr = self._jobs(frames)
+        self.engine._check(self.lib.ptr_render_batch(self.engine.ctx, arr, len(arr)))
+
+    def profile(self, frames):
+        """Render batched once with CUDA events around every launch; per kernel class
+        (summed device ms, launch count)."""
+        self.engine._check(self.lib.ptr_profile_batch_next(self.engine.ctx, abi.PROFILE_TIMING))
+        self.render(frames)
+        ms = (C.c_float * 5)()
+        n = (C.c_int * 5)()
+        self.engine._check(self.lib.ptr_get_batch_profile(self.engine.ctx, ms, n, 5))
+        return {k: (ms[i], n[i]) for i, k in enumerate(CudaEngine.KERNEL_CLASSES)}
+
+    def render_plain(self, frames, sync=True):
+        arr = self._jobs(frames)
+        for j in range(len(arr)):
+            self.engine._check(self.lib.ptr_render(self.programs[j], self.scenes[j], C.byref(arr[j].frame)))
+        if sync:
+            self.engine.sync()
+
+    def read_export(self, j, name="radiance"):
+        w, h = self.sizes[j]
+        out = np.empty((h, w, 3), np.float32)
+        self.engine._check(self.lib.ptr_read_export(self.programs[j], name.encode(),
+                                                    out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    def counters(self):
+        c = abi.Counters()
+        self.engine._check(self.lib.ptr_get_batch_counters(self.engine.ctx, C.byref(c)))
+        return {"paths": c.paths, "closest_queries": c.closest_queries, "shadow_queries": c.shadow_queries}
+
+    def close(self):
+        for p in self.programs:
+            self.lib.ptr_free_program(p)
+        for h in self.scenes:
+            self.lib.ptr_free_scene(h)
+        self.programs, self.scenes = [], []
 
 
 def render(scene, strategy, width, height, spp, params=None, salt=0, device=0, engine=None):

@@ -203,3 +203,59 @@ def mesh_scene(level=8, instances=16, seed=0, width=1920, height=1080, spp=256, 
         "view": {"tonemap": {"type": "none"}},
     }
     return scene, strategy, (width, height, spp)
+
+
+# ------------------------------------------------------------------------- scene batches
+def batch_scene(seed, max_spheres=200):
+    """One seeded Cornell-style scene of the batched workload: the Cornell box's five
+    walls and ceiling light with 1..`max_spheres` non-overlapping spheres of radius
+    U(0.05, 0.3) inside it (count log-uniform), each with a material drawn uniformly from
+    Lambert (albedo U(0.2, 0.9) per channel), smooth dielectric (IOR U(1.3, 1.8)) and GGX
+    (alpha U(0.05, 0.6), F0 = albedo); resolution 128..1024 squared (log-uniform, a
+    multiple of 16), spp 16..256 (a power of two) and max depth 4..32.
+    Returns (scene, strategy, (width, height, spp))."""
+    rng = _np.random.RandomState(1000 + seed)
+    base, strategy = cornell()
+    objects = list(base["objects"][:5])
+    materials = {k: base["materials"][k] for k in ("white", "red", "green")}
+    n = int(round(math.exp(rng.uniform(0.0, math.log(max_spheres)))))
+    n = max(1, min(max_spheres, n))
+    placed = []
+    for k in range(n):
+        r = float(rng.uniform(0.05, 0.3))
+        for _attempt in range(200):
+            c = _np.array([rng.uniform(-1 + r, 1 - r), rng.uniform(r, 1.9 - r), rng.uniform(-1 + r, 1 - r)])
+            if all(_np.linalg.norm(c - pc) > r + pr + 1e-3 for pc, pr in placed):
+                break
+            if _attempt % 20 == 19:
+                r = max(0.02, r * 0.8)
+        else:
+            continue
+        placed.append((c, r))
+        kind = int(rng.randint(3))
+        name = f"s{k}"
+        if kind == 0:
+            materials[name] = {"model": "lambert", "albedo": [float(a) for a in rng.uniform(0.2, 0.9, 3)]}
+        elif kind == 1:
+            materials[name] = {"model": "dielectric", "ior": float(rng.uniform(1.3, 1.8))}
+        else:
+            alpha = float(rng.uniform(0.05, 0.6))
+            materials[name] = {"model": "ggx", "f0": [float(a) for a in rng.uniform(0.2, 0.9, 3)],
+                               "roughness": math.sqrt(alpha)}
+        objects.append({"type": "sphere", "parameters": {"center": [float(x) for x in c], "radius": r},
+                        "material": name})
+    scene = dict(base, id=f"batch-{seed}", objects=objects, materials=materials)
+    res = int(round(math.exp(rng.uniform(math.log(128), math.log(1024))) / 16.0)) * 16
+    spp = int(2 ** rng.randint(4, 9))
+    depth = int(rng.randint(4, 33))
+    strategy = dict(strategy, id=f"batch-{seed}-pt-mis",
+                    measurement=dict(strategy["measurement"], maxBounces=depth))
+    return scene, strategy, (res, res, spp)
+
+
+BATCH_SIZE = 64
+
+
+def batch_scenes(n=BATCH_SIZE, seed=0, max_spheres=200):
+    """The batched workload: `n` seeded Cornell-style scenes (``batch_scene``)."""
+    return [batch_scene(seed * 100003 + k, max_spheres) for k in range(n)]
