@@ -155,6 +155,15 @@ typedef struct ptr_scene_desc {
 #define PTR_DIRECT_MIS 2
 #define PTR_ACCEL_BVH 0   /* binary SAH BVH (bvh.ts)                   */
 #define PTR_ACCEL_CWBVH 1 /* compressed wide BVH (cwbvh.ts)            */
+/* estimator.mediumLightSampling: 'vertex' (NEE at medium scattering vertices) or
+ * 'equiangular' (one Kulla-Fajardo estimate per medium segment,
+ * transport/techniques/equiangular/equiangular.glsl:18-57).  The reference pins it to
+ * delta lights and plain NEE; PTR_EQUIANGULAR_AREA is this library's extension that also
+ * admits quad and sphere lights (a uniform point on the light's area, then the
+ * equiangular distance towards it). */
+#define PTR_EQUIANGULAR_OFF 0
+#define PTR_EQUIANGULAR_DELTA 1
+#define PTR_EQUIANGULAR_AREA 2
 
 typedef struct ptr_program_desc {
     int32_t abi_version;
@@ -165,7 +174,7 @@ typedef struct ptr_program_desc {
     float rr_max_survival;      /* russianRoulette.maxSurvival (0.95)                 */
     int32_t scattering;         /* measurement.scattering: 1 full, 0 ignored           */
     int32_t accel;              /* PTR_ACCEL_*  (meshTraversal / instanceAccel)        */
-    int32_t equiangular;        /* mediumLightSampling 'equiangular'                  */
+    int32_t equiangular;        /* PTR_EQUIANGULAR_*  (mediumLightSampling)            */
     int32_t pad[7];
 } ptr_program_desc;
 

@@ -1111,6 +1111,78 @@ struct Tracer {
         return f2 / fmaxf_(1e-20f, f2 + pg * pg);
     }
 
+    // ---- equiangular medium NEE, one estimate per medium segment with segment-start
+    // throughput (transport/techniques/equiangular/equiangular.glsl:18-57; Kulla & Fajardo
+    // 2012).  The light is picked by the lighting CDF (lighting_query_delta,
+    // features/lighting.ts:303-341): a delta light gives its position and intensity as in
+    // the reference.  Area lights (quad, sphere) are an extension the reference's
+    // Validator rejects: a uniform point on the light's area is drawn first (two more
+    // numbers), the estimate then carries Le * cos_l / (d^2 * pdf_area).
+    void equiangular_sample_direct(const Ray& r, int med_mat, float t_max, v3 thr, v3& radiance, int crossings_left) {
+        const ptr_material& mm = d.materials[med_mat];
+        float uc = rng.next();
+        int id = d.n_lights - 1;
+        if (d.n_lights > 1)
+            for (int i = 0; i < d.n_lights - 1; ++i)
+                if (uc < d.lights[i].select_cdf) { id = i; break; }
+        const ptr_light& l = d.lights[id];
+        const float sel = d.n_lights == 1 ? 1.0f : l.select_pdf;
+        v3 pos, nl(0.0f);
+        float pdf_area = 1.0f;
+        const bool area = l.kind != PTR_LIGHT_POINT;
+        if (area) {
+            float y0 = rng.next(), y1 = rng.next();
+            if (l.kind == PTR_LIGHT_QUAD) {
+                pos = ld3(l.p) + y0 * ld3(l.p + 3) + y1 * ld3(l.p + 6);
+                nl = ld3(l.p + 9);
+                pdf_area = 1.0f / l.p[12];
+            } else {
+                float z = 1.0f - 2.0f * y0;
+                float rr = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
+                float phi = TWO_PI * y1;
+                nl = v3(rr * std::cos(phi), z, rr * std::sin(phi));
+                pos = ld3(l.p) + nl * l.p[3];
+                pdf_area = 1.0f / (4.0f * PI * l.p[3] * l.p[3]);
+            }
+        } else {
+            pos = ld3(l.p);
+        }
+        // the light's frame over the segment: closest approach t_c, perpendicular h
+        v3 D = pos - r.o;
+        float t_c = dot(D, r.d);
+        float h2 = fmaxf_(dot(D, D) - t_c * t_c, 1e-8f);
+        float h = std::sqrt(h2);
+        float theta_a = std::atan2(0.0f - t_c, h);
+        float theta_b = std::atan2(t_max - t_c, h);
+        float u = rng.next();
+        float theta = theta_a * (1.0f - u) + theta_b * u;
+        float t = t_c + h * std::tan(theta);
+        float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
+        v3 p_evt = r.o + r.d * t;
+        v3 sigma_s = ld3(mm.sigma_s);
+        if (spectrum_is_black(sigma_s)) return;
+        v3 T_seg = vexp(-(ld3(mm.sigma_a) + sigma_s) * t);
+        v3 to_light = pos - p_evt;
+        float d2 = fmaxf_(dot(to_light, to_light), 1e-8f);
+        float dist = std::sqrt(d2);
+        v3 wi = to_light / dist;
+        v3 Le;
+        float denom;
+        if (area) {
+            float cos_l = dot(nl, -wi);
+            if (cos_l <= 0.0f) return;
+            Le = ld3(l.radiance) * (cos_l / d2);
+            denom = pdf_t * (pdf_area * sel);
+        } else {
+            Le = ld3(l.radiance) / d2;
+            denom = pdf_t * sel;
+        }
+        v3 vis = shadow_transmittance(Ray{p_evt, wi}, pos, crossings_left);
+        if (spectrum_is_black(vis)) return;
+        v3 ph(hg_eval(wi, -r.d, mm.phase_g));
+        radiance = radiance + thr * T_seg * sigma_s * ph * Le * vis / denom;
+    }
+
     // ---- the walk (transport/integrators/pt/pt.ts:299-464, as emitted for media scenes)
     v3 transport_trace(Ray ray) {
         const bool nee = P.direct != PTR_DIRECT_NONE;
@@ -1169,6 +1241,11 @@ struct Tracer {
                 // every medium arm, scattering or absorbing-only (features/materials.ts:675-746)
                 int med_mat = S.material_of(current_medium);
                 if (S.material_has_medium(med_mat)) {
+                    // the per-segment equiangular site precedes the transmittance sample
+                    // (pt.ts:322-328); it places an event, so it is part of the budget
+                    if (P.equiangular && bounce < N)
+                        equiangular_sample_direct(r, med_mat, boundary ? hit.t : MAX_DIST, throughput, radiance,
+                                                  shadow_left_base - null_crossings);
                     float x0 = rng.next(), x1 = rng.next();
                     float t_max = boundary ? hit.t : MAX_DIST;
                     const ptr_material& mm = d.materials[med_mat];
@@ -1182,8 +1259,9 @@ struct Tracer {
                             if (bounce == N) break;
                             v3 p_evt = ms.exit_p;
                             v3 wo_med = -ms.exit_dir;
-                            // light_sample_direct_medium (techniques/light/light_medium.glsl:7-18)
-                            if (nee) {
+                            // light_sample_direct_medium (techniques/light/light_medium.glsl:7-18);
+                            // the equiangular site replaces it (pt.ts:379)
+                            if (nee && !P.equiangular) {
                                 float y0 = rng.next(), y1 = rng.next();
                                 LightSample ls = lighting_sample(p_evt, y0, y1);
                                 if (ls.pdf > 0.0f) {

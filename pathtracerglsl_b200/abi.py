@@ -23,6 +23,7 @@ LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT = range(3)
 ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)
 DIRECT_NONE, DIRECT_NEE, DIRECT_MIS = range(3)
 ACCEL_BVH, ACCEL_CWBVH = range(2)
+EQUIANGULAR_OFF, EQUIANGULAR_DELTA, EQUIANGULAR_AREA = range(3)
 
 F4 = C.c_float * 4
 

@@ -290,13 +290,24 @@ class Compiler:
         vs = est.get("volumeSampling", "analytic")
         if vs not in ("analytic", None):
             bag.error("unsupported", f"volumeSampling {vs!r} is not available in this build")
-        if est.get("mediumLightSampling", "vertex") == "equiangular":
-            # Validator.ts:506-540: equiangular is pinned to delta lights and plain NEE.
+        mls = est.get("mediumLightSampling", "vertex")
+        if mls not in ("vertex", "equiangular"):
+            bag.error("invalid-setting", f"mediumLightSampling {mls!r} (available: vertex, equiangular)")
+        if mls == "equiangular":
+            # Validator.ts:506-540: equiangular is pinned to delta lights and plain NEE.  The
+            # strategy key 'equiangularAreaLights' (this library's extension, not in the
+            # reference) also admits quad and sphere lights.
             if est.get("directLighting") != "nee":
                 bag.error("invalid-setting", "mediumLightSampling 'equiangular' requires directLighting 'nee'")
-            if any(l.get("kind") != "point" for l in scene.get("lights", [])):
-                bag.error("invalid-setting", "mediumLightSampling 'equiangular' supports delta (point) lights only")
-            bag.error("unsupported", "mediumLightSampling 'equiangular' is not available in this build")
+            area_ok = bool(est.get("equiangularAreaLights", False))
+            kinds = ("point", "quad", "sphere") if area_ok else ("point",)
+            if any(l.get("kind") not in kinds for l in scene.get("lights", [])):
+                bag.error("invalid-setting", "mediumLightSampling 'equiangular' supports delta (point) lights only"
+                          if not area_ok else "mediumLightSampling 'equiangular' supports point, quad and sphere lights")
+            if not scene.get("lights"):
+                bag.error("invalid-setting", "mediumLightSampling 'equiangular' needs at least one light")
+            if meas.get("scattering") == "ignored":
+                bag.error("invalid-setting", "mediumLightSampling 'equiangular' requires scattering media")
         for key in ("meshTraversal", "instanceAccel"):
             v = est.get(key)
             if v is not None and v not in ACCELS:
@@ -646,7 +657,9 @@ class Compiler:
         prog.rr_max_survival = float(rr.get("maxSurvival", 0.95)) if rr else 1.0
         prog.scattering = 0 if meas.get("scattering") == "ignored" else 1
         prog.accel = ACCELS[est.get("meshTraversal") or est.get("instanceAccel") or "bvh"]
-        prog.equiangular = 1 if est.get("mediumLightSampling") == "equiangular" else 0
+        prog.equiangular = abi.EQUIANGULAR_OFF
+        if est.get("mediumLightSampling") == "equiangular":
+            prog.equiangular = abi.EQUIANGULAR_AREA if est.get("equiangularAreaLights") else abi.EQUIANGULAR_DELTA
         cam = meas.get("camera", {})
         fov = cam.get("fov", 0.8)
         fov_default = fov.get("default", 0.8) if is_param(fov) else fov

@@ -411,4 +411,77 @@ __device__ __forceinline__ MediumSample medium_sample_analytic(const ptr_materia
     return ms;
 }
 
+// ---- equiangular medium NEE (transport/techniques/equiangular/equiangular.glsl:18-57;
+// Kulla & Fajardo 2012): one estimate per medium segment with segment-start throughput.
+// A light is picked by the lighting CDF (lighting_query_delta, features/lighting.ts:303-341);
+// for a delta light its position and intensity are used as in the reference; area lights
+// (quad, sphere: an extension the reference's Validator rejects) first draw a uniform point
+// on their area and carry Le * cos_l / (d^2 * pdf_area).  The distance t along the segment
+// is uniform in the angle subtended at the light point.  Returns true when a shadow query
+// is due: from p_evt towards light_pos, adding contrib * visibility / denom.
+struct EquiangularQuery { f3 p_evt, wi, light_pos, contrib; float denom; };
+__device__ __forceinline__ bool equiangular_site(const DevScene& S, const ptr_material& mm, const Ray& r, float t_max,
+                                                 Rng& rng, f3 thr, EquiangularQuery& q) {
+    float uc = rng.next();
+    int id = S.n_lights - 1;
+    if (S.n_lights > 1)
+        for (int i = 0; i < S.n_lights - 1; ++i)
+            if (uc < S.lights[i].select_cdf) { id = i; break; }
+    const ptr_light& l = S.lights[id];
+    const float sel = S.n_lights == 1 ? 1.0f : l.select_pdf;
+    f3 pos, nl(0.0f);
+    float pdf_area = 1.0f;
+    const bool area = l.kind != PTR_LIGHT_POINT;
+    if (area) {
+        float y0 = rng.next();
+        float y1 = rng.next();
+        if (l.kind == PTR_LIGHT_QUAD) {
+            pos = ld3(l.p) + y0 * ld3(l.p + 3) + y1 * ld3(l.p + 6);
+            nl = ld3(l.p + 9);
+            pdf_area = 1.0f / l.p[12];
+        } else {
+            float z = 1.0f - 2.0f * y0;
+            float rr = sqrtf(gmax(0.0f, 1.0f - z * z));
+            float phi = kTwoPi * y1;
+            nl = f3(rr * cosf(phi), z, rr * sinf(phi));
+            pos = ld3(l.p) + nl * l.p[3];
+            pdf_area = 1.0f / (4.0f * kPi * l.p[3] * l.p[3]);
+        }
+    } else {
+        pos = ld3(l.p);
+    }
+    f3 D = pos - r.o;
+    float t_c = dot(D, r.d);
+    float h2 = gmax(dot(D, D) - t_c * t_c, 1e-8f);
+    float h = sqrtf(h2);
+    float theta_a = atan2f(0.0f - t_c, h);
+    float theta_b = atan2f(t_max - t_c, h);
+    float u = rng.next();
+    float theta = theta_a * (1.0f - u) + theta_b * u;
+    float t = t_c + h * tanf(theta);
+    float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
+    q.p_evt = r.o + r.d * t;
+    f3 sigma_s = ld3(mm.sigma_s);
+    if (spectrum_is_black(sigma_s)) return false;
+    f3 T_seg = vexp(-(ld3(mm.sigma_a) + sigma_s) * t);
+    f3 to_light = pos - q.p_evt;
+    float d2 = gmax(dot(to_light, to_light), 1e-8f);
+    float dist = sqrtf(d2);
+    q.wi = to_light / dist;
+    f3 Le;
+    if (area) {
+        float cos_l = dot(nl, -q.wi);
+        if (cos_l <= 0.0f) return false;
+        Le = ld3(l.radiance) * (cos_l / d2);
+        q.denom = pdf_t * (pdf_area * sel);
+    } else {
+        Le = ld3(l.radiance) / d2;
+        q.denom = pdf_t * sel;
+    }
+    q.light_pos = pos;
+    f3 ph(hg_eval(q.wi, -r.d, mm.phase_g));
+    q.contrib = thr * T_seg * sigma_s * ph * Le;
+    return true;
+}
+
 }  // namespace ptx

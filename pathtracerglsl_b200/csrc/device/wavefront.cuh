@@ -39,9 +39,16 @@ struct PathPool {
     float4* sh_d;      // direction.xyz, crossings left (as int)
     float4* sh_lp;     // light point.xyz, MIS weight
     float4* sh_c;      // contribution prefix throughput*Le*f*cos (xyz), pdf
+    // second shadow slot: the per-segment equiangular query of the same iteration (a path
+    // may issue it and a surface NEE query in one walk iteration); NULL when unused
+    float4* sh2_o;
+    float4* sh2_d;
+    float4* sh2_lp;
+    float4* sh2_c;
     int* q[2];         // live-path queues (ping-pong)
     int* shq;          // shadow queue
-    unsigned int* cnt; // [0],[1] queue counts, [2] shadow count, [3] error flags
+    int* shq2;         // second-slot shadow queue (count in cnt[4])
+    unsigned int* cnt; // [0],[1] queue counts, [2] shadow count, [3] error flags, [4] slot-2 shadow count
     unsigned long long* stats; // [0] closest queries, [1] shadow queries, [2] paths
     long long* wave;   // [0] first global path index of the wave, [1] wave size
     int* job;          // batched renders: the job (scene x program x frame) of each path
@@ -60,6 +67,7 @@ struct ProgParams {
     int max_bounces, direct, rr_start, max_null;
     float rr_max_survival;
     int scattering;
+    int equiangular;   // PTR_EQUIANGULAR_*: per-segment medium NEE replaces the at-vertex site
 };
 
 // Batched renders: per job its scene, program knobs, frame and film; offsets[j] is the
@@ -336,6 +344,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         pool.cnt[in ^ 1] = 0u;
         pool.cnt[2] = 0u;
+        pool.cnt[4] = 0u;
         pool.stats[0] += n;
     }
     const int* q = pool.q[in];
@@ -354,8 +363,11 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
 }
 
 // One walk iteration for every live path.
+#ifndef PTR_SHADE_MIN_BLOCKS
+#define PTR_SHADE_MIN_BLOCKS 3
+#endif
 template <int DIRECT, bool MEDIA, bool BATCH>
-__global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt) {
+__global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt) {
     const unsigned n = pool.cnt[in];
     const int* q = pool.q[in];
     int* qout = pool.q[in ^ 1];
@@ -364,7 +376,7 @@ __global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, Batch
     const unsigned stride = gridDim.x * blockDim.x;
     const unsigned n_round = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n_round + 0u; k += stride) {
-        bool alive = false, shadow = false;
+        bool alive = false, shadow = false, shadow2 = false;
         int i = -1;
         if (k < n) {
             i = q[k];
@@ -401,10 +413,22 @@ __global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, Batch
             if (MEDIA) {
                 int med_mat = material_of(S, cur_med);
                 if (mat_has_medium(S, med_mat)) {
+                    const ptr_material& mm = S.materials[med_mat];
+                    // the per-segment equiangular site precedes the transmittance sample
+                    // (pt.ts:322-328) and rides the second shadow slot
+                    if (P.equiangular && bounce < N) {
+                        EquiangularQuery eq;
+                        if (equiangular_site(S, mm, r, boundary ? hr.t : kMaxDist, rng, thr, eq)) {
+                            pool.sh2_o[i] = f4(eq.p_evt, 0.0f);
+                            pool.sh2_d[i] = f4(eq.wi, __int_as_float(P.max_null - nulls));
+                            pool.sh2_lp[i] = f4(eq.light_pos, 1.0f);
+                            pool.sh2_c[i] = f4(eq.contrib, eq.denom);
+                            shadow2 = true;
+                        }
+                    }
                     float x0 = rng.next();
                     float x1 = rng.next();
                     float t_max = boundary ? hr.t : kMaxDist;
-                    const ptr_material& mm = S.materials[med_mat];
                     if (!scatter_live(S, P, med_mat)) {
                         thr = thr * vexp(-ld3(mm.sigma_a) * t_max);
                     } else {
@@ -417,7 +441,7 @@ __global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, Batch
                             } else {
                                 f3 p_evt = ms.exit_p;
                                 f3 wo_med = -ms.exit_dir;
-                                if (nee) {   // light_sample_direct_medium (light_medium.glsl:7-18)
+                                if (nee && !P.equiangular) {   // light_sample_direct_medium (light_medium.glsl:7-18)
                                     float y0 = rng.next();
                                     float y1 = rng.next();
                                     LightSample ls = lighting_sample(S, p_evt, y0, y1);
@@ -583,22 +607,35 @@ __global__ void k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, Batch
         if (alive) qout[slot] = i;
         int sslot = warp_append(&pool.cnt[2], shadow);
         if (shadow) pool.shq[sslot] = i;
+        if (MEDIA) {
+            int s2 = warp_append(&pool.cnt[4], shadow2);
+            if (shadow2) pool.shq2[s2] = i;
+        }
     }
 }
 
 // Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
 // segment walker (shadow/media/media.glsl:29-62); the surviving fraction scales the
 // stored contribution prefix into the path's radiance.
+// slot 1 reads the second shadow slot (the equiangular segment queries); its launch
+// precedes the slot-0 launch of the same iteration, so the two never add to one path's
+// radiance concurrently.
 template <bool MEDIA, bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt) {
-    const unsigned n = pool.cnt[2];
+__global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt,
+                                                                      int slot) {
+    const unsigned n = pool.cnt[slot ? 4 : 2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
+    const int* shq = slot ? pool.shq2 : pool.shq;
+    const float4* a_o = slot ? pool.sh2_o : pool.sh_o;
+    const float4* a_d = slot ? pool.sh2_d : pool.sh_d;
+    const float4* a_lp = slot ? pool.sh2_lp : pool.sh_lp;
+    const float4* a_c = slot ? pool.sh2_c : pool.sh_c;
     Work wk{0u, 0u, 0u, 0u};
     for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int i = pool.shq[k];
+        int i = shq[k];
         const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
-        float4 so = pool.sh_o[i], sd = pool.sh_d[i], lp = pool.sh_lp[i], c = pool.sh_c[i];
+        float4 so = a_o[i], sd = a_d[i], lp = a_lp[i], c = a_c[i];
         Ray sr;
         sr.o = xyz(so);
         sr.d = xyz(sd);

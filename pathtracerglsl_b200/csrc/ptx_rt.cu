@@ -37,6 +37,7 @@ struct ptr_scene {
     std::vector<void*> allocs;
     int has_media = 0;
     int max_stack_depth = 0;
+    int n_lights = 0, n_delta_lights = 0, env_samplable = 0;
 };
 
 struct ptr_program {
@@ -108,7 +109,7 @@ void free_pool(ptr_program* p) {
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
 }
 
-int alloc_pool(ptr_program* p, int capacity) {
+int alloc_pool(ptr_program* p, int capacity, bool slot2) {
     free_pool(p);
     ptr_ctx* ctx = p->ctx;
     auto get = [&](size_t bytes, void** out) -> int {
@@ -131,6 +132,13 @@ int alloc_pool(ptr_program* p, int capacity) {
         (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
         (rc = get(64, (void**)&q.wave))) {
+        free_pool(p);
+        return rc;
+    }
+    // the second shadow slot only for programs with the per-segment equiangular site
+    if (slot2 && ((rc = get(c * 16, (void**)&q.sh2_o)) || (rc = get(c * 16, (void**)&q.sh2_d)) ||
+                  (rc = get(c * 16, (void**)&q.sh2_lp)) || (rc = get(c * 16, (void**)&q.sh2_c)) ||
+                  (rc = get(c * 4, (void**)&q.shq2)))) {
         free_pool(p);
         return rc;
     }
@@ -173,6 +181,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     P.max_null = p->desc.max_null_crossings;
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
+    P.equiangular = p->desc.equiangular;
     const int grid = launch_grid(n_sm), block = 256;
     ProfRec* r = mark(0);
     const BatchTables nob{};
@@ -197,14 +206,17 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
             r = mark(3);
-            if (S.work) {
-                DevScene Sq = S;
-                Sq.work = S.work + 4;   // the shadow queries' own tallies
-                if (media) k_shadow<true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob);
-                else k_shadow<false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob);
-            } else {
-                if (media) k_shadow<true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob);
-                else k_shadow<false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob);
+            // slot 1 (equiangular segment queries) before slot 0 (surface / vertex NEE)
+            for (int slot = P.equiangular ? 1 : 0; slot >= 0; --slot) {
+                if (S.work) {
+                    DevScene Sq = S;
+                    Sq.work = S.work + 4;   // the shadow queries' own tallies
+                    if (media) k_shadow<true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
+                    else k_shadow<false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
+                } else {
+                    if (media) k_shadow<true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
+                    else k_shadow<false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
+                }
             }
             done(r);
         }
@@ -218,7 +230,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
 // One wave of a batched render: the same kernel sequence over the concatenated job space;
 // scene, program knobs and frame come from the per-job tables.
 void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTables& bt, int direct, bool media,
-                       cudaStream_t st, int iters, int n_sm, std::vector<ProfRec>* prof = nullptr) {
+                       bool equiangular, cudaStream_t st, int iters, int n_sm, std::vector<ProfRec>* prof = nullptr) {
     const int grid = launch_grid(n_sm), block = 256;
     ProgParams P0{};
     auto mark = [&](int cls) -> ProfRec* {
@@ -251,8 +263,10 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTabl
         done(r);
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
-            if (media) k_shadow<true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt);
-            else k_shadow<false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt);
+            for (int slot = equiangular ? 1 : 0; slot >= 0; --slot) {
+                if (media) k_shadow<true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
+                else k_shadow<false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
+            }
             done(r);
         }
     }
@@ -500,10 +514,24 @@ int prepare_film(ptr_program* p, const ptr_frame* f, cudaStream_t st) {
     return PTR_OK;
 }
 
+// The scene-dependent pins of the equiangular site: the reference admits delta lights only
+// (Validator.ts:506-540); PTR_EQUIANGULAR_AREA also admits quad and sphere lights.  The
+// site covers finite lights, so a sampled environment is rejected (its medium-vertex NEE
+// would be lost).
+int check_equiangular(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
+    if (!p->desc.equiangular) return PTR_OK;
+    if (s->n_lights == 0) return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' needs at least one light");
+    if (p->desc.equiangular == PTR_EQUIANGULAR_DELTA && s->n_delta_lights != s->n_lights)
+        return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' supports delta (point) lights only");
+    if (s->env_samplable) return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' does not cover a sampled environment");
+    return PTR_OK;
+}
+
 int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples_dev) {
     ptr_ctx* ctx = p->ctx;
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return fail(ctx, PTR_E_INVALID, "frame: width, height and spp must be positive");
     if (s->ctx != ctx) return fail(ctx, PTR_E_INVALID, "scene belongs to another context");
+    if (int rc = check_equiangular(ctx, p, s)) return rc;
     CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const size_t npix = (size_t)f->width * f->height;
@@ -536,8 +564,9 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     if ((long long)npix <= cap_max) cap = (cap_max / (long long)npix) * (long long)npix;
     else cap = cap_max;
     if (cap > total) cap = total;
-    if (p->capacity < cap) {
-        int rc = alloc_pool(p, (int)cap);
+    const bool slot2 = p->desc.equiangular != 0;
+    if (p->capacity < cap || (slot2 && !p->pool.sh2_o)) {
+        int rc = alloc_pool(p, (int)cap, slot2);
         if (rc) return rc;
     }
     if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
@@ -695,6 +724,9 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         if (d->materials[i].flags & PTR_MATF_MEDIUM) media = true;
     S.has_media = media ? 1 : 0;
     s->has_media = S.has_media;
+    s->n_lights = d->n_lights;
+    for (int i = 0; i < d->n_lights; ++i) s->n_delta_lights += d->lights[i].kind == PTR_LIGHT_POINT ? 1 : 0;
+    s->env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
     S.env_kind = d->env.kind;
     S.env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
     S.env_select_live = S.env_samplable && d->n_lights > 0;
@@ -748,7 +780,13 @@ int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* d, ptr_program** out) {
     if (d->rr_start >= 0 && !(d->rr_max_survival > 0.0f && d->rr_max_survival <= 1.0f))
         return fail(ctx, PTR_E_INVALID, "program: russianRoulette.maxSurvival must be in (0, 1]");
     if (d->max_null_crossings < 0 || d->max_null_crossings > 4096) return fail(ctx, PTR_E_INVALID, "program: maxNullCrossings out of range");
-    if (d->equiangular) return fail(ctx, PTR_E_UNSUPPORTED, "program: equiangular medium NEE is not available in this build");
+    // the reference's pins (Validator.ts:506-540): equiangular placement only under plain NEE
+    if (d->equiangular < PTR_EQUIANGULAR_OFF || d->equiangular > PTR_EQUIANGULAR_AREA)
+        return fail(ctx, PTR_E_INVALID, "program: unknown mediumLightSampling");
+    if (d->equiangular && d->direct != PTR_DIRECT_NEE)
+        return fail(ctx, PTR_E_INVALID, "program: mediumLightSampling 'equiangular' requires directLighting 'nee'");
+    if (d->equiangular && !d->scattering)
+        return fail(ctx, PTR_E_INVALID, "program: mediumLightSampling 'equiangular' requires scattering media");
     ptr_program* p = new ptr_program();
     p->ctx = ctx;
     p->desc = *d;
@@ -780,7 +818,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const int direct = jobs[0].prog ? jobs[0].prog->desc.direct : -1;
-    bool media = false;
+    bool media = false, equi = false;
     for (int j = 0; j < n_jobs; ++j) {
         const ptr_batch_job& J = jobs[j];
         if (!J.prog || !J.scene || J.prog->ctx != ctx || J.scene->ctx != ctx)
@@ -790,6 +828,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         if (J.frame.width <= 0 || J.frame.height <= 0 || J.frame.spp <= 0)
             return fail(ctx, PTR_E_INVALID, "ptr_render_batch: job " + std::to_string(j) + " has an empty frame");
         if (J.scene->has_media) media = true;
+        if (int rc = check_equiangular(ctx, J.prog, J.scene)) return rc;
         for (int k = 0; k < j; ++k)
             if (jobs[k].prog == J.prog)
                 return fail(ctx, PTR_E_INVALID, "ptr_render_batch: jobs " + std::to_string(k) + " and " + std::to_string(j) + " share a program (one film per job)");
@@ -814,6 +853,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         P.max_null = p->desc.max_null_crossings;
         P.rr_max_survival = p->desc.rr_max_survival;
         P.scattering = p->desc.scattering;
+        P.equiangular = p->desc.equiangular;
+        if (P.equiangular) equi = true;
         const long long total_j = (long long)J.frame.width * J.frame.height * J.frame.spp;
         FrameParams& F = bjobs[j].frame;
         F.width = J.frame.width;
@@ -840,8 +881,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     long long cap_max = 1ll << 21;
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
     long long cap = std::min(total, cap_max);
-    if (bp->capacity < cap) {
-        int rc = alloc_pool(bp, (int)cap);
+    if (bp->capacity < cap || (equi && !bp->pool.sh2_o)) {
+        int rc = alloc_pool(bp, (int)std::max<long long>(cap, bp->capacity), equi || bp->pool.sh2_o);
         if (rc) return rc;
     }
     // device tables (a few KB; refreshed every call)
@@ -881,7 +922,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         std::vector<ProfRec> prof;
         prof.reserve((size_t)waves * (iters * 3 + 2));
         for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, st, iters, n_sm, &prof);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, &prof);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -897,7 +938,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     } else {
         if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, st, iters, n_sm);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm);
             e = cudaStreamEndCapture(st, &g);
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
