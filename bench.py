@@ -195,6 +195,11 @@ def run_reference(args):
     if args.workload == "batch":
         jobs, cfg = batch_workload()
         sc, st, (w, h, spp) = jobs[0]
+    elif args.workload == "adjoint":
+        from pathtracerglsl_b200 import scenes
+        sc, st, (w, h, _spp_p, spp) = scenes.adjoint_scene(0)
+        cfg = {"workload": "adjoint-c5 scene, forward walk only (the CPU restatement has no adjoint)",
+               "width": w, "height": h, "spp": spp}
     else:
         sc, st, w, h, spp, cfg = workload(args.workload)
     oracle.build()
@@ -476,6 +481,133 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------------- adjoint
+def run_adjoint(args):
+    """The inverse-rendering workload: loss = L2 between the image at the current
+    parameters (64 spp primal) and a target rendered at seeded +-10 % perturbed parameters;
+    one step = one path-replay adjoint pass at 16 spp (forward walk + replay, gradients of
+    every material parameter in float64).  Reported beside it: the forward render at the
+    same 16 spp (the adjoint's cost ratio) and the 64-spp primal."""
+    import torch
+    import numpy as np
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from pathtracerglsl_b200 import adjoint, scenes
+    from pathtracerglsl_b200.compiler import Compiler
+    from pathtracerglsl_b200.engine import CudaEngine
+
+    sc, st, (w, h, spp_p, spp_a) = scenes.adjoint_scene(0)
+    renderer, packed = Compiler().compile(sc, st)
+    eng = CudaEngine(local)
+    eng.register_scene(packed)
+    eng.load_renderer(renderer)
+    theta = adjoint.param_table(packed)
+    mask = adjoint.live_mask(packed)
+    rng = np.random.RandomState(11)
+    pert = theta * (1 + 0.1 * rng.uniform(-1, 1, theta.shape))
+    eng.update_params(adjoint.with_params(packed, pert))
+    eng.pin_reset_salt(1000 + rank)
+    eng.render_frame(w, h, spp_p)
+    target = eng.read_export("radiance").copy()
+    eng.update_params(adjoint.with_params(packed, theta))
+    eng.pin_reset_salt(2000 + rank)
+    eng.reset()
+    eng.render_frame(w, h, spp_p)
+    primal = eng.read_export("radiance").copy()
+    loss, dl = adjoint.l2_loss(primal, target)
+    dl = dl.astype(np.float32)
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def timed(fn, k_steps):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(k_steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(k_steps)]
+        barrier(dist)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(k_steps):
+                flush.fill_(float(k))
+                starts[k].record(stream)
+                fn(k)
+                ends[k].record(stream)
+        eng.sync()
+        torch.cuda.synchronize()
+        return reduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, ends)))
+
+    def adj_step(k):
+        return eng.backward(dl, w, h, spp_a, salt=3000 + 17 * k + rank)
+
+    def fwd_step(k):
+        eng.pin_reset_salt(3000 + 17 * k + rank)
+        eng.reset()
+        eng.render_frame(w, h, spp_a)
+
+    for k in range(args.warmup):
+        adj_step(k)
+        fwd_step(k)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    t_window = time.time()
+    adj_ms = timed(adj_step, args.steps)
+    clocks.mark(t_window, time.time())
+    clk = clocks.stop()
+    fwd_ms = timed(fwd_step, args.steps)
+    samples = w * h * spp_a * args.steps * world
+    value = samples / (adj_ms / 1000.0)
+    # end to end: adjoint image from host memory in, gradient vector out to host memory
+    barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = None
+    for k in range(args.steps):
+        g = adj_step(k)
+    el = reduce_max(dist, time.perf_counter() - t0)
+    e2e = {"value": samples / el, "unit": "samples/s", "h2d_bytes_per_step": int(dl.nbytes) + 160,
+           "d2h_bytes_per_step": int(g.nbytes)}
+    # the forward pass of the same frame, instrumented: per-kernel-class device time
+    eng.pin_reset_salt(77)
+    eng.reset()
+    from pathtracerglsl_b200 import abi as _abi
+    prof = eng.profile_render(w, h, spp_a, _abi.PROFILE_TIMING)
+    eng.reset()
+    eng.profile_render(w, h, spp_a, _abi.PROFILE_WORK)
+    cnt = eng.counters()
+    if rank == 0:
+        kernel, (kms, klaunch) = max(prof.items(), key=lambda kv: kv[1][0])
+        peak, peak_kind = measured_peaks()
+        launch_ms = kms / max(klaunch, 1)
+        bytes_per_launch = algorithmic_bytes(kernel, cnt) / max(klaunch, 1)
+        achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9
+        total_prof_ms = sum(v[0] for v in prof.values())
+        line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": adj_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "adjoint-c5: Cornell walls + ceiling light, 64 seeded spheres (Lambert RGB albedo / "
+                                       "GGX alpha / dielectric IOR) + one grey-medium sphere (sigma_t 2, albedo 0.9, g 0.6); "
+                                       "loss = L2 to a target at seeded +-10 % parameters; path-replay adjoint",
+                           "width": w, "height": h, "spp_primal": spp_p, "spp_adjoint": spp_a, "max_depth": 8,
+                           "parameters": int(mask.sum()), "color": "rgb",
+                           "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
+                           "step": "one adjoint pass (forward walk + replay + float64 gradient scatter) at 16 spp"},
+                "forward": {"value": samples / (fwd_ms / 1000.0), "unit": "samples/s", "ms_per_step": fwd_ms / args.steps,
+                            "adjoint_over_forward_cost": adj_ms / fwd_ms},
+                "loss": loss, "gradient_l2": float(np.linalg.norm(g[mask])),
+                "e2e": e2e, "clocks": clk,
+                "roofline": {"bound": "hbm", "kernel": "k_" + kernel + " (forward pass of the step)", "achieved": achieved,
+                             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                             "traffic": None, "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
+                             "share": {k: v[0] / total_prof_ms for k, v in prof.items()}},
+                "gpu_launches": args.steps * 2 * (sum(v[1] for v in prof.values()) + prof["film"][1])}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp_a)
+            line["cpu_baseline"]["sample"] = "forward only (the oracle has no adjoint): " + line["cpu_baseline"]["sample"]
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -491,6 +623,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

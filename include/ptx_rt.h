@@ -302,6 +302,39 @@ int ptr_get_stream(ptr_ctx* ctx, void** stream);
 int ptr_render_noalloc(const ptr_scene_desc* scene, const ptr_program_desc* prog, const ptr_frame* frame,
                        double* sum_dev, double* sumsq_dev, void* stream);
 
+/* ---- adjoint (path replay backpropagation) ----------------------------------------
+ * No counterpart in the reference (it renders only).  Parameters are per material,
+ * PTR_GRAD_SLOTS each, in material-table order; a slot that a material's model does not
+ * use receives 0.  The IOR gradient holds the interface terms (Fresnel lobe choice and
+ * the eta^2 radiance factor), not the refracted direction's own dependence on the IOR.
+ * Media must be grey (sigma_a, sigma_s equal in r, g, b); the medium's parameters are
+ * sigma_t = sigma_a + sigma_s and the single-scattering albedo sigma_s / sigma_t. */
+#define PTR_GRAD_SLOTS 8
+#define PTR_GRAD_ALBEDO_R 0        /* Lambert albedo r, g, b: slots 0, 1, 2         */
+#define PTR_GRAD_ALPHA 3           /* GGX alpha (materials without per-triangle alpha) */
+#define PTR_GRAD_IOR 4             /* dielectric IOR (interface terms)               */
+#define PTR_GRAD_SIGMA_T 5         /* grey homogeneous medium sigma_t               */
+#define PTR_GRAD_MEDIUM_ALBEDO 6   /* its single-scattering albedo                  */
+#define PTR_GRAD_HG_G 7            /* its HG asymmetry g                            */
+
+/* Gradient of a loss with respect to the scene's material parameters: renders
+ * frame->spp samples per pixel of the frame twice on the same random numbers — the
+ * forward walk, then its replay, which scatters dL_dimage[pixel] * d(sample)/d(theta) / spp
+ * into float64 accumulators — and writes grads[PTR_GRAD_SLOTS * material + slot]
+ * (n >= PTR_GRAD_SLOTS * n_materials doubles, host memory).  dL_dimage is host memory,
+ * 3 floats per pixel (row 0 at the bottom), typically 2 (I - target) / n for an L2 loss on
+ * an image I rendered with ptr_render.  The program's film is left untouched.  Synchronises.
+ * Not available for equiangular programs.  (The SURVEY's ptr_backward.) */
+int ptr_backward(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, const float* dL_dimage,
+                 double* grads, size_t n);
+
+/* Live parameters (ptr_set_params of the engine contract; UniformBinding.compute,
+ * src/compiler/types.ts:793-812, evaluated on the host): replace the uploaded material
+ * table and, when regions is not NULL, the regions' IOR values.  Shapes and counts must
+ * equal the uploaded scene's (PTR_E_INVALID otherwise).  Ordered on the context's stream. */
+int ptr_update_params(ptr_scene* scene, const ptr_material* materials, int n_materials,
+                      const ptr_region* regions, int n_regions);
+
 /* Wait for the context's stream, at most timeout_ms (<0 = no limit). */
 int ptr_sync(ptr_ctx* ctx, int timeout_ms);
 

@@ -35,6 +35,9 @@ SIGNATURES = {
     "ptr_get_batch_counters": (C.c_int, [C.c_void_p, C.POINTER(abi.Counters)]),
     "ptr_profile_batch_next": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_get_batch_profile": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int), C.c_int]),
+    "ptr_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame), C.POINTER(C.c_float),
+                               C.POINTER(C.c_double), C.c_size_t]),
+    "ptr_update_params": (C.c_int, [C.c_void_p, C.POINTER(abi.Material), C.c_int, C.POINTER(abi.Region), C.c_int]),
     "ptr_sync": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_read_export": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_float), C.c_size_t]),
     "ptr_read_export_device": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t]),

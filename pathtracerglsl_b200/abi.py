@@ -24,6 +24,10 @@ ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)
 DIRECT_NONE, DIRECT_NEE, DIRECT_MIS = range(3)
 ACCEL_BVH, ACCEL_CWBVH = range(2)
 EQUIANGULAR_OFF, EQUIANGULAR_DELTA, EQUIANGULAR_AREA = range(3)
+# adjoint parameter slots per material (include/ptx_rt.h PTR_GRAD_*)
+GRAD_SLOTS = 8
+GRAD_ALBEDO_R, GRAD_ALBEDO_G, GRAD_ALBEDO_B, GRAD_ALPHA, GRAD_IOR, GRAD_SIGMA_T, GRAD_MEDIUM_ALBEDO, GRAD_HG_G = range(8)
+GRAD_NAMES = ("albedo.r", "albedo.g", "albedo.b", "alpha", "ior", "sigma_t", "medium_albedo", "g")
 
 F4 = C.c_float * 4
 

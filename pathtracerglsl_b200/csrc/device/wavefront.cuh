@@ -20,6 +20,7 @@
 #pragma once
 #include "occupants.cuh"
 #include "bvh.cuh"
+#include "adjoint.cuh"
 
 namespace ptx {
 
@@ -52,6 +53,19 @@ struct PathPool {
     unsigned long long* stats; // [0] closest queries, [1] shadow queries, [2] paths
     long long* wave;   // [0] first global path index of the wave, [1] wave size
     int* job;          // batched renders: the job (scene x program x frame) of each path
+    // adjoint replay only (NULL otherwise)
+    float4* l_rem;     // radiance the path has still to gather (forward total minus what it gathered)
+    float4* dl;        // adjoint radiance of the path: dLoss/dI of its pixel / spp
+    float4* sh_g;      // shadow query: lobe derivative D = dlog f(wi_light) - dlog w_cont (xyz)
+    int* sh_gm;        // shadow query: vertex material | kind << 16
+};
+
+// Adjoint replay tables: the adjoint image (3 floats per pixel, row 0 at the bottom), the
+// per-sample scale and the float64 gradient buffer (PTR_GRAD_SLOTS per material).
+struct AdjParams {
+    const float* dl_image;
+    float inv_spp;
+    double* grads;
 };
 
 struct FrameParams {
@@ -279,7 +293,8 @@ __device__ __forceinline__ f3 medium_transmittance(const DevScene& S, const Prog
 // ---- kernels ---------------------------------------------------------------------------
 
 // Camera rays for one wave (accumulation.ts:14-26 cameraSample; pinhole.glsl:4-18).
-__global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp) {
+template <bool ADJ = false>
+__global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, AdjParams adj = AdjParams{}) {
     const FrameParams F = *fp;
     long long base = pool.wave[0];
     long long n = F.total - base;
@@ -311,6 +326,11 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp) {
                            ndcy * F.cam.tan_fov * ld3(F.cam.up));
         f3 o = ld3(F.cam.position);
         int medium = S.has_media ? scene_region_at(S, o) : -1;
+        if (ADJ) {   // replay: the forward pass left this path's total radiance in rad
+            pool.l_rem[i] = pool.rad[i];
+            const float* g = adj.dl_image + 3 * (size_t)pix;
+            pool.dl[i] = make_float4(g[0] * adj.inv_spp, g[1] * adj.inv_spp, g[2] * adj.inv_spp, 0.f);
+        }
         pool.ray_o[i] = f4(o, 0.0f);
         pool.ray_d[i] = f4(dir, 1.0f);
         pool.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
@@ -366,8 +386,14 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
 #ifndef PTR_SHADE_MIN_BLOCKS
 #define PTR_SHADE_MIN_BLOCKS 3
 #endif
-template <int DIRECT, bool MEDIA, bool BATCH>
-__global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt) {
+// ADJ: the replay pass of the adjoint — the same walk on the same random numbers, which
+// also scatters d Loss / d theta into per-block float64 accumulators (dynamic shared
+// memory: PTR_GRAD_SLOTS doubles per material).
+template <int DIRECT, bool MEDIA, bool BATCH, bool ADJ = false>
+__global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt,
+                                                                     AdjParams adj = AdjParams{}) {
+    extern __shared__ double s_grad[];
+    if (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[in];
     const int* q = pool.q[in];
     int* qout = pool.q[in ^ 1];
@@ -398,6 +424,15 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             Rng rng;
             rng.base = rs.x;
             rng.dim = rs.y;
+            f3 lrem(0.0f);
+            GradAcc ga;
+            int sh_kind = kGradKindNone, sh_mat = 0;
+            f3 sh_dnee(0.0f);   // dlog f at the light direction of this vertex's NEE query
+            if (ADJ) {
+                lrem = xyz(pool.l_rem[i]);
+                ga.s = s_grad;
+                ga.dl = xyz(pool.dl[i]);
+            }
             float4 hf = pool.hit[i];
             int4 hi = pool.hit_i[i];
             HitRec hr;
@@ -431,9 +466,24 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                     float t_max = boundary ? hr.t : kMaxDist;
                     if (!scatter_live(S, P, med_mat)) {
                         thr = thr * vexp(-ld3(mm.sigma_a) * t_max);
+                        if (ADJ) {   // w = exp(-(1-a) st t)
+                            GreyMedium gm = grey_medium(mm);
+                            ga.scl(med_mat, PTR_GRAD_SIGMA_T, lrem, -(1.0f - gm.a) * t_max);
+                            ga.scl(med_mat, PTR_GRAD_MEDIUM_ALBEDO, lrem, gm.st * t_max);
+                        }
                     } else {
                         MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
                         thr = thr * ms.weight;
+                        if (ADJ) {   // scattered at t: w = a st exp(-st t)/pdf; passed: exp(-st t_max)/P
+                            GreyMedium gm = grey_medium(mm);
+                            if (ms.scattered) {
+                                float t_evt = dot(ms.exit_p - r.o, r.d);
+                                ga.scl(med_mat, PTR_GRAD_SIGMA_T, lrem, 1.0f / gm.st - t_evt);
+                                ga.scl(med_mat, PTR_GRAD_MEDIUM_ALBEDO, lrem, 1.0f / gm.a);
+                            } else {
+                                ga.scl(med_mat, PTR_GRAD_SIGMA_T, lrem, -t_max);
+                            }
+                        }
                         if (ms.scattered) {
                             handled = true;
                             if (bounce == N) {
@@ -455,12 +505,22 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         pool.sh_lp[i] = f4(light_p, w);
                                         pool.sh_c[i] = f4(thr * ls.radiance * f3(ph), ls.pdf);
                                         shadow = true;
+                                        if (ADJ) {
+                                            sh_kind = kGradKindPhase;
+                                            sh_mat = med_mat;
+                                            sh_dnee = f3(hg_dlog_g(ls.wi, wo_med, mm.phase_g), 0.0f, 0.0f);
+                                        }
                                     }
                                 }
                                 float z0 = rng.next();
                                 float z1 = rng.next();
                                 ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
                                 thr = thr * ps.weight;
+                                if (ADJ) {   // phase continuation: w = p_HG / pdf_detached
+                                    float dg = hg_dlog_g(ps.wi, wo_med, mm.phase_g);
+                                    ga.scl(med_mat, PTR_GRAD_HG_G, lrem, dg);
+                                    if (shadow) sh_dnee.x -= dg;
+                                }
                                 prev_delta = false;
                                 prev_bsdf_pdf = ps.pdf;
                                 prev_qp = p_evt;
@@ -493,7 +553,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             w = power_heuristic(prev_bsdf_pdf, pe * env_pdf(S, r.d));
                         }
                     }
-                    rad = rad + thr * w * env_radiance(S, r.d);
+                    f3 e = thr * w * env_radiance(S, r.d);
+                    rad = rad + e;
+                    if (ADJ) lrem = lrem - e;
                     done = true;
                 } else {
                     if (MEDIA && hit.region_from != cur_med) cur_med = hit.region_from;
@@ -519,7 +581,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p));
                                 }
                             }
-                            rad = rad + thr * w * ld3(S.materials[mat_emit].emission);
+                            f3 e = thr * w * ld3(S.materials[mat_emit].emission);
+                            rad = rad + e;
+                            if (ADJ) lrem = lrem - e;
                         }
                         if (bounce == N) {
                             done = true;
@@ -550,6 +614,16 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     pool.sh_lp[i] = f4(light_p, w);
                                     pool.sh_c[i] = f4(thr * ls.radiance * f * cos_i, ls.pdf);
                                     shadow = true;
+                                    if (ADJ) {
+                                        sh_mat = mat;
+                                        if (m.model == PTR_MAT_LAMBERT) {
+                                            sh_kind = kGradKindAlbedo;
+                                            sh_dnee = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
+                                        } else if (hit.alpha < 0.0f) {
+                                            sh_kind = kGradKindAlpha;
+                                            sh_dnee = f3(ggx_dlog_alpha(ls.wi, wo, hit, alpha), 0.0f, 0.0f);
+                                        }
+                                    }
                                 }
                             }
                             // kernel_sample_continuation (kernel.glsl:27-34)
@@ -564,6 +638,27 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 done = true;
                             } else {
                                 thr = thr * bs.weight;
+                                if (ADJ) {   // the continuation lobe: d log w_cont
+                                    if (m.model == PTR_MAT_LAMBERT) {
+                                        f3 dlog = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
+                                        ga.vec(mat, PTR_GRAD_ALBEDO_R, lrem, dlog);
+                                        if (shadow) sh_dnee = sh_dnee - dlog;
+                                    } else if (m.model == PTR_MAT_GGX) {
+                                        if (hit.alpha < 0.0f) {
+                                            float da = ggx_dlog_alpha(bs.wi, wo, hit, alpha);
+                                            ga.scl(mat, PTR_GRAD_ALPHA, lrem, da);
+                                            if (shadow) sh_dnee.x -= da;
+                                        }
+                                    } else if (m.model == PTR_MAT_DIELECTRIC) {
+                                        const bool entering = hit.region_to == hit.region_owner;
+                                        if (entering || hit.region_from == hit.region_owner) {
+                                            float ci = dot(wo, hit.frame.n);
+                                            float d = dielectric_dlog_ior(ci, ior_of(S, hit.region_from), ior_of(S, hit.region_to),
+                                                                          entering, (bs.flags & kLobeTransmission) != 0u);
+                                            ga.scl(mat, PTR_GRAD_IOR, lrem, d);
+                                        }
+                                    }
+                                }
                                 prev_delta = (bs.flags & kLobeDelta) != 0u;
                                 prev_bsdf_pdf = bs.pdf;
                                 prev_qp = hit.p;
@@ -594,6 +689,13 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             }
             (void)done;
             pool.rad[i] = f4(rad, 0.0f);
+            if (ADJ) {
+                pool.l_rem[i] = f4(lrem, 0.0f);
+                if (shadow) {
+                    pool.sh_g[i] = f4(sh_dnee, 0.0f);
+                    pool.sh_gm[i] = sh_mat | (sh_kind << 16);
+                }
+            }
             if (alive) {
                 pool.ray_o[i] = f4(r.o, prev_bsdf_pdf);
                 pool.ray_d[i] = f4(r.d, eta_scale);
@@ -612,6 +714,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if (shadow2) pool.shq2[s2] = i;
         }
     }
+    if (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
 }
 
 // Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
@@ -620,9 +723,15 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
 // slot 1 reads the second shadow slot (the equiangular segment queries); its launch
 // precedes the slot-0 launch of the same iteration, so the two never add to one path's
 // radiance concurrently.
-template <bool MEDIA, bool COUNT, bool BATCH>
+// ADJ: the replay pass also folds the query's gradient terms — the lobe derivative D of
+// its vertex and d log T / d theta of every medium segment the shadow ray crossed.
+constexpr int kAdjMaxMedia = 4;            // distinct media one adjoint shadow query may cross
+constexpr unsigned kErrAdjMedia = 8u;      // ... more were crossed (their terms were dropped)
+template <bool MEDIA, bool COUNT, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt,
-                                                                      int slot) {
+                                                                      int slot, AdjParams adj = AdjParams{}) {
+    extern __shared__ double s_grad[];
+    if (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[slot ? 4 : 2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
     const int* shq = slot ? pool.shq2 : pool.shq;
@@ -640,6 +749,9 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
         sr.o = xyz(so);
         sr.d = xyz(sd);
         f3 vis;
+        int mm_id[kAdjMaxMedia];
+        float mm_len[kAdjMaxMedia];
+        int n_mm = 0;
         if (!MEDIA) {
             vis = scene_any(S, sr, so.w, COUNT ? &wk : nullptr) ? f3(0.0f) : f3(1.0f);
         } else {
@@ -656,7 +768,16 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 bool hit_boundary = hr.region >= 0 && hr.t < remaining;
                 float seg_len = hit_boundary ? hr.t : remaining;
                 int med_mat = material_of(S, medium);
-                if (mat_has_medium(S, med_mat)) T = T * medium_transmittance(S, P, med_mat, seg_len);
+                if (mat_has_medium(S, med_mat)) {
+                    T = T * medium_transmittance(S, P, med_mat, seg_len);
+                    if (ADJ) {
+                        int e = 0;
+                        while (e < n_mm && mm_id[e] != med_mat) e++;
+                        if (e < n_mm) mm_len[e] += seg_len;
+                        else if (n_mm < kAdjMaxMedia) { mm_id[n_mm] = med_mat; mm_len[n_mm] = seg_len; n_mm++; }
+                        else flag_error(S, kErrAdjMedia);
+                    }
+                }
                 if (!hit_boundary) { finished = true; break; }
                 Hit h;
                 fill_hit(S, seg, hr, h);
@@ -673,9 +794,32 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
             f3 add = xyz(c) * vis * w / c.w;
             float4 rr = pool.rad[i];
             pool.rad[i] = make_float4(rr.x + add.x, rr.y + add.y, rr.z + add.z, 0.f);
+            if (ADJ) {
+                GradAcc ga;
+                ga.s = s_grad;
+                ga.dl = xyz(pool.dl[i]);
+                float4 lr = pool.l_rem[i];
+                pool.l_rem[i] = make_float4(lr.x - add.x, lr.y - add.y, lr.z - add.z, 0.f);
+                const int gm = pool.sh_gm[i];
+                const int kind = gm >> 16, vmat = gm & 0xFFFF;
+                const f3 D = xyz(pool.sh_g[i]);
+                if (kind == kGradKindAlbedo) ga.vec(vmat, PTR_GRAD_ALBEDO_R, add, D);
+                else if (kind == kGradKindAlpha) ga.scl(vmat, PTR_GRAD_ALPHA, add, D.x);
+                else if (kind == kGradKindPhase) ga.scl(vmat, PTR_GRAD_HG_G, add, D.x);
+                for (int e = 0; e < n_mm; ++e) {   // T = exp(-st len) (scattering) or exp(-(1-a) st len)
+                    GreyMedium g = grey_medium(S.materials[mm_id[e]]);
+                    if (scatter_live(S, P, mm_id[e])) {
+                        ga.scl(mm_id[e], PTR_GRAD_SIGMA_T, add, -mm_len[e]);
+                    } else {
+                        ga.scl(mm_id[e], PTR_GRAD_SIGMA_T, add, -(1.0f - g.a) * mm_len[e]);
+                        ga.scl(mm_id[e], PTR_GRAD_MEDIUM_ALBEDO, add, g.st * mm_len[e]);
+                    }
+                }
+            }
         }
     }
     if (COUNT) flush_work(S0, wk);
+    if (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
 }
 
 // Fold the wave's per-path radiance into the film, per pixel in sample order; then

@@ -38,6 +38,8 @@ struct ptr_scene {
     int has_media = 0;
     int max_stack_depth = 0;
     int n_lights = 0, n_delta_lights = 0, env_samplable = 0;
+    std::vector<ptr_material> h_materials;   // host copies for ptr_update_params / ptr_backward
+    std::vector<ptr_region> h_regions;
 };
 
 struct ptr_program {
@@ -67,6 +69,11 @@ struct ptr_program {
     int profile_next = 0;
     float prof_ms[5] = {0, 0, 0, 0, 0};
     int prof_launches[5] = {0, 0, 0, 0, 0};
+    // adjoint
+    float* adj_dl = nullptr;          // W*H*3 adjoint image
+    size_t adj_dl_n = 0;
+    double* adj_grads = nullptr;      // PTR_GRAD_SLOTS per material
+    size_t adj_grads_n = 0;
 };
 
 namespace {
@@ -109,7 +116,7 @@ void free_pool(ptr_program* p) {
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
 }
 
-int alloc_pool(ptr_program* p, int capacity, bool slot2) {
+int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false) {
     free_pool(p);
     ptr_ctx* ctx = p->ctx;
     auto get = [&](size_t bytes, void** out) -> int {
@@ -142,6 +149,12 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2) {
         free_pool(p);
         return rc;
     }
+    // the adjoint replay's per-path records
+    if (adj && ((rc = get(c * 16, (void**)&q.l_rem)) || (rc = get(c * 16, (void**)&q.dl)) ||
+                (rc = get(c * 16, (void**)&q.sh_g)) || (rc = get(c * 4, (void**)&q.sh_gm)))) {
+        free_pool(p);
+        return rc;
+    }
     p->capacity = capacity;
     return PTR_OK;
 }
@@ -158,7 +171,7 @@ int wave_iterations(const ptr_program* p, const ptr_scene* s) {
 struct ProfRec { int cls; cudaEvent_t a, b; };
 
 void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
-                 std::vector<ProfRec>* prof = nullptr) {
+                 std::vector<ProfRec>* prof = nullptr, bool film = true) {
     DevScene Sp = s->dev;
     Sp.accel = p->desc.accel;
     Sp.work = (p->profile_next & PTR_PROFILE_WORK) ? p->work_dev : nullptr;
@@ -185,7 +198,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     const int grid = launch_grid(n_sm), block = 256;
     ProfRec* r = mark(0);
     const BatchTables nob{};
-    k_generate<<<grid, block, 0, st>>>(S, pool, p->fp_dev);
+    k_generate<false><<<grid, block, 0, st>>>(S, pool, p->fp_dev);
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
@@ -221,10 +234,50 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
             done(r);
         }
     }
+    if (!film) return;
     r = mark(4);
     k_film<<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples);
     k_advance<<<1, 32, 0, st>>>(pool);
     done(r);
+}
+
+// The adjoint's replay of one wave (after launch_wave(..., film = false) left every path's
+// forward radiance in the pool): the same kernels with ADJ = true, then the wave cursor.
+void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, int n_sm, const AdjParams& adj) {
+    DevScene S = s->dev;
+    S.accel = p->desc.accel;
+    S.work = nullptr;
+    const PathPool& pool = p->pool;
+    ProgParams P;
+    P.max_bounces = p->desc.max_bounces;
+    P.direct = p->desc.direct;
+    P.rr_start = p->desc.rr_start;
+    P.max_null = p->desc.max_null_crossings;
+    P.rr_max_survival = p->desc.rr_max_survival;
+    P.scattering = p->desc.scattering;
+    P.equiangular = 0;
+    const int grid = launch_grid(n_sm), block = 256;
+    const size_t smem = sizeof(double) * PTR_GRAD_SLOTS * (size_t)S.n_materials;
+    const BatchTables nob{};
+    const bool media = s->has_media != 0;
+    k_generate<true><<<grid, block, 0, st>>>(S, pool, p->fp_dev, adj);
+    for (int it = 0; it < iters; ++it) {
+        int in = it & 1;
+        k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
+        switch (P.direct * 2 + (media ? 1 : 0)) {
+            case 0: k_shade<PTR_DIRECT_NONE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 1: k_shade<PTR_DIRECT_NONE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 2: k_shade<PTR_DIRECT_NEE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 3: k_shade<PTR_DIRECT_NEE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 4: k_shade<PTR_DIRECT_MIS, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            default: k_shade<PTR_DIRECT_MIS, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+        }
+        if (P.direct != PTR_DIRECT_NONE) {
+            if (media) k_shadow<true, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
+            else k_shadow<false, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
+        }
+    }
+    k_advance<<<1, 32, 0, st>>>(pool);
 }
 
 // One wave of a batched render: the same kernel sequence over the concatenated job space;
@@ -566,7 +619,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     if (cap > total) cap = total;
     const bool slot2 = p->desc.equiangular != 0;
     if (p->capacity < cap || (slot2 && !p->pool.sh2_o)) {
-        int rc = alloc_pool(p, (int)cap, slot2);
+        int rc = alloc_pool(p, (int)cap, slot2, p->pool.l_rem != nullptr);
         if (rc) return rc;
     }
     if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
@@ -725,6 +778,8 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     S.has_media = media ? 1 : 0;
     s->has_media = S.has_media;
     s->n_lights = d->n_lights;
+    s->h_materials.assign(d->materials, d->materials + d->n_materials);
+    s->h_regions.assign(d->regions, d->regions + d->n_regions);
     for (int i = 0; i < d->n_lights; ++i) s->n_delta_lights += d->lights[i].kind == PTR_LIGHT_POINT ? 1 : 0;
     s->env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
     S.env_kind = d->env.kind;
@@ -804,6 +859,8 @@ int ptr_free_program(ptr_program* p) {
     if (p->export_buf) cudaFree(p->export_buf);
     if (p->fp_dev) cudaFree(p->fp_dev);
     if (p->work_dev) cudaFree(p->work_dev);
+    if (p->adj_dl) cudaFree(p->adj_dl);
+    if (p->adj_grads) cudaFree(p->adj_grads);
     delete p;
     return PTR_OK;
 }
@@ -1030,6 +1087,116 @@ int ptr_trace_closest(ptr_ctx* ctx, ptr_scene* s, int accel, const float* rays, 
 int ptr_get_stream(ptr_ctx* ctx, void** stream) {
     if (!ctx || !stream) return PTR_E_INVALID;
     *stream = (void*)ctx->stream;
+    return PTR_OK;
+}
+
+int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* dl_dimage, double* grads, size_t n) {
+    if (!p || !s || !f || !dl_dimage || !grads) return fail(p ? p->ctx : nullptr, PTR_E_INVALID, "ptr_backward: null argument");
+    ptr_ctx* ctx = p->ctx;
+    if (s->ctx != ctx) return fail(ctx, PTR_E_INVALID, "scene belongs to another context");
+    if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return fail(ctx, PTR_E_INVALID, "frame: width, height and spp must be positive");
+    const int n_mat = (int)s->h_materials.size();
+    if (n < (size_t)PTR_GRAD_SLOTS * n_mat)
+        return fail(ctx, PTR_E_INVALID, "ptr_backward: grads needs PTR_GRAD_SLOTS * n_materials doubles");
+    if (n_mat > 512) return fail(ctx, PTR_E_INVALID, "ptr_backward: at most 512 materials");
+    if (p->desc.equiangular) return fail(ctx, PTR_E_INVALID, "ptr_backward: equiangular programs are not differentiated");
+    for (const ptr_material& m : s->h_materials)
+        if ((m.flags & PTR_MATF_MEDIUM) && !(m.sigma_a[0] == m.sigma_a[1] && m.sigma_a[0] == m.sigma_a[2] &&
+                                             m.sigma_s[0] == m.sigma_s[1] && m.sigma_s[0] == m.sigma_s[2]))
+            return fail(ctx, PTR_E_INVALID, "ptr_backward: media must be grey (chromatic media are not differentiated)");
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t npix = (size_t)f->width * f->height;
+    const long long total = (long long)npix * f->spp;
+    long long cap_max = 1ll << 21;
+    if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
+    long long cap = (long long)npix <= cap_max ? (cap_max / (long long)npix) * (long long)npix : cap_max;
+    if (cap > total) cap = total;
+    if (p->capacity < cap || !p->pool.l_rem) {
+        int rc = alloc_pool(p, (int)std::max<long long>(cap, p->capacity), p->pool.sh2_o != nullptr, true);
+        if (rc) return rc;
+    }
+    if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
+    if (p->adj_dl_n < npix * 3) {
+        if (p->adj_dl) cudaFree(p->adj_dl);
+        p->adj_dl = nullptr;
+        if (cudaMalloc(&p->adj_dl, npix * 3 * sizeof(float)) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, "ptr_backward: adjoint image");
+        p->adj_dl_n = npix * 3;
+    }
+    const size_t ng = (size_t)PTR_GRAD_SLOTS * n_mat;
+    if (p->adj_grads_n < ng) {
+        if (p->adj_grads) cudaFree(p->adj_grads);
+        p->adj_grads = nullptr;
+        if (cudaMalloc(&p->adj_grads, ng * sizeof(double)) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, "ptr_backward: gradients");
+        p->adj_grads_n = ng;
+    }
+    // the graph of a previous ptr_render reads the same pool; it is re-captured on demand
+    FrameParams F;
+    F.width = f->width;
+    F.height = f->height;
+    F.spp = f->spp;
+    F.first_sample = f->first_sample;
+    F.salt = f->reset_salt;
+    F.px_off = f->pixel_offset[0];
+    F.py_off = f->pixel_offset[1];
+    F.total = total;
+    F.capacity = (int)cap;
+    F.cam = f->camera;
+    k_set_frame<<<1, 1, 0, st>>>(p->fp_dev, F);
+    CK(ctx, cudaGetLastError());
+    CK(ctx, cudaMemcpyAsync(p->adj_dl, dl_dimage, npix * 3 * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemsetAsync(p->adj_grads, 0, ng * sizeof(double), st));
+    CK(ctx, cudaMemsetAsync(p->pool.wave, 0, 64, st));
+    CK(ctx, cudaMemsetAsync(p->pool.stats, 0, 64, st));
+    CK(ctx, cudaMemsetAsync(p->pool.cnt, 0, 64, st));
+    AdjParams adj;
+    adj.dl_image = p->adj_dl;
+    adj.inv_spp = 1.0f / (float)f->spp;
+    adj.grads = p->adj_grads;
+    const int iters = wave_iterations(p, s);
+    const long long waves = (total + cap - 1) / cap;
+    const int n_sm = device_sms(ctx->device);
+    const int saved_profile = p->profile_next;
+    p->profile_next = 0;
+    for (long long w = 0; w < waves; ++w) {
+        launch_wave(p, s, st, iters, nullptr, n_sm, nullptr, false);
+        launch_replay(p, s, st, iters, n_sm, adj);
+    }
+    p->profile_next = saved_profile;
+    CK(ctx, cudaGetLastError());
+    CK(ctx, cudaMemcpyAsync(grads, p->adj_grads, ng * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaStreamSynchronize(st));
+    unsigned flags = 0;
+    if (s->dev.err_flags) CK(ctx, cudaMemcpy(&flags, s->dev.err_flags, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (flags) return fail(ctx, PTR_E_DEVICE, "ptr_backward: device guard flags " + std::to_string(flags));
+    for (size_t k = ng; k < n; ++k) grads[k] = 0.0;
+    return PTR_OK;
+}
+
+int ptr_update_params(ptr_scene* s, const ptr_material* materials, int n_materials, const ptr_region* regions, int n_regions) {
+    if (!s || !materials) return fail(s ? s->ctx : nullptr, PTR_E_INVALID, "ptr_update_params: null argument");
+    ptr_ctx* ctx = s->ctx;
+    if (n_materials != (int)s->h_materials.size()) return fail(ctx, PTR_E_INVALID, "ptr_update_params: material count differs from the uploaded scene");
+    for (int i = 0; i < n_materials; ++i)
+        if (materials[i].model != s->h_materials[i].model || materials[i].flags != s->h_materials[i].flags)
+            return fail(ctx, PTR_E_INVALID, "ptr_update_params: a material's model or flags changed");
+    if (regions) {
+        if (n_regions != (int)s->h_regions.size()) return fail(ctx, PTR_E_INVALID, "ptr_update_params: region count differs from the uploaded scene");
+        for (int i = 0; i < n_regions; ++i) {
+            const ptr_region& a = regions[i];
+            const ptr_region& b = s->h_regions[i];
+            if (a.shape != b.shape || a.material != b.material || a.thin != b.thin || a.ref != b.ref ||
+                std::memcmp(a.p, b.p, sizeof(a.p)) != 0)
+                return fail(ctx, PTR_E_INVALID, "ptr_update_params: only a region's IOR may change");
+        }
+    }
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    CK(ctx, cudaMemcpyAsync((void*)s->dev.materials, materials, sizeof(ptr_material) * n_materials, cudaMemcpyHostToDevice, st));
+    if (regions) CK(ctx, cudaMemcpyAsync((void*)s->dev.regions, regions, sizeof(ptr_region) * n_regions, cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaStreamSynchronize(st));   // the host arrays may be released on return
+    s->h_materials.assign(materials, materials + n_materials);
+    if (regions) s->h_regions.assign(regions, regions + n_regions);
     return PTR_OK;
 }
 

@@ -152,6 +152,37 @@ class CudaEngine:
                                              out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
         return out
 
+    # -- differentiation ---------------------------------------------------------------------
+    def backward(self, dl_dimage, width, height, spp, first_sample=0, salt=None):
+        """Path-replay adjoint: gradient of a loss whose derivative with respect to the
+        current renderer's image is ``dl_dimage`` ((H, W, 3), row 0 = bottom), estimated
+        from ``spp`` samples per pixel.  Returns an (n_materials, GRAD_SLOTS) float64 array
+        (slots: abi.GRAD_NAMES).  The film is left untouched."""
+        n_mat = len(self._scene_data.materials)
+        dl = np.ascontiguousarray(dl_dimage, dtype=np.float32)
+        if dl.shape != (height, width, 3):
+            raise ValueError(f"dl_dimage must have shape {(height, width, 3)}")
+        r = self.renderers[self.current]
+        fr = abi.Frame()
+        fr.width, fr.height, fr.spp = width, height, spp
+        fr.first_sample = first_sample
+        fr.reset_salt = (self.reset_salt if salt is None else salt) & 0xFFFFFFFF
+        fr.camera = r.camera(self.params, width, height)
+        g = np.zeros((n_mat, abi.GRAD_SLOTS), np.float64)
+        self._check(self.lib.ptr_backward(self.programs[self.current], self.scene, C.byref(fr),
+                                          dl.ctypes.data_as(C.POINTER(C.c_float)),
+                                          g.ctypes.data_as(C.POINTER(C.c_double)), g.size))
+        return g
+
+    def update_params(self, packed):
+        """Push a packed scene's (edited) material table and region IORs to the device
+        (the live-parameter path; shapes must be unchanged)."""
+        self._check(self.lib.ptr_update_params(
+            self.scene, packed.materials.ctypes.data_as(C.POINTER(abi.Material)), len(packed.materials),
+            packed.regions.ctypes.data_as(C.POINTER(abi.Region)), len(packed.regions)))
+        self._scene_data = packed
+        self.reset()
+
     KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film")
 
     def profile_render(self, width, height, spp, mode=abi.PROFILE_TIMING):

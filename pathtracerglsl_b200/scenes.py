@@ -259,3 +259,46 @@ BATCH_SIZE = 64
 def batch_scenes(n=BATCH_SIZE, seed=0, max_spheres=200):
     """The batched workload: `n` seeded Cornell-style scenes (``batch_scene``)."""
     return [batch_scene(seed * 100003 + k, max_spheres) for k in range(n)]
+
+
+# ------------------------------------------------------------------------- adjoint workload
+def adjoint_scene(seed=0, n_spheres=64, width=256, height=256, spp_primal=64, spp_adjoint=16, max_depth=8):
+    """The inverse-rendering workload: the Cornell box's walls and ceiling light with
+    `n_spheres` seeded non-overlapping spheres of radius U(0.06, 0.16), each with its own
+    material drawn uniformly from Lambert (albedo U(0.2, 0.9) per channel), GGX (alpha
+    U(0.05, 0.6), F0 (0.9, 0.6, 0.3)) and smooth dielectric (IOR U(1.3, 1.8)), plus one
+    sphere of radius 0.3 holding a grey homogeneous medium behind a null interface
+    (sigma_t 2.0, single-scattering albedo 0.9, HG g 0.6).  MIS, no roulette, max depth 8.
+    Returns (scene, strategy, (width, height, spp_primal, spp_adjoint))."""
+    rng = _np.random.RandomState(7000 + seed)
+    base, strategy = cornell(rr_start=None, max_depth=max_depth)
+    objects = list(base["objects"][:5])
+    materials = {k: base["materials"][k] for k in ("white", "red", "green")}
+    fog_c, fog_r = _np.array([0.0, 1.0, -0.2]), 0.3
+    placed = [(fog_c, fog_r)]
+    k = 0
+    while k < n_spheres:
+        r = float(rng.uniform(0.06, 0.16))
+        c = _np.array([rng.uniform(-1 + r, 1 - r), rng.uniform(r, 1.9 - r), rng.uniform(-1 + r, 1 - r)])
+        if not all(_np.linalg.norm(c - pc) > r + pr + 1e-3 for pc, pr in placed):
+            continue
+        placed.append((c, r))
+        kind = int(rng.randint(3))
+        name = f"s{k}"
+        if kind == 0:
+            materials[name] = {"model": "lambert", "albedo": [float(a) for a in rng.uniform(0.2, 0.9, 3)]}
+        elif kind == 1:
+            alpha = float(rng.uniform(0.05, 0.6))
+            materials[name] = {"model": "ggx", "f0": [0.9, 0.6, 0.3], "roughness": math.sqrt(alpha)}
+        else:
+            materials[name] = {"model": "dielectric", "ior": float(rng.uniform(1.3, 1.8))}
+        objects.append({"type": "sphere", "parameters": {"center": [float(x) for x in c], "radius": r},
+                        "material": name})
+        k += 1
+    materials["fog"] = {"model": "none", "medium": {"sigma_a": [0.2, 0.2, 0.2], "sigma_s": [1.8, 1.8, 1.8],
+                                                    "phase_g": 0.6}}
+    objects.append({"type": "sphere", "parameters": {"center": [float(x) for x in fog_c], "radius": fog_r},
+                    "material": "fog"})
+    scene = dict(base, id=f"adjoint-{seed}", objects=objects, materials=materials)
+    strategy = dict(strategy, id="adjoint-pt-mis")
+    return scene, strategy, (width, height, spp_primal, spp_adjoint)
