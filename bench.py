@@ -56,6 +56,17 @@ def workload(name):
                "max_depth": 12, "color": "rgb",
                "step": f"one {spp}-spp frame of the {spp_total}-spp configuration (samples/s is per sample)"}
         return sc, st, w, h, spp, cfg
+    if name == "media":
+        sc, st, (w, h, spp_total) = scenes.media_scene()
+        spp = 16
+        cfg = {"workload": "media-c3: dielectric sphere (IOR 1.33) holding a chromatic medium (sigma_t (0.5,1,2), "
+                           "albedo 0.9, HG g 0.6) + null-interface sphere with a grey medium (sigma_t 2), Lambert "
+                           "ground; sphere light r=0.05 emitting a 3000 K blackbody + 1x1 quad light of radiance 20; "
+                           "NEE with equiangular placement (area-light extension), RR from depth 3",
+               "width": w, "height": h, "spp": spp_total, "spp_per_step": spp, "max_depth": 64,
+               "color": "spectral: 4 hero wavelengths, visible (sech^2) density over 380-780 nm",
+               "step": f"one {spp}-spp frame of the {spp_total}-spp configuration (samples/s is per sample)"}
+        return sc, st, w, h, spp, cfg
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -360,7 +371,14 @@ def run_ours(args):
                          "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
                          "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
+            if args.workload == "media":   # the CPU restatement has no spectral model: its RGB walk
+                from pathtracerglsl_b200 import scenes as _sc
+                sc_rgb, st_rgb, _ = _sc.media_scene(spectral=False)
+                line["cpu_baseline"] = cpu_baseline(sc_rgb, st_rgb, w, h, spp)
+                line["cpu_baseline"]["sample"] = "RGB walk of the same scene (no spectral model on the CPU): " + \
+                    line["cpu_baseline"]["sample"]
+            else:
+                line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define PTR_ABI_VERSION 1
+#define PTR_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------------- */
 #define PTR_OK 0
@@ -133,6 +133,43 @@ typedef struct ptr_batch_desc {
     const float* placements;   /* 8*N: quaternion xyzw (world->local rigid), ts = (t_rigid.xyz, s) */
 } ptr_batch_desc;
 
+/* ---- spectral colour model (src/components/color/spectral, sensor/cie1931) ----------
+ * The host lifts every constant RGB colour of the scene once (the table lookup of
+ * lookup.glsl:15-36 over the shipped Jakob-Hanika atlas); the device evaluates
+ *   value(lambda) = scale * base(lambda) * (d65 ? D65(lambda) : 1)
+ * with base = 1 (PTR_SPEC_GREY: exact greys bypass the table), the bounded sigmoid
+ * clamp(0.5 + 0.5 p / sqrt(1 + p^2), 0, 1), p = (c0 t + c1) t + c2, t = (lambda - 360) / 470
+ * (PTR_SPEC_LIFTED), or Planck relative to 550 nm with c0 = kelvin and c1 = the unit-Y
+ * normalization (PTR_SPEC_BLACKBODY, blackbody.glsl:4-10). */
+#define PTR_COLOR_RGB 0
+#define PTR_COLOR_SPECTRAL 1
+#define PTR_WAVELENGTHS_VISIBLE 0   /* sech^2 density (visible.glsl:3-13)  */
+#define PTR_WAVELENGTHS_UNIFORM 1   /* uniform density (uniform.glsl:1-2)  */
+#define PTR_SPEC_GREY 0
+#define PTR_SPEC_LIFTED 1
+#define PTR_SPEC_BLACKBODY 2
+
+typedef struct ptr_spectrum {
+    int32_t kind;              /* PTR_SPEC_*                                              */
+    int32_t d65;               /* 1: multiply by the D65 curve (emission lift)            */
+    float scale;
+    float c[3];
+    int32_t pad[2];
+} ptr_spectrum;                /* 32 bytes */
+
+typedef struct ptr_spectral_material {
+    ptr_spectrum albedo, emission, transmittance, f0, sigma_a, sigma_s;
+} ptr_spectral_material;       /* 192 bytes; lifts of the ptr_material colours */
+
+typedef struct ptr_spectral_desc {
+    const ptr_spectral_material* materials;  /* n_materials                                */
+    const ptr_spectrum* lights;              /* n_lights: the lights' radiance / intensity  */
+    ptr_spectrum env;                        /* constant environment colour                 */
+    const float* curves;                     /* 95 x 4: CIE 1931 x, y, z and D65 at 5 nm from 360 nm */
+    float xyz_to_rgb[9];                     /* row-major, XYZ -> linear sRGB               */
+    float cie_y_integral;                    /* int ybar d lambda                           */
+} ptr_spectral_desc;
+
 typedef struct ptr_scene_desc {
     int32_t abi_version;       /* PTR_ABI_VERSION                                         */
     int32_t n_regions;
@@ -147,6 +184,7 @@ typedef struct ptr_scene_desc {
     const ptr_mesh_desc* meshes;
     int32_t n_batches;
     const ptr_batch_desc* batches;
+    const ptr_spectral_desc* spectral;  /* NULL: the scene renders in RGB only             */
 } ptr_scene_desc;
 
 /* ---- program (strategy) ---------------------------------------------------------- */
@@ -175,7 +213,11 @@ typedef struct ptr_program_desc {
     int32_t scattering;         /* measurement.scattering: 1 full, 0 ignored           */
     int32_t accel;              /* PTR_ACCEL_*  (meshTraversal / instanceAccel)        */
     int32_t equiangular;        /* PTR_EQUIANGULAR_*  (mediumLightSampling)            */
-    int32_t pad[7];
+    int32_t color;              /* PTR_COLOR_*  (measurement.color)                    */
+    int32_t wavelengths;        /* PTR_WAVELENGTHS_*  (estimator.wavelengths)          */
+    float lambda_min;           /* sampled range, nm (the reference's 360..830)        */
+    float lambda_max;
+    int32_t pad[3];
 } ptr_program_desc;
 
 /* The per-frame builtins + camera uniforms (Engine.ts:231-258, camera.ts:69-160). */

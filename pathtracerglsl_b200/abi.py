@@ -6,7 +6,7 @@ their descriptors from these types, so the two consume byte-identical scenes.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 PTR_OK = 0
 PTR_E_INVALID = -1
@@ -69,20 +69,42 @@ class BatchDesc(C.Structure):
                 ("placements", C.POINTER(C.c_float))]
 
 
+COLOR_RGB, COLOR_SPECTRAL = range(2)
+WAVELENGTHS_VISIBLE, WAVELENGTHS_UNIFORM = range(2)
+SPEC_GREY, SPEC_LIFTED, SPEC_BLACKBODY = range(3)
+
+
+class Spectrum(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("d65", C.c_int32), ("scale", C.c_float), ("c", C.c_float * 3),
+                ("pad", C.c_int32 * 2)]
+
+
+class SpectralMaterial(C.Structure):
+    _fields_ = [("albedo", Spectrum), ("emission", Spectrum), ("transmittance", Spectrum), ("f0", Spectrum),
+                ("sigma_a", Spectrum), ("sigma_s", Spectrum)]
+
+
+class SpectralDesc(C.Structure):
+    _fields_ = [("materials", C.POINTER(SpectralMaterial)), ("lights", C.POINTER(Spectrum)), ("env", Spectrum),
+                ("curves", C.POINTER(C.c_float)), ("xyz_to_rgb", C.c_float * 9), ("cie_y_integral", C.c_float)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("n_regions", C.c_int32), ("regions", C.POINTER(Region)),
                 ("n_materials", C.c_int32), ("materials", C.POINTER(Material)),
                 ("n_lights", C.c_int32), ("lights", C.POINTER(Light)),
                 ("ambient_material", C.c_int32), ("env", Env),
                 ("n_meshes", C.c_int32), ("meshes", C.POINTER(MeshDesc)),
-                ("n_batches", C.c_int32), ("batches", C.POINTER(BatchDesc))]
+                ("n_batches", C.c_int32), ("batches", C.POINTER(BatchDesc)),
+                ("spectral", C.POINTER(SpectralDesc))]
 
 
 class ProgramDesc(C.Structure):
     _fields_ = [("abi_version", C.c_int32), ("max_bounces", C.c_int32),
                 ("max_null_crossings", C.c_int32), ("direct", C.c_int32), ("rr_start", C.c_int32),
                 ("rr_max_survival", C.c_float), ("scattering", C.c_int32), ("accel", C.c_int32),
-                ("equiangular", C.c_int32), ("pad", C.c_int32 * 7)]
+                ("equiangular", C.c_int32), ("color", C.c_int32), ("wavelengths", C.c_int32),
+                ("lambda_min", C.c_float), ("lambda_max", C.c_float), ("pad", C.c_int32 * 3)]
 
 
 class Camera(C.Structure):
@@ -111,4 +133,5 @@ PROFILE_TIMING, PROFILE_WORK = 1, 2
 
 
 # Sizes the header documents (checked by the CPU tests).
-EXPECTED_SIZES = {"Region": 80, "Material": 128, "Light": 96}
+EXPECTED_SIZES = {"Region": 80, "Material": 128, "Light": 96, "Spectrum": 32, "SpectralMaterial": 192,
+                  "ProgramDesc": 64}

@@ -77,13 +77,34 @@ def resolve(v, params, default=None):
     return v
 
 
+_BUNDLED_SPECTRAL = None
+
+
+def _bundled_spectral():
+    global _BUNDLED_SPECTRAL
+    if _BUNDLED_SPECTRAL is None:
+        from .spectral import SpectralModel
+        _BUNDLED_SPECTRAL = SpectralModel.bundled()
+    return _BUNDLED_SPECTRAL
+
+
+def is_blackbody(v):
+    return isinstance(v, dict) and "blackbody" in v
+
+
 def rgb(v, params, default):
-    """A SpectrumProperty as RGB: scalars broadcast (types.ts SpectrumProperty)."""
+    """A SpectrumProperty as RGB: scalars broadcast (types.ts SpectrumProperty); a
+    ``{blackbody: {kelvin, scale}}`` emission becomes its RGB stand-in, the unit-Y Planck
+    colour times scale (spectra/blackbody/blackbody.ts blackbodyRGB)."""
     v = resolve(v, params, default)
     if v is None:
         v = default
     if isinstance(v, (int, float)):
         return [float(v)] * 3
+    if is_blackbody(v):
+        b = v["blackbody"]
+        return _bundled_spectral().blackbody_rgb(float(resolve(b.get("kelvin"), params, 6500.0)),
+                                                 float(resolve(b.get("scale"), params, 1.0)))
     if isinstance(v, dict):
         raise ValueError(f"unsupported spectrum value {v!r}")
     return [float(x) for x in v]
@@ -138,6 +159,7 @@ class PackedScene:
     batches: list = field(default_factory=list)
     region_names: list = field(default_factory=list)
     material_names: list = field(default_factory=list)
+    spectral: object = None     # spectral.SpectralTables of spectral strategies, else None
 
     def desc(self):
         """A ``ptr_scene_desc`` pointing into this object's arrays (keep self alive)."""
@@ -185,6 +207,9 @@ class PackedScene:
                 bd.placements = b["placements"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
             d.n_batches = len(self.batches)
             d.batches = self._batch_arr
+        if self.spectral is not None:
+            self._spec_desc = self.spectral.desc()
+            d.spectral = abi.C.pointer(self._spec_desc)
         return d
 
 
@@ -225,7 +250,13 @@ class CompiledScene:
 # ----------------------------------------------------------------------------- compiler
 
 class Compiler:
-    """``Compiler.compile`` / ``compileScene`` (src/compiler/Compiler.ts:14-72)."""
+    """``Compiler.compile`` / ``compileScene`` (src/compiler/Compiler.ts:14-72).
+
+    ``spectral_model``: the spectral colour model spectral strategies lift colours with
+    (``spectral.SpectralModel``; default: the package's bundled subset)."""
+
+    def __init__(self, spectral_model=None):
+        self.spectral_model = spectral_model
 
     def compile(self, scene, strategy, params=None):
         out = self.compile_scene(scene, [strategy], params)
@@ -285,8 +316,17 @@ class Compiler:
             ms = rr.get("maxSurvival", 0.95)
             if not (0.0 < ms <= 1.0):
                 bag.error("invalid-setting", "russianRoulette.maxSurvival must be in (0, 1]")
-        if meas.get("color", "rgb") != "rgb":
-            bag.error("unsupported", "measurement.color 'spectral' is not available in this build")
+        color = meas.get("color", "rgb")
+        if color not in ("rgb", "spectral"):
+            bag.error("invalid-setting", f"measurement.color {color!r} (available: rgb, spectral)")
+        if color == "spectral":
+            if scene.get("environment", {}).get("type", "none") not in ("none", "constant"):
+                bag.error("unsupported", "spectral rendering supports constant environments only")
+            if est.get("wavelengths", "visible") not in ("visible", "uniform"):
+                bag.error("invalid-setting", f"estimator.wavelengths {est.get('wavelengths')!r} (available: visible, uniform)")
+            lo, hi = meas.get("wavelengthRange", [360.0, 830.0])
+            if not (360.0 <= lo < hi <= 830.0):
+                bag.error("invalid-setting", "measurement.wavelengthRange must lie in [360, 830] nm")
         vs = est.get("volumeSampling", "analytic")
         if vs not in ("analytic", None):
             bag.error("unsupported", f"volumeSampling {vs!r} is not available in this build")
@@ -319,8 +359,10 @@ class Compiler:
         mat_names = list(mats_src.keys())
         mat_index = {n: i for i, n in enumerate(mat_names)}
         materials = []
+        spec_src = []          # per material: the authored material, or a light's raw emission
         for n in mat_names:
             materials.append(self._material(mats_src[n], params))
+            spec_src.append(("material", mats_src[n]))
 
         regions, region_names, lights = [], [], []
         meshes, batches = [], []
@@ -378,6 +420,7 @@ class Compiler:
                 vals = list(corner) + list(e1) + list(e2) + nrm + [area]
                 rec.p = (abi.C.c_float * 16)(*vals)
                 materials.append(self._light_material(e))
+                spec_src.append(("light", l.get("emission", 1.0)))
                 reg = abi.Region()
                 reg.shape = abi.SHAPE_QUAD
                 reg.thin = 1
@@ -393,6 +436,7 @@ class Compiler:
                 rad = l["radius"]
                 rec.p = (abi.C.c_float * 16)(*(list(center) + [rad]))
                 materials.append(self._light_material(e))
+                spec_src.append(("light", l.get("emission", 1.0)))
                 reg = abi.Region()
                 reg.shape = abi.SHAPE_SPHERE
                 reg.thin = 0
@@ -406,7 +450,7 @@ class Compiler:
             else:   # point: delta, registry entry only
                 rec.p = (abi.C.c_float * 16)(*list(l["position"]))
                 geom = None
-            lights.append((rec, kind, e, geom))
+            lights.append((rec, kind, e, geom, l.get("emission", 1.0)))
         for i, o in enumerate(scene.get("objects", [])):
             if o.get("kind") is not None:
                 continue
@@ -431,7 +475,7 @@ class Compiler:
                 area = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
                 rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:12]) + [area]))
                 geom = area
-            lights.append((rec, o["type"], e, geom))
+            lights.append((rec, o["type"], e, geom, m.get("emission")))
 
         # Selection CDF (features/lighting.ts computeSelectPdf; power per kind from the
         # descriptors: quad pi*A*Le, sphere pi*4*pi*r^2*Le, point 4*pi*I).
@@ -439,12 +483,12 @@ class Compiler:
         for st in strategies:
             sel_mode = st.get("estimator", {}).get("lightSelection", "power")
         weights = [1.0 if sel_mode == "uniform" else _light_power(rec.kind, e, geom)
-                   for rec, kind, e, geom in lights]
+                   for rec, kind, e, geom, _raw in lights]
         total = sum(weights)
         acc = 0.0
         light_arr = np.zeros(len(lights), dtype=np.dtype((np.void, abi.C.sizeof(abi.Light))))
         light_recs = (abi.Light * max(len(lights), 1))()
-        for i, (rec, kind, e, geom) in enumerate(lights):
+        for i, (rec, kind, e, geom, _raw) in enumerate(lights):
             pdf = weights[i] / total
             acc += pdf
             rec.select_pdf = pdf
@@ -462,7 +506,46 @@ class Compiler:
             env=env, meshes=meshes, batches=batches,
             region_names=region_names, material_names=mat_names,
         )
+        if any(st.get("measurement", {}).get("color", "rgb") == "spectral" for st in strategies):
+            packed.spectral = self._spectral_tables(spec_src, [raw for *_x, raw in lights],
+                                                    scene.get("environment") or {"type": "none"}, params)
         return packed
+
+    # -- the spectral colour model: every constant colour lifted once (lookup.glsl:38-59)
+    def _spectral_tables(self, spec_src, light_raw, env, params):
+        model = self.spectral_model or _bundled_spectral()
+
+        def emission(v, default):
+            v = resolve(v, params, default)
+            if is_blackbody(v):
+                b = v["blackbody"]
+                return model.blackbody(float(resolve(b.get("kelvin"), params, 6500.0)),
+                                       float(resolve(b.get("scale"), params, 1.0)))
+            return model.emission(rgb(v, params, default))
+
+        mats = []
+        for kind, src in spec_src:
+            sm = abi.SpectralMaterial()
+            if kind == "light":
+                sm.albedo = model.reflectance([0.0, 0.0, 0.0])
+                sm.emission = emission(src, 1.0)
+                sm.transmittance = model.reflectance([1.0, 1.0, 1.0])
+                sm.f0 = model.reflectance([0.9, 0.9, 0.9])
+                sm.sigma_a = sm.sigma_s = model.coefficient([0.0, 0.0, 0.0])
+            else:
+                m = src
+                sm.albedo = model.reflectance(rgb(m.get("albedo"), params, [0.8, 0.8, 0.8]))
+                sm.emission = emission(m.get("emission"), [0.0, 0.0, 0.0])
+                sm.transmittance = model.reflectance(rgb(m.get("transmittance"), params, [1.0, 1.0, 1.0]))
+                sm.f0 = model.reflectance(rgb(m.get("f0"), params, [0.9, 0.9, 0.9]))
+                med = m.get("medium") or {}
+                sm.sigma_a = model.coefficient(rgb(med.get("sigma_a"), params, [0.0, 0.0, 0.0]))
+                sm.sigma_s = model.coefficient(rgb(med.get("sigma_s"), params, [0.0, 0.0, 0.0]))
+            mats.append(sm)
+        lights = [emission(raw, 1.0) for raw in light_raw]
+        env_spec = model.emission(rgb(env.get("color"), params, [1.0, 1.0, 1.0])) \
+            if env.get("type") == "constant" else model.coefficient([0.0, 0.0, 0.0])
+        return model.spectral_desc(mats, lights, env_spec)
 
     def _primitive(self, o, params):
         t = o["type"]
@@ -640,7 +723,7 @@ class Compiler:
                     extent += max(v) if isinstance(v, (list, tuple)) else float(v)
             r = max(r, center + extent)
         phi_env = 4 * math.pi * math.pi * r * r * mean_l * intensity
-        phi_fin = sum(_light_power(rec.kind, e, geom) for rec, kind, e, geom in lights)
+        phi_fin = sum(_light_power(rec.kind, e, geom) for rec, kind, e, geom, _raw in lights)
         return min(0.99, max(0.01, phi_env / max(phi_env + phi_fin, 1e-20)))
 
     # -- Generate: the program description (flags of plan/types.ts:39-112) -------------
@@ -657,6 +740,10 @@ class Compiler:
         prog.rr_max_survival = float(rr.get("maxSurvival", 0.95)) if rr else 1.0
         prog.scattering = 0 if meas.get("scattering") == "ignored" else 1
         prog.accel = ACCELS[est.get("meshTraversal") or est.get("instanceAccel") or "bvh"]
+        prog.color = abi.COLOR_SPECTRAL if meas.get("color", "rgb") == "spectral" else abi.COLOR_RGB
+        prog.wavelengths = abi.WAVELENGTHS_UNIFORM if est.get("wavelengths") == "uniform" else abi.WAVELENGTHS_VISIBLE
+        lo, hi = meas.get("wavelengthRange", [360.0, 830.0])
+        prog.lambda_min, prog.lambda_max = float(lo), float(hi)
         prog.equiangular = abi.EQUIANGULAR_OFF
         if est.get("mediumLightSampling") == "equiangular":
             prog.equiangular = abi.EQUIANGULAR_AREA if est.get("equiangularAreaLights") else abi.EQUIANGULAR_DELTA

@@ -43,6 +43,24 @@ __device__ __forceinline__ f3 ld3(const float* p) { return f3(p[0], p[1], p[2]);
 __device__ __forceinline__ f3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
 __device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
+// The spectral colour model's carrier: four wavelength lanes (color/spectral/types.glsl,
+// Spectrum = vec4), with the same component-wise operations as the RGB f3.
+struct s4 {
+    float x, y, z, w;
+    __host__ __device__ s4() : x(0.f), y(0.f), z(0.f), w(0.f) {}
+    __host__ __device__ s4(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+    __host__ __device__ explicit s4(float s) : x(s), y(s), z(s), w(s) {}
+    __device__ float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
+};
+__device__ __forceinline__ s4 operator+(s4 a, s4 b) { return s4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ s4 operator-(s4 a, s4 b) { return s4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+__device__ __forceinline__ s4 operator*(s4 a, s4 b) { return s4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+__device__ __forceinline__ s4 operator/(s4 a, s4 b) { return s4(a.x / b.x, a.y / b.y, a.z / b.z, a.w / b.w); }
+__device__ __forceinline__ s4 operator*(s4 a, float s) { return s4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ s4 operator*(float s, s4 a) { return s4(s * a.x, s * a.y, s * a.z, s * a.w); }
+__device__ __forceinline__ s4 operator/(s4 a, float s) { return s4(a.x / s, a.y / s, a.z / s, a.w / s); }
+__device__ __forceinline__ s4 operator-(s4 a) { return s4(-a.x, -a.y, -a.z, -a.w); }
+
 // Scalar constants of the reference's core math (glsl/core/math.glsl).
 constexpr float kPi = 3.14159265359f;
 constexpr float kTwoPi = 6.28318530718f;
@@ -61,6 +79,21 @@ __device__ __forceinline__ float spectrum_average(f3 s) { float a = s.x; a += s.
 __device__ __forceinline__ float spectrum_max(f3 s) { float m = s.z; m = gmax(s.y, m); m = gmax(s.x, m); return m; }
 __device__ __forceinline__ bool spectrum_is_black(f3 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f; }
 __device__ __forceinline__ int spectrum_sample_channel(float u) { int c = (int)(u * 3.0f); return c < 2 ? c : 2; }
+__device__ __forceinline__ float spectrum_average(s4 s) { float a = s.x; a += s.y; a += s.z; a += s.w; return a * (1.0f / 4.0f); }
+__device__ __forceinline__ float spectrum_max(s4 s) { float m = s.w; m = gmax(s.z, m); m = gmax(s.y, m); m = gmax(s.x, m); return m; }
+__device__ __forceinline__ bool spectrum_is_black(s4 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f && s.w <= 0.f; }
+__device__ __forceinline__ s4 vexp(s4 a) { return s4(expf(a.x), expf(a.y), expf(a.z), expf(a.w)); }
+__device__ __forceinline__ s4 vmax(s4 a, s4 b) { return s4(gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z), gmax(a.w, b.w)); }
+// Uniform lane choice for channel-MIS: min(int(u * N), N - 1).
+template <class Col> __device__ __forceinline__ int sample_channel(float u);
+template <> __device__ __forceinline__ int sample_channel<f3>(float u) { return spectrum_sample_channel(u); }
+template <> __device__ __forceinline__ int sample_channel<s4>(float u) { int c = (int)(u * 4.0f); return c < 3 ? c : 3; }
+// Pool records: colours live in float4 slots (RGB uses xyz).
+template <class Col> __device__ __forceinline__ Col col_ld(float4 v);
+template <> __device__ __forceinline__ f3 col_ld<f3>(float4 v) { return f3(v.x, v.y, v.z); }
+template <> __device__ __forceinline__ s4 col_ld<s4>(float4 v) { return s4(v.x, v.y, v.z, v.w); }
+__device__ __forceinline__ float4 col_st(f3 c, float w) { return make_float4(c.x, c.y, c.z, w); }
+__device__ __forceinline__ float4 col_st(s4 c, float) { return make_float4(c.x, c.y, c.z, c.w); }
 
 // ---- counter-based sampler: the pcg4d hash of Jarzynski & Olano ("Hash Functions for
 // GPU Rendering", JCGT 2020), keyed per (pixel, sample, reset salt) with a dimension
@@ -120,8 +153,9 @@ __device__ __forceinline__ float dielectric_fresnel(float cos_i, float eta) {
     float r_perp = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
     return 0.5f * (r_par * r_par + r_perp * r_perp);
 }
-__device__ __forceinline__ f3 schlick_fresnel(f3 f0, float c) {
-    return f0 + (f3(1.0f) - f0) * powf(1.0f - c, 5.0f);
+template <class Col>
+__device__ __forceinline__ Col schlick_fresnel(Col f0, float c) {
+    return f0 + (Col(1.0f) - f0) * powf(1.0f - c, 5.0f);
 }
 __device__ __forceinline__ float power_heuristic(float pf, float pg) {
     float f2 = pf * pf;

@@ -8,15 +8,78 @@
 
 namespace ptx {
 
-struct ISample { f3 wi; f3 weight; float pdf; uint32_t flags; };
-struct LightSample { f3 wi; float distance; f3 radiance; float pdf; uint32_t flags; int light_id; };
+template <class Col = f3> struct ISample { f3 wi; Col weight; float pdf; uint32_t flags; };
+template <class Col = f3> struct LightSample { f3 wi; float distance; Col radiance; float pdf; uint32_t flags; int light_id; };
+
+// ---- colour models ---------------------------------------------------------------------
+// RGB reads the material/light records' rgb directly; the spectral model evaluates the
+// host-lifted ptr_spectrum of each colour at the path's four wavelengths
+// (color/spectral/lookup.glsl:38-59, spectra/blackbody/blackbody.glsl:4-10).
+struct Wl { float4 lambda; };
+
+__device__ __forceinline__ float4 spectral_curves(const DevScene& S, float lambda) {
+    float x = (lambda - 360.0f) / 5.0f;
+    int i = (int)x;
+    i = i < 93 ? i : 93;
+    float4 a = __ldg(S.spec_curves + i), b = __ldg(S.spec_curves + i + 1);
+    float f = x - (float)i;
+    return make_float4(a.x * (1.0f - f) + b.x * f, a.y * (1.0f - f) + b.y * f, a.z * (1.0f - f) + b.z * f,
+                       a.w * (1.0f - f) + b.w * f);
+}
+__device__ __forceinline__ float spec_lane(const DevScene& S, const ptr_spectrum& sp, float lambda) {
+    float v;
+    if (sp.kind == PTR_SPEC_LIFTED) {
+        float t = (lambda - 360.0f) / 470.0f;
+        float p = (sp.c[0] * t + sp.c[1]) * t + sp.c[2];
+        v = clampf(0.5f + 0.5f * p / sqrtf(1.0f + p * p), 0.0f, 1.0f);
+        v = sp.scale * v;
+    } else if (sp.kind == PTR_SPEC_BLACKBODY) {
+        float q = 14387768.775039338f / sp.c[0];
+        float ratio = 550.0f / lambda;
+        float ratio2 = ratio * ratio;
+        v = sp.c[1] * (expf(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (expf(q / lambda) - 1.0f);
+        v = sp.scale * v;
+    } else {
+        v = sp.scale;
+    }
+    if (sp.d65) v = v * spectral_curves(S, lambda).w;
+    return v;
+}
+__device__ __forceinline__ s4 spec_eval(const DevScene& S, const ptr_spectrum& sp, const Wl& wl) {
+    return s4(spec_lane(S, sp, wl.lambda.x), spec_lane(S, sp, wl.lambda.y), spec_lane(S, sp, wl.lambda.z),
+              spec_lane(S, sp, wl.lambda.w));
+}
+
+template <class Col> struct Colors;
+template <> struct Colors<f3> {
+    __device__ static f3 albedo(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].albedo); }
+    __device__ static f3 emission(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].emission); }
+    __device__ static f3 tint(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].transmittance); }
+    __device__ static f3 f0(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].f0); }
+    __device__ static f3 sigma_a(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].sigma_a); }
+    __device__ static f3 sigma_s(const DevScene& S, int mi, const Wl&) { return ld3(S.materials[mi].sigma_s); }
+    __device__ static f3 light(const DevScene& S, int li, const Wl&) { return ld3(S.lights[li].radiance); }
+    __device__ static f3 env_color(const DevScene& S, const Wl&) { return ld3(S.env_color); }
+};
+template <> struct Colors<s4> {
+    __device__ static s4 albedo(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].albedo, w); }
+    __device__ static s4 emission(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].emission, w); }
+    __device__ static s4 tint(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].transmittance, w); }
+    __device__ static s4 f0(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].f0, w); }
+    __device__ static s4 sigma_a(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].sigma_a, w); }
+    __device__ static s4 sigma_s(const DevScene& S, int mi, const Wl& w) { return spec_eval(S, S.spec_mats[mi].sigma_s, w); }
+    __device__ static s4 light(const DevScene& S, int li, const Wl& w) { return spec_eval(S, S.spec_lights[li], w); }
+    __device__ static s4 env_color(const DevScene& S, const Wl& w) { return spec_eval(S, S.spec_env, w); }
+};
 
 // ---- Lambert (materials/lambert/lambert.glsl:7-37) --------------------------------------
-__device__ __forceinline__ f3 lambert_eval(f3 wi, f3 wo, const Hit& h, const ptr_material& m) {
-    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return f3(0.0f);
-    return ld3(m.albedo) * (1.0f / kPi);
+template <class Col>
+__device__ __forceinline__ Col lambert_eval(f3 wi, f3 wo, const Hit& h, Col albedo) {
+    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return Col(0.0f);
+    return albedo * (1.0f / kPi);
 }
-__device__ __forceinline__ ISample lambert_sample(f3 wo, const Hit& h, const ptr_material& m, float u0, float u1) {
+template <class Col>
+__device__ __forceinline__ ISample<Col> lambert_sample(f3 wo, const Hit& h, Col albedo, float u0, float u1) {
     f3 n = dot(wo, h.frame.n) < 0.0f ? -h.frame.n : h.frame.n;
     float cos_theta = sqrtf(u1);
     float sin_theta = sqrtf(gmax(0.0f, 1.0f - u1));
@@ -24,9 +87,9 @@ __device__ __forceinline__ ISample lambert_sample(f3 wo, const Hit& h, const ptr
     float sp, cp;
     sp = sinf(phi);
     cp = cosf(phi);
-    ISample s;
+    ISample<Col> s;
     s.wi = normalize(h.frame.t * (sin_theta * cp) + h.frame.b * (sin_theta * sp) + n * cos_theta);
-    s.weight = ld3(m.albedo);
+    s.weight = albedo;
     s.pdf = cos_theta * (1.0f / kPi);
     s.flags = kLobeReflection;
     return s;
@@ -63,23 +126,25 @@ __device__ __forceinline__ f3 mf_sample_vndf(f3 wol, float a, float u0, float u1
     f3 nh = t1 * T1 + t2 * T2 + sqrtf(gmax(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
     return normalize(f3(a * nh.x, a * nh.y, gmax(1e-6f, nh.z)));
 }
-__device__ __forceinline__ f3 ggx_eval(f3 wi, f3 wo, const Hit& h, f3 f0, float a) {
+template <class Col>
+__device__ __forceinline__ Col ggx_eval(f3 wi, f3 wo, const Hit& h, Col f0, float a) {
     f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return f3(0.0f);
+    if (wil.z * wol.z <= 0.0f) return Col(0.0f);
     f3 hh = normalize(wil + wol);
-    f3 F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
+    Col F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
     return F * (mf_D(hh, a) * mf_G1(wil, a) * mf_G1(wol, a) / (4.0f * fabsf(wil.z) * fabsf(wol.z)));
 }
-__device__ __forceinline__ ISample ggx_sample(f3 wo, const Hit& h, f3 f0, float a, float u0, float u1) {
+template <class Col>
+__device__ __forceinline__ ISample<Col> ggx_sample(f3 wo, const Hit& h, Col f0, float a, float u0, float u1) {
     f3 wol = mf_to_local(h.frame, wo);
     float side = wol.z < 0.0f ? -1.0f : 1.0f;
     wol = wol * side;
     f3 hh = mf_sample_vndf(wol, a, u0, u1);
     f3 i = -wol;
     f3 wil = i - 2.0f * dot(hh, i) * hh;
-    ISample s;
-    if (wil.z <= 0.0f) { s.wi = wo; s.weight = f3(0.0f); s.pdf = 0.0f; s.flags = kLobeReflection; return s; }
-    f3 F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
+    ISample<Col> s;
+    if (wil.z <= 0.0f) { s.wi = wo; s.weight = Col(0.0f); s.pdf = 0.0f; s.flags = kLobeReflection; return s; }
+    Col F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
     s.weight = F * mf_G1(wil, a);
     s.pdf = mf_G1(wol, a) * mf_D(hh, a) / (4.0f * fabsf(wol.z));
     s.flags = kLobeReflection;
@@ -94,16 +159,16 @@ __device__ __forceinline__ float ggx_pdf(f3 wi, f3 wo, const Hit& h, float a) {
 }
 
 // ---- smooth dielectric with the eta^2 radiance factor (dielectric.glsl:14-52) ----------
-__device__ __forceinline__ ISample dielectric_sample(f3 wo, const Hit& h, const ptr_material& m,
-                                                     float n_i, float n_t, float uc) {
+template <class Col>
+__device__ __forceinline__ ISample<Col> dielectric_sample(f3 wo, const Hit& h, Col tint, float n_i, float n_t, float uc) {
     float eta = n_i / n_t;
     f3 n = h.frame.n;
     float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
     float F = dielectric_fresnel(cos_i, eta);
-    ISample s;
+    ISample<Col> s;
     if (uc < F) {
         s.wi = normalize(2.0f * cos_i * n - wo);
-        s.weight = f3(1.0f);
+        s.weight = Col(1.0f);
         s.pdf = 0.0f;
         s.flags = kLobeReflection | kLobeDelta;
     } else {
@@ -111,7 +176,7 @@ __device__ __forceinline__ ISample dielectric_sample(f3 wo, const Hit& h, const 
         float cos_t = sqrtf(gmax(0.0f, 1.0f - sin2_t));
         s.wi = normalize(-eta * wo + (eta * cos_i - cos_t) * n);
         float radiance_scale = (n_i * n_i) / (n_t * n_t);
-        s.weight = ld3(m.transmittance) * radiance_scale;
+        s.weight = tint * radiance_scale;
         s.pdf = 0.0f;
         s.flags = kLobeTransmission | kLobeDelta;
     }
@@ -124,7 +189,8 @@ __device__ __forceinline__ float hg_eval(f3 wi, f3 wo, float g) {
     float d = 1.0f + g * g - 2.0f * g * c;
     return (1.0f - g * g) / (4.0f * kPi * d * sqrtf(gmax(d, 1e-8f)));
 }
-__device__ __forceinline__ ISample hg_sample(f3 wo, float g, float x0, float x1) {
+template <class Col>
+__device__ __forceinline__ ISample<Col> hg_sample(f3 wo, float g, float x0, float x1) {
     float cos_theta;
     if (fabsf(g) < 1e-3f) {
         cos_theta = 1.0f - 2.0f * x0;
@@ -136,11 +202,11 @@ __device__ __forceinline__ ISample hg_sample(f3 wo, float g, float x0, float x1)
     float phi = kTwoPi * x1;
     f3 t, b;
     build_basis(-wo, t, b);
-    ISample s;
+    ISample<Col> s;
     s.wi = normalize(t * (sin_theta * cosf(phi)) + b * (sin_theta * sinf(phi)) + (-wo) * cos_theta);
-    s.weight = f3(1.0f);
+    s.weight = Col(1.0f);
     float e = hg_eval(s.wi, wo, g);
-    s.pdf = spectrum_average(f3(e));
+    s.pdf = spectrum_average(Col(e));
     s.flags = kLobeMedium;
     return s;
 }
@@ -175,10 +241,15 @@ __device__ __forceinline__ f3 env_map_bilinear(const DevScene& S, float2 uv) {
     f3 bot = xyz(c01) * (1.0f - ax) + xyz(c11) * ax;
     return top * (1.0f - ay) + bot * ay;
 }
-__device__ __forceinline__ f3 env_radiance(const DevScene& S, f3 dir) {
-    if (S.env_kind == PTR_ENV_CONSTANT) return ld3(S.env_color) * S.env_intensity;
-    if (S.env_kind == PTR_ENV_IMAGE) return env_map_bilinear(S, equirect_uv(S, dir)) * S.env_intensity;
-    return f3(0.0f);
+// The spectral model supports the constant environment only (image environments are
+// rejected on the host).
+template <class Col>
+__device__ __forceinline__ Col env_radiance(const DevScene& S, f3 dir, const Wl& wl) {
+    if (S.env_kind == PTR_ENV_CONSTANT) return Colors<Col>::env_color(S, wl) * S.env_intensity;
+    if constexpr (sizeof(Col) == sizeof(f3)) {
+        if (S.env_kind == PTR_ENV_IMAGE) return env_map_bilinear(S, equirect_uv(S, dir)) * S.env_intensity;
+    }
+    return Col(0.0f);
 }
 __device__ __forceinline__ float env_marg(const DevScene& S, int j) { return __ldg(S.env_marg + j); }
 __device__ __forceinline__ float env_cond(const DevScene& S, int j, int i) { return __ldg(S.env_cond + (size_t)j * S.env_w + i); }
@@ -242,8 +313,9 @@ __device__ __forceinline__ float env_pdf(const DevScene& S, f3 dir) {
     float a = env_uniform_fraction(S);
     return (1.0f - a) * env_table_pdf(S, dir) + a / (4.0f * kPi);
 }
-__device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, float x1) {
-    LightSample ls;
+template <class Col>
+__device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float x0, float x1, const Wl& wl) {
+    LightSample<Col> ls;
     if (S.env_kind == PTR_ENV_IMAGE) {
         float a = env_uniform_fraction(S);
         if (x0 < a) {
@@ -255,7 +327,7 @@ __device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, f
             ls.wi = env_sample_table(S, (x0 - a) / (1.0f - a), x1);
         }
         ls.distance = kMaxDist;
-        ls.radiance = env_radiance(S, ls.wi);
+        ls.radiance = env_radiance<Col>(S, ls.wi, wl);
         ls.pdf = env_pdf(S, ls.wi);
         ls.flags = 0u;
         ls.light_id = -1;
@@ -266,7 +338,7 @@ __device__ __forceinline__ LightSample env_sample(const DevScene& S, float x0, f
     float phi = kTwoPi * x1;
     ls.wi = f3(r * cosf(phi), z, r * sinf(phi));
     ls.distance = kMaxDist;
-    ls.radiance = ld3(S.env_color) * S.env_intensity;
+    ls.radiance = Colors<Col>::env_color(S, wl) * S.env_intensity;
     ls.pdf = 1.0f / (4.0f * kPi);
     ls.flags = 0u;
     ls.light_id = -1;
@@ -279,9 +351,10 @@ __device__ __forceinline__ float sphere_omc_max(float r, float dc2) {
     float sin2_max = r * r / dc2;
     return sin2_max / (1.0f + sqrtf(gmax(0.0f, 1.0f - sin2_max)));
 }
-__device__ LightSample light_sample_one(const ptr_light& l, f3 p, float x0, float x1) {
-    LightSample ls;
-    ls.radiance = ld3(l.radiance);
+template <class Col>
+__device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, float x0, float x1) {
+    LightSample<Col> ls;
+    ls.radiance = le;
     ls.flags = 0u;
     ls.light_id = -1;
     if (l.kind == PTR_LIGHT_QUAD) {
@@ -320,7 +393,7 @@ __device__ LightSample light_sample_one(const ptr_light& l, f3 p, float x0, floa
     float d2 = dot(dd, dd);
     ls.wi = dd * (1.0f / sqrtf(d2));
     ls.distance = sqrtf(d2);
-    ls.radiance = ld3(l.radiance) / d2;
+    ls.radiance = le / d2;
     ls.pdf = 1.0f;
     ls.flags = kLightDelta;
     return ls;
@@ -342,9 +415,10 @@ __device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 ligh
     return 0.0f;
 }
 // Finite-light selection by the power CDF with the rescaled coordinate (lighting.ts:546-637).
-__device__ LightSample lighting_sample_finite(const DevScene& S, f3 p, float x0, float x1) {
+template <class Col>
+__device__ LightSample<Col> lighting_sample_finite(const DevScene& S, f3 p, float x0, float x1, const Wl& wl) {
     if (S.n_lights == 1) {
-        LightSample ls = light_sample_one(S.lights[0], p, x0, x1);
+        LightSample<Col> ls = light_sample_one(S.lights[0], Colors<Col>::light(S, 0, wl), p, x0, x1);
         ls.light_id = 0;
         return ls;
     }
@@ -354,28 +428,29 @@ __device__ LightSample lighting_sample_finite(const DevScene& S, f3 p, float x0,
     float lo = id == 0 ? 0.0f : S.lights[id - 1].select_cdf;
     float sel = S.lights[id].select_pdf;
     float xr = (x0 - lo) / sel;
-    LightSample ls = light_sample_one(S.lights[id], p, clampf(xr, 0.0f, 0.9999999f), x1);
+    LightSample<Col> ls = light_sample_one(S.lights[id], Colors<Col>::light(S, id, wl), p, clampf(xr, 0.0f, 0.9999999f), x1);
     ls.light_id = id;
     ls.pdf *= sel;
     return ls;
 }
 // Two-stage env-vs-finite draw (lighting.ts generateLightSampling).
-__device__ LightSample lighting_sample(const DevScene& S, f3 p, float x0, float x1) {
+template <class Col>
+__device__ LightSample<Col> lighting_sample(const DevScene& S, f3 p, float x0, float x1, const Wl& wl) {
     if (S.n_lights == 0) {
-        if (S.env_samplable) return env_sample(S, x0, x1);
-        LightSample ls;
+        if (S.env_samplable) return env_sample<Col>(S, x0, x1, wl);
+        LightSample<Col> ls;
         ls.pdf = 0.0f;
         return ls;
     }
-    if (!S.env_select_live) return lighting_sample_finite(S, p, x0, x1);
+    if (!S.env_select_live) return lighting_sample_finite<Col>(S, p, x0, x1, wl);
     float pe = S.env_select_prob;
     if (x0 < pe) {
-        LightSample ls = env_sample(S, clampf(x0 / pe, 0.0f, 0.9999999f), x1);
+        LightSample<Col> ls = env_sample<Col>(S, clampf(x0 / pe, 0.0f, 0.9999999f), x1, wl);
         ls.pdf *= pe;
         return ls;
     }
     float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
-    LightSample ls = lighting_sample_finite(S, p, fx, x1);
+    LightSample<Col> ls = lighting_sample_finite<Col>(S, p, fx, x1, wl);
     ls.pdf *= (1.0f - pe);
     return ls;
 }
@@ -387,23 +462,24 @@ __device__ __forceinline__ float lighting_pdf(const DevScene& S, f3 qp, f3 wi, i
 }
 
 // ---- homogeneous media: chromatic channel-MIS free flight (analytic.glsl:9-51) ---------
-struct MediumSample { bool scattered; f3 weight; f3 exit_p, exit_dir; };
-__device__ __forceinline__ MediumSample medium_sample_analytic(const ptr_material& m, const Ray& r, float t_max,
-                                                               float x0, float x1) {
-    f3 sigma_t = ld3(m.sigma_a) + ld3(m.sigma_s);
-    int c = spectrum_sample_channel(x0);
+template <class Col> struct MediumSample { bool scattered; Col weight; f3 exit_p, exit_dir; };
+template <class Col>
+__device__ __forceinline__ MediumSample<Col> medium_sample_analytic(Col sigma_a, Col sigma_s, const Ray& r, float t_max,
+                                                                    float x0, float x1) {
+    Col sigma_t = sigma_a + sigma_s;
+    int c = sample_channel<Col>(x0);
     float sc = sigma_t[c];
     float t = sc == 0.0f ? t_max : -logf(1.0f - x1) / sc;
-    MediumSample ms;
+    MediumSample<Col> ms;
     if (t < t_max) {
-        f3 tr = vexp(-sigma_t * t);
+        Col tr = vexp(-sigma_t * t);
         float pdf = spectrum_average(sigma_t * tr);
         ms.scattered = true;
         ms.exit_p = r.o + r.d * t;
         ms.exit_dir = r.d;
-        ms.weight = ld3(m.sigma_s) * tr / gmax(pdf, 1e-20f);
+        ms.weight = sigma_s * tr / gmax(pdf, 1e-20f);
     } else {
-        f3 tr = vexp(-sigma_t * t_max);
+        Col tr = vexp(-sigma_t * t_max);
         float pdf = spectrum_average(tr);
         ms.scattered = false;
         ms.weight = tr / gmax(pdf, 1e-20f);
@@ -419,9 +495,11 @@ __device__ __forceinline__ MediumSample medium_sample_analytic(const ptr_materia
 // on their area and carry Le * cos_l / (d^2 * pdf_area).  The distance t along the segment
 // is uniform in the angle subtended at the light point.  Returns true when a shadow query
 // is due: from p_evt towards light_pos, adding contrib * visibility / denom.
-struct EquiangularQuery { f3 p_evt, wi, light_pos, contrib; float denom; };
-__device__ __forceinline__ bool equiangular_site(const DevScene& S, const ptr_material& mm, const Ray& r, float t_max,
-                                                 Rng& rng, f3 thr, EquiangularQuery& q) {
+template <class Col> struct EquiangularQuery { f3 p_evt, wi, light_pos; Col contrib; float denom; };
+template <class Col>
+__device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat, const Ray& r, float t_max,
+                                                 Rng& rng, Col thr, const Wl& wl, EquiangularQuery<Col>& q) {
+    const ptr_material& mm = S.materials[med_mat];
     float uc = rng.next();
     int id = S.n_lights - 1;
     if (S.n_lights > 1)
@@ -461,25 +539,25 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, const ptr_ma
     float t = t_c + h * tanf(theta);
     float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
     q.p_evt = r.o + r.d * t;
-    f3 sigma_s = ld3(mm.sigma_s);
+    Col sigma_s = Colors<Col>::sigma_s(S, med_mat, wl);
     if (spectrum_is_black(sigma_s)) return false;
-    f3 T_seg = vexp(-(ld3(mm.sigma_a) + sigma_s) * t);
+    Col T_seg = vexp(-(Colors<Col>::sigma_a(S, med_mat, wl) + sigma_s) * t);
     f3 to_light = pos - q.p_evt;
     float d2 = gmax(dot(to_light, to_light), 1e-8f);
     float dist = sqrtf(d2);
     q.wi = to_light / dist;
-    f3 Le;
+    Col Le;
     if (area) {
         float cos_l = dot(nl, -q.wi);
         if (cos_l <= 0.0f) return false;
-        Le = ld3(l.radiance) * (cos_l / d2);
+        Le = Colors<Col>::light(S, id, wl) * (cos_l / d2);
         q.denom = pdf_t * (pdf_area * sel);
     } else {
-        Le = ld3(l.radiance) / d2;
+        Le = Colors<Col>::light(S, id, wl) / d2;
         q.denom = pdf_t * sel;
     }
     q.light_pos = pos;
-    f3 ph(hg_eval(q.wi, -r.d, mm.phase_g));
+    Col ph(hg_eval(q.wi, -r.d, mm.phase_g));
     q.contrib = thr * T_seg * sigma_s * ph * Le;
     return true;
 }

@@ -57,6 +57,14 @@ struct DevScene {
     const float4* env_map;    // W*H RGBA, row 0 = v = 0 (+Y pole)
     const float* env_marg;    // H cumulative (marginal over rows)
     const float* env_cond;    // H*W cumulative (conditional within each row)
+    // spectral colour model (NULL / unused for RGB scenes): the lifted colours of every
+    // material and light, the constant environment, and the sensor tables
+    const ptr_spectral_material* spec_mats;
+    const ptr_spectrum* spec_lights;
+    const float4* spec_curves;   // 95 x (xbar, ybar, zbar, D65) at 5 nm from 360 nm
+    ptr_spectrum spec_env;
+    float spec_m[9];             // XYZ -> linear sRGB, row-major
+    float spec_y;                // int ybar d lambda
 };
 
 // ---- closed-form arms (components/geometry/*/*.glsl) ------------------------------------

@@ -58,6 +58,12 @@ struct PathPool {
     float4* dl;        // adjoint radiance of the path: dLoss/dI of its pixel / spp
     float4* sh_g;      // shadow query: lobe derivative D = dlog f(wi_light) - dlog w_cont (xyz)
     int* sh_gm;        // shadow query: vertex material | kind << 16
+    // spectral colour model only (NULL otherwise): the path's four wavelengths and their
+    // sampling densities; the shadow queries' pdfs (the colour fills all four lanes)
+    float4* wl;
+    float4* wl_pdf;
+    float* sh_pdf;
+    float* sh2_pdf;
 };
 
 // Adjoint replay tables: the adjoint image (3 floats per pixel, row 0 at the bottom), the
@@ -75,6 +81,8 @@ struct FrameParams {
     long long total;   // width*height*spp
     int capacity;
     ptr_camera cam;
+    int wavelengths;   // PTR_WAVELENGTHS_* (spectral programs)
+    float lambda_min, lambda_max;
 };
 
 struct ProgParams {
@@ -284,16 +292,55 @@ __device__ __forceinline__ bool mat_has_medium(const DevScene& S, int m) {
 __device__ __forceinline__ bool scatter_live(const DevScene& S, const ProgParams& P, int m) {
     return P.scattering && (S.materials[m].flags & PTR_MATF_SCATTERING);
 }
-__device__ __forceinline__ f3 medium_transmittance(const DevScene& S, const ProgParams& P, int m, float len) {
-    const ptr_material& mm = S.materials[m];
-    f3 st = scatter_live(S, P, m) ? ld3(mm.sigma_a) + ld3(mm.sigma_s) : ld3(mm.sigma_a);
+template <class Col>
+__device__ __forceinline__ Col medium_transmittance(const DevScene& S, const ProgParams& P, int m, float len, const Wl& wl) {
+    Col st = scatter_live(S, P, m) ? Colors<Col>::sigma_a(S, m, wl) + Colors<Col>::sigma_s(S, m, wl)
+                                   : Colors<Col>::sigma_a(S, m, wl);
     return vexp(-st * len);
+}
+
+// wavelengths_sample (color/spectral/spectral.glsl:1-10): one number, four cyclic
+// quarter-interval offsets in CDF space, each lane with its own marginal density; the
+// visible density is the normalised sech^2 (visible.glsl:3-13), or uniform (uniform.glsl).
+__device__ __forceinline__ void wavelengths_sample(const FrameParams& F, float u, float4& lam, float4& pdf) {
+    float l[4], p[4];
+    for (int k = 0; k < 4; ++k) {
+        float v = u + 0.25f * (float)k;
+        v = v - floorf(v);
+        if (F.wavelengths == PTR_WAVELENGTHS_UNIFORM) {
+            l[k] = F.lambda_min + (F.lambda_max - F.lambda_min) * v;
+            p[k] = 1.0f / (F.lambda_max - F.lambda_min);
+        } else {
+            float a = tanhf(0.0072f * (F.lambda_min - 538.0f));
+            float b = tanhf(0.0072f * (F.lambda_max - 538.0f));
+            l[k] = 538.0f + atanhf(a * (1.0f - v) + b * v) / 0.0072f;
+            float c = coshf(0.0072f * (l[k] - 538.0f));
+            p[k] = 0.0072f / ((b - a) * c * c);
+        }
+    }
+    lam = make_float4(l[0], l[1], l[2], l[3]);
+    pdf = make_float4(p[0], p[1], p[2], p[3]);
+}
+
+// color_to_pixel (spectral.glsl:27-33) with the CIE 1931 sensor (sensor/cie1931/cie1931.glsl:3-5):
+// 0.25 * sum_i M xyz(lambda_i) / int(ybar) * (L_i / pdf_i).
+__device__ __forceinline__ f3 color_to_pixel(const DevScene& S, float4 L, float4 lam, float4 pdf) {
+    const float Ls[4] = {L.x, L.y, L.z, L.w}, ls[4] = {lam.x, lam.y, lam.z, lam.w}, ps[4] = {pdf.x, pdf.y, pdf.z, pdf.w};
+    f3 pixel(0.0f);
+    for (int k = 0; k < 4; ++k) {
+        float4 c = spectral_curves(S, ls[k]);
+        f3 rgb(S.spec_m[0] * c.x + S.spec_m[1] * c.y + S.spec_m[2] * c.z,
+               S.spec_m[3] * c.x + S.spec_m[4] * c.y + S.spec_m[5] * c.z,
+               S.spec_m[6] * c.x + S.spec_m[7] * c.y + S.spec_m[8] * c.z);
+        pixel = pixel + rgb / S.spec_y * (Ls[k] / ps[k]);
+    }
+    return 0.25f * pixel;
 }
 
 // ---- kernels ---------------------------------------------------------------------------
 
 // Camera rays for one wave (accumulation.ts:14-26 cameraSample; pinhole.glsl:4-18).
-template <bool ADJ = false>
+template <bool ADJ = false, bool SPECTRAL = false>
 __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, AdjParams adj = AdjParams{}) {
     const FrameParams F = *fp;
     long long base = pool.wave[0];
@@ -317,6 +364,12 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, Adj
         float a0 = rng.next();
         float a1 = rng.next();
         float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+        if (SPECTRAL) {   // wavelengths_sample, between the film point and the camera ray
+            float4 lam, pdf;
+            wavelengths_sample(F, rng.next(), lam, pdf);
+            pool.wl[i] = lam;
+            pool.wl_pdf[i] = pdf;
+        }
         rng.next();   // the lens draw (a pinhole has no aperture)
         rng.next();
         float ndcx = (2.0f * fx / (float)F.width) - 1.0f;
@@ -333,7 +386,7 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, Adj
         }
         pool.ray_o[i] = f4(o, 0.0f);
         pool.ray_d[i] = f4(dir, 1.0f);
-        pool.thr[i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        pool.thr[i] = make_float4(1.f, 1.f, 1.f, 1.f);   // the spectral model's fourth lane included
         pool.rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         pool.prev_q[i] = f4(o, 0.0f);
         pool.st[i] = make_int4(0, medium, 0, 1);
@@ -389,11 +442,15 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
 // ADJ: the replay pass of the adjoint — the same walk on the same random numbers, which
 // also scatters d Loss / d theta into per-block float64 accumulators (dynamic shared
 // memory: PTR_GRAD_SLOTS doubles per material).
-template <int DIRECT, bool MEDIA, bool BATCH, bool ADJ = false>
+// Col: f3 (RGB) or s4 (spectral, four wavelength lanes; the adjoint is RGB only).
+template <class Col, int DIRECT, bool MEDIA, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt,
                                                                      AdjParams adj = AdjParams{}) {
+    constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
+    static_assert(!(ADJ && SPECTRAL), "the adjoint replay is RGB only");
+    using CM = Colors<Col>;
     extern __shared__ double s_grad[];
-    if (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
+    if constexpr (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[in];
     const int* q = pool.q[in];
     int* qout = pool.q[in ^ 1];
@@ -414,9 +471,11 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             r.d = xyz(rd);
             float prev_bsdf_pdf = ro.w;
             float eta_scale = rd.w;
-            f3 thr = xyz(pool.thr[i]);
-            f3 rad = xyz(pool.rad[i]);
+            Col thr = col_ld<Col>(pool.thr[i]);
+            Col rad = col_ld<Col>(pool.rad[i]);
             f3 prev_qp = xyz(pool.prev_q[i]);
+            Wl wl;
+            if constexpr (SPECTRAL) wl.lambda = pool.wl[i];
             int4 st = pool.st[i];
             int bounce = st.x, cur_med = st.y, nulls = st.z;
             bool prev_delta = st.w != 0;
@@ -424,11 +483,11 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             Rng rng;
             rng.base = rs.x;
             rng.dim = rs.y;
-            f3 lrem(0.0f);
+            Col lrem(0.0f);
             GradAcc ga;
             int sh_kind = kGradKindNone, sh_mat = 0;
             f3 sh_dnee(0.0f);   // dlog f at the light direction of this vertex's NEE query
-            if (ADJ) {
+            if constexpr (ADJ) {
                 lrem = xyz(pool.l_rem[i]);
                 ga.s = s_grad;
                 ga.dl = xyz(pool.dl[i]);
@@ -452,12 +511,13 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                     // the per-segment equiangular site precedes the transmittance sample
                     // (pt.ts:322-328) and rides the second shadow slot
                     if (P.equiangular && bounce < N) {
-                        EquiangularQuery eq;
-                        if (equiangular_site(S, mm, r, boundary ? hr.t : kMaxDist, rng, thr, eq)) {
+                        EquiangularQuery<Col> eq;
+                        if (equiangular_site<Col>(S, med_mat, r, boundary ? hr.t : kMaxDist, rng, thr, wl, eq)) {
                             pool.sh2_o[i] = f4(eq.p_evt, 0.0f);
                             pool.sh2_d[i] = f4(eq.wi, __int_as_float(P.max_null - nulls));
                             pool.sh2_lp[i] = f4(eq.light_pos, 1.0f);
-                            pool.sh2_c[i] = f4(eq.contrib, eq.denom);
+                            pool.sh2_c[i] = col_st(eq.contrib, eq.denom);
+                            if constexpr (SPECTRAL) pool.sh2_pdf[i] = eq.denom;
                             shadow2 = true;
                         }
                     }
@@ -465,16 +525,17 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                     float x1 = rng.next();
                     float t_max = boundary ? hr.t : kMaxDist;
                     if (!scatter_live(S, P, med_mat)) {
-                        thr = thr * vexp(-ld3(mm.sigma_a) * t_max);
-                        if (ADJ) {   // w = exp(-(1-a) st t)
+                        thr = thr * vexp(-CM::sigma_a(S, med_mat, wl) * t_max);
+                        if constexpr (ADJ) {   // w = exp(-(1-a) st t)
                             GreyMedium gm = grey_medium(mm);
                             ga.scl(med_mat, PTR_GRAD_SIGMA_T, lrem, -(1.0f - gm.a) * t_max);
                             ga.scl(med_mat, PTR_GRAD_MEDIUM_ALBEDO, lrem, gm.st * t_max);
                         }
                     } else {
-                        MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
+                        MediumSample<Col> ms = medium_sample_analytic<Col>(CM::sigma_a(S, med_mat, wl), CM::sigma_s(S, med_mat, wl),
+                                                                           r, t_max, x0, x1);
                         thr = thr * ms.weight;
-                        if (ADJ) {   // scattered at t: w = a st exp(-st t)/pdf; passed: exp(-st t_max)/P
+                        if constexpr (ADJ) {   // scattered at t: w = a st exp(-st t)/pdf; passed: exp(-st t_max)/P
                             GreyMedium gm = grey_medium(mm);
                             if (ms.scattered) {
                                 float t_evt = dot(ms.exit_p - r.o, r.d);
@@ -494,18 +555,19 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 if (nee && !P.equiangular) {   // light_sample_direct_medium (light_medium.glsl:7-18)
                                     float y0 = rng.next();
                                     float y1 = rng.next();
-                                    LightSample ls = lighting_sample(S, p_evt, y0, y1);
+                                    LightSample<Col> ls = lighting_sample<Col>(S, p_evt, y0, y1, wl);
                                     if (ls.pdf > 0.0f) {
                                         f3 light_p = p_evt + ls.wi * ls.distance;
                                         float ph = hg_eval(ls.wi, wo_med, mm.phase_g);
                                         float w = 1.0f;
-                                        if (mis && !(ls.flags & kLightDelta)) w = power_heuristic(ls.pdf, spectrum_average(f3(ph)));
+                                        if (mis && !(ls.flags & kLightDelta)) w = power_heuristic(ls.pdf, spectrum_average(Col(ph)));
                                         pool.sh_o[i] = f4(p_evt, 0.0f);
                                         pool.sh_d[i] = f4(ls.wi, __int_as_float(P.max_null - nulls));
                                         pool.sh_lp[i] = f4(light_p, w);
-                                        pool.sh_c[i] = f4(thr * ls.radiance * f3(ph), ls.pdf);
+                                        pool.sh_c[i] = col_st(thr * ls.radiance * Col(ph), ls.pdf);
+                                        if constexpr (SPECTRAL) pool.sh_pdf[i] = ls.pdf;
                                         shadow = true;
-                                        if (ADJ) {
+                                        if constexpr (ADJ) {
                                             sh_kind = kGradKindPhase;
                                             sh_mat = med_mat;
                                             sh_dnee = f3(hg_dlog_g(ls.wi, wo_med, mm.phase_g), 0.0f, 0.0f);
@@ -514,9 +576,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 }
                                 float z0 = rng.next();
                                 float z1 = rng.next();
-                                ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
+                                ISample<Col> ps = hg_sample<Col>(wo_med, mm.phase_g, z0, z1);
                                 thr = thr * ps.weight;
-                                if (ADJ) {   // phase continuation: w = p_HG / pdf_detached
+                                if constexpr (ADJ) {   // phase continuation: w = p_HG / pdf_detached
                                     float dg = hg_dlog_g(ps.wi, wo_med, mm.phase_g);
                                     ga.scl(med_mat, PTR_GRAD_HG_G, lrem, dg);
                                     if (shadow) sh_dnee.x -= dg;
@@ -529,8 +591,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 // roulette_interior (pt.ts:230-283)
                                 bool survive = true;
                                 if (P.rr_start >= 0 && bounce >= P.rr_start) {
-                                    f3 ss = ld3(mm.sigma_s), sa = ld3(mm.sigma_a);
-                                    f3 surv = ss / vmax(ss + sa, f3(1e-9f));
+                                    Col ss = CM::sigma_s(S, med_mat, wl), sa = CM::sigma_a(S, med_mat, wl);
+                                    Col surv = ss / vmax(ss + sa, Col(1e-9f));
                                     float p_survive = spectrum_max(surv);
                                     if (p_survive <= 0.0f) survive = false;
                                     else if (rng.next() > p_survive) survive = false;
@@ -553,9 +615,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             w = power_heuristic(prev_bsdf_pdf, pe * env_pdf(S, r.d));
                         }
                     }
-                    f3 e = thr * w * env_radiance(S, r.d);
+                    Col e = thr * w * env_radiance<Col>(S, r.d, wl);
                     rad = rad + e;
-                    if (ADJ) lrem = lrem - e;
+                    if constexpr (ADJ) lrem = lrem - e;
                     done = true;
                 } else {
                     if (MEDIA && hit.region_from != cur_med) cur_med = hit.region_from;
@@ -581,9 +643,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p));
                                 }
                             }
-                            f3 e = thr * w * ld3(S.materials[mat_emit].emission);
+                            Col e = thr * w * CM::emission(S, mat_emit, wl);
                             rad = rad + e;
-                            if (ADJ) lrem = lrem - e;
+                            if constexpr (ADJ) lrem = lrem - e;
                         }
                         if (bounce == N) {
                             done = true;
@@ -594,13 +656,13 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             if (nee && nondelta) {
                                 float y0 = rng.next();
                                 float y1 = rng.next();
-                                LightSample ls = lighting_sample(S, hit.p, y0, y1);
+                                LightSample<Col> ls = lighting_sample<Col>(S, hit.p, y0, y1, wl);
                                 if (ls.pdf > 0.0f) {
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
                                     sr.d = normalize(light_p - sr.o);
-                                    f3 f = m.model == PTR_MAT_LAMBERT ? lambert_eval(ls.wi, wo, hit, m)
-                                                                      : ggx_eval(ls.wi, wo, hit, ld3(m.f0), alpha);
+                                    Col f = m.model == PTR_MAT_LAMBERT ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
+                                                                       : ggx_eval(ls.wi, wo, hit, CM::f0(S, mat, wl), alpha);
                                     float cos_i = fabsf(dot(ls.wi, hit.frame.n));
                                     float w = 1.0f;
                                     if (mis && !(ls.flags & kLightDelta)) {
@@ -612,9 +674,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     pool.sh_o[i] = f4(sr.o, maxd);
                                     pool.sh_d[i] = f4(sr.d, __int_as_float(P.max_null - nulls));
                                     pool.sh_lp[i] = f4(light_p, w);
-                                    pool.sh_c[i] = f4(thr * ls.radiance * f * cos_i, ls.pdf);
+                                    pool.sh_c[i] = col_st(thr * ls.radiance * f * cos_i, ls.pdf);
+                                    if constexpr (SPECTRAL) pool.sh_pdf[i] = ls.pdf;
                                     shadow = true;
-                                    if (ADJ) {
+                                    if constexpr (ADJ) {
                                         sh_mat = mat;
                                         if (m.model == PTR_MAT_LAMBERT) {
                                             sh_kind = kGradKindAlbedo;
@@ -630,15 +693,16 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             float uc = rng.next();
                             float u0 = rng.next();
                             float u1 = rng.next();
-                            ISample bs;
-                            if (m.model == PTR_MAT_LAMBERT) bs = lambert_sample(wo, hit, m, u0, u1);
-                            else if (m.model == PTR_MAT_GGX) bs = ggx_sample(wo, hit, ld3(m.f0), alpha, u0, u1);
-                            else bs = dielectric_sample(wo, hit, m, ior_of(S, hit.region_from), ior_of(S, hit.region_to), uc);
+                            ISample<Col> bs;
+                            if (m.model == PTR_MAT_LAMBERT) bs = lambert_sample(wo, hit, CM::albedo(S, mat, wl), u0, u1);
+                            else if (m.model == PTR_MAT_GGX) bs = ggx_sample(wo, hit, CM::f0(S, mat, wl), alpha, u0, u1);
+                            else bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), ior_of(S, hit.region_from),
+                                                        ior_of(S, hit.region_to), uc);
                             if (spectrum_is_black(bs.weight)) {
                                 done = true;
                             } else {
                                 thr = thr * bs.weight;
-                                if (ADJ) {   // the continuation lobe: d log w_cont
+                                if constexpr (ADJ) {   // the continuation lobe: d log w_cont
                                     if (m.model == PTR_MAT_LAMBERT) {
                                         f3 dlog = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
                                         ga.vec(mat, PTR_GRAD_ALBEDO_R, lrem, dlog);
@@ -688,8 +752,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                 }
             }
             (void)done;
-            pool.rad[i] = f4(rad, 0.0f);
-            if (ADJ) {
+            pool.rad[i] = col_st(rad, 0.0f);
+            if constexpr (ADJ) {
                 pool.l_rem[i] = f4(lrem, 0.0f);
                 if (shadow) {
                     pool.sh_g[i] = f4(sh_dnee, 0.0f);
@@ -699,7 +763,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if (alive) {
                 pool.ray_o[i] = f4(r.o, prev_bsdf_pdf);
                 pool.ray_d[i] = f4(r.d, eta_scale);
-                pool.thr[i] = f4(thr, 0.0f);
+                pool.thr[i] = col_st(thr, 0.0f);
                 pool.prev_q[i] = f4(prev_qp, 0.0f);
                 pool.st[i] = make_int4(bounce, cur_med, nulls, prev_delta ? 1 : 0);
                 pool.rng[i] = make_uint2(rng.base, rng.dim);
@@ -714,7 +778,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if (shadow2) pool.shq2[s2] = i;
         }
     }
-    if (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
+    if constexpr (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
 }
 
 // Shadow queries: opaque visibility (shadow/opaque/opaque.glsl:16-19) or the media
@@ -727,11 +791,13 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
 // its vertex and d log T / d theta of every medium segment the shadow ray crossed.
 constexpr int kAdjMaxMedia = 4;            // distinct media one adjoint shadow query may cross
 constexpr unsigned kErrAdjMedia = 8u;      // ... more were crossed (their terms were dropped)
-template <bool MEDIA, bool COUNT, bool BATCH, bool ADJ = false>
+template <class Col, bool MEDIA, bool COUNT, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt,
                                                                       int slot, AdjParams adj = AdjParams{}) {
+    constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
+    static_assert(!(ADJ && SPECTRAL), "the adjoint replay is RGB only");
     extern __shared__ double s_grad[];
-    if (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
+    if constexpr (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[slot ? 4 : 2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
     const int* shq = slot ? pool.shq2 : pool.shq;
@@ -745,19 +811,26 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
         const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
         float4 so = a_o[i], sd = a_d[i], lp = a_lp[i], c = a_c[i];
+        Col cc = col_ld<Col>(c);
+        float cpdf = c.w;
+        Wl wl;
+        if constexpr (SPECTRAL) {
+            cpdf = slot ? pool.sh2_pdf[i] : pool.sh_pdf[i];
+            wl.lambda = pool.wl[i];
+        }
         Ray sr;
         sr.o = xyz(so);
         sr.d = xyz(sd);
-        f3 vis;
+        Col vis;
         int mm_id[kAdjMaxMedia];
         float mm_len[kAdjMaxMedia];
         int n_mm = 0;
         if (!MEDIA) {
-            vis = scene_any(S, sr, so.w, COUNT ? &wk : nullptr) ? f3(0.0f) : f3(1.0f);
+            vis = scene_any(S, sr, so.w, COUNT ? &wk : nullptr) ? Col(0.0f) : Col(1.0f);
         } else {
             f3 light_p = xyz(lp);
             int crossings_left = __float_as_int(sd.w);
-            f3 T(1.0f);
+            Col T(1.0f);
             int medium = scene_region_at(S, sr.o);
             Ray seg = sr;
             bool finished = false;
@@ -769,8 +842,8 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 float seg_len = hit_boundary ? hr.t : remaining;
                 int med_mat = material_of(S, medium);
                 if (mat_has_medium(S, med_mat)) {
-                    T = T * medium_transmittance(S, P, med_mat, seg_len);
-                    if (ADJ) {
+                    T = T * medium_transmittance<Col>(S, P, med_mat, seg_len, wl);
+                    if constexpr (ADJ) {
                         int e = 0;
                         while (e < n_mm && mm_id[e] != med_mat) e++;
                         if (e < n_mm) mm_len[e] += seg_len;
@@ -782,19 +855,18 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 Hit h;
                 fill_hit(S, seg, hr, h);
                 int om = material_of(S, h.region_owner);
-                if (!(om >= 0 && S.materials[om].model == PTR_MAT_NONE)) { T = f3(0.0f); finished = true; break; }
+                if (!(om >= 0 && S.materials[om].model == PTR_MAT_NONE)) { T = Col(0.0f); finished = true; break; }
                 medium = h.region_to;
                 seg = ray_spawn(h, seg.d);
                 seg.d = normalize(light_p - seg.o);
             }
-            vis = finished ? T : f3(0.0f);
+            vis = finished ? T : Col(0.0f);
         }
         if (!spectrum_is_black(vis)) {
             float w = lp.w;
-            f3 add = xyz(c) * vis * w / c.w;
-            float4 rr = pool.rad[i];
-            pool.rad[i] = make_float4(rr.x + add.x, rr.y + add.y, rr.z + add.z, 0.f);
-            if (ADJ) {
+            Col add = cc * vis * w / cpdf;
+            pool.rad[i] = col_st(col_ld<Col>(pool.rad[i]) + add, 0.0f);
+            if constexpr (ADJ) {
                 GradAcc ga;
                 ga.s = s_grad;
                 ga.dl = xyz(pool.dl[i]);
@@ -819,12 +891,15 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
         }
     }
     if (COUNT) flush_work(S0, wk);
-    if (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
+    if constexpr (ADJ) grad_block_flush(s_grad, PTR_GRAD_SLOTS * S0.n_materials, adj.grads);
 }
 
 // Fold the wave's per-path radiance into the film, per pixel in sample order; then
 // advance the wave cursor.
-__global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double* sumsq, float* samples_out) {
+// SPECTRAL: each sample's four lanes are projected to linear sRGB first (color_to_pixel).
+template <bool SPECTRAL = false>
+__global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double* sumsq, float* samples_out,
+                       DevScene S = DevScene{}) {
     const FrameParams F = *fp;
     const long long base = pool.wave[0];
     const long long n = pool.wave[1];
@@ -836,6 +911,10 @@ __global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double
         double q0 = sumsq[3 * pix + 0], q1 = sumsq[3 * pix + 1], q2 = sumsq[3 * pix + 2];
         for (long long i = j; i < n; i += npix) {
             float4 L = pool.rad[i];
+            if (SPECTRAL) {
+                f3 px = color_to_pixel(S, L, pool.wl[i], pool.wl_pdf[i]);
+                L = make_float4(px.x, px.y, px.z, 0.0f);
+            }
             s0 += (double)L.x; s1 += (double)L.y; s2 += (double)L.z;
             q0 += (double)L.x * (double)L.x; q1 += (double)L.y * (double)L.y; q2 += (double)L.z * (double)L.z;
             if (samples_out) {

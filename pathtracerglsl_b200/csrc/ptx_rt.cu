@@ -116,7 +116,7 @@ void free_pool(ptr_program* p) {
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
 }
 
-int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false) {
+int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool spectral = false) {
     free_pool(p);
     ptr_ctx* ctx = p->ctx;
     auto get = [&](size_t bytes, void** out) -> int {
@@ -155,6 +155,12 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false) {
         free_pool(p);
         return rc;
     }
+    // the spectral colour model's wavelengths and shadow pdfs
+    if (spectral && ((rc = get(c * 16, (void**)&q.wl)) || (rc = get(c * 16, (void**)&q.wl_pdf)) ||
+                     (rc = get(c * 4, (void**)&q.sh_pdf)) || (rc = get(c * 4, (void**)&q.sh2_pdf)))) {
+        free_pool(p);
+        return rc;
+    }
     p->capacity = capacity;
     return PTR_OK;
 }
@@ -170,8 +176,10 @@ int wave_iterations(const ptr_program* p, const ptr_scene* s) {
 // Event pairs around each launch of an instrumented render (kernel class, start, end).
 struct ProfRec { int cls; cudaEvent_t a, b; };
 
-void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
-                 std::vector<ProfRec>* prof = nullptr, bool film = true) {
+template <class Col>
+void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
+                   std::vector<ProfRec>* prof, bool film) {
+    constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     DevScene Sp = s->dev;
     Sp.accel = p->desc.accel;
     Sp.work = (p->profile_next & PTR_PROFILE_WORK) ? p->work_dev : nullptr;
@@ -198,7 +206,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     const int grid = launch_grid(n_sm), block = 256;
     ProfRec* r = mark(0);
     const BatchTables nob{};
-    k_generate<false><<<grid, block, 0, st>>>(S, pool, p->fp_dev);
+    k_generate<false, SPECTRAL><<<grid, block, 0, st>>>(S, pool, p->fp_dev);
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
@@ -209,12 +217,12 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
         const bool media = s->has_media != 0;
         r = mark(2);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<PTR_DIRECT_NONE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 1: k_shade<PTR_DIRECT_NONE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 2: k_shade<PTR_DIRECT_NEE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 3: k_shade<PTR_DIRECT_NEE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 4: k_shade<PTR_DIRECT_MIS, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            default: k_shade<PTR_DIRECT_MIS, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 0: k_shade<Col, PTR_DIRECT_NONE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 1: k_shade<Col, PTR_DIRECT_NONE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 2: k_shade<Col, PTR_DIRECT_NEE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 3: k_shade<Col, PTR_DIRECT_NEE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 4: k_shade<Col, PTR_DIRECT_MIS, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            default: k_shade<Col, PTR_DIRECT_MIS, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
         }
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
@@ -224,11 +232,11 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
                 if (S.work) {
                     DevScene Sq = S;
                     Sq.work = S.work + 4;   // the shadow queries' own tallies
-                    if (media) k_shadow<true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
-                    else k_shadow<false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
+                    if (media) k_shadow<Col, true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
+                    else k_shadow<Col, false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
                 } else {
-                    if (media) k_shadow<true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
-                    else k_shadow<false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
+                    if (media) k_shadow<Col, true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
+                    else k_shadow<Col, false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
                 }
             }
             done(r);
@@ -236,10 +244,17 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
     }
     if (!film) return;
     r = mark(4);
-    k_film<<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples);
+    k_film<SPECTRAL><<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples, S);
     k_advance<<<1, 32, 0, st>>>(pool);
     done(r);
 }
+
+void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
+                 std::vector<ProfRec>* prof = nullptr, bool film = true) {
+    if (p->desc.color == PTR_COLOR_SPECTRAL) launch_wave_t<s4>(p, s, st, iters, samples, n_sm, prof, film);
+    else launch_wave_t<f3>(p, s, st, iters, samples, n_sm, prof, film);
+}
+
 
 // The adjoint's replay of one wave (after launch_wave(..., film = false) left every path's
 // forward radiance in the pool): the same kernels with ADJ = true, then the wave cursor.
@@ -265,16 +280,16 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         int in = it & 1;
         k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<PTR_DIRECT_NONE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 1: k_shade<PTR_DIRECT_NONE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 2: k_shade<PTR_DIRECT_NEE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 3: k_shade<PTR_DIRECT_NEE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 4: k_shade<PTR_DIRECT_MIS, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            default: k_shade<PTR_DIRECT_MIS, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 0: k_shade<f3, PTR_DIRECT_NONE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 1: k_shade<f3, PTR_DIRECT_NONE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 2: k_shade<f3, PTR_DIRECT_NEE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 3: k_shade<f3, PTR_DIRECT_NEE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 4: k_shade<f3, PTR_DIRECT_MIS, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            default: k_shade<f3, PTR_DIRECT_MIS, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
         }
         if (P.direct != PTR_DIRECT_NONE) {
-            if (media) k_shadow<true, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
-            else k_shadow<false, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
+            if (media) k_shadow<f3, true, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
+            else k_shadow<f3, false, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
         }
     }
     k_advance<<<1, 32, 0, st>>>(pool);
@@ -306,19 +321,19 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTabl
         done(r);
         r = mark(2);
         switch (direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<PTR_DIRECT_NONE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 1: k_shade<PTR_DIRECT_NONE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 2: k_shade<PTR_DIRECT_NEE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 3: k_shade<PTR_DIRECT_NEE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 4: k_shade<PTR_DIRECT_MIS, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            default: k_shade<PTR_DIRECT_MIS, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 0: k_shade<f3, PTR_DIRECT_NONE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 1: k_shade<f3, PTR_DIRECT_NONE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 2: k_shade<f3, PTR_DIRECT_NEE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 3: k_shade<f3, PTR_DIRECT_NEE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 4: k_shade<f3, PTR_DIRECT_MIS, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            default: k_shade<f3, PTR_DIRECT_MIS, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
         }
         done(r);
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
             for (int slot = equiangular ? 1 : 0; slot >= 0; --slot) {
-                if (media) k_shadow<true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
-                else k_shadow<false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
+                if (media) k_shadow<f3, true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
+                else k_shadow<f3, false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
             }
             done(r);
         }
@@ -580,8 +595,17 @@ int check_equiangular(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
     return PTR_OK;
 }
 
+// A spectral program needs the scene's lifted colours; image environments are RGB only.
+int check_color(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
+    if (p->desc.color != PTR_COLOR_SPECTRAL) return PTR_OK;
+    if (!s->dev.spec_mats) return fail(ctx, PTR_E_INVALID, "measurement.color 'spectral' needs the scene's spectral tables (ptr_scene_desc.spectral)");
+    if (s->dev.env_kind == PTR_ENV_IMAGE) return fail(ctx, PTR_E_UNSUPPORTED, "spectral rendering of image environments is not available");
+    return PTR_OK;
+}
+
 int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples_dev) {
     ptr_ctx* ctx = p->ctx;
+    if (int rc = check_color(ctx, p, s)) return rc;
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return fail(ctx, PTR_E_INVALID, "frame: width, height and spp must be positive");
     if (s->ctx != ctx) return fail(ctx, PTR_E_INVALID, "scene belongs to another context");
     if (int rc = check_equiangular(ctx, p, s)) return rc;
@@ -618,8 +642,10 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     else cap = cap_max;
     if (cap > total) cap = total;
     const bool slot2 = p->desc.equiangular != 0;
-    if (p->capacity < cap || (slot2 && !p->pool.sh2_o)) {
-        int rc = alloc_pool(p, (int)cap, slot2, p->pool.l_rem != nullptr);
+    const bool spectral = p->desc.color == PTR_COLOR_SPECTRAL;
+    if (p->capacity < cap || (slot2 && !p->pool.sh2_o) || (spectral && !p->pool.wl)) {
+        int rc = alloc_pool(p, (int)std::max<long long>(cap, p->capacity), slot2 || p->pool.sh2_o,
+                            p->pool.l_rem != nullptr, spectral || p->pool.wl);
         if (rc) return rc;
     }
     if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
@@ -636,6 +662,9 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     F.total = total;
     F.capacity = (int)cap;
     F.cam = f->camera;
+    F.wavelengths = p->desc.wavelengths;
+    F.lambda_min = p->desc.lambda_min;
+    F.lambda_max = p->desc.lambda_max;
     k_set_frame<<<1, 1, 0, st>>>(p->fp_dev, F);
     CK(ctx, cudaGetLastError());
     CK(ctx, cudaMemsetAsync(p->pool.wave, 0, 64, st));
@@ -785,6 +814,24 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     S.env_kind = d->env.kind;
     S.env_samplable = d->env.kind != PTR_ENV_NONE && d->env.sample_as_light;
     S.env_select_live = S.env_samplable && d->n_lights > 0;
+    if (d->spectral) {   // the lifted colours and the sensor tables of the spectral model
+        const ptr_spectral_desc* sp = d->spectral;
+        if (!sp->materials || !sp->curves || (d->n_lights > 0 && !sp->lights) || !(sp->cie_y_integral > 0.0f)) {
+            ptr_free_scene(s);
+            return fail(ctx, PTR_E_INVALID, "scene: incomplete spectral tables");
+        }
+        const float4* curves = nullptr;
+        if ((rc = dev_copy(ctx, s->allocs, sp->materials, (size_t)d->n_materials, &S.spec_mats)) ||
+            (rc = dev_copy(ctx, s->allocs, sp->lights, (size_t)d->n_lights, &S.spec_lights)) ||
+            (rc = dev_copy(ctx, s->allocs, (const float4*)sp->curves, (size_t)95, &curves))) {
+            ptr_free_scene(s);
+            return rc;
+        }
+        S.spec_curves = curves;
+        S.spec_env = sp->env;
+        for (int k = 0; k < 9; ++k) S.spec_m[k] = sp->xyz_to_rgb[k];
+        S.spec_y = sp->cie_y_integral;
+    }
     for (int k = 0; k < 4; ++k) S.env_color[k] = d->env.color[k];
     S.env_intensity = d->env.intensity;
     S.env_select_prob = d->env.select_prob;
@@ -842,6 +889,11 @@ int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* d, ptr_program** out) {
         return fail(ctx, PTR_E_INVALID, "program: mediumLightSampling 'equiangular' requires directLighting 'nee'");
     if (d->equiangular && !d->scattering)
         return fail(ctx, PTR_E_INVALID, "program: mediumLightSampling 'equiangular' requires scattering media");
+    if (d->color != PTR_COLOR_RGB && d->color != PTR_COLOR_SPECTRAL) return fail(ctx, PTR_E_INVALID, "program: unknown measurement.color");
+    if (d->color == PTR_COLOR_SPECTRAL &&
+        (d->wavelengths < PTR_WAVELENGTHS_VISIBLE || d->wavelengths > PTR_WAVELENGTHS_UNIFORM ||
+         !(d->lambda_min >= 360.0f && d->lambda_max <= 830.0f && d->lambda_min < d->lambda_max)))
+        return fail(ctx, PTR_E_INVALID, "program: the sampled wavelength range must lie in [360, 830] nm");
     ptr_program* p = new ptr_program();
     p->ctx = ctx;
     p->desc = *d;
@@ -885,6 +937,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         if (J.frame.width <= 0 || J.frame.height <= 0 || J.frame.spp <= 0)
             return fail(ctx, PTR_E_INVALID, "ptr_render_batch: job " + std::to_string(j) + " has an empty frame");
         if (J.scene->has_media) media = true;
+        if (J.prog->desc.color != PTR_COLOR_RGB)
+            return fail(ctx, PTR_E_UNSUPPORTED, "ptr_render_batch: spectral programs render one per launch (ptr_render)");
         if (int rc = check_equiangular(ctx, J.prog, J.scene)) return rc;
         for (int k = 0; k < j; ++k)
             if (jobs[k].prog == J.prog)
@@ -1100,6 +1154,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
         return fail(ctx, PTR_E_INVALID, "ptr_backward: grads needs PTR_GRAD_SLOTS * n_materials doubles");
     if (n_mat > 512) return fail(ctx, PTR_E_INVALID, "ptr_backward: at most 512 materials");
     if (p->desc.equiangular) return fail(ctx, PTR_E_INVALID, "ptr_backward: equiangular programs are not differentiated");
+    if (p->desc.color != PTR_COLOR_RGB) return fail(ctx, PTR_E_INVALID, "ptr_backward: the adjoint is RGB only");
     for (const ptr_material& m : s->h_materials)
         if ((m.flags & PTR_MATF_MEDIUM) && !(m.sigma_a[0] == m.sigma_a[1] && m.sigma_a[0] == m.sigma_a[2] &&
                                              m.sigma_s[0] == m.sigma_s[1] && m.sigma_s[0] == m.sigma_s[2]))
@@ -1394,7 +1449,8 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
         return PTR_E_UNSUPPORTED;
     }
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return PTR_E_INVALID;
-    if (pd->max_bounces < 0 || pd->max_bounces > 4096 || pd->direct < 0 || pd->direct > 2 || pd->equiangular) return PTR_E_INVALID;
+    if (pd->max_bounces < 0 || pd->max_bounces > 4096 || pd->direct < 0 || pd->direct > 2 || pd->equiangular ||
+        pd->color != PTR_COLOR_RGB) return PTR_E_INVALID;
     for (int i = 0; i < d->n_regions; ++i)
         if (d->regions[i].shape > PTR_SHAPE_BOX || d->regions[i].material < 0 || d->regions[i].material >= d->n_materials)
             return PTR_E_INVALID;

@@ -302,3 +302,50 @@ def adjoint_scene(seed=0, n_spheres=64, width=256, height=256, spp_primal=64, sp
     scene = dict(base, id=f"adjoint-{seed}", objects=objects, materials=materials)
     strategy = dict(strategy, id="adjoint-pt-mis")
     return scene, strategy, (width, height, spp_primal, spp_adjoint)
+
+
+# ------------------------------------------------------------------------- media + spectral workload
+def media_scene(width=1024, height=1024, spp=512, max_depth=64, spectral=True, lambda_range=(380.0, 780.0)):
+    """The media and spectral workload: a sphere of radius 1 with a dielectric boundary
+    (IOR 1.33) holding a chromatic homogeneous medium (sigma_t (0.5, 1.0, 2.0), single-scattering
+    albedo 0.9, HG g 0.6); a second sphere of radius 1 behind a null interface holding a grey
+    medium of sigma_t 2.0 (albedo 0.9, isotropic); a Lambert ground plane (albedo 0.5); lit by a
+    spherical light of radius 0.05 emitting a 3000 K blackbody spectrum and a 1 x 1 quad light
+    of radiance 20; NEE with equiangular placement in the media (the area-light extension),
+    roulette from depth 3, max depth 64; spectral with four hero wavelengths over 380-780 nm.
+    Returns (scene, strategy, (width, height, spp))."""
+    st_rgb = [0.5, 1.0, 2.0]
+    scene = {
+        "id": "media-c3",
+        "objects": [
+            {"type": "plane", "parameters": {"normal": [0, 1, 0], "offset": 0.0}, "material": "ground"},
+            {"type": "sphere", "parameters": {"center": [-1.15, 1.0, 0.0], "radius": 1.0}, "material": "glass_medium"},
+            {"type": "sphere", "parameters": {"center": [1.15, 1.0, 0.0], "radius": 1.0}, "material": "grey_fog"},
+        ],
+        "materials": {
+            "ground": {"model": "lambert", "albedo": [0.5, 0.5, 0.5]},
+            "glass_medium": {"model": "dielectric", "ior": 1.33,
+                             "medium": {"sigma_a": [0.1 * v for v in st_rgb], "sigma_s": [0.9 * v for v in st_rgb],
+                                        "phase_g": 0.6}},
+            "grey_fog": {"model": "none", "medium": {"sigma_a": [0.2] * 3, "sigma_s": [1.8] * 3, "phase_g": 0.0}},
+        },
+        "lights": [
+            {"kind": "sphere", "position": [0.0, 2.4, 1.2], "radius": 0.05,
+             "emission": {"blackbody": {"kelvin": 3000.0, "scale": 400.0}}},
+            # cross(edge1, edge2) = -y: the 1 x 1 panel emits downward
+            {"kind": "quad", "corner": [-0.5, 3.5, -0.5], "edge1": [1.0, 0.0, 0.0], "edge2": [0.0, 0.0, 1.0],
+             "emission": 20.0},
+        ],
+    }
+    meas = {"camera": {"type": "pinhole", "fov": math.radians(45.0), "position": [0.0, 1.4, 5.5],
+                       "target": [0.0, 0.9, 0.0]},
+            "maxBounces": max_depth}
+    if spectral:
+        meas["color"] = "spectral"
+        meas["wavelengthRange"] = list(lambda_range)
+    strategy = {"id": "pt-nee-eq", "measurement": meas,
+                "estimator": {"directLighting": "nee", "russianRoulette": {"startDepth": 3},
+                              "volumeSampling": "analytic", "mediumLightSampling": "equiangular",
+                              "equiangularAreaLights": True, "wavelengths": "visible"},
+                "view": {"tonemap": {"type": "none"}}}
+    return scene, strategy, (width, height, spp)
