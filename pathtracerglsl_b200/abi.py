@@ -132,6 +132,10 @@ class Counters(C.Structure):
 PROFILE_TIMING, PROFILE_WORK = 1, 2
 
 
+class Tuning(C.Structure):
+    _fields_ = [("capacity", C.c_int32), ("block", C.c_int32), ("sort_buckets", C.c_int32), ("pad", C.c_int32)]
+
+
 # Sizes the header documents (checked by the CPU tests).
 EXPECTED_SIZES = {"Region": 80, "Material": 128, "Light": 96, "Spectrum": 32, "SpectralMaterial": 192,
                   "ProgramDesc": 64}

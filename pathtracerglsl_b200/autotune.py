@@ -1,0 +1,67 @@
+"""Autotuner of the wavefront's launch knobs: path-pool capacity, block size and the
+occupant-sort bucket count (ptr_tuning).  No counterpart in the reference (its WebGL engine
+has no such knobs).
+
+``tune(engine, render, candidates)`` times ``render()`` under every candidate on the
+engine's context (device time through ptr_sync, best of ``repeats`` after one untimed
+warm-up), keeps the fastest, applies it to the context and returns a record that
+``save``/``load`` write to and read from a JSON file keyed by workload and GPU name.
+"""
+import itertools
+import json
+import os
+import time
+
+DEFAULT_CANDIDATES = [{"capacity": c, "block": b, "sort_buckets": k}
+                      for c, b, k in itertools.product((1 << 20, 1 << 21, 1 << 22), (128, 256), (1, 8, 16))]
+
+
+def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
+    """Time render() under each candidate tuning; apply and return the best record."""
+    candidates = list(candidates or DEFAULT_CANDIDATES)
+    results = []
+    t_start = time.perf_counter()
+    for cand in candidates:
+        engine.set_tuning(**cand)
+        render()                       # warm-up: pool allocation, graph capture
+        engine.sync()
+        best = float("inf")
+        for _ in range(max(1, repeats)):
+            t0 = time.perf_counter()
+            render()
+            engine.sync()
+            best = min(best, time.perf_counter() - t0)
+        results.append(dict(cand, ms=1000.0 * best))
+        if time.perf_counter() - t_start > budget_s:
+            break
+    best = min(results, key=lambda r: r["ms"])
+    engine.set_tuning(**{k: best[k] for k in ("capacity", "block", "sort_buckets")})
+    return {"best": best, "results": results}
+
+
+def gpu_name():
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:   # no torch / no device: the record still keys by workload
+        return "unknown"
+
+
+def save(path, workload, record):
+    data = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    data.setdefault(gpu_name(), {})[workload] = record
+    with open(path, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+
+
+def load(path, workload):
+    """The recorded best tuning of a workload on this GPU, or None."""
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        data = json.load(f)
+    rec = data.get(gpu_name(), {}).get(workload)
+    return {k: rec["best"][k] for k in ("capacity", "block", "sort_buckets")} if rec else None

@@ -106,6 +106,12 @@ __device__ __forceinline__ bool walk_binary(const DevScene& S, const float4* nod
 
 // ---- compressed wide BVH walk ---------------------------------------------------------------
 __device__ __forceinline__ int find_msb24(unsigned v) { return 31 - __clz(v); }
+// Byte k of word as a float, exactly: the byte is permuted into the mantissa of 2^23
+// (bits 0x4B0000bb) and 2^23 is subtracted.  One PRMT + one FADD on the integer / FMA pipes
+// instead of an I2F conversion (the conversion unit was the walk's busiest pipe).
+__device__ __forceinline__ float byte_as_float(unsigned word, unsigned k) {
+    return __fadd_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u | k)), -8388608.0f);
+}
 __device__ __forceinline__ float clamp_dir(float d) { return fabsf(d) < 1e-20f ? (d < 0.0f ? -1e-20f : 1e-20f) : d; }
 
 // Leaf(item) for one leaf item index (wide-order); returns true to stop.
@@ -149,12 +155,13 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
             const unsigned sh = 8u * (sl & 3u);
             unsigned m = ((sl < 4u ? n1.z : n1.w) >> sh) & 0xFFu;
             if (m == 0u) continue;
-            float qlx = (float)(((sl < 4u ? n2.x : n2.y) >> sh) & 0xFFu);
-            float qly = (float)(((sl < 4u ? n2.z : n2.w) >> sh) & 0xFFu);
-            float qlz = (float)(((sl < 4u ? n3.x : n3.y) >> sh) & 0xFFu);
-            float qhx = (float)(((sl < 4u ? n3.z : n3.w) >> sh) & 0xFFu);
-            float qhy = (float)(((sl < 4u ? n4.x : n4.y) >> sh) & 0xFFu);
-            float qhz = (float)(((sl < 4u ? n4.z : n4.w) >> sh) & 0xFFu);
+            const unsigned kb = sl & 3u;
+            float qlx = byte_as_float(sl < 4u ? n2.x : n2.y, kb);
+            float qly = byte_as_float(sl < 4u ? n2.z : n2.w, kb);
+            float qlz = byte_as_float(sl < 4u ? n3.x : n3.y, kb);
+            float qhx = byte_as_float(sl < 4u ? n3.z : n3.w, kb);
+            float qhy = byte_as_float(sl < 4u ? n4.x : n4.y, kb);
+            float qhz = byte_as_float(sl < 4u ? n4.z : n4.w, kb);
             float lox = __fmaf_rn(qlx, dq.x, oq.x), hix = __fmaf_rn(qhx, dq.x, oq.x);
             float loy = __fmaf_rn(qly, dq.y, oq.y), hiy = __fmaf_rn(qhy, dq.y, oq.y);
             float loz = __fmaf_rn(qlz, dq.z, oq.z), hiz = __fmaf_rn(qhz, dq.z, oq.z);

@@ -64,6 +64,14 @@ struct PathPool {
     float4* wl_pdf;
     float* sh_pdf;
     float* sh2_pdf;
+    // occupant-sorted shading queue: k_closest keys every live path by the occupant it will
+    // shade (material model of the hit, inside a medium or not) and counts the keys; a scan
+    // and a scatter rebuild the live queue grouped by key before k_shade (sort_buckets <= 1:
+    // off, k_shade reads the compacted queue as it is)
+    int sort_buckets;
+    int* q_sorted;
+    unsigned char* sort_key;  // per queue position
+    unsigned* bins;           // [0, 32) counts, [32, 64) running offsets
 };
 
 // Adjoint replay tables: the adjoint image (3 floats per pixel, row 0 at the bottom), the
@@ -410,15 +418,37 @@ __device__ __forceinline__ void flush_work(const DevScene& S, const Work& w) {
     }
 }
 
-// Nearest hit of every live path.
+constexpr int kMaxSortBuckets = 32;
+// Shading class of a live path: 0 miss, 1 + the material model of the surface it hit; with
+// more than 8 buckets, + 8 when its segment starts inside a medium (the medium arm runs first).
+__device__ __forceinline__ unsigned shade_key(const DevScene& S, int region, int cur_med, int buckets) {
+    unsigned k = 0u;
+    if (region >= 0) {
+        const int m = S.regions[region].material;
+        k = 1u + (unsigned)(m >= 0 ? S.materials[m].model : 0);
+    }
+    if (buckets > 8) {
+        const int mm = cur_med < 0 ? S.ambient_material : S.regions[cur_med].material;
+        if (mm >= 0 && (S.materials[mm].flags & PTR_MATF_MEDIUM)) k += 8u;
+    }
+    return k < (unsigned)buckets ? k : (unsigned)buckets - 1u;
+}
+
+// Nearest hit of every live path (and, for the sorted queue, its shading key).
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S0, PathPool pool, int in, BatchTables bt) {
+    __shared__ unsigned s_hist[kMaxSortBuckets];
+    const int buckets = pool.sort_buckets;
     unsigned n = pool.cnt[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         pool.cnt[in ^ 1] = 0u;
         pool.cnt[2] = 0u;
         pool.cnt[4] = 0u;
         pool.stats[0] += n;
+    }
+    if (buckets > 1) {
+        if (threadIdx.x < kMaxSortBuckets) s_hist[threadIdx.x] = 0u;
+        __syncthreads();
     }
     const int* q = pool.q[in];
     Work w{0u, 0u, 0u, 0u};
@@ -431,8 +461,47 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         HitRec h = scene_closest(S, r, COUNT ? &w : nullptr);
         pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
         pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
+        if (buckets > 1) {
+            unsigned key = shade_key(S, h.region, pool.st[i].y, buckets);
+            pool.sort_key[k] = (unsigned char)key;
+            atomicAdd(&s_hist[key], 1u);
+        }
+    }
+    if (buckets > 1) {
+        __syncthreads();
+        if (threadIdx.x < (unsigned)buckets && s_hist[threadIdx.x]) atomicAdd(&pool.bins[threadIdx.x], s_hist[threadIdx.x]);
     }
     if (COUNT) flush_work(S0, w);
+}
+
+// Exclusive scan of the key counts into running offsets; the counts are cleared for the
+// next iteration.  One warp.
+__global__ void k_bin_scan(PathPool pool) {
+    if (threadIdx.x == 0) {
+        unsigned acc = 0u;
+        for (int b = 0; b < pool.sort_buckets; ++b) {
+            unsigned c = pool.bins[b];
+            pool.bins[kMaxSortBuckets + b] = acc;
+            pool.bins[b] = 0u;
+            acc += c;
+        }
+    }
+}
+
+// Scatter the live queue into key order (warp-aggregated slot reservation per key).
+__global__ void k_bin_scatter(PathPool pool, int in) {
+    const unsigned n = pool.cnt[in];
+    const int* q = pool.q[in];
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const unsigned key = pool.sort_key[k];
+        const unsigned mask = __activemask();
+        const unsigned peers = __match_any_sync(mask, key);
+        const int leader = __ffs(peers) - 1;
+        unsigned base = 0u;
+        if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&pool.bins[kMaxSortBuckets + key], (unsigned)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        pool.q_sorted[base + __popc(peers & lanemask_lt())] = q[k];
+    }
 }
 
 // One walk iteration for every live path.
@@ -452,7 +521,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
     extern __shared__ double s_grad[];
     if constexpr (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[in];
-    const int* q = pool.q[in];
+    const int* q = pool.sort_buckets > 1 ? pool.q_sorted : pool.q[in];
     int* qout = pool.q[in ^ 1];
     const bool nee = DIRECT != PTR_DIRECT_NONE;
     const bool mis = DIRECT == PTR_DIRECT_MIS;

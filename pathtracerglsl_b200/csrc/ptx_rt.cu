@@ -29,6 +29,7 @@ struct ptr_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     ptr_program* batch = nullptr;     // path pool + tables of batched renders
+    ptr_tuning tune{1 << 21, 256, 1, 0};   // pool capacity, block size, sort buckets
 };
 
 struct ptr_scene {
@@ -60,6 +61,7 @@ struct ptr_program {
     cudaGraphExec_t graph = nullptr;
     const ptr_scene* graph_scene = nullptr;
     int graph_w = 0, graph_h = 0, graph_iters = 0;
+    ptr_tuning graph_tune{};
     float* graph_samples = nullptr;
     // counters / profiling
     ptr_counters last{};
@@ -106,7 +108,8 @@ int dev_copy(ptr_ctx* ctx, std::vector<void*>& allocs, const T* host, size_t n, 
     return PTR_OK;
 }
 
-int launch_grid(int n_sm) { return n_sm * 8; }   // 8 resident blocks of 256 threads per SM
+// Grid of the grid-stride wavefront kernels: 2048 resident threads per SM.
+int launch_grid(int n_sm, int block = 256) { return n_sm * (2048 / block); }
 
 void free_pool(ptr_program* p) {
     for (void* a : p->pool_allocs) cudaFree(a);
@@ -138,9 +141,14 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
         (rc = get(c * 4, (void**)&q.q[1])) || (rc = get(c * 4, (void**)&q.shq)) ||
         (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
-        (rc = get(64, (void**)&q.wave))) {
+        (rc = get(64, (void**)&q.wave)) || (rc = get(c * 4, (void**)&q.q_sorted)) ||
+        (rc = get(c, (void**)&q.sort_key)) || (rc = get(2 * kMaxSortBuckets * sizeof(unsigned), (void**)&q.bins))) {
         free_pool(p);
         return rc;
+    }
+    if (cudaMemset(q.bins, 0, 2 * kMaxSortBuckets * sizeof(unsigned)) != cudaSuccess) {
+        free_pool(p);
+        return fail(ctx, PTR_E_CUDA, "path pool: clearing the sort bins failed");
     }
     // the second shadow slot only for programs with the per-segment equiangular site
     if (slot2 && ((rc = get(c * 16, (void**)&q.sh2_o)) || (rc = get(c * 16, (void**)&q.sh2_d)) ||
@@ -173,6 +181,11 @@ int wave_iterations(const ptr_program* p, const ptr_scene* s) {
     return it;
 }
 
+// The launch tuning of a program's context; a program without a context (the
+// allocation-free entry point's) launches with the defaults.
+const ptr_tuning kDefaultTuning{1 << 21, 256, 1, 0};
+const ptr_tuning& tuning_of(const ptr_program* p) { return p->ctx ? p->ctx->tune : kDefaultTuning; }
+
 // Event pairs around each launch of an instrumented render (kernel class, start, end).
 struct ProfRec { int cls; cudaEvent_t a, b; };
 
@@ -194,7 +207,6 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     };
     auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
     const DevScene& S = Sp;
-    const PathPool& pool = p->pool;
     ProgParams P;
     P.max_bounces = p->desc.max_bounces;
     P.direct = p->desc.direct;
@@ -203,7 +215,9 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = p->desc.equiangular;
-    const int grid = launch_grid(n_sm), block = 256;
+    const int block = tuning_of(p).block, grid = launch_grid(n_sm, block);
+    PathPool pool = p->pool;
+    pool.sort_buckets = tuning_of(p).sort_buckets;
     ProfRec* r = mark(0);
     const BatchTables nob{};
     k_generate<false, SPECTRAL><<<grid, block, 0, st>>>(S, pool, p->fp_dev);
@@ -213,6 +227,10 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         r = mark(1);
         if (S.work) k_closest<true, false><<<grid, block, 0, st>>>(S, pool, in, nob);
         else k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
+        if (pool.sort_buckets > 1) {   // occupant-sorted shading queue (counted with the traversal)
+            k_bin_scan<<<1, 32, 0, st>>>(pool);
+            k_bin_scatter<<<grid, block, 0, st>>>(pool, in);
+        }
         done(r);
         const bool media = s->has_media != 0;
         r = mark(2);
@@ -271,7 +289,7 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = 0;
-    const int grid = launch_grid(n_sm), block = 256;
+    const int block = tuning_of(p).block, grid = launch_grid(n_sm, block);
     const size_t smem = sizeof(double) * PTR_GRAD_SLOTS * (size_t)S.n_materials;
     const BatchTables nob{};
     const bool media = s->has_media != 0;
@@ -297,9 +315,12 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
 
 // One wave of a batched render: the same kernel sequence over the concatenated job space;
 // scene, program knobs and frame come from the per-job tables.
-void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTables& bt, int direct, bool media,
-                       bool equiangular, cudaStream_t st, int iters, int n_sm, std::vector<ProfRec>* prof = nullptr) {
-    const int grid = launch_grid(n_sm), block = 256;
+void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchTables& bt, int direct, bool media,
+                       bool equiangular, cudaStream_t st, int iters, int n_sm, const ptr_tuning& tune,
+                       std::vector<ProfRec>* prof = nullptr) {
+    const int block = tune.block, grid = launch_grid(n_sm, block);
+    PathPool pool = pool_in;
+    pool.sort_buckets = tune.sort_buckets;
     ProgParams P0{};
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
@@ -318,6 +339,10 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool, const BatchTabl
         int in = it & 1;
         r = mark(1);
         k_closest<false, true><<<grid, block, 0, st>>>(S0, pool, in, bt);
+        if (pool.sort_buckets > 1) {
+            k_bin_scan<<<1, 32, 0, st>>>(pool);
+            k_bin_scatter<<<grid, block, 0, st>>>(pool, in);
+        }
         done(r);
         r = mark(2);
         switch (direct * 2 + (media ? 1 : 0)) {
@@ -634,7 +659,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     }
     const long long total = (long long)npix * f->spp;
     // capacity: whole sample passes when a pass fits the pool, else a chunk of pixels
-    long long cap_max = 1ll << 21;
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::atoll(env);
     if (cap_max < 1024) cap_max = 1024;
     long long cap;
@@ -686,7 +711,8 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     const bool use_graph = std::getenv("PTR_NO_GRAPH") == nullptr && !profiling && !counting;
     if (use_graph) {
         if (!p->graph || p->graph_scene != s || p->graph_w != f->width || p->graph_h != f->height ||
-            p->graph_iters != iters || p->graph_samples != samples_dev) {
+            p->graph_iters != iters || p->graph_samples != samples_dev ||
+            std::memcmp(&p->graph_tune, &ctx->tune, sizeof(ptr_tuning)) != 0) {
             if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
             cudaGraph_t g = nullptr;
             CK(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -701,6 +727,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
             p->graph_h = f->height;
             p->graph_iters = iters;
             p->graph_samples = samples_dev;
+            p->graph_tune = ctx->tune;
         }
         for (long long w = 0; w < waves; ++w) CK(ctx, cudaGraphLaunch(p->graph, st));
     } else if (profiling) {
@@ -989,7 +1016,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         ctx->batch->ctx = ctx;
     }
     ptr_program* bp = ctx->batch;
-    long long cap_max = 1ll << 21;
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
     long long cap = std::min(total, cap_max);
     if (bp->capacity < cap || (equi && !bp->pool.sh2_o)) {
@@ -1033,7 +1060,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         std::vector<ProfRec> prof;
         prof.reserve((size_t)waves * (iters * 3 + 2));
         for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, &prof);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, &prof);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1049,7 +1076,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     } else {
         if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune);
             e = cudaStreamEndCapture(st, &g);
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
@@ -1163,7 +1190,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     cudaStream_t st = ctx->stream;
     const size_t npix = (size_t)f->width * f->height;
     const long long total = (long long)npix * f->spp;
-    long long cap_max = 1ll << 21;
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
     long long cap = (long long)npix <= cap_max ? (cap_max / (long long)npix) * (long long)npix : cap_max;
     if (cap > total) cap = total;
@@ -1252,6 +1279,24 @@ int ptr_update_params(ptr_scene* s, const ptr_material* materials, int n_materia
     CK(ctx, cudaStreamSynchronize(st));   // the host arrays may be released on return
     s->h_materials.assign(materials, materials + n_materials);
     if (regions) s->h_regions.assign(regions, regions + n_regions);
+    return PTR_OK;
+}
+
+int ptr_set_tuning(ptr_ctx* ctx, const ptr_tuning* t) {
+    if (!ctx || !t) return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: null argument");
+    if (t->capacity < 0 || (t->capacity > 0 && t->capacity < 1024) || t->capacity > (1 << 26))
+        return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: capacity must be 0 (default) or in [1024, 2^26]");
+    if (t->block != 128 && t->block != 256) return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: block must be 128 or 256");
+    if (t->sort_buckets < 1 || t->sort_buckets > kMaxSortBuckets)
+        return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: sort_buckets must be in [1, 32]");
+    ctx->tune = *t;
+    ctx->tune.pad = 0;
+    return PTR_OK;
+}
+
+int ptr_get_tuning(ptr_ctx* ctx, ptr_tuning* out) {
+    if (!ctx || !out) return fail(ctx, PTR_E_INVALID, "ptr_get_tuning: null argument");
+    *out = ctx->tune;
     return PTR_OK;
 }
 
