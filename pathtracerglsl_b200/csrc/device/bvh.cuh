@@ -16,6 +16,12 @@
 
 namespace ptx {
 
+#ifndef PTR_CW_NEARFAR
+#define PTR_CW_NEARFAR 0
+#endif
+#ifndef PTR_CW_SMEM_STACK
+#define PTR_CW_SMEM_STACK 0
+#endif
 constexpr float kBvhTfarPad = 1.00000024f;   // BVH_TFAR_PAD (Ize 2013 far-plane pad)
 constexpr int kBvhStack = 64;                // BVH_STACK_DEPTH
 constexpr int kCwStack = 24;                 // CWBVH_STACK_DEPTH
@@ -121,15 +127,31 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
     f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
     unsigned octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
     f3 inv(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
+#if PTR_CW_SMEM_STACK
+    // the node-group stack in shared memory, one column per thread (blocks of <= 256 threads)
+    constexpr int kDepth = 22;   // 22 x 256 x 8 B + the sort histogram stays within 48 KB
+    __shared__ uint2 s_cw_stack[kDepth * 256];
+    uint2* stack_base = s_cw_stack + threadIdx.x;
+#define CW_STACK(i) stack_base[(i) * 256]
+#else
+    constexpr int kDepth = kCwStack;
     uint2 stack[kCwStack];
+#define CW_STACK(i) stack[i]
+#endif
     int ptr = -1;
     unsigned g_base = 0u, g_hits = 1u << (octinv & 7u), g_imask = 1u;
+#if PTR_CW_NEARFAR
+    // the ray's octant picks which quantized bound of each axis is the near plane (the slab
+    // values are the same as min / max of the two, without computing both orders)
+    const bool nx = rdc.x < 0.0f, ny = rdc.y < 0.0f, nz = rdc.z < 0.0f;
+#endif
     for (int guard = 0; guard < 65536; guard++) {
         if (g_hits == 0u) {
             if (ptr < 0) return false;
-            g_base = stack[ptr].x;
-            g_hits = stack[ptr].y & 0xFFu;
-            g_imask = stack[ptr].y >> 8;
+            const uint2 top = CW_STACK(ptr);
+            g_base = top.x;
+            g_hits = top.y & 0xFFu;
+            g_imask = top.y >> 8;
             ptr--;
             continue;
         }
@@ -138,7 +160,7 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
         unsigned slot = ((unsigned)bit ^ octinv) & 7u;
         unsigned child = g_base + __popc(g_imask & ((1u << slot) - 1u));
         if (g_hits != 0u) {
-            if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
+            if (ptr + 1 < kDepth) { ptr++; CW_STACK(ptr) = make_uint2(g_base, g_hits | (g_imask << 8)); }
             else flag_error(S, kErrCwStack);
         }
         const uint4* nd = nodes + 5 * (size_t)child;
@@ -156,17 +178,26 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
             unsigned m = ((sl < 4u ? n1.z : n1.w) >> sh) & 0xFFu;
             if (m == 0u) continue;
             const unsigned kb = sl & 3u;
-            float qlx = byte_as_float(sl < 4u ? n2.x : n2.y, kb);
-            float qly = byte_as_float(sl < 4u ? n2.z : n2.w, kb);
-            float qlz = byte_as_float(sl < 4u ? n3.x : n3.y, kb);
-            float qhx = byte_as_float(sl < 4u ? n3.z : n3.w, kb);
-            float qhy = byte_as_float(sl < 4u ? n4.x : n4.y, kb);
-            float qhz = byte_as_float(sl < 4u ? n4.z : n4.w, kb);
+            const unsigned wlx = sl < 4u ? n2.x : n2.y, wly = sl < 4u ? n2.z : n2.w, wlz = sl < 4u ? n3.x : n3.y;
+            const unsigned whx = sl < 4u ? n3.z : n3.w, why = sl < 4u ? n4.x : n4.y, whz = sl < 4u ? n4.z : n4.w;
+#if PTR_CW_NEARFAR
+            float nearx = __fmaf_rn(byte_as_float(nx ? whx : wlx, kb), dq.x, oq.x);
+            float fary = __fmaf_rn(byte_as_float(ny ? wly : why, kb), dq.y, oq.y);
+            float neary = __fmaf_rn(byte_as_float(ny ? why : wly, kb), dq.y, oq.y);
+            float farx = __fmaf_rn(byte_as_float(nx ? wlx : whx, kb), dq.x, oq.x);
+            float nearz = __fmaf_rn(byte_as_float(nz ? whz : wlz, kb), dq.z, oq.z);
+            float farz = __fmaf_rn(byte_as_float(nz ? wlz : whz, kb), dq.z, oq.z);
+            float tn = gmax(gmax(nearx, neary), gmax(nearz, 0.0f));
+            float tf = gmin(gmin(farx, fary), gmin(farz, tmax)) * kBvhTfarPad;
+#else
+            float qlx = byte_as_float(wlx, kb), qly = byte_as_float(wly, kb), qlz = byte_as_float(wlz, kb);
+            float qhx = byte_as_float(whx, kb), qhy = byte_as_float(why, kb), qhz = byte_as_float(whz, kb);
             float lox = __fmaf_rn(qlx, dq.x, oq.x), hix = __fmaf_rn(qhx, dq.x, oq.x);
             float loy = __fmaf_rn(qly, dq.y, oq.y), hiy = __fmaf_rn(qhy, dq.y, oq.y);
             float loz = __fmaf_rn(qlz, dq.z, oq.z), hiz = __fmaf_rn(qhz, dq.z, oq.z);
             float tn = gmax(gmax(gmin(lox, hix), gmin(loy, hiy)), gmax(gmin(loz, hiz), 0.0f));
             float tf = gmin(gmin(gmax(lox, hix), gmax(loy, hiy)), gmin(gmax(loz, hiz), tmax)) * kBvhTfarPad;
+#endif
             if (tf < tn) continue;
             if ((m & 0xE0u) == 0x20u && (m & 0x1Fu) >= 24u) hits |= 1u << ((((m & 0x1Fu) - 24u) ^ octinv) & 7u);
             else leaf_bits |= (m >> 5) << (m & 0x1Fu);
@@ -181,6 +212,7 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
     }
     flag_error(S, kErrCwGuard);
     return false;
+#undef CW_STACK
 }
 
 // ---- one mesh BLAS in a given frame (ro/rd already in the mesh's local frame) --------------

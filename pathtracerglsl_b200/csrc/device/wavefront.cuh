@@ -72,6 +72,35 @@ struct PathPool {
     int* q_sorted;
     unsigned char* sort_key;  // per queue position
     unsigned* bins;           // [0, 32) counts, [32, 64) running offsets
+    // work tickets of the queue kernels ([0] k_closest, [1] / [2] k_shadow slots 0 / 1,
+    // [3] k_shade), each cleared by the kernel that runs before its consumer; NULL: the
+    // kernels fall back to a static grid-stride loop
+    unsigned* fetch;
+};
+
+// Warp-uniform cursor over a device-counted queue.  With a ticket counter every warp takes
+// the next 32 entries when it is done with its last ones, so warps whose rays are long do
+// not hold the others' work back (dynamic balance on a one-wave resident grid); without
+// one, a grid-stride loop whose trip count is rounded to whole warps.
+struct QueueCursor {
+    unsigned n, stride, k;
+    unsigned* ticket;
+    __device__ __forceinline__ QueueCursor(unsigned n_, unsigned* t) : n(n_), ticket(t) {
+        stride = gridDim.x * blockDim.x;
+        k = blockIdx.x * blockDim.x + threadIdx.x - stride;
+    }
+    __device__ __forceinline__ bool next(unsigned& out) {
+        if (ticket) {
+            unsigned base = 0u;
+            if ((threadIdx.x & 31u) == 0u) base = atomicAdd(ticket, 32u);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            out = base + (threadIdx.x & 31u);
+            return base < n;
+        }
+        k += stride;
+        out = k;
+        return k < ((n + 31u) & ~31u);
+    }
 };
 
 // Adjoint replay tables: the adjoint image (3 floats per pixel, row 0 at the bottom), the
@@ -358,6 +387,7 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, Adj
         pool.cnt[0] = (unsigned)n;
         pool.wave[1] = n;
         pool.stats[2] += (unsigned long long)n;
+        if (pool.fetch) pool.fetch[0] = 0u;
     }
     const long long npix = (long long)F.width * F.height;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -445,6 +475,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         pool.cnt[2] = 0u;
         pool.cnt[4] = 0u;
         pool.stats[0] += n;
+        if (pool.fetch) { pool.fetch[1] = 0u; pool.fetch[2] = 0u; pool.fetch[3] = 0u; }
     }
     if (buckets > 1) {
         if (threadIdx.x < kMaxSortBuckets) s_hist[threadIdx.x] = 0u;
@@ -452,7 +483,10 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     }
     const int* q = pool.q[in];
     Work w{0u, 0u, 0u, 0u};
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
+    unsigned k;
+    while (cur.next(k)) {
+        if (k >= n) continue;
         int i = q[k];
         const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         Ray r;
@@ -525,9 +559,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
     int* qout = pool.q[in ^ 1];
     const bool nee = DIRECT != PTR_DIRECT_NONE;
     const bool mis = DIRECT == PTR_DIRECT_MIS;
-    const unsigned stride = gridDim.x * blockDim.x;
-    const unsigned n_round = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n_round + 0u; k += stride) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && pool.fetch) pool.fetch[0] = 0u;   // the next k_closest's ticket
+    QueueCursor cur(n, pool.fetch ? pool.fetch + 3 : nullptr);
+    unsigned k;
+    while (cur.next(k)) {
         bool alive = false, shadow = false, shadow2 = false;
         int i = -1;
         if (k < n) {
@@ -875,7 +910,10 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     const float4* a_lp = slot ? pool.sh2_lp : pool.sh_lp;
     const float4* a_c = slot ? pool.sh2_c : pool.sh_c;
     Work wk{0u, 0u, 0u, 0u};
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    QueueCursor cur(n, pool.fetch ? pool.fetch + 1 + slot : nullptr);
+    unsigned k;
+    while (cur.next(k)) {
+        if (k >= n) continue;
         int i = shq[k];
         const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
@@ -1015,6 +1053,7 @@ __global__ void k_generate_batch(PathPool pool, BatchTables bt) {
         pool.cnt[0] = (unsigned)n;
         pool.wave[1] = n;
         pool.stats[2] += (unsigned long long)n;
+        if (pool.fetch) pool.fetch[0] = 0u;
     }
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         long long g = base + i;

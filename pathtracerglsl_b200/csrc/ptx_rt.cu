@@ -10,7 +10,9 @@
 #include <cuda_runtime.h>
 #include <chrono>
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -111,6 +113,38 @@ int dev_copy(ptr_ctx* ctx, std::vector<void*>& allocs, const T* host, size_t n, 
 // Grid of the grid-stride wavefront kernels: 2048 resident threads per SM.
 int launch_grid(int n_sm, int block = 256) { return n_sm * (2048 / block); }
 
+// One wave of resident blocks per SM for a kernel (the occupancy calculator's figure for its
+// registers / shared memory at this block size, cached per kernel): a grid-stride kernel
+// sized for more blocks than fit runs them in a second wave whose tail leaves SMs idle.
+int resident_grid(const void* kern, int block, size_t smem, int n_sm) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, size_t>, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_tuple(kern, block, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second * n_sm;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, block, smem) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 2048 / block;
+    }
+    cache[key] = nb;
+    return nb * n_sm;
+}
+
+// Launches a wavefront kernel on its resident grid.  A dry launcher only fills the
+// occupancy cache (run once outside stream capture, before the first captured wave).
+struct Launcher {
+    int block, n_sm;
+    cudaStream_t st;
+    bool dry;
+    template <class... KA, class... A>
+    void operator()(void (*kern)(KA...), size_t smem, A... args) const {
+        const int g = resident_grid((const void*)kern, block, smem, n_sm);
+        if (!dry) kern<<<g, block, smem, st>>>(args...);
+    }
+};
+
 void free_pool(ptr_program* p) {
     for (void* a : p->pool_allocs) cudaFree(a);
     p->pool_allocs.clear();
@@ -142,11 +176,13 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
         (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
         (rc = get(64, (void**)&q.wave)) || (rc = get(c * 4, (void**)&q.q_sorted)) ||
-        (rc = get(c, (void**)&q.sort_key)) || (rc = get(2 * kMaxSortBuckets * sizeof(unsigned), (void**)&q.bins))) {
+        (rc = get(c, (void**)&q.sort_key)) || (rc = get(2 * kMaxSortBuckets * sizeof(unsigned), (void**)&q.bins)) ||
+        (rc = get(4 * sizeof(unsigned), (void**)&q.fetch))) {
         free_pool(p);
         return rc;
     }
-    if (cudaMemset(q.bins, 0, 2 * kMaxSortBuckets * sizeof(unsigned)) != cudaSuccess) {
+    if (cudaMemset(q.bins, 0, 2 * kMaxSortBuckets * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(q.fetch, 0, 4 * sizeof(unsigned)) != cudaSuccess) {
         free_pool(p);
         return fail(ctx, PTR_E_CUDA, "path pool: clearing the sort bins failed");
     }
@@ -191,7 +227,7 @@ struct ProfRec { int cls; cudaEvent_t a, b; };
 
 template <class Col>
 void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
-                   std::vector<ProfRec>* prof, bool film) {
+                   std::vector<ProfRec>* prof, bool film, bool dry) {
     constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     DevScene Sp = s->dev;
     Sp.accel = p->desc.accel;
@@ -215,32 +251,33 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = p->desc.equiangular;
-    const int block = tuning_of(p).block, grid = launch_grid(n_sm, block);
+    const int block = tuning_of(p).block;
+    const Launcher L{block, n_sm, st, dry};
     PathPool pool = p->pool;
     pool.sort_buckets = tuning_of(p).sort_buckets;
     ProfRec* r = mark(0);
     const BatchTables nob{};
-    k_generate<false, SPECTRAL><<<grid, block, 0, st>>>(S, pool, p->fp_dev);
+    L(k_generate<false, SPECTRAL>, 0, S, pool, p->fp_dev, AdjParams{});
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
         r = mark(1);
-        if (S.work) k_closest<true, false><<<grid, block, 0, st>>>(S, pool, in, nob);
-        else k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
+        if (S.work) L(k_closest<true, false>, 0, S, pool, in, nob);
+        else L(k_closest<false, false>, 0, S, pool, in, nob);
         if (pool.sort_buckets > 1) {   // occupant-sorted shading queue (counted with the traversal)
-            k_bin_scan<<<1, 32, 0, st>>>(pool);
-            k_bin_scatter<<<grid, block, 0, st>>>(pool, in);
+            if (!dry) k_bin_scan<<<1, 32, 0, st>>>(pool);
+            L(k_bin_scatter, 0, pool, in);
         }
         done(r);
         const bool media = s->has_media != 0;
         r = mark(2);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<Col, PTR_DIRECT_NONE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 1: k_shade<Col, PTR_DIRECT_NONE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 2: k_shade<Col, PTR_DIRECT_NEE, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 3: k_shade<Col, PTR_DIRECT_NEE, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            case 4: k_shade<Col, PTR_DIRECT_MIS, false, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
-            default: k_shade<Col, PTR_DIRECT_MIS, true, false><<<grid, block, 0, st>>>(S, pool, P, in, nob); break;
+            case 0: L(k_shade<Col, PTR_DIRECT_NONE, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            case 1: L(k_shade<Col, PTR_DIRECT_NONE, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            case 2: L(k_shade<Col, PTR_DIRECT_NEE, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            case 3: L(k_shade<Col, PTR_DIRECT_NEE, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            case 4: L(k_shade<Col, PTR_DIRECT_MIS, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            default: L(k_shade<Col, PTR_DIRECT_MIS, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
         }
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
@@ -250,11 +287,11 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
                 if (S.work) {
                     DevScene Sq = S;
                     Sq.work = S.work + 4;   // the shadow queries' own tallies
-                    if (media) k_shadow<Col, true, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
-                    else k_shadow<Col, false, true, false><<<grid, block, 0, st>>>(Sq, pool, P, nob, slot);
+                    if (media) L(k_shadow<Col, true, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
+                    else L(k_shadow<Col, false, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
                 } else {
-                    if (media) k_shadow<Col, true, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
-                    else k_shadow<Col, false, false, false><<<grid, block, 0, st>>>(S, pool, P, nob, slot);
+                    if (media) L(k_shadow<Col, true, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
+                    else L(k_shadow<Col, false, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
                 }
             }
             done(r);
@@ -262,15 +299,15 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     }
     if (!film) return;
     r = mark(4);
-    k_film<SPECTRAL><<<grid, block, 0, st>>>(pool, p->fp_dev, p->sum, p->sumsq, samples, S);
-    k_advance<<<1, 32, 0, st>>>(pool);
+    L(k_film<SPECTRAL>, 0, pool, p->fp_dev, p->sum, p->sumsq, samples, S);
+    if (!dry) k_advance<<<1, 32, 0, st>>>(pool);
     done(r);
 }
 
 void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
-                 std::vector<ProfRec>* prof = nullptr, bool film = true) {
-    if (p->desc.color == PTR_COLOR_SPECTRAL) launch_wave_t<s4>(p, s, st, iters, samples, n_sm, prof, film);
-    else launch_wave_t<f3>(p, s, st, iters, samples, n_sm, prof, film);
+                 std::vector<ProfRec>* prof = nullptr, bool film = true, bool dry = false) {
+    if (p->desc.color == PTR_COLOR_SPECTRAL) launch_wave_t<s4>(p, s, st, iters, samples, n_sm, prof, film, dry);
+    else launch_wave_t<f3>(p, s, st, iters, samples, n_sm, prof, film, dry);
 }
 
 
@@ -289,25 +326,26 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = 0;
-    const int block = tuning_of(p).block, grid = launch_grid(n_sm, block);
+    const int block = tuning_of(p).block;
+    const Launcher L{block, n_sm, st, false};
     const size_t smem = sizeof(double) * PTR_GRAD_SLOTS * (size_t)S.n_materials;
     const BatchTables nob{};
     const bool media = s->has_media != 0;
-    k_generate<true><<<grid, block, 0, st>>>(S, pool, p->fp_dev, adj);
+    L(k_generate<true>, 0, S, pool, p->fp_dev, adj);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
-        k_closest<false, false><<<grid, block, 0, st>>>(S, pool, in, nob);
+        L(k_closest<false, false>, 0, S, pool, in, nob);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<f3, PTR_DIRECT_NONE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 1: k_shade<f3, PTR_DIRECT_NONE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 2: k_shade<f3, PTR_DIRECT_NEE, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 3: k_shade<f3, PTR_DIRECT_NEE, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            case 4: k_shade<f3, PTR_DIRECT_MIS, false, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
-            default: k_shade<f3, PTR_DIRECT_MIS, true, false, true><<<grid, block, smem, st>>>(S, pool, P, in, nob, adj); break;
+            case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, false, true>, smem, S, pool, P, in, nob, adj); break;
+            case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, false, true>, smem, S, pool, P, in, nob, adj); break;
+            case 2: L(k_shade<f3, PTR_DIRECT_NEE, false, false, true>, smem, S, pool, P, in, nob, adj); break;
+            case 3: L(k_shade<f3, PTR_DIRECT_NEE, true, false, true>, smem, S, pool, P, in, nob, adj); break;
+            case 4: L(k_shade<f3, PTR_DIRECT_MIS, false, false, true>, smem, S, pool, P, in, nob, adj); break;
+            default: L(k_shade<f3, PTR_DIRECT_MIS, true, false, true>, smem, S, pool, P, in, nob, adj); break;
         }
         if (P.direct != PTR_DIRECT_NONE) {
-            if (media) k_shadow<f3, true, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
-            else k_shadow<f3, false, false, false, true><<<grid, block, smem, st>>>(S, pool, P, nob, 0, adj);
+            if (media) L(k_shadow<f3, true, false, false, true>, smem, S, pool, P, nob, 0, adj);
+            else L(k_shadow<f3, false, false, false, true>, smem, S, pool, P, nob, 0, adj);
         }
     }
     k_advance<<<1, 32, 0, st>>>(pool);
@@ -317,8 +355,9 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
 // scene, program knobs and frame come from the per-job tables.
 void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchTables& bt, int direct, bool media,
                        bool equiangular, cudaStream_t st, int iters, int n_sm, const ptr_tuning& tune,
-                       std::vector<ProfRec>* prof = nullptr) {
-    const int block = tune.block, grid = launch_grid(n_sm, block);
+                       std::vector<ProfRec>* prof = nullptr, bool dry = false) {
+    const int block = tune.block;
+    const Launcher L{block, n_sm, st, dry};
     PathPool pool = pool_in;
     pool.sort_buckets = tune.sort_buckets;
     ProgParams P0{};
@@ -333,39 +372,39 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
     };
     auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
     ProfRec* r = mark(0);
-    k_generate_batch<<<grid, block, 0, st>>>(pool, bt);
+    L(k_generate_batch, 0, pool, bt);
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
         r = mark(1);
-        k_closest<false, true><<<grid, block, 0, st>>>(S0, pool, in, bt);
+        L(k_closest<false, true>, 0, S0, pool, in, bt);
         if (pool.sort_buckets > 1) {
-            k_bin_scan<<<1, 32, 0, st>>>(pool);
-            k_bin_scatter<<<grid, block, 0, st>>>(pool, in);
+            if (!dry) k_bin_scan<<<1, 32, 0, st>>>(pool);
+            L(k_bin_scatter, 0, pool, in);
         }
         done(r);
         r = mark(2);
         switch (direct * 2 + (media ? 1 : 0)) {
-            case 0: k_shade<f3, PTR_DIRECT_NONE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 1: k_shade<f3, PTR_DIRECT_NONE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 2: k_shade<f3, PTR_DIRECT_NEE, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 3: k_shade<f3, PTR_DIRECT_NEE, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            case 4: k_shade<f3, PTR_DIRECT_MIS, false, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
-            default: k_shade<f3, PTR_DIRECT_MIS, true, true><<<grid, block, 0, st>>>(S0, pool, P0, in, bt); break;
+            case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            case 2: L(k_shade<f3, PTR_DIRECT_NEE, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            case 3: L(k_shade<f3, PTR_DIRECT_NEE, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            case 4: L(k_shade<f3, PTR_DIRECT_MIS, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            default: L(k_shade<f3, PTR_DIRECT_MIS, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
         }
         done(r);
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
             for (int slot = equiangular ? 1 : 0; slot >= 0; --slot) {
-                if (media) k_shadow<f3, true, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
-                else k_shadow<f3, false, false, true><<<grid, block, 0, st>>>(S0, pool, P0, bt, slot);
+                if (media) L(k_shadow<f3, true, false, true>, 0, S0, pool, P0, bt, slot, AdjParams{});
+                else L(k_shadow<f3, false, false, true>, 0, S0, pool, P0, bt, slot, AdjParams{});
             }
             done(r);
         }
     }
     r = mark(4);
-    k_film_batch<<<grid, block, 0, st>>>(pool, bt);
-    k_advance<<<1, 32, 0, st>>>(pool);
+    L(k_film_batch, 0, pool, bt);
+    if (!dry) k_advance<<<1, 32, 0, st>>>(pool);
     done(r);
 }
 
@@ -715,6 +754,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
             std::memcmp(&p->graph_tune, &ctx->tune, sizeof(ptr_tuning)) != 0) {
             if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
             cudaGraph_t g = nullptr;
+            launch_wave(p, s, st, iters, samples_dev, n_sm, nullptr, true, true);   // occupancy queries, outside capture
             CK(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             launch_wave(p, s, st, iters, samples_dev, n_sm);
             cudaError_t ce = cudaStreamEndCapture(st, &g);
@@ -1074,6 +1114,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
             cudaEventDestroy(pr.b);
         }
     } else {
+        // occupancy queries outside capture, then the captured wave
+        launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, nullptr, true);
         if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune);
