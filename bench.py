@@ -246,6 +246,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per launch of the roofline kernel, from one ncu capture of one whole wave of the
+# same command (profiles/k_closest_mesh_full.md, profiles/k_shade_cornell_full.md):
+# (workload, kernel) -> bytes per launch averaged over the wave's launches.
+NCU_TRAFFIC = {("mesh", "closest"): 58.77e6, ("cornell", "shade"): 288.2e6}
+# the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
+ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
+
+
 def algorithmic_bytes(kernel, c, cw=True):
     """Bytes the algorithm must move per render for one kernel class.  Path state: the
     SoA records each kernel reads and writes.  Traversal: every node popped (80 B wide /
@@ -343,14 +351,16 @@ def run_ours(args):
     eng.reset()
     eng.profile_render(w, h, spp, _abi.PROFILE_WORK)
     cnt = eng.counters()
-    kernel, (kms, klaunch) = max(prof.items(), key=lambda kv: kv[1][0])
+    kernel = ROOFLINE_KERNEL.get(args.workload) or max(prof.items(), key=lambda kv: kv[1][0])[0]
+    kms, klaunch = prof[kernel]
     peak, peak_kind = measured_peaks()
     launch_ms = kms / max(klaunch, 1)
     bytes_per_launch = algorithmic_bytes(kernel, cnt, cfg.get("mesh_accel", "cwbvh") == "cwbvh") / max(klaunch, 1)
     achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9
     total_prof_ms = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": "k_" + kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": NCU_TRAFFIC.get((args.workload, kernel)),
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                 "share": {k: v[0] / total_prof_ms for k, v in prof.items()}}
     # the film class is k_film + k_advance per wave; + the frame-parameter kernel
