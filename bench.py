@@ -169,25 +169,15 @@ def cpu_baseline(sc, st, w, h, spp, seconds=10.0):
 
 
 def dist_setup(gpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    if world <= 1:
-        return 0, 0, 1, None
-    import torch
-    import torch.distributed as dist
-    import datetime
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    return dist.get_rank(), local, world, dist
+    """One process per GPU (torchrun's environment): replicas, NCCL for the barrier and the
+    max over ranks (pathtracerglsl_b200.replicas)."""
+    from pathtracerglsl_b200.replicas import Replicas
+    r = Replicas.from_env("nccl")
+    return r.rank, r.local, r.world, (r if r.world > 1 else None)
 
 
 def reduce_max(dist, x):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return x if dist is None else dist.max(x)
 
 
 def barrier(dist):
@@ -392,7 +382,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:
-        dist.destroy_process_group()
+        dist.close()
 
 
 # ---------------------------------------------------------------------------------- batch
@@ -513,7 +503,7 @@ def run_batch(args):
     b.close()
     eng.close()
     if dist is not None:
-        dist.destroy_process_group()
+        dist.close()
 
 
 # ---------------------------------------------------------------------------------- adjoint
@@ -640,7 +630,7 @@ def run_adjoint(args):
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:
-        dist.destroy_process_group()
+        dist.close()
 
 
 def main():

@@ -51,11 +51,14 @@ SIGNATURES = {
 _lib = None
 
 
-def load(path=LIB_PATH):
-    """Load the library and bind every entry point; raises if anything is missing."""
+def load(path=None):
+    """Load the library and bind every entry point; raises if anything is missing.
+    PTX_RT_LIB names another build of the same library (e.g. one compiled with different
+    launch bounds, for an A/B measurement)."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("PTX_RT_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise RuntimeError(f"CUDA library not built: {path} (run pathtracerglsl_b200.build.build())")
     lib = C.CDLL(path)
