@@ -217,7 +217,9 @@ typedef struct ptr_program_desc {
     int32_t wavelengths;        /* PTR_WAVELENGTHS_*  (estimator.wavelengths)          */
     float lambda_min;           /* sampled range, nm (the reference's 360..830)        */
     float lambda_max;
-    int32_t pad[3];
+    int32_t instance_accel;     /* PTR_ACCEL_* of instanced batches' TLAS (estimator.instanceAccel:
+                                   'tlas' binary, 'cwbvh' wide; intersection/index.ts:68-159) */
+    int32_t pad[2];
 } ptr_program_desc;
 
 /* The per-frame builtins + camera uniforms (Engine.ts:231-258, camera.ts:69-160). */

@@ -104,7 +104,8 @@ class ProgramDesc(C.Structure):
                 ("max_null_crossings", C.c_int32), ("direct", C.c_int32), ("rr_start", C.c_int32),
                 ("rr_max_survival", C.c_float), ("scattering", C.c_int32), ("accel", C.c_int32),
                 ("equiangular", C.c_int32), ("color", C.c_int32), ("wavelengths", C.c_int32),
-                ("lambda_min", C.c_float), ("lambda_max", C.c_float), ("pad", C.c_int32 * 3)]
+                ("lambda_min", C.c_float), ("lambda_max", C.c_float), ("instance_accel", C.c_int32),
+                ("pad", C.c_int32 * 2)]
 
 
 class Camera(C.Structure):

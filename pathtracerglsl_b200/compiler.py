@@ -141,7 +141,9 @@ PRIMITIVES = {"plane": abi.SHAPE_PLANE, "sphere": abi.SHAPE_SPHERE, "quad": abi.
               "box": abi.SHAPE_BOX}
 LIGHT_KINDS = {"quad": abi.LIGHT_QUAD, "sphere": abi.LIGHT_SPHERE, "point": abi.LIGHT_POINT}
 DIRECT = {"none": abi.DIRECT_NONE, "nee": abi.DIRECT_NEE, "mis": abi.DIRECT_MIS}
-ACCELS = {"bvh": abi.ACCEL_BVH, "tlas": abi.ACCEL_BVH, "cwbvh": abi.ACCEL_CWBVH}
+# meshTraversal 'bvh' / 'cwbvh'; instanceAccel 'tlas' / 'cwbvh' ('linear', the reference's
+# scan over every instance, returns the same nearest hit: it walks the binary TLAS here)
+ACCELS = {"bvh": abi.ACCEL_BVH, "tlas": abi.ACCEL_BVH, "linear": abi.ACCEL_BVH, "cwbvh": abi.ACCEL_CWBVH}
 THIN_SHAPES = {"quad"}
 
 
@@ -739,7 +741,8 @@ class Compiler:
         prog.rr_start = int(rr.get("startDepth", 0)) if rr else -1
         prog.rr_max_survival = float(rr.get("maxSurvival", 0.95)) if rr else 1.0
         prog.scattering = 0 if meas.get("scattering") == "ignored" else 1
-        prog.accel = ACCELS[est.get("meshTraversal") or est.get("instanceAccel") or "bvh"]
+        prog.accel = ACCELS[est.get("meshTraversal") or "bvh"]                 # mesh BLAS walk
+        prog.instance_accel = ACCELS[est.get("instanceAccel") or "tlas"]       # instanced batches' TLAS
         prog.color = abi.COLOR_SPECTRAL if meas.get("color", "rgb") == "spectral" else abi.COLOR_RGB
         prog.wavelengths = abi.WAVELENGTHS_UNIFORM if est.get("wavelengths") == "uniform" else abi.WAVELENGTHS_VISIBLE
         lo, hi = meas.get("wavelengthRange", [360.0, 830.0])

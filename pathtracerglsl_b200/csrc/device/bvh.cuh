@@ -19,9 +19,6 @@ namespace ptx {
 #ifndef PTR_CW_NEARFAR
 #define PTR_CW_NEARFAR 0
 #endif
-#ifndef PTR_CW_SMEM_STACK
-#define PTR_CW_SMEM_STACK 0
-#endif
 constexpr float kBvhTfarPad = 1.00000024f;   // BVH_TFAR_PAD (Ize 2013 far-plane pad)
 constexpr int kBvhStack = 64;                // BVH_STACK_DEPTH
 constexpr int kCwStack = 24;                 // CWBVH_STACK_DEPTH
@@ -127,17 +124,11 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
     f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
     unsigned octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
     f3 inv(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
-#if PTR_CW_SMEM_STACK
-    // the node-group stack in shared memory, one column per thread (blocks of <= 256 threads)
-    constexpr int kDepth = 22;   // 22 x 256 x 8 B + the sort histogram stays within 48 KB
-    __shared__ uint2 s_cw_stack[kDepth * 256];
-    uint2* stack_base = s_cw_stack + threadIdx.x;
-#define CW_STACK(i) stack_base[(i) * 256]
-#else
+    // node-group stack in thread-local memory (a wide TLAS walk nests a BLAS walk inside
+    // its leaves, each with its own stack)
     constexpr int kDepth = kCwStack;
     uint2 stack[kCwStack];
 #define CW_STACK(i) stack[i]
-#endif
     int ptr = -1;
     unsigned g_base = 0u, g_hits = 1u << (octinv & 7u), g_imask = 1u;
 #if PTR_CW_NEARFAR
@@ -285,27 +276,35 @@ __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_regio
     }
     const DevBatch& b = S.batches[g.ref];
     float t_near = h.t;
-    walk_binary(S, b.tlas, r.o, r.d, t_near, [&](int off, int cnt) {
-        for (int i = off; i < off + cnt; ++i) {
-            if (b.proto_shape == PTR_SHAPE_SPHERE) {
-                float4 rec = __ldg(b.place + 2 * i);
-                float t;
-                if (sphere_intersect(r, xyz(rec), rec.w, t) && t < t_near) {
-                    t_near = t; h.t = t; h.region = region; h.element = i; h.prim = -1;
-                }
-            } else {
-                float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
-                float s = ts.w;
-                if (w) w->inst++;
-                f3 ro = placement_rigid(q, ts, r.o) / s;
-                f3 rd = qrot(q, r.d) / s;
-                int prim = -1;
-                float t = t_near;
-                if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim, w)) {
-                    t_near = t; h.t = t; h.region = region; h.element = i; h.prim = prim;
-                }
+    const bool wide = S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w;
+    const float4* place = wide ? b.place_w : b.place;
+    // one instance: the params-tier sphere, or the mesh prototype in the placement's frame
+    auto instance = [&](int i) {
+        if (b.proto_shape == PTR_SHAPE_SPHERE) {
+            float4 rec = __ldg(place + 2 * i);
+            float t;
+            if (sphere_intersect(r, xyz(rec), rec.w, t) && t < t_near) {
+                t_near = t; h.t = t; h.region = region; h.element = i; h.prim = -1;
+            }
+        } else {
+            float4 q = __ldg(place + 2 * i), ts = __ldg(place + 2 * i + 1);
+            float s = ts.w;
+            if (w) w->inst++;
+            f3 ro = placement_rigid(q, ts, r.o) / s;
+            f3 rd = qrot(q, r.d) / s;
+            int prim = -1;
+            float t = t_near;
+            if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim, w)) {
+                t_near = t; h.t = t; h.region = region; h.element = i; h.prim = prim;
             }
         }
+    };
+    if (wide) {   // the reference's CWBVH instance accel (intersection/index.ts:99-158)
+        walk_wide(S, b.tlas_w, r.o, r.d, t_near, [&](int i) { instance(i); return false; }, w ? &w->tlas : nullptr);
+        return;
+    }
+    walk_binary(S, b.tlas, r.o, r.d, t_near, [&](int off, int cnt) {
+        for (int i = off; i < off + cnt; ++i) instance(i);
         return false;
     }, w ? &w->tlas : nullptr);
 }
@@ -314,21 +313,25 @@ __device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g
                                           Work* w = nullptr) {
     if (g.shape == PTR_SHAPE_MESH) return mesh_any(S, S.meshes[g.ref], r.o, r.d, max_dist, w);
     const DevBatch& b = S.batches[g.ref];
-    return walk_binary(S, b.tlas, r.o, r.d, max_dist, [&](int off, int cnt) {
-        for (int i = off; i < off + cnt; ++i) {
-            if (b.proto_shape == PTR_SHAPE_SPHERE) {
-                float4 rec = __ldg(b.place + 2 * i);
-                float t;
-                if (sphere_intersect(r, xyz(rec), rec.w, t) && t < max_dist) return true;
-            } else {
-                float4 q = __ldg(b.place + 2 * i), ts = __ldg(b.place + 2 * i + 1);
-                float s = ts.w;
-                if (w) w->inst++;
-                f3 ro = placement_rigid(q, ts, r.o) / s;
-                f3 rd = qrot(q, r.d) / s;
-                if (mesh_any(S, S.meshes[b.proto_mesh], ro, rd, max_dist, w)) return true;
-            }
+    const bool wide = S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w;
+    const float4* place = wide ? b.place_w : b.place;
+    auto instance = [&](int i) -> bool {
+        if (b.proto_shape == PTR_SHAPE_SPHERE) {
+            float4 rec = __ldg(place + 2 * i);
+            float t;
+            return sphere_intersect(r, xyz(rec), rec.w, t) && t < max_dist;
         }
+        float4 q = __ldg(place + 2 * i), ts = __ldg(place + 2 * i + 1);
+        float s = ts.w;
+        if (w) w->inst++;
+        f3 ro = placement_rigid(q, ts, r.o) / s;
+        f3 rd = qrot(q, r.d) / s;
+        return mesh_any(S, S.meshes[b.proto_mesh], ro, rd, max_dist, w);
+    };
+    if (wide) return walk_wide(S, b.tlas_w, r.o, r.d, max_dist, instance, w ? &w->tlas : nullptr);
+    return walk_binary(S, b.tlas, r.o, r.d, max_dist, [&](int off, int cnt) {
+        for (int i = off; i < off + cnt; ++i)
+            if (instance(i)) return true;
         return false;
     }, w ? &w->tlas : nullptr);
 }
@@ -371,14 +374,16 @@ __device__ __forceinline__ f3 accel_hit_normal(const DevScene& S, const ptr_regi
     h.eps = fp_uncertainty(h.p);
     if (g.shape == PTR_SHAPE_INSTANCES) {
         const DevBatch& b = S.batches[g.ref];
+        // hr.element indexes the placements of the TLAS the hit was found with
+        const float4* place = (S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w) ? b.place_w : b.place;
         if (b.proto_shape == PTR_SHAPE_SPHERE) {
-            float4 rec = __ldg(b.place + 2 * hr.element);
+            float4 rec = __ldg(place + 2 * hr.element);
             f3 n = normalize(h.p - xyz(rec));
             ng = n;   // a primitive's normal is its true surface normal (set from frame.n)
             return n;
         }
         const DevMesh& m = S.meshes[b.proto_mesh];
-        float4 q = __ldg(b.place + 2 * hr.element);
+        float4 q = __ldg(place + 2 * hr.element);
         const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
         f3 a, e1, e2;
         load_tri(tri, hr.prim, a, e1, e2);

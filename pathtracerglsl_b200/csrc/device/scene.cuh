@@ -29,6 +29,8 @@ struct DevBatch {
     const float4* place;
     const float4* tlas;       // binary BVH over the instances' world boxes
     int n_inst, proto_shape, proto_mesh, n_tlas;
+    const uint4* tlas_w;      // compressed wide BVH over the same boxes (NULL: binary only)
+    const float4* place_w;    // the placements in the wide BVH's leaf order
 };
 
 struct DevScene {
@@ -49,6 +51,7 @@ struct DevScene {
     int n_linear, n_region_nodes, pad_r0, pad_r1;
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
+    int inst_accel, pad_i0, pad_i1, pad_i2;   // PTR_ACCEL_* of the instanced batches' TLAS
     // environment
     int env_kind, env_samplable, env_select_live, env_w;
     int env_h, pad0, pad1, pad2;

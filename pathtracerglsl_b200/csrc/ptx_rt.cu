@@ -231,6 +231,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     DevScene Sp = s->dev;
     Sp.accel = p->desc.accel;
+    Sp.inst_accel = p->desc.instance_accel;
     Sp.work = (p->profile_next & PTR_PROFILE_WORK) ? p->work_dev : nullptr;
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
@@ -316,6 +317,7 @@ void launch_wave(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters,
 void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, int n_sm, const AdjParams& adj) {
     DevScene S = s->dev;
     S.accel = p->desc.accel;
+    S.inst_accel = p->desc.instance_accel;
     S.work = nullptr;
     const PathPool& pool = p->pool;
     ProgParams P;
@@ -536,6 +538,23 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
         b.place = p4;
         if ((rc = dev_copy(ctx, s->allocs, (const float4*)tl.nodes.data(), 2 * (size_t)tl.node_count, &p4))) return rc;
         b.tlas = p4;
+        // the compressed wide twin of the TLAS (instanceAccel 'cwbvh', cwbvh.ts:80-372 over
+        // the same instance boxes) with the placements in its leaf order
+        b.tlas_w = nullptr;
+        b.place_w = nullptr;
+        ptx_host::WideBvh wt = ptx_host::build_cwbvh(boxes.data(), N, ptx_host::kCwbvhCPrim);
+        if (!wt.error && wt.node_count > 0) {
+            std::vector<float4> rec_w(2 * (size_t)N);
+            for (int i = 0; i < N; ++i) {
+                rec_w[2 * (size_t)i] = rec[2 * (size_t)wt.order[i]];
+                rec_w[2 * (size_t)i + 1] = rec[2 * (size_t)wt.order[i] + 1];
+            }
+            const uint4* u4 = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, rec_w.data(), rec_w.size(), &p4))) return rc;
+            b.place_w = p4;
+            if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wt.nodes.data(), 5 * (size_t)wt.node_count, &u4))) return rc;
+            b.tlas_w = u4;
+        }
         b.n_inst = N;
         b.proto_shape = bd.prototype_shape;
         b.proto_mesh = bd.prototype_ref;
@@ -957,6 +976,9 @@ int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* d, ptr_program** out) {
     if (d->equiangular && !d->scattering)
         return fail(ctx, PTR_E_INVALID, "program: mediumLightSampling 'equiangular' requires scattering media");
     if (d->color != PTR_COLOR_RGB && d->color != PTR_COLOR_SPECTRAL) return fail(ctx, PTR_E_INVALID, "program: unknown measurement.color");
+    if (d->accel != PTR_ACCEL_BVH && d->accel != PTR_ACCEL_CWBVH) return fail(ctx, PTR_E_INVALID, "program: unknown meshTraversal");
+    if (d->instance_accel != PTR_ACCEL_BVH && d->instance_accel != PTR_ACCEL_CWBVH)
+        return fail(ctx, PTR_E_INVALID, "program: unknown instanceAccel");
     if (d->color == PTR_COLOR_SPECTRAL &&
         (d->wavelengths < PTR_WAVELENGTHS_VISIBLE || d->wavelengths > PTR_WAVELENGTHS_UNIFORM ||
          !(d->lambda_min >= 360.0f && d->lambda_max <= 830.0f && d->lambda_min < d->lambda_max)))
@@ -1023,6 +1045,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         if (rc) return rc;
         scenes[j] = J.scene->dev;
         scenes[j].accel = p->desc.accel;
+        scenes[j].inst_accel = p->desc.instance_accel;
         scenes[j].work = nullptr;
         ProgParams& P = progs[j];
         P.max_bounces = p->desc.max_bounces;
