@@ -420,8 +420,8 @@ def run_batch(args):
     from pathtracerglsl_b200 import autotune
     small = [(w, h, max(1, spp // 16), 0, 7) for (w, h, spp, _f, _s) in frames]
     tuned = autotune.tune(eng, lambda: b.render(small), budget_s=90.0)
-    cfg = dict(cfg, tuning={k: tuned["best"][k] for k in ("capacity", "block", "sort_buckets")},
-               tuning_search=[{k: r[k] for k in ("capacity", "block", "sort_buckets", "ms")} for r in tuned["results"]])
+    cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
+               tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     for _ in range(args.warmup):

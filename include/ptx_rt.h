@@ -380,17 +380,20 @@ int ptr_update_params(ptr_scene* scene, const ptr_material* materials, int n_mat
                       const ptr_region* regions, int n_regions);
 
 /* ---- launch tuning (no counterpart in the reference: WebGL draws one fragment per pixel) ----
- * capacity: paths in flight per wave (0 = the default 2^21); block: threads per block of the
+ * capacity: paths in flight per wave (0 = the default 2^24); block: threads per block of the
  * wavefront kernels (128 or 256; the grid keeps 2048 resident threads per SM);
  * sort_buckets: the occupant-sorted shading queue — 1 = off, 8 = live paths grouped by the
- * material model they shade, 16 = by model and whether the segment starts in a medium.
+ * material model they shade, 16 = by model and whether the segment starts in a medium;
+ * ray_sort: the ray-coherence order of the traversal queues.  Every knob changes the order
+ * of work only: each path's samples are bit-identical under any tuning.
  * Applies to every later ptr_render / ptr_render_batch / ptr_backward on the context.
  * pathtracerglsl_b200.autotune picks and records these per workload. */
 typedef struct ptr_tuning {
     int32_t capacity;
     int32_t block;
     int32_t sort_buckets;
-    int32_t pad;
+    int32_t ray_sort;          /* 1: closest-hit and shadow queues grouped by (direction octant,
+                                  origin octant) before each traversal; 0: off               */
 } ptr_tuning;
 int ptr_set_tuning(ptr_ctx* ctx, const ptr_tuning* t);
 int ptr_get_tuning(ptr_ctx* ctx, ptr_tuning* out);

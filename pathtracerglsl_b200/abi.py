@@ -134,7 +134,7 @@ PROFILE_TIMING, PROFILE_WORK = 1, 2
 
 
 class Tuning(C.Structure):
-    _fields_ = [("capacity", C.c_int32), ("block", C.c_int32), ("sort_buckets", C.c_int32), ("pad", C.c_int32)]
+    _fields_ = [("capacity", C.c_int32), ("block", C.c_int32), ("sort_buckets", C.c_int32), ("ray_sort", C.c_int32)]
 
 
 # Sizes the header documents (checked by the CPU tests).

@@ -1,6 +1,6 @@
-"""Autotuner of the wavefront's launch knobs: path-pool capacity, block size and the
-occupant-sort bucket count (ptr_tuning).  No counterpart in the reference (its WebGL engine
-has no such knobs).
+"""Autotuner of the wavefront's launch knobs: path-pool capacity, block size, the
+occupant-sort bucket count and the ray-coherence queue order (ptr_tuning).  No counterpart
+in the reference (its WebGL engine has no such knobs).
 
 ``tune(engine, render, candidates)`` times ``render()`` under every candidate on the
 engine's context (device time through ptr_sync, best of ``repeats`` after one untimed
@@ -12,8 +12,10 @@ import json
 import os
 import time
 
-DEFAULT_CANDIDATES = [{"capacity": c, "block": b, "sort_buckets": k}
-                      for c, b, k in itertools.product((1 << 20, 1 << 21, 1 << 22), (128, 256), (1, 8, 16))]
+DEFAULT_CANDIDATES = [{"capacity": c, "block": b, "sort_buckets": k, "ray_sort": r}
+                      for c, b, k, r in itertools.product((1 << 23, 1 << 24), (128, 256), (1, 8, 16), (0, 1))]
+KNOBS = ("capacity", "block", "sort_buckets", "ray_sort")
+DEFAULTS = {"capacity": 0, "block": 256, "sort_buckets": 1, "ray_sort": 0}
 
 
 def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
@@ -22,6 +24,7 @@ def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
     results = []
     t_start = time.perf_counter()
     for cand in candidates:
+        cand = dict(DEFAULTS, **cand)
         engine.set_tuning(**cand)
         render()                       # warm-up: pool allocation, graph capture
         engine.sync()
@@ -35,7 +38,7 @@ def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
         if time.perf_counter() - t_start > budget_s:
             break
     best = min(results, key=lambda r: r["ms"])
-    engine.set_tuning(**{k: best[k] for k in ("capacity", "block", "sort_buckets")})
+    engine.set_tuning(**{k: best[k] for k in KNOBS})
     return {"best": best, "results": results}
 
 
@@ -64,4 +67,4 @@ def load(path, workload):
     with open(path) as f:
         data = json.load(f)
     rec = data.get(gpu_name(), {}).get(workload)
-    return {k: rec["best"][k] for k in ("capacity", "block", "sort_buckets")} if rec else None
+    return {k: rec["best"][k] for k in KNOBS if k in rec["best"]} if rec else None

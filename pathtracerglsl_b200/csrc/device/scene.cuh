@@ -52,6 +52,7 @@ struct DevScene {
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
     int inst_accel, pad_i0, pad_i1, pad_i2;   // PTR_ACCEL_* of the instanced batches' TLAS
+    float sort_c[4];          // centre of the bounded geometry (ray-coherence keys)
     // environment
     int env_kind, env_samplable, env_select_live, env_w;
     int env_h, pad0, pad1, pad2;

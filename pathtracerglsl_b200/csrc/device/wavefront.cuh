@@ -70,13 +70,32 @@ struct PathPool {
     // off, k_shade reads the compacted queue as it is)
     int sort_buckets;
     int* q_sorted;
-    unsigned char* sort_key;  // per queue position
-    unsigned* bins;           // [0, 32) counts, [32, 64) running offsets
+    unsigned char* sort_key;  // shading class per path (indexed by path)
+    unsigned* sort_hist;      // counting-sort scratch: [key][chunk] counts, then offsets
     // work tickets of the queue kernels ([0] k_closest, [1] / [2] k_shadow slots 0 / 1,
     // [3] k_shade), each cleared by the kernel that runs before its consumer; NULL: the
     // kernels fall back to a static grid-stride loop
     unsigned* fetch;
+    // ray-coherence order (tuning ray_sort): k_shade keys every spawned ray and every shadow
+    // query by (direction octant, origin octant about the scene centre); counting sorts
+    // rebuild the closest-hit and shadow queues grouped by key for the traversal kernels
+    // (k_shade itself keeps reading the compacted queue q[in])
+    int ray_sort;             // keys and sorted queues are written
+    int ray_in;               // this k_closest reads q_ray (set per launch; 0 for camera rays)
+    unsigned char* rkey;      // key per position of the next live queue
+    unsigned char* skey;      // key per position of the shadow queue
+    int* q_ray;
+    int* shq_s;
 };
+
+constexpr int kRayBuckets = 64;   // ray_key values
+__device__ __forceinline__ unsigned ray_key(const DevScene& S, f3 o, f3 d) {
+    unsigned k = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    k = (k << 3) | (o.x > S.sort_c[0] ? 1u : 0u) | (o.y > S.sort_c[1] ? 2u : 0u) | (o.z > S.sort_c[2] ? 4u : 0u);
+    return k;
+}
+// The queue a k_closest of iteration `in` reads.
+__device__ __forceinline__ const int* closest_queue(const PathPool& pool, int in);
 
 // Warp-uniform cursor over a device-counted queue.  With a ticket counter every warp takes
 // the next 32 entries when it is done with its last ones, so warps whose rays are long do
@@ -467,7 +486,6 @@ __device__ __forceinline__ unsigned shade_key(const DevScene& S, int region, int
 // Nearest hit of every live path (and, for the sorted queue, its shading key).
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S0, PathPool pool, int in, BatchTables bt) {
-    __shared__ unsigned s_hist[kMaxSortBuckets];
     const int buckets = pool.sort_buckets;
     unsigned n = pool.cnt[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -477,11 +495,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         pool.stats[0] += n;
         if (pool.fetch) { pool.fetch[1] = 0u; pool.fetch[2] = 0u; pool.fetch[3] = 0u; }
     }
-    if (buckets > 1) {
-        if (threadIdx.x < kMaxSortBuckets) s_hist[threadIdx.x] = 0u;
-        __syncthreads();
-    }
-    const int* q = pool.q[in];
+    const int* q = closest_queue(pool, in);
     Work w{0u, 0u, 0u, 0u};
     QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
     unsigned k;
@@ -495,47 +509,204 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         HitRec h = scene_closest(S, r, COUNT ? &w : nullptr);
         pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
         pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
-        if (buckets > 1) {
-            unsigned key = shade_key(S, h.region, pool.st[i].y, buckets);
-            pool.sort_key[k] = (unsigned char)key;
-            atomicAdd(&s_hist[key], 1u);
-        }
-    }
-    if (buckets > 1) {
-        __syncthreads();
-        if (threadIdx.x < (unsigned)buckets && s_hist[threadIdx.x]) atomicAdd(&pool.bins[threadIdx.x], s_hist[threadIdx.x]);
+        if (buckets > 1) pool.sort_key[i] = (unsigned char)shade_key(S, h.region, pool.st[i].y, buckets);
     }
     if (COUNT) flush_work(S0, w);
 }
 
-// Exclusive scan of the key counts into running offsets; the counts are cleared for the
-// next iteration.  One warp.
-__global__ void k_bin_scan(PathPool pool) {
-    if (threadIdx.x == 0) {
-        unsigned acc = 0u;
-        for (int b = 0; b < pool.sort_buckets; ++b) {
-            unsigned c = pool.bins[b];
-            pool.bins[kMaxSortBuckets + b] = acc;
-            pool.bins[b] = 0u;
-            acc += c;
+// Counting sort of a device-counted queue by 1-byte keys (< kMaxKeys), in three launches
+// on fixed grids: per-chunk key counts, one scan into per-(key, chunk) offsets, and a
+// scatter that reserves slots from shared-memory offsets.  Each of kSortChunks blocks owns
+// one contiguous chunk of the queue (a multiple of kSortVec entries), so global traffic is
+// the keys twice, the source once and the destination once, and no global atomics are
+// taken.  Each thread reads kSortVec consecutive keys with one 16-byte load (and their
+// sources with four), and lanes with equal keys find each other with seven ballots (a
+// warp multi-split).  The consumers are order-independent; the order within a key only
+// matters for their memory coalescing.
+// GATHER: the keys are indexed by path (keys[src[k]]) rather than by queue position.
+// Queues shorter than kSortMin are not sorted: every consumer reads the unsorted queue
+// then (sorted_queue), deciding from the same device count as the sort kernels.
+constexpr int kSortChunks = 512;
+constexpr int kMaxKeys = 64;
+constexpr int kSortThreads = 256;
+constexpr int kSortVec = 16;
+constexpr int kSortScanThreads = 1024;
+constexpr int kSortEntries = kMaxKeys * kSortChunks;
+constexpr int kSortScanPer = kSortEntries / kSortScanThreads;   // 32: one padded smem row per thread
+static_assert(kSortScanPer == 32, "the scan's padded layout assumes 32 entries per thread");
+constexpr size_t kSortScanSmem = (size_t)(kSortEntries + kSortEntries / 32) * sizeof(unsigned);
+constexpr unsigned kSortMin = 65536u;
+constexpr unsigned kNoKey = (unsigned)kMaxKeys;   // 7-bit key of an idle lane
+__device__ __forceinline__ const int* sorted_queue(const int* sorted, const int* plain, unsigned n) {
+    return n >= kSortMin ? sorted : plain;
+}
+__device__ __forceinline__ void sort_chunk(unsigned n, unsigned& lo, unsigned& hi) {
+    unsigned chunk = (n + kSortChunks - 1) / kSortChunks;
+    chunk = (chunk + kSortVec - 1) & ~(unsigned)(kSortVec - 1);
+    lo = min(n, blockIdx.x * chunk);
+    hi = min(n, lo + chunk);
+}
+// Lanes of the warp whose 7-bit key equals this lane's (all lanes take part).
+__device__ __forceinline__ unsigned warp_peers(unsigned key) {
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const unsigned m = __ballot_sync(0xffffffffu, (key >> b) & 1u);
+        peers &= ((key >> b) & 1u) ? m : ~m;
+    }
+    return peers;
+}
+// Keys (and, if asked or gathering, sources) of entries [base, base + kSortVec) below hi;
+// base is a multiple of kSortVec, so the full-width loads are 16-byte aligned.
+template <bool GATHER>
+__device__ __forceinline__ void sort_load(const int* src, const unsigned char* keys, unsigned base, unsigned hi,
+                                          unsigned (&key)[kSortVec], int (&val)[kSortVec], bool want_val) {
+    if (base + kSortVec <= hi) {
+        if (GATHER || want_val) {
+#pragma unroll
+            for (int v = 0; v < kSortVec / 4; ++v) {
+                const int4 x = *reinterpret_cast<const int4*>(src + base + 4 * v);
+                val[4 * v] = x.x; val[4 * v + 1] = x.y; val[4 * v + 2] = x.z; val[4 * v + 3] = x.w;
+            }
+        }
+        if (GATHER) {
+#pragma unroll
+            for (int j = 0; j < kSortVec; ++j) key[j] = keys[(unsigned)val[j]];
+        } else {
+            const uint4 x = *reinterpret_cast<const uint4*>(keys + base);
+            const unsigned w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int j = 0; j < kSortVec; ++j) key[j] = (w[j >> 2] >> (8 * (j & 3))) & 0xffu;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kSortVec; ++j) {
+            const unsigned k = base + j;
+            const bool v = k < hi;
+            val[j] = (v && (GATHER || want_val)) ? src[k] : 0;
+            key[j] = v ? (unsigned)keys[GATHER ? (unsigned)val[j] : k] : kNoKey;
         }
     }
 }
-
-// Scatter the live queue into key order (warp-aggregated slot reservation per key).
-__global__ void k_bin_scatter(PathPool pool, int in) {
-    const unsigned n = pool.cnt[in];
-    const int* q = pool.q[in];
-    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const unsigned key = pool.sort_key[k];
-        const unsigned mask = __activemask();
-        const unsigned peers = __match_any_sync(mask, key);
-        const int leader = __ffs(peers) - 1;
-        unsigned base = 0u;
-        if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&pool.bins[kMaxSortBuckets + key], (unsigned)__popc(peers));
-        base = __shfl_sync(peers, base, leader);
-        pool.q_sorted[base + __popc(peers & lanemask_lt())] = q[k];
+// Counts of every key (all kMaxKeys rows are written, unused ones zero).
+template <bool GATHER>
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const int* src, const unsigned char* keys, const unsigned* count, unsigned* hist) {
+    const unsigned n = *count;
+    if (n < kSortMin) return;
+    __shared__ unsigned h[kMaxKeys];
+    if (threadIdx.x < kMaxKeys) h[threadIdx.x] = 0u;
+    __syncthreads();
+    unsigned lo, hi;
+    sort_chunk(n, lo, hi);
+    for (unsigned k0 = lo; k0 < hi; k0 += kSortThreads * kSortVec) {   // block-uniform trip count
+        unsigned key[kSortVec];
+        int val[kSortVec];
+        sort_load<GATHER>(src, keys, k0 + threadIdx.x * kSortVec, hi, key, val, false);
+#pragma unroll
+        for (int j = 0; j < kSortVec; ++j) {
+            const unsigned peers = warp_peers(key[j]);
+            if (key[j] != kNoKey && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[key[j]], (unsigned)__popc(peers));
+        }
     }
+    __syncthreads();
+    if (threadIdx.x < kMaxKeys) hist[threadIdx.x * kSortChunks + blockIdx.x] = h[threadIdx.x];
+}
+// Exclusive scan, in place, of the key-major [kMaxKeys][kSortChunks] counts: one block
+// stages them in shared memory with coalesced loads (one padding word per 32 entries, so
+// the per-thread rows below are bank-conflict free), scans, and writes them back.
+__global__ void __launch_bounds__(kSortScanThreads) k_sort_scan(const unsigned* count, unsigned* hist) {
+    if (*count < kSortMin) return;
+    extern __shared__ unsigned sm[];
+    __shared__ unsigned warp_sum[kSortScanThreads / 32];
+    for (int e = threadIdx.x; e < kSortEntries; e += kSortScanThreads) sm[e + (e >> 5)] = hist[e];
+    __syncthreads();
+    const int row = threadIdx.x * (kSortScanPer + 1);   // entries [32 t, 32 t + 32) of the padded layout
+    unsigned s = 0u;
+#pragma unroll
+    for (int j = 0; j < kSortScanPer; ++j) s += sm[row + j];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned w = warp_sum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        warp_sum[lane] = w;
+    }
+    __syncthreads();
+    unsigned run = incl - s + (warp ? warp_sum[warp - 1] : 0u);
+#pragma unroll
+    for (int j = 0; j < kSortScanPer; ++j) {
+        const unsigned c = sm[row + j];
+        sm[row + j] = run;
+        run += c;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kSortEntries; e += kSortScanThreads) hist[e] = sm[e + (e >> 5)];
+}
+// The scatter stages each warp's 32 * kSortVec entries in shared memory (16-byte loads),
+// then places them in rounds of 32 consecutive entries: peers of one round land in one
+// contiguous run, so a sorted queue keeps the compaction's ascending path order within
+// its runs (the pool's SoA reads of its consumers stay coalesced).
+template <bool GATHER>
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const int* src, const unsigned char* keys, const unsigned* count,
+                                                               const unsigned* offsets, int* dst) {
+    const unsigned n = *count;
+    if (n < kSortMin) return;
+    constexpr int kSpan = 32 * kSortVec;   // entries one warp stages per round
+    __shared__ unsigned base[kMaxKeys];
+    __shared__ __align__(16) int s_val[kSortThreads / 32][kSpan];
+    __shared__ __align__(16) unsigned char s_key[kSortThreads / 32][kSpan];
+    if (threadIdx.x < kMaxKeys) base[threadIdx.x] = offsets[threadIdx.x * kSortChunks + blockIdx.x];
+    __syncthreads();
+    unsigned lo, hi;
+    sort_chunk(n, lo, hi);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int* sv = s_val[warp];
+    unsigned char* sk = s_key[warp];
+    for (unsigned k0 = lo; k0 < hi; k0 += kSortThreads * kSortVec) {   // block-uniform trip count
+        const unsigned ws = k0 + warp * kSpan;
+        const unsigned b = ws + lane * kSortVec;
+        if (b + kSortVec <= hi) {
+#pragma unroll
+            for (int v = 0; v < kSortVec / 4; ++v)
+                *reinterpret_cast<int4*>(sv + lane * kSortVec + 4 * v) = *reinterpret_cast<const int4*>(src + b + 4 * v);
+            if (!GATHER) *reinterpret_cast<uint4*>(sk + lane * kSortVec) = *reinterpret_cast<const uint4*>(keys + b);
+        } else {
+            for (int j = 0; j < kSortVec; ++j) {
+                if (b + j < hi) {
+                    sv[lane * kSortVec + j] = src[b + j];
+                    if (!GATHER) sk[lane * kSortVec + j] = keys[b + j];
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll 4
+        for (int j = 0; j < kSortVec; ++j) {
+            const int e = j * 32 + lane;
+            const bool valid = ws + e < hi;
+            const int val = valid ? sv[e] : 0;
+            const unsigned key = valid ? (unsigned)(GATHER ? keys[(unsigned)val] : sk[e]) : kNoKey;
+            const unsigned peers = warp_peers(key);
+            const int leader = __ffs(peers) - 1;
+            unsigned o = 0u;
+            if (valid && lane == leader) o = atomicAdd(&base[key], (unsigned)__popc(peers));
+            o = __shfl_sync(0xffffffffu, o, leader);
+            if (valid) dst[o + __popc(peers & lanemask_lt())] = val;
+        }
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ const int* closest_queue(const PathPool& pool, int in) {
+    return pool.ray_in ? sorted_queue(pool.q_ray, pool.q[in], pool.cnt[in]) : pool.q[in];
 }
 
 // One walk iteration for every live path.
@@ -555,7 +726,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
     extern __shared__ double s_grad[];
     if constexpr (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[in];
-    const int* q = pool.sort_buckets > 1 ? pool.q_sorted : pool.q[in];
+    // the compacted queue, not the ray-coherence one: compaction keeps path indices nearly
+    // ascending, so the pool's SoA reads and writes stay coalesced
+    const int* q = pool.sort_buckets > 1 ? sorted_queue(pool.q_sorted, pool.q[in], n) : pool.q[in];
     int* qout = pool.q[in ^ 1];
     const bool nee = DIRECT != PTR_DIRECT_NONE;
     const bool mis = DIRECT == PTR_DIRECT_MIS;
@@ -565,6 +738,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
     while (cur.next(k)) {
         bool alive = false, shadow = false, shadow2 = false;
         int i = -1;
+        unsigned rk = 0u, sk = 0u;   // ray-coherence keys of the spawned ray / shadow query
         if (k < n) {
             i = q[k];
             const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
@@ -856,6 +1030,13 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                 }
             }
             (void)done;
+            if (pool.ray_sort) {
+                if (alive) rk = ray_key(S, r.o, r.d);
+                if (shadow) {
+                    float4 so = pool.sh_o[i], sd = pool.sh_d[i];
+                    sk = ray_key(S, xyz(so), xyz(sd));
+                }
+            }
             pool.rad[i] = col_st(rad, 0.0f);
             if constexpr (ADJ) {
                 pool.l_rem[i] = f4(lrem, 0.0f);
@@ -877,6 +1058,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
         if (alive) qout[slot] = i;
         int sslot = warp_append(&pool.cnt[2], shadow);
         if (shadow) pool.shq[sslot] = i;
+        if (pool.ray_sort) {
+            if (alive) pool.rkey[slot] = (unsigned char)rk;
+            if (shadow) pool.skey[sslot] = (unsigned char)sk;
+        }
         if (MEDIA) {
             int s2 = warp_append(&pool.cnt[4], shadow2);
             if (shadow2) pool.shq2[s2] = i;
@@ -904,7 +1089,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     if constexpr (ADJ) grad_block_init(s_grad, PTR_GRAD_SLOTS * S0.n_materials);
     const unsigned n = pool.cnt[slot ? 4 : 2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
-    const int* shq = slot ? pool.shq2 : pool.shq;
+    const int* shq = slot ? pool.shq2 : (pool.ray_sort ? sorted_queue(pool.shq_s, pool.shq, n) : pool.shq);
     const float4* a_o = slot ? pool.sh2_o : pool.sh_o;
     const float4* a_d = slot ? pool.sh2_d : pool.sh_d;
     const float4* a_lp = slot ? pool.sh2_lp : pool.sh_lp;

@@ -31,7 +31,7 @@ struct ptr_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     ptr_program* batch = nullptr;     // path pool + tables of batched renders
-    ptr_tuning tune{1 << 21, 256, 1, 0};   // pool capacity, block size, sort buckets
+    ptr_tuning tune{1 << 24, 256, 1, 0};   // pool capacity, block size, sort buckets, ray sort
 };
 
 struct ptr_scene {
@@ -176,15 +176,16 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
         (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
         (rc = get(64, (void**)&q.wave)) || (rc = get(c * 4, (void**)&q.q_sorted)) ||
-        (rc = get(c, (void**)&q.sort_key)) || (rc = get(2 * kMaxSortBuckets * sizeof(unsigned), (void**)&q.bins)) ||
-        (rc = get(4 * sizeof(unsigned), (void**)&q.fetch))) {
+        (rc = get(c, (void**)&q.sort_key)) || (rc = get((size_t)kMaxKeys * kSortChunks * sizeof(unsigned), (void**)&q.sort_hist)) ||
+        (rc = get(4 * sizeof(unsigned), (void**)&q.fetch)) || (rc = get(c, (void**)&q.rkey)) ||
+        (rc = get(c, (void**)&q.skey)) || (rc = get(c * 4, (void**)&q.q_ray)) ||
+        (rc = get(c * 4, (void**)&q.shq_s))) {
         free_pool(p);
         return rc;
     }
-    if (cudaMemset(q.bins, 0, 2 * kMaxSortBuckets * sizeof(unsigned)) != cudaSuccess ||
-        cudaMemset(q.fetch, 0, 4 * sizeof(unsigned)) != cudaSuccess) {
+    if (cudaMemset(q.fetch, 0, 4 * sizeof(unsigned)) != cudaSuccess) {
         free_pool(p);
-        return fail(ctx, PTR_E_CUDA, "path pool: clearing the sort bins failed");
+        return fail(ctx, PTR_E_CUDA, "path pool: clearing the work tickets failed");
     }
     // the second shadow slot only for programs with the per-segment equiangular site
     if (slot2 && ((rc = get(c * 16, (void**)&q.sh2_o)) || (rc = get(c * 16, (void**)&q.sh2_d)) ||
@@ -219,7 +220,29 @@ int wave_iterations(const ptr_program* p, const ptr_scene* s) {
 
 // The launch tuning of a program's context; a program without a context (the
 // allocation-free entry point's) launches with the defaults.
-const ptr_tuning kDefaultTuning{1 << 21, 256, 1, 0};
+const ptr_tuning kDefaultTuning{1 << 24, 256, 1, 0};
+// Counting sort of a device-counted queue (src[0, *count)) by its keys into dst (a no-op on
+// the device below kSortMin entries).
+template <bool GATHER>
+void launch_sort(const PathPool& pool, const int* src, const unsigned char* keys, const unsigned* count, int* dst,
+                 cudaStream_t st, bool dry) {
+    if (dry) return;
+    k_sort_hist<GATHER><<<kSortChunks, kSortThreads, 0, st>>>(src, keys, count, pool.sort_hist);
+    k_sort_scan<<<1, kSortScanThreads, kSortScanSmem, st>>>(count, pool.sort_hist);
+    k_sort_scatter<GATHER><<<kSortChunks, kSortThreads, 0, st>>>(src, keys, count, pool.sort_hist, dst);
+}
+// After k_closest: the compacted live queue grouped by shading class (occupant-sorted
+// shading), keyed by path index, so each class keeps the compaction's ascending order.
+void launch_shade_sort(const PathPool& pool, int in, cudaStream_t st, bool dry) {
+    if (pool.sort_buckets <= 1) return;
+    launch_sort<true>(pool, pool.q[in], pool.sort_key, pool.cnt + in, pool.q_sorted, st, dry);
+}
+// After k_shade: the next closest-hit queue and the shadow queue in ray-coherence order.
+void launch_ray_sort(const PathPool& pool, int in, bool shadows, cudaStream_t st, bool dry) {
+    if (!pool.ray_sort) return;
+    launch_sort<false>(pool, pool.q[in ^ 1], pool.rkey, pool.cnt + (in ^ 1), pool.q_ray, st, dry);
+    if (shadows) launch_sort<false>(pool, pool.shq, pool.skey, pool.cnt + 2, pool.shq_s, st, dry);
+}
 const ptr_tuning& tuning_of(const ptr_program* p) { return p->ctx ? p->ctx->tune : kDefaultTuning; }
 
 // Event pairs around each launch of an instrumented render (kernel class, start, end).
@@ -256,30 +279,31 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     const Launcher L{block, n_sm, st, dry};
     PathPool pool = p->pool;
     pool.sort_buckets = tuning_of(p).sort_buckets;
+    pool.ray_sort = tuning_of(p).ray_sort;
     ProfRec* r = mark(0);
     const BatchTables nob{};
     L(k_generate<false, SPECTRAL>, 0, S, pool, p->fp_dev, AdjParams{});
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
+        PathPool pi = pool;   // camera rays keep their generation order; later queues are key-sorted
+        pi.ray_in = pool.ray_sort && it > 0;
         r = mark(1);
-        if (S.work) L(k_closest<true, false>, 0, S, pool, in, nob);
-        else L(k_closest<false, false>, 0, S, pool, in, nob);
-        if (pool.sort_buckets > 1) {   // occupant-sorted shading queue (counted with the traversal)
-            if (!dry) k_bin_scan<<<1, 32, 0, st>>>(pool);
-            L(k_bin_scatter, 0, pool, in);
-        }
+        if (S.work) L(k_closest<true, false>, 0, S, pi, in, nob);
+        else L(k_closest<false, false>, 0, S, pi, in, nob);
+        launch_shade_sort(pi, in, st, dry);   // occupant-sorted shading queue (counted with the traversal)
         done(r);
         const bool media = s->has_media != 0;
         r = mark(2);
         switch (P.direct * 2 + (media ? 1 : 0)) {
-            case 0: L(k_shade<Col, PTR_DIRECT_NONE, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
-            case 1: L(k_shade<Col, PTR_DIRECT_NONE, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
-            case 2: L(k_shade<Col, PTR_DIRECT_NEE, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
-            case 3: L(k_shade<Col, PTR_DIRECT_NEE, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
-            case 4: L(k_shade<Col, PTR_DIRECT_MIS, false, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
-            default: L(k_shade<Col, PTR_DIRECT_MIS, true, false>, 0, S, pool, P, in, nob, AdjParams{}); break;
+            case 0: L(k_shade<Col, PTR_DIRECT_NONE, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
+            case 1: L(k_shade<Col, PTR_DIRECT_NONE, true, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
+            case 2: L(k_shade<Col, PTR_DIRECT_NEE, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
+            case 3: L(k_shade<Col, PTR_DIRECT_NEE, true, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
+            case 4: L(k_shade<Col, PTR_DIRECT_MIS, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
+            default: L(k_shade<Col, PTR_DIRECT_MIS, true, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
         }
+        launch_ray_sort(pool, in, P.direct != PTR_DIRECT_NONE, st, dry);
         done(r);
         if (P.direct != PTR_DIRECT_NONE) {
             r = mark(3);
@@ -362,6 +386,7 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
     const Launcher L{block, n_sm, st, dry};
     PathPool pool = pool_in;
     pool.sort_buckets = tune.sort_buckets;
+    pool.ray_sort = tune.ray_sort;
     ProgParams P0{};
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
@@ -378,22 +403,22 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
     done(r);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
+        PathPool pi = pool;
+        pi.ray_in = pool.ray_sort && it > 0;
         r = mark(1);
-        L(k_closest<false, true>, 0, S0, pool, in, bt);
-        if (pool.sort_buckets > 1) {
-            if (!dry) k_bin_scan<<<1, 32, 0, st>>>(pool);
-            L(k_bin_scatter, 0, pool, in);
-        }
+        L(k_closest<false, true>, 0, S0, pi, in, bt);
+        launch_shade_sort(pi, in, st, dry);
         done(r);
         r = mark(2);
         switch (direct * 2 + (media ? 1 : 0)) {
-            case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
-            case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
-            case 2: L(k_shade<f3, PTR_DIRECT_NEE, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
-            case 3: L(k_shade<f3, PTR_DIRECT_NEE, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
-            case 4: L(k_shade<f3, PTR_DIRECT_MIS, false, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
-            default: L(k_shade<f3, PTR_DIRECT_MIS, true, true>, 0, S0, pool, P0, in, bt, AdjParams{}); break;
+            case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
+            case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
+            case 2: L(k_shade<f3, PTR_DIRECT_NEE, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
+            case 3: L(k_shade<f3, PTR_DIRECT_NEE, true, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
+            case 4: L(k_shade<f3, PTR_DIRECT_MIS, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
+            default: L(k_shade<f3, PTR_DIRECT_MIS, true, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
         }
+        launch_ray_sort(pool, in, direct != PTR_DIRECT_NONE, st, dry);
         done(r);
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
@@ -422,6 +447,12 @@ int device_sms(int dev) {
 // (leaf 2) over the instances' world boxes with the placements in leaf order.
 int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     DevScene& S = s->dev;
+    // the bounded geometry's box: its centre splits ray origins into octants for the
+    // ray-coherence queue keys
+    double world_lo[3] = {1e300, 1e300, 1e300}, world_hi[3] = {-1e300, -1e300, -1e300};
+    auto grow = [&](const double* lo, const double* hi) {
+        for (int a = 0; a < 3; ++a) { world_lo[a] = std::min(world_lo[a], lo[a]); world_hi[a] = std::max(world_hi[a], hi[a]); }
+    };
     std::vector<DevMesh> meshes(d->n_meshes > 0 ? d->n_meshes : 0);
     std::vector<std::vector<double>> root_box(meshes.size());
     for (int mi = 0; mi < d->n_meshes; ++mi) {
@@ -479,6 +510,7 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
         m.n_nodes = bin.node_count;
         m.n_cw_nodes = wide.node_count;
         root_box[mi] = {bin.nodes[0], bin.nodes[1], bin.nodes[2], bin.nodes[4], bin.nodes[5], bin.nodes[6]};
+        grow(root_box[mi].data(), root_box[mi].data() + 3);
         s->max_stack_depth = std::max(s->max_stack_depth, bin.max_depth);
     }
     std::vector<DevBatch> batches(d->n_batches > 0 ? d->n_batches : 0);
@@ -524,6 +556,7 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
                 rec[2 * (size_t)i + 1] = make_float4(pl[4], pl[5], pl[6], pl[7]);
             }
             for (int a = 0; a < 3; ++a) { boxes[6 * (size_t)i + a] = mn[a]; boxes[6 * (size_t)i + 3 + a] = mx[a]; }
+            grow(mn, mx);
         }
         ptx_host::BinaryBvh tl = ptx_host::build_bvh(boxes.data(), N, ptx_host::kBvhLeafSize, false);
         std::vector<float4> rec_leaf(2 * (size_t)N);
@@ -573,6 +606,28 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     const unsigned* ef = nullptr;
     if ((rc = dev_copy(ctx, s->allocs, &zero, 1, &ef))) return rc;
     S.err_flags = (unsigned*)ef;
+    for (int i = 0; i < d->n_regions; ++i) {
+        const ptr_region& g = d->regions[i];
+        const float* q = g.p;
+        double mn[3], mx[3];
+        if (g.shape == PTR_SHAPE_SPHERE) {
+            for (int a = 0; a < 3; ++a) { mn[a] = (double)q[a] - q[3]; mx[a] = (double)q[a] + q[3]; }
+        } else if (g.shape == PTR_SHAPE_BOX) {
+            for (int a = 0; a < 3; ++a) { mn[a] = (double)q[a] - q[3 + a]; mx[a] = (double)q[a] + q[3 + a]; }
+        } else if (g.shape == PTR_SHAPE_QUAD) {
+            for (int a = 0; a < 3; ++a) {
+                double c0 = q[a], c1 = c0 + q[3 + a], c2 = c0 + q[6 + a], c3 = c0 + q[3 + a] + q[6 + a];
+                mn[a] = std::min(std::min(c0, c1), std::min(c2, c3));
+                mx[a] = std::max(std::max(c0, c1), std::max(c2, c3));
+            }
+        } else {
+            continue;
+        }
+        grow(mn, mx);
+    }
+    for (int a = 0; a < 3; ++a)
+        S.sort_c[a] = world_lo[a] <= world_hi[a] ? (float)(0.5 * (world_lo[a] + world_hi[a])) : 0.0f;
+    S.sort_c[3] = 0.0f;
     return PTR_OK;
 }
 
@@ -717,7 +772,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     }
     const long long total = (long long)npix * f->spp;
     // capacity: whole sample passes when a pass fits the pool, else a chunk of pixels
-    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 24);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::atoll(env);
     if (cap_max < 1024) cap_max = 1024;
     long long cap;
@@ -829,6 +884,12 @@ int ptr_create(int device_ordinal, ptr_ctx** out) {
     ptr_ctx* c = new ptr_ctx();
     c->device = device_ordinal;
     if (cudaSetDevice(device_ordinal) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PTR_E_CUDA;
+    }
+    // the counting sort's scan stages its whole table in shared memory (above the 48 KB default)
+    if (cudaFuncSetAttribute((const void*)k_sort_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortScanSmem) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
         delete c;
         return PTR_E_CUDA;
     }
@@ -1079,7 +1140,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         ctx->batch->ctx = ctx;
     }
     ptr_program* bp = ctx->batch;
-    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 24);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
     long long cap = std::min(total, cap_max);
     if (bp->capacity < cap || (equi && !bp->pool.sh2_o)) {
@@ -1255,7 +1316,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     cudaStream_t st = ctx->stream;
     const size_t npix = (size_t)f->width * f->height;
     const long long total = (long long)npix * f->spp;
-    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 21);
+    long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 24);
     if (const char* env = std::getenv("PTR_CAPACITY")) cap_max = std::max(1024ll, (long long)std::atoll(env));
     long long cap = (long long)npix <= cap_max ? (cap_max / (long long)npix) * (long long)npix : cap_max;
     if (cap > total) cap = total;
@@ -1354,8 +1415,8 @@ int ptr_set_tuning(ptr_ctx* ctx, const ptr_tuning* t) {
     if (t->block != 128 && t->block != 256) return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: block must be 128 or 256");
     if (t->sort_buckets < 1 || t->sort_buckets > kMaxSortBuckets)
         return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: sort_buckets must be in [1, 32]");
+    if (t->ray_sort != 0 && t->ray_sort != 1) return fail(ctx, PTR_E_INVALID, "ptr_set_tuning: ray_sort must be 0 or 1");
     ctx->tune = *t;
-    ctx->tune.pad = 0;
     return PTR_OK;
 }
 

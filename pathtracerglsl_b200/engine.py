@@ -184,16 +184,17 @@ class CudaEngine:
         self.reset()
 
     # -- launch tuning ---------------------------------------------------------------------
-    def set_tuning(self, capacity=0, block=256, sort_buckets=1):
-        """Pool capacity (0 = default), block size (128/256) and occupant-sort buckets
-        (1 = off) of every later render on this context (ptr_set_tuning)."""
-        t = abi.Tuning(int(capacity), int(block), int(sort_buckets), 0)
+    def set_tuning(self, capacity=0, block=256, sort_buckets=1, ray_sort=0):
+        """Pool capacity (0 = default), block size (128/256), occupant-sort buckets (1 = off)
+        and the ray-coherence queue order (0/1) of every later render on this context
+        (ptr_set_tuning)."""
+        t = abi.Tuning(int(capacity), int(block), int(sort_buckets), int(ray_sort))
         self._check(self.lib.ptr_set_tuning(self.ctx, C.byref(t)))
 
     def get_tuning(self):
         t = abi.Tuning()
         self._check(self.lib.ptr_get_tuning(self.ctx, C.byref(t)))
-        return {"capacity": t.capacity, "block": t.block, "sort_buckets": t.sort_buckets}
+        return {"capacity": t.capacity, "block": t.block, "sort_buckets": t.sort_buckets, "ray_sort": t.ray_sort}
 
     KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film")
 

@@ -1,8 +1,8 @@
 """Launch tuning (ptr_set_tuning) and the autotuner: the knobs change scheduling only.
 
 Every path's walk depends on its own counter-based random numbers only, so the occupant-
-sorted shading queue, the block size and the pool capacity (waves of any size) must leave
-every sample bit-identical.  No counterpart in the reference.
+sorted shading queue, the ray-coherence queue order, the block size and the pool capacity
+(waves of any size) must leave every sample bit-identical.  No counterpart in the reference.
 """
 import numpy as np
 import pytest
@@ -33,14 +33,15 @@ def test_sorting_block_and_capacity_leave_samples_identical(engine, case):
     engine.params = dict(cam)
     out = []
     for t in ({"capacity": 0, "block": 256, "sort_buckets": 1}, {"capacity": 0, "block": 256, "sort_buckets": 16},
-              {"capacity": 4096, "block": 128, "sort_buckets": 8}):
+              {"capacity": 4096, "block": 128, "sort_buckets": 8}, {"capacity": 0, "block": 256, "ray_sort": 1},
+              {"capacity": 4096, "block": 128, "sort_buckets": 16, "ray_sort": 1}):
         engine.set_tuning(**t)
         engine.pin_reset_salt(9)
         engine.reset()
-        out.append(engine.render_samples(40, 30, 4))
+        out.append(engine.render_samples(160, 120, 8))   # 153,600 paths: above the sorts' 65,536-entry floor
     engine.set_tuning()
-    np.testing.assert_array_equal(out[1], out[0])
-    np.testing.assert_array_equal(out[2], out[0])
+    for o in out[1:]:
+        np.testing.assert_array_equal(o, out[0])
 
 
 def test_tuning_validation_and_autotune(engine):
@@ -48,6 +49,8 @@ def test_tuning_validation_and_autotune(engine):
         engine.set_tuning(block=192)
     with pytest.raises(EngineError):
         engine.set_tuning(sort_buckets=0)
+    with pytest.raises(EngineError):
+        engine.set_tuning(ray_sort=2)
     sc, st = scenes.cornell()
     r, pk = Compiler().compile(sc, st)
     engine.register_scene(pk)
