@@ -414,13 +414,16 @@ int ptr_read_export_device(ptr_program* prog, const char* name, float* dst_devic
 int ptr_get_counters(ptr_program* prog, ptr_counters* out);
 
 /* Instrument the next ptr_render (mode bits): PTR_PROFILE_TIMING runs it without the
- * CUDA graph with a pair of CUDA events around every kernel launch on the context's
- * stream — ptr_get_profile then returns, per kernel class k (0 generate, 1 closest-hit,
- * 2 shade, 3 shadow, 4 film), the summed device time ms_out[k] and the number of
- * launches launches_out[k]; PTR_PROFILE_WORK runs the traversal kernels' counting
- * variants, which tally nodes, triangles, TLAS nodes and instances into ptr_counters. */
+ * CUDA graph with a pair of CUDA events around each kernel class's launches of every
+ * walk iteration on the context's stream — ptr_get_profile then returns, per kernel
+ * class k (0 generate, 1 closest-hit, 2 shade, 3 shadow, 4 film, 5 queue sorts), the
+ * summed device time ms_out[k] and the number of kernel launches launches_out[k]
+ * (n <= PTR_PROFILE_CLASSES entries); PTR_PROFILE_WORK runs the traversal kernels'
+ * counting variants, which tally nodes, triangles, TLAS nodes and instances into
+ * ptr_counters. */
 #define PTR_PROFILE_TIMING 1
 #define PTR_PROFILE_WORK 2
+#define PTR_PROFILE_CLASSES 6
 int ptr_profile_next(ptr_program* prog, int enable);
 int ptr_get_profile(ptr_program* prog, float* ms_out, int* launches_out, int n);
 

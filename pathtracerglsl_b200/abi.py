@@ -131,6 +131,7 @@ class Counters(C.Structure):
 
 
 PROFILE_TIMING, PROFILE_WORK = 1, 2
+PROFILE_CLASSES = 6
 
 
 class Tuning(C.Structure):

@@ -117,93 +117,115 @@ __device__ __forceinline__ float byte_as_float(unsigned word, unsigned k) {
 }
 __device__ __forceinline__ float clamp_dir(float d) { return fabsf(d) < 1e-20f ? (d < 0.0f ? -1e-20f : 1e-20f) : d; }
 
+// Per-ray set-up of a wide walk: the direction with zero components clamped (slab
+// reciprocals stay finite), its reciprocal and the inverted octant that orders children.
+struct CwRay { f3 inv; unsigned octinv; };
+__device__ __forceinline__ CwRay cw_ray(f3 rd) {
+    f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
+    CwRay c;
+    c.octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
+    c.inv = f3(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
+    return c;
+}
+// One CWBVH node against the ray: the hit internal children as an octant-ordered bit mask
+// (hits, with the node's child base and internal-child mask for the group) and the hit
+// leaf triangles as bits above the node's triangle base (leaf_bits, leaf_base).
+struct CwNodeHits { unsigned hits, leaf_bits, child_base, imask, leaf_base; };
+__device__ __forceinline__ CwNodeHits cw_node(const uint4* nd, f3 ro, const CwRay& cr, float tmax) {
+    uint4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
+    f3 p(__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z));
+    f3 dq = f3(__uint_as_float((n0.w & 0xFFu) << 23), __uint_as_float(((n0.w >> 8) & 0xFFu) << 23),
+               __uint_as_float(((n0.w >> 16) & 0xFFu) << 23)) * cr.inv;
+    f3 oq = (p - ro) * cr.inv;
+#if PTR_CW_NEARFAR
+    // the ray's octant picks which quantized bound of each axis is the near plane (the slab
+    // values are the same as min / max of the two, without computing both orders)
+    const bool nx = (cr.octinv & 1u) == 0u, ny = (cr.octinv & 2u) == 0u, nz = (cr.octinv & 4u) == 0u;
+#endif
+    CwNodeHits o;
+    o.hits = 0u;
+    o.leaf_bits = 0u;
+    o.child_base = n1.x;
+    o.leaf_base = n1.y;
+    o.imask = (n0.w >> 24) & 0xFFu;
+#pragma unroll
+    for (unsigned sl = 0u; sl < 8u; sl++) {
+        const unsigned sh = 8u * (sl & 3u);
+        unsigned m = ((sl < 4u ? n1.z : n1.w) >> sh) & 0xFFu;
+        if (m == 0u) continue;
+        const unsigned kb = sl & 3u;
+        const unsigned wlx = sl < 4u ? n2.x : n2.y, wly = sl < 4u ? n2.z : n2.w, wlz = sl < 4u ? n3.x : n3.y;
+        const unsigned whx = sl < 4u ? n3.z : n3.w, why = sl < 4u ? n4.x : n4.y, whz = sl < 4u ? n4.z : n4.w;
+#if PTR_CW_NEARFAR
+        float nearx = __fmaf_rn(byte_as_float(nx ? whx : wlx, kb), dq.x, oq.x);
+        float fary = __fmaf_rn(byte_as_float(ny ? wly : why, kb), dq.y, oq.y);
+        float neary = __fmaf_rn(byte_as_float(ny ? why : wly, kb), dq.y, oq.y);
+        float farx = __fmaf_rn(byte_as_float(nx ? wlx : whx, kb), dq.x, oq.x);
+        float nearz = __fmaf_rn(byte_as_float(nz ? whz : wlz, kb), dq.z, oq.z);
+        float farz = __fmaf_rn(byte_as_float(nz ? wlz : whz, kb), dq.z, oq.z);
+        float tn = gmax(gmax(nearx, neary), gmax(nearz, 0.0f));
+        float tf = gmin(gmin(farx, fary), gmin(farz, tmax)) * kBvhTfarPad;
+#else
+        float qlx = byte_as_float(wlx, kb), qly = byte_as_float(wly, kb), qlz = byte_as_float(wlz, kb);
+        float qhx = byte_as_float(whx, kb), qhy = byte_as_float(why, kb), qhz = byte_as_float(whz, kb);
+        float lox = __fmaf_rn(qlx, dq.x, oq.x), hix = __fmaf_rn(qhx, dq.x, oq.x);
+        float loy = __fmaf_rn(qly, dq.y, oq.y), hiy = __fmaf_rn(qhy, dq.y, oq.y);
+        float loz = __fmaf_rn(qlz, dq.z, oq.z), hiz = __fmaf_rn(qhz, dq.z, oq.z);
+        float tn = gmax(gmax(gmin(lox, hix), gmin(loy, hiy)), gmax(gmin(loz, hiz), 0.0f));
+        float tf = gmin(gmin(gmax(lox, hix), gmax(loy, hiy)), gmin(gmax(loz, hiz), tmax)) * kBvhTfarPad;
+#endif
+        if (tf < tn) continue;
+        if ((m & 0xE0u) == 0x20u && (m & 0x1Fu) >= 24u) o.hits |= 1u << ((((m & 0x1Fu) - 24u) ^ cr.octinv) & 7u);
+        else o.leaf_bits |= (m >> 5) << (m & 0x1Fu);
+    }
+    return o;
+}
+// The next child of a node group: pops the highest hit bit and maps it to the child index.
+__device__ __forceinline__ unsigned cw_next_child(unsigned& g_hits, unsigned g_base, unsigned g_imask, unsigned octinv) {
+    int bit = find_msb24(g_hits);
+    g_hits &= ~(1u << (unsigned)bit);
+    unsigned slot = ((unsigned)bit ^ octinv) & 7u;
+    return g_base + __popc(g_imask & ((1u << slot) - 1u));
+}
+
 // Leaf(item) for one leaf item index (wide-order); returns true to stop.
 template <class Leaf>
 __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes, f3 ro, f3 rd, const float& tmax, Leaf leaf,
                                           unsigned* visits = nullptr) {
-    f3 rdc(clamp_dir(rd.x), clamp_dir(rd.y), clamp_dir(rd.z));
-    unsigned octinv = 7u - ((rdc.x < 0.0f ? 1u : 0u) | (rdc.y < 0.0f ? 2u : 0u) | (rdc.z < 0.0f ? 4u : 0u));
-    f3 inv(1.0f / rdc.x, 1.0f / rdc.y, 1.0f / rdc.z);
+    const CwRay cr = cw_ray(rd);
     // node-group stack in thread-local memory (a wide TLAS walk nests a BLAS walk inside
     // its leaves, each with its own stack)
-    constexpr int kDepth = kCwStack;
     uint2 stack[kCwStack];
-#define CW_STACK(i) stack[i]
     int ptr = -1;
-    unsigned g_base = 0u, g_hits = 1u << (octinv & 7u), g_imask = 1u;
-#if PTR_CW_NEARFAR
-    // the ray's octant picks which quantized bound of each axis is the near plane (the slab
-    // values are the same as min / max of the two, without computing both orders)
-    const bool nx = rdc.x < 0.0f, ny = rdc.y < 0.0f, nz = rdc.z < 0.0f;
-#endif
+    unsigned g_base = 0u, g_hits = 1u << (cr.octinv & 7u), g_imask = 1u;
     for (int guard = 0; guard < 65536; guard++) {
         if (g_hits == 0u) {
             if (ptr < 0) return false;
-            const uint2 top = CW_STACK(ptr);
+            const uint2 top = stack[ptr];
             g_base = top.x;
             g_hits = top.y & 0xFFu;
             g_imask = top.y >> 8;
             ptr--;
             continue;
         }
-        int bit = find_msb24(g_hits);
-        g_hits &= ~(1u << (unsigned)bit);
-        unsigned slot = ((unsigned)bit ^ octinv) & 7u;
-        unsigned child = g_base + __popc(g_imask & ((1u << slot) - 1u));
+        const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
         if (g_hits != 0u) {
-            if (ptr + 1 < kDepth) { ptr++; CW_STACK(ptr) = make_uint2(g_base, g_hits | (g_imask << 8)); }
+            if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
             else flag_error(S, kErrCwStack);
         }
-        const uint4* nd = nodes + 5 * (size_t)child;
         if (visits) (*visits)++;
-        uint4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3), n4 = __ldg(nd + 4);
-        f3 p(__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z));
-        f3 dq = f3(__uint_as_float((n0.w & 0xFFu) << 23), __uint_as_float(((n0.w >> 8) & 0xFFu) << 23),
-                   __uint_as_float(((n0.w >> 16) & 0xFFu) << 23)) * inv;
-        unsigned imask = (n0.w >> 24) & 0xFFu;
-        f3 oq = (p - ro) * inv;
-        unsigned hits = 0u, leaf_bits = 0u;
-#pragma unroll
-        for (unsigned sl = 0u; sl < 8u; sl++) {
-            const unsigned sh = 8u * (sl & 3u);
-            unsigned m = ((sl < 4u ? n1.z : n1.w) >> sh) & 0xFFu;
-            if (m == 0u) continue;
-            const unsigned kb = sl & 3u;
-            const unsigned wlx = sl < 4u ? n2.x : n2.y, wly = sl < 4u ? n2.z : n2.w, wlz = sl < 4u ? n3.x : n3.y;
-            const unsigned whx = sl < 4u ? n3.z : n3.w, why = sl < 4u ? n4.x : n4.y, whz = sl < 4u ? n4.z : n4.w;
-#if PTR_CW_NEARFAR
-            float nearx = __fmaf_rn(byte_as_float(nx ? whx : wlx, kb), dq.x, oq.x);
-            float fary = __fmaf_rn(byte_as_float(ny ? wly : why, kb), dq.y, oq.y);
-            float neary = __fmaf_rn(byte_as_float(ny ? why : wly, kb), dq.y, oq.y);
-            float farx = __fmaf_rn(byte_as_float(nx ? wlx : whx, kb), dq.x, oq.x);
-            float nearz = __fmaf_rn(byte_as_float(nz ? whz : wlz, kb), dq.z, oq.z);
-            float farz = __fmaf_rn(byte_as_float(nz ? wlz : whz, kb), dq.z, oq.z);
-            float tn = gmax(gmax(nearx, neary), gmax(nearz, 0.0f));
-            float tf = gmin(gmin(farx, fary), gmin(farz, tmax)) * kBvhTfarPad;
-#else
-            float qlx = byte_as_float(wlx, kb), qly = byte_as_float(wly, kb), qlz = byte_as_float(wlz, kb);
-            float qhx = byte_as_float(whx, kb), qhy = byte_as_float(why, kb), qhz = byte_as_float(whz, kb);
-            float lox = __fmaf_rn(qlx, dq.x, oq.x), hix = __fmaf_rn(qhx, dq.x, oq.x);
-            float loy = __fmaf_rn(qly, dq.y, oq.y), hiy = __fmaf_rn(qhy, dq.y, oq.y);
-            float loz = __fmaf_rn(qlz, dq.z, oq.z), hiz = __fmaf_rn(qhz, dq.z, oq.z);
-            float tn = gmax(gmax(gmin(lox, hix), gmin(loy, hiy)), gmax(gmin(loz, hiz), 0.0f));
-            float tf = gmin(gmin(gmax(lox, hix), gmax(loy, hiy)), gmin(gmax(loz, hiz), tmax)) * kBvhTfarPad;
-#endif
-            if (tf < tn) continue;
-            if ((m & 0xE0u) == 0x20u && (m & 0x1Fu) >= 24u) hits |= 1u << ((((m & 0x1Fu) - 24u) ^ octinv) & 7u);
-            else leaf_bits |= (m >> 5) << (m & 0x1Fu);
-        }
+        const CwNodeHits nh = cw_node(nodes + 5 * (size_t)child, ro, cr, tmax);
+        unsigned leaf_bits = nh.leaf_bits;
         while (leaf_bits != 0u) {
             int lb = find_msb24(leaf_bits);
             leaf_bits &= ~(1u << (unsigned)lb);
-            if (leaf((int)n1.y + lb)) return true;
+            if (leaf((int)nh.leaf_base + lb)) return true;
         }
-        if (hits != 0u) { g_base = n1.x; g_hits = hits; g_imask = imask; }
+        if (nh.hits != 0u) { g_base = nh.child_base; g_hits = nh.hits; g_imask = nh.imask; }
         else g_hits = 0u;
     }
     flag_error(S, kErrCwGuard);
     return false;
-#undef CW_STACK
 }
 
 // ---- one mesh BLAS in a given frame (ro/rd already in the mesh's local frame) --------------
@@ -259,6 +281,138 @@ __device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3
     }, w ? &w->nodes : nullptr);
 }
 
+// ---- instanced meshes: binary TLAS over CWBVH BLAS as one flat loop -------------------------
+// The nested form (accel_closest / accel_any) runs each instance's BLAS walk to the end
+// inside the TLAS leaf that reached it, so in a warp every lane whose TLAS step did not
+// enter an instance waits for the other lanes' whole BLAS walks.  Here one loop advances
+// each lane by one step — a TLAS node, the next instance of the current TLAS leaf, or a
+// BLAS node with its leaf triangles — so lanes at different levels proceed together.  Per
+// lane the sequence of node visits, leaf tests and tmax updates is that of the nested
+// walks, so hits (and the work tallies) are identical.  ANY: stop at the first triangle hit.
+template <bool ANY>
+__device__ __forceinline__ bool inst_mesh_flat(const DevScene& S, const DevBatch& b, int region, const Ray& r, HitRec& h,
+                                               float max_dist, Work* w) {
+    const DevMesh& m = S.meshes[b.proto_mesh];
+    const float4* tlas = b.tlas;
+    const float4* place = b.place;
+    const uint4* nodes = m.cwbvh;
+    const float4* tri = m.tri_w;
+    float t_near = ANY ? max_dist : h.t;   // TLAS culling distance
+    const f3 winv(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+    int tstack[kBvhStack];
+    int tptr = 0;
+    tstack[0] = 0;
+    int li = 0, lend = 0;                  // instances of the current TLAS leaf not yet entered
+    // the BLAS walk of the entered instance
+    f3 ro(0.f, 0.f, 0.f), rd(0.f, 0.f, 0.f);
+    CwRay cr{f3(0.f, 0.f, 0.f), 0u};
+    uint2 stack[kCwStack];
+    int ptr = -1;
+    unsigned g_base = 0u, g_hits = 0u, g_imask = 0u;
+    float t = 0.0f;
+    int prim = -1, inst = -1;
+    bool found = false;
+    int phase = 0;                         // 0 TLAS node, 1 next instance, 2 BLAS step
+    for (int guard = 0; guard < (1 << 22); ++guard) {
+        if (phase == 0) {
+            if (tptr < 0) return false;
+            const int ni = tstack[tptr--];
+            if (w) w->tlas++;
+            const float4 n0 = __ldg(tlas + 2 * ni), n1 = __ldg(tlas + 2 * ni + 1);
+            if (!aabb_hit(n0, n1, r.o, winv, t_near)) continue;
+            if (n0.w >= 0.0f) {
+                li = (int)n1.w;
+                lend = li + (int)n0.w;
+                phase = 1;
+            } else {
+                const int axis = (int)(-n0.w - 1.0f);
+                const int L = ni + 1, R = (int)n1.w;
+                const bool nf = (axis == 0 ? r.d.x : (axis == 1 ? r.d.y : r.d.z)) >= 0.0f;
+                if (tptr + 2 < kBvhStack) {
+                    tstack[++tptr] = nf ? R : L;
+                    tstack[++tptr] = nf ? L : R;
+                } else {
+                    flag_error(S, kErrBvhStack);
+                }
+            }
+        } else if (phase == 1) {
+            if (li >= lend) { phase = 0; continue; }
+            inst = li++;
+            const float4 q = __ldg(place + 2 * inst), ts = __ldg(place + 2 * inst + 1);
+            const float s = ts.w;
+            if (w) w->inst++;
+            ro = placement_rigid(q, ts, r.o) / s;
+            rd = qrot(q, r.d) / s;
+            cr = cw_ray(rd);
+            ptr = -1;
+            g_base = 0u;
+            g_hits = 1u << (cr.octinv & 7u);
+            g_imask = 1u;
+            t = t_near;
+            prim = -1;
+            found = false;
+            phase = 2;
+        } else {
+            if (g_hits == 0u) {
+                if (ptr < 0) {             // this instance's BLAS walk is done
+                    if (!ANY && found) {
+                        t_near = t;
+                        h.t = t;
+                        h.region = region;
+                        h.element = inst;
+                        h.prim = prim;
+                    }
+                    phase = 1;
+                    continue;
+                }
+                const uint2 top = stack[ptr];
+                g_base = top.x;
+                g_hits = top.y & 0xFFu;
+                g_imask = top.y >> 8;
+                ptr--;
+                continue;
+            }
+            const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
+            if (g_hits != 0u) {
+                if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
+                else flag_error(S, kErrCwStack);
+            }
+            if (w) w->nodes++;
+            const CwNodeHits nh = cw_node(nodes + 5 * (size_t)child, ro, cr, ANY ? max_dist : t);
+            unsigned leaf_bits = nh.leaf_bits;
+            while (leaf_bits != 0u) {
+                const int lb = find_msb24(leaf_bits);
+                leaf_bits &= ~(1u << (unsigned)lb);
+                const int i = (int)nh.leaf_base + lb;
+                f3 a, e1, e2;
+                if (w) w->tris++;
+                load_tri(tri, i, a, e1, e2);
+                float tt;
+                if (ANY) {
+                    if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < max_dist) return true;
+                } else if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < t) {
+                    t = tt;
+                    prim = i;
+                    found = true;
+                }
+            }
+            if (nh.hits != 0u) { g_base = nh.child_base; g_hits = nh.hits; g_imask = nh.imask; }
+            else g_hits = 0u;
+        }
+    }
+    flag_error(S, kErrCwGuard);
+    return false;
+}
+// The flat loop applies to mesh prototypes walked as CWBVH under the binary TLAS
+// (PTR_FLAT_INST=0 builds keep the nested walks everywhere).
+#ifndef PTR_FLAT_INST
+#define PTR_FLAT_INST 1
+#endif
+__device__ __forceinline__ bool inst_mesh_flat_ok(const DevScene& S, const DevBatch& b) {
+    return PTR_FLAT_INST && b.proto_shape == PTR_SHAPE_MESH && S.accel == PTR_ACCEL_CWBVH &&
+           !(S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w) && S.meshes[b.proto_mesh].cwbvh != nullptr;
+}
+
 // ---- region arms ------------------------------------------------------------------------
 __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_region& g, int region, const Ray& r, HitRec& h,
                                               Work* w = nullptr) {
@@ -275,6 +429,10 @@ __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_regio
         return;
     }
     const DevBatch& b = S.batches[g.ref];
+    if (inst_mesh_flat_ok(S, b)) {
+        inst_mesh_flat<false>(S, b, region, r, h, 0.0f, w);
+        return;
+    }
     float t_near = h.t;
     const bool wide = S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w;
     const float4* place = wide ? b.place_w : b.place;
@@ -313,6 +471,10 @@ __device__ __forceinline__ bool accel_any(const DevScene& S, const ptr_region& g
                                           Work* w = nullptr) {
     if (g.shape == PTR_SHAPE_MESH) return mesh_any(S, S.meshes[g.ref], r.o, r.d, max_dist, w);
     const DevBatch& b = S.batches[g.ref];
+    if (inst_mesh_flat_ok(S, b)) {
+        HitRec unused;
+        return inst_mesh_flat<true>(S, b, 0, r, unused, max_dist, w);
+    }
     const bool wide = S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w;
     const float4* place = wide ? b.place_w : b.place;
     auto instance = [&](int i) -> bool {

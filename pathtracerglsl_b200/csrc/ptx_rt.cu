@@ -71,8 +71,8 @@ struct ptr_program {
     const ptr_scene* last_scene = nullptr;
     int work_valid = 0;
     int profile_next = 0;
-    float prof_ms[5] = {0, 0, 0, 0, 0};
-    int prof_launches[5] = {0, 0, 0, 0, 0};
+    float prof_ms[PTR_PROFILE_CLASSES] = {};
+    int prof_launches[PTR_PROFILE_CLASSES] = {};
     // adjoint
     float* adj_dl = nullptr;          // W*H*3 adjoint image
     size_t adj_dl_n = 0;
@@ -134,15 +134,20 @@ int resident_grid(const void* kern, int block, size_t smem, int n_sm) {
 
 // Launches a wavefront kernel on its resident grid.  A dry launcher only fills the
 // occupancy cache (run once outside stream capture, before the first captured wave).
+// count: if set, incremented per launch (the instrumented passes report kernel launches).
 struct Launcher {
     int block, n_sm;
     cudaStream_t st;
     bool dry;
+    int* count = nullptr;
     template <class... KA, class... A>
     void operator()(void (*kern)(KA...), size_t smem, A... args) const {
         const int g = resident_grid((const void*)kern, block, smem, n_sm);
-        if (!dry) kern<<<g, block, smem, st>>>(args...);
+        if (dry) return;
+        kern<<<g, block, smem, st>>>(args...);
+        if (count) ++*count;
     }
+    void count_raw(int n) const { if (!dry && count) *count += n; }
 };
 
 void free_pool(ptr_program* p) {
@@ -224,29 +229,29 @@ const ptr_tuning kDefaultTuning{1 << 24, 256, 1, 0};
 // Counting sort of a device-counted queue (src[0, *count)) by its keys into dst (a no-op on
 // the device below kSortMin entries).
 template <bool GATHER>
-void launch_sort(const PathPool& pool, const int* src, const unsigned char* keys, const unsigned* count, int* dst,
-                 cudaStream_t st, bool dry) {
-    if (dry) return;
-    k_sort_hist<GATHER><<<kSortChunks, kSortThreads, 0, st>>>(src, keys, count, pool.sort_hist);
-    k_sort_scan<<<1, kSortScanThreads, kSortScanSmem, st>>>(count, pool.sort_hist);
-    k_sort_scatter<GATHER><<<kSortChunks, kSortThreads, 0, st>>>(src, keys, count, pool.sort_hist, dst);
+void launch_sort(const Launcher& L, const PathPool& pool, const int* src, const unsigned char* keys, const unsigned* count, int* dst) {
+    if (L.dry) return;
+    k_sort_hist<GATHER><<<kSortChunks, kSortThreads, 0, L.st>>>(src, keys, count, pool.sort_hist);
+    k_sort_scan<<<1, kSortScanThreads, kSortScanSmem, L.st>>>(count, pool.sort_hist);
+    k_sort_scatter<GATHER><<<kSortChunks, kSortThreads, 0, L.st>>>(src, keys, count, pool.sort_hist, dst);
+    L.count_raw(3);
 }
 // After k_closest: the compacted live queue grouped by shading class (occupant-sorted
 // shading), keyed by path index, so each class keeps the compaction's ascending order.
-void launch_shade_sort(const PathPool& pool, int in, cudaStream_t st, bool dry) {
+void launch_shade_sort(const Launcher& L, const PathPool& pool, int in) {
     if (pool.sort_buckets <= 1) return;
-    launch_sort<true>(pool, pool.q[in], pool.sort_key, pool.cnt + in, pool.q_sorted, st, dry);
+    launch_sort<true>(L, pool, pool.q[in], pool.sort_key, pool.cnt + in, pool.q_sorted);
 }
 // After k_shade: the next closest-hit queue and the shadow queue in ray-coherence order.
-void launch_ray_sort(const PathPool& pool, int in, bool shadows, cudaStream_t st, bool dry) {
+void launch_ray_sort(const Launcher& L, const PathPool& pool, int in, bool shadows) {
     if (!pool.ray_sort) return;
-    launch_sort<false>(pool, pool.q[in ^ 1], pool.rkey, pool.cnt + (in ^ 1), pool.q_ray, st, dry);
-    if (shadows) launch_sort<false>(pool, pool.shq, pool.skey, pool.cnt + 2, pool.shq_s, st, dry);
+    launch_sort<false>(L, pool, pool.q[in ^ 1], pool.rkey, pool.cnt + (in ^ 1), pool.q_ray);
+    if (shadows) launch_sort<false>(L, pool, pool.shq, pool.skey, pool.cnt + 2, pool.shq_s);
 }
 const ptr_tuning& tuning_of(const ptr_program* p) { return p->ctx ? p->ctx->tune : kDefaultTuning; }
 
 // Event pairs around each launch of an instrumented render (kernel class, start, end).
-struct ProfRec { int cls; cudaEvent_t a, b; };
+struct ProfRec { int cls; cudaEvent_t a, b; int n0, n; };   // n: kernels launched in the region
 
 template <class Col>
 void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iters, float* samples, int n_sm,
@@ -256,16 +261,21 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     Sp.accel = p->desc.accel;
     Sp.inst_accel = p->desc.instance_accel;
     Sp.work = (p->profile_next & PTR_PROFILE_WORK) ? p->work_dev : nullptr;
+    int n_launched = 0;
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
-        ProfRec r{cls, nullptr, nullptr};
+        ProfRec r{cls, nullptr, nullptr, n_launched, 0};
         cudaEventCreate(&r.a);
         cudaEventCreate(&r.b);
         cudaEventRecord(r.a, st);
         prof->push_back(r);
         return &prof->back();
     };
-    auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
+    auto done = [&](ProfRec* r) {
+        if (!r) return;
+        cudaEventRecord(r->b, st);
+        r->n = n_launched - r->n0;
+    };
     const DevScene& S = Sp;
     ProgParams P;
     P.max_bounces = p->desc.max_bounces;
@@ -276,7 +286,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.scattering = p->desc.scattering;
     P.equiangular = p->desc.equiangular;
     const int block = tuning_of(p).block;
-    const Launcher L{block, n_sm, st, dry};
+    const Launcher L{block, n_sm, st, dry, &n_launched};
     PathPool pool = p->pool;
     pool.sort_buckets = tuning_of(p).sort_buckets;
     pool.ray_sort = tuning_of(p).ray_sort;
@@ -291,8 +301,12 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         r = mark(1);
         if (S.work) L(k_closest<true, false>, 0, S, pi, in, nob);
         else L(k_closest<false, false>, 0, S, pi, in, nob);
-        launch_shade_sort(pi, in, st, dry);   // occupant-sorted shading queue (counted with the traversal)
         done(r);
+        if (pool.sort_buckets > 1) {   // occupant-sorted shading queue
+            r = mark(5);
+            launch_shade_sort(L, pi, in);
+            done(r);
+        }
         const bool media = s->has_media != 0;
         r = mark(2);
         switch (P.direct * 2 + (media ? 1 : 0)) {
@@ -303,8 +317,12 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
             case 4: L(k_shade<Col, PTR_DIRECT_MIS, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
             default: L(k_shade<Col, PTR_DIRECT_MIS, true, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
         }
-        launch_ray_sort(pool, in, P.direct != PTR_DIRECT_NONE, st, dry);
         done(r);
+        if (pool.ray_sort) {
+            r = mark(5);
+            launch_ray_sort(L, pool, in, P.direct != PTR_DIRECT_NONE);
+            done(r);
+        }
         if (P.direct != PTR_DIRECT_NONE) {
             r = mark(3);
             // slot 1 (equiangular segment queries) before slot 0 (surface / vertex NEE)
@@ -326,6 +344,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     r = mark(4);
     L(k_film<SPECTRAL>, 0, pool, p->fp_dev, p->sum, p->sumsq, samples, S);
     if (!dry) k_advance<<<1, 32, 0, st>>>(pool);
+    L.count_raw(1);
     done(r);
 }
 
@@ -383,21 +402,26 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
                        bool equiangular, cudaStream_t st, int iters, int n_sm, const ptr_tuning& tune,
                        std::vector<ProfRec>* prof = nullptr, bool dry = false) {
     const int block = tune.block;
-    const Launcher L{block, n_sm, st, dry};
+    int n_launched = 0;
+    const Launcher L{block, n_sm, st, dry, &n_launched};
     PathPool pool = pool_in;
     pool.sort_buckets = tune.sort_buckets;
     pool.ray_sort = tune.ray_sort;
     ProgParams P0{};
     auto mark = [&](int cls) -> ProfRec* {
         if (!prof) return nullptr;
-        ProfRec r{cls, nullptr, nullptr};
+        ProfRec r{cls, nullptr, nullptr, n_launched, 0};
         cudaEventCreate(&r.a);
         cudaEventCreate(&r.b);
         cudaEventRecord(r.a, st);
         prof->push_back(r);
         return &prof->back();
     };
-    auto done = [&](ProfRec* r) { if (r) cudaEventRecord(r->b, st); };
+    auto done = [&](ProfRec* r) {
+        if (!r) return;
+        cudaEventRecord(r->b, st);
+        r->n = n_launched - r->n0;
+    };
     ProfRec* r = mark(0);
     L(k_generate_batch, 0, pool, bt);
     done(r);
@@ -407,8 +431,12 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
         pi.ray_in = pool.ray_sort && it > 0;
         r = mark(1);
         L(k_closest<false, true>, 0, S0, pi, in, bt);
-        launch_shade_sort(pi, in, st, dry);
         done(r);
+        if (pool.sort_buckets > 1) {
+            r = mark(5);
+            launch_shade_sort(L, pi, in);
+            done(r);
+        }
         r = mark(2);
         switch (direct * 2 + (media ? 1 : 0)) {
             case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
@@ -418,8 +446,12 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
             case 4: L(k_shade<f3, PTR_DIRECT_MIS, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
             default: L(k_shade<f3, PTR_DIRECT_MIS, true, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
         }
-        launch_ray_sort(pool, in, direct != PTR_DIRECT_NONE, st, dry);
         done(r);
+        if (pool.ray_sort) {
+            r = mark(5);
+            launch_ray_sort(L, pool, in, direct != PTR_DIRECT_NONE);
+            done(r);
+        }
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
             for (int slot = equiangular ? 1 : 0; slot >= 0; --slot) {
@@ -432,6 +464,7 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
     r = mark(4);
     L(k_film_batch, 0, pool, bt);
     if (!dry) k_advance<<<1, 32, 0, st>>>(pool);
+    L.count_raw(1);
     done(r);
 }
 
@@ -846,16 +879,16 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
         for (long long w = 0; w < waves; ++w) CK(ctx, cudaGraphLaunch(p->graph, st));
     } else if (profiling) {
         std::vector<ProfRec> prof;
-        prof.reserve((size_t)waves * (iters * 3 + 2));
+        prof.reserve((size_t)waves * (iters * 5 + 2));
         for (long long w = 0; w < waves; ++w) launch_wave(p, s, st, iters, samples_dev, n_sm, &prof);
         CK(ctx, cudaGetLastError());
         CK(ctx, cudaStreamSynchronize(st));
-        for (int k = 0; k < 5; ++k) { p->prof_ms[k] = 0.f; p->prof_launches[k] = 0; }
+        for (int k = 0; k < PTR_PROFILE_CLASSES; ++k) { p->prof_ms[k] = 0.f; p->prof_launches[k] = 0; }
         for (ProfRec& r : prof) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, r.a, r.b);
             p->prof_ms[r.cls] += ms;
-            p->prof_launches[r.cls] += 1;
+            p->prof_launches[r.cls] += r.n;
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
         }
@@ -1182,18 +1215,18 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     if (profiling) {
         // instrumented: plain launches with events around each (no graph)
         std::vector<ProfRec> prof;
-        prof.reserve((size_t)waves * (iters * 3 + 2));
+        prof.reserve((size_t)waves * (iters * 5 + 2));
         for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
             launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, &prof);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        for (int k = 0; k < 5; ++k) { bp->prof_ms[k] = 0.0f; bp->prof_launches[k] = 0; }
+        for (int k = 0; k < PTR_PROFILE_CLASSES; ++k) { bp->prof_ms[k] = 0.0f; bp->prof_launches[k] = 0; }
         for (ProfRec& pr : prof) {
             float ms = 0.0f;
             if (e == cudaSuccess) cudaEventElapsedTime(&ms, pr.a, pr.b);
             bp->prof_ms[pr.cls] += ms;
-            bp->prof_launches[pr.cls] += 1;
+            bp->prof_launches[pr.cls] += pr.n;
             cudaEventDestroy(pr.a);
             cudaEventDestroy(pr.b);
         }
@@ -1519,7 +1552,7 @@ int ptr_profile_next(ptr_program* p, int enable) {
 
 int ptr_get_profile(ptr_program* p, float* ms_out, int* launches_out, int n) {
     if (!p) return PTR_E_INVALID;
-    for (int i = 0; i < n && i < 5; ++i) {
+    for (int i = 0; i < n && i < PTR_PROFILE_CLASSES; ++i) {
         if (ms_out) ms_out[i] = p->prof_ms[i];
         if (launches_out) launches_out[i] = p->prof_launches[i];
     }

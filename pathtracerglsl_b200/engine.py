@@ -196,7 +196,7 @@ class CudaEngine:
         self._check(self.lib.ptr_get_tuning(self.ctx, C.byref(t)))
         return {"capacity": t.capacity, "block": t.block, "sort_buckets": t.sort_buckets, "ray_sort": t.ray_sort}
 
-    KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film")
+    KERNEL_CLASSES = ("generate", "closest", "shade", "shadow", "film", "sort")
 
     def profile_render(self, width, height, spp, mode=abi.PROFILE_TIMING):
         """Render once instrumented: PROFILE_TIMING (CUDA events around every launch; per
@@ -204,9 +204,10 @@ class CudaEngine:
         traversal tallies, read with counters())."""
         self._check(self.lib.ptr_profile_next(self.programs[self.current], mode))
         self.render_frame(width, height, spp, sync=True)
-        ms = (C.c_float * 5)()
-        n = (C.c_int * 5)()
-        self._check(self.lib.ptr_get_profile(self.programs[self.current], ms, n, 5))
+        nc = len(self.KERNEL_CLASSES)
+        ms = (C.c_float * nc)()
+        n = (C.c_int * nc)()
+        self._check(self.lib.ptr_get_profile(self.programs[self.current], ms, n, nc))
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
 
     def counters(self):
@@ -302,13 +303,14 @@ class Batch:
         self.engine._check(self.lib.ptr_render_batch(self.engine.ctx, arr, len(arr)))
 
     def profile(self, frames):
-        """Render batched once with CUDA events around every launch; per kernel class
-        (summed device ms, launch count)."""
+        """Render batched once with CUDA events around each kernel class's launches; per
+        kernel class (summed device ms, kernel launches)."""
         self.engine._check(self.lib.ptr_profile_batch_next(self.engine.ctx, abi.PROFILE_TIMING))
         self.render(frames)
-        ms = (C.c_float * 5)()
-        n = (C.c_int * 5)()
-        self.engine._check(self.lib.ptr_get_batch_profile(self.engine.ctx, ms, n, 5))
+        nc = len(CudaEngine.KERNEL_CLASSES)
+        ms = (C.c_float * nc)()
+        n = (C.c_int * nc)()
+        self.engine._check(self.lib.ptr_get_batch_profile(self.engine.ctx, ms, n, nc))
         return {k: (ms[i], n[i]) for i, k in enumerate(CudaEngine.KERNEL_CLASSES)}
 
     def render_plain(self, frames, sync=True):
