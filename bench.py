@@ -270,6 +270,15 @@ def algorithmic_bytes(kernel, c, cw=True):
     return 0
 
 
+def parse_tuning(text):
+    """'sort_buckets=16,ray_sort=1' -> {'sort_buckets': 16, 'ray_sort': 1}."""
+    out = {}
+    for item in text.split(","):
+        k, v = item.split("=")
+        out[k.strip()] = int(v)
+    return out
+
+
 def run_ours(args):
     import torch
     rank, local, world, dist = dist_setup(args.gpus)
@@ -294,10 +303,15 @@ def run_ours(args):
     # queue order for this workload (two steps per candidate, before the warm-up and the
     # timed region); the default pool capacity and block size stay
     from pathtracerglsl_b200 import autotune
-    cands = [dict(capacity=0, block=256, sort_buckets=k, ray_sort=r) for k in (1, 8, 16) for r in (0, 1)]
-    tuned = autotune.tune(eng, step, cands, repeats=2, budget_s=60.0)
-    cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
-               tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
+    if args.tuning:   # a recorded pick (e.g. for a profiler run of the same configuration)
+        pick = dict(autotune.DEFAULTS, **parse_tuning(args.tuning))
+        eng.set_tuning(**pick)
+        cfg = dict(cfg, tuning=pick, tuning_search="given on the command line")
+    else:
+        cands = [dict(capacity=0, block=256, sort_buckets=k, ray_sort=r) for k in (1, 8, 16) for r in (0, 1)]
+        tuned = autotune.tune(eng, step, cands, repeats=2, budget_s=60.0)
+        cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
+                   tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
 
     for _ in range(args.warmup):
         step()
@@ -649,6 +663,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="", help="skip the autotuner: e.g. sort_buckets=16,ray_sort=1")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

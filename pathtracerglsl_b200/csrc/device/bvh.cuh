@@ -289,37 +289,41 @@ __device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3
 // BLAS node with its leaf triangles — so lanes at different levels proceed together.  Per
 // lane the sequence of node visits, leaf tests and tmax updates is that of the nested
 // walks, so hits (and the work tallies) are identical.  ANY: stop at the first triangle hit.
-template <bool ANY>
-__device__ __forceinline__ bool inst_mesh_flat(const DevScene& S, const DevBatch& b, int region, const Ray& r, HitRec& h,
-                                               float max_dist, Work* w) {
-    const DevMesh& m = S.meshes[b.proto_mesh];
-    const float4* tlas = b.tlas;
-    const float4* place = b.place;
-    const uint4* nodes = m.cwbvh;
-    const float4* tri = m.tri_w;
-    float t_near = ANY ? max_dist : h.t;   // TLAS culling distance
-    const f3 winv(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+// The walk as a resumable state: init() for one ray, then step() until it reports the end.
+struct InstFlat {
+    f3 winv;                               // TLAS: world-ray reciprocal, node stack, leaf range
     int tstack[kBvhStack];
-    int tptr = 0;
-    tstack[0] = 0;
-    int li = 0, lend = 0;                  // instances of the current TLAS leaf not yet entered
-    // the BLAS walk of the entered instance
-    f3 ro(0.f, 0.f, 0.f), rd(0.f, 0.f, 0.f);
-    CwRay cr{f3(0.f, 0.f, 0.f), 0u};
+    int tptr, li, lend;
+    f3 ro, rd;                             // BLAS: the entered instance's frame and group stack
+    CwRay cr;
     uint2 stack[kCwStack];
-    int ptr = -1;
-    unsigned g_base = 0u, g_hits = 0u, g_imask = 0u;
-    float t = 0.0f;
-    int prim = -1, inst = -1;
-    bool found = false;
-    int phase = 0;                         // 0 TLAS node, 1 next instance, 2 BLAS step
-    for (int guard = 0; guard < (1 << 22); ++guard) {
+    int ptr;
+    unsigned g_base, g_hits, g_imask;
+    float t, t_near;                       // t: BLAS tmax; t_near: TLAS culling distance
+    int prim, inst, phase;                 // phase: 0 TLAS node, 1 next instance, 2 BLAS step
+    bool found;
+    __device__ __forceinline__ void init(const Ray& r, float t0) {
+        winv = f3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+        tptr = 0;
+        tstack[0] = 0;
+        li = lend = 0;
+        ptr = -1;
+        g_hits = 0u;
+        t_near = t0;
+        phase = 0;
+        found = false;
+    }
+    // One step; false once the query is over.  Closest (ANY = false): h takes every nearer
+    // instance hit.  Any-hit: returns false with `found` set at the first hit.
+    template <bool ANY>
+    __device__ __forceinline__ bool step(const DevScene& S, const DevBatch& b, const DevMesh& m, int region, const Ray& r,
+                                         HitRec& h, float max_dist, Work* w) {
         if (phase == 0) {
             if (tptr < 0) return false;
             const int ni = tstack[tptr--];
             if (w) w->tlas++;
-            const float4 n0 = __ldg(tlas + 2 * ni), n1 = __ldg(tlas + 2 * ni + 1);
-            if (!aabb_hit(n0, n1, r.o, winv, t_near)) continue;
+            const float4 n0 = __ldg(b.tlas + 2 * ni), n1 = __ldg(b.tlas + 2 * ni + 1);
+            if (!aabb_hit(n0, n1, r.o, winv, t_near)) return true;
             if (n0.w >= 0.0f) {
                 li = (int)n1.w;
                 lend = li + (int)n0.w;
@@ -335,10 +339,12 @@ __device__ __forceinline__ bool inst_mesh_flat(const DevScene& S, const DevBatch
                     flag_error(S, kErrBvhStack);
                 }
             }
-        } else if (phase == 1) {
-            if (li >= lend) { phase = 0; continue; }
+            return true;
+        }
+        if (phase == 1) {
+            if (li >= lend) { phase = 0; return true; }
             inst = li++;
-            const float4 q = __ldg(place + 2 * inst), ts = __ldg(place + 2 * inst + 1);
+            const float4 q = __ldg(b.place + 2 * inst), ts = __ldg(b.place + 2 * inst + 1);
             const float s = ts.w;
             if (w) w->inst++;
             ro = placement_rigid(q, ts, r.o) / s;
@@ -352,54 +358,68 @@ __device__ __forceinline__ bool inst_mesh_flat(const DevScene& S, const DevBatch
             prim = -1;
             found = false;
             phase = 2;
-        } else {
-            if (g_hits == 0u) {
-                if (ptr < 0) {             // this instance's BLAS walk is done
-                    if (!ANY && found) {
-                        t_near = t;
-                        h.t = t;
-                        h.region = region;
-                        h.element = inst;
-                        h.prim = prim;
-                    }
-                    phase = 1;
-                    continue;
-                }
-                const uint2 top = stack[ptr];
-                g_base = top.x;
-                g_hits = top.y & 0xFFu;
-                g_imask = top.y >> 8;
-                ptr--;
-                continue;
-            }
-            const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
-            if (g_hits != 0u) {
-                if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
-                else flag_error(S, kErrCwStack);
-            }
-            if (w) w->nodes++;
-            const CwNodeHits nh = cw_node(nodes + 5 * (size_t)child, ro, cr, ANY ? max_dist : t);
-            unsigned leaf_bits = nh.leaf_bits;
-            while (leaf_bits != 0u) {
-                const int lb = find_msb24(leaf_bits);
-                leaf_bits &= ~(1u << (unsigned)lb);
-                const int i = (int)nh.leaf_base + lb;
-                f3 a, e1, e2;
-                if (w) w->tris++;
-                load_tri(tri, i, a, e1, e2);
-                float tt;
-                if (ANY) {
-                    if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < max_dist) return true;
-                } else if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < t) {
-                    t = tt;
-                    prim = i;
-                    found = true;
-                }
-            }
-            if (nh.hits != 0u) { g_base = nh.child_base; g_hits = nh.hits; g_imask = nh.imask; }
-            else g_hits = 0u;
+            return true;
         }
+        if (g_hits == 0u) {
+            if (ptr < 0) {                 // this instance's BLAS walk is done
+                if (!ANY && found) {
+                    t_near = t;
+                    h.t = t;
+                    h.region = region;
+                    h.element = inst;
+                    h.prim = prim;
+                }
+                phase = 1;
+                return true;
+            }
+            const uint2 top = stack[ptr];
+            g_base = top.x;
+            g_hits = top.y & 0xFFu;
+            g_imask = top.y >> 8;
+            ptr--;
+            return true;
+        }
+        const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
+        if (g_hits != 0u) {
+            if (ptr + 1 < kCwStack) { ptr++; stack[ptr] = make_uint2(g_base, g_hits | (g_imask << 8)); }
+            else flag_error(S, kErrCwStack);
+        }
+        if (w) w->nodes++;
+        const CwNodeHits nh = cw_node(m.cwbvh + 5 * (size_t)child, ro, cr, ANY ? max_dist : t);
+        unsigned leaf_bits = nh.leaf_bits;
+        while (leaf_bits != 0u) {
+            const int lb = find_msb24(leaf_bits);
+            leaf_bits &= ~(1u << (unsigned)lb);
+            const int i = (int)nh.leaf_base + lb;
+            f3 a, e1, e2;
+            if (w) w->tris++;
+            load_tri(m.tri_w, i, a, e1, e2);
+            float tt;
+            if (ANY) {
+                if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < max_dist) {
+                    found = true;
+                    return false;
+                }
+            } else if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < t) {
+                t = tt;
+                prim = i;
+                found = true;
+            }
+        }
+        if (nh.hits != 0u) { g_base = nh.child_base; g_hits = nh.hits; g_imask = nh.imask; }
+        else g_hits = 0u;
+        return true;
     }
+};
+constexpr int kFlatGuard = 1 << 22;        // steps of one query before the walk gives up
+template <bool ANY>
+__device__ __forceinline__ bool inst_mesh_flat(const DevScene& S, const DevBatch& b, int region, const Ray& r, HitRec& h,
+                                               float max_dist, Work* w) {
+    const DevMesh& m = S.meshes[b.proto_mesh];
+    InstFlat f;
+    f.init(r, ANY ? max_dist : h.t);
+    for (int guard = 0; guard < kFlatGuard; ++guard)
+        if (!f.step<ANY>(S, b, m, region, r, h, max_dist, w)) return ANY && f.found;
     flag_error(S, kErrCwGuard);
     return false;
 }

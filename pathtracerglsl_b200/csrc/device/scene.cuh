@@ -51,7 +51,10 @@ struct DevScene {
     int n_linear, n_region_nodes, pad_r0, pad_r1;
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
-    int inst_accel, pad_i0, pad_i1, pad_i2;   // PTR_ACCEL_* of the instanced batches' TLAS
+    int inst_accel;           // PTR_ACCEL_* of the instanced batches' TLAS
+    int flat_region = -1;     // the one acceleration region when every other region is analytic
+                              // and there is no region BVH (refilling closest-hit loop), else -1
+    int pad_i1, pad_i2;
     float sort_c[4];          // centre of the bounded geometry (ray-coherence keys)
     // environment
     int env_kind, env_samplable, env_select_live, env_w;

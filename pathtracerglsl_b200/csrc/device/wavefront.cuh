@@ -484,6 +484,79 @@ __device__ __forceinline__ unsigned shade_key(const DevScene& S, int region, int
 }
 
 // Nearest hit of every live path (and, for the sorted queue, its shading key).
+// Closest hits of a queue whose scene is analytic regions plus one instanced mesh batch
+// walked by the flat two-level loop: a lane whose query ends takes the next ray at once
+// (warp-aggregated tickets whenever at least kRefillMin lanes are idle) instead of idling
+// until the warp's slowest ray is done.  The regions before and after the instanced one
+// are tested in region order around the walk, as in scene_closest, so hits are identical.
+// (PTR_REFILL=0 builds keep the per-warp queue cursor everywhere.)
+#ifndef PTR_REFILL
+#define PTR_REFILL 1
+#endif
+constexpr int kRefillMin = 8;
+template <bool COUNT>
+__device__ __forceinline__ void closest_refill(const DevScene& S, const PathPool& pool, const int* q, unsigned n, int buckets,
+                                               unsigned* ticket, Work* w) {
+    const int fr = S.flat_region;
+    const DevBatch& b = S.batches[S.regions[fr].ref];
+    const DevMesh& m = S.meshes[b.proto_mesh];
+    const unsigned lane = threadIdx.x & 31u;
+    InstFlat f;
+    Ray r;
+    HitRec h;
+    int i = -1, steps = 0;
+    bool active = false, exhausted = false;
+    for (;;) {
+        if (!exhausted) {
+            const unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (__popc(need) >= kRefillMin) {
+                const int leader = __ffs(need) - 1;
+                unsigned base = 0u;
+                if ((int)lane == leader) base = atomicAdd(ticket, (unsigned)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (unsigned)__popc(need) >= n) exhausted = true;
+                if (!active) {
+                    const unsigned k = base + __popc(need & lanemask_lt());
+                    if (k < n) {
+                        i = q[k];
+                        r.o = xyz(pool.ray_o[i]);
+                        r.d = xyz(pool.ray_d[i]);
+                        h.t = kMaxDist;
+                        h.u = h.v = 0.f;
+                        h.region = -1;
+                        h.element = 0;
+                        h.prim = -1;
+                        for (int g = 0; g < fr; ++g) {
+                            float t;
+                            if (analytic_root(S.regions[g], r, t) && t < h.t) { h.t = t; h.region = g; h.element = 0; h.prim = -1; }
+                        }
+                        f.init(r, h.t);
+                        steps = 0;
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+        bool more = f.step<false>(S, b, m, fr, r, h, 0.0f, COUNT ? w : nullptr);
+        if (more && ++steps >= kFlatGuard) {
+            flag_error(S, kErrCwGuard);
+            more = false;
+        }
+        if (!more) {
+            for (int g = fr + 1; g < S.n_regions; ++g) {
+                float t;
+                if (analytic_root(S.regions[g], r, t) && t < h.t) { h.t = t; h.region = g; h.element = 0; h.prim = -1; }
+            }
+            pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
+            pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
+            if (buckets > 1) pool.sort_key[i] = (unsigned char)shade_key(S, h.region, pool.st[i].y, buckets);
+            active = false;
+        }
+    }
+}
+
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S0, PathPool pool, int in, BatchTables bt) {
     const int buckets = pool.sort_buckets;
@@ -497,6 +570,11 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     }
     const int* q = closest_queue(pool, in);
     Work w{0u, 0u, 0u, 0u};
+    if (PTR_REFILL && !BATCH && pool.fetch && S0.flat_region >= 0 && inst_mesh_flat_ok(S0, S0.batches[S0.regions[S0.flat_region].ref])) {
+        closest_refill<COUNT>(S0, pool, q, n, buckets, pool.fetch + 0, &w);
+        if (COUNT) flush_work(S0, w);
+        return;
+    }
     QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
     unsigned k;
     while (cur.next(k)) {
@@ -1080,6 +1158,82 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
 // its vertex and d log T / d theta of every medium segment the shadow ray crossed.
 constexpr int kAdjMaxMedia = 4;            // distinct media one adjoint shadow query may cross
 constexpr unsigned kErrAdjMedia = 8u;      // ... more were crossed (their terms were dropped)
+// Opaque shadow queries over the same scene form, with the same per-lane refill: the
+// regions before the instanced one, the flat any-hit walk, then the regions after it (the
+// order of scene_any); an unoccluded query adds its stored contribution as k_shadow does.
+template <class Col, bool COUNT>
+__device__ __forceinline__ void shadow_refill(const DevScene& S, const PathPool& pool, const int* shq, unsigned n, int slot,
+                                              const float4* a_o, const float4* a_d, const float4* a_lp, const float4* a_c,
+                                              unsigned* ticket, Work* w) {
+    constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
+    const int fr = S.flat_region;
+    const DevBatch& b = S.batches[S.regions[fr].ref];
+    const DevMesh& m = S.meshes[b.proto_mesh];
+    const unsigned lane = threadIdx.x & 31u;
+    InstFlat f;
+    Ray r;
+    HitRec unused;
+    float max_dist = 0.0f;
+    int i = -1, steps = 0;
+    bool active = false, exhausted = false;
+    for (;;) {
+        if (!exhausted) {
+            const unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (__popc(need) >= kRefillMin) {
+                const int leader = __ffs(need) - 1;
+                unsigned base = 0u;
+                if ((int)lane == leader) base = atomicAdd(ticket, (unsigned)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (unsigned)__popc(need) >= n) exhausted = true;
+                if (!active) {
+                    const unsigned k = base + __popc(need & lanemask_lt());
+                    if (k < n) {
+                        i = shq[k];
+                        const float4 so = a_o[i], sd = a_d[i];
+                        r.o = xyz(so);
+                        r.d = xyz(sd);
+                        max_dist = so.w;
+                        bool blocked = false;
+                        for (int g = 0; g < fr && !blocked; ++g) {
+                            float t;
+                            blocked = analytic_root(S.regions[g], r, t) && t < max_dist;
+                        }
+                        if (!blocked) {            // an occluded query is finished: nothing to add
+                            f.init(r, max_dist);
+                            steps = 0;
+                            active = true;
+                        }
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+        bool more = f.step<true>(S, b, m, fr, r, unused, max_dist, COUNT ? w : nullptr);
+        if (more && ++steps >= kFlatGuard) {
+            flag_error(S, kErrCwGuard);
+            more = false;
+        }
+        if (!more) {
+            bool blocked = f.found;
+            for (int g = fr + 1; g < S.n_regions && !blocked; ++g) {
+                float t;
+                blocked = analytic_root(S.regions[g], r, t) && t < max_dist;
+            }
+            if (!blocked) {
+                const float4 c = a_c[i];
+                const Col cc = col_ld<Col>(c);
+                float cpdf = c.w;
+                if constexpr (SPECTRAL) cpdf = slot ? pool.sh2_pdf[i] : pool.sh_pdf[i];
+                const Col vis(1.0f);
+                const Col add = cc * vis * a_lp[i].w / cpdf;
+                pool.rad[i] = col_st(col_ld<Col>(pool.rad[i]) + add, 0.0f);
+            }
+            active = false;
+        }
+    }
+}
+
 template <class Col, bool MEDIA, bool COUNT, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt,
                                                                       int slot, AdjParams adj = AdjParams{}) {
@@ -1095,6 +1249,12 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     const float4* a_lp = slot ? pool.sh2_lp : pool.sh_lp;
     const float4* a_c = slot ? pool.sh2_c : pool.sh_c;
     Work wk{0u, 0u, 0u, 0u};
+    if (PTR_REFILL && !MEDIA && !BATCH && !ADJ && pool.fetch && S0.flat_region >= 0 &&
+        inst_mesh_flat_ok(S0, S0.batches[S0.regions[S0.flat_region].ref])) {
+        shadow_refill<Col, COUNT>(S0, pool, shq, n, slot, a_o, a_d, a_lp, a_c, pool.fetch + 1 + slot, &wk);
+        if (COUNT) flush_work(S0, wk);
+        return;
+    }
     QueueCursor cur(n, pool.fetch ? pool.fetch + 1 + slot : nullptr);
     unsigned k;
     while (cur.next(k)) {

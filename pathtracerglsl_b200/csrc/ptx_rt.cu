@@ -1034,6 +1034,18 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     }
     rc = upload_accels(ctx, s, d);
     if (!rc) rc = upload_region_bvh(ctx, s, d);
+    if (!rc) {
+        // the refilling closest-hit loop's scene form: analytic regions and exactly one
+        // acceleration region, an instanced mesh batch, with no region BVH
+        int accel_regions = 0, flat = -1;
+        for (int i = 0; i < d->n_regions; ++i) {
+            if (d->regions[i].shape < PTR_SHAPE_MESH) continue;
+            ++accel_regions;
+            if (d->regions[i].shape == PTR_SHAPE_INSTANCES && d->batches[d->regions[i].ref].prototype_shape == PTR_SHAPE_MESH)
+                flat = i;
+        }
+        s->dev.flat_region = (accel_regions == 1 && !s->dev.region_bvh) ? flat : -1;
+    }
     if (rc) {
         ptr_free_scene(s);
         return rc;
