@@ -236,10 +236,12 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes per launch of the roofline kernel, from one ncu capture of one whole wave of the
-# same command (profiles/k_closest_mesh_full.md, profiles/k_shade_cornell_full.md):
-# (workload, kernel) -> bytes per launch averaged over the wave's launches.
-NCU_TRAFFIC = {("mesh", "closest"): 58.77e6, ("cornell", "shade"): 288.2e6}
+# DRAM bytes of the roofline kernel per closest-hit query (a shaded path, for k_shade), from
+# one ncu capture of one whole wave of the workload at 1 spp with the autotuner's pick
+# (dram__bytes_read.sum + dram__bytes_write.sum over the wave's launches / the wave's
+# queries; profiles/k_closest_mesh_full.md, profiles/k_shade_cornell_full.md).  Scaled to a
+# launch of the timed configuration by its queries per launch.
+NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 393.66}
 # the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
 ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
 
@@ -287,6 +289,9 @@ def run_ours(args):
     from pathtracerglsl_b200.engine import CudaEngine
 
     sc, st, w, h, spp, cfg = workload(args.workload)
+    if args.spp:      # a smaller step of the same scene (profiler captures)
+        spp = args.spp
+        cfg = dict(cfg, spp_per_step=spp)
     renderer, packed = Compiler().compile(sc, st)
     eng = CudaEngine(local)
     eng.register_scene(packed)
@@ -309,7 +314,7 @@ def run_ours(args):
         cfg = dict(cfg, tuning=pick, tuning_search="given on the command line")
     else:
         cands = [dict(capacity=0, block=256, sort_buckets=k, ray_sort=r) for k in (1, 8, 16) for r in (0, 1)]
-        tuned = autotune.tune(eng, step, cands, repeats=2, budget_s=60.0)
+        tuned = autotune.tune(eng, step, cands, repeats=2, budget_s=60.0, min_time_s=0.25)
         cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
                    tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
 
@@ -373,7 +378,8 @@ def run_ours(args):
     total_prof_ms = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": "k_" + kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": NCU_TRAFFIC.get((args.workload, kernel)),
+                "traffic": (NCU_TRAFFIC_PER_QUERY[(args.workload, kernel)] * cnt["closest_queries"] / max(klaunch, 1)
+                            if (args.workload, kernel) in NCU_TRAFFIC_PER_QUERY else None),
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                 "share": {k: v[0] / total_prof_ms for k, v in prof.items()}}
     launches = sum(v[1] for v in prof.values()) + 1   # + the frame-parameter kernel
@@ -664,6 +670,7 @@ def main():
     ap.add_argument("--workload", default="mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="", help="skip the autotuner: e.g. sort_buckets=16,ray_sort=1")
+    ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0: the workload's own)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -18,8 +18,12 @@ KNOBS = ("capacity", "block", "sort_buckets", "ray_sort")
 DEFAULTS = {"capacity": 0, "block": 256, "sort_buckets": 1, "ray_sort": 0}
 
 
-def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
-    """Time render() under each candidate tuning; apply and return the best record."""
+def tune(engine, render, candidates=None, repeats=1, budget_s=60.0, min_time_s=0.0):
+    """Time render() under each candidate tuning; apply and return the best record.
+
+    Each candidate runs `repeats` timed renders, and more while their total stays under
+    `min_time_s` (short renders need many repetitions to separate candidates a few per
+    cent apart); its time is the best single render."""
     candidates = list(candidates or DEFAULT_CANDIDATES)
     results = []
     t_start = time.perf_counter()
@@ -29,11 +33,16 @@ def tune(engine, render, candidates=None, repeats=1, budget_s=60.0):
         render()                       # warm-up: pool allocation, graph capture
         engine.sync()
         best = float("inf")
-        for _ in range(max(1, repeats)):
+        spent = 0.0
+        k = 0
+        while k < max(1, repeats) or spent < min_time_s:
             t0 = time.perf_counter()
             render()
             engine.sync()
-            best = min(best, time.perf_counter() - t0)
+            dt = time.perf_counter() - t0
+            best = min(best, dt)
+            spent += dt
+            k += 1
         results.append(dict(cand, ms=1000.0 * best))
         if time.perf_counter() - t_start > budget_s:
             break
