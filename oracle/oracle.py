@@ -50,6 +50,8 @@ def lib():
         _lib.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_mesh_brute.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.oracle_forward_tile.restype = ctypes.c_int
+        _lib.oracle_forward_tile.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 2 + [ctypes.c_int]
     return _lib
 
 
@@ -81,6 +83,30 @@ def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=
     if samples is not None:
         out["samples"] = samples
     return out
+
+
+def forward(packed, renderer, width, height, spp, first_sample=0, salt=0, params=None, threads=0):
+    """Forward-mode reference of the path-replay adjoint (float64 tangents along the
+    oracle's own walk, same random numbers as a render with the same frame).  Returns
+    dict(jac, mean): jac[y, x, c, PTR_GRAD_SLOTS * material + slot] = d I / d theta of the
+    pixel's mean over the frame's samples, row 0 = bottom; mean = the image itself."""
+    from pathtracerglsl_b200 import abi
+    desc = packed.desc()
+    fr = abi.Frame()
+    fr.width, fr.height = width, height
+    fr.first_sample, fr.spp = first_sample, spp
+    fr.reset_salt = salt
+    fr.camera = renderer.camera(params or {}, width, height)
+    K = abi.GRAD_SLOTS * len(packed.materials)
+    jac = np.zeros((height, width, 3, K), np.float64)
+    s = np.zeros((height, width, 3), np.float64)
+    rc = lib().oracle_forward_tile(ctypes.addressof(desc), ctypes.addressof(renderer.program), ctypes.addressof(fr),
+                                   0, 0, width, height, jac.ctypes.data, s.ctypes.data, threads)
+    if rc == -2:
+        raise ValueError("forward mode covers the adjoint's model only: RGB, no equiangular NEE, grey media")
+    if rc != 0:
+        raise RuntimeError(f"oracle_forward_tile failed: {rc}")
+    return {"jac": jac / spp, "mean": s / spp}
 
 
 def render_tile(packed, renderer, width, height, tile, spp, first_sample=0, salt=0, params=None, threads=0):

@@ -783,6 +783,69 @@ inline ISample hg_sample(v3 wo, float g, float x0, float x1) {
     return s;
 }
 
+// ---------------------------------------------------------------- forward-mode duals
+// FP64 dual numbers (value, derivative along one parameter) for the forward-mode reference
+// of the path-replay adjoint (oracle_forward_tile).  The functions below are the BSDF,
+// phase and Fresnel formulas of this file (same expressions, in float64), differentiated
+// by the dual arithmetic itself: they check the adjoint's hand-derived log-derivatives.
+struct Dual { double v, d; };
+inline Dual dc(double v) { return {v, 0.0}; }
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+inline Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+inline Dual dsqrt(Dual a) { double r = std::sqrt(a.v); return {r, r > 0.0 ? a.d / (2.0 * r) : 0.0}; }
+inline Dual dexp(Dual a) { double e = std::exp(a.v); return {e, e * a.d}; }
+constexpr double PI_D = 3.14159265359;   // the same constant as PI, in float64
+
+// Trowbridge-Reitz D, separable Smith G1 (microfacet.glsl:22-54) with a dual alpha.
+inline Dual mf_D_dual(double hz, Dual a) {
+    Dual a2 = a * a;
+    Dual t = hz * hz * (a2 - 1.0) + 1.0;
+    return a2 / (PI_D * t * t);
+}
+inline Dual mf_G1_dual(double c, Dual a) {
+    c = std::fabs(c);
+    Dual a2 = a * a;
+    return 2.0 * c / (c + dsqrt(a2 + (1.0 - a2) * c * c));
+}
+// The GGX conductor's f without its Fresnel factor (ggx.glsl:16-64), dual alpha.
+inline Dual ggx_fs_dual(v3 wi, v3 wo, const Frame& f, Dual a) {
+    const double wil[3] = {(double)dot(wi, f.t), (double)dot(wi, f.b), (double)dot(wi, f.n)};
+    const double wol[3] = {(double)dot(wo, f.t), (double)dot(wo, f.b), (double)dot(wo, f.n)};
+    if (wil[2] * wol[2] <= 0.0) return dc(0.0);
+    double h[3] = {wil[0] + wol[0], wil[1] + wol[1], wil[2] + wol[2]};
+    const double hl = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    const double hz = h[2] / hl;
+    return mf_D_dual(hz, a) * mf_G1_dual(wil[2], a) * mf_G1_dual(wol[2], a) /
+           (4.0 * std::fabs(wil[2]) * std::fabs(wol[2]));
+}
+// Henyey-Greenstein (hg.glsl:11-42, forward convention), dual g.
+inline Dual hg_dual(v3 wi, v3 wo, Dual g) {
+    const double c = (double)dot(wi, -wo);
+    Dual d = 1.0 + g * g - 2.0 * g * c;
+    Dual dd = d.v > 1e-8 ? d : dc(1e-8);
+    return (1.0 - g * g) / (4.0 * PI_D * d * dsqrt(dd));
+}
+// Unpolarised dielectric Fresnel (math.glsl:95-102), dual relative IOR.
+inline Dual fresnel_dual(double cos_i, Dual eta) {
+    Dual sin2_t = eta * eta * (1.0 - cos_i * cos_i);
+    if (sin2_t.v >= 1.0) return dc(1.0);
+    Dual cos_t = dsqrt(1.0 - sin2_t);
+    Dual r_par = (cos_i - eta * cos_t) / (cos_i + eta * cos_t);
+    Dual r_perp = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
+    return 0.5 * (r_par * r_par + r_perp * r_perp);
+}
+
 // ---------------------------------------------------------------- the renderer
 struct Counters { uint64_t closest = 0, shadow = 0; };
 
@@ -793,6 +856,60 @@ struct Tracer {
     Rng rng;
     Counters cnt;
     Tracer(const Scene& s) : S(s), d(*s.d), P(*s.prog) {}
+
+    // ---- forward-mode tangents (oracle_forward_tile only; null in the plain renders, whose
+    // float32 walk they never touch).  d throughput / d theta_k and d radiance / d theta_k
+    // per channel in float64, k = PTR_GRAD_SLOTS * material + slot, stored at [3 k + c].
+    // The estimator differentiated is the adjoint's: sampled directions and distances,
+    // sampling densities, MIS weights and roulette probabilities are held fixed (detached),
+    // and each weight site contributes the derivative of its own formula.
+    struct Tan { int K = 0; std::vector<double> thr, rad; };
+    Tan* tan = nullptr;
+    struct DW { int k; double d[3]; };   // one parameter's derivative of a weight, per channel
+    static constexpr int kMaxDW = 16;
+    int slot_k(int mat, int slot) const { return PTR_GRAD_SLOTS * mat + slot; }
+    void tan_reset() {
+        std::fill(tan->thr.begin(), tan->thr.end(), 0.0);
+        std::fill(tan->rad.begin(), tan->rad.end(), 0.0);
+    }
+    // throughput <- throughput * W:  d thr = d thr * W + thr * dW
+    void tan_mul(v3 thr, v3 W, const DW* dw, int n) {
+        if (!tan) return;
+        for (int k = 0; k < tan->K; ++k)
+            for (int c = 0; c < 3; ++c) tan->thr[3 * k + c] *= (double)W[c];
+        for (int j = 0; j < n; ++j)
+            for (int c = 0; c < 3; ++c) tan->thr[3 * dw[j].k + c] += (double)thr[c] * dw[j].d[c];
+    }
+    // radiance += throughput * X:  d rad += d thr * X + thr * dX
+    void tan_add(v3 thr, v3 X, const DW* dw, int n) {
+        if (!tan) return;
+        for (int k = 0; k < tan->K; ++k)
+            for (int c = 0; c < 3; ++c) tan->rad[3 * k + c] += tan->thr[3 * k + c] * (double)X[c];
+        for (int j = 0; j < n; ++j)
+            for (int c = 0; c < 3; ++c) tan->rad[3 * dw[j].k + c] += (double)thr[c] * dw[j].d[c];
+    }
+    // grey homogeneous medium parameters (channel 0): sigma_t and the albedo a
+    void grey_params(int med, double& st, double& a) const {
+        const ptr_material& m = d.materials[med];
+        st = (double)m.sigma_a[0] + (double)m.sigma_s[0];
+        a = st > 0.0 ? (double)m.sigma_s[0] / st : 0.0;
+    }
+    // the dielectric IOR parameter a region's IOR follows, or -1
+    int ior_param(int region) const {
+        if (region < 0) return -1;
+        const int m = d.regions[region].material;
+        return (m >= 0 && d.materials[m].model == PTR_MAT_DIELECTRIC) ? slot_k(m, PTR_GRAD_IOR) : -1;
+    }
+    // the per-parameter derivatives X dlog_k of X from its log-derivatives, appended at n
+    static int dw_from_dlog(v3 X, const std::vector<std::pair<int, double>>& dlog, std::vector<DW>& out, int n) {
+        if (out.size() < (size_t)n + dlog.size()) out.resize((size_t)n + dlog.size());
+        for (const auto& e : dlog) {
+            out[n].k = e.first;
+            for (int c = 0; c < 3; ++c) out[n].d[c] = (double)X[c] * e.second;
+            ++n;
+        }
+        return n;
+    }
 
     bool intersect(const Ray& r, Hit& h) { cnt.closest++; return S.scene_intersect(r, h); }
 
@@ -1079,7 +1196,8 @@ struct Tracer {
 
     // shadow_transmittance: opaque (transport/shadow/opaque/opaque.glsl:16-19) or the
     // media segment walker (transport/shadow/media/media.glsl:29-62)
-    v3 shadow_transmittance(Ray sr, v3 light_p, int crossings_left) {
+    // dlog (forward mode): d log T / d theta_k of every medium segment crossed, appended
+    v3 shadow_transmittance(Ray sr, v3 light_p, int crossings_left, std::vector<std::pair<int, double>>* dlog = nullptr) {
         cnt.shadow++;
         if (!S.has_media) {
             float maxDist = length(light_p - sr.o) - SHADOW_BACKOFF;
@@ -1095,7 +1213,19 @@ struct Tracer {
             bool hit_boundary = S.scene_intersect(seg, h) && h.t < remaining;
             float seg_len = hit_boundary ? h.t : remaining;
             int med_mat = S.material_of(medium);
-            if (S.material_has_medium(med_mat)) T = T * medium_transmittance(med_mat, seg_len);
+            if (S.material_has_medium(med_mat)) {
+                T = T * medium_transmittance(med_mat, seg_len);
+                if (dlog) {   // T_seg = exp(-sigma len), sigma = st (scattering) or (1 - a) st
+                    double st, a;
+                    grey_params(med_mat, st, a);
+                    if (scatter_live(med_mat)) {
+                        dlog->push_back({slot_k(med_mat, PTR_GRAD_SIGMA_T), -(double)seg_len});
+                    } else {
+                        dlog->push_back({slot_k(med_mat, PTR_GRAD_SIGMA_T), -(1.0 - a) * (double)seg_len});
+                        dlog->push_back({slot_k(med_mat, PTR_GRAD_MEDIUM_ALBEDO), st * (double)seg_len});
+                    }
+                }
+            }
             if (!hit_boundary) return T;
             if (!S.is_null_interface(S.material_of(h.region_owner))) return v3(0.0f);
             medium = h.region_to;
@@ -1183,6 +1313,50 @@ struct Tracer {
         radiance = radiance + thr * T_seg * sigma_s * ph * Le * vis / denom;
     }
 
+    // The continuation lobe's weight derivative (forward mode).  Lambert: w = albedo.
+    // GGX: w = f cos / pdf with the pdf detached, so dw = w d log fs(alpha).  Dielectric:
+    // w = F / F_detached (reflection) or T (n_i / n_t)^2 (1 - F) / (1 - F)_detached
+    // (refraction), differentiated along the IORs of the two regions the interface joins.
+    void tan_continuation(const ptr_material& m, int mat, v3 wo, const Hit& hit, const ISample& bs, v3 thr, DW* dw) {
+        int n = 0;
+        if (m.model == PTR_MAT_LAMBERT) {
+            for (int c = 0; c < 3; ++c) {
+                dw[n].k = slot_k(mat, PTR_GRAD_ALBEDO_R + c);
+                dw[n].d[0] = dw[n].d[1] = dw[n].d[2] = 0.0;
+                dw[n].d[c] = 1.0;
+                ++n;
+            }
+        } else if (m.model == PTR_MAT_GGX) {
+            if (hit_alpha < 0.0f) {
+                const Dual fs = ggx_fs_dual(bs.wi, wo, hit.frame, Dual{(double)m.alpha, 1.0});
+                dw[n].k = slot_k(mat, PTR_GRAD_ALPHA);
+                for (int c = 0; c < 3; ++c) dw[n].d[c] = fs.v > 0.0 ? (double)bs.weight[c] * fs.d / fs.v : 0.0;
+                ++n;
+            }
+        } else if (m.model == PTR_MAT_DIELECTRIC) {
+            const float n_i = S.ior_of(hit.region_from), n_t = S.ior_of(hit.region_to);
+            const float cos_i = clampf(dot(wo, hit.frame.n), 1e-6f, 1.0f);
+            const float F_det = dielectric_fresnel(cos_i, n_i / n_t);
+            const int kf = ior_param(hit.region_from), kt = ior_param(hit.region_to);
+            const int ks[2] = {kf, kt != kf ? kt : -1};
+            for (int j = 0; j < 2; ++j) {
+                if (ks[j] < 0) continue;
+                const Dual ni{(double)n_i, ks[j] == kf ? 1.0 : 0.0}, nt{(double)n_t, ks[j] == kt ? 1.0 : 0.0};
+                const Dual F = fresnel_dual((double)cos_i, ni / nt);
+                dw[n].k = ks[j];
+                if (bs.flags & LOBE_REFLECTION) {
+                    for (int c = 0; c < 3; ++c) dw[n].d[c] = F.d / (double)F_det;
+                } else {
+                    const Dual scale = (ni * ni) / (nt * nt);
+                    const double dd = (scale.d * (1.0 - F.v) - scale.v * F.d) / (1.0 - (double)F_det);
+                    for (int c = 0; c < 3; ++c) dw[n].d[c] = (double)m.transmittance[c] * dd;
+                }
+                ++n;
+            }
+        }
+        tan_mul(thr, bs.weight, dw, n);
+    }
+
     // ---- the walk (transport/integrators/pt/pt.ts:299-464, as emitted for media scenes)
     v3 transport_trace(Ray ray) {
         const bool nee = P.direct != PTR_DIRECT_NONE;
@@ -1205,6 +1379,7 @@ struct Tracer {
             float p_survive = fminf_(P.rr_max_survival, spectrum_max(throughput) * eta_scale);
             if (p_survive <= 0.0f) return false;
             if (rng.next() > p_survive) return false;
+            if (tan) for (double& x : tan->thr) x /= (double)p_survive;
             throughput = throughput / p_survive;
             return true;
         };
@@ -1214,6 +1389,7 @@ struct Tracer {
             float p_survive = spectrum_max(survival);
             if (p_survive <= 0.0f) return false;
             if (rng.next() > p_survive) return false;
+            if (tan) for (double& x : tan->thr) x /= (double)p_survive;
             throughput = throughput / p_survive;
             return true;
         };
@@ -1232,6 +1408,9 @@ struct Tracer {
             return power_heuristic(prev_bsdf_pdf, pe * environment_pdf(r.d));
         };
         int shadow_left_base = P.max_null_crossings;
+        if (tan) tan_reset();
+        std::vector<DW> dw(tan ? kMaxDW : 0);
+        std::vector<std::pair<int, double>> dlog_vis;
 
         for (int bounce = 0; bounce <= N; bounce++) {
             Hit hit;
@@ -1251,9 +1430,36 @@ struct Tracer {
                     const ptr_material& mm = d.materials[med_mat];
                     if (!scatter_live(med_mat)) {
                         // absorbing-only arm (deterministic): weight = exp(-sigma_a t_max)
+                        if (tan) {   // exp(-(1 - a) st t_max)
+                            double st, a;
+                            grey_params(med_mat, st, a);
+                            const Dual w_st = dexp(-(1.0 - a) * Dual{st, 1.0} * (double)t_max);
+                            const Dual w_a = dexp(-(1.0 - Dual{a, 1.0}) * st * (double)t_max);
+                            dw[0] = {slot_k(med_mat, PTR_GRAD_SIGMA_T), {w_st.d, w_st.d, w_st.d}};
+                            dw[1] = {slot_k(med_mat, PTR_GRAD_MEDIUM_ALBEDO), {w_a.d, w_a.d, w_a.d}};
+                            tan_mul(throughput, vexp(-ld3(mm.sigma_a) * t_max), dw.data(), 2);
+                        }
                         throughput = throughput * vexp(-ld3(mm.sigma_a) * t_max);
                     } else {
                         MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
+                        if (tan) {   // free flight with the detached channel-MIS density
+                            double st, a;
+                            grey_params(med_mat, st, a);
+                            const v3 sigma_t = ld3(mm.sigma_a) + ld3(mm.sigma_s);
+                            if (ms.scattered) {   // a st exp(-st t) / pdf
+                                const float pdf = fmaxf_(spectrum_average(sigma_t * vexp(-sigma_t * ms.t)), 1e-20f);
+                                const Dual w_st = a * Dual{st, 1.0} * dexp(-Dual{st, 1.0} * (double)ms.t) / (double)pdf;
+                                const Dual w_a = Dual{a, 1.0} * st * std::exp(-st * (double)ms.t) / (double)pdf;
+                                dw[0] = {slot_k(med_mat, PTR_GRAD_SIGMA_T), {w_st.d, w_st.d, w_st.d}};
+                                dw[1] = {slot_k(med_mat, PTR_GRAD_MEDIUM_ALBEDO), {w_a.d, w_a.d, w_a.d}};
+                                tan_mul(throughput, ms.weight, dw.data(), 2);
+                            } else {              // exp(-st t_max) / P
+                                const float pdf = fmaxf_(spectrum_average(vexp(-sigma_t * t_max)), 1e-20f);
+                                const Dual w_st = dexp(-Dual{st, 1.0} * (double)t_max) / (double)pdf;
+                                dw[0] = {slot_k(med_mat, PTR_GRAD_SIGMA_T), {w_st.d, w_st.d, w_st.d}};
+                                tan_mul(throughput, ms.weight, dw.data(), 1);
+                            }
+                        }
                         throughput = throughput * ms.weight;
                         if (ms.scattered) {
                             if (bounce == N) break;
@@ -1266,11 +1472,23 @@ struct Tracer {
                                 LightSample ls = lighting_sample(p_evt, y0, y1);
                                 if (ls.pdf > 0.0f) {
                                     v3 light_p = p_evt + ls.wi * ls.distance;
-                                    v3 vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings);
+                                    dlog_vis.clear();
+                                    v3 vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings,
+                                                                  tan ? &dlog_vis : nullptr);
                                     if (!spectrum_is_black(vis)) {
                                         float w = 1.0f;
                                         if (mis && !(ls.flags & LIGHT_DELTA))   // hg_pdf = spectrum_average(hg_eval)
                                             w = power_heuristic(ls.pdf, spectrum_average(v3(hg_eval(ls.wi, wo_med, mm.phase_g))));
+                                        if (tan) {   // X = Le p_HG(g) T w / pdf
+                                            const v3 X = ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
+                                            const Dual ph = hg_dual(ls.wi, wo_med, Dual{(double)mm.phase_g, 1.0});
+                                            int n = 0;
+                                            dw[n].k = slot_k(med_mat, PTR_GRAD_HG_G);
+                                            for (int c = 0; c < 3; ++c)
+                                                dw[n].d[c] = (double)ls.radiance[c] * ph.d * (double)vis[c] * (double)w / (double)ls.pdf;
+                                            n = dw_from_dlog(X, dlog_vis, dw, n + 1);
+                                            tan_add(throughput, X, dw.data(), n);
+                                        }
                                         radiance = radiance + throughput * ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
                                     }
                                 }
@@ -1278,6 +1496,12 @@ struct Tracer {
                             // kernel_sample_phase (techniques/kernel/kernel_phase.glsl:7-15)
                             float z0 = rng.next(), z1 = rng.next();
                             ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
+                            if (tan) {   // p_HG(g) / pdf
+                                const Dual ph = hg_dual(ps.wi, wo_med, Dual{(double)mm.phase_g, 1.0});
+                                const double dg = ph.d / (double)ps.pdf;
+                                dw[0] = {slot_k(med_mat, PTR_GRAD_HG_G), {dg, dg, dg}};
+                                tan_mul(throughput, ps.weight, dw.data(), 1);
+                            }
                             throughput = throughput * ps.weight;
                             prev_was_delta = false;
                             prev_bsdf_pdf = ps.pdf;
@@ -1290,6 +1514,7 @@ struct Tracer {
                 }
             }
             if (!boundary) {   // kernel_score_miss (kernel.glsl:11-14)
+                if (tan) tan_add(throughput, w_env() * environment_radiance(r.d), nullptr, 0);
                 radiance = radiance + throughput * w_env() * environment_radiance(r.d);
                 break;
             }
@@ -1307,8 +1532,10 @@ struct Tracer {
             hit_alpha = hit.alpha;
             // kernel_score_emitter_hit (kernel.glsl:16-25)
             int mat_emit = S.material_of(hit.region_to);
-            if (S.material_is_emissive(mat_emit))
+            if (S.material_is_emissive(mat_emit)) {
+                if (tan) tan_add(throughput, w_emitter(hit) * ld3(d.materials[mat_emit].emission), nullptr, 0);
                 radiance = radiance + throughput * w_emitter(hit) * ld3(d.materials[mat_emit].emission);
+            }
             if (bounce == N) break;
             const ptr_material& m = d.materials[mat];
             // light_sample_direct (techniques/light/light.glsl:8-28)
@@ -1319,12 +1546,34 @@ struct Tracer {
                     v3 light_p = hit.p + ls.wi * ls.distance;
                     Ray sr = ray_spawn(hit, ls.wi);
                     sr.d = normalize(light_p - sr.o);
-                    v3 vis = shadow_transmittance(sr, light_p, shadow_left_base - null_crossings);
+                    dlog_vis.clear();
+                    v3 vis = shadow_transmittance(sr, light_p, shadow_left_base - null_crossings, tan ? &dlog_vis : nullptr);
                     if (!spectrum_is_black(vis)) {
                         v3 f = surface_eval(m, ls.wi, wo, hit);
                         float cos_i = std::fabs(dot(ls.wi, hit.frame.n));
                         float w = 1.0f;
                         if (mis && !(ls.flags & LIGHT_DELTA)) w = power_heuristic(ls.pdf, surface_pdf(m, ls.wi, wo, hit));
+                        if (tan) {   // X = Le f cos T w / pdf
+                            const v3 X = ls.radiance * f * cos_i * vis * w / ls.pdf;
+                            int n = 0;
+                            if (m.model == PTR_MAT_LAMBERT) {   // f = albedo / pi
+                                for (int c = 0; c < 3; ++c) {
+                                    dw[n].k = slot_k(mat, PTR_GRAD_ALBEDO_R + c);
+                                    dw[n].d[0] = dw[n].d[1] = dw[n].d[2] = 0.0;
+                                    if (f[c] != 0.0f)
+                                        dw[n].d[c] = (double)ls.radiance[c] * (1.0 / PI_D) * (double)cos_i * (double)vis[c] *
+                                                     (double)w / (double)ls.pdf;
+                                    ++n;
+                                }
+                            } else if (m.model == PTR_MAT_GGX && hit_alpha < 0.0f) {   // f = F fs(alpha)
+                                const Dual fs = ggx_fs_dual(ls.wi, wo, hit.frame, Dual{(double)m.alpha, 1.0});
+                                dw[n].k = slot_k(mat, PTR_GRAD_ALPHA);
+                                for (int c = 0; c < 3; ++c) dw[n].d[c] = fs.v > 0.0 ? (double)X[c] * fs.d / fs.v : 0.0;
+                                ++n;
+                            }
+                            n = dw_from_dlog(X, dlog_vis, dw, n);
+                            tan_add(throughput, X, dw.data(), n);
+                        }
                         radiance = radiance + throughput * ls.radiance * f * cos_i * vis * w / ls.pdf;
                     }
                 }
@@ -1334,6 +1583,7 @@ struct Tracer {
             float u0 = rng.next(), u1 = rng.next();
             ISample bs = surface_sample(m, wo, hit, uc, u0, u1);
             if (spectrum_is_black(bs.weight)) break;
+            if (tan) tan_continuation(m, mat, wo, hit, bs, throughput, dw.data());
             throughput = throughput * bs.weight;
             prev_was_delta = (bs.flags & LOBE_DELTA) != 0u;
             prev_bsdf_pdf = bs.pdf;
@@ -1415,6 +1665,63 @@ int oracle_session_render_tile(void* h, const ptr_frame* fr, int x0, int y0, int
                                double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
     OracleSession* s = (OracleSession*)h;
     return render_tile_scene(*s->scene, fr, x0, y0, tw, th, sum, sumsq, samples_out, out_counts, threads);
+}
+
+// Forward-mode reference of the path-replay adjoint (ptr_backward), in float64.  The walk
+// and its random numbers are the plain render's (float32, so every sampling decision is
+// the GPU's); alongside it each path carries d throughput / d theta and d radiance /
+// d theta for every material slot, with the adjoint's detached conventions (Tracer::Tan).
+// Output per pixel of the tile and channel: the sum over the frame's samples of
+// d L / d theta_k, jac[(3 * pixel + c) * K + k], K = PTR_GRAD_SLOTS * n_materials; and
+// the sample sum of L (sum[3 * pixel + c]).  Returns -2 for programs outside the
+// adjoint's model (equiangular medium NEE, spectral colour, chromatic media).
+int oracle_forward_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, const ptr_frame* fr,
+                        int x0, int y0, int tw, int th, double* jac, double* sum, int threads) {
+    if (!sd || !pd || !fr || !jac) return -1;
+    if (pd->equiangular != PTR_EQUIANGULAR_OFF || pd->color != PTR_COLOR_RGB) return -2;
+    for (int i = 0; i < sd->n_materials; ++i) {
+        const ptr_material& m = sd->materials[i];
+        if ((m.flags & PTR_MATF_MEDIUM) && !(m.sigma_a[0] == m.sigma_a[1] && m.sigma_a[0] == m.sigma_a[2] &&
+                                             m.sigma_s[0] == m.sigma_s[1] && m.sigma_s[0] == m.sigma_s[2]))
+            return -2;
+    }
+    Scene S(sd, pd);
+    const int W = fr->width, H = fr->height;
+    const int K = PTR_GRAD_SLOTS * sd->n_materials;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel
+    {
+        Tracer T(S);
+        Tracer::Tan tan;
+        tan.K = K;
+        tan.thr.assign(3 * (size_t)K, 0.0);
+        tan.rad.assign(3 * (size_t)K, 0.0);
+        T.tan = &tan;
+#pragma omp for schedule(dynamic, 1)
+        for (int ty = 0; ty < th; ++ty) {
+            const int y = y0 + ty;
+            for (int tx = 0; tx < tw; ++tx) {
+                const int x = x0 + tx;
+                const size_t pix = (size_t)ty * tw + tx;
+                for (int k = 0; k < fr->spp; ++k) {
+                    T.rng.init((uint32_t)(x + fr->pixel_offset[0]), (uint32_t)(y + fr->pixel_offset[1]),
+                               (uint32_t)(fr->first_sample + k), fr->reset_salt);
+                    float pxf = (float)x + 0.5f + (float)fr->pixel_offset[0];
+                    float pyf = (float)y + 0.5f + (float)fr->pixel_offset[1];
+                    float a0 = T.rng.next(), a1 = T.rng.next();
+                    float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+                    T.rng.next(); T.rng.next();
+                    v3 L = T.transport_trace(camera_ray(fr->camera, W, H, fx, fy));
+                    for (int c = 0; c < 3; ++c) {
+                        if (sum) sum[3 * pix + c] += (double)L[c];
+                        double* jrow = jac + (3 * pix + c) * (size_t)K;
+                        for (int q = 0; q < K; ++q) jrow[q] += tan.rad[3 * (size_t)q + c];
+                    }
+                }
+            }
+        }
+    }
+    return 0;
 }
 
 static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,

@@ -262,6 +262,23 @@ def batch_scenes(n=BATCH_SIZE, seed=0, max_spheres=200):
 
 
 # ------------------------------------------------------------------------- adjoint workload
+def adjoint_box_scene():
+    """The adjoint's check scene: the Cornell box without roulette, with a Lambert sphere,
+    a GGX sphere and a grey scattering medium behind a null interface."""
+    sc, st = cornell(direct="mis", rr_start=None)
+    sc = dict(sc)
+    sc["objects"] = list(sc["objects"][:5]) + [
+        {"type": "sphere", "parameters": {"center": [-0.45, 0.35, -0.3], "radius": 0.35}, "material": "matte"},
+        {"type": "sphere", "parameters": {"center": [0.45, 0.3, 0.2], "radius": 0.3}, "material": "metal"},
+        {"type": "sphere", "parameters": {"center": [0.0, 1.1, -0.3], "radius": 0.3}, "material": "fog"},
+    ]
+    sc["materials"] = dict(sc["materials"], matte={"model": "lambert", "albedo": [0.7, 0.5, 0.3]},
+                           metal={"model": "ggx", "f0": [0.9, 0.6, 0.3], "roughness": 0.5},
+                           fog={"model": "none", "medium": {"sigma_a": [0.3] * 3, "sigma_s": [1.7] * 3,
+                                                            "phase_g": 0.5}})
+    return sc, st
+
+
 def adjoint_scene(seed=0, n_spheres=64, width=256, height=256, spp_primal=64, spp_adjoint=16, max_depth=8):
     """The inverse-rendering workload: the Cornell box's walls and ceiling light with
     `n_spheres` seeded non-overlapping spheres of radius U(0.06, 0.16), each with its own
