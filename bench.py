@@ -272,6 +272,37 @@ def algorithmic_bytes(kernel, c, cw=True):
     return 0
 
 
+def image_error(eng, w, h, spp, salt, budget=5e9):
+    """RMSE of one step's image against an FP64-accumulated reference of the same frame
+    rendered by this build with independent random numbers: 65,536 spp when that is at most
+    `budget` samples, else 4,096 spp (at least 256x the step, so the reference's own noise is
+    under 0.4 % of the step's variance).  Matched RMSE: the measured RMSE equals the one the
+    per-pixel variance predicts (ratio ~1), and ~99.7 % of pixel channels lie within 3 sigma."""
+    import numpy as np
+    ref_spp = 65536 if w * h * 65536 <= budget else 4096
+    chunk = 256
+    eng.pin_reset_salt(0x5EED0000 + salt)
+    eng.reset()
+    for _ in range(ref_spp // chunk):
+        eng.render_frame(w, h, chunk)
+    ref = eng.read_export("radiance").astype(np.float64)
+    ref_var = eng.read_export("variance").astype(np.float64)
+    eng.pin_reset_salt(salt)
+    eng.reset()
+    eng.render_frame(w, h, spp)
+    img = eng.read_export("radiance").astype(np.float64)
+    var = eng.read_export("variance").astype(np.float64)
+    sig2 = var / spp + ref_var / ref_spp
+    d = img - ref
+    rmse = float(np.sqrt(np.mean(d * d)))
+    expected = float(np.sqrt(np.mean(sig2)))
+    live = sig2 > 0
+    within = float(np.mean(np.abs(d[live]) <= 3.0 * np.sqrt(sig2[live]))) if live.any() else 1.0
+    return {"value": rmse, "expected": expected, "ratio": rmse / expected if expected > 0 else None,
+            "within_3sigma": within, "reference_spp": ref_spp, "step_spp": spp,
+            "reference": "FP64-accumulated film of this build, independent random numbers"}
+
+
 def parse_tuning(text):
     """'sort_buckets=16,ray_sort=1' -> {'sort_buckets': 16, 'ray_sort': 1}."""
     out = {}
@@ -304,16 +335,17 @@ def run_ours(args):
         eng.reset()
         eng.render_frame(w, h, spp)
 
-    # the project's autotuner picks the occupant-sorted shading queue and the ray-coherence
-    # queue order for this workload (two steps per candidate, before the warm-up and the
-    # timed region); the default pool capacity and block size stay
+    # the project's autotuner picks the pool capacity (2^24 or 2^25 paths), the
+    # occupant-sorted shading queue and the ray-coherence queue order for this workload
+    # (at least two steps and 0.25 s per candidate, before the warm-up and the timed region)
     from pathtracerglsl_b200 import autotune
     if args.tuning:   # a recorded pick (e.g. for a profiler run of the same configuration)
         pick = dict(autotune.DEFAULTS, **parse_tuning(args.tuning))
         eng.set_tuning(**pick)
         cfg = dict(cfg, tuning=pick, tuning_search="given on the command line")
     else:
-        cands = [dict(capacity=0, block=256, sort_buckets=k, ray_sort=r) for k in (1, 8, 16) for r in (0, 1)]
+        cands = [dict(capacity=c, block=256, sort_buckets=k, ray_sort=r)
+                 for c in (0, 1 << 25) for k in (1, 8, 16) for r in (0, 1)]
         tuned = autotune.tune(eng, step, cands, repeats=2, budget_s=60.0, min_time_s=0.25)
         cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
                    tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
@@ -361,6 +393,9 @@ def run_ours(args):
     e2e = {"value": samples_total / el, "unit": "samples/s",
            "h2d_bytes_per_step": 160, "d2h_bytes_per_step": int(img.nbytes)}
 
+    # ---- image error of a step against a high-spp reference of the same frame (untimed)
+    rmse = image_error(eng, w, h, spp, 1 + rank) if not args.no_rmse else None
+
     # ---- instrumented passes (not part of the timed region): per-kernel-class device
     # time with CUDA events, then the traversal tallies of the counting kernels
     from pathtracerglsl_b200 import abi as _abi
@@ -391,7 +426,7 @@ def run_ours(args):
                 "config": dict(cfg, l2="flushed between steps (256 MiB write, untimed)",
                                parallelism=f"replicas x{world}"),
                 "e2e": e2e, "roofline": roofline, "gpu_launches": launches * args.steps,
-                "clocks": clk,
+                "clocks": clk, "rmse": rmse,
                 "traversal": {k: cnt[k] for k in ("blas_nodes", "triangles", "tlas_nodes", "instances",
                                                    "shadow_blas_nodes", "shadow_triangles", "shadow_tlas_nodes",
                                                    "shadow_instances")},
@@ -671,6 +706,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="", help="skip the autotuner: e.g. sort_buckets=16,ray_sort=1")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0: the workload's own)")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the high-spp image-error reference")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
