@@ -335,6 +335,18 @@ def run_ours(args):
         eng.reset()
         eng.render_frame(w, h, spp)
 
+    # per-scene kernels (ptr_specialize: NVRTC, this scene x strategy), compiled before the
+    # tuning search and the timed region
+    if args.generic:
+        cfg = dict(cfg, kernels="generic (precompiled, table-driven)")
+    else:
+        from pathtracerglsl_b200.engine import EngineError
+        try:
+            secs = eng.specialize()
+            cfg = dict(cfg, kernels=f"specialised for this scene x strategy (NVRTC, {secs:.1f} s compile, untimed)")
+        except EngineError as e:
+            cfg = dict(cfg, kernels=f"generic: specialisation unavailable ({e})")
+
     # the project's autotuner picks the pool capacity (2^24 or 2^25 paths), the
     # occupant-sorted shading queue and the ray-coherence queue order for this workload
     # (at least two steps and 0.25 s per candidate, before the warm-up and the timed region)
@@ -707,6 +719,7 @@ def main():
     ap.add_argument("--tuning", default="", help="skip the autotuner: e.g. sort_buckets=16,ray_sort=1")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0: the workload's own)")
     ap.add_argument("--no-rmse", action="store_true", help="skip the high-spp image-error reference")
+    ap.add_argument("--generic", action="store_true", help="keep the generic kernels (no ptr_specialize)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -20,8 +20,10 @@
 #ifndef PTX_RT_H
 #define PTX_RT_H
 
+#ifndef __CUDACC_RTC__   /* the runtime-compiled kernels (ptr_specialize) define these themselves */
 #include <stddef.h>
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -378,6 +380,20 @@ int ptr_backward(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, co
  * equal the uploaded scene's (PTR_E_INVALID otherwise).  Ordered on the context's stream. */
 int ptr_update_params(ptr_scene* scene, const ptr_material* materials, int n_materials,
                       const ptr_region* regions, int n_regions);
+
+/* ---- per-scene kernels (replaces the reference's per scene x strategy code generation:
+ * Generate emits GLSL for each scene x strategy, src/compiler/generate/Generator.ts:10-91,
+ * compiled by the WebGL driver in RenderExecutor.ts:86-107).
+ * Compiles the program's closest-hit, shading and shadow kernels for this scene with NVRTC
+ * (sm_100a): material models, light kinds, environment kind and region shapes the scene
+ * lacks fold away, and with at most 16 regions the region loops unroll into one arm per
+ * region with its intersection routine fixed, like the reference's generated arms (in
+ * place of the region BVH, which returns the same hits).  Later ptr_render calls of the program with this scene use them (samples
+ * are bit-identical to the generic kernels); the batch, adjoint replay and counting passes
+ * keep the generic kernels.  Modules are cached per occupant census for the process.
+ * seconds_out (may be NULL): compile time (0 for a cached module).  scene = NULL returns
+ * the program to the generic kernels.  PTR_E_UNSUPPORTED when NVRTC cannot be loaded. */
+int ptr_specialize(ptr_program* prog, ptr_scene* scene, double* seconds_out);
 
 /* ---- launch tuning (no counterpart in the reference: WebGL draws one fragment per pixel) ----
  * capacity: paths in flight per wave (0 = the default 2^24); block: threads per block of the

@@ -4,11 +4,48 @@
 // round exactly as written (the reference's GLSL operation order), which keeps the device
 // results comparable sample-for-sample with the CPU restatement.
 #pragma once
+#ifndef __CUDACC_RTC__   // NVRTC builds (ptr_specialize) get the fixed-width types from their prelude
 #include <cstdint>
 #include <cuda_runtime.h>
-#include "../../../include/ptx_rt.h"
+#endif
+#include "ptx_rt.h"
 
 namespace ptx {
+
+// ---- scene specialisation.  The generic library keeps every occupant (all masks on, the
+// region list read from the scene).  A build for one scene x strategy defines the masks of
+// the occupants it holds and, optionally, its region count and region shapes as
+// compile-time lists: absent occupants fold away (smaller kernels, fewer instruction-cache
+// misses in divergent warps) and the region loops unroll into one arm per region with its
+// intersection routine resolved at compile time, like the reference's generated arms.
+#ifndef PTR_SPEC_MATS
+#define PTR_SPEC_MATS 0xFFu     // bit per PTR_MAT_*
+#endif
+#ifndef PTR_SPEC_LIGHTS
+#define PTR_SPEC_LIGHTS 0xFFu   // bit per PTR_LIGHT_*
+#endif
+#ifndef PTR_SPEC_ENVS
+#define PTR_SPEC_ENVS 0xFFu     // bit per PTR_ENV_*
+#endif
+#ifndef PTR_SPEC_SHAPES
+#define PTR_SPEC_SHAPES 0xFFu   // bit per PTR_SHAPE_*
+#endif
+#ifndef PTR_SPEC_NREGIONS
+#define PTR_SPEC_NREGIONS 0     // 1..16: the region count and PTR_SPEC_SHAPE_CODE (the region BVH unused)
+#endif
+__host__ __device__ constexpr bool has_mat(int m) { return ((PTR_SPEC_MATS) >> m) & 1u; }
+__host__ __device__ constexpr bool has_light(int k) { return ((PTR_SPEC_LIGHTS) >> k) & 1u; }
+__host__ __device__ constexpr bool has_env(int k) { return ((PTR_SPEC_ENVS) >> k) & 1u; }
+__host__ __device__ constexpr bool has_shape(int k) { return ((PTR_SPEC_SHAPES) >> k) & 1u; }
+// kind k present, and the only one of the three light kinds / of the surface models
+__host__ __device__ constexpr bool only_light(int k) { return ((PTR_SPEC_LIGHTS) & 7u) == (1u << k); }
+#define PTR_IS_LIGHT(l, K) (has_light(K) && (only_light(K) || (l).kind == (K)))
+#define PTR_IS_MAT(m, M) (has_mat(M) && (m).model == (M))
+#if PTR_SPEC_NREGIONS > 0
+static_assert(PTR_SPEC_NREGIONS <= 16, "the shape code holds 16 regions");
+// region k's PTR_SHAPE_* in bits [4k, 4k + 4) of PTR_SPEC_SHAPE_CODE
+__host__ __device__ constexpr int spec_shape(int k) { return (int)(((unsigned long long)(PTR_SPEC_SHAPE_CODE) >> (4 * k)) & 0xFull); }
+#endif
 
 struct f3 {
     float x, y, z;

@@ -245,9 +245,10 @@ __device__ __forceinline__ f3 env_map_bilinear(const DevScene& S, float2 uv) {
 // rejected on the host).
 template <class Col>
 __device__ __forceinline__ Col env_radiance(const DevScene& S, f3 dir, const Wl& wl) {
-    if (S.env_kind == PTR_ENV_CONSTANT) return Colors<Col>::env_color(S, wl) * S.env_intensity;
+    if (has_env(PTR_ENV_CONSTANT) && S.env_kind == PTR_ENV_CONSTANT) return Colors<Col>::env_color(S, wl) * S.env_intensity;
     if constexpr (sizeof(Col) == sizeof(f3)) {
-        if (S.env_kind == PTR_ENV_IMAGE) return env_map_bilinear(S, equirect_uv(S, dir)) * S.env_intensity;
+        if (has_env(PTR_ENV_IMAGE) && S.env_kind == PTR_ENV_IMAGE)
+            return env_map_bilinear(S, equirect_uv(S, dir)) * S.env_intensity;
     }
     return Col(0.0f);
 }
@@ -309,14 +310,14 @@ __device__ __forceinline__ f3 env_sample_table(const DevScene& S, float x0, floa
     return env_chart_sample(S, i, j, u_frac, v_frac);
 }
 __device__ __forceinline__ float env_pdf(const DevScene& S, f3 dir) {
-    if (S.env_kind != PTR_ENV_IMAGE) return 1.0f / (4.0f * kPi);
+    if (!has_env(PTR_ENV_IMAGE) || S.env_kind != PTR_ENV_IMAGE) return 1.0f / (4.0f * kPi);
     float a = env_uniform_fraction(S);
     return (1.0f - a) * env_table_pdf(S, dir) + a / (4.0f * kPi);
 }
 template <class Col>
 __device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float x0, float x1, const Wl& wl) {
     LightSample<Col> ls;
-    if (S.env_kind == PTR_ENV_IMAGE) {
+    if (has_env(PTR_ENV_IMAGE) && S.env_kind == PTR_ENV_IMAGE) {
         float a = env_uniform_fraction(S);
         if (x0 < a) {
             float y = 1.0f - 2.0f * (x0 / a);
@@ -357,7 +358,7 @@ __device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, f
     ls.radiance = le;
     ls.flags = 0u;
     ls.light_id = -1;
-    if (l.kind == PTR_LIGHT_QUAD) {
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
         f3 q = ld3(l.p) + x0 * ld3(l.p + 3) + x1 * ld3(l.p + 6);
         f3 dd = q - p;
         float d2 = dot(dd, dd);
@@ -368,7 +369,7 @@ __device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, f
         ls.pdf = d2 / (l.p[12] * cos_l);
         return ls;
     }
-    if (l.kind == PTR_LIGHT_SPHERE) {
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_SPHERE)) {
         f3 to_c = ld3(l.p) - p;
         float r = l.p[3];
         float dc2 = dot(to_c, to_c);
@@ -389,6 +390,12 @@ __device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, f
         ls.distance = (dc2 - r * r) / (proj + sqrtf(disc));
         return ls;
     }
+    if (!has_light(PTR_LIGHT_POINT)) {   // unreachable in a build that holds the scene's kinds
+        ls.wi = f3(0.f, 1.f, 0.f);
+        ls.distance = 1.0f;
+        ls.pdf = 0.0f;
+        return ls;
+    }
     f3 dd = ld3(l.p) - p;
     float d2 = dot(dd, dd);
     ls.wi = dd * (1.0f / sqrtf(d2));
@@ -399,13 +406,13 @@ __device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, f
     return ls;
 }
 __device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 light_p, f3 wi) {
-    if (l.kind == PTR_LIGHT_QUAD) {
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
         float cos_l = dot(ld3(l.p + 9), -wi);
         if (cos_l <= 0.0f) return 0.0f;
         f3 dd = light_p - p;
         return dot(dd, dd) / (l.p[12] * cos_l);
     }
-    if (l.kind == PTR_LIGHT_SPHERE) {
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_SPHERE)) {
         f3 to_c = ld3(l.p) - p;
         float dc2 = dot(to_c, to_c);
         float r = l.p[3];

@@ -134,25 +134,31 @@ __device__ __forceinline__ f3 box_normal(f3 p, f3 c, f3 h) {
     return f3(0.f, 0.f, signf(q.z));
 }
 
-// One analytic arm: root of region g along r (false when the shape is not analytic).
-__device__ __forceinline__ bool analytic_root(const ptr_region& g, const Ray& r, float& t) {
-    switch (g.shape) {
-        case PTR_SHAPE_PLANE: return plane_intersect(r, ld3(g.p), g.p[3], t);
-        case PTR_SHAPE_SPHERE: return sphere_intersect(r, ld3(g.p), g.p[3], t);
-        case PTR_SHAPE_QUAD: return quad_intersect(r, ld3(g.p), ld3(g.p + 3), ld3(g.p + 6), ld3(g.p + 9), t);
-        case PTR_SHAPE_BOX: return box_intersect(r, ld3(g.p), ld3(g.p + 3), t);
+// One analytic arm: root of region g (of the given shape) along r (false when the shape
+// is not analytic).
+__device__ __forceinline__ bool analytic_root_shape(int shape, const ptr_region& g, const Ray& r, float& t) {
+    switch (shape) {
+        case PTR_SHAPE_PLANE: return has_shape(PTR_SHAPE_PLANE) && plane_intersect(r, ld3(g.p), g.p[3], t);
+        case PTR_SHAPE_SPHERE: return has_shape(PTR_SHAPE_SPHERE) && sphere_intersect(r, ld3(g.p), g.p[3], t);
+        case PTR_SHAPE_QUAD:
+            return has_shape(PTR_SHAPE_QUAD) && quad_intersect(r, ld3(g.p), ld3(g.p + 3), ld3(g.p + 6), ld3(g.p + 9), t);
+        case PTR_SHAPE_BOX: return has_shape(PTR_SHAPE_BOX) && box_intersect(r, ld3(g.p), ld3(g.p + 3), t);
         default: return false;
     }
 }
+__device__ __forceinline__ bool analytic_root(const ptr_region& g, const Ray& r, float& t) {
+    return analytic_root_shape(g.shape, g, r, t);
+}
 // Signed distance of an analytic solid (thin owners and meshes never claim containment).
-__device__ __forceinline__ float analytic_sdf(const ptr_region& g, f3 p) {
-    switch (g.shape) {
-        case PTR_SHAPE_PLANE: return dot(p, ld3(g.p)) + g.p[3];
-        case PTR_SHAPE_SPHERE: return length(p - ld3(g.p)) - g.p[3];
-        case PTR_SHAPE_BOX: return box_sdf(p, ld3(g.p), ld3(g.p + 3));
+__device__ __forceinline__ float analytic_sdf_shape(int shape, const ptr_region& g, f3 p) {
+    switch (shape) {
+        case PTR_SHAPE_PLANE: return has_shape(PTR_SHAPE_PLANE) ? dot(p, ld3(g.p)) + g.p[3] : 1.0e20f;
+        case PTR_SHAPE_SPHERE: return has_shape(PTR_SHAPE_SPHERE) ? length(p - ld3(g.p)) - g.p[3] : 1.0e20f;
+        case PTR_SHAPE_BOX: return has_shape(PTR_SHAPE_BOX) ? box_sdf(p, ld3(g.p), ld3(g.p + 3)) : 1.0e20f;
         default: return 1.0e20f;
     }
 }
+__device__ __forceinline__ float analytic_sdf(const ptr_region& g, f3 p) { return analytic_sdf_shape(g.shape, g, p); }
 // Outward normal of an analytic arm at its hit point.
 __device__ __forceinline__ f3 analytic_normal(const ptr_region& g, f3 p) {
     switch (g.shape) {

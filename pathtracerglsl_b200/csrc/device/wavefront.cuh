@@ -195,23 +195,31 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
     h.region = -1;
     h.element = 0;
     h.prim = -1;
-    const bool tabled = S.region_bvh != nullptr;
-    const int n = tabled ? S.n_linear : S.n_regions;
-    for (int k = 0; k < n; ++k) {
-        const int i = tabled ? S.linear_regions[k] : k;
-        const ptr_region& g = S.regions[i];
-        if (g.shape >= PTR_SHAPE_MESH) {
+    auto arm = [&](int i, const ptr_region& g, int shape) {
+        if (shape >= PTR_SHAPE_MESH) {
             accel_closest(S, g, i, r, h, w);
-            continue;
+            return;
         }
         float t;
-        if (analytic_root(g, r, t) && t < h.t) {
+        if (analytic_root_shape(shape, g, r, t) && t < h.t) {
             h.t = t;
             h.region = i;
             h.element = 0;
             h.prim = -1;
         }
+    };
+#if PTR_SPEC_NREGIONS > 0
+    constexpr bool tabled = false;
+#pragma unroll
+    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) arm(k, S.regions[k], spec_shape(k));
+#else
+    const bool tabled = S.region_bvh != nullptr;
+    const int n = tabled ? S.n_linear : S.n_regions;
+    for (int k = 0; k < n; ++k) {
+        const int i = tabled ? S.linear_regions[k] : k;
+        arm(i, S.regions[i], S.regions[i].shape);
     }
+#endif
     if (tabled) {
         float tb = h.t;
         walk_binary(S, S.region_bvh, r.o, r.d, tb, [&](int off, int cnt) {
@@ -235,18 +243,24 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
 }
 
 __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float max_dist, Work* w = nullptr) {
+    auto arm = [&](const ptr_region& g, int shape) -> bool {
+        if (shape >= PTR_SHAPE_MESH) return accel_any(S, g, r, max_dist, w);
+        float t;
+        return analytic_root_shape(shape, g, r, t) && t < max_dist;
+    };
+#if PTR_SPEC_NREGIONS > 0
+    constexpr bool tabled = false;
+#pragma unroll
+    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k)
+        if (arm(S.regions[k], spec_shape(k))) return true;
+#else
     const bool tabled = S.region_bvh != nullptr;
     const int n = tabled ? S.n_linear : S.n_regions;
     for (int k = 0; k < n; ++k) {
         const int i = tabled ? S.linear_regions[k] : k;
-        const ptr_region& g = S.regions[i];
-        if (g.shape >= PTR_SHAPE_MESH) {
-            if (accel_any(S, g, r, max_dist, w)) return true;
-            continue;
-        }
-        float t;
-        if (analytic_root(g, r, t) && t < max_dist) return true;
+        if (arm(S.regions[i], S.regions[i].shape)) return true;
     }
+#endif
     if (tabled) {
         return walk_binary(S, S.region_bvh, r.o, r.d, max_dist, [&](int off, int cnt) {
             for (int j = off; j < off + cnt; ++j) {
@@ -264,14 +278,22 @@ __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float
 __device__ __forceinline__ int scene_region_at(const DevScene& S, f3 p) {
     int region = -1;
     float best = -1.0e20f;
+    auto arm = [&](int i, const ptr_region& g, int shape) {
+        float d = shape == PTR_SHAPE_INSTANCES ? accel_region_sdf(S, g, p) : analytic_sdf_shape(shape, g, p);
+        if (d < 0.0f && (d > best || (d == best && i < region))) { best = d; region = i; }
+    };
+#if PTR_SPEC_NREGIONS > 0
+    constexpr bool tabled = false;
+#pragma unroll
+    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) arm(k, S.regions[k], spec_shape(k));
+#else
     const bool tabled = S.region_bvh != nullptr;
     const int n = tabled ? S.n_linear : S.n_regions;
     for (int k = 0; k < n; ++k) {
         const int i = tabled ? S.linear_regions[k] : k;
-        const ptr_region& g = S.regions[i];
-        float d = g.shape == PTR_SHAPE_INSTANCES ? accel_region_sdf(S, g, p) : analytic_sdf(g, p);
-        if (d < 0.0f && (d > best || (d == best && i < region))) { best = d; region = i; }
+        arm(i, S.regions[i], S.regions[i].shape);
     }
+#endif
     if (tabled) {
         int stack[kBvhStack];
         int ptr = 0;
@@ -1007,7 +1029,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             done = true;
                         } else {
                             const float alpha = hit.alpha >= 0.0f ? hit.alpha : m.alpha;
-                            const bool nondelta = m.model == PTR_MAT_LAMBERT || m.model == PTR_MAT_GGX;
+                            const bool nondelta = PTR_IS_MAT(m, PTR_MAT_LAMBERT) || PTR_IS_MAT(m, PTR_MAT_GGX);
+                            // of the two non-delta models, Lambert (folded when the build holds one only)
+                            const bool lam = has_mat(PTR_MAT_LAMBERT) && (!has_mat(PTR_MAT_GGX) || m.model == PTR_MAT_LAMBERT);
                             // light_sample_direct (light.glsl:8-28)
                             if (nee && nondelta) {
                                 float y0 = rng.next();
@@ -1017,13 +1041,12 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
                                     sr.d = normalize(light_p - sr.o);
-                                    Col f = m.model == PTR_MAT_LAMBERT ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
-                                                                       : ggx_eval(ls.wi, wo, hit, CM::f0(S, mat, wl), alpha);
+                                    Col f = lam ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
+                                                : ggx_eval(ls.wi, wo, hit, CM::f0(S, mat, wl), alpha);
                                     float cos_i = fabsf(dot(ls.wi, hit.frame.n));
                                     float w = 1.0f;
                                     if (mis && !(ls.flags & kLightDelta)) {
-                                        float bp = m.model == PTR_MAT_LAMBERT ? lambert_pdf(ls.wi, wo, hit)
-                                                                              : ggx_pdf(ls.wi, wo, hit, alpha);
+                                        float bp = lam ? lambert_pdf(ls.wi, wo, hit) : ggx_pdf(ls.wi, wo, hit, alpha);
                                         w = power_heuristic(ls.pdf, bp);
                                     }
                                     float maxd = length(light_p - sr.o) - kShadowBackoff;
@@ -1050,10 +1073,12 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             float u0 = rng.next();
                             float u1 = rng.next();
                             ISample<Col> bs;
-                            if (m.model == PTR_MAT_LAMBERT) bs = lambert_sample(wo, hit, CM::albedo(S, mat, wl), u0, u1);
-                            else if (m.model == PTR_MAT_GGX) bs = ggx_sample(wo, hit, CM::f0(S, mat, wl), alpha, u0, u1);
-                            else bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), ior_of(S, hit.region_from),
-                                                        ior_of(S, hit.region_to), uc);
+                            if (PTR_IS_MAT(m, PTR_MAT_LAMBERT)) bs = lambert_sample(wo, hit, CM::albedo(S, mat, wl), u0, u1);
+                            else if (PTR_IS_MAT(m, PTR_MAT_GGX)) bs = ggx_sample(wo, hit, CM::f0(S, mat, wl), alpha, u0, u1);
+                            else if (has_mat(PTR_MAT_DIELECTRIC) || has_mat(PTR_MAT_MIRROR) || has_mat(PTR_MAT_NONE))
+                                bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), ior_of(S, hit.region_from),
+                                                       ior_of(S, hit.region_to), uc);
+                            else bs.weight = Col(0.0f);   // unreachable in a build that holds the scene's models
                             if (spectrum_is_black(bs.weight)) {
                                 done = true;
                             } else {

@@ -19,6 +19,9 @@
 #include <string>
 #include <thread>
 #include <vector>
+#include <atomic>
+#include <string>
+#include <dlfcn.h>
 
 #include "device/wavefront.cuh"
 #include "host/accel_build.h"
@@ -43,6 +46,21 @@ struct ptr_scene {
     int n_lights = 0, n_delta_lights = 0, env_samplable = 0;
     std::vector<ptr_material> h_materials;   // host copies for ptr_update_params / ptr_backward
     std::vector<ptr_region> h_regions;
+    // identity and occupant census for ptr_specialize: material models, light kinds,
+    // environment kind and region shapes present (bit per PTR_* value); with at most 16
+    // regions, their count and shapes (4 bits each)
+    uint64_t id = 0;
+    unsigned spec_mats = 0, spec_lights = 0, spec_envs = 0, spec_shapes = 0;
+    int spec_nregions = 0;
+    unsigned long long spec_shape_code = 0;
+};
+
+// Kernels of one program compiled for one scene (ptr_specialize).
+struct SpecKernels {
+    uint64_t scene_id = 0;
+    const void* closest = nullptr;
+    const void* shade = nullptr;
+    const void* shadow = nullptr;
 };
 
 struct ptr_program {
@@ -62,6 +80,7 @@ struct ptr_program {
     // graph cache
     cudaGraphExec_t graph = nullptr;
     const ptr_scene* graph_scene = nullptr;
+    uint64_t graph_scene_id = 0;
     int graph_w = 0, graph_h = 0, graph_iters = 0;
     ptr_tuning graph_tune{};
     float* graph_samples = nullptr;
@@ -73,6 +92,9 @@ struct ptr_program {
     int profile_next = 0;
     float prof_ms[PTR_PROFILE_CLASSES] = {};
     int prof_launches[PTR_PROFILE_CLASSES] = {};
+    // per-scene kernels (ptr_specialize), used while rendering that scene
+    SpecKernels spec{};
+    const void* graph_spec = nullptr;
     // adjoint
     float* adj_dl = nullptr;          // W*H*3 adjoint image
     size_t adj_dl_n = 0;
@@ -148,6 +170,16 @@ struct Launcher {
         if (count) ++*count;
     }
     void count_raw(int n) const { if (!dry && count) *count += n; }
+    // a kernel handle of a runtime-compiled library (ptr_specialize); the arguments must
+    // have the kernel's parameter types
+    template <class... A>
+    void raw(const void* kern, size_t smem, A... args) const {
+        const int g = resident_grid(kern, block, smem, n_sm);
+        if (dry) return;
+        void* argv[] = {(void*)&args...};
+        cudaLaunchKernel(kern, dim3((unsigned)g), dim3((unsigned)block), argv, smem, st);
+        if (count) ++*count;
+    }
 };
 
 void free_pool(ptr_program* p) {
@@ -292,6 +324,8 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     pool.ray_sort = tuning_of(p).ray_sort;
     ProfRec* r = mark(0);
     const BatchTables nob{};
+    // this scene's compiled kernels (ptr_specialize); the counting pass keeps the generic ones
+    const SpecKernels* sk = (p->spec.scene_id == s->id && p->spec.shade) ? &p->spec : nullptr;
     L(k_generate<false, SPECTRAL>, 0, S, pool, p->fp_dev, AdjParams{});
     done(r);
     for (int it = 0; it < iters; ++it) {
@@ -300,6 +334,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         pi.ray_in = pool.ray_sort && it > 0;
         r = mark(1);
         if (S.work) L(k_closest<true, false>, 0, S, pi, in, nob);
+        else if (sk) L.raw(sk->closest, 0, S, pi, in, nob);
         else L(k_closest<false, false>, 0, S, pi, in, nob);
         done(r);
         if (pool.sort_buckets > 1) {   // occupant-sorted shading queue
@@ -309,7 +344,8 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         }
         const bool media = s->has_media != 0;
         r = mark(2);
-        switch (P.direct * 2 + (media ? 1 : 0)) {
+        if (sk) L.raw(sk->shade, 0, S, pi, P, in, nob, AdjParams{});
+        else switch (P.direct * 2 + (media ? 1 : 0)) {
             case 0: L(k_shade<Col, PTR_DIRECT_NONE, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
             case 1: L(k_shade<Col, PTR_DIRECT_NONE, true, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
             case 2: L(k_shade<Col, PTR_DIRECT_NEE, false, false>, 0, S, pi, P, in, nob, AdjParams{}); break;
@@ -332,6 +368,8 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
                     Sq.work = S.work + 4;   // the shadow queries' own tallies
                     if (media) L(k_shadow<Col, true, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
                     else L(k_shadow<Col, false, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
+                } else if (sk) {
+                    L.raw(sk->shadow, 0, S, pool, P, nob, slot, AdjParams{});
                 } else {
                     if (media) L(k_shadow<Col, true, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
                     else L(k_shadow<Col, false, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
@@ -856,9 +894,10 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     }
     const bool use_graph = std::getenv("PTR_NO_GRAPH") == nullptr && !profiling && !counting;
     if (use_graph) {
-        if (!p->graph || p->graph_scene != s || p->graph_w != f->width || p->graph_h != f->height ||
-            p->graph_iters != iters || p->graph_samples != samples_dev ||
-            std::memcmp(&p->graph_tune, &ctx->tune, sizeof(ptr_tuning)) != 0) {
+        const void* cur_spec = p->spec.scene_id == s->id ? p->spec.shade : nullptr;
+        if (!p->graph || p->graph_scene != s || p->graph_scene_id != s->id || p->graph_w != f->width ||
+            p->graph_h != f->height || p->graph_iters != iters || p->graph_samples != samples_dev ||
+            p->graph_spec != cur_spec || std::memcmp(&p->graph_tune, &ctx->tune, sizeof(ptr_tuning)) != 0) {
             if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
             cudaGraph_t g = nullptr;
             launch_wave(p, s, st, iters, samples_dev, n_sm, nullptr, true, true);   // occupancy queries, outside capture
@@ -870,6 +909,8 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
             cudaGraphDestroy(g);
             if (ce != cudaSuccess) return cuda_fail(ctx, ce, "graph instantiate");
             p->graph_scene = s;
+            p->graph_scene_id = s->id;
+            p->graph_spec = cur_spec;
             p->graph_w = f->width;
             p->graph_h = f->height;
             p->graph_iters = iters;
@@ -899,6 +940,139 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
         p->profile_next = 0;
     }
     p->nsamples += (double)f->spp;
+    return PTR_OK;
+}
+
+
+// ---- per-scene kernels (ptr_specialize) ------------------------------------------------
+// NVRTC, opened at run time so that the library needs neither it nor libcuda to load.
+struct Nvrtc {
+    using Prog = void*;
+    int (*create)(Prog*, const char*, const char*, int, const char* const*, const char* const*) = nullptr;
+    int (*add_name)(Prog, const char*) = nullptr;
+    int (*compile)(Prog, int, const char* const*) = nullptr;
+    int (*log_size)(Prog, size_t*) = nullptr;
+    int (*log)(Prog, char*) = nullptr;
+    int (*lowered)(Prog, const char*, const char**) = nullptr;
+    int (*cubin_size)(Prog, size_t*) = nullptr;
+    int (*cubin)(Prog, char*) = nullptr;
+    int (*destroy)(Prog*) = nullptr;
+    bool ok = false;
+    std::string why;
+};
+Nvrtc& nvrtc() {
+    static Nvrtc n;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* names[] = {std::getenv("PTR_NVRTC_LIB"), "libnvrtc.so.12", "libnvrtc.so",
+                               "/usr/local/cuda/lib64/libnvrtc.so.12"};
+        void* h = nullptr;
+        for (const char* nm : names)
+            if (nm && (h = dlopen(nm, RTLD_NOW | RTLD_LOCAL))) break;
+        if (!h) { n.why = "NVRTC (libnvrtc.so.12) not found"; return; }
+        auto sym = [&](auto& fp, const char* name) { fp = reinterpret_cast<std::remove_reference_t<decltype(fp)>>(dlsym(h, name)); return fp != nullptr; };
+        n.ok = sym(n.create, "nvrtcCreateProgram") && sym(n.add_name, "nvrtcAddNameExpression") &&
+               sym(n.compile, "nvrtcCompileProgram") && sym(n.log_size, "nvrtcGetProgramLogSize") &&
+               sym(n.log, "nvrtcGetProgramLog") && sym(n.lowered, "nvrtcGetLoweredName") &&
+               sym(n.cubin_size, "nvrtcGetCUBINSize") && sym(n.cubin, "nvrtcGetCUBIN") &&
+               sym(n.destroy, "nvrtcDestroyProgram");
+        if (!n.ok) n.why = "NVRTC lacks an entry point this build uses";
+    });
+    return n;
+}
+// The device sources beside the library: <package>/csrc/device and <package>/../include
+// (PTR_DEVICE_SRC / PTR_INCLUDE override).
+std::string lib_dir() {
+    Dl_info info{};
+    if (!dladdr((void*)&nvrtc, &info) || !info.dli_fname) return ".";
+    std::string f = info.dli_fname;
+    size_t k = f.find_last_of('/');
+    return k == std::string::npos ? std::string(".") : f.substr(0, k);
+}
+struct SpecModule { cudaLibrary_t lib = nullptr; const void* closest = nullptr; const void* shade = nullptr; const void* shadow = nullptr; };
+// Compile (or fetch) the closest-hit, shading and shadow kernels of a program for a scene's
+// occupant census.  The key is the option list, so equal scenes share one module.
+int spec_compile(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* sc, SpecModule& out, bool& compiled) {
+    compiled = false;
+    static std::mutex mu;
+    static std::map<std::string, SpecModule> cache;
+    Nvrtc& nv = nvrtc();
+    if (!nv.ok) return fail(ctx, PTR_E_UNSUPPORTED, "ptr_specialize: " + nv.why);
+    const bool spectral = p->desc.color == PTR_COLOR_SPECTRAL;
+    const bool media = sc->has_media != 0;
+    const char* col = spectral ? "ptx::s4" : "ptx::f3";
+    const char* md = media ? "true" : "false";
+    const std::string n_closest = "ptx::k_closest<false, false>";
+    const std::string n_shade = std::string("ptx::k_shade<") + col + ", " + std::to_string(p->desc.direct) + ", " + md +
+                                ", false, false>";
+    const std::string n_shadow = std::string("ptx::k_shadow<") + col + ", " + md + ", false, false, false>";
+    const std::string dir = lib_dir();
+    const char* dev_env = std::getenv("PTR_DEVICE_SRC");
+    const char* inc_env = std::getenv("PTR_INCLUDE");
+    std::vector<std::string> opts = {
+        "-arch=sm_100a", "-std=c++17", "-fmad=false", "-lineinfo",
+        "-default-device",   // the public header's host prototypes, declared only
+        std::string("-I") + (dev_env ? dev_env : dir + "/csrc/device"),
+        std::string("-I") + (inc_env ? inc_env : dir + "/../include"),
+        "-DPTR_SPEC_MATS=" + std::to_string(sc->spec_mats) + "u",
+        "-DPTR_SPEC_LIGHTS=" + std::to_string(sc->spec_lights) + "u",
+        "-DPTR_SPEC_ENVS=" + std::to_string(sc->spec_envs) + "u",
+        "-DPTR_SPEC_SHAPES=" + std::to_string(sc->spec_shapes) + "u",
+        "-DPTR_SPEC_NREGIONS=" + std::to_string(sc->spec_nregions),
+        "-DPTR_SPEC_SHAPE_CODE=" + std::to_string(sc->spec_shape_code) + "ull"};
+    std::string key;
+    for (const auto& o : opts) key += o + "\n";
+    key += n_shade + "\n" + n_shadow;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) { out = it->second; return PTR_OK; }
+    static const char* kSource =
+        "typedef signed char int8_t; typedef unsigned char uint8_t; typedef short int16_t;\n"
+        "typedef unsigned short uint16_t; typedef int int32_t; typedef unsigned int uint32_t;\n"
+        "typedef long long int64_t; typedef unsigned long long uint64_t;\n"
+        "#include \"wavefront.cuh\"\n";
+    Nvrtc::Prog prog = nullptr;
+    if (nv.create(&prog, kSource, "ptr_specialize.cu", 0, nullptr, nullptr) != 0)
+        return fail(ctx, PTR_E_CUDA, "ptr_specialize: nvrtcCreateProgram failed");
+    nv.add_name(prog, n_closest.c_str());
+    nv.add_name(prog, n_shade.c_str());
+    nv.add_name(prog, n_shadow.c_str());
+    std::vector<const char*> argv;
+    for (const auto& o : opts) argv.push_back(o.c_str());
+    const int rc = nv.compile(prog, (int)argv.size(), argv.data());
+    if (rc != 0) {
+        size_t n = 0;
+        nv.log_size(prog, &n);
+        std::string log(n, '\0');
+        if (n) nv.log(prog, &log[0]);
+        nv.destroy(&prog);
+        return fail(ctx, PTR_E_CUDA, "ptr_specialize: NVRTC compile failed:\n" + log.substr(0, 4000));
+    }
+    size_t nbin = 0;
+    nv.cubin_size(prog, &nbin);
+    std::vector<char> bin(nbin);
+    nv.cubin(prog, bin.data());
+    const char *l_closest = nullptr, *l_shade = nullptr, *l_shadow = nullptr;
+    nv.lowered(prog, n_closest.c_str(), &l_closest);
+    nv.lowered(prog, n_shade.c_str(), &l_shade);
+    nv.lowered(prog, n_shadow.c_str(), &l_shadow);
+    const std::string s_closest = l_closest ? l_closest : "", s_shade = l_shade ? l_shade : "",
+                      s_shadow = l_shadow ? l_shadow : "";
+    nv.destroy(&prog);
+    SpecModule m;
+    cudaError_t e = cudaLibraryLoadData(&m.lib, bin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "ptr_specialize: cudaLibraryLoadData");
+    cudaKernel_t kc = nullptr, ks = nullptr, kw = nullptr;
+    if ((e = cudaLibraryGetKernel(&kc, m.lib, s_closest.c_str())) != cudaSuccess ||
+        (e = cudaLibraryGetKernel(&ks, m.lib, s_shade.c_str())) != cudaSuccess ||
+        (e = cudaLibraryGetKernel(&kw, m.lib, s_shadow.c_str())) != cudaSuccess)
+        return cuda_fail(ctx, e, "ptr_specialize: cudaLibraryGetKernel");
+    m.closest = (const void*)kc;
+    m.shade = (const void*)ks;
+    m.shadow = (const void*)kw;
+    cache[key] = m;
+    out = m;
+    compiled = true;
     return PTR_OK;
 }
 
@@ -1045,6 +1219,20 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
                 flat = i;
         }
         s->dev.flat_region = (accel_regions == 1 && !s->dev.region_bvh) ? flat : -1;
+        // occupant census for ptr_specialize
+        static std::atomic<uint64_t> next_id{1};
+        s->id = next_id++;
+        for (int i = 0; i < d->n_materials; ++i) s->spec_mats |= 1u << (d->materials[i].model & 31);
+        for (int i = 0; i < d->n_lights; ++i) s->spec_lights |= 1u << (d->lights[i].kind & 31);
+        s->spec_envs = 1u << (d->env.kind & 31);
+        for (int i = 0; i < d->n_regions; ++i) s->spec_shapes |= 1u << (d->regions[i].shape & 31);
+        // up to 16 regions unroll in region order even where a region BVH was built: the
+        // BVH walk's tie rule (lower region index wins) makes both give the same hits
+        if (d->n_regions > 0 && d->n_regions <= 16) {
+            s->spec_nregions = d->n_regions;
+            for (int i = 0; i < d->n_regions; ++i)
+                s->spec_shape_code |= (unsigned long long)(d->regions[i].shape & 15) << (4 * i);
+        }
     }
     if (rc) {
         ptr_free_scene(s);
@@ -1450,6 +1638,28 @@ int ptr_update_params(ptr_scene* s, const ptr_material* materials, int n_materia
     CK(ctx, cudaStreamSynchronize(st));   // the host arrays may be released on return
     s->h_materials.assign(materials, materials + n_materials);
     if (regions) s->h_regions.assign(regions, regions + n_regions);
+    return PTR_OK;
+}
+
+int ptr_specialize(ptr_program* p, ptr_scene* s, double* seconds_out) {
+    if (!p || !p->ctx) return fail(p ? p->ctx : nullptr, PTR_E_INVALID, "ptr_specialize: null program");
+    ptr_ctx* ctx = p->ctx;
+    if (seconds_out) *seconds_out = 0.0;
+    if (!s) {                                      // back to the generic kernels
+        p->spec = SpecKernels{};
+        return PTR_OK;
+    }
+    if (s->ctx != ctx) return fail(ctx, PTR_E_INVALID, "ptr_specialize: scene belongs to another context");
+    CK(ctx, cudaSetDevice(ctx->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    SpecModule m;
+    bool compiled = false;
+    if (int rc = spec_compile(ctx, p, s, m, compiled)) return rc;
+    p->spec.scene_id = s->id;
+    p->spec.closest = m.closest;
+    p->spec.shade = m.shade;
+    p->spec.shadow = m.shadow;
+    if (seconds_out && compiled) *seconds_out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return PTR_OK;
 }
 

@@ -184,6 +184,16 @@ class CudaEngine:
         self.reset()
 
     # -- launch tuning ---------------------------------------------------------------------
+    def specialize(self, enable=True):
+        """Compile the current renderer's kernels for the registered scene (ptr_specialize:
+        NVRTC, per scene x strategy, cached per occupant census); later renders of this
+        pair use them.  enable=False returns to the generic kernels.  Returns the compile
+        seconds (0 when the module was cached)."""
+        secs = C.c_double(0.0)
+        self._check(self.lib.ptr_specialize(self.programs[self.current], self.scene if enable else None,
+                                            C.byref(secs)))
+        return secs.value
+
     def set_tuning(self, capacity=0, block=256, sort_buckets=1, ray_sort=0):
         """Pool capacity (0 = default), block size (128/256), occupant-sort buckets (1 = off)
         and the ray-coherence queue order (0/1) of every later render on this context
