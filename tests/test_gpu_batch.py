@@ -114,3 +114,21 @@ def test_batch_rejects_mixed_direct_lighting(engine):
             b.render([(16, 16, 1), (16, 16, 1)])
     finally:
         b.close()
+
+
+def test_region_bvh_equals_the_linear_scan(engine, monkeypatch):
+    """The region BVH (forced for 8+ bounded regions) returns the linear scan's hits: same
+    nearest region, and on an exact tie the lower region index, so samples are identical."""
+    sc, st, _ = scenes.batch_scene(7, max_spheres=60)
+    assert len(sc["objects"]) - 5 >= 8
+    r, pk = Compiler().compile(sc, st)
+    out = []
+    for minimum in ("1000000", "8"):
+        monkeypatch.setenv("PTR_REGION_BVH_MIN", minimum)
+        engine.register_scene(pk)
+        engine.load_renderer(r)
+        engine.select_renderer(r.id)
+        engine.pin_reset_salt(6)
+        engine.reset()
+        out.append(engine.render_samples(40, 40, 4))
+    np.testing.assert_array_equal(out[1], out[0])
