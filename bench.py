@@ -241,7 +241,7 @@ def run_reference(args):
 # (dram__bytes_read.sum + dram__bytes_write.sum over the wave's launches / the wave's
 # queries; profiles/k_closest_mesh_full.md, profiles/k_shade_cornell_full.md).  Scaled to a
 # launch of the timed configuration by its queries per launch.
-NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 393.66}
+NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 392.93}
 # the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
 ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
 
