@@ -63,8 +63,9 @@ typedef struct ptr_region {
 #define PTR_MAT_LAMBERT 0
 #define PTR_MAT_DIELECTRIC 1
 #define PTR_MAT_GGX 2
-#define PTR_MAT_MIRROR 3
+#define PTR_MAT_MIRROR 3   /* one delta lobe, Schlick F0 (materials/mirror/mirror.glsl)       */
 #define PTR_MAT_NONE 4 /* null interface: a medium boundary with no optical surface */
+#define PTR_MAT_ROUGH_DIELECTRIC 5 /* two-lobe microfacet dielectric (rough_dielectric.glsl) */
 
 #define PTR_MATF_EMISSIVE 1
 #define PTR_MATF_MEDIUM 2       /* material_has_medium                               */

@@ -50,6 +50,8 @@ def lib():
         _lib.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_mesh_brute.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.oracle_rough_dielectric_eval_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 5
+        _lib.oracle_rough_dielectric_sample_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 7
         _lib.oracle_forward_tile.restype = ctypes.c_int
         _lib.oracle_forward_tile.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 2 + [ctypes.c_int]
     return _lib
@@ -107,6 +109,33 @@ def forward(packed, renderer, width, height, spp, first_sample=0, salt=0, params
     if rc != 0:
         raise RuntimeError(f"oracle_forward_tile failed: {rc}")
     return {"jac": jac / spp, "mean": s / spp}
+
+
+def rough_dielectric_eval(alpha, n_i, n_t, wi, wo, tint=(1.0, 1.0, 1.0)):
+    """The oracle's rough dielectric in its local frame (n = +z): f (n, 3) and pdf (n,) for
+    direction arrays wi, wo (n, 3)."""
+    wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
+    wo = np.ascontiguousarray(np.broadcast_to(np.asarray(wo, np.float32), wi.shape))
+    t = np.ascontiguousarray(tint, np.float32)
+    f = np.zeros(wi.shape, np.float32)
+    pdf = np.zeros(len(wi), np.float32)
+    lib().oracle_rough_dielectric_eval_n(len(wi), alpha, n_i, n_t, t.ctypes.data, wi.ctypes.data, wo.ctypes.data,
+                                         f.ctypes.data, pdf.ctypes.data)
+    return f, pdf
+
+
+def rough_dielectric_sample(alpha, n_i, n_t, wo, u, tint=(1.0, 1.0, 1.0)):
+    """One sample per row of u (n, 3) = (uc, u0, u1): wi (n, 3), weight (n, 3), pdf, flags."""
+    u = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+    wo = np.ascontiguousarray(np.broadcast_to(np.asarray(wo, np.float32), u.shape))
+    t = np.ascontiguousarray(tint, np.float32)
+    wi = np.zeros(u.shape, np.float32)
+    w = np.zeros(u.shape, np.float32)
+    pdf = np.zeros(len(u), np.float32)
+    flags = np.zeros(len(u), np.int32)
+    lib().oracle_rough_dielectric_sample_n(len(u), alpha, n_i, n_t, t.ctypes.data, wo.ctypes.data, u.ctypes.data,
+                                           wi.ctypes.data, w.ctypes.data, pdf.ctypes.data, flags.ctypes.data)
+    return wi, w, pdf, flags
 
 
 def render_tile(packed, renderer, width, height, tile, spp, first_sample=0, salt=0, params=None, threads=0):

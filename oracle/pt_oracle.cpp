@@ -468,7 +468,7 @@ struct Scene {
     bool material_has_medium(int m) const { auto* p = mat(m); return p && (p->flags & PTR_MATF_MEDIUM); }
     bool material_has_nondelta_lobes(int m) const {
         auto* p = mat(m);
-        return p && (p->model == PTR_MAT_LAMBERT || p->model == PTR_MAT_GGX);
+        return p && (p->model == PTR_MAT_LAMBERT || p->model == PTR_MAT_GGX || p->model == PTR_MAT_ROUGH_DIELECTRIC);
     }
 
     // primitive_intersect (features/intersection.ts:801-824, primitiveHitFill :695-715),
@@ -730,6 +730,98 @@ inline float ggx_pdf(v3 wi, v3 wo, const Hit& h, float a) {
     if (wil.z * wol.z <= 0.0f) return 0.0f;
     v3 hh = normalize(wil + wol);
     return mf_G1(wol, a) * mf_D(hh, a) / (4.0f * std::fabs(wol.z));
+}
+
+// mirror (materials/mirror/mirror.glsl): one delta lobe weighted by Schlick Fresnel
+inline ISample mirror_sample(v3 wo, const Hit& h, const ptr_material& m) {
+    v3 n = h.frame.n;
+    float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
+    ISample s;
+    s.wi = normalize(2.0f * cos_i * n - wo);
+    s.weight = schlick_fresnel(ld3(m.f0), cos_i);
+    s.pdf = 0.0f;
+    s.flags = LOBE_REFLECTION | LOBE_DELTA;
+    return s;
+}
+// rough dielectric (materials/rough_dielectric/rough_dielectric.glsl): Walter 2007 two-lobe
+// microfacet BSDF, VNDF sampling, exact Fresnel, eta^2 on the transmission lobe; wo in the
+// frame's upper hemisphere, eta = n_i / n_t, equal indices = delta pass-through
+inline bool rough_half(v3 wil, v3 wol, float eta, v3& m) {
+    float etap = wil.z > 0.0f ? 1.0f : 1.0f / eta;
+    m = wil * etap + wol;
+    if (dot(m, m) <= 0.0f) return false;
+    m = normalize(m);
+    if (m.z < 0.0f) m = -m;
+    return dot(m, wil) * wil.z >= 0.0f && dot(m, wol) * wol.z >= 0.0f;
+}
+inline v3 rough_dielectric_eval_local(v3 wil, v3 wol, const ptr_material& mt, float a, float n_i, float n_t) {
+    if (wol.z <= 0.0f || wil.z == 0.0f) return v3(0.0f);
+    if (n_i == n_t) return v3(0.0f);
+    float eta = n_i / n_t;
+    v3 m;
+    if (!rough_half(wil, wol, eta, m)) return v3(0.0f);
+    float cos_om = clampf(std::fabs(dot(wol, m)), 1e-6f, 1.0f);
+    float F = dielectric_fresnel(cos_om, eta);
+    float DG = mf_D(m, a) * mf_G1(wol, a) * mf_G1(wil, a);
+    if (wil.z > 0.0f) return v3(1.0f) * (DG * F / (4.0f * wil.z * wol.z));
+    float denom = dot(wil, m) + dot(wol, m) * eta;
+    denom *= denom;
+    float ft = DG * (1.0f - F) * std::fabs(dot(wil, m) * dot(wol, m) / (wil.z * wol.z * denom));
+    return ld3(mt.transmittance) * (ft * eta * eta);
+}
+inline float rough_dielectric_pdf_local(v3 wil, v3 wol, float a, float n_i, float n_t) {
+    if (wol.z <= 0.0f || wil.z == 0.0f) return 0.0f;
+    if (n_i == n_t) return 0.0f;
+    float eta = n_i / n_t;
+    v3 m;
+    if (!rough_half(wil, wol, eta, m)) return 0.0f;
+    float cos_om = clampf(std::fabs(dot(wol, m)), 1e-6f, 1.0f);
+    float F = dielectric_fresnel(cos_om, eta);
+    if (wil.z > 0.0f) return F * mf_G1(wol, a) * mf_D(m, a) / (4.0f * wol.z);
+    float denom = dot(wil, m) + dot(wol, m) * eta;
+    denom *= denom;
+    return (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * std::fabs(dot(wil, m)) / denom;
+}
+// the sampled lobe in the local frame (wil); the caller maps it out of the frame
+inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, float a, float n_i, float n_t,
+                                             float uc, float u0, float u1) {
+    ISample s;
+    s.wi = wol;
+    s.weight = v3(0.0f);
+    s.pdf = 0.0f;
+    s.flags = LOBE_REFLECTION;
+    if (wol.z <= 0.0f) return s;
+    float eta = n_i / n_t;
+    if (n_i == n_t) {
+        s.wi = -wol;
+        s.weight = ld3(mt.transmittance);
+        s.flags = LOBE_TRANSMISSION | LOBE_DELTA;
+        return s;
+    }
+    v3 m = mf_sample_vndf(wol, a, u0, u1);
+    float cos_om = clampf(dot(wol, m), 1e-6f, 1.0f);
+    float F = dielectric_fresnel(cos_om, eta);
+    v3 wil;
+    if (uc < F) {
+        v3 i = -wol;
+        wil = i - 2.0f * dot(m, i) * m;
+        if (wil.z <= 0.0f) return s;
+        s.weight = v3(1.0f) * mf_G1(wil, a);
+        s.pdf = F * mf_G1(wol, a) * mf_D(m, a) / (4.0f * wol.z);
+        s.flags = LOBE_REFLECTION;
+    } else {
+        float sin2_t = eta * eta * (1.0f - cos_om * cos_om);
+        float cos_t = std::sqrt(fmaxf_(0.0f, 1.0f - sin2_t));
+        wil = normalize(-eta * wol + (eta * cos_om - cos_t) * m);
+        if (wil.z >= 0.0f) return s;
+        float denom = dot(wil, m) + dot(wol, m) * eta;
+        denom *= denom;
+        s.weight = ld3(mt.transmittance) * (mf_G1(wil, a) * eta * eta);
+        s.pdf = (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * std::fabs(dot(wil, m)) / denom;
+        s.flags = LOBE_TRANSMISSION;
+    }
+    s.wi = wil;
+    return s;
 }
 
 // ---------------------------------------------------------------- media (transport/volume/analytic)
@@ -1144,6 +1236,15 @@ struct Tracer {
     ISample surface_sample(const ptr_material& m, v3 wo, const Hit& h, float uc, float u0, float u1) const {
         if (m.model == PTR_MAT_LAMBERT) return lambert_sample(wo, h, m, uc, u0, u1);
         if (m.model == PTR_MAT_GGX) return ggx_sample(wo, h, m, alpha_of(m), u0, u1);
+        if (m.model == PTR_MAT_MIRROR) return mirror_sample(wo, h, m);
+        if (m.model == PTR_MAT_ROUGH_DIELECTRIC) {
+            ISample s = rough_dielectric_sample_local(mf_to_local(h.frame, wo), m, alpha_of(m), S.ior_of(h.region_from),
+                                                      S.ior_of(h.region_to), uc, u0, u1);
+            if (s.weight.x == 0.0f && s.weight.y == 0.0f && s.weight.z == 0.0f && !(s.flags & LOBE_DELTA)) s.wi = wo;
+            else if (s.flags & LOBE_DELTA) s.wi = -wo;
+            else s.wi = mf_from_local(h.frame, s.wi);
+            return s;
+        }
         // dielectric (materials/dielectric/dielectric.glsl:14-52)
         float n_i = S.ior_of(h.region_from), n_t = S.ior_of(h.region_to);
         float eta = n_i / n_t;
@@ -1170,11 +1271,17 @@ struct Tracer {
     v3 surface_eval(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
         if (m.model == PTR_MAT_LAMBERT) return lambert_eval(wi, wo, h, m);
         if (m.model == PTR_MAT_GGX) return ggx_eval(wi, wo, h, m, alpha_of(m));
+        if (m.model == PTR_MAT_ROUGH_DIELECTRIC)
+            return rough_dielectric_eval_local(mf_to_local(h.frame, wi), mf_to_local(h.frame, wo), m, alpha_of(m),
+                                               S.ior_of(h.region_from), S.ior_of(h.region_to));
         return v3(0.0f);
     }
     float surface_pdf(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
         if (m.model == PTR_MAT_LAMBERT) return lambert_pdf(wi, wo, h);
         if (m.model == PTR_MAT_GGX) return ggx_pdf(wi, wo, h, alpha_of(m));
+        if (m.model == PTR_MAT_ROUGH_DIELECTRIC)
+            return rough_dielectric_pdf_local(mf_to_local(h.frame, wi), mf_to_local(h.frame, wo), alpha_of(m),
+                                              S.ior_of(h.region_from), S.ior_of(h.region_to));
         return 0.0f;
     }
 
@@ -1770,6 +1877,35 @@ static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0
     return 0;
 }
 
+
+// The rough dielectric in its local frame (n = +z, wo in the upper hemisphere), for the
+// BSDF property tests: eval (rgb) and pdf of n (wi, wo) pairs; n samples for n (uc, u0, u1).
+int oracle_rough_dielectric_eval_n(int n, float alpha, float n_i, float n_t, const float* tint, const float* wi,
+                                   const float* wo, float* f_out, float* pdf_out) {
+    ptr_material m{};
+    for (int c = 0; c < 3; ++c) m.transmittance[c] = tint[c];
+    for (int k = 0; k < n; ++k) {
+        v3 wil(wi[3 * k], wi[3 * k + 1], wi[3 * k + 2]), wol(wo[3 * k], wo[3 * k + 1], wo[3 * k + 2]);
+        v3 f = rough_dielectric_eval_local(wil, wol, m, alpha, n_i, n_t);
+        f_out[3 * k] = f.x; f_out[3 * k + 1] = f.y; f_out[3 * k + 2] = f.z;
+        pdf_out[k] = rough_dielectric_pdf_local(wil, wol, alpha, n_i, n_t);
+    }
+    return 0;
+}
+int oracle_rough_dielectric_sample_n(int n, float alpha, float n_i, float n_t, const float* tint, const float* wo,
+                                     const float* u, float* wi_out, float* weight_out, float* pdf_out, int* flags_out) {
+    ptr_material m{};
+    for (int c = 0; c < 3; ++c) m.transmittance[c] = tint[c];
+    for (int k = 0; k < n; ++k) {
+        ISample smp = rough_dielectric_sample_local(v3(wo[3 * k], wo[3 * k + 1], wo[3 * k + 2]), m, alpha, n_i, n_t,
+                                                    u[3 * k], u[3 * k + 1], u[3 * k + 2]);
+        wi_out[3 * k] = smp.wi.x; wi_out[3 * k + 1] = smp.wi.y; wi_out[3 * k + 2] = smp.wi.z;
+        weight_out[3 * k] = smp.weight.x; weight_out[3 * k + 1] = smp.weight.y; weight_out[3 * k + 2] = smp.weight.z;
+        pdf_out[k] = smp.pdf;
+        flags_out[k] = (int)smp.flags;
+    }
+    return 0;
+}
 
 // Nearest-hit queries with the oracle's own acceleration: per ray (o.xyz, d.xyz) the
 // region (-1 = miss), the original triangle index (-1 if not a mesh hit) and t.

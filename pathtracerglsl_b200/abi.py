@@ -17,7 +17,7 @@ PTR_E_DEVICE = -5
 PTR_E_UNSUPPORTED = -6
 
 SHAPE_PLANE, SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_MESH, SHAPE_INSTANCES = range(6)
-MAT_LAMBERT, MAT_DIELECTRIC, MAT_GGX, MAT_MIRROR, MAT_NONE = range(5)
+MAT_LAMBERT, MAT_DIELECTRIC, MAT_GGX, MAT_MIRROR, MAT_NONE, MAT_ROUGH_DIELECTRIC = range(6)
 MATF_EMISSIVE, MATF_MEDIUM, MATF_SCATTERING = 1, 2, 4
 LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT = range(3)
 ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)

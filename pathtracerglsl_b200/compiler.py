@@ -136,7 +136,8 @@ def camera_basis(position, target):
 # The occupant registries this build implements (one row per occupant, like the
 # reference's MATERIAL_MODELS / LIGHT_KINDS / PRIMITIVES registries).
 MATERIAL_MODELS = {"lambert": abi.MAT_LAMBERT, "dielectric": abi.MAT_DIELECTRIC,
-                   "ggx": abi.MAT_GGX, "none": abi.MAT_NONE}
+                   "ggx": abi.MAT_GGX, "mirror": abi.MAT_MIRROR, "rough_dielectric": abi.MAT_ROUGH_DIELECTRIC,
+                   "none": abi.MAT_NONE}
 PRIMITIVES = {"plane": abi.SHAPE_PLANE, "sphere": abi.SHAPE_SPHERE, "quad": abi.SHAPE_QUAD,
               "box": abi.SHAPE_BOX}
 LIGHT_KINDS = {"quad": abi.LIGHT_QUAD, "sphere": abi.LIGHT_SPHERE, "point": abi.LIGHT_POINT}
@@ -637,7 +638,7 @@ class Compiler:
 
     @staticmethod
     def _ior(m, params):
-        if m.get("model") == "dielectric":
+        if m.get("model") in ("dielectric", "rough_dielectric"):   # the region-table ior row
             return float(resolve(m.get("ior"), params, 1.5))
         return 1.0
 

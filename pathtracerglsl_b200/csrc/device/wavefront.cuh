@@ -1029,9 +1029,12 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             done = true;
                         } else {
                             const float alpha = hit.alpha >= 0.0f ? hit.alpha : m.alpha;
-                            const bool nondelta = PTR_IS_MAT(m, PTR_MAT_LAMBERT) || PTR_IS_MAT(m, PTR_MAT_GGX);
-                            // of the two non-delta models, Lambert (folded when the build holds one only)
-                            const bool lam = has_mat(PTR_MAT_LAMBERT) && (!has_mat(PTR_MAT_GGX) || m.model == PTR_MAT_LAMBERT);
+                            const bool rough = PTR_IS_MAT(m, PTR_MAT_ROUGH_DIELECTRIC);
+                            const bool nondelta = PTR_IS_MAT(m, PTR_MAT_LAMBERT) || PTR_IS_MAT(m, PTR_MAT_GGX) || rough;
+                            // of the non-delta models, Lambert (folded when the build holds it alone)
+                            const bool lam = has_mat(PTR_MAT_LAMBERT) &&
+                                             ((!has_mat(PTR_MAT_GGX) && !has_mat(PTR_MAT_ROUGH_DIELECTRIC)) || m.model == PTR_MAT_LAMBERT);
+                            const float n_from = ior_of(S, hit.region_from), n_to = ior_of(S, hit.region_to);
                             // light_sample_direct (light.glsl:8-28)
                             if (nee && nondelta) {
                                 float y0 = rng.next();
@@ -1041,12 +1044,14 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
                                     sr.d = normalize(light_p - sr.o);
-                                    Col f = lam ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
+                                    Col f = rough ? rough_dielectric_eval(ls.wi, wo, hit, CM::tint(S, mat, wl), alpha, n_from, n_to)
+                                          : lam ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
                                                 : ggx_eval(ls.wi, wo, hit, CM::f0(S, mat, wl), alpha);
                                     float cos_i = fabsf(dot(ls.wi, hit.frame.n));
                                     float w = 1.0f;
                                     if (mis && !(ls.flags & kLightDelta)) {
-                                        float bp = lam ? lambert_pdf(ls.wi, wo, hit) : ggx_pdf(ls.wi, wo, hit, alpha);
+                                        float bp = rough ? rough_dielectric_pdf(ls.wi, wo, hit, alpha, n_from, n_to)
+                                                   : lam ? lambert_pdf(ls.wi, wo, hit) : ggx_pdf(ls.wi, wo, hit, alpha);
                                         w = power_heuristic(ls.pdf, bp);
                                     }
                                     float maxd = length(light_p - sr.o) - kShadowBackoff;
@@ -1061,7 +1066,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         if (m.model == PTR_MAT_LAMBERT) {
                                             sh_kind = kGradKindAlbedo;
                                             sh_dnee = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
-                                        } else if (hit.alpha < 0.0f) {
+                                        } else if (m.model == PTR_MAT_GGX && hit.alpha < 0.0f) {
                                             sh_kind = kGradKindAlpha;
                                             sh_dnee = f3(ggx_dlog_alpha(ls.wi, wo, hit, alpha), 0.0f, 0.0f);
                                         }
@@ -1075,9 +1080,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             ISample<Col> bs;
                             if (PTR_IS_MAT(m, PTR_MAT_LAMBERT)) bs = lambert_sample(wo, hit, CM::albedo(S, mat, wl), u0, u1);
                             else if (PTR_IS_MAT(m, PTR_MAT_GGX)) bs = ggx_sample(wo, hit, CM::f0(S, mat, wl), alpha, u0, u1);
-                            else if (has_mat(PTR_MAT_DIELECTRIC) || has_mat(PTR_MAT_MIRROR) || has_mat(PTR_MAT_NONE))
-                                bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), ior_of(S, hit.region_from),
-                                                       ior_of(S, hit.region_to), uc);
+                            else if (rough) bs = rough_dielectric_sample(wo, hit, CM::tint(S, mat, wl), alpha, n_from, n_to, uc, u0, u1);
+                            else if (PTR_IS_MAT(m, PTR_MAT_MIRROR)) bs = mirror_sample(wo, hit, CM::f0(S, mat, wl));
+                            else if (has_mat(PTR_MAT_DIELECTRIC) || has_mat(PTR_MAT_NONE))
+                                bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), n_from, n_to, uc);
                             else bs.weight = Col(0.0f);   // unreachable in a build that holds the scene's models
                             if (spectrum_is_black(bs.weight)) {
                                 done = true;

@@ -55,6 +55,18 @@ def cornell(direct="mis", max_depth=8, rr_start=3):
 CORNELL_SIZE = (256, 256, 64)   # width, height, spp
 
 
+def cornell_rough(direct="mis", roughness=0.3, max_depth=8, rr_start=3):
+    """The Cornell box with the remaining surface occupants: the glass sphere a rough
+    dielectric (IOR 1.5, tinted), the matte sphere a mirror (Schlick F0)."""
+    scene, strategy = cornell(direct, max_depth, rr_start)
+    scene = dict(scene, id="cornell-rough")
+    scene["materials"] = dict(scene["materials"],
+                              matte={"model": "mirror", "f0": [0.95, 0.85, 0.6]},
+                              glass={"model": "rough_dielectric", "ior": 1.5, "roughness": roughness,
+                                     "transmittance": [1.0, 0.95, 0.9]})
+    return scene, strategy
+
+
 def furnace(direct="mis", max_depth=8):
     scene = {
         "id": "furnace-c1",

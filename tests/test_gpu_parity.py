@@ -71,6 +71,15 @@ def test_cornell_config_matches_oracle(engine, oracle_lib, direct):
     compare(engine, oracle_lib, sc, st, 64, 64, 8, {})
 
 
+@pytest.mark.parametrize("direct", ["mis", "nee", "none"])
+@pytest.mark.parametrize("roughness", [0.08, 0.3, 0.7])
+def test_rough_dielectric_and_mirror_match_oracle(engine, oracle_lib, direct, roughness):
+    """The rough dielectric (both lobes, NEE and MIS through the interface) and the mirror
+    occupant against the oracle's restatement, sample for sample."""
+    sc, st = scenes.cornell_rough(direct=direct, roughness=roughness)
+    compare(engine, oracle_lib, sc, st, 64, 64, 8, {})
+
+
 def test_furnace_variant_value(engine, oracle_lib):
     sc, st = scenes.furnace()
     compare(engine, oracle_lib, sc, st, 32, 32, 16, {})

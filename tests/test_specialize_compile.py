@@ -34,6 +34,7 @@ def _code(shapes):
 # (material models, light kinds, environment kinds, region shapes in order, colour, direct, media)
 CENSUS = {
     "cornell": (0b11, 0b1, 0b1, [2, 2, 2, 2, 2, 1, 1, 2], "ptx::f3", 2, "false"),
+    "cornell-rough": (0b101001, 0b1, 0b1, [2, 2, 2, 2, 2, 1, 1, 2], "ptx::f3", 2, "false"),
     "mesh": (0b101, 0b0, 0b100, [0, 5], "ptx::f3", 2, "false"),
     "media-spectral": (0b10011, 0b11, 0b1, [0, 1, 1, 1, 2, 2, 2, 2], "ptx::s4", 1, "true"),
     "many-regions": (0b1, 0b1, 0b10, [2] * 16, "ptx::f3", 2, "false"),
