@@ -86,10 +86,13 @@ typedef struct ptr_material {
     float pad2, pad3;
 } ptr_material;             /* 128 bytes */
 
-/* ---- lights (src/components/lights/{quad,sphere,point}) ---------------------------- */
+/* ---- lights (src/components/lights/{quad,sphere,point,mesh}) ---------------------------- */
 #define PTR_LIGHT_QUAD 0   /* p: corner(3) edge1(3) edge2(3) normal(3) area(1) */
 #define PTR_LIGHT_SPHERE 1 /* p: center(3) radius(1)                            */
 #define PTR_LIGHT_POINT 2  /* p: position(3)     radiance = intensity (W/sr)    */
+#define PTR_LIGHT_MESH 3   /* p: mesh index(1, as float) .. world area(p[12]); one-sided    
+                      emission from the cross(b-a, c-a) side; only from an emissive
+                      mesh object (lights/mesh/mesh.ts), region = that object     */
 
 typedef struct ptr_light {
     int32_t kind;

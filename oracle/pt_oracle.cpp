@@ -226,6 +226,8 @@ inline bool tri_test(v3 ro, v3 rd, v3 a, v3 e1, v3 e2, float& t) {
 // the minimum of the same per-triangle t values whatever the tree.
 struct OMesh {
     std::vector<v3> a, e1, e2;
+    std::vector<v3> pb, pc;            // the second and third vertices (mesh lights)
+    std::vector<float> light_cdf;      // normalised cumulative world area (mesh lights)
     std::vector<float> alpha;
     struct Node { float mn[3], mx[3]; int left, right, start, count; };
     std::vector<Node> nodes;
@@ -241,6 +243,8 @@ struct OMesh {
             const float* p1 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 1];
             const float* p2 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 2];
             a[t] = v3(p0[0], p0[1], p0[2]);
+            pb.push_back(v3(p1[0], p1[1], p1[2]));
+            pc.push_back(v3(p2[0], p2[1], p2[2]));
             e1[t] = v3(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]);
             e2[t] = v3(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]);
             if (md.tri_alpha) alpha[t] = md.tri_alpha[t];
@@ -250,6 +254,27 @@ struct OMesh {
                 cen[3 * (size_t)t + k] = 0.5f * (bmn[3 * (size_t)t + k] + bmx[3 * (size_t)t + k]);
             }
         }
+        // lights/mesh/mesh.ts:69-95 packMeshLight: float64 triangle areas from the float32
+        // world vertices, the normalised running sum rounded to float32, the last entry 1
+        std::vector<double> area(T);
+        double acc = 0.0;
+        for (int t = 0; t < T; ++t) {
+            const float* p0 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t];
+            const float* p1 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 1];
+            const float* p2 = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 2];
+            double u[3], w[3];
+            for (int k = 0; k < 3; ++k) { u[k] = (double)p1[k] - p0[k]; w[k] = (double)p2[k] - p0[k]; }
+            const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+            area[t] = std::sqrt(cx * cx + cy * cy + cz * cz) / 2.0;
+            acc += area[t];
+        }
+        light_cdf.resize(T);
+        double run = 0.0;
+        for (int t = 0; t < T; ++t) {
+            run += area[t];
+            light_cdf[t] = acc > 0.0 ? (float)(run / acc) : (float)((double)(t + 1) / T);
+        }
+        if (T > 0) light_cdf[T - 1] = 1.0f;
         idx.resize(T);
         for (int i = 0; i < T; ++i) idx[i] = i;
         nodes.clear();
@@ -1114,12 +1139,43 @@ struct Tracer {
         return (1.0f - a) * table_pdf(dir) + a / (4.0f * PI);
     }
 
-    // ---- lights (lights/quad/quad.glsl:14-41, sphere/sphere.glsl:21-71, point/point.glsl:11-23)
+    // ---- lights (lights/quad/quad.glsl:14-41, sphere/sphere.glsl:21-71, point/point.glsl:11-23,
+    // mesh/mesh.glsl:18-75)
+    // mesh light point: binary search for the smallest triangle whose cumulative area
+    // exceeds x0, x0 rescaled within its span, the square-root map; n = unit winding normal
+    v3 mesh_light_point(const ptr_light& l, float x0, float x1, v3& n) const {
+        const OMesh& m = S.meshes[(int)l.p[0]];
+        int lo = 0, hi = (int)m.light_cdf.size() - 1;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (m.light_cdf[mid] <= x0) lo = mid + 1;
+            else hi = mid;
+        }
+        float c0 = lo > 0 ? m.light_cdf[lo - 1] : 0.0f;
+        float c1 = m.light_cdf[lo];
+        float xr = clampf((x0 - c0) / fmaxf_(c1 - c0, 1.0e-12f), 0.0f, 0.9999999f);
+        v3 a = m.a[lo], b = m.pb[lo], c = m.pc[lo];
+        float su = std::sqrt(xr);
+        n = normalize(cross(b - a, c - a));
+        return a * (1.0f - su) + b * (su * (1.0f - x1)) + c * (su * x1);
+    }
     LightSample light_sample_one(const ptr_light& l, v3 p, float x0, float x1) const {
         LightSample ls;
         ls.radiance = ld3(l.radiance);
         ls.flags = 0u;
         ls.light_id = -1;
+        if (l.kind == PTR_LIGHT_MESH) {   // radiance without falloff; one-sided
+            v3 n;
+            v3 q = mesh_light_point(l, x0, x1, n);
+            v3 dd = q - p;
+            float d2 = dot(dd, dd);
+            ls.wi = dd * (1.0f / std::sqrt(d2));
+            ls.distance = std::sqrt(d2);
+            float cos_l = dot(n, -ls.wi);
+            if (!(cos_l > 0.0f)) { ls.pdf = 0.0f; return ls; }
+            ls.pdf = d2 / (l.p[12] * cos_l);
+            return ls;
+        }
         if (l.kind == PTR_LIGHT_QUAD) {
             v3 corner = ld3(l.p), e1 = ld3(l.p + 3), e2 = ld3(l.p + 6), nrm = ld3(l.p + 9);
             float area = l.p[12];
@@ -1167,7 +1223,13 @@ struct Tracer {
         ls.flags = LIGHT_DELTA;
         return ls;
     }
-    float light_pdf_one(const ptr_light& l, v3 p, v3 light_p, v3 wi) const {
+    float light_pdf_one(const ptr_light& l, v3 p, v3 light_p, v3 light_n, v3 wi) const {
+        if (l.kind == PTR_LIGHT_MESH) {   // d^2 / (A cos_l) whichever triangle was hit
+            float cos_l = dot(light_n, -wi);
+            if (cos_l <= 0.0f) return 0.0f;
+            v3 dd = light_p - p;
+            return dot(dd, dd) / (l.p[12] * cos_l);
+        }
         if (l.kind == PTR_LIGHT_QUAD) {
             float cos_l = dot(ld3(l.p + 9), -wi);
             if (cos_l <= 0.0f) return 0.0f;
@@ -1227,7 +1289,7 @@ struct Tracer {
         const ptr_light& l = d.lights[lid];
         float sel = d.n_lights == 1 ? 1.0f : l.select_pdf;
         float pe = S.env_select_live ? (1.0f - d.env.select_prob) : 1.0f;
-        return sel * pe * light_pdf_one(l, qp, lh.p, wi);
+        return sel * pe * light_pdf_one(l, qp, lh.p, lh.ng, wi);
     }
 
     // ---- material dispatch (features/materials.ts:902-954)
@@ -1373,6 +1435,9 @@ struct Tracer {
                 pos = ld3(l.p) + y0 * ld3(l.p + 3) + y1 * ld3(l.p + 6);
                 nl = ld3(l.p + 9);
                 pdf_area = 1.0f / l.p[12];
+            } else if (l.kind == PTR_LIGHT_MESH) {
+                pos = mesh_light_point(l, y0, y1, nl);
+                pdf_area = 1.0f / l.p[12];
             } else {
                 float z = 1.0f - 2.0f * y0;
                 float rr = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
@@ -1407,7 +1472,7 @@ struct Tracer {
         float denom;
         if (area) {
             float cos_l = dot(nl, -wi);
-            if (cos_l <= 0.0f) return;
+            if (!(cos_l > 0.0f)) return;
             Le = ld3(l.radiance) * (cos_l / d2);
             denom = pdf_t * (pdf_area * sel);
         } else {

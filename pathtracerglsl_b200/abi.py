@@ -19,7 +19,7 @@ PTR_E_UNSUPPORTED = -6
 SHAPE_PLANE, SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_MESH, SHAPE_INSTANCES = range(6)
 MAT_LAMBERT, MAT_DIELECTRIC, MAT_GGX, MAT_MIRROR, MAT_NONE, MAT_ROUGH_DIELECTRIC = range(6)
 MATF_EMISSIVE, MATF_MEDIUM, MATF_SCATTERING = 1, 2, 4
-LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT = range(3)
+LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT, LIGHT_MESH = range(4)
 ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)
 DIRECT_NONE, DIRECT_NEE, DIRECT_MIS = range(3)
 ACCEL_BVH, ACCEL_CWBVH = range(2)

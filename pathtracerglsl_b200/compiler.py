@@ -299,7 +299,11 @@ class Compiler:
                 bag.error("unknown-model", f"material {name!r}: unknown model {m.get('model')!r} "
                           f"(available: {', '.join(MATERIAL_MODELS)})")
         for i, l in enumerate(scene.get("lights", [])):
-            if l.get("kind") not in LIGHT_KINDS:
+            if l.get("kind") == "mesh":
+                # lights/mesh/mesh.ts validateAuthored: the only route is an emissive mesh object
+                bag.error("unknown-light", f"light {i}: mesh lights are not authored as light records; set "
+                          "`sampleAsLight` (or leave it on) on an emissive material used by a mesh object")
+            elif l.get("kind") not in LIGHT_KINDS:
                 bag.error("unknown-light", f"light {i}: unknown kind {l.get('kind')!r}")
         env = scene.get("environment", {"type": "none"})
         if env.get("type") not in ("none", "constant", "image", "procedural"):
@@ -455,19 +459,33 @@ class Compiler:
                 geom = None
             lights.append((rec, kind, e, geom, l.get("emission", 1.0)))
         for i, o in enumerate(scene.get("objects", [])):
-            if o.get("kind") is not None:
+            if o.get("kind") not in (None, "mesh"):
                 continue
             m = mats_src[o["material"]]
             if m.get("sampleAsLight") is False or m.get("model") != "lambert":
                 continue
             e = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
-            if max(e) <= 0.0 or o["type"] not in ("sphere", "quad"):
+            if max(e) <= 0.0 or (o.get("kind") is None and o["type"] not in ("sphere", "quad")):
                 continue
             rec = abi.Light()
             rec.region = i
             rec.radiance = abi.F4(*(e + [0.0]))
             reg = regions[i]
             pp = o.get("parameters", {})
+            if o.get("kind") == "mesh":
+                # lights/mesh/mesh.ts: one-sided uniform area over the whole mesh; the world
+                # total area (meshWorldArea, float64 over the float32 vertices) is the one
+                # constant of its density and of its power pi * A * Le
+                mesh = meshes[reg.ref]
+                area = _mesh_area(mesh["positions"], mesh["indices"])
+                if not area > 0.0:
+                    continue
+                rec.kind = abi.LIGHT_MESH
+                vals = [float(reg.ref)] + [0.0] * 11 + [area]
+                rec.p = (abi.C.c_float * 16)(*vals)
+                geom = area
+                lights.append((rec, "mesh", e, geom, m.get("emission")))
+                continue
             if o["type"] == "sphere":
                 rec.kind = abi.LIGHT_SPHERE
                 rec.p = (abi.C.c_float * 16)(*(list(reg.p[0:4])))
@@ -794,12 +812,24 @@ def build_env_importance(table):
     return np.ascontiguousarray(cond), np.ascontiguousarray(marg), total
 
 
+def _mesh_area(positions, indices):
+    """World surface area of a triangle mesh in float64 from its float32 vertices
+    (lights/mesh/mesh.ts:52-62 meshWorldArea; mesh objects carry world positions)."""
+    p = np.asarray(positions, np.float32).reshape(-1, 3).astype(np.float64)
+    t = np.asarray(indices, np.int64).reshape(-1, 3)
+    u = p[t[:, 1]] - p[t[:, 0]]
+    v = p[t[:, 2]] - p[t[:, 0]]
+    c = np.cross(u, v)
+    a = np.sqrt(c[:, 0] * c[:, 0] + c[:, 1] * c[:, 1] + c[:, 2] * c[:, 2]) / 2.0
+    return float(np.cumsum(a)[-1]) if len(a) else 0.0   # the sequential float64 sum
+
+
 def _light_power(kind, e, geom):
     """Emitted power for the selection CDF, from the authored float64 values like the
     kind descriptors (lights/quad/quad.ts:46 pi*A*Le, sphere.ts:24 pi*4*pi*r^2*Le,
-    point.ts:24 4*pi*I; radiantScalar = channel mean)."""
+    point.ts:24 4*pi*I, mesh.ts:34-36 pi*A_total*Le; radiantScalar = channel mean)."""
     mean = (e[0] + e[1] + e[2]) / 3.0
-    if kind == abi.LIGHT_QUAD:
+    if kind in (abi.LIGHT_QUAD, abi.LIGHT_MESH):   # lights/mesh/mesh.ts:34-36: pi*A_total*Le
         return max(1e-8, math.pi * geom * mean)
     if kind == abi.LIGHT_SPHERE:
         return max(1e-8, math.pi * 4 * math.pi * geom * geom * mean)

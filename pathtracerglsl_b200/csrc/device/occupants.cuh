@@ -448,18 +448,52 @@ __device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float 
     return ls;
 }
 
-// ---- lights: quad (area -> solid angle), sphere (visible cone), point (delta) -----------
-// (lights/quad/quad.glsl:14-41, lights/sphere/sphere.glsl:21-71, lights/point/point.glsl)
+// ---- lights: quad (area -> solid angle), sphere (visible cone), point (delta), mesh ------
+// (lights/quad/quad.glsl:14-41, lights/sphere/sphere.glsl:21-71, lights/point/point.glsl,
+// lights/mesh/mesh.glsl:18-75)
 __device__ __forceinline__ float sphere_omc_max(float r, float dc2) {
     float sin2_max = r * r / dc2;
     return sin2_max / (1.0f + sqrtf(gmax(0.0f, 1.0f - sin2_max)));
 }
+// Mesh light point (lights/mesh/mesh.glsl:18-42): the smallest triangle whose cumulative
+// area exceeds x0 (a zero-area triangle is never picked), x0 rescaled within its span, a
+// uniform point by the square-root map; n is the unit winding normal cross(b-a, c-a),
+// NaN for a triangle degenerate in float32.
+__device__ __forceinline__ f3 mesh_light_point(const DevScene& S, const ptr_light& l, float x0, float x1, f3& n) {
+    const DevMesh& m = S.meshes[(int)l.p[0]];
+    const float* cdf = m.light_cdf;
+    int lo = 0, hi = m.n_tris - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) <= x0) lo = mid + 1;
+        else hi = mid;
+    }
+    float c0 = lo > 0 ? __ldg(cdf + lo - 1) : 0.0f;
+    float c1 = __ldg(cdf + lo);
+    float xr = clampf((x0 - c0) / gmax(c1 - c0, 1.0e-12f), 0.0f, 0.9999999f);
+    f3 a = xyz(__ldg(m.light_tri + 3 * lo)), b = xyz(__ldg(m.light_tri + 3 * lo + 1)), c = xyz(__ldg(m.light_tri + 3 * lo + 2));
+    float su = sqrtf(xr);
+    n = normalize(cross(b - a, c - a));
+    return a * (1.0f - su) + b * (su * (1.0f - x1)) + c * (su * x1);
+}
 template <class Col>
-__device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, float x0, float x1) {
+__device__ LightSample<Col> light_sample_one(const DevScene& S, const ptr_light& l, Col le, f3 p, float x0, float x1) {
     LightSample<Col> ls;
     ls.radiance = le;
     ls.flags = 0u;
     ls.light_id = -1;
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_MESH)) {   // no distance falloff; one-sided
+        f3 n;
+        f3 q = mesh_light_point(S, l, x0, x1, n);
+        f3 dd = q - p;
+        float d2 = dot(dd, dd);
+        ls.wi = dd * (1.0f / sqrtf(d2));
+        ls.distance = sqrtf(d2);
+        float cos_l = dot(n, -ls.wi);
+        if (!(cos_l > 0.0f)) { ls.pdf = 0.0f; return ls; }
+        ls.pdf = d2 / (l.p[12] * cos_l);
+        return ls;
+    }
     if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
         f3 q = ld3(l.p) + x0 * ld3(l.p + 3) + x1 * ld3(l.p + 6);
         f3 dd = q - p;
@@ -507,7 +541,15 @@ __device__ LightSample<Col> light_sample_one(const ptr_light& l, Col le, f3 p, f
     ls.flags = kLightDelta;
     return ls;
 }
-__device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 light_p, f3 wi) {
+// light_n: the hit's geometric normal (mesh lights; mesh.glsl:70-75: uniform area over the
+// whole mesh makes the density d^2 / (A cos_l) whichever triangle was hit)
+__device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 light_p, f3 light_n, f3 wi) {
+    if (PTR_IS_LIGHT(l, PTR_LIGHT_MESH)) {
+        float cos_l = dot(light_n, -wi);
+        if (cos_l <= 0.0f) return 0.0f;
+        f3 dd = light_p - p;
+        return dot(dd, dd) / (l.p[12] * cos_l);
+    }
     if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
         float cos_l = dot(ld3(l.p + 9), -wi);
         if (cos_l <= 0.0f) return 0.0f;
@@ -527,7 +569,7 @@ __device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 ligh
 template <class Col>
 __device__ LightSample<Col> lighting_sample_finite(const DevScene& S, f3 p, float x0, float x1, const Wl& wl) {
     if (S.n_lights == 1) {
-        LightSample<Col> ls = light_sample_one(S.lights[0], Colors<Col>::light(S, 0, wl), p, x0, x1);
+        LightSample<Col> ls = light_sample_one(S, S.lights[0], Colors<Col>::light(S, 0, wl), p, x0, x1);
         ls.light_id = 0;
         return ls;
     }
@@ -537,7 +579,7 @@ __device__ LightSample<Col> lighting_sample_finite(const DevScene& S, f3 p, floa
     float lo = id == 0 ? 0.0f : S.lights[id - 1].select_cdf;
     float sel = S.lights[id].select_pdf;
     float xr = (x0 - lo) / sel;
-    LightSample<Col> ls = light_sample_one(S.lights[id], Colors<Col>::light(S, id, wl), p, clampf(xr, 0.0f, 0.9999999f), x1);
+    LightSample<Col> ls = light_sample_one(S, S.lights[id], Colors<Col>::light(S, id, wl), p, clampf(xr, 0.0f, 0.9999999f), x1);
     ls.light_id = id;
     ls.pdf *= sel;
     return ls;
@@ -563,11 +605,11 @@ __device__ LightSample<Col> lighting_sample(const DevScene& S, f3 p, float x0, f
     ls.pdf *= (1.0f - pe);
     return ls;
 }
-__device__ __forceinline__ float lighting_pdf(const DevScene& S, f3 qp, f3 wi, int lid, f3 light_p) {
+__device__ __forceinline__ float lighting_pdf(const DevScene& S, f3 qp, f3 wi, int lid, f3 light_p, f3 light_n) {
     const ptr_light& l = S.lights[lid];
     float sel = S.n_lights == 1 ? 1.0f : l.select_pdf;
     float pe = S.env_select_live ? (1.0f - S.env_select_prob) : 1.0f;
-    return sel * pe * light_pdf_one(l, qp, light_p, wi);
+    return sel * pe * light_pdf_one(l, qp, light_p, light_n, wi);
 }
 
 // ---- homogeneous media: chromatic channel-MIS free flight (analytic.glsl:9-51) ---------
@@ -600,7 +642,7 @@ __device__ __forceinline__ MediumSample<Col> medium_sample_analytic(Col sigma_a,
 // Kulla & Fajardo 2012): one estimate per medium segment with segment-start throughput.
 // A light is picked by the lighting CDF (lighting_query_delta, features/lighting.ts:303-341);
 // for a delta light its position and intensity are used as in the reference; area lights
-// (quad, sphere: an extension the reference's Validator rejects) first draw a uniform point
+// (quad, sphere, mesh: an extension the reference's Validator rejects) first draw a uniform point
 // on their area and carry Le * cos_l / (d^2 * pdf_area).  The distance t along the segment
 // is uniform in the angle subtended at the light point.  Returns true when a shadow query
 // is due: from p_evt towards light_pos, adding contrib * visibility / denom.
@@ -625,6 +667,9 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat,
         if (l.kind == PTR_LIGHT_QUAD) {
             pos = ld3(l.p) + y0 * ld3(l.p + 3) + y1 * ld3(l.p + 6);
             nl = ld3(l.p + 9);
+            pdf_area = 1.0f / l.p[12];
+        } else if (has_light(PTR_LIGHT_MESH) && l.kind == PTR_LIGHT_MESH) {
+            pos = mesh_light_point(S, l, y0, y1, nl);
             pdf_area = 1.0f / l.p[12];
         } else {
             float z = 1.0f - 2.0f * y0;
@@ -658,7 +703,7 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat,
     Col Le;
     if (area) {
         float cos_l = dot(nl, -q.wi);
-        if (cos_l <= 0.0f) return false;
+        if (!(cos_l > 0.0f)) return false;
         Le = Colors<Col>::light(S, id, wl) * (cos_l / d2);
         q.denom = pdf_t * (pdf_area * sel);
     } else {

@@ -20,6 +20,10 @@ struct DevMesh {
     const float4* bvh;
     const uint4* cwbvh;
     int n_tris, n_nodes, n_cw_nodes, pad;
+    // mesh lights only (NULL otherwise), in the caller's triangle order: the normalised
+    // cumulative world-area CDF (T floats) and the vertices a, b, c (3 float4 per triangle)
+    const float* light_cdf;
+    const float4* light_tri;
 };
 
 // Instanced batch: placements in TLAS leaf order, 2 float4 each — mesh prototypes

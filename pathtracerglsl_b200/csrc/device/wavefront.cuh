@@ -1018,7 +1018,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 int lid = hit.region_to >= 0 ? S.light_of_region[hit.region_to] : -1;
                                 if (lid >= 0 && !prev_delta) {
                                     if (!mis) w = 0.0f;
-                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p));
+                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p, hit.ng));
                                 }
                             }
                             Col e = thr * w * CM::emission(S, mat_emit, wl);

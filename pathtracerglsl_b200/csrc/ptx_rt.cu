@@ -526,6 +526,9 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     };
     std::vector<DevMesh> meshes(d->n_meshes > 0 ? d->n_meshes : 0);
     std::vector<std::vector<double>> root_box(meshes.size());
+    std::vector<char> is_light(meshes.size(), 0);
+    for (int i = 0; i < d->n_lights; ++i)
+        if (d->lights[i].kind == PTR_LIGHT_MESH) is_light[(int)d->lights[i].p[0]] = 1;
     for (int mi = 0; mi < d->n_meshes; ++mi) {
         const ptr_mesh_desc& md = d->meshes[mi];
         if (md.n_triangles <= 0 || md.n_vertices <= 0 || !md.positions || !md.indices)
@@ -577,6 +580,40 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
         m.bvh = p4;
         if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wide.nodes.data(), 5 * (size_t)wide.node_count, &u4))) return rc;
         m.cwbvh = u4;
+        m.light_cdf = nullptr;
+        m.light_tri = nullptr;
+        if (is_light[mi]) {
+            // lights/mesh/mesh.ts packMeshLight: float64 world areas from the float32
+            // vertices, the normalised running sum rounded to float32, the last entry 1
+            std::vector<double> area(T);
+            double acc = 0.0;
+            std::vector<float4> lt(3 * (size_t)T);
+            for (int t = 0; t < T; ++t) {
+                const float* a = md.positions + 3 * (size_t)md.indices[3 * (size_t)t];
+                const float* b = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 1];
+                const float* c = md.positions + 3 * (size_t)md.indices[3 * (size_t)t + 2];
+                const double ux = (double)b[0] - a[0], uy = (double)b[1] - a[1], uz = (double)b[2] - a[2];
+                const double vx = (double)c[0] - a[0], vy = (double)c[1] - a[1], vz = (double)c[2] - a[2];
+                const double cx = uy * vz - uz * vy, cy = uz * vx - ux * vz, cz = ux * vy - uy * vx;
+                area[t] = std::sqrt(cx * cx + cy * cy + cz * cz) / 2.0;
+                acc += area[t];
+                lt[3 * (size_t)t] = make_float4(a[0], a[1], a[2], 0.0f);
+                lt[3 * (size_t)t + 1] = make_float4(b[0], b[1], b[2], 0.0f);
+                lt[3 * (size_t)t + 2] = make_float4(c[0], c[1], c[2], 0.0f);
+            }
+            std::vector<float> cdf(T);
+            double run = 0.0;
+            for (int t = 0; t < T; ++t) {
+                run += area[t];
+                cdf[t] = acc > 0.0 ? (float)(run / acc) : (float)((double)(t + 1) / T);
+            }
+            cdf[T - 1] = 1.0f;
+            const float* pf = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, cdf.data(), cdf.size(), &pf))) return rc;
+            m.light_cdf = pf;
+            if ((rc = dev_copy(ctx, s->allocs, lt.data(), lt.size(), &p4))) return rc;
+            m.light_tri = p4;
+        }
         m.n_tris = T;
         m.n_nodes = bin.node_count;
         m.n_cw_nodes = wide.node_count;
@@ -1135,6 +1172,13 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         const ptr_light& l = d->lights[i];
         if (l.region >= d->n_regions) return fail(ctx, PTR_E_INVALID, "scene: light region out of range");
         if (!(l.select_pdf > 0.0f) || !std::isfinite(l.select_pdf)) return fail(ctx, PTR_E_INVALID, "scene: light selection pdf must be positive");
+        if (l.kind < PTR_LIGHT_QUAD || l.kind > PTR_LIGHT_MESH) return fail(ctx, PTR_E_INVALID, "scene: light " + std::to_string(i) + " has an unknown kind");
+        if (l.kind == PTR_LIGHT_MESH) {
+            const int mi = (int)l.p[0];
+            if (l.region < 0 || d->regions[l.region].shape != PTR_SHAPE_MESH || d->regions[l.region].ref != mi ||
+                (float)mi != l.p[0] || !(l.p[12] > 0.0f) || !std::isfinite(l.p[12]))
+                return fail(ctx, PTR_E_INVALID, "scene: mesh light " + std::to_string(i) + " must name its mesh region, its mesh and a positive area");
+        }
     }
     if (d->ambient_material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: ambient material out of range");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PTR_E_CUDA, "cudaSetDevice");

@@ -67,6 +67,32 @@ def cornell_rough(direct="mis", roughness=0.3, max_depth=8, rr_start=3):
     return scene, strategy
 
 
+def cornell_mesh_light(direct="mis", emitter="panel", max_depth=8, rr_start=3):
+    """The Cornell box lit by an emissive mesh object in place of the authored quad light
+    (the mesh light's one route: an emissive Lambert material on a mesh object).
+    ``panel``: the same 0.5x0.5 ceiling panel (radiance 15, emitting downward), fanned into
+    four triangles of unequal area around an off-centre point, so the image equals the
+    quad-lit box's; ``sphere``: an outward-wound level-2 icosphere (320 triangles) of
+    radius 0.15 under the ceiling, radiance 6."""
+    scene, strategy = cornell(direct, max_depth, rr_start)
+    scene = dict(scene, id="cornell-mesh-" + emitter, lights=[])
+    if emitter == "panel":
+        y = 1.99
+        pos = [[0.1, y, -0.05], [-0.25, y, -0.25], [0.25, y, -0.25], [0.25, y, 0.25], [-0.25, y, 0.25]]
+        # (centre, corner i, corner i+1): cross(b - a, c - a) points down (-y)
+        idx = [[0, 1, 2], [0, 2, 3], [0, 3, 4], [0, 4, 1]]
+        obj = {"kind": "mesh", "positions": pos, "indices": idx, "material": "lamp", "closed": False}
+        lamp = {"model": "lambert", "albedo": [0.0, 0.0, 0.0], "emission": 15.0}
+    else:
+        v, f = icosphere(2)
+        v = v * 0.15 + _np.array([0.0, 1.6, 0.0])
+        obj = {"kind": "mesh", "positions": v.tolist(), "indices": f.tolist(), "material": "lamp", "closed": True}
+        lamp = {"model": "lambert", "albedo": [0.0, 0.0, 0.0], "emission": 6.0}
+    scene["objects"] = list(scene["objects"]) + [obj]
+    scene["materials"] = dict(scene["materials"], lamp=lamp)
+    return scene, strategy
+
+
 def furnace(direct="mis", max_depth=8):
     scene = {
         "id": "furnace-c1",

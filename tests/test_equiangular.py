@@ -55,6 +55,20 @@ def area_fog():
     return sc, base, eq
 
 
+def area_fog_mesh():
+    """area_fog with a third light: an emissive level-1 icosphere (80 triangles, radius
+    0.12) — equiangular over a mesh light draws the light point from the area CDF."""
+    sc, base, eq = area_fog()
+    v, f = scenes.icosphere(1)
+    v = v * 0.12 + np.array([0.9, 1.7, -1.2])
+    sc = dict(sc, id="area-fog-mesh",
+              objects=list(sc["objects"]) + [{"kind": "mesh", "positions": v.tolist(), "indices": f.tolist(),
+                                               "material": "lamp", "closed": True}],
+              materials=dict(sc["materials"], lamp={"model": "lambert", "albedo": [0.0, 0.0, 0.0],
+                                                    "emission": [60.0, 50.0, 40.0]}))
+    return sc, base, eq
+
+
 AREA_CAM = {"camera.position": [0, 1.2, 4.5], "camera.target": [0, 1.0, -1], "camera.fov": 0.9}
 
 
@@ -154,12 +168,34 @@ def test_single_scatter_quad_light_exact(oracle_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["haze", "area"])
+@pytest.mark.parametrize("case", ["haze", "area", "area-mesh"])
 def test_equiangular_cuda_matches_oracle(engine, oracle_lib, case):
     from test_gpu_parity import compare
     if case == "haze":
         _, st = haze_strategies()
         compare(engine, oracle_lib, ref_scenes.HAZE, st, 40, 30, 8, HAZE_CAM, salt=5)
-    else:
+    elif case == "area":
         sc, _, st = area_fog()
         compare(engine, oracle_lib, sc, st, 40, 30, 8, AREA_CAM, salt=5)
+    else:
+        sc, _, st = area_fog_mesh()
+        compare(engine, oracle_lib, sc, st, 40, 30, 8, AREA_CAM, salt=5)
+
+
+def test_equiangular_over_a_mesh_light_converges_to_vertex_placement(oracle_lib):
+    """The haze witness's estimator equality with a mesh light among the lights: the
+    equiangular placement (light point from the area CDF) and the at-vertex placement give
+    the same image on the oracle."""
+    sc, base, eq = area_fog_mesh()
+    imgs = []
+    for k, st in enumerate((base, eq)):
+        r, pk = Compiler().compile(sc, st)
+        assert abi.LIGHT_MESH in [abi.Light.from_buffer_copy(bytes(x)).kind for x in pk.lights]
+        imgs.append(oracle_lib.render(pk, r, 24, 18, 256, salt=21 + k, params=AREA_CAM))
+    a, b = imgs
+    ma, mb = a["mean"].mean(), b["mean"].mean()
+    se = np.sqrt(a["var"].mean() / (256 * 24 * 18) + b["var"].mean() / (256 * 24 * 18))
+    assert abs(ma - mb) < 4.0 * se, (ma, mb, se)
+    bl = lambda im: im[:18, :24].reshape(3, 6, 4, 6, 3).mean(axis=(1, 3))
+    z = np.abs(bl(a["mean"]) - bl(b["mean"])) / (np.sqrt((bl(a["var"]) + bl(b["var"])) / (256 * 36)) + 1e-9)
+    assert (z < 3.0).mean() > 0.9, z

@@ -80,6 +80,20 @@ def test_rough_dielectric_and_mirror_match_oracle(engine, oracle_lib, direct, ro
     compare(engine, oracle_lib, sc, st, 64, 64, 8, {})
 
 
+@pytest.mark.parametrize("direct", ["nee", "mis"])
+@pytest.mark.parametrize("emitter", ["panel", "sphere", "degenerate"])
+def test_mesh_lights_match_oracle(engine, oracle_lib, direct, emitter):
+    """Mesh area lights (area CDF pick, square-root map, identity-free emitter-hit density)
+    against the oracle's restatement, sample for sample; 'degenerate' puts a zero-area
+    triangle first in the CDF."""
+    from test_mesh_lights import _degenerate_panel
+    if emitter == "degenerate":
+        sc, st = _degenerate_panel(direct)
+    else:
+        sc, st = scenes.cornell_mesh_light(direct=direct, emitter=emitter)
+    compare(engine, oracle_lib, sc, st, 64, 64, 8, {})
+
+
 def test_furnace_variant_value(engine, oracle_lib):
     sc, st = scenes.furnace()
     compare(engine, oracle_lib, sc, st, 32, 32, 16, {})

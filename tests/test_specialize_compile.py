@@ -36,6 +36,8 @@ CENSUS = {
     "cornell": (0b11, 0b1, 0b1, [2, 2, 2, 2, 2, 1, 1, 2], "ptx::f3", 2, "false"),
     "cornell-rough": (0b101001, 0b1, 0b1, [2, 2, 2, 2, 2, 1, 1, 2], "ptx::f3", 2, "false"),
     "mesh": (0b101, 0b0, 0b100, [0, 5], "ptx::f3", 2, "false"),
+    "cornell-mesh-light": (0b11, 0b1000, 0b1, [2, 2, 2, 2, 2, 1, 1, 4], "ptx::f3", 2, "false"),
+    "fog-mesh-light": (0b10001, 0b1011, 0b1, [0, 0, 1, 4], "ptx::f3", 1, "true"),
     "media-spectral": (0b10011, 0b11, 0b1, [0, 1, 1, 1, 2, 2, 2, 2], "ptx::s4", 1, "true"),
     "many-regions": (0b1, 0b1, 0b10, [2] * 16, "ptx::f3", 2, "false"),
 }
