@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PTR_ABI_VERSION 2
+#define PTR_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------------- */
 #define PTR_OK 0
@@ -96,7 +96,8 @@ typedef struct ptr_material {
 
 typedef struct ptr_light {
     int32_t kind;
-    int32_t region;        /* the hittable region desugared from this light, -1 for delta */
+    int32_t region;        /* the hittable region desugared from this light; -1 for delta
+                              lights and for instance lights (their batch's light_base)   */
     float select_pdf;      /* selection probability among finite lights (power CDF)       */
     float select_cdf;      /* cumulative probability up to and including this light       */
     float radiance[4];
@@ -134,7 +135,8 @@ typedef struct ptr_batch_desc {
     int32_t prototype_shape;   /* PTR_SHAPE_SPHERE or PTR_SHAPE_MESH                     */
     int32_t prototype_ref;     /* mesh index for mesh prototypes                          */
     int32_t n_instances;
-    int32_t pad;
+    int32_t light_base;        /* light-tree selection: instance i (placement order) is light
+                                  light_base + i (a sphere light row); -1 = not lights     */
     float proto[4];            /* sphere prototype: center.xyz, radius                   */
     const float* placements;   /* 8*N: quaternion xyzw (world->local rigid), ts = (t_rigid.xyz, s) */
 } ptr_batch_desc;
@@ -191,6 +193,13 @@ typedef struct ptr_scene_desc {
     int32_t n_batches;
     const ptr_batch_desc* batches;
     const ptr_spectral_desc* spectral;  /* NULL: the scene renders in RGB only             */
+    /* light tree (estimator.lightSelection 'bvh'; accel/light_tree/light_tree.ts), from
+     * ptr_build_light_tree over all n_lights; NULL = the power CDF selects.  Nodes: 8 floats
+     * (min.xyz, phi, max.xyz, link), preorder, left child = node + 1, link >= 0 the right
+     * child, link < 0 a leaf of light -link - 1.  Trails: 2 words per light. */
+    int32_t n_tree_nodes;      /* 2 n_lights - 1, or 0                                    */
+    const float* light_tree;
+    const uint32_t* light_trails;
 } ptr_scene_desc;
 
 /* ---- program (strategy) ---------------------------------------------------------- */
@@ -225,7 +234,9 @@ typedef struct ptr_program_desc {
     float lambda_max;
     int32_t instance_accel;     /* PTR_ACCEL_* of instanced batches' TLAS (estimator.instanceAccel:
                                    'tlas' binary, 'cwbvh' wide; intersection/index.ts:68-159) */
-    int32_t pad[2];
+    int32_t light_tree;         /* estimator.lightSelection 'bvh': the scene's light tree
+                                   selects (stochastic descent, trail-replayed pmf)      */
+    int32_t pad;
 } ptr_program_desc;
 
 /* The per-frame builtins + camera uniforms (Engine.ts:231-258, camera.ts:69-160). */
@@ -327,6 +338,13 @@ int ptr_build_bvh(const double* boxes, int n, int leaf_size, int always_split,
                   float* nodes_out, int nodes_cap, uint32_t* order_out, int* node_count, int* max_depth);
 int ptr_build_cwbvh(const double* boxes, int n, double c_prim,
                     uint32_t* nodes_out, int nodes_cap, uint32_t* order_out, int* node_count, int* max_depth);
+/* The light tree of buildLightTree (src/components/accel/light_tree/light_tree.ts:44-72)
+ * over n lights: boxes 6 doubles each (min.xyz, max.xyz; degenerate boxes allowed),
+ * powers > 0.  Writes 2n - 1 nodes (8 floats each, the ptr_scene_desc.light_tree layout)
+ * and 2 trail words per light (root-to-leaf decisions, LSB first, levels 0-23 and 24-47).
+ * Returns the tree's depth (<= 47), or PTR_E_INVALID. */
+int ptr_build_light_tree(const double* boxes, const double* powers, int32_t n, float* nodes_out,
+                         uint32_t* trails_out);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that order their own work
  * (timing events, cache flushes) with the library's launches. */

@@ -417,6 +417,8 @@ struct Scene {
     const ptr_scene_desc* d;
     const ptr_program_desc* prog;
     std::vector<int> light_of_region;  // region -> light index (light_of), -1 none
+    std::vector<int> batch_light_base; // batch -> light id of its instance 0, -1 none
+    bool tree = false;                 // light-tree selection
     bool env_samplable, env_select_live;
     bool has_media;
 
@@ -475,6 +477,8 @@ struct Scene {
         light_of_region.assign(sd->n_regions, -1);
         for (int i = 0; i < sd->n_lights; ++i)
             if (sd->lights[i].region >= 0) light_of_region[sd->lights[i].region] = i;
+        for (int i = 0; i < sd->n_batches; ++i) batch_light_base.push_back(sd->batches[i].light_base);
+        tree = pd->light_tree != 0 && sd->n_tree_nodes > 0;
         env_samplable = sd->env.kind != PTR_ENV_NONE && sd->env.sample_as_light;
         env_select_live = env_samplable && sd->n_lights > 0;
         has_media = sd->ambient_material >= 0 && (sd->materials[sd->ambient_material].flags & PTR_MATF_MEDIUM);
@@ -1266,13 +1270,95 @@ struct Tracer {
         ls.pdf *= sel;
         return ls;
     }
+    // ---- light-tree selection (accel/light_tree/light_tree.glsl:28-77; the walk pair of
+    // features/lighting.ts:767-824).  Query: receiving point, shading normal (0 at a medium
+    // event), two-sided receiver (rough dielectric: no below-horizon cull).
+    struct Query { v3 p, n; bool two_sided; };
+    static float tree_importance(v3 bmin, v3 bmax, float phi, const Query& q) {
+        v3 c = 0.5f * (bmin + bmax);
+        v3 e = bmax - bmin;
+        v3 dd = c - q.p;
+        float d2raw = dot(dd, dd);
+        float diag2 = 0.25f * dot(e, e);
+        float base = phi / fmaxf_(d2raw, fmaxf_(diag2, 1e-8f));
+        if (dot(q.n, q.n) < 0.5f) return base;
+        v3 far_c(q.n.x >= 0.0f ? bmax.x : bmin.x, q.n.y >= 0.0f ? bmax.y : bmin.y, q.n.z >= 0.0f ? bmax.z : bmin.z);
+        float h = dot(q.n, far_c - q.p);
+        if (q.two_sided) {
+            v3 near_c = bmin + bmax - far_c;
+            h = fmaxf_(h, -dot(q.n, near_c - q.p));
+        } else if (h <= 0.0f) {
+            return 0.0f;
+        }
+        float cos_c = dot(q.n, dd) * (1.0f / std::sqrt(fmaxf_(d2raw, 1e-12f)));
+        if (q.two_sided) cos_c = std::fabs(cos_c);
+        v3 a = q.p - bmin, b = bmax - q.p;
+        v3 dmx(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z));
+        float lo = h * (1.0f / std::sqrt(fmaxf_(dot(dmx, dmx), 1e-12f)));
+        return base * fminf_(1.0f, fmaxf_(cos_c, lo));
+    }
+    // node i: (min.xyz, phi) at 8i, (max.xyz, link) at 8i + 4; p_l of the left child, or
+    // -1 on a dead descent
+    float tree_left(int ni, const Query& q, int& L, int& R) const {
+        const float* T = d.light_tree;
+        L = ni + 1;
+        R = (int)T[8 * (size_t)ni + 7];
+        float iw_l = tree_importance(ld3(T + 8 * (size_t)L), ld3(T + 8 * (size_t)L + 4), T[8 * (size_t)L + 3], q);
+        float iw_r = tree_importance(ld3(T + 8 * (size_t)R), ld3(T + 8 * (size_t)R + 4), T[8 * (size_t)R + 3], q);
+        float isum = iw_l + iw_r;
+        if (!(isum > 0.0f)) return -1.0f;
+        return iw_l / isum;
+    }
+    int tree_pick(const Query& q, float xi, float& pmf) {
+        const float* T = d.light_tree;
+        pmf = 1.0f;
+        int ni = 0;
+        for (int lvl = 0; lvl < 48 && T[8 * (size_t)ni + 7] >= 0.0f; ++lvl) {
+            int L, R;
+            float p_l = tree_left(ni, q, L, R);
+            if (p_l < 0.0f) { pmf = 0.0f; return -1; }
+            if (xi < p_l) { pmf *= p_l; ni = L; }
+            else { pmf *= (1.0f - p_l); ni = R; }
+            xi = rng.next();
+        }
+        if (T[8 * (size_t)ni + 7] >= 0.0f) { pmf = 0.0f; return -1; }
+        return (int)(-T[8 * (size_t)ni + 7] - 1.0f);
+    }
+    float tree_pmf(const Query& q, int light) const {
+        const float* T = d.light_tree;
+        uint32_t tw = d.light_trails[2 * (size_t)light];
+        float pmf = 1.0f;
+        int ni = 0;
+        for (int lvl = 0; lvl < 48 && T[8 * (size_t)ni + 7] >= 0.0f; ++lvl) {
+            if (lvl == 24) tw = d.light_trails[2 * (size_t)light + 1];
+            int L, R;
+            float p_l = tree_left(ni, q, L, R);
+            if (p_l < 0.0f) return 0.0f;
+            if ((tw & 1u) == 0u) { pmf *= p_l; ni = L; }
+            else { pmf *= (1.0f - p_l); ni = R; }
+            tw >>= 1u;
+        }
+        return pmf;
+    }
+    LightSample lighting_sample_tree(const Query& q, float x0, float x1) {
+        LightSample ls;
+        float sel;
+        int id = tree_pick(q, x0, sel);
+        if (id < 0) { ls.pdf = 0.0f; return ls; }
+        float lx = rng.next();
+        ls = light_sample_one(d.lights[id], q.p, lx, x1);
+        ls.light_id = id;
+        ls.pdf *= sel;
+        return ls;
+    }
+
     // lighting_sample: two-stage env-vs-finite (features/lighting.ts generateLightSampling)
-    LightSample lighting_sample(v3 p, float x0, float x1) const {
+    LightSample lighting_sample(const Query& q, float x0, float x1) {
         if (d.n_lights == 0) {
             if (S.env_samplable) return environment_sample(x0, x1);
             LightSample ls; ls.pdf = 0.0f; return ls;
         }
-        if (!S.env_select_live) return lighting_sample_finite(p, x0, x1);
+        if (!S.env_select_live) return S.tree ? lighting_sample_tree(q, x0, x1) : lighting_sample_finite(q.p, x0, x1);
         float pe = d.env.select_prob;
         if (x0 < pe) {
             LightSample ls = environment_sample(clampf(x0 / pe, 0.0f, 0.9999999f), x1);
@@ -1280,16 +1366,25 @@ struct Tracer {
             return ls;
         }
         float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
-        LightSample ls = lighting_sample_finite(p, fx, x1);
+        LightSample ls = S.tree ? lighting_sample_tree(q, fx, x1) : lighting_sample_finite(q.p, fx, x1);
         ls.pdf *= (1.0f - pe);
         return ls;
     }
-    // lighting_pdf (features/lighting.ts:639-693)
-    float lighting_pdf(v3 qp, v3 wi, int lid, const Hit& lh) const {
+    // lighting_pdf (features/lighting.ts:639-693, 903-940): q = the stored selection context
+    float lighting_pdf(const Query& q, v3 wi, int lid, const Hit& lh) const {
         const ptr_light& l = d.lights[lid];
-        float sel = d.n_lights == 1 ? 1.0f : l.select_pdf;
+        float sel = S.tree ? tree_pmf(q, lid) : d.n_lights == 1 ? 1.0f : l.select_pdf;
         float pe = S.env_select_live ? (1.0f - d.env.select_prob) : 1.0f;
-        return sel * pe * light_pdf_one(l, qp, lh.p, lh.ng, wi);
+        return sel * pe * light_pdf_one(l, q.p, lh.p, lh.ng, wi);
+    }
+    // the light of an emitter hit: its region's, or an instance light of its batch
+    int emitter_light(const Hit& hit) const {
+        int lid = S.light_of_region[hit.region_to];
+        if (lid < 0 && hit.region_to == hit.region_owner) {
+            const ptr_region& g = d.regions[hit.region_owner];
+            if (g.shape == PTR_SHAPE_INSTANCES && S.batch_light_base[g.ref] >= 0) lid = S.batch_light_base[g.ref] + hit.element;
+        }
+        return lid;
     }
 
     // ---- material dispatch (features/materials.ts:902-954)
@@ -1540,6 +1635,8 @@ struct Tracer {
         bool prev_was_delta = true;
         float prev_bsdf_pdf = 0.0f;
         v3 prev_qp = ray.o;
+        v3 prev_qn(0.0f);
+        bool prev_q2 = false;
         float eta_scale = 1.0f;
         int current_medium = media ? S.scene_region_at(ray.o) : -1;
         int null_crossings = 0;
@@ -1567,10 +1664,10 @@ struct Tracer {
         };
         auto w_emitter = [&](const Hit& hit) -> float {   // combiner.ts:27-46
             if (!nee) return 1.0f;
-            int lid = hit.region_to >= 0 ? S.light_of_region[hit.region_to] : -1;
+            int lid = hit.region_to >= 0 ? emitter_light(hit) : -1;
             if (lid < 0 || prev_was_delta) return 1.0f;
             if (!mis) return 0.0f;
-            return power_heuristic(prev_bsdf_pdf, lighting_pdf(prev_qp, r.d, lid, hit));
+            return power_heuristic(prev_bsdf_pdf, lighting_pdf(Query{prev_qp, prev_qn, prev_q2}, r.d, lid, hit));
         };
         auto w_env = [&]() -> float {   // combiner.ts:49-65
             if (!(S.env_samplable && nee)) return 1.0f;
@@ -1641,7 +1738,7 @@ struct Tracer {
                             // the equiangular site replaces it (pt.ts:379)
                             if (nee && !P.equiangular) {
                                 float y0 = rng.next(), y1 = rng.next();
-                                LightSample ls = lighting_sample(p_evt, y0, y1);
+                                LightSample ls = lighting_sample(Query{p_evt, v3(0.0f), false}, y0, y1);
                                 if (ls.pdf > 0.0f) {
                                     v3 light_p = p_evt + ls.wi * ls.distance;
                                     dlog_vis.clear();
@@ -1678,6 +1775,8 @@ struct Tracer {
                             prev_was_delta = false;
                             prev_bsdf_pdf = ps.pdf;
                             prev_qp = p_evt;
+                            prev_qn = v3(0.0f);
+                            prev_q2 = false;
                             r = Ray{p_evt, ps.wi};
                             if (!roulette_interior(bounce, medium_survival(med_mat))) break;
                             continue;
@@ -1713,7 +1812,7 @@ struct Tracer {
             // light_sample_direct (techniques/light/light.glsl:8-28)
             if (nee && S.material_has_nondelta_lobes(mat)) {
                 float y0 = rng.next(), y1 = rng.next();
-                LightSample ls = lighting_sample(hit.p, y0, y1);
+                LightSample ls = lighting_sample(Query{hit.p, hit.frame.n, m.model == PTR_MAT_ROUGH_DIELECTRIC}, y0, y1);
                 if (ls.pdf > 0.0f) {
                     v3 light_p = hit.p + ls.wi * ls.distance;
                     Ray sr = ray_spawn(hit, ls.wi);
@@ -1760,6 +1859,8 @@ struct Tracer {
             prev_was_delta = (bs.flags & LOBE_DELTA) != 0u;
             prev_bsdf_pdf = bs.pdf;
             prev_qp = hit.p;
+            prev_qn = hit.frame.n;
+            prev_q2 = m.model == PTR_MAT_ROUGH_DIELECTRIC;
             if (bs.flags & LOBE_TRANSMISSION) {
                 if (media) current_medium = hit.region_to;
                 float rr = S.ior_of(hit.region_to) / S.ior_of(hit.region_from);   // pt.ts:447-455

@@ -29,6 +29,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "ptr_build_cwbvh": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
                                   C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ptr_build_light_tree": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "ptr_render_noalloc": (C.c_int, [C.POINTER(abi.SceneDesc), C.POINTER(abi.ProgramDesc), C.POINTER(abi.Frame),
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "ptr_render_batch": (C.c_int, [C.c_void_p, C.POINTER(abi.BatchJob), C.c_int]),

@@ -6,7 +6,7 @@ their descriptors from these types, so the two consume byte-identical scenes.
 """
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 PTR_OK = 0
 PTR_E_INVALID = -1
@@ -65,7 +65,7 @@ class MeshDesc(C.Structure):
 
 class BatchDesc(C.Structure):
     _fields_ = [("prototype_shape", C.c_int32), ("prototype_ref", C.c_int32),
-                ("n_instances", C.c_int32), ("pad", C.c_int32), ("proto", F4),
+                ("n_instances", C.c_int32), ("light_base", C.c_int32), ("proto", F4),
                 ("placements", C.POINTER(C.c_float))]
 
 
@@ -96,7 +96,9 @@ class SceneDesc(C.Structure):
                 ("ambient_material", C.c_int32), ("env", Env),
                 ("n_meshes", C.c_int32), ("meshes", C.POINTER(MeshDesc)),
                 ("n_batches", C.c_int32), ("batches", C.POINTER(BatchDesc)),
-                ("spectral", C.POINTER(SpectralDesc))]
+                ("spectral", C.POINTER(SpectralDesc)),
+                ("n_tree_nodes", C.c_int32), ("light_tree", C.POINTER(C.c_float)),
+                ("light_trails", C.POINTER(C.c_uint32))]
 
 
 class ProgramDesc(C.Structure):
@@ -105,7 +107,7 @@ class ProgramDesc(C.Structure):
                 ("rr_max_survival", C.c_float), ("scattering", C.c_int32), ("accel", C.c_int32),
                 ("equiangular", C.c_int32), ("color", C.c_int32), ("wavelengths", C.c_int32),
                 ("lambda_min", C.c_float), ("lambda_max", C.c_float), ("instance_accel", C.c_int32),
-                ("pad", C.c_int32 * 2)]
+                ("light_tree", C.c_int32), ("pad", C.c_int32)]
 
 
 class Camera(C.Structure):

@@ -67,6 +67,16 @@ def is_param(v):
     return isinstance(v, dict) and "param" in v
 
 
+def _has_param(v):
+    if is_param(v):
+        return True
+    if isinstance(v, (list, tuple)):
+        return any(_has_param(x) for x in v)
+    if isinstance(v, dict):
+        return any(_has_param(x) for x in v.values())
+    return False
+
+
 def resolve(v, params, default=None):
     """``Value<T>`` -> concrete value: constants as is, ``{param}`` from ``params`` or
     its default (contracts §2.8 in the reference's types.ts:257-275)."""
@@ -163,6 +173,8 @@ class PackedScene:
     region_names: list = field(default_factory=list)
     material_names: list = field(default_factory=list)
     spectral: object = None     # spectral.SpectralTables of spectral strategies, else None
+    light_tree: object = None   # float32 nodes (8 per node) under light-tree selection, else None
+    light_trails: object = None # uint32 trail words (2 per light)
 
     def desc(self):
         """A ``ptr_scene_desc`` pointing into this object's arrays (keep self alive)."""
@@ -207,12 +219,17 @@ class PackedScene:
                 bd.prototype_ref = b.get("prototype_ref", -1)
                 bd.n_instances = len(b["placements"]) // 8
                 bd.proto = abi.F4(*b.get("proto", [0, 0, 0, 0]))
+                bd.light_base = b.get("light_base", -1)
                 bd.placements = b["placements"].ctypes.data_as(abi.C.POINTER(abi.C.c_float))
             d.n_batches = len(self.batches)
             d.batches = self._batch_arr
         if self.spectral is not None:
             self._spec_desc = self.spectral.desc()
             d.spectral = abi.C.pointer(self._spec_desc)
+        if self.light_tree is not None:
+            d.n_tree_nodes = len(self.light_tree) // 8
+            d.light_tree = self.light_tree.ctypes.data_as(abi.C.POINTER(abi.C.c_float))
+            d.light_trails = self.light_trails.ctypes.data_as(abi.C.POINTER(abi.C.c_uint32))
         return d
 
 
@@ -337,6 +354,20 @@ class Compiler:
         vs = est.get("volumeSampling", "analytic")
         if vs not in ("analytic", None):
             bag.error("unsupported", f"volumeSampling {vs!r} is not available in this build")
+        sel = est.get("lightSelection", "power")
+        if sel not in ("power", "uniform", "bvh"):
+            bag.error("invalid-setting", f"estimator.lightSelection {sel!r} (available: power, uniform, bvh)")
+        if sel == "bvh":
+            # Validator.ts:629-665: the tree needs constant emission and keeps equiangular
+            # on the CDF path
+            if est.get("mediumLightSampling", "vertex") == "equiangular":
+                bag.error("unsupported", "estimator.lightSelection 'bvh' with mediumLightSampling 'equiangular' "
+                          "is reserved; use 'vertex'")
+            driven = [l.get("kind") for l in scene.get("lights", []) if _has_param(l.get("emission"))]
+            driven += [n for n, m in mats.items() if _has_param(m.get("emission"))]
+            if driven:
+                bag.error("unsupported", "estimator.lightSelection 'bvh' requires constant light emission "
+                          f"(driven: {', '.join(map(str, driven))}); use 'power'")
         mls = est.get("mediumLightSampling", "vertex")
         if mls not in ("vertex", "equiangular"):
             bag.error("invalid-setting", f"mediumLightSampling {mls!r} (available: vertex, equiangular)")
@@ -498,11 +529,40 @@ class Compiler:
                 geom = area
             lights.append((rec, o["type"], e, geom, m.get("emission")))
 
-        # Selection CDF (features/lighting.ts computeSelectPdf; power per kind from the
-        # descriptors: quad pi*A*Le, sphere pi*4*pi*r^2*Le, point 4*pi*I).
         sel_mode = "power"
+        tree_direct = False
         for st in strategies:
             sel_mode = st.get("estimator", {}).get("lightSelection", "power")
+            tree_direct = st.get("estimator", {}).get("directLighting", "none") != "none"
+        if sel_mode == "bvh" and tree_direct:
+            # instanced emitters (dataTenants.ts batchLightEligible): a sphere-prototype batch
+            # with a constant emissive Lambert material makes every instance a sphere light
+            # of the tree, in placement order from the batch's light_base
+            for i, o in enumerate(scene.get("objects", [])):
+                if o.get("kind") != "instanced":
+                    continue
+                proto = o["prototype"]
+                m = mats_src[proto["material"]]
+                if proto.get("kind") == "mesh" or proto.get("type") != "sphere":
+                    continue
+                if m.get("sampleAsLight") is False or m.get("model") != "lambert":
+                    continue
+                e = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
+                if max(e) <= 0.0:
+                    continue
+                b = batches[regions[i].ref]
+                b["light_base"] = len(lights)
+                cen, rad = _instance_spheres(b["placements"], b["proto"])
+                for k in range(len(rad)):
+                    rec = abi.Light()
+                    rec.kind = abi.LIGHT_SPHERE
+                    rec.region = -1
+                    rec.radiance = abi.F4(*(e + [0.0]))
+                    rec.p = (abi.C.c_float * 16)(float(cen[k, 0]), float(cen[k, 1]), float(cen[k, 2]), float(rad[k]))
+                    lights.append((rec, "sphere", e, float(rad[k]), m.get("emission")))
+
+        # Selection CDF (features/lighting.ts computeSelectPdf; power per kind from the
+        # descriptors: quad pi*A*Le, sphere pi*4*pi*r^2*Le, point 4*pi*I).
         weights = [1.0 if sel_mode == "uniform" else _light_power(rec.kind, e, geom)
                    for rec, kind, e, geom, _raw in lights]
         total = sum(weights)
@@ -516,8 +576,15 @@ class Compiler:
             rec.select_cdf = acc
             light_recs[i] = rec
         light_arr = np.frombuffer(bytes(light_recs), dtype=np.uint8).reshape(max(len(lights), 1), -1)[:len(lights)].copy()
+        tree = trails = None
+        if sel_mode == "bvh" and tree_direct and lights:
+            tree, trails = _light_tree([rec for rec, *_x in lights],
+                                       [_light_power(rec.kind, e, geom) for rec, kind, e, geom, _raw in lights],
+                                       meshes)
 
         env = self._environment(scene.get("environment") or {"type": "none"}, params, scene, lights, bag)
+        if tree is not None and "select_prob" in env:
+            env["select_prob"] = 0.5   # lighting.ts:476-481: the env against the whole tree
         am = scene.get("ambientMedium")
         packed = PackedScene(
             regions=_as_bytes(regions, abi.Region),
@@ -526,6 +593,7 @@ class Compiler:
             ambient_material=mat_index[am] if am is not None else -1,
             env=env, meshes=meshes, batches=batches,
             region_names=region_names, material_names=mat_names,
+            light_tree=tree, light_trails=trails,
         )
         if any(st.get("measurement", {}).get("color", "rgb") == "spectral" for st in strategies):
             packed.spectral = self._spectral_tables(spec_src, [raw for *_x, raw in lights],
@@ -766,6 +834,8 @@ class Compiler:
         prog.wavelengths = abi.WAVELENGTHS_UNIFORM if est.get("wavelengths") == "uniform" else abi.WAVELENGTHS_VISIBLE
         lo, hi = meas.get("wavelengthRange", [360.0, 830.0])
         prog.lambda_min, prog.lambda_max = float(lo), float(hi)
+        prog.light_tree = int(est.get("lightSelection") == "bvh" and prog.direct != abi.DIRECT_NONE
+                              and getattr(data, "light_tree", None) is not None)
         prog.equiangular = abi.EQUIANGULAR_OFF
         if est.get("mediumLightSampling") == "equiangular":
             prog.equiangular = abi.EQUIANGULAR_AREA if est.get("equiangularAreaLights") else abi.EQUIANGULAR_DELTA
@@ -810,6 +880,52 @@ def build_env_importance(table):
     macc = np.cumsum(row_sum)
     marg = (macc / total if total > 0 else np.zeros(H)).astype(np.float32)
     return np.ascontiguousarray(cond), np.ascontiguousarray(marg), total
+
+
+def _instance_spheres(placements, proto):
+    """World centres and radii of a sphere batch's instances, in placement order: the
+    placement record maps world -> rigid frame, so world = rotate(conj(q), s * c - t_rigid)
+    (float64, then float32 like the device's placement records)."""
+    pl = np.asarray(placements, np.float32).reshape(-1, 8).astype(np.float64)
+    q, t, sc = pl[:, 0:4], pl[:, 4:7], pl[:, 7]
+    c = np.asarray(proto[:3], np.float32).astype(np.float64)
+    v = sc[:, None] * c[None, :] - t
+    cq = -q[:, :3]
+    c1 = np.cross(cq, v) + q[:, 3:4] * v
+    c2 = np.cross(cq, c1)
+    cen = (v + 2.0 * c2).astype(np.float32)
+    rad = (sc * float(np.float32(proto[3]))).astype(np.float32)
+    return cen, rad
+
+
+def _light_bounds(rec, meshes):
+    """The tree-leaf box of a light row (light descriptors' treeBounds)."""
+    p = np.asarray(list(rec.p), np.float64)
+    if rec.kind == abi.LIGHT_QUAD:
+        pts = np.array([p[0:3], p[0:3] + p[3:6], p[0:3] + p[6:9], p[0:3] + p[3:6] + p[6:9]])
+        return np.concatenate([pts.min(0), pts.max(0)])
+    if rec.kind == abi.LIGHT_SPHERE:
+        return np.concatenate([p[0:3] - p[3], p[0:3] + p[3]])
+    if rec.kind == abi.LIGHT_MESH:
+        m = meshes[int(p[0])]
+        v = np.asarray(m["positions"], np.float32).reshape(-1, 3)[np.asarray(m["indices"], np.int64)]
+        v = v.reshape(-1, 3).astype(np.float64)
+        return np.concatenate([v.min(0), v.max(0)])
+    return np.concatenate([p[0:3], p[0:3]])
+
+
+def _light_tree(recs, powers, meshes):
+    """Nodes and trails of the light tree over the roster (ptr_build_light_tree)."""
+    from . import _native
+    n = len(recs)
+    boxes = np.ascontiguousarray(np.stack([_light_bounds(r, meshes) for r in recs]), np.float64)
+    pw = np.ascontiguousarray(powers, np.float64)
+    nodes = np.zeros(8 * (2 * n - 1), np.float32)
+    trails = np.zeros(2 * n, np.uint32)
+    rc = _native.load().ptr_build_light_tree(boxes.ctypes.data, pw.ctypes.data, n, nodes.ctypes.data, trails.ctypes.data)
+    if rc < 0:
+        raise CompileError([Diagnostic("error", "light-tree", f"light tree build failed over {n} lights")])
+    return nodes, trails
 
 
 def _mesh_area(positions, indices):

@@ -30,6 +30,9 @@ namespace ptx {
 #ifndef PTR_SPEC_SHAPES
 #define PTR_SPEC_SHAPES 0xFFu   // bit per PTR_SHAPE_*
 #endif
+#ifndef PTR_SPEC_TREE
+#define PTR_SPEC_TREE 1         // 0: the build never selects lights with the light tree
+#endif
 #ifndef PTR_SPEC_NREGIONS
 #define PTR_SPEC_NREGIONS 0     // 1..16: the region count and PTR_SPEC_SHAPE_CODE (the region BVH unused)
 #endif

@@ -565,6 +565,106 @@ __device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 ligh
     }
     return 0.0f;
 }
+// ---- light-tree selection (accel/light_tree/light_tree.glsl:28-77; the walk pair of
+// features/lighting.ts:767-824) ----------------------------------------------------------
+// The selection context: the receiving point, its shading normal (zero at a medium event:
+// no orientation) and whether the receiver's BSDF covers the whole sphere (rough
+// dielectric), which disarms the below-horizon cull (pt.ts:125-139).
+struct LightQuery { f3 p, n; bool two_sided; };
+
+// Importance of a subtree for the query: phi over the clamped squared distance to the box
+// centre (Conty-Kulla's near-field rule), times a best-case cosine built from the box's
+// corner that lies farthest along n (an exact below-horizon cull for one-sided receivers)
+// and the centre cosine.
+__device__ __forceinline__ float light_tree_importance(f3 bmin, f3 bmax, float phi, const LightQuery& q) {
+    f3 c = 0.5f * (bmin + bmax);
+    f3 e = bmax - bmin;
+    f3 d = c - q.p;
+    float d2raw = dot(d, d);
+    float diag2 = 0.25f * dot(e, e);
+    float base = phi / gmax(d2raw, gmax(diag2, 1e-8f));
+    if (dot(q.n, q.n) < 0.5f) return base;
+    f3 far_c(q.n.x >= 0.0f ? bmax.x : bmin.x, q.n.y >= 0.0f ? bmax.y : bmin.y, q.n.z >= 0.0f ? bmax.z : bmin.z);
+    float h = dot(q.n, far_c - q.p);
+    if (q.two_sided) {
+        f3 near_c = bmin + bmax - far_c;
+        h = gmax(h, -dot(q.n, near_c - q.p));
+    } else if (h <= 0.0f) {
+        return 0.0f;
+    }
+    float cos_c = dot(q.n, d) * (1.0f / sqrtf(gmax(d2raw, 1e-12f)));
+    if (q.two_sided) cos_c = fabsf(cos_c);
+    f3 dmx = vmax(q.p - bmin, bmax - q.p);
+    float lo = h * (1.0f / sqrtf(gmax(dot(dmx, dmx), 1e-12f)));
+    return base * gmin(1.0f, gmax(cos_c, lo));
+}
+// One descent step shared by the pick and the pmf walks: both children's importances and
+// the left probability (isum <= 0: a dead descent).
+struct TreeStep { int L, R; float4 l1, r1; float p_l; bool dead; };
+__device__ __forceinline__ TreeStep light_tree_step(const float4* T, int ni, float4 n1, const LightQuery& q) {
+    TreeStep s;
+    s.L = ni + 1;
+    s.R = (int)n1.w;
+    float4 l0 = __ldg(T + 2 * s.L), r0 = __ldg(T + 2 * s.R);
+    s.l1 = __ldg(T + 2 * s.L + 1);
+    s.r1 = __ldg(T + 2 * s.R + 1);
+    float iw_l = light_tree_importance(xyz(l0), xyz(s.l1), l0.w, q);
+    float iw_r = light_tree_importance(xyz(r0), xyz(s.r1), r0.w, q);
+    float isum = iw_l + iw_r;
+    s.dead = !(isum > 0.0f);
+    s.p_l = s.dead ? 0.0f : iw_l / isum;
+    return s;
+}
+// Stochastic descent: importance-weighted child choice with a fresh number per level below
+// the first; returns the light (or -1 on a dead descent, pmf 0) and the product pmf.
+__device__ __forceinline__ int light_tree_pick(const DevScene& S, const LightQuery& q, float xi, Rng& rng, float& pmf) {
+    const float4* T = S.light_tree;
+    pmf = 1.0f;
+    int ni = 0;
+    float4 n1 = __ldg(T + 1);
+    for (int lvl = 0; lvl < 48 && n1.w >= 0.0f; ++lvl) {
+        TreeStep st = light_tree_step(T, ni, n1, q);
+        if (st.dead) { pmf = 0.0f; return -1; }
+        if (xi < st.p_l) { pmf *= st.p_l; ni = st.L; n1 = st.l1; }
+        else { pmf *= (1.0f - st.p_l); ni = st.R; n1 = st.r1; }
+        xi = rng.next();
+    }
+    if (n1.w >= 0.0f) { pmf = 0.0f; return -1; }
+    return (int)(-n1.w - 1.0f);
+}
+// The MIS pmf of a light: its stored trail replayed with the stored query, through the
+// same step arithmetic as the pick (p_l and 1 - p_l).
+__device__ __forceinline__ float light_tree_pmf(const DevScene& S, const LightQuery& q, int light) {
+    const float4* T = S.light_tree;
+    uint2 tr = __ldg(S.light_trails + light);
+    unsigned tw = tr.x;
+    float pmf = 1.0f;
+    int ni = 0;
+    float4 n1 = __ldg(T + 1);
+    for (int lvl = 0; lvl < 48 && n1.w >= 0.0f; ++lvl) {
+        if (lvl == 24) tw = tr.y;
+        TreeStep st = light_tree_step(T, ni, n1, q);
+        if (st.dead) return 0.0f;
+        if ((tw & 1u) == 0u) { pmf *= st.p_l; ni = st.L; n1 = st.l1; }
+        else { pmf *= (1.0f - st.p_l); ni = st.R; n1 = st.r1; }
+        tw >>= 1u;
+    }
+    return pmf;
+}
+template <class Col>
+__device__ LightSample<Col> lighting_sample_tree(const DevScene& S, const LightQuery& q, float x0, float x1, Rng& rng,
+                                                 const Wl& wl) {
+    LightSample<Col> ls;
+    float sel;
+    int id = light_tree_pick(S, q, x0, rng, sel);
+    if (id < 0) { ls.pdf = 0.0f; return ls; }   // dead descent: a zero-contribution event
+    float lx = rng.next();
+    ls = light_sample_one(S, S.lights[id], Colors<Col>::light(S, id, wl), q.p, lx, x1);
+    ls.light_id = id;
+    ls.pdf *= sel;
+    return ls;
+}
+
 // Finite-light selection by the power CDF with the rescaled coordinate (lighting.ts:546-637).
 template <class Col>
 __device__ LightSample<Col> lighting_sample_finite(const DevScene& S, f3 p, float x0, float x1, const Wl& wl) {
@@ -585,15 +685,19 @@ __device__ LightSample<Col> lighting_sample_finite(const DevScene& S, f3 p, floa
     return ls;
 }
 // Two-stage env-vs-finite draw (lighting.ts generateLightSampling).
+// (tree: the light-tree walk replaces the finite stage, lighting.ts:830-900)
 template <class Col>
-__device__ LightSample<Col> lighting_sample(const DevScene& S, f3 p, float x0, float x1, const Wl& wl) {
+__device__ LightSample<Col> lighting_sample(const DevScene& S, const LightQuery& q, float x0, float x1, Rng& rng,
+                                            bool tree, const Wl& wl) {
     if (S.n_lights == 0) {
         if (S.env_samplable) return env_sample<Col>(S, x0, x1, wl);
         LightSample<Col> ls;
         ls.pdf = 0.0f;
         return ls;
     }
-    if (!S.env_select_live) return lighting_sample_finite<Col>(S, p, x0, x1, wl);
+    tree = PTR_SPEC_TREE && tree;
+    if (!S.env_select_live)
+        return tree ? lighting_sample_tree<Col>(S, q, x0, x1, rng, wl) : lighting_sample_finite<Col>(S, q.p, x0, x1, wl);
     float pe = S.env_select_prob;
     if (x0 < pe) {
         LightSample<Col> ls = env_sample<Col>(S, clampf(x0 / pe, 0.0f, 0.9999999f), x1, wl);
@@ -601,15 +705,31 @@ __device__ LightSample<Col> lighting_sample(const DevScene& S, f3 p, float x0, f
         return ls;
     }
     float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
-    LightSample<Col> ls = lighting_sample_finite<Col>(S, p, fx, x1, wl);
+    LightSample<Col> ls = tree ? lighting_sample_tree<Col>(S, q, fx, x1, rng, wl) : lighting_sample_finite<Col>(S, q.p, fx, x1, wl);
     ls.pdf *= (1.0f - pe);
     return ls;
 }
-__device__ __forceinline__ float lighting_pdf(const DevScene& S, f3 qp, f3 wi, int lid, f3 light_p, f3 light_n) {
+// q: the selection context stored when the path left the previous vertex
+__device__ __forceinline__ float lighting_pdf(const DevScene& S, const LightQuery& q, f3 wi, int lid, f3 light_p,
+                                              f3 light_n, bool tree) {
     const ptr_light& l = S.lights[lid];
-    float sel = S.n_lights == 1 ? 1.0f : l.select_pdf;
+    float sel = (PTR_SPEC_TREE && tree) ? light_tree_pmf(S, q, lid) : S.n_lights == 1 ? 1.0f : l.select_pdf;
     float pe = S.env_select_live ? (1.0f - S.env_select_prob) : 1.0f;
-    return sel * pe * light_pdf_one(l, qp, light_p, light_n, wi);
+    return sel * pe * light_pdf_one(l, q.p, light_p, light_n, wi);
+}
+// The light id of an emitter hit: the region's light, or an instance light of the batch
+// (the TLAS leaf order the hit was found in)
+__device__ __forceinline__ int emitter_light(const DevScene& S, const Hit& hit) {
+    int lid = S.light_of_region[hit.region_to];
+    if (PTR_SPEC_TREE && has_shape(PTR_SHAPE_INSTANCES) && lid < 0 && hit.region_to == hit.region_owner) {
+        const ptr_region& g = S.regions[hit.region_owner];
+        if (g.shape == PTR_SHAPE_INSTANCES) {
+            const DevBatch& b = S.batches[g.ref];
+            const int* lo = (S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w) ? b.light_of_w : b.light_of;
+            if (lo) lid = __ldg(lo + hit.element);
+        }
+    }
+    return lid;
 }
 
 // ---- homogeneous media: chromatic channel-MIS free flight (analytic.glsl:9-51) ---------

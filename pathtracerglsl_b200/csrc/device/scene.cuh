@@ -35,6 +35,10 @@ struct DevBatch {
     int n_inst, proto_shape, proto_mesh, n_tlas;
     const uint4* tlas_w;      // compressed wide BVH over the same boxes (NULL: binary only)
     const float4* place_w;    // the placements in the wide BVH's leaf order
+    // light-tree selection with this batch's instances as lights: the light id of each
+    // placement in the binary / wide TLAS leaf order (NULL: the instances are no lights)
+    const int* light_of;
+    const int* light_of_w;
 };
 
 struct DevScene {
@@ -76,6 +80,10 @@ struct DevScene {
     ptr_spectrum spec_env;
     float spec_m[9];             // XYZ -> linear sRGB, row-major
     float spec_y;                // int ybar d lambda
+    // light tree (light-tree selection; NULL otherwise): 2 float4 per node (min.xyz, phi |
+    // max.xyz, link), and the two trail words of every light
+    const float4* light_tree;
+    const uint2* light_trails;
 };
 
 // ---- closed-form arms (components/geometry/*/*.glsl) ------------------------------------

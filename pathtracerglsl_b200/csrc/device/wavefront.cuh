@@ -31,6 +31,7 @@ struct PathPool {
     float4* thr;       // throughput.xyz, -
     float4* rad;       // radiance.xyz, -
     float4* prev_q;    // stored light-query point (prev_query.p)
+    float4* prev_n;    // stored light-query normal and two-sidedness (light-tree selection)
     int4* st;          // bounce, current_medium, null_crossings, prev_was_delta
     uint2* rng;        // sampler base, dimension
     float4* hit;       // t, u, v, - ; (region, element, prim) in hit_i
@@ -146,6 +147,7 @@ struct ProgParams {
     float rr_max_survival;
     int scattering;
     int equiangular;   // PTR_EQUIANGULAR_*: per-segment medium NEE replaces the at-vertex site
+    int light_tree;    // light-tree selection (the scene carries the tree)
 };
 
 // Batched renders: per job its scene, program knobs, frame and film; offsets[j] is the
@@ -853,10 +855,15 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             Col rad = col_ld<Col>(pool.rad[i]);
             f3 prev_qp = xyz(pool.prev_q[i]);
             Wl wl;
+            const bool tree = PTR_SPEC_TREE && P.light_tree;
             if constexpr (SPECTRAL) wl.lambda = pool.wl[i];
             int4 st = pool.st[i];
             int bounce = st.x, cur_med = st.y, nulls = st.z;
             bool prev_delta = st.w != 0;
+            // the stored selection context's normal and sidedness (light-tree selection)
+            float4 pqn = (tree && !prev_delta) ? pool.prev_n[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            f3 prev_qn = xyz(pqn);
+            bool prev_q2 = pqn.w != 0.0f;
             uint2 rs = pool.rng[i];
             Rng rng;
             rng.base = rs.x;
@@ -933,7 +940,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 if (nee && !P.equiangular) {   // light_sample_direct_medium (light_medium.glsl:7-18)
                                     float y0 = rng.next();
                                     float y1 = rng.next();
-                                    LightSample<Col> ls = lighting_sample<Col>(S, p_evt, y0, y1, wl);
+                                    LightQuery lq{p_evt, f3(0.0f), false};   // no orientation at a medium event
+                                    LightSample<Col> ls = lighting_sample<Col>(S, lq, y0, y1, rng, tree, wl);
                                     if (ls.pdf > 0.0f) {
                                         f3 light_p = p_evt + ls.wi * ls.distance;
                                         float ph = hg_eval(ls.wi, wo_med, mm.phase_g);
@@ -964,6 +972,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 prev_delta = false;
                                 prev_bsdf_pdf = ps.pdf;
                                 prev_qp = p_evt;
+                                prev_qn = f3(0.0f);
+                                prev_q2 = false;
                                 r.o = p_evt;
                                 r.d = ps.wi;
                                 // roulette_interior (pt.ts:230-283)
@@ -1015,10 +1025,11 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                         if (mat_emit >= 0 && (S.materials[mat_emit].flags & PTR_MATF_EMISSIVE)) {
                             float w = 1.0f;
                             if (nee) {
-                                int lid = hit.region_to >= 0 ? S.light_of_region[hit.region_to] : -1;
+                                int lid = hit.region_to >= 0 ? emitter_light(S, hit) : -1;
                                 if (lid >= 0 && !prev_delta) {
                                     if (!mis) w = 0.0f;
-                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, prev_qp, r.d, lid, hit.p, hit.ng));
+                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, LightQuery{prev_qp, prev_qn, prev_q2}, r.d, lid,
+                                                                                         hit.p, hit.ng, tree));
                                 }
                             }
                             Col e = thr * w * CM::emission(S, mat_emit, wl);
@@ -1039,7 +1050,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             if (nee && nondelta) {
                                 float y0 = rng.next();
                                 float y1 = rng.next();
-                                LightSample<Col> ls = lighting_sample<Col>(S, hit.p, y0, y1, wl);
+                                LightQuery lq{hit.p, hit.frame.n, rough};   // rough glass: sphere support
+                                LightSample<Col> ls = lighting_sample<Col>(S, lq, y0, y1, rng, tree, wl);
                                 if (ls.pdf > 0.0f) {
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
@@ -1113,6 +1125,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 prev_delta = (bs.flags & kLobeDelta) != 0u;
                                 prev_bsdf_pdf = bs.pdf;
                                 prev_qp = hit.p;
+                                prev_qn = hit.frame.n;
+                                prev_q2 = rough;
                                 if (bs.flags & kLobeTransmission) {
                                     if (MEDIA) cur_med = hit.region_to;
                                     float rr = ior_of(S, hit.region_to) / ior_of(S, hit.region_from);
@@ -1159,6 +1173,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                 pool.ray_d[i] = f4(r.d, eta_scale);
                 pool.thr[i] = col_st(thr, 0.0f);
                 pool.prev_q[i] = f4(prev_qp, 0.0f);
+                if (tree) pool.prev_n[i] = f4(prev_qn, prev_q2 ? 1.0f : 0.0f);
                 pool.st[i] = make_int4(bounce, cur_med, nulls, prev_delta ? 1 : 0);
                 pool.rng[i] = make_uint2(rng.base, rng.dim);
             }

@@ -204,7 +204,7 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
     int rc = PTR_OK;
     if ((rc = get(c * 16, (void**)&q.ray_o)) || (rc = get(c * 16, (void**)&q.ray_d)) ||
         (rc = get(c * 16, (void**)&q.thr)) || (rc = get(c * 16, (void**)&q.rad)) ||
-        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.st)) ||
+        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.prev_n)) || (rc = get(c * 16, (void**)&q.st)) ||
         (rc = get(c * 8, (void**)&q.rng)) || (rc = get(c * 16, (void**)&q.hit)) ||
         (rc = get(c * 16, (void**)&q.hit_i)) || (rc = get(c * 16, (void**)&q.sh_o)) ||
         (rc = get(c * 16, (void**)&q.sh_d)) || (rc = get(c * 16, (void**)&q.sh_lp)) ||
@@ -317,6 +317,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = p->desc.equiangular;
+    P.light_tree = p->desc.light_tree;
     const int block = tuning_of(p).block;
     const Launcher L{block, n_sm, st, dry, &n_launched};
     PathPool pool = p->pool;
@@ -409,6 +410,7 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     P.rr_max_survival = p->desc.rr_max_survival;
     P.scattering = p->desc.scattering;
     P.equiangular = 0;
+    P.light_tree = p->desc.light_tree;
     const int block = tuning_of(p).block;
     const Launcher L{block, n_sm, st, false};
     const size_t smem = sizeof(double) * PTR_GRAD_SLOTS * (size_t)S.n_materials;
@@ -675,6 +677,15 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
         DevBatch& b = batches[bi];
         const float4* p4 = nullptr;
         int rc;
+        b.light_of = nullptr;
+        b.light_of_w = nullptr;
+        if (bd.light_base >= 0) {   // instance lights: the light id of each leaf slot
+            std::vector<int> lo(N);
+            for (int i = 0; i < N; ++i) lo[i] = bd.light_base + (int)tl.order[i];
+            const int* pi = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, lo.data(), lo.size(), &pi))) return rc;
+            b.light_of = pi;
+        }
         if ((rc = dev_copy(ctx, s->allocs, rec_leaf.data(), rec_leaf.size(), &p4))) return rc;
         b.place = p4;
         if ((rc = dev_copy(ctx, s->allocs, (const float4*)tl.nodes.data(), 2 * (size_t)tl.node_count, &p4))) return rc;
@@ -693,6 +704,13 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
             const uint4* u4 = nullptr;
             if ((rc = dev_copy(ctx, s->allocs, rec_w.data(), rec_w.size(), &p4))) return rc;
             b.place_w = p4;
+            if (bd.light_base >= 0) {
+                std::vector<int> lo(N);
+                for (int i = 0; i < N; ++i) lo[i] = bd.light_base + (int)wt.order[i];
+                const int* pi = nullptr;
+                if ((rc = dev_copy(ctx, s->allocs, lo.data(), lo.size(), &pi))) return rc;
+                b.light_of_w = pi;
+            }
             if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wt.nodes.data(), 5 * (size_t)wt.node_count, &u4))) return rc;
             b.tlas_w = u4;
         }
@@ -834,6 +852,10 @@ int prepare_film(ptr_program* p, const ptr_frame* f, cudaStream_t st) {
 // site covers finite lights, so a sampled environment is rejected (its medium-vertex NEE
 // would be lost).
 int check_equiangular(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
+    if (p->desc.light_tree && !s->dev.light_tree)
+        return fail(ctx, PTR_E_INVALID, "lightSelection 'bvh' needs a scene uploaded with its light tree");
+    if (p->desc.light_tree && p->desc.equiangular)
+        return fail(ctx, PTR_E_INVALID, "lightSelection 'bvh' with mediumLightSampling 'equiangular' is reserved");
     if (!p->desc.equiangular) return PTR_OK;
     if (s->n_lights == 0) return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' needs at least one light");
     if (p->desc.equiangular == PTR_EQUIANGULAR_DELTA && s->n_delta_lights != s->n_lights)
@@ -1057,7 +1079,8 @@ int spec_compile(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* sc, SpecMo
         "-DPTR_SPEC_ENVS=" + std::to_string(sc->spec_envs) + "u",
         "-DPTR_SPEC_SHAPES=" + std::to_string(sc->spec_shapes) + "u",
         "-DPTR_SPEC_NREGIONS=" + std::to_string(sc->spec_nregions),
-        "-DPTR_SPEC_SHAPE_CODE=" + std::to_string(sc->spec_shape_code) + "ull"};
+        "-DPTR_SPEC_SHAPE_CODE=" + std::to_string(sc->spec_shape_code) + "ull",
+        std::string("-DPTR_SPEC_TREE=") + (p->desc.light_tree ? "1" : "0")};
     std::string key;
     for (const auto& o : opts) key += o + "\n";
     key += n_shade + "\n" + n_shadow;
@@ -1181,6 +1204,37 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         }
     }
     if (d->ambient_material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: ambient material out of range");
+    for (int b = 0; b < d->n_batches; ++b) {
+        const ptr_batch_desc& bd = d->batches[b];
+        if (bd.light_base >= 0 && ((long long)bd.light_base + bd.n_instances > d->n_lights || bd.prototype_shape != PTR_SHAPE_SPHERE))
+            return fail(ctx, PTR_E_INVALID, "scene: instance lights of batch " + std::to_string(b) + " exceed the light table");
+    }
+    if (d->n_tree_nodes != 0) {
+        // a preorder tree of one light per leaf: every link points forward inside the
+        // table, every light is reached once, and its trail lands on its own leaf
+        const int nn = d->n_tree_nodes;
+        if (d->n_lights <= 0 || nn != 2 * d->n_lights - 1 || !d->light_tree || !d->light_trails)
+            return fail(ctx, PTR_E_INVALID, "scene: the light tree must hold 2 n_lights - 1 nodes and the trails");
+        std::vector<char> seen(d->n_lights, 0);
+        for (int i = 0; i < nn; ++i) {
+            const float link = d->light_tree[8 * (size_t)i + 7];
+            const int li = (int)link;
+            if ((float)li != link || (li >= 0 && (li <= i + 1 || li >= nn || i + 1 >= nn)) ||
+                (li < 0 && (-li - 1 >= d->n_lights || seen[-li - 1]++)))
+                return fail(ctx, PTR_E_INVALID, "scene: malformed light tree node " + std::to_string(i));
+        }
+        for (int l = 0; l < d->n_lights; ++l) {
+            uint32_t tw = d->light_trails[2 * (size_t)l];
+            int ni = 0, lvl = 0;
+            for (; lvl < 48 && d->light_tree[8 * (size_t)ni + 7] >= 0.0f; ++lvl) {
+                if (lvl == 24) tw = d->light_trails[2 * (size_t)l + 1];
+                ni = (tw & 1u) ? (int)d->light_tree[8 * (size_t)ni + 7] : ni + 1;
+                tw >>= 1u;
+            }
+            if (d->light_tree[8 * (size_t)ni + 7] != (float)(-(l + 1)))
+                return fail(ctx, PTR_E_INVALID, "scene: the trail of light " + std::to_string(l) + " misses its leaf");
+        }
+    }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PTR_E_CUDA, "cudaSetDevice");
     ptr_scene* s = new ptr_scene();
     s->ctx = ctx;
@@ -1193,6 +1247,14 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         (rc = dev_copy(ctx, s->allocs, d->materials, (size_t)d->n_materials, &S.materials)) ||
         (rc = dev_copy(ctx, s->allocs, d->lights, (size_t)d->n_lights, &S.lights)) ||
         (rc = dev_copy(ctx, s->allocs, lor.data(), lor.size(), &S.light_of_region))) {
+        ptr_free_scene(s);
+        return rc;
+    }
+    S.light_tree = nullptr;
+    S.light_trails = nullptr;
+    if (d->n_tree_nodes > 0 &&
+        ((rc = dev_copy(ctx, s->allocs, (const float4*)d->light_tree, 2 * (size_t)d->n_tree_nodes, &S.light_tree)) ||
+         (rc = dev_copy(ctx, s->allocs, (const uint2*)d->light_trails, (size_t)d->n_lights, &S.light_trails)))) {
         ptr_free_scene(s);
         return rc;
     }
@@ -1394,6 +1456,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         P.rr_max_survival = p->desc.rr_max_survival;
         P.scattering = p->desc.scattering;
         P.equiangular = p->desc.equiangular;
+        P.light_tree = p->desc.light_tree;
         if (P.equiangular) equi = true;
         const long long total_j = (long long)J.frame.width * J.frame.height * J.frame.spp;
         FrameParams& F = bjobs[j].frame;
@@ -1585,6 +1648,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
         return fail(ctx, PTR_E_INVALID, "ptr_backward: grads needs PTR_GRAD_SLOTS * n_materials doubles");
     if (n_mat > 512) return fail(ctx, PTR_E_INVALID, "ptr_backward: at most 512 materials");
     if (p->desc.equiangular) return fail(ctx, PTR_E_INVALID, "ptr_backward: equiangular programs are not differentiated");
+    if (p->desc.light_tree) return fail(ctx, PTR_E_INVALID, "ptr_backward: light-tree programs are not differentiated");
     if (p->desc.color != PTR_COLOR_RGB) return fail(ctx, PTR_E_INVALID, "ptr_backward: the adjoint is RGB only");
     for (const ptr_material& m : s->h_materials)
         if ((m.flags & PTR_MATF_MEDIUM) && !(m.sigma_a[0] == m.sigma_a[1] && m.sigma_a[0] == m.sigma_a[2] &&
@@ -1893,7 +1957,7 @@ PathPool na_pool(unsigned char* base) {
     unsigned char* p = base + kNaPool;
     auto take = [&](size_t bytes) { unsigned char* r = p; p += bytes * c; return (void*)r; };
     q.ray_o = (float4*)take(16); q.ray_d = (float4*)take(16); q.thr = (float4*)take(16);
-    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.st = (int4*)take(16);
+    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.prev_n = nullptr; q.st = (int4*)take(16);
     q.hit = (float4*)take(16); q.hit_i = (int4*)take(16); q.sh_o = (float4*)take(16);
     q.sh_d = (float4*)take(16); q.sh_lp = (float4*)take(16); q.sh_c = (float4*)take(16);
     q.rng = (uint2*)take(8); q.q[0] = (int*)take(4); q.q[1] = (int*)take(4); q.shq = (int*)take(4);
@@ -1915,8 +1979,8 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
                      kNoAllocMaxTable);
         return PTR_E_INVALID;
     }
-    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE) {
-        std::fprintf(stderr, "ptr_render_noalloc: only analytic scenes with a constant or no environment are supported\n");
+    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE || d->n_tree_nodes != 0 || pd->light_tree) {
+        std::fprintf(stderr, "ptr_render_noalloc: only analytic scenes with a constant or no environment and power or uniform light selection are supported\n");
         return PTR_E_UNSUPPORTED;
     }
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return PTR_E_INVALID;

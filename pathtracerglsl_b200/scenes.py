@@ -93,6 +93,44 @@ def cornell_mesh_light(direct="mis", emitter="panel", max_depth=8, rr_start=3):
     return scene, strategy
 
 
+def many_lights(direct="mis", selection="bvh", n=64, seed=0, fog=False, max_depth=6, rr_start=3):
+    """The Cornell walls lit by many small lamps: ``n`` emissive instanced spheres in two
+    batches (warm and cool, radii U(0.02, 0.05) in the upper half; under
+    lightSelection 'bvh' every instance is a light of the tree), the ceiling quad light at
+    radiance 5 and a fanned mesh panel; a GGX sphere and a rough glass sphere below.
+    ``fog`` fills the box with a thin scattering medium (medium events query the tree
+    without a normal)."""
+    scene, strategy = cornell(direct, max_depth, rr_start)
+    rng = _np.random.RandomState(seed)
+    objects = list(scene["objects"][:5])
+    objects.append({"type": "sphere", "parameters": {"center": [-0.4, 0.3, -0.3], "radius": 0.3}, "material": "metal"})
+    objects.append({"type": "sphere", "parameters": {"center": [0.4, 0.3, 0.3], "radius": 0.3}, "material": "frost"})
+    materials = dict(scene["materials"],
+                     metal={"model": "ggx", "f0": [0.9, 0.8, 0.6], "roughness": 0.4},
+                     frost={"model": "rough_dielectric", "ior": 1.5, "roughness": 0.3})
+    for b, (col, le) in enumerate((([1.0, 0.6, 0.3], 40.0), ([0.3, 0.6, 1.0], 25.0))):
+        pl = [{"position": [float(rng.uniform(-0.9, 0.9)), float(rng.uniform(0.8, 1.9)), float(rng.uniform(-0.9, 0.6))],
+               "scale": float(rng.uniform(0.02, 0.05))} for _ in range(n // 2)]
+        objects.append({"kind": "instanced", "placements": pl,
+                        "prototype": {"type": "sphere", "parameters": {"center": [0, 0, 0], "radius": 1.0},
+                                      "material": f"lamp{b}"}})
+        materials[f"lamp{b}"] = {"model": "lambert", "albedo": [0.0, 0.0, 0.0], "emission": [le * c for c in col]}
+    y = 1.98
+    objects.append({"kind": "mesh", "material": "panel", "closed": False,
+                    "positions": [[0.55, y, 0.45], [0.3, y, 0.3], [0.8, y, 0.3], [0.8, y, 0.6], [0.3, y, 0.6]],
+                    "indices": [[0, 1, 2], [0, 2, 3], [0, 3, 4], [0, 4, 1]]})
+    materials["panel"] = {"model": "lambert", "albedo": [0.0, 0.0, 0.0], "emission": [4.0, 8.0, 4.0]}
+    lights = [dict(scene["lights"][0], emission=5.0)]
+    scene = dict(scene, id=f"many-lights-{n}", objects=objects, materials=materials, lights=lights)
+    if fog:
+        scene["materials"]["fog"] = {"model": "none", "medium": {"sigma_a": [0.02, 0.02, 0.02],
+                                                                 "sigma_s": [0.15, 0.15, 0.15], "phase_g": 0.3}}
+        scene["ambientMedium"] = "fog"
+    strategy = dict(strategy, id=strategy["id"] + "-" + selection,
+                    estimator=dict(strategy["estimator"], lightSelection=selection))
+    return scene, strategy
+
+
 def furnace(direct="mis", max_depth=8):
     scene = {
         "id": "furnace-c1",

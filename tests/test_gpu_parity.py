@@ -94,6 +94,17 @@ def test_mesh_lights_match_oracle(engine, oracle_lib, direct, emitter):
     compare(engine, oracle_lib, sc, st, 64, 64, 8, {})
 
 
+@pytest.mark.parametrize("case", ["nee", "mis", "mis-fog", "mis-cwbvh-tlas"])
+def test_light_tree_matches_oracle(engine, oracle_lib, case):
+    """Light-tree selection over 64 instanced lamps, a quad and a mesh light: the pick walk
+    (a fresh number per level), the trail-replayed MIS pmf with the stored query, medium
+    events querying without a normal, and instance-light identity through either TLAS."""
+    sc, st = scenes.many_lights(direct="nee" if case == "nee" else "mis", selection="bvh", fog=case == "mis-fog")
+    if case == "mis-cwbvh-tlas":
+        st = dict(st, estimator=dict(st["estimator"], instanceAccel="cwbvh"))
+    compare(engine, oracle_lib, sc, st, 48, 48, 8, CASE_CAMERAS["cornell"])
+
+
 def test_furnace_variant_value(engine, oracle_lib):
     sc, st = scenes.furnace()
     compare(engine, oracle_lib, sc, st, 32, 32, 16, {})

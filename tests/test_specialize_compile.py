@@ -38,6 +38,7 @@ CENSUS = {
     "mesh": (0b101, 0b0, 0b100, [0, 5], "ptx::f3", 2, "false"),
     "cornell-mesh-light": (0b11, 0b1000, 0b1, [2, 2, 2, 2, 2, 1, 1, 4], "ptx::f3", 2, "false"),
     "fog-mesh-light": (0b10001, 0b1011, 0b1, [0, 0, 1, 4], "ptx::f3", 1, "true"),
+    "many-lights-no-tree": (0b100101, 0b1011, 0b1, [2, 2, 2, 2, 2, 1, 1, 5, 5, 4, 2], "ptx::f3", 2, "false", 0),
     "media-spectral": (0b10011, 0b11, 0b1, [0, 1, 1, 1, 2, 2, 2, 2], "ptx::s4", 1, "true"),
     "many-regions": (0b1, 0b1, 0b10, [2] * 16, "ptx::f3", 2, "false"),
 }
@@ -46,7 +47,7 @@ CENSUS = {
 @pytest.mark.parametrize("case", sorted(CENSUS))
 def test_specialised_kernels_compile(case):
     lib = _nvrtc()
-    mats, lights, envs, shapes, col, direct, media = CENSUS[case]
+    mats, lights, envs, shapes, col, direct, media, *tree = CENSUS[case]
     names = [b"ptx::k_closest<false, false>",
              f"ptx::k_shade<{col}, {direct}, {media}, false, false>".encode(),
              f"ptx::k_shadow<{col}, {media}, false, false, false>".encode()]
@@ -56,7 +57,8 @@ def test_specialised_kernels_compile(case):
             f"-DPTR_SPEC_MATS={mats}u".encode(), f"-DPTR_SPEC_LIGHTS={lights}u".encode(),
             f"-DPTR_SPEC_ENVS={envs}u".encode(),
             f"-DPTR_SPEC_SHAPES={sum(1 << s for s in set(shapes))}u".encode(),
-            f"-DPTR_SPEC_NREGIONS={len(shapes)}".encode(), f"-DPTR_SPEC_SHAPE_CODE={_code(shapes)}ull".encode()]
+            f"-DPTR_SPEC_NREGIONS={len(shapes)}".encode(), f"-DPTR_SPEC_SHAPE_CODE={_code(shapes)}ull".encode(),
+            f"-DPTR_SPEC_TREE={tree[0] if tree else 1}".encode()]
     prog = C.c_void_p()
     assert lib.nvrtcCreateProgram(C.byref(prog), PRELUDE, b"ptr_specialize.cu", 0, None, None) == 0
     try:
