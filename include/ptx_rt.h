@@ -74,7 +74,9 @@ typedef struct ptr_region {
 typedef struct ptr_material {
     int32_t model;          /* PTR_MAT_*                                                  */
     int32_t flags;          /* PTR_MATF_*                                                 */
-    int32_t pad0, pad1;
+    int32_t field_a;        /* heterogeneous medium: 1 + the word offset of sigma_a's
+                               program in field_code; 0 = the constant sigma_a below      */
+    int32_t field_s;        /* likewise sigma_s                                           */
     float albedo[4];        /* lambert albedo (rgb)                                       */
     float emission[4];      /* emitted radiance (rgb)                                     */
     float transmittance[4]; /* dielectric interface tint                                  */
@@ -83,8 +85,24 @@ typedef struct ptr_material {
     float sigma_s[4];       /* medium scattering (rgb)                                    */
     float alpha;            /* ggx alpha = max(1e-3, roughness^2)  (ggx.glsl:7-9)          */
     float phase_g;          /* HG asymmetry                                               */
-    float pad2, pad3;
+    float majorant;         /* heterogeneous medium: the density ceiling sigma_bar; the
+                               rendered medium is the field scaled so max sigma_t <= it   */
+    float pad3;
 } ptr_material;             /* 128 bytes */
+
+/* ---- heterogeneous media: coefficient fields ----------------------------------------
+ * A medium coefficient given as a GLSL expression of the position p (the reference's
+ * {kind: 'glsl', source, params} coefficients, delta_tracking.glsl) travels as a stack
+ * program: uint32 opcodes, CONST followed by three float bit patterns, SWZ by a component
+ * index.  Every slot holds three floats (scalars broadcast); the host validates each
+ * program (known opcodes, stack within PTR_FIELD_MAX_STACK, END inside the table). */
+#define PTR_FIELD_MAX_STACK 16
+enum {
+    PTR_FOP_END, PTR_FOP_CONST, PTR_FOP_P, PTR_FOP_SWZ, PTR_FOP_ADD, PTR_FOP_SUB, PTR_FOP_MUL, PTR_FOP_DIV,
+    PTR_FOP_NEG, PTR_FOP_EXP, PTR_FOP_LOG, PTR_FOP_SIN, PTR_FOP_COS, PTR_FOP_SQRT, PTR_FOP_ABS, PTR_FOP_FLOOR,
+    PTR_FOP_FRACT, PTR_FOP_POW, PTR_FOP_MIN, PTR_FOP_MAX, PTR_FOP_MOD, PTR_FOP_STEP, PTR_FOP_CLAMP, PTR_FOP_MIX,
+    PTR_FOP_SMOOTHSTEP, PTR_FOP_DOT, PTR_FOP_LENGTH, PTR_FOP_VEC3, PTR_FOP_COUNT
+};
 
 /* ---- lights (src/components/lights/{quad,sphere,point,mesh}) ---------------------------- */
 #define PTR_LIGHT_QUAD 0   /* p: corner(3) edge1(3) edge2(3) normal(3) area(1) */
@@ -200,6 +218,8 @@ typedef struct ptr_scene_desc {
     int32_t n_tree_nodes;      /* 2 n_lights - 1, or 0                                    */
     const float* light_tree;
     const uint32_t* light_trails;
+    int32_t n_field_code;      /* words of the heterogeneous media's field programs       */
+    const uint32_t* field_code;
 } ptr_scene_desc;
 
 /* ---- program (strategy) ---------------------------------------------------------- */

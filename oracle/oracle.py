@@ -52,6 +52,7 @@ def lib():
         _lib.oracle_mesh_brute.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_rough_dielectric_eval_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 5
         _lib.oracle_rough_dielectric_sample_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 7
+        _lib.oracle_field_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         _lib.oracle_forward_tile.restype = ctypes.c_int
         _lib.oracle_forward_tile.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 2 + [ctypes.c_int]
     return _lib
@@ -109,6 +110,15 @@ def forward(packed, renderer, width, height, spp, first_sample=0, salt=0, params
     if rc != 0:
         raise RuntimeError(f"oracle_forward_tile failed: {rc}")
     return {"jac": jac / spp, "mean": s / spp}
+
+
+def field_eval(code, points):
+    """The oracle's interpretation of a coefficient field program at points (n, 3)."""
+    code = np.ascontiguousarray(code, np.uint32)
+    p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    out = np.zeros(p.shape, np.float32)
+    lib().oracle_field_eval(code.ctypes.data, 0, p.ctypes.data, len(p), out.ctypes.data)
+    return out
 
 
 def rough_dielectric_eval(alpha, n_i, n_t, wi, wo, tint=(1.0, 1.0, 1.0)):

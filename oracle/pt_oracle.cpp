@@ -94,6 +94,18 @@ struct Rng {
     }
 };
 
+// The shadow query's own stream (heterogeneous media): hashed from the path's base and its
+// sampler dimension at the NEE site (the device queues shadow queries, so they cannot draw
+// from the path's own stream in the reference's order).
+inline Rng shadow_rng(uint32_t base, uint32_t seed) {
+    uint32_t v[4] = {base, seed, 0x53484457u, 0u};
+    Rng::pcg4d(v);
+    Rng r;
+    r.base = v[0];
+    r.dim = 0;
+    return r;
+}
+
 // ---------------------------------------------------------------- core structs (structs.glsl)
 struct Frame { v3 t, b, n; };
 struct Ray { v3 o, d; };
@@ -855,6 +867,89 @@ inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, flo
 
 // ---------------------------------------------------------------- media (transport/volume/analytic)
 struct MediumSample { bool scattered; float t; v3 weight; v3 exit_p, exit_dir; };
+
+// ---- heterogeneous media (transport/volume/delta_tracking/delta_tracking.glsl)
+// The coefficient field: the stack program of a GLSL expression of p, interpreted with
+// the same operations in the same order as the device.
+inline float fract_(float x) { return x - std::floor(x); }
+inline v3 field_eval(const uint32_t* code, v3 p) {
+    v3 st[PTR_FIELD_MAX_STACK];
+    int sp = 0;
+    auto fl = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
+    for (int pc = 0;;) {
+        const uint32_t op = code[pc++];
+        if (op == PTR_FOP_END) break;
+        if (op == PTR_FOP_CONST) { st[sp++] = v3(fl(code[pc]), fl(code[pc + 1]), fl(code[pc + 2])); pc += 3; continue; }
+        if (op == PTR_FOP_P) { st[sp++] = p; continue; }
+        if (op == PTR_FOP_SWZ) { float x = st[sp - 1][(int)code[pc++]]; st[sp - 1] = v3(x, x, x); continue; }
+        if (op >= PTR_FOP_ADD && op <= PTR_FOP_DIV) {
+            v3 b = st[--sp], a = st[sp - 1];
+            st[sp - 1] = op == PTR_FOP_ADD ? a + b : op == PTR_FOP_SUB ? a - b : op == PTR_FOP_MUL ? a * b
+                       : v3(a.x / b.x, a.y / b.y, a.z / b.z);
+            continue;
+        }
+        if (op >= PTR_FOP_NEG && op <= PTR_FOP_FRACT) {
+            v3 a = st[sp - 1];
+            for (int k = 0; k < 3; ++k) {
+                float x = a[k];
+                switch (op) {
+                    case PTR_FOP_NEG: x = -x; break;
+                    case PTR_FOP_EXP: x = std::exp(x); break;
+                    case PTR_FOP_LOG: x = std::log(x); break;
+                    case PTR_FOP_SIN: x = std::sin(x); break;
+                    case PTR_FOP_COS: x = std::cos(x); break;
+                    case PTR_FOP_SQRT: x = std::sqrt(x); break;
+                    case PTR_FOP_ABS: x = std::fabs(x); break;
+                    case PTR_FOP_FLOOR: x = std::floor(x); break;
+                    default: x = fract_(x); break;
+                }
+                a[k] = x;
+            }
+            st[sp - 1] = a;
+            continue;
+        }
+        if (op >= PTR_FOP_POW && op <= PTR_FOP_STEP) {
+            v3 b = st[--sp], a = st[sp - 1];
+            for (int k = 0; k < 3; ++k) {
+                float x = a[k], y = b[k];
+                switch (op) {
+                    case PTR_FOP_POW: x = std::pow(x, y); break;
+                    case PTR_FOP_MIN: x = y < x ? y : x; break;
+                    case PTR_FOP_MAX: x = x < y ? y : x; break;
+                    case PTR_FOP_MOD: x = x - y * std::floor(x / y); break;
+                    default: x = y < x ? 0.0f : 1.0f; break;   // step(edge = a, x = b)
+                }
+                a[k] = x;
+            }
+            st[sp - 1] = a;
+            continue;
+        }
+        if (op >= PTR_FOP_CLAMP && op <= PTR_FOP_SMOOTHSTEP) {
+            v3 c = st[--sp], b = st[--sp], a = st[sp - 1];
+            for (int k = 0; k < 3; ++k) {
+                float x;
+                if (op == PTR_FOP_CLAMP) {
+                    x = a[k] < b[k] ? b[k] : a[k];
+                    x = c[k] < x ? c[k] : x;
+                } else if (op == PTR_FOP_MIX) {
+                    x = a[k] * (1.0f - c[k]) + b[k] * c[k];
+                } else {
+                    float t = (c[k] - a[k]) / (b[k] - a[k]);
+                    t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+                    x = t * t * (3.0f - 2.0f * t);
+                }
+                a[k] = x;
+            }
+            st[sp - 1] = a;
+            continue;
+        }
+        if (op == PTR_FOP_DOT) { v3 b = st[--sp]; float dd = dot(st[sp - 1], b); st[sp - 1] = v3(dd, dd, dd); continue; }
+        if (op == PTR_FOP_LENGTH) { float l = std::sqrt(dot(st[sp - 1], st[sp - 1])); st[sp - 1] = v3(l, l, l); continue; }
+        v3 z = st[--sp], y = st[--sp], x = st[sp - 1];   // VEC3
+        st[sp - 1] = v3(x.x, y.x, z.x);
+    }
+    return st[0];
+}
 // medium_sample_analytic (transport/volume/analytic/analytic.glsl:9-43)
 inline MediumSample medium_sample_analytic(const ptr_material& m, const Ray& r, float t_max, float x0, float x1) {
     v3 sigma_t = ld3(m.sigma_a) + ld3(m.sigma_s);
@@ -1452,6 +1547,78 @@ struct Tracer {
         v3 st = scatter_live(med) ? ld3(m.sigma_a) + ld3(m.sigma_s) : ld3(m.sigma_a);
         return vexp(-st * len);
     }
+    // ---- heterogeneous media: the D1-clamped fields and the tracking arms
+    bool is_het(int med) const { return d.materials[med].field_a != 0 || d.materials[med].field_s != 0; }
+    void het_props(const ptr_material& m, v3 p, v3& sa, v3& ss) const {
+        sa = m.field_a ? field_eval(d.field_code + (m.field_a - 1), p) : ld3(m.sigma_a);
+        ss = m.field_s ? field_eval(d.field_code + (m.field_s - 1), p) : ld3(m.sigma_s);
+        v3 st = sa + ss;
+        float smax = fmaxf_(st.x, fmaxf_(st.y, st.z));
+        float scale = smax > m.majorant ? m.majorant / smax : 1.0f;
+        sa = sa * scale;
+        ss = ss * scale;
+    }
+    static int tracking_cap(float lambda) { return (int)std::ceil(lambda + 6.5f * std::sqrt(lambda) + 12.0f); }
+    // delta tracking (Kutz et al. 2017, Algorithm 4; average-based probabilities)
+    MediumSample medium_sample_delta(const ptr_material& m, const Ray& r, float t_max, float x0, float x1) {
+        MediumSample ms;
+        ms.scattered = false;
+        ms.t = t_max;
+        const float sbar = m.majorant;
+        v3 w(1.0f);
+        float t = 0.0f, xd = x0, xe = x1;
+        const int cap = tracking_cap(sbar * t_max);
+        for (int i = 0; i < cap; ++i) {
+            t += -std::log(1.0f - xd) / sbar;
+            if (t >= t_max) { ms.weight = w; return ms; }
+            v3 p = r.o + r.d * t;
+            v3 sa, ss;
+            het_props(m, p, sa, ss);
+            v3 sn = vmax(v3(sbar) - (sa + ss), v3(0.0f));
+            float pa = spectrum_average(sa * w);
+            float ps = spectrum_average(ss * w);
+            float pn = spectrum_average(sn * w);
+            float c = pa + ps + pn;
+            if (c <= 0.0f) { ms.weight = v3(0.0f); return ms; }
+            pa /= c; ps /= c; pn /= c;
+            if (xe < pa) { ms.weight = v3(0.0f); return ms; }
+            if (xe < pa + ps) {
+                ms.scattered = true;
+                ms.t = t;
+                ms.exit_p = p;
+                ms.exit_dir = r.d;
+                ms.weight = w * ss / (sbar * fmaxf_(ps, 1e-20f));
+                return ms;
+            }
+            w = w * sn / (sbar * fmaxf_(pn, 1e-20f));
+            xd = rng.next();
+            xe = rng.next();
+        }
+        ms.weight = w;
+        return ms;
+    }
+    // ratio tracking (Novak et al. 2014): sigma_a for the pass-through arm, sigma_t with
+    // pbrt's roulette for shadow segments
+    v3 medium_ratio_track(const ptr_material& m, const Ray& r, float len, Rng& g, bool extinction) const {
+        const float sbar = m.majorant;
+        v3 T(1.0f);
+        float t = 0.0f;
+        const int cap = tracking_cap(sbar * len);
+        for (int i = 0; i < cap; ++i) {
+            t += -std::log(1.0f - g.next()) / sbar;
+            if (t >= len) return T;
+            v3 sa, ss;
+            het_props(m, r.o + r.d * t, sa, ss);
+            T = T * (vmax(v3(sbar) - (extinction ? sa + ss : sa), v3(0.0f)) / sbar);
+            if (extinction && spectrum_max(T) < 0.05f) {
+                if (g.next() < 0.75f) return v3(0.0f);
+                T = T / 0.25f;
+            }
+        }
+        return T;
+    }
+    uint32_t shadow_seed = 0;   // the path's sampler dimension at the current NEE site
+
     v3 medium_survival(int med) const {
         const ptr_material& m = d.materials[med];
         v3 sa = ld3(m.sigma_a), ss = ld3(m.sigma_s);
@@ -1470,6 +1637,8 @@ struct Tracer {
         v3 T(1.0f);
         int medium = S.scene_region_at(sr.o);
         Ray seg = sr;
+        Rng srng;
+        bool srng_live = false;
         for (int crossed = 0; crossed <= crossings_left; crossed++) {
             float remaining = length(light_p - seg.o) - SHADOW_BACKOFF;
             if (remaining <= 0.0f) return T;
@@ -1477,7 +1646,10 @@ struct Tracer {
             bool hit_boundary = S.scene_intersect(seg, h) && h.t < remaining;
             float seg_len = hit_boundary ? h.t : remaining;
             int med_mat = S.material_of(medium);
-            if (S.material_has_medium(med_mat)) {
+            if (S.material_has_medium(med_mat) && is_het(med_mat)) {
+                if (!srng_live) { srng = shadow_rng(rng.base, shadow_seed); srng_live = true; }
+                T = T * medium_ratio_track(d.materials[med_mat], seg, seg_len, srng, scatter_live(med_mat));
+            } else if (S.material_has_medium(med_mat)) {
                 T = T * medium_transmittance(med_mat, seg_len);
                 if (dlog) {   // T_seg = exp(-sigma len), sigma = st (scattering) or (1 - a) st
                     double st, a;
@@ -1697,7 +1869,10 @@ struct Tracer {
                     float x0 = rng.next(), x1 = rng.next();
                     float t_max = boundary ? hit.t : MAX_DIST;
                     const ptr_material& mm = d.materials[med_mat];
-                    if (!scatter_live(med_mat)) {
+                    const bool het = is_het(med_mat);
+                    if (het && !scatter_live(med_mat)) {   // ratio-tracked pass-through
+                        throughput = throughput * medium_ratio_track(mm, r, t_max, rng, false);
+                    } else if (!scatter_live(med_mat)) {
                         // absorbing-only arm (deterministic): weight = exp(-sigma_a t_max)
                         if (tan) {   // exp(-(1 - a) st t_max)
                             double st, a;
@@ -1710,7 +1885,8 @@ struct Tracer {
                         }
                         throughput = throughput * vexp(-ld3(mm.sigma_a) * t_max);
                     } else {
-                        MediumSample ms = medium_sample_analytic(mm, r, t_max, x0, x1);
+                        MediumSample ms = het ? medium_sample_delta(mm, r, t_max, x0, x1)
+                                              : medium_sample_analytic(mm, r, t_max, x0, x1);
                         if (tan) {   // free flight with the detached channel-MIS density
                             double st, a;
                             grey_params(med_mat, st, a);
@@ -1739,6 +1915,7 @@ struct Tracer {
                             if (nee && !P.equiangular) {
                                 float y0 = rng.next(), y1 = rng.next();
                                 LightSample ls = lighting_sample(Query{p_evt, v3(0.0f), false}, y0, y1);
+                                shadow_seed = rng.dim;
                                 if (ls.pdf > 0.0f) {
                                     v3 light_p = p_evt + ls.wi * ls.distance;
                                     dlog_vis.clear();
@@ -1778,7 +1955,8 @@ struct Tracer {
                             prev_qn = v3(0.0f);
                             prev_q2 = false;
                             r = Ray{p_evt, ps.wi};
-                            if (!roulette_interior(bounce, medium_survival(med_mat))) break;
+                            // tracking arms settled absorption in their lottery: nothing is owed
+                            if (!het && !roulette_interior(bounce, medium_survival(med_mat))) break;
                             continue;
                         }
                     }
@@ -1813,6 +1991,7 @@ struct Tracer {
             if (nee && S.material_has_nondelta_lobes(mat)) {
                 float y0 = rng.next(), y1 = rng.next();
                 LightSample ls = lighting_sample(Query{hit.p, hit.frame.n, m.model == PTR_MAT_ROUGH_DIELECTRIC}, y0, y1);
+                shadow_seed = rng.dim;
                 if (ls.pdf > 0.0f) {
                     v3 light_p = hit.p + ls.wi * ls.distance;
                     Ray sr = ray_spawn(hit, ls.wi);
@@ -1885,6 +2064,17 @@ inline Ray camera_ray(const ptr_camera& c, int W, int H, float fx, float fy) {
 }  // namespace
 
 extern "C" {
+
+// The coefficient field program starting at code[start], evaluated at n points (3 floats
+// each) into out (3 floats each).
+void oracle_field_eval(const uint32_t* code, int start, const float* p, int n, float* out) {
+    for (int i = 0; i < n; ++i) {
+        v3 v = field_eval(code + start, v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]));
+        out[3 * i] = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    }
+}
 
 // Render frame->spp samples for every pixel; accumulate per-pixel sum / sum of squares
 // (float64, 3 per pixel, row 0 = bottom).  Returns counters through out_counts[2]

@@ -7,6 +7,7 @@ their descriptors from these types, so the two consume byte-identical scenes.
 import ctypes as C
 
 ABI_VERSION = 3
+FIELD_MAX_STACK = 16
 
 PTR_OK = 0
 PTR_E_INVALID = -1
@@ -38,10 +39,10 @@ class Region(C.Structure):
 
 
 class Material(C.Structure):
-    _fields_ = [("model", C.c_int32), ("flags", C.c_int32), ("pad0", C.c_int32), ("pad1", C.c_int32),
+    _fields_ = [("model", C.c_int32), ("flags", C.c_int32), ("field_a", C.c_int32), ("field_s", C.c_int32),
                 ("albedo", F4), ("emission", F4), ("transmittance", F4), ("f0", F4),
                 ("sigma_a", F4), ("sigma_s", F4), ("alpha", C.c_float), ("phase_g", C.c_float),
-                ("pad2", C.c_float), ("pad3", C.c_float)]
+                ("majorant", C.c_float), ("pad3", C.c_float)]
 
 
 class Light(C.Structure):
@@ -98,7 +99,8 @@ class SceneDesc(C.Structure):
                 ("n_batches", C.c_int32), ("batches", C.POINTER(BatchDesc)),
                 ("spectral", C.POINTER(SpectralDesc)),
                 ("n_tree_nodes", C.c_int32), ("light_tree", C.POINTER(C.c_float)),
-                ("light_trails", C.POINTER(C.c_uint32))]
+                ("light_trails", C.POINTER(C.c_uint32)),
+                ("n_field_code", C.c_int32), ("field_code", C.POINTER(C.c_uint32))]
 
 
 class ProgramDesc(C.Structure):

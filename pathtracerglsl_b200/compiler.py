@@ -18,6 +18,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import abi
+from . import field as medium_field
 
 # ----------------------------------------------------------------------------- diagnostics
 
@@ -175,6 +176,7 @@ class PackedScene:
     spectral: object = None     # spectral.SpectralTables of spectral strategies, else None
     light_tree: object = None   # float32 nodes (8 per node) under light-tree selection, else None
     light_trails: object = None # uint32 trail words (2 per light)
+    field_code: object = None   # uint32 programs of heterogeneous media coefficients
 
     def desc(self):
         """A ``ptr_scene_desc`` pointing into this object's arrays (keep self alive)."""
@@ -226,6 +228,9 @@ class PackedScene:
         if self.spectral is not None:
             self._spec_desc = self.spectral.desc()
             d.spectral = abi.C.pointer(self._spec_desc)
+        if self.field_code is not None:
+            d.n_field_code = len(self.field_code)
+            d.field_code = self.field_code.ctypes.data_as(abi.C.POINTER(abi.C.c_uint32))
         if self.light_tree is not None:
             d.n_tree_nodes = len(self.light_tree) // 8
             d.light_tree = self.light_tree.ctypes.data_as(abi.C.POINTER(abi.C.c_float))
@@ -352,8 +357,27 @@ class Compiler:
             if not (360.0 <= lo < hi <= 830.0):
                 bag.error("invalid-setting", "measurement.wavelengthRange must lie in [360, 830] nm")
         vs = est.get("volumeSampling", "analytic")
-        if vs not in ("analytic", None):
+        if vs not in ("analytic", "delta-tracking", None):
             bag.error("unsupported", f"volumeSampling {vs!r} is not available in this build")
+        for name, m in mats.items():
+            med = m.get("medium") or {}
+            het = [k for k in ("sigma_a", "sigma_s") if medium_field.is_field(med.get(k))]
+            if not het:
+                continue
+            # Validator.ts:320-360: expression coefficients need a finite positive majorant
+            maj = med.get("majorant")
+            if not (isinstance(maj, (int, float)) and math.isfinite(maj) and maj > 0):
+                bag.error("invalid-medium", f"Material '{name}': medium.{het[0]} is a GLSL expression but the medium "
+                          "declares no majorant; heterogeneous media require a density ceiling (majorant: <finite number > 0>)")
+            if meas.get("color", "rgb") == "spectral":
+                bag.error("unsupported", f"Material '{name}': heterogeneous media render in RGB only in this build")
+            if est.get("mediumLightSampling", "vertex") == "equiangular":
+                bag.error("unsupported", f"Material '{name}': equiangular sampling through heterogeneous media is not available")
+            for k in het:
+                try:
+                    medium_field.compile_field(med[k], {})
+                except medium_field.FieldError as e:
+                    bag.error("invalid-medium", f"Material '{name}': medium.{k}: {e}")
         sel = est.get("lightSelection", "power")
         if sel not in ("power", "uniform", "bvh"):
             bag.error("invalid-setting", f"estimator.lightSelection {sel!r} (available: power, uniform, bvh)")
@@ -397,6 +421,7 @@ class Compiler:
         mat_names = list(mats_src.keys())
         mat_index = {n: i for i, n in enumerate(mat_names)}
         materials = []
+        self._field_code = []
         spec_src = []          # per material: the authored material, or a light's raw emission
         for n in mat_names:
             materials.append(self._material(mats_src[n], params))
@@ -594,6 +619,7 @@ class Compiler:
             env=env, meshes=meshes, batches=batches,
             region_names=region_names, material_names=mat_names,
             light_tree=tree, light_trails=trails,
+            field_code=np.asarray(self._field_code, np.uint32) if self._field_code else None,
         )
         if any(st.get("measurement", {}).get("color", "rgb") == "spectral" for st in strategies):
             packed.spectral = self._spectral_tables(spec_src, [raw for *_x, raw in lights],
@@ -699,13 +725,25 @@ class Compiler:
             flags |= abi.MATF_EMISSIVE
         med = m.get("medium")
         if med is not None:
-            sa = rgb(med.get("sigma_a"), params, [0.0, 0.0, 0.0])
-            ss = rgb(med.get("sigma_s"), params, [0.0, 0.0, 0.0])
-            rec.sigma_a = abi.F4(*(sa + [0.0]))
-            rec.sigma_s = abi.F4(*(ss + [0.0]))
+            def coef(key, slot):
+                v = med.get(key)
+                if medium_field.is_field(v):   # heterogeneous: the stack program, 1 + its offset
+                    code = getattr(self, "_field_code", None)
+                    if code is None:
+                        code = self._field_code = []
+                    setattr(rec, slot, 1 + len(code))
+                    code.extend(medium_field.compile_field(v, params))
+                    return None
+                return rgb(v, params, [0.0, 0.0, 0.0])
+            sa = coef("sigma_a", "field_a")
+            ss = coef("sigma_s", "field_s")
+            rec.sigma_a = abi.F4(*((sa or [0.0] * 3) + [0.0]))
+            rec.sigma_s = abi.F4(*((ss or [0.0] * 3) + [0.0]))
             rec.phase_g = float(resolve(med.get("phase_g", med.get("g")), params, 0.0))
+            if rec.field_a or rec.field_s:
+                rec.majorant = float(med["majorant"])
             flags |= abi.MATF_MEDIUM
-            if max(ss) > 0.0:
+            if ss is None or max(ss) > 0.0:
                 flags |= abi.MATF_SCATTERING
         rec.flags = flags
         return rec

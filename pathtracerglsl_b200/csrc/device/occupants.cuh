@@ -734,6 +734,200 @@ __device__ __forceinline__ int emitter_light(const DevScene& S, const Hit& hit) 
 
 // ---- homogeneous media: chromatic channel-MIS free flight (analytic.glsl:9-51) ---------
 template <class Col> struct MediumSample { bool scattered; Col weight; f3 exit_p, exit_dir; };
+
+// ---- heterogeneous media (transport/volume/delta_tracking/delta_tracking.glsl) ----------
+// A coefficient field: the stack program of a GLSL expression of p (validated at upload:
+// known opcodes, stack depth within PTR_FIELD_MAX_STACK, END inside the table).
+__device__ __forceinline__ float fract_(float x) { return x - floorf(x); }
+__device__ f3 field_eval(const uint32_t* code, f3 p) {
+    f3 st[PTR_FIELD_MAX_STACK];
+    int sp = 0;
+    for (int pc = 0;;) {
+        const uint32_t op = __ldg(code + pc++);
+        if (op == PTR_FOP_END) break;
+        if (op == PTR_FOP_CONST) {
+            st[sp++] = f3(__uint_as_float(__ldg(code + pc)), __uint_as_float(__ldg(code + pc + 1)),
+                          __uint_as_float(__ldg(code + pc + 2)));
+            pc += 3;
+            continue;
+        }
+        if (op == PTR_FOP_P) { st[sp++] = p; continue; }
+        if (op == PTR_FOP_SWZ) {
+            const uint32_t c = __ldg(code + pc++);
+            f3 v = st[sp - 1];
+            float x = c == 0 ? v.x : c == 1 ? v.y : v.z;
+            st[sp - 1] = f3(x, x, x);
+            continue;
+        }
+        if (op >= PTR_FOP_ADD && op <= PTR_FOP_DIV) {
+            f3 b = st[--sp], a = st[sp - 1];
+            st[sp - 1] = op == PTR_FOP_ADD ? a + b : op == PTR_FOP_SUB ? a - b
+                       : op == PTR_FOP_MUL ? a * b : f3(a.x / b.x, a.y / b.y, a.z / b.z);
+            continue;
+        }
+        if (op >= PTR_FOP_NEG && op <= PTR_FOP_FRACT) {
+            f3 a = st[sp - 1];
+            float r[3] = {a.x, a.y, a.z};
+            for (int k = 0; k < 3; ++k) {
+                float x = r[k];
+                switch (op) {
+                    case PTR_FOP_NEG: x = -x; break;
+                    case PTR_FOP_EXP: x = expf(x); break;
+                    case PTR_FOP_LOG: x = logf(x); break;
+                    case PTR_FOP_SIN: x = sinf(x); break;
+                    case PTR_FOP_COS: x = cosf(x); break;
+                    case PTR_FOP_SQRT: x = sqrtf(x); break;
+                    case PTR_FOP_ABS: x = fabsf(x); break;
+                    case PTR_FOP_FLOOR: x = floorf(x); break;
+                    default: x = fract_(x); break;
+                }
+                r[k] = x;
+            }
+            st[sp - 1] = f3(r[0], r[1], r[2]);
+            continue;
+        }
+        if (op >= PTR_FOP_POW && op <= PTR_FOP_STEP) {
+            f3 b = st[--sp], a = st[sp - 1];
+            float ra[3] = {a.x, a.y, a.z}, rb[3] = {b.x, b.y, b.z};
+            for (int k = 0; k < 3; ++k) {
+                float x = ra[k], y = rb[k];
+                switch (op) {
+                    case PTR_FOP_POW: x = powf(x, y); break;
+                    case PTR_FOP_MIN: x = y < x ? y : x; break;
+                    case PTR_FOP_MAX: x = x < y ? y : x; break;
+                    case PTR_FOP_MOD: x = x - y * floorf(x / y); break;
+                    default: x = y < x ? 0.0f : 1.0f; break;   // step(edge = a, x = b)
+                }
+                ra[k] = x;
+            }
+            st[sp - 1] = f3(ra[0], ra[1], ra[2]);
+            continue;
+        }
+        if (op >= PTR_FOP_CLAMP && op <= PTR_FOP_SMOOTHSTEP) {
+            f3 c = st[--sp], b = st[--sp], a = st[sp - 1];
+            float ra[3] = {a.x, a.y, a.z}, rb[3] = {b.x, b.y, b.z}, rc[3] = {c.x, c.y, c.z};
+            for (int k = 0; k < 3; ++k) {
+                float x;
+                if (op == PTR_FOP_CLAMP) {
+                    x = ra[k] < rb[k] ? rb[k] : ra[k];
+                    x = rc[k] < x ? rc[k] : x;
+                } else if (op == PTR_FOP_MIX) {
+                    x = ra[k] * (1.0f - rc[k]) + rb[k] * rc[k];
+                } else {   // smoothstep(e0 = a, e1 = b, x = c)
+                    float t = (rc[k] - ra[k]) / (rb[k] - ra[k]);
+                    t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+                    x = t * t * (3.0f - 2.0f * t);
+                }
+                ra[k] = x;
+            }
+            st[sp - 1] = f3(ra[0], ra[1], ra[2]);
+            continue;
+        }
+        if (op == PTR_FOP_DOT) {
+            f3 b = st[--sp], a = st[sp - 1];
+            float d = dot(a, b);
+            st[sp - 1] = f3(d, d, d);
+            continue;
+        }
+        if (op == PTR_FOP_LENGTH) {
+            float l = sqrtf(dot(st[sp - 1], st[sp - 1]));
+            st[sp - 1] = f3(l, l, l);
+            continue;
+        }
+        // PTR_FOP_VEC3: three broadcast scalars into one vector
+        f3 z = st[--sp], y = st[--sp], x = st[sp - 1];
+        st[sp - 1] = f3(x.x, y.x, z.x);
+    }
+    return st[0];
+}
+__device__ __forceinline__ bool mat_is_het(const ptr_material& m) { return (m.field_a | m.field_s) != 0; }
+// The rendered medium at p: the fields (or constants), scaled down proportionally where the
+// maximum extinction exceeds the majorant (the D1 ceiling of the generated lookup).
+struct HetProps { f3 sa, ss; };
+__device__ __forceinline__ HetProps het_props(const DevScene& S, const ptr_material& m, f3 p) {
+    HetProps h;
+    h.sa = m.field_a ? field_eval(S.field_code + (m.field_a - 1), p) : ld3(m.sigma_a);
+    h.ss = m.field_s ? field_eval(S.field_code + (m.field_s - 1), p) : ld3(m.sigma_s);
+    f3 st = h.sa + h.ss;
+    float smax = gmax(st.x, gmax(st.y, st.z));
+    float scale = smax > m.majorant ? m.majorant / smax : 1.0f;
+    h.sa = h.sa * scale;
+    h.ss = h.ss * scale;
+    return h;
+}
+// The loop bound of a tracking walk of mean lambda tentative collisions (overrun chance
+// below 1e-10 for every lambda)
+__device__ __forceinline__ int tracking_cap(float lambda) {
+    return (int)ceilf(lambda + 6.5f * sqrtf(lambda) + 12.0f);
+}
+// Delta tracking of a scattering segment (Kutz et al. 2017, Algorithm 4, with the
+// history-aware average-based probabilities): xi are the site's two numbers, later
+// collisions draw from the path's stream.  Absorption terminates (weight 0).
+__device__ MediumSample<f3> medium_sample_delta(const DevScene& S, const ptr_material& m, const Ray& r, float t_max,
+                                                float x0, float x1, Rng& rng) {
+    MediumSample<f3> ms;
+    ms.scattered = false;
+    ms.weight = f3(1.0f);
+    const float sbar = m.majorant;
+    f3 w(1.0f);
+    float t = 0.0f, xd = x0, xe = x1;
+    const int cap = tracking_cap(sbar * t_max);
+    for (int i = 0; i < cap; ++i) {
+        t += -logf(1.0f - xd) / sbar;
+        if (t >= t_max) { ms.weight = w; return ms; }
+        f3 p = r.o + r.d * t;
+        HetProps h = het_props(S, m, p);
+        f3 sn = vmax(f3(sbar) - (h.sa + h.ss), f3(0.0f));
+        float pa = spectrum_average(h.sa * w);
+        float ps = spectrum_average(h.ss * w);
+        float pn = spectrum_average(sn * w);
+        float c = pa + ps + pn;
+        if (c <= 0.0f) { ms.weight = f3(0.0f); return ms; }
+        pa /= c; ps /= c; pn /= c;
+        if (xe < pa) { ms.weight = f3(0.0f); return ms; }
+        if (xe < pa + ps) {
+            ms.scattered = true;
+            ms.exit_p = p;
+            ms.exit_dir = r.d;
+            ms.weight = w * h.ss / (sbar * gmax(ps, 1e-20f));
+            return ms;
+        }
+        w = w * sn / (sbar * gmax(pn, 1e-20f));
+        xd = rng.next();
+        xe = rng.next();
+    }
+    ms.weight = w;
+    return ms;
+}
+// Ratio tracking of exp(-int sigma) along a segment (Novak et al. 2014): sigma_a alone
+// for the absorbing-only pass-through of the walk, sigma_t with pbrt's roulette (below
+// 0.05, survive 1/4 with weight 4) for shadow segments.
+__device__ f3 medium_ratio_track(const DevScene& S, const ptr_material& m, const Ray& r, float len, Rng& rng,
+                                 bool extinction) {
+    const float sbar = m.majorant;
+    f3 T(1.0f);
+    float t = 0.0f;
+    const int cap = tracking_cap(sbar * len);
+    for (int i = 0; i < cap; ++i) {
+        t += -logf(1.0f - rng.next()) / sbar;
+        if (t >= len) return T;
+        HetProps h = het_props(S, m, r.o + r.d * t);
+        T = T * (vmax(f3(sbar) - (extinction ? h.sa + h.ss : h.sa), f3(0.0f)) / sbar);
+        if (extinction && spectrum_max(T) < 0.05f) {
+            if (rng.next() < 0.75f) return f3(0.0f);
+            T = T / 0.25f;
+        }
+    }
+    return T;
+}
+// The shadow query's own stream: hashed from the path's sampler base and its dimension
+// at the NEE site, so a queued shadow query draws independently of the path's order.
+__device__ __forceinline__ Rng shadow_rng(uint32_t base, uint32_t seed) {
+    Rng r;
+    r.base = pcg4d(make_uint4(base, seed, 0x53484457u, 0u)).x;
+    r.dim = 0u;
+    return r;
+}
 template <class Col>
 __device__ __forceinline__ MediumSample<Col> medium_sample_analytic(Col sigma_a, Col sigma_s, const Ray& r, float t_max,
                                                                     float x0, float x1) {

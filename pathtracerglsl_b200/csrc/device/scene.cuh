@@ -62,7 +62,8 @@ struct DevScene {
     int inst_accel;           // PTR_ACCEL_* of the instanced batches' TLAS
     int flat_region = -1;     // the one acceleration region when every other region is analytic
                               // and there is no region BVH (refilling closest-hit loop), else -1
-    int pad_i1, pad_i2;
+    int has_het;              // some medium has a coefficient field (heterogeneous media)
+    int pad_i2;
     float sort_c[4];          // centre of the bounded geometry (ray-coherence keys)
     // environment
     int env_kind, env_samplable, env_select_live, env_w;
@@ -84,6 +85,8 @@ struct DevScene {
     // max.xyz, link), and the two trail words of every light
     const float4* light_tree;
     const uint2* light_trails;
+    // heterogeneous media: the coefficient fields' stack programs (NULL: none)
+    const uint32_t* field_code;
 };
 
 // ---- closed-form arms (components/geometry/*/*.glsl) ------------------------------------

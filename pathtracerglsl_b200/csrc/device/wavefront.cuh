@@ -32,6 +32,7 @@ struct PathPool {
     float4* rad;       // radiance.xyz, -
     float4* prev_q;    // stored light-query point (prev_query.p)
     float4* prev_n;    // stored light-query normal and two-sidedness (light-tree selection)
+    unsigned* sh_seed; // the shadow query's sampler dimension at its NEE site (heterogeneous media)
     int4* st;          // bounce, current_medium, null_crossings, prev_was_delta
     uint2* rng;        // sampler base, dimension
     float4* hit;       // t, u, v, - ; (region, element, prim) in hit_i
@@ -909,7 +910,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                     float x0 = rng.next();
                     float x1 = rng.next();
                     float t_max = boundary ? hr.t : kMaxDist;
-                    if (!scatter_live(S, P, med_mat)) {
+                    // heterogeneous media take the tracking arms (delta_tracking.glsl)
+                    const bool het = !SPECTRAL && S.has_het && mat_is_het(mm);
+                    if (!scatter_live(S, P, med_mat) && !het) {
                         thr = thr * vexp(-CM::sigma_a(S, med_mat, wl) * t_max);
                         if constexpr (ADJ) {   // w = exp(-(1-a) st t)
                             GreyMedium gm = grey_medium(mm);
@@ -917,8 +920,21 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             ga.scl(med_mat, PTR_GRAD_MEDIUM_ALBEDO, lrem, gm.st * t_max);
                         }
                     } else {
-                        MediumSample<Col> ms = medium_sample_analytic<Col>(CM::sigma_a(S, med_mat, wl), CM::sigma_s(S, med_mat, wl),
-                                                                           r, t_max, x0, x1);
+                        MediumSample<Col> ms;
+                        if constexpr (!SPECTRAL) {
+                            if (het && scatter_live(S, P, med_mat)) {
+                                ms = medium_sample_delta(S, mm, r, t_max, x0, x1, rng);
+                            } else if (het) {   // absorbing only: the ratio-tracked pass-through
+                                ms.scattered = false;
+                                ms.weight = medium_ratio_track(S, mm, r, t_max, rng, false);
+                            } else {
+                                ms = medium_sample_analytic<Col>(CM::sigma_a(S, med_mat, wl), CM::sigma_s(S, med_mat, wl),
+                                                                 r, t_max, x0, x1);
+                            }
+                        } else {
+                            ms = medium_sample_analytic<Col>(CM::sigma_a(S, med_mat, wl), CM::sigma_s(S, med_mat, wl),
+                                                             r, t_max, x0, x1);
+                        }
                         thr = thr * ms.weight;
                         if constexpr (ADJ) {   // scattered at t: w = a st exp(-st t)/pdf; passed: exp(-st t_max)/P
                             GreyMedium gm = grey_medium(mm);
@@ -942,6 +958,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     float y1 = rng.next();
                                     LightQuery lq{p_evt, f3(0.0f), false};   // no orientation at a medium event
                                     LightSample<Col> ls = lighting_sample<Col>(S, lq, y0, y1, rng, tree, wl);
+                                    if (S.has_het) pool.sh_seed[i] = rng.dim;
                                     if (ls.pdf > 0.0f) {
                                         f3 light_p = p_evt + ls.wi * ls.distance;
                                         float ph = hg_eval(ls.wi, wo_med, mm.phase_g);
@@ -976,9 +993,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 prev_q2 = false;
                                 r.o = p_evt;
                                 r.d = ps.wi;
-                                // roulette_interior (pt.ts:230-283)
+                                // roulette_interior (pt.ts:230-283); nothing is owed after a
+                                // tracking arm, whose lottery settled absorption already
                                 bool survive = true;
-                                if (P.rr_start >= 0 && bounce >= P.rr_start) {
+                                if (P.rr_start >= 0 && bounce >= P.rr_start && !het) {
                                     Col ss = CM::sigma_s(S, med_mat, wl), sa = CM::sigma_a(S, med_mat, wl);
                                     Col surv = ss / vmax(ss + sa, Col(1e-9f));
                                     float p_survive = spectrum_max(surv);
@@ -1052,6 +1070,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 float y1 = rng.next();
                                 LightQuery lq{hit.p, hit.frame.n, rough};   // rough glass: sphere support
                                 LightSample<Col> ls = lighting_sample<Col>(S, lq, y0, y1, rng, tree, wl);
+                                if (MEDIA && S.has_het) pool.sh_seed[i] = rng.dim;
                                 if (ls.pdf > 0.0f) {
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
@@ -1329,6 +1348,8 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
             f3 light_p = xyz(lp);
             int crossings_left = __float_as_int(sd.w);
             Col T(1.0f);
+            Rng srng;
+            bool srng_live = false;
             int medium = scene_region_at(S, sr.o);
             Ray seg = sr;
             bool finished = false;
@@ -1340,7 +1361,16 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 float seg_len = hit_boundary ? hr.t : remaining;
                 int med_mat = material_of(S, medium);
                 if (mat_has_medium(S, med_mat)) {
-                    T = T * medium_transmittance<Col>(S, P, med_mat, seg_len, wl);
+                    bool het = false;
+                    if constexpr (!SPECTRAL) {
+                        const ptr_material& smm = S.materials[med_mat];
+                        if (S.has_het && mat_is_het(smm)) {   // ratio tracking on the query's own stream
+                            het = true;
+                            if (!srng_live) { srng = shadow_rng(pool.rng[i].x, pool.sh_seed[i]); srng_live = true; }
+                            T = T * medium_ratio_track(S, smm, seg, seg_len, srng, scatter_live(S, P, med_mat));
+                        }
+                    }
+                    if (!het) T = T * medium_transmittance<Col>(S, P, med_mat, seg_len, wl);
                     if constexpr (ADJ) {
                         int e = 0;
                         while (e < n_mm && mm_id[e] != med_mat) e++;

@@ -204,7 +204,7 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
     int rc = PTR_OK;
     if ((rc = get(c * 16, (void**)&q.ray_o)) || (rc = get(c * 16, (void**)&q.ray_d)) ||
         (rc = get(c * 16, (void**)&q.thr)) || (rc = get(c * 16, (void**)&q.rad)) ||
-        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.prev_n)) || (rc = get(c * 16, (void**)&q.st)) ||
+        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.prev_n)) || (rc = get(c * 4, (void**)&q.sh_seed)) || (rc = get(c * 16, (void**)&q.st)) ||
         (rc = get(c * 8, (void**)&q.rng)) || (rc = get(c * 16, (void**)&q.hit)) ||
         (rc = get(c * 16, (void**)&q.hit_i)) || (rc = get(c * 16, (void**)&q.sh_o)) ||
         (rc = get(c * 16, (void**)&q.sh_d)) || (rc = get(c * 16, (void**)&q.sh_lp)) ||
@@ -856,6 +856,10 @@ int check_equiangular(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
         return fail(ctx, PTR_E_INVALID, "lightSelection 'bvh' needs a scene uploaded with its light tree");
     if (p->desc.light_tree && p->desc.equiangular)
         return fail(ctx, PTR_E_INVALID, "lightSelection 'bvh' with mediumLightSampling 'equiangular' is reserved");
+    if (s->dev.has_het && p->desc.equiangular)
+        return fail(ctx, PTR_E_INVALID, "equiangular sampling through heterogeneous media is not available");
+    if (s->dev.has_het && p->desc.color == PTR_COLOR_SPECTRAL)
+        return fail(ctx, PTR_E_UNSUPPORTED, "heterogeneous media render in RGB only");
     if (!p->desc.equiangular) return PTR_OK;
     if (s->n_lights == 0) return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' needs at least one light");
     if (p->desc.equiangular == PTR_EQUIANGULAR_DELTA && s->n_delta_lights != s->n_lights)
@@ -1177,6 +1181,37 @@ int ptr_destroy(ptr_ctx* ctx) {
 
 const char* ptr_last_error(const ptr_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+namespace {
+// A field program is safe to interpret: known opcodes with their immediates inside the
+// table, every pop backed by the stack, the stack within PTR_FIELD_MAX_STACK, and END
+// reached with exactly one value.
+bool field_program_ok(const uint32_t* code, int n, int start) {
+    if (start < 0 || start >= n) return false;
+    int sp = 0;
+    for (int pc = start; pc < n;) {
+        const uint32_t op = code[pc++];
+        int pop = 0, push = 0;
+        switch (op) {
+            case PTR_FOP_END: return sp == 1;
+            case PTR_FOP_CONST: if (pc + 3 > n) return false; pc += 3; push = 1; break;
+            case PTR_FOP_P: push = 1; break;
+            case PTR_FOP_SWZ: if (pc + 1 > n || code[pc] > 2u) return false; pc += 1; pop = 1; push = 1; break;
+            case PTR_FOP_ADD: case PTR_FOP_SUB: case PTR_FOP_MUL: case PTR_FOP_DIV:
+            case PTR_FOP_POW: case PTR_FOP_MIN: case PTR_FOP_MAX: case PTR_FOP_MOD: case PTR_FOP_STEP:
+            case PTR_FOP_DOT: pop = 2; push = 1; break;
+            case PTR_FOP_CLAMP: case PTR_FOP_MIX: case PTR_FOP_SMOOTHSTEP: case PTR_FOP_VEC3: pop = 3; push = 1; break;
+            default:
+                if (op >= PTR_FOP_COUNT) return false;
+                pop = 1; push = 1;   // the unary built-ins and LENGTH
+        }
+        if (sp < pop) return false;
+        sp += push - pop;
+        if (sp > PTR_FIELD_MAX_STACK) return false;
+    }
+    return false;
+}
+}  // namespace
+
 int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
     *out = nullptr;
@@ -1204,6 +1239,17 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         }
     }
     if (d->ambient_material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: ambient material out of range");
+    bool has_het = false;
+    for (int i = 0; i < d->n_materials; ++i) {
+        const ptr_material& m = d->materials[i];
+        if (!m.field_a && !m.field_s) continue;
+        has_het = true;
+        if (!(m.flags & PTR_MATF_MEDIUM) || !(m.majorant > 0.0f) || !std::isfinite(m.majorant) || !d->field_code ||
+            (m.field_a && !field_program_ok(d->field_code, d->n_field_code, m.field_a - 1)) ||
+            (m.field_s && !field_program_ok(d->field_code, d->n_field_code, m.field_s - 1)))
+            return fail(ctx, PTR_E_INVALID, "scene: material " + std::to_string(i) +
+                                                " has a malformed coefficient field or no positive majorant");
+    }
     for (int b = 0; b < d->n_batches; ++b) {
         const ptr_batch_desc& bd = d->batches[b];
         if (bd.light_base >= 0 && ((long long)bd.light_base + bd.n_instances > d->n_lights || bd.prototype_shape != PTR_SHAPE_SPHERE))
@@ -1252,6 +1298,12 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     }
     S.light_tree = nullptr;
     S.light_trails = nullptr;
+    S.field_code = nullptr;
+    S.has_het = has_het ? 1 : 0;
+    if (has_het && (rc = dev_copy(ctx, s->allocs, d->field_code, (size_t)d->n_field_code, &S.field_code))) {
+        ptr_free_scene(s);
+        return rc;
+    }
     if (d->n_tree_nodes > 0 &&
         ((rc = dev_copy(ctx, s->allocs, (const float4*)d->light_tree, 2 * (size_t)d->n_tree_nodes, &S.light_tree)) ||
          (rc = dev_copy(ctx, s->allocs, (const uint2*)d->light_trails, (size_t)d->n_lights, &S.light_trails)))) {
@@ -1649,6 +1701,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     if (n_mat > 512) return fail(ctx, PTR_E_INVALID, "ptr_backward: at most 512 materials");
     if (p->desc.equiangular) return fail(ctx, PTR_E_INVALID, "ptr_backward: equiangular programs are not differentiated");
     if (p->desc.light_tree) return fail(ctx, PTR_E_INVALID, "ptr_backward: light-tree programs are not differentiated");
+    if (s->dev.has_het) return fail(ctx, PTR_E_INVALID, "ptr_backward: scenes with heterogeneous media are not differentiated");
     if (p->desc.color != PTR_COLOR_RGB) return fail(ctx, PTR_E_INVALID, "ptr_backward: the adjoint is RGB only");
     for (const ptr_material& m : s->h_materials)
         if ((m.flags & PTR_MATF_MEDIUM) && !(m.sigma_a[0] == m.sigma_a[1] && m.sigma_a[0] == m.sigma_a[2] &&
@@ -1728,8 +1781,10 @@ int ptr_update_params(ptr_scene* s, const ptr_material* materials, int n_materia
     ptr_ctx* ctx = s->ctx;
     if (n_materials != (int)s->h_materials.size()) return fail(ctx, PTR_E_INVALID, "ptr_update_params: material count differs from the uploaded scene");
     for (int i = 0; i < n_materials; ++i)
-        if (materials[i].model != s->h_materials[i].model || materials[i].flags != s->h_materials[i].flags)
-            return fail(ctx, PTR_E_INVALID, "ptr_update_params: a material's model or flags changed");
+        if (materials[i].model != s->h_materials[i].model || materials[i].flags != s->h_materials[i].flags ||
+            materials[i].field_a != s->h_materials[i].field_a || materials[i].field_s != s->h_materials[i].field_s ||
+            ((materials[i].field_a || materials[i].field_s) && !(materials[i].majorant > 0.0f && std::isfinite(materials[i].majorant))))
+            return fail(ctx, PTR_E_INVALID, "ptr_update_params: a material's model, flags or coefficient fields changed");
     if (regions) {
         if (n_regions != (int)s->h_regions.size()) return fail(ctx, PTR_E_INVALID, "ptr_update_params: region count differs from the uploaded scene");
         for (int i = 0; i < n_regions; ++i) {
@@ -1957,7 +2012,7 @@ PathPool na_pool(unsigned char* base) {
     unsigned char* p = base + kNaPool;
     auto take = [&](size_t bytes) { unsigned char* r = p; p += bytes * c; return (void*)r; };
     q.ray_o = (float4*)take(16); q.ray_d = (float4*)take(16); q.thr = (float4*)take(16);
-    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.prev_n = nullptr; q.st = (int4*)take(16);
+    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.prev_n = nullptr; q.sh_seed = nullptr; q.st = (int4*)take(16);
     q.hit = (float4*)take(16); q.hit_i = (int4*)take(16); q.sh_o = (float4*)take(16);
     q.sh_d = (float4*)take(16); q.sh_lp = (float4*)take(16); q.sh_c = (float4*)take(16);
     q.rng = (uint2*)take(8); q.q[0] = (int*)take(4); q.q[1] = (int*)take(4); q.shq = (int*)take(4);
@@ -1979,7 +2034,7 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
                      kNoAllocMaxTable);
         return PTR_E_INVALID;
     }
-    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE || d->n_tree_nodes != 0 || pd->light_tree) {
+    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE || d->n_tree_nodes != 0 || pd->light_tree || d->n_field_code != 0) {
         std::fprintf(stderr, "ptr_render_noalloc: only analytic scenes with a constant or no environment and power or uniform light selection are supported\n");
         return PTR_E_UNSUPPORTED;
     }

@@ -131,6 +131,46 @@ def many_lights(direct="mis", selection="bvh", n=64, seed=0, fog=False, max_dept
     return scene, strategy
 
 
+def het_fog(direct="nee", kind="ground", max_depth=12, rr_start=4):
+    """Heterogeneous media in the Cornell walls (the reference's groundfog and fogblobs
+    demos, as closed rooms):
+    ``ground``: ambient ground fog sigma_s(p) = gain exp(-falloff y)(0.6 + 0.4 sin 4x sin 4z),
+    gain 1.2, falloff 1.5, majorant 2.0 (delta tracking, ratio-tracked shadows);
+    ``blobs``: two merging coloured Gaussian puffs inside a null-interface sphere, majorant 6
+    (the field exceeds it at the puff centres: the clamped, rendered medium);
+    ``absorb``: an absorbing-only field sigma_a(p) = 0.8 (1 + sin 3x) / 2 + 0.1 filling the
+    room (the ratio-tracked pass-through).
+    The ceiling quad light and a point light light the room."""
+    scene, strategy = cornell(direct, max_depth, rr_start)
+    objects = list(scene["objects"][:5]) + [
+        {"type": "sphere", "parameters": {"center": [0.5, 0.3, 0.2], "radius": 0.3}, "material": "matte"}]
+    materials = {k: scene["materials"][k] for k in ("white", "red", "green", "matte")}
+    lights = [dict(scene["lights"][0], emission=12.0), {"kind": "point", "position": [-0.5, 1.5, 0.4], "emission": 1.5}]
+    scene = dict(scene, id="het-" + kind, objects=objects, materials=materials, lights=lights)
+    if kind == "ground":
+        materials["fog"] = {"model": "none", "medium": {
+            "sigma_a": [0.02, 0.02, 0.02],
+            "sigma_s": {"kind": "glsl", "source": "u_fog_gain * exp(-u_fog_falloff * p.y) * (0.6 + 0.4 * sin(4.0 * p.x) * sin(4.0 * p.z))",
+                        "params": [{"param": "fog.gain", "default": 1.2}, {"param": "fog.falloff", "default": 1.5}]},
+            "majorant": 2.0, "phase_g": 0.3}}
+        scene["ambientMedium"] = "fog"
+    elif kind == "blobs":
+        src = ("vec3(1.0, 0.7, 0.4) * u_blob_gain * (exp(-u_blob_sharp * dot(p - vec3(-0.25, 1.1, -0.2), p - vec3(-0.25, 1.1, -0.2)))"
+               " + exp(-u_blob_sharp * dot(p - vec3(0.2, 0.9, -0.2), p - vec3(0.2, 0.9, -0.2))))")
+        materials["puff"] = {"model": "none", "medium": {
+            "sigma_a": [0.05, 0.05, 0.05],
+            "sigma_s": {"kind": "glsl", "source": src,
+                        "params": [{"param": "blob.gain", "default": 6.0}, {"param": "blob.sharp", "default": 14.0}]},
+            "majorant": 6.0, "phase_g": 0.2}}
+        objects.append({"type": "sphere", "parameters": {"center": [0.0, 1.0, -0.2], "radius": 0.65}, "material": "puff"})
+    else:
+        materials["smoke"] = {"model": "none", "medium": {
+            "sigma_a": {"kind": "glsl", "source": "0.8 * (1.0 + sin(3.0 * p.x)) * 0.5 + 0.1"}, "majorant": 1.0}}
+        scene["ambientMedium"] = "smoke"
+    strategy = dict(strategy, estimator=dict(strategy["estimator"], volumeSampling="delta-tracking"))
+    return scene, strategy
+
+
 def furnace(direct="mis", max_depth=8):
     scene = {
         "id": "furnace-c1",

@@ -105,6 +105,30 @@ def test_light_tree_matches_oracle(engine, oracle_lib, case):
     compare(engine, oracle_lib, sc, st, 48, 48, 8, CASE_CAMERAS["cornell"])
 
 
+@pytest.mark.parametrize("kind,direct", [("ground", "nee"), ("ground", "mis"), ("blobs", "mis"), ("absorb", "nee")])
+def test_heterogeneous_media_match_oracle(engine, oracle_lib, kind, direct):
+    """Delta tracking (scattering fields, the D1 clamp at the puff centres), the
+    ratio-tracked pass-through (absorbing field) and ratio-tracked shadow segments on the
+    queries' own streams, against the oracle sample by sample.  The fields' exp/sin run on
+    CUDA's and the host's libm, so a rare lottery may fall differently: 98 % of samples."""
+    sc, st = scenes.het_fog(direct=direct, kind=kind)
+    compare(engine, oracle_lib, sc, st, 40, 40, 8, CASE_CAMERAS["cornell"], frac_samples=0.98)
+
+
+def test_upload_rejects_malformed_field_programs(engine):
+    """The upload validator refuses field programs that would leave their stack or table,
+    before anything reaches the device."""
+    from pathtracerglsl_b200 import field
+    sc, st = scenes.het_fog(kind="absorb")
+    _, pk = Compiler().compile(sc, st)
+    ops = field.OPS
+    for bad in ([ops["ADD"], ops["END"]], [ops["P"]] * 17 + [ops["END"]], [ops["CONST"], 0],
+                [ops["P"], ops["SWZ"], 7, ops["END"]], [99, ops["END"]], [ops["P"]]):
+        pk.field_code = np.asarray(bad, np.uint32)
+        with pytest.raises(Exception, match="coefficient field"):
+            engine.register_scene(pk)
+
+
 def test_furnace_variant_value(engine, oracle_lib):
     sc, st = scenes.furnace()
     compare(engine, oracle_lib, sc, st, 32, 32, 16, {})

@@ -23,6 +23,7 @@ CASES = {
     "cornell-rough": (lambda: scenes.cornell_rough(direct="mis"), {}, (48, 40, 4)),
     "cornell-mesh-light": (lambda: scenes.cornell_mesh_light(direct="mis", emitter="sphere"), {}, (48, 40, 4)),
     "many-lights-tree": (lambda: scenes.many_lights(direct="mis", selection="bvh"), {}, (48, 40, 4)),
+    "het-blobs": (lambda: scenes.het_fog(direct="mis", kind="blobs"), {}, (40, 40, 4)),
     "fog-area-mis": (lambda: (ref_scenes.FOG_AREA, ref_scenes.FOG_AREA_MIS),
                      {"camera.position": [0, 1, 4], "camera.target": [0, 1, 0], "camera.fov": 0.8}, (40, 30, 4)),
     "media-spectral": (lambda: scenes.media_scene()[:2], {}, (40, 40, 4)),
