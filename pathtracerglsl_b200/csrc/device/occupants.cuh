@@ -459,7 +459,7 @@ __device__ __forceinline__ float sphere_omc_max(float r, float dc2) {
 // area exceeds x0 (a zero-area triangle is never picked), x0 rescaled within its span, a
 // uniform point by the square-root map; n is the unit winding normal cross(b-a, c-a),
 // NaN for a triangle degenerate in float32.
-__device__ __forceinline__ f3 mesh_light_point(const DevScene& S, const ptr_light& l, float x0, float x1, f3& n) {
+__device__ __noinline__ f3 mesh_light_point(const DevScene& S, const ptr_light& l, float x0, float x1, f3& n) {
     const DevMesh& m = S.meshes[(int)l.p[0]];
     const float* cdf = m.light_cdf;
     int lo = 0, hi = m.n_tris - 1;

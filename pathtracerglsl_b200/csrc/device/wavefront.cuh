@@ -861,10 +861,6 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             int4 st = pool.st[i];
             int bounce = st.x, cur_med = st.y, nulls = st.z;
             bool prev_delta = st.w != 0;
-            // the stored selection context's normal and sidedness (light-tree selection)
-            float4 pqn = (tree && !prev_delta) ? pool.prev_n[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            f3 prev_qn = xyz(pqn);
-            bool prev_q2 = pqn.w != 0.0f;
             uint2 rs = pool.rng[i];
             Rng rng;
             rng.base = rs.x;
@@ -989,8 +985,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 prev_delta = false;
                                 prev_bsdf_pdf = ps.pdf;
                                 prev_qp = p_evt;
-                                prev_qn = f3(0.0f);
-                                prev_q2 = false;
+                                if (tree) pool.prev_n[i] = make_float4(0.f, 0.f, 0.f, 0.f);   // no orientation
                                 r.o = p_evt;
                                 r.d = ps.wi;
                                 // roulette_interior (pt.ts:230-283); nothing is owed after a
@@ -1046,8 +1041,17 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 int lid = hit.region_to >= 0 ? emitter_light(S, hit) : -1;
                                 if (lid >= 0 && !prev_delta) {
                                     if (!mis) w = 0.0f;
-                                    else w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, LightQuery{prev_qp, prev_qn, prev_q2}, r.d, lid,
-                                                                                         hit.p, hit.ng, tree));
+                                    else {
+                                        // the stored selection context (its normal and sidedness
+                                        // only under light-tree selection)
+                                        LightQuery pq{prev_qp, f3(0.0f), false};
+                                        if (tree) {
+                                            float4 pqn = pool.prev_n[i];
+                                            pq.n = xyz(pqn);
+                                            pq.two_sided = pqn.w != 0.0f;
+                                        }
+                                        w = power_heuristic(prev_bsdf_pdf, lighting_pdf(S, pq, r.d, lid, hit.p, hit.ng, tree));
+                                    }
                                 }
                             }
                             Col e = thr * w * CM::emission(S, mat_emit, wl);
@@ -1144,8 +1148,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 prev_delta = (bs.flags & kLobeDelta) != 0u;
                                 prev_bsdf_pdf = bs.pdf;
                                 prev_qp = hit.p;
-                                prev_qn = hit.frame.n;
-                                prev_q2 = rough;
+                                if (tree) pool.prev_n[i] = f4(hit.frame.n, rough ? 1.0f : 0.0f);
                                 if (bs.flags & kLobeTransmission) {
                                     if (MEDIA) cur_med = hit.region_to;
                                     float rr = ior_of(S, hit.region_to) / ior_of(S, hit.region_from);
@@ -1192,7 +1195,6 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                 pool.ray_d[i] = f4(r.d, eta_scale);
                 pool.thr[i] = col_st(thr, 0.0f);
                 pool.prev_q[i] = f4(prev_qp, 0.0f);
-                if (tree) pool.prev_n[i] = f4(prev_qn, prev_q2 ? 1.0f : 0.0f);
                 pool.st[i] = make_int4(bounce, cur_med, nulls, prev_delta ? 1 : 0);
                 pool.rng[i] = make_uint2(rng.base, rng.dim);
             }
