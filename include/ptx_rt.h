@@ -256,8 +256,16 @@ typedef struct ptr_program_desc {
                                    'tlas' binary, 'cwbvh' wide; intersection/index.ts:68-159) */
     int32_t light_tree;         /* estimator.lightSelection 'bvh': the scene's light tree
                                    selects (stochastic descent, trail-replayed pmf)      */
-    int32_t pad;
+    int32_t aovs;               /* measurement.aovs (components/aov): PTR_AOV_* bits; each
+                                   is read with ptr_read_export("albedo" / "normal")     */
 } ptr_program_desc;
+/* First-hit pictures (denoiser guides): at the first non-null surface a path reaches
+ * before any scattering event, the material's albedo fact clamped to [0, 1] (lambert
+ * albedo, dielectrics' transmittance, GGX / mirror f0) times the path's throughput, and
+ * the shading normal faced toward the arriving ray times the throughput's channel mean;
+ * 0 otherwise.  RGB programs only. */
+#define PTR_AOV_ALBEDO 1
+#define PTR_AOV_NORMAL 2
 
 /* The per-frame builtins + camera uniforms (Engine.ts:231-258, camera.ts:69-160). */
 typedef struct ptr_camera {

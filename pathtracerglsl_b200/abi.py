@@ -109,7 +109,9 @@ class ProgramDesc(C.Structure):
                 ("rr_max_survival", C.c_float), ("scattering", C.c_int32), ("accel", C.c_int32),
                 ("equiangular", C.c_int32), ("color", C.c_int32), ("wavelengths", C.c_int32),
                 ("lambda_min", C.c_float), ("lambda_max", C.c_float), ("instance_accel", C.c_int32),
-                ("light_tree", C.c_int32), ("pad", C.c_int32)]
+                ("light_tree", C.c_int32), ("aovs", C.c_int32)]
+
+AOV_ALBEDO, AOV_NORMAL = 1, 2
 
 
 class Camera(C.Structure):

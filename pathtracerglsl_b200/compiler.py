@@ -378,6 +378,11 @@ class Compiler:
                     medium_field.compile_field(med[k], {})
                 except medium_field.FieldError as e:
                     bag.error("invalid-medium", f"Material '{name}': medium.{k}: {e}")
+        aovs = meas.get("aovs") or []
+        if any(a not in ("albedo", "normal") for a in aovs) or len(set(aovs)) != len(aovs):
+            bag.error("invalid-setting", f"measurement.aovs {aovs!r}: each of albedo, normal at most once")
+        if aovs and meas.get("color", "rgb") == "spectral":
+            bag.error("unsupported", "measurement.aovs are RGB only")
         sel = est.get("lightSelection", "power")
         if sel not in ("power", "uniform", "bvh"):
             bag.error("invalid-setting", f"estimator.lightSelection {sel!r} (available: power, uniform, bvh)")
@@ -872,6 +877,7 @@ class Compiler:
         prog.wavelengths = abi.WAVELENGTHS_UNIFORM if est.get("wavelengths") == "uniform" else abi.WAVELENGTHS_VISIBLE
         lo, hi = meas.get("wavelengthRange", [360.0, 830.0])
         prog.lambda_min, prog.lambda_max = float(lo), float(hi)
+        prog.aovs = sum({"albedo": abi.AOV_ALBEDO, "normal": abi.AOV_NORMAL}[a] for a in set(meas.get("aovs") or []))
         prog.light_tree = int(est.get("lightSelection") == "bvh" and prog.direct != abi.DIRECT_NONE
                               and getattr(data, "light_tree", None) is not None)
         prog.equiangular = abi.EQUIANGULAR_OFF
@@ -887,6 +893,8 @@ class Compiler:
         }
         rid = f"{st.get('id', 'strategy')}-{scene.get('id', 'scene')}"
         exports = {"radiance": {"format": "float"}, "variance": {"format": "float"}}
+        for a in meas.get("aovs") or []:   # first-hit pictures (components/aov)
+            exports[a] = {"format": "float"}
         return CompiledRenderer(rid, prog, st, parameters, exports)
 
 

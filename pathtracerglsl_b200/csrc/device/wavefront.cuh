@@ -33,6 +33,11 @@ struct PathPool {
     float4* prev_q;    // stored light-query point (prev_query.p)
     float4* prev_n;    // stored light-query normal and two-sidedness (light-tree selection)
     unsigned* sh_seed; // the shadow query's sampler dimension at its NEE site (heterogeneous media)
+    // first-hit pictures (programs with measurement.aovs; NULL otherwise): per path its
+    // albedo and normal samples (2 float4), per pixel their FP64 sums (albedo block of 3
+    // doubles per pixel, then the normal block)
+    float4* aov;
+    double* aov_sum;
     int4* st;          // bounce, current_medium, null_crossings, prev_was_delta
     uint2* rng;        // sampler base, dimension
     float4* hit;       // t, u, v, - ; (region, element, prim) in hit_i
@@ -473,6 +478,7 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, Adj
         pool.prev_q[i] = f4(o, 0.0f);
         pool.st[i] = make_int4(0, medium, 0, 1);
         pool.rng[i] = make_uint2(rng.base, rng.dim);
+        if (pool.aov) { pool.aov[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f); pool.aov[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f); }
         pool.q[0][i] = (int)i;
     }
 }
@@ -1033,6 +1039,19 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                         else alive = true;
                     } else {
                         f3 wo = -r.d;
+                        // the AOV capture (pt.ts:422-433): the first non-null surface before
+                        // any event, weighted by the arrival throughput
+                        if constexpr (!SPECTRAL) {
+                            if (bounce == 0 && pool.aov) {
+                                f3 fact = PTR_IS_MAT(m, PTR_MAT_LAMBERT) ? ld3(m.albedo)
+                                        : (PTR_IS_MAT(m, PTR_MAT_GGX) || PTR_IS_MAT(m, PTR_MAT_MIRROR)) ? ld3(m.f0)
+                                                                                                        : ld3(m.transmittance);
+                                fact = vmin(vmax(fact, f3(0.0f)), f3(1.0f));
+                                f3 nf = dot(hit.frame.n, wo) < 0.0f ? -hit.frame.n : hit.frame.n;
+                                pool.aov[2 * i] = f4(fact * thr, 0.0f);
+                                pool.aov[2 * i + 1] = f4(nf * spectrum_average(thr), 0.0f);
+                            }
+                        }
                         // kernel_score_emitter_hit (kernel.glsl:16-25; combiner.ts:27-46)
                         int mat_emit = material_of(S, hit.region_to);
                         if (mat_emit >= 0 && (S.materials[mat_emit].flags & PTR_MATF_EMISSIVE)) {
@@ -1454,6 +1473,18 @@ __global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double
         }
         sum[3 * pix + 0] = s0; sum[3 * pix + 1] = s1; sum[3 * pix + 2] = s2;
         sumsq[3 * pix + 0] = q0; sumsq[3 * pix + 1] = q1; sumsq[3 * pix + 2] = q2;
+        if (pool.aov_sum) {   // the first-hit pictures, in the same sample order
+            double* as = pool.aov_sum + 3 * (size_t)pix;
+            double* ns = pool.aov_sum + 3 * ((size_t)npix + pix);
+            double a0 = as[0], a1 = as[1], a2 = as[2], n0 = ns[0], n1 = ns[1], n2 = ns[2];
+            for (long long i = j; i < n; i += npix) {
+                float4 a = pool.aov[2 * i], b = pool.aov[2 * i + 1];
+                a0 += (double)a.x; a1 += (double)a.y; a2 += (double)a.z;
+                n0 += (double)b.x; n1 += (double)b.y; n2 += (double)b.z;
+            }
+            as[0] = a0; as[1] = a1; as[2] = a2;
+            ns[0] = n0; ns[1] = n1; ns[2] = n2;
+        }
     }
 }
 

@@ -70,6 +70,8 @@ struct ptr_program {
     int fw = 0, fh = 0;
     double* sum = nullptr;
     double* sumsq = nullptr;
+    double* aov_sum = nullptr;   // first-hit pictures: 6 doubles per pixel (programs with aovs)
+    size_t aov_n = 0;
     double nsamples = 0.0;
     float* export_buf = nullptr;
     // path pool
@@ -820,6 +822,24 @@ int upload_region_bvh(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     return PTR_OK;
 }
 
+// The first-hit pictures' FP64 sums (programs with AOVs), sized and cleared with the film.
+int prepare_aov_film(ptr_program* p, const ptr_frame* f, size_t npix, cudaStream_t st) {
+    ptr_ctx* ctx = p->ctx;
+    if (p->desc.aovs) {
+        if (!p->aov_sum || p->aov_n != npix) {
+            if (p->aov_sum) cudaFree(p->aov_sum);
+            p->aov_sum = nullptr;
+            if (cudaMalloc(&p->aov_sum, npix * 6 * sizeof(double)) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, "AOV film allocation failed");
+            p->aov_n = npix;
+            CK(ctx, cudaMemsetAsync(p->aov_sum, 0, npix * 6 * sizeof(double), st));
+        } else if (!f->accumulate) {
+            CK(ctx, cudaMemsetAsync(p->aov_sum, 0, npix * 6 * sizeof(double), st));
+        }
+        p->pool.aov_sum = p->aov_sum;
+    }
+    return PTR_OK;
+}
+
 // Size (and clear unless accumulating) a program's FP64 film for a frame.
 int prepare_film(ptr_program* p, const ptr_frame* f, cudaStream_t st) {
     ptr_ctx* ctx = p->ctx;
@@ -844,6 +864,7 @@ int prepare_film(ptr_program* p, const ptr_frame* f, cudaStream_t st) {
         CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
         CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
     }
+    if (int rc = prepare_aov_film(p, f, npix, st)) return rc;
     return PTR_OK;
 }
 
@@ -860,6 +881,9 @@ int check_equiangular(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* s) {
         return fail(ctx, PTR_E_INVALID, "equiangular sampling through heterogeneous media is not available");
     if (s->dev.has_het && p->desc.color == PTR_COLOR_SPECTRAL)
         return fail(ctx, PTR_E_UNSUPPORTED, "heterogeneous media render in RGB only");
+    if (p->desc.aovs && p->desc.color == PTR_COLOR_SPECTRAL)
+        return fail(ctx, PTR_E_UNSUPPORTED, "AOVs are RGB only");
+    if (p->desc.aovs & ~(PTR_AOV_ALBEDO | PTR_AOV_NORMAL)) return fail(ctx, PTR_E_INVALID, "unknown AOV bits");
     if (!p->desc.equiangular) return PTR_OK;
     if (s->n_lights == 0) return fail(ctx, PTR_E_INVALID, "mediumLightSampling 'equiangular' needs at least one light");
     if (p->desc.equiangular == PTR_EQUIANGULAR_DELTA && s->n_delta_lights != s->n_lights)
@@ -905,6 +929,7 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
         CK(ctx, cudaMemsetAsync(p->sum, 0, npix * 3 * sizeof(double), st));
         CK(ctx, cudaMemsetAsync(p->sumsq, 0, npix * 3 * sizeof(double), st));
     }
+    if (int rc = prepare_aov_film(p, f, npix, st)) return rc;
     const long long total = (long long)npix * f->spp;
     // capacity: whole sample passes when a pass fits the pool, else a chunk of pixels
     long long cap_max = ctx->tune.capacity > 0 ? ctx->tune.capacity : (1ll << 24);
@@ -921,6 +946,14 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
                             p->pool.l_rem != nullptr, spectral || p->pool.wl);
         if (rc) return rc;
     }
+    if (p->desc.aovs && !p->pool.aov) {   // two float4 per path slot; a captured graph predates them
+        void* a = nullptr;
+        if (cudaMalloc(&a, (size_t)p->capacity * 32) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, "AOV pool allocation failed");
+        p->pool_allocs.push_back(a);
+        p->pool.aov = (float4*)a;
+        if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+    }
+    p->pool.aov_sum = p->desc.aovs ? p->aov_sum : nullptr;
     if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
     // The frame's parameters travel as a kernel argument into a device block: no host
     // synchronisation, and the captured graph (which reads the block) stays valid.
@@ -1450,6 +1483,7 @@ int ptr_free_program(ptr_program* p) {
     free_pool(p);
     if (p->sum) cudaFree(p->sum);
     if (p->sumsq) cudaFree(p->sumsq);
+    if (p->aov_sum) cudaFree(p->aov_sum);
     if (p->export_buf) cudaFree(p->export_buf);
     if (p->fp_dev) cudaFree(p->fp_dev);
     if (p->work_dev) cudaFree(p->work_dev);
@@ -1482,6 +1516,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         if (J.prog->desc.color != PTR_COLOR_RGB)
             return fail(ctx, PTR_E_UNSUPPORTED, "ptr_render_batch: spectral programs render one per launch (ptr_render)");
         if (int rc = check_equiangular(ctx, J.prog, J.scene)) return rc;
+        if (J.prog->desc.aovs) return fail(ctx, PTR_E_INVALID, "batched renders do not take programs with AOVs");
         for (int k = 0; k < j; ++k)
             if (jobs[k].prog == J.prog)
                 return fail(ctx, PTR_E_INVALID, "ptr_render_batch: jobs " + std::to_string(k) + " and " + std::to_string(j) + " share a program (one film per job)");
@@ -1701,6 +1736,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     if (n_mat > 512) return fail(ctx, PTR_E_INVALID, "ptr_backward: at most 512 materials");
     if (p->desc.equiangular) return fail(ctx, PTR_E_INVALID, "ptr_backward: equiangular programs are not differentiated");
     if (p->desc.light_tree) return fail(ctx, PTR_E_INVALID, "ptr_backward: light-tree programs are not differentiated");
+    if (p->desc.aovs) return fail(ctx, PTR_E_INVALID, "ptr_backward: programs with AOVs are not differentiated");
     if (s->dev.has_het) return fail(ctx, PTR_E_INVALID, "ptr_backward: scenes with heterogeneous media are not differentiated");
     if (p->desc.color != PTR_COLOR_RGB) return fail(ctx, PTR_E_INVALID, "ptr_backward: the adjoint is RGB only");
     for (const ptr_material& m : s->h_materials)
@@ -1877,10 +1913,13 @@ static int export_impl(ptr_program* p, const char* name, float* dst, size_t n, b
     int what;
     if (std::strcmp(name, "radiance") == 0) what = 0;
     else if (std::strcmp(name, "variance") == 0) what = 1;
+    else if (std::strcmp(name, "albedo") == 0 && (p->desc.aovs & PTR_AOV_ALBEDO) && p->aov_sum) what = 2;
+    else if (std::strcmp(name, "normal") == 0 && (p->desc.aovs & PTR_AOV_NORMAL) && p->aov_sum) what = 3;
     else return fail(ctx, PTR_E_INVALID, std::string("export: unknown export '") + name + "'");
     if (n < npix * 3) return fail(ctx, PTR_E_INVALID, "export: destination too small");
     float* target = device_dst ? dst : p->export_buf;
-    k_export<<<256, 256, 0, ctx->stream>>>(p->sum, p->sumsq, p->nsamples > 0 ? p->nsamples : 1.0, (int)npix, what, target);
+    const double* src = what == 2 ? p->aov_sum : what == 3 ? p->aov_sum + 3 * npix : p->sum;   // a picture's mean
+    k_export<<<256, 256, 0, ctx->stream>>>(src, p->sumsq, p->nsamples > 0 ? p->nsamples : 1.0, (int)npix, what >= 2 ? 0 : what, target);
     CK(ctx, cudaGetLastError());
     if (!device_dst) {
         CK(ctx, cudaMemcpyAsync(dst, p->export_buf, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
@@ -2034,7 +2073,7 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
                      kNoAllocMaxTable);
         return PTR_E_INVALID;
     }
-    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE || d->n_tree_nodes != 0 || pd->light_tree || d->n_field_code != 0) {
+    if (d->n_meshes != 0 || d->n_batches != 0 || d->env.kind == PTR_ENV_IMAGE || d->n_tree_nodes != 0 || pd->light_tree || d->n_field_code != 0 || pd->aovs) {
         std::fprintf(stderr, "ptr_render_noalloc: only analytic scenes with a constant or no environment and power or uniform light selection are supported\n");
         return PTR_E_UNSUPPORTED;
     }
