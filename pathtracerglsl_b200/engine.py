@@ -153,6 +153,25 @@ class CudaEngine:
         return out
 
     # -- differentiation ---------------------------------------------------------------------
+    def render_stamp(self, picture="radiance", scene_id=None, resolution=None, spp=None):
+        """The reproducibility stamp of a saved picture (App.ts buildRenderStamp): the
+        picture, the scene id, the active strategy, the live parameters, the sample count,
+        the resolution and the reset salt, plus this library's ABI version and a UTC date.
+        A tiled render passes the full image's resolution and spp."""
+        import datetime
+        r = self.renderers.get(self.current)
+        return {
+            "picture": picture,
+            "scene": scene_id or "unknown",
+            "strategy": r.strategy if r is not None else None,
+            "parameters": dict(self.params),
+            "spp": int(self.sample_count if spp is None else spp),
+            "resolution": list(resolution or (self.width, self.height)),
+            "resetSalt": int(self.reset_salt),
+            "abi": int(self.lib.ptr_abi_version()),
+            "date": datetime.datetime.now(datetime.timezone.utc).isoformat(),
+        }
+
     def backward(self, dl_dimage, width, height, spp, first_sample=0, salt=None):
         """Path-replay adjoint: gradient of a loss whose derivative with respect to the
         current renderer's image is ``dl_dimage`` ((H, W, 3), row 0 = bottom), estimated

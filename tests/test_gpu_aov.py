@@ -66,3 +66,14 @@ def test_aovs_carry_the_camera_ray_transmittance(engine):
     np.testing.assert_allclose(c, np.broadcast_to(0.5 * np.exp(-np.array([1.0, 2.0, 4.0])), c.shape), rtol=1.2e-2)
     nz = out["normal"][3:5, 3:5, 2].reshape(-1)
     np.testing.assert_allclose(nz, np.exp(-np.array([1.0, 2.0, 4.0])).mean(), rtol=1.2e-2)
+
+
+def test_render_stamp(engine):
+    """The reproducibility stamp (App.ts buildRenderStamp) of the frame just rendered."""
+    sc, st = scenes.cornell(direct="mis")
+    st = dict(st, measurement=dict(st["measurement"], aovs=["albedo"]))
+    _render(engine, sc, st, 32, 24, 8, {})
+    stamp = engine.render_stamp("albedo", sc["id"])
+    assert stamp["picture"] == "albedo" and stamp["scene"] == "cornell-c1"
+    assert stamp["spp"] == 8 and stamp["resolution"] == [32, 24] and stamp["resetSalt"] == 3
+    assert stamp["strategy"]["measurement"]["aovs"] == ["albedo"] and stamp["abi"] >= 3
