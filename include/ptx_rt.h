@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PTR_ABI_VERSION 3
+#define PTR_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------------- */
 #define PTR_OK 0
@@ -278,13 +278,17 @@ typedef struct ptr_camera {
 } ptr_camera;
 
 typedef struct ptr_frame {
-    int32_t width, height;      /* engine.imageSize                                   */
+    int32_t width, height;      /* the film rendered by this call (a tile's size)     */
     int32_t first_sample;       /* engine.sampleCount of the first sample             */
     int32_t spp;                /* samples per pixel rendered by this call            */
     uint32_t reset_salt;        /* engine.resetSalt                                   */
     int32_t pixel_offset[2];    /* engine.pixelOffset (tiled renders)                 */
     int32_t accumulate;         /* 0 = clear the film first, 1 = add to it            */
     ptr_camera camera;
+    int32_t image_size[2];      /* engine.imageSize: the full image the camera maps film
+                                   points through (pinhole.glsl:6); 0, 0 = width, height.
+                                   A tile of a larger image (TiledRenderer.ts:63-117)
+                                   passes the full size here and its own size above.  */
 } ptr_frame;
 
 typedef struct ptr_counters {
@@ -392,9 +396,12 @@ int ptr_get_stream(ptr_ctx* ctx, void** stream);
  * the process exits, for at most 65536 paths in flight (larger frames run in waves) and
  * at most 256 regions, materials and lights (more returns PTR_E_INVALID).
  * The first call on each device looks the array's device address up (with that device
- * current); make that first call before any stream capture.  Every call shares the
- * array: calls that overlap on the GPU race.  The current device must be set by the
- * caller.  Returns a PTR_E_* status (messages go to stderr; there is no context). */
+ * current); make that first call before any stream capture.  The address is kept for
+ * the life of the process, so resetting a device (cudaDeviceReset) after its first call
+ * is not supported.  Every call shares the array: calls that overlap on the GPU race.
+ * The scene tables pass the same checks as ptr_upload_scene's, and only quad, sphere and
+ * point lights are accepted.  The current device must be set by the caller.  Returns a
+ * PTR_E_* status (messages go to stderr; there is no context). */
 int ptr_render_noalloc(const ptr_scene_desc* scene, const ptr_program_desc* prog, const ptr_frame* frame,
                        double* sum_dev, double* sumsq_dev, void* stream);
 

@@ -59,8 +59,10 @@ def lib():
 
 
 def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=None,
-           threads=0, keep_samples=False, pixel_offset=(0, 0)):
-    """Render with the oracle.  Returns dict(mean, var, sum, sumsq, samples?, counts)."""
+           threads=0, keep_samples=False, pixel_offset=(0, 0), image_size=None):
+    """Render with the oracle.  Returns dict(mean, var, sum, sumsq, samples?, counts).
+    ``pixel_offset`` / ``image_size``: the frame is a width x height tile at that offset of
+    an image of that size (engine.pixelOffset / engine.imageSize)."""
     from pathtracerglsl_b200 import abi
     desc = packed.desc()
     fr = abi.Frame()
@@ -68,7 +70,9 @@ def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=
     fr.first_sample, fr.spp = first_sample, spp
     fr.reset_salt = salt
     fr.pixel_offset = (ctypes.c_int32 * 2)(*pixel_offset)
-    fr.camera = renderer.camera(params or {}, width, height)
+    iw, ih = image_size or (width, height)
+    fr.image_size = (ctypes.c_int32 * 2)(iw, ih)
+    fr.camera = renderer.camera(params or {}, iw, ih)
     s = np.zeros((height, width, 3), np.float64)
     q = np.zeros((height, width, 3), np.float64)
     samples = np.zeros((spp, height, width, 3), np.float32) if keep_samples else None

@@ -2149,7 +2149,9 @@ int oracle_forward_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, co
             return -2;
     }
     Scene S(sd, pd);
-    const int W = fr->width, H = fr->height;
+    // engine.imageSize: the full image when this frame is a tile of it (pinhole.glsl:6)
+    const int W = fr->image_size[0] > 0 ? fr->image_size[0] : fr->width;
+    const int H = fr->image_size[1] > 0 ? fr->image_size[1] : fr->height;
     const int K = PTR_GRAD_SLOTS * sd->n_materials;
     if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel
@@ -2189,7 +2191,9 @@ int oracle_forward_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, co
 
 static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
                              double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
-    const int W = fr->width, H = fr->height;
+    // engine.imageSize: the full image when this frame is a tile of it (pinhole.glsl:6)
+    const int W = fr->image_size[0] > 0 ? fr->image_size[0] : fr->width;
+    const int H = fr->image_size[1] > 0 ? fr->image_size[1] : fr->height;
     uint64_t closest = 0, shadow = 0;
     if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel reduction(+ : closest, shadow)

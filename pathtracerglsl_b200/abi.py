@@ -6,7 +6,7 @@ their descriptors from these types, so the two consume byte-identical scenes.
 """
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 FIELD_MAX_STACK = 16
 
 PTR_OK = 0
@@ -122,7 +122,7 @@ class Camera(C.Structure):
 class Frame(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("first_sample", C.c_int32),
                 ("spp", C.c_int32), ("reset_salt", C.c_uint32), ("pixel_offset", C.c_int32 * 2),
-                ("accumulate", C.c_int32), ("camera", Camera)]
+                ("accumulate", C.c_int32), ("camera", Camera), ("image_size", C.c_int32 * 2)]
 
 
 class BatchJob(C.Structure):

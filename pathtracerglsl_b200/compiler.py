@@ -248,6 +248,7 @@ class CompiledRenderer:
     strategy: dict
     parameters: dict
     export_targets: dict
+    measurement: dict = None   # the strategy's measurement with every default filled in
 
     def camera(self, params, width, height):
         """Evaluate the camera uniforms (features/camera.ts:69-160) into a ``ptr_camera``."""
@@ -895,7 +896,36 @@ class Compiler:
         exports = {"radiance": {"format": "float"}, "variance": {"format": "float"}}
         for a in meas.get("aovs") or []:   # first-hit pictures (components/aov)
             exports[a] = {"format": "float"}
-        return CompiledRenderer(rid, prog, st, parameters, exports)
+        return CompiledRenderer(rid, prog, st, parameters, exports, resolve_measurement(scene, st))
+
+
+DEFAULT_MAX_NULL_CROSSINGS = 32
+DEFAULT_SENSORS = {"rgb": "ideal", "spectral": "cie1931"}
+
+
+def resolve_measurement(scene, strategy):
+    """``resolveMeasurement`` (src/compiler/plan/measurement.ts:14-35): the strategy's
+    measurement section with every default filled in, i.e. what the image estimates,
+    truncations included.  The reproducibility stamp records it."""
+    m = strategy.get("measurement", {})
+    color = m.get("color", "rgb")
+    out = {
+        "camera": m.get("camera"),
+        "ambient": (scene.get("ambientSpace") or {}).get("type", "euclidean"),
+        "response": m.get("response", "radiance"),
+        "maxBounces": m.get("maxBounces"),
+        "maxNullCrossings": m.get("maxNullCrossings", DEFAULT_MAX_NULL_CROSSINGS),
+        "scattering": m.get("scattering", "full"),
+        "shadows": m.get("shadows", "opaque-dielectrics"),
+        "color": color,
+        "sensor": m.get("sensor", DEFAULT_SENSORS.get(color)),
+    }
+    if color == "spectral":
+        from .spectral import MODEL_VERSION
+        out["colorModelVersion"] = MODEL_VERSION
+    if m.get("aovs"):
+        out["aovs"] = list(m["aovs"])
+    return out
 
 
 def build_env_importance(table):

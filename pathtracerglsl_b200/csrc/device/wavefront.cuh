@@ -141,6 +141,7 @@ struct FrameParams {
     int width, height, spp, first_sample;
     uint32_t salt;
     int px_off, py_off;
+    int img_w, img_h;  // the full image the camera maps film points through
     long long total;   // width*height*spp
     int capacity;
     ptr_camera cam;
@@ -459,8 +460,8 @@ __global__ void k_generate(DevScene S, PathPool pool, const FrameParams* fp, Adj
         }
         rng.next();   // the lens draw (a pinhole has no aperture)
         rng.next();
-        float ndcx = (2.0f * fx / (float)F.width) - 1.0f;
-        float ndcy = (2.0f * fy / (float)F.height) - 1.0f;
+        float ndcx = (2.0f * fx / (float)F.img_w) - 1.0f;
+        float ndcy = (2.0f * fy / (float)F.img_h) - 1.0f;
         ndcx *= F.cam.aspect;
         f3 dir = normalize(ld3(F.cam.forward) + ndcx * F.cam.tan_fov * ld3(F.cam.right) +
                            ndcy * F.cam.tan_fov * ld3(F.cam.up));
@@ -1528,8 +1529,8 @@ __global__ void k_generate_batch(PathPool pool, BatchTables bt) {
         float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
         rng.next();
         rng.next();
-        float ndcx = (2.0f * fx / (float)F.width) - 1.0f;
-        float ndcy = (2.0f * fy / (float)F.height) - 1.0f;
+        float ndcx = (2.0f * fx / (float)F.img_w) - 1.0f;
+        float ndcy = (2.0f * fy / (float)F.img_h) - 1.0f;
         ndcx *= F.cam.aspect;
         f3 dir = normalize(ld3(F.cam.forward) + ndcx * F.cam.tan_fov * ld3(F.cam.right) +
                            ndcy * F.cam.tan_fov * ld3(F.cam.up));

@@ -965,6 +965,8 @@ int render_impl(ptr_program* p, ptr_scene* s, const ptr_frame* f, float* samples
     F.salt = f->reset_salt;
     F.px_off = f->pixel_offset[0];
     F.py_off = f->pixel_offset[1];
+    F.img_w = f->image_size[0] > 0 ? f->image_size[0] : f->width;
+    F.img_h = f->image_size[1] > 0 ? f->image_size[1] : f->height;
     F.total = total;
     F.capacity = (int)cap;
     F.cam = f->camera;
@@ -1245,33 +1247,39 @@ bool field_program_ok(const uint32_t* code, int n, int start) {
 }
 }  // namespace
 
-int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
-    if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
-    *out = nullptr;
-    if (d->abi_version != PTR_ABI_VERSION) return fail(ctx, PTR_E_INVALID, "scene: ABI version mismatch");
-    if (d->n_regions < 0 || d->n_materials <= 0 || d->n_lights < 0) return fail(ctx, PTR_E_INVALID, "scene: bad table sizes");
+namespace {
+// The scene description's own consistency: table sizes and pointers, region shapes,
+// materials and parameters, light kinds, regions and selection pdfs, coefficient-field
+// programs, instance lights and the light tree.  Every entry point that takes a
+// ptr_scene_desc runs it before copying anything to the device.
+int check_scene_desc(const ptr_scene_desc* d, std::string& why) {
+    auto bad = [&why](const std::string& m) { why = m; return PTR_E_INVALID; };
+    if (d->abi_version != PTR_ABI_VERSION) return bad("scene: ABI version mismatch");
+    if (d->n_regions < 0 || d->n_materials <= 0 || d->n_lights < 0) return bad("scene: bad table sizes");
+    if ((d->n_regions > 0 && !d->regions) || !d->materials || (d->n_lights > 0 && !d->lights))
+        return bad("scene: a table with entries has a null pointer");
     for (int i = 0; i < d->n_regions; ++i) {
         const ptr_region& g = d->regions[i];
-        if (g.shape < 0 || g.shape > PTR_SHAPE_INSTANCES) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has an unknown shape");
-        if (g.material < 0 || g.material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has a material out of range");
-        if (g.shape == PTR_SHAPE_MESH && (g.ref < 0 || g.ref >= d->n_meshes)) return fail(ctx, PTR_E_INVALID, "scene: mesh region references a missing mesh");
-        if (g.shape == PTR_SHAPE_INSTANCES && (g.ref < 0 || g.ref >= d->n_batches)) return fail(ctx, PTR_E_INVALID, "scene: instanced region references a missing batch");
+        if (g.shape < 0 || g.shape > PTR_SHAPE_INSTANCES) return bad("scene: region " + std::to_string(i) + " has an unknown shape");
+        if (g.material < 0 || g.material >= d->n_materials) return bad("scene: region " + std::to_string(i) + " has a material out of range");
+        if (g.shape == PTR_SHAPE_MESH && (g.ref < 0 || g.ref >= d->n_meshes)) return bad("scene: mesh region references a missing mesh");
+        if (g.shape == PTR_SHAPE_INSTANCES && (g.ref < 0 || g.ref >= d->n_batches)) return bad("scene: instanced region references a missing batch");
         for (int k = 0; k < 15; ++k)
-            if (!std::isfinite(g.p[k])) return fail(ctx, PTR_E_INVALID, "scene: region " + std::to_string(i) + " has a non-finite parameter");
+            if (!std::isfinite(g.p[k])) return bad("scene: region " + std::to_string(i) + " has a non-finite parameter");
     }
     for (int i = 0; i < d->n_lights; ++i) {
         const ptr_light& l = d->lights[i];
-        if (l.region >= d->n_regions) return fail(ctx, PTR_E_INVALID, "scene: light region out of range");
-        if (!(l.select_pdf > 0.0f) || !std::isfinite(l.select_pdf)) return fail(ctx, PTR_E_INVALID, "scene: light selection pdf must be positive");
-        if (l.kind < PTR_LIGHT_QUAD || l.kind > PTR_LIGHT_MESH) return fail(ctx, PTR_E_INVALID, "scene: light " + std::to_string(i) + " has an unknown kind");
+        if (l.region >= d->n_regions) return bad("scene: light region out of range");
+        if (!(l.select_pdf > 0.0f) || !std::isfinite(l.select_pdf)) return bad("scene: light selection pdf must be positive");
+        if (l.kind < PTR_LIGHT_QUAD || l.kind > PTR_LIGHT_MESH) return bad("scene: light " + std::to_string(i) + " has an unknown kind");
         if (l.kind == PTR_LIGHT_MESH) {
             const int mi = (int)l.p[0];
             if (l.region < 0 || d->regions[l.region].shape != PTR_SHAPE_MESH || d->regions[l.region].ref != mi ||
                 (float)mi != l.p[0] || !(l.p[12] > 0.0f) || !std::isfinite(l.p[12]))
-                return fail(ctx, PTR_E_INVALID, "scene: mesh light " + std::to_string(i) + " must name its mesh region, its mesh and a positive area");
+                return bad("scene: mesh light " + std::to_string(i) + " must name its mesh region, its mesh and a positive area");
         }
     }
-    if (d->ambient_material >= d->n_materials) return fail(ctx, PTR_E_INVALID, "scene: ambient material out of range");
+    if (d->ambient_material >= d->n_materials) return bad("scene: ambient material out of range");
     bool has_het = false;
     for (int i = 0; i < d->n_materials; ++i) {
         const ptr_material& m = d->materials[i];
@@ -1280,27 +1288,27 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         if (!(m.flags & PTR_MATF_MEDIUM) || !(m.majorant > 0.0f) || !std::isfinite(m.majorant) || !d->field_code ||
             (m.field_a && !field_program_ok(d->field_code, d->n_field_code, m.field_a - 1)) ||
             (m.field_s && !field_program_ok(d->field_code, d->n_field_code, m.field_s - 1)))
-            return fail(ctx, PTR_E_INVALID, "scene: material " + std::to_string(i) +
+            return bad("scene: material " + std::to_string(i) +
                                                 " has a malformed coefficient field or no positive majorant");
     }
     for (int b = 0; b < d->n_batches; ++b) {
         const ptr_batch_desc& bd = d->batches[b];
         if (bd.light_base >= 0 && ((long long)bd.light_base + bd.n_instances > d->n_lights || bd.prototype_shape != PTR_SHAPE_SPHERE))
-            return fail(ctx, PTR_E_INVALID, "scene: instance lights of batch " + std::to_string(b) + " exceed the light table");
+            return bad("scene: instance lights of batch " + std::to_string(b) + " exceed the light table");
     }
     if (d->n_tree_nodes != 0) {
         // a preorder tree of one light per leaf: every link points forward inside the
         // table, every light is reached once, and its trail lands on its own leaf
         const int nn = d->n_tree_nodes;
         if (d->n_lights <= 0 || nn != 2 * d->n_lights - 1 || !d->light_tree || !d->light_trails)
-            return fail(ctx, PTR_E_INVALID, "scene: the light tree must hold 2 n_lights - 1 nodes and the trails");
+            return bad("scene: the light tree must hold 2 n_lights - 1 nodes and the trails");
         std::vector<char> seen(d->n_lights, 0);
         for (int i = 0; i < nn; ++i) {
             const float link = d->light_tree[8 * (size_t)i + 7];
             const int li = (int)link;
             if ((float)li != link || (li >= 0 && (li <= i + 1 || li >= nn || i + 1 >= nn)) ||
                 (li < 0 && (-li - 1 >= d->n_lights || seen[-li - 1]++)))
-                return fail(ctx, PTR_E_INVALID, "scene: malformed light tree node " + std::to_string(i));
+                return bad("scene: malformed light tree node " + std::to_string(i));
         }
         for (int l = 0; l < d->n_lights; ++l) {
             uint32_t tw = d->light_trails[2 * (size_t)l];
@@ -1311,9 +1319,18 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
                 tw >>= 1u;
             }
             if (d->light_tree[8 * (size_t)ni + 7] != (float)(-(l + 1)))
-                return fail(ctx, PTR_E_INVALID, "scene: the trail of light " + std::to_string(l) + " misses its leaf");
+                return bad("scene: the trail of light " + std::to_string(l) + " misses its leaf");
         }
     }
+    return PTR_OK;
+}
+}  // namespace
+
+int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
+    if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
+    *out = nullptr;
+    std::string why;
+    if (int rc = check_scene_desc(d, why)) return fail(ctx, rc, why);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, PTR_E_CUDA, "cudaSetDevice");
     ptr_scene* s = new ptr_scene();
     s->ctx = ctx;
@@ -1332,6 +1349,8 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
     S.light_tree = nullptr;
     S.light_trails = nullptr;
     S.field_code = nullptr;
+    bool has_het = false;
+    for (int i = 0; i < d->n_materials; ++i) has_het |= d->materials[i].field_a || d->materials[i].field_s;
     S.has_het = has_het ? 1 : 0;
     if (has_het && (rc = dev_copy(ctx, s->allocs, d->field_code, (size_t)d->n_field_code, &S.field_code))) {
         ptr_free_scene(s);
@@ -1554,6 +1573,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         F.salt = J.frame.reset_salt;
         F.px_off = J.frame.pixel_offset[0];
         F.py_off = J.frame.pixel_offset[1];
+    F.img_w = J.frame.image_size[0] > 0 ? J.frame.image_size[0] : J.frame.width;
+    F.img_h = J.frame.image_size[1] > 0 ? J.frame.image_size[1] : J.frame.height;
         F.total = total_j;
         F.capacity = 0;
         F.cam = J.frame.camera;
@@ -1778,6 +1799,8 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     F.salt = f->reset_salt;
     F.px_off = f->pixel_offset[0];
     F.py_off = f->pixel_offset[1];
+    F.img_w = f->image_size[0] > 0 ? f->image_size[0] : f->width;
+    F.img_h = f->image_size[1] > 0 ? f->image_size[1] : f->height;
     F.total = total;
     F.capacity = (int)cap;
     F.cam = f->camera;
@@ -2080,17 +2103,31 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
     if (f->width <= 0 || f->height <= 0 || f->spp <= 0) return PTR_E_INVALID;
     if (pd->max_bounces < 0 || pd->max_bounces > 4096 || pd->direct < 0 || pd->direct > 2 || pd->equiangular ||
         pd->color != PTR_COLOR_RGB) return PTR_E_INVALID;
+    // the same scene checks as ptr_upload_scene, then the analytic subset this entry
+    // point renders: shapes up to boxes and quad, sphere or point lights (a mesh light
+    // would need mesh tables that are never uploaded here)
+    std::string why;
+    if (int rc = check_scene_desc(d, why)) {
+        std::fprintf(stderr, "ptr_render_noalloc: %s\n", why.c_str());
+        return rc;
+    }
     for (int i = 0; i < d->n_regions; ++i)
-        if (d->regions[i].shape > PTR_SHAPE_BOX || d->regions[i].material < 0 || d->regions[i].material >= d->n_materials)
+        if (d->regions[i].shape > PTR_SHAPE_BOX) {
+            std::fprintf(stderr, "ptr_render_noalloc: region %d is not an analytic shape\n", i);
             return PTR_E_INVALID;
-    if (d->ambient_material >= d->n_materials) return PTR_E_INVALID;
+        }
+    for (int i = 0; i < d->n_lights; ++i)
+        if (d->lights[i].kind < PTR_LIGHT_QUAD || d->lights[i].kind > PTR_LIGHT_POINT) {
+            std::fprintf(stderr, "ptr_render_noalloc: light %d is not a quad, sphere or point light\n", i);
+            return PTR_E_INVALID;
+        }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return PTR_E_CUDA;
     unsigned char* base = nullptr;
-    const char* why = "";
-    int rc = na_address(dev, &base, &why);
+    const char* why_addr = "";
+    int rc = na_address(dev, &base, &why_addr);
     if (rc) {
-        std::fprintf(stderr, "ptr_render_noalloc: cudaGetSymbolAddress failed: %s\n", why);
+        std::fprintf(stderr, "ptr_render_noalloc: cudaGetSymbolAddress failed: %s\n", why_addr);
         return rc;
     }
     cudaStream_t st = (cudaStream_t)stream;
@@ -2143,6 +2180,8 @@ extern "C" int ptr_render_noalloc(const ptr_scene_desc* d, const ptr_program_des
     F.salt = f->reset_salt;
     F.px_off = f->pixel_offset[0];
     F.py_off = f->pixel_offset[1];
+    F.img_w = f->image_size[0] > 0 ? f->image_size[0] : f->width;
+    F.img_h = f->image_size[1] > 0 ? f->image_size[1] : f->height;
     F.total = total;
     F.capacity = (int)cap;
     F.cam = f->camera;

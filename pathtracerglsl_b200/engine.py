@@ -25,6 +25,44 @@ class EngineError(RuntimeError):
         super().__init__(f"ptx_rt error {code}: {message}")
 
 
+# Tile offsets are multiples of this (src/app/tiling.ts: TILE_ALIGN); the default tile
+# edge of a production render (src/app/TiledRenderer.ts: DEFAULT_TILE_SIZE).
+TILE_ALIGN = 64
+DEFAULT_TILE_SIZE = 1024
+
+
+def plan_tiles(width, height, tile_size):
+    """``planTiles`` (src/app/tiling.ts:43-63): cover a width x height image with tiles of
+    the requested size rounded up to TILE_ALIGN, anchored at the lower-left corner (engine
+    coordinates, y from the bottom), listed top row first and left to right; the last
+    column and the top row are cut to the image."""
+    for name, v in (("width", width), ("height", height), ("tileSize", tile_size)):
+        if not isinstance(v, int) or v < 1:
+            raise ValueError(f"planTiles: {name} must be a positive integer (got {v})")
+    size = -(-tile_size // TILE_ALIGN) * TILE_ALIGN
+    cols, rows = -(-width // size), -(-height // size)
+    tiles = []
+    for row in range(rows):
+        y = (rows - 1 - row) * size
+        for col in range(cols):
+            x = col * size
+            tiles.append({"col": col, "row": row, "x": x, "y": y,
+                          "width": min(size, width - x), "height": min(size, height - y)})
+    return {"cols": cols, "rows": rows, "size": size, "tiles": tiles}
+
+
+def _source_revision():
+    """The source revision of this package (git HEAD), or 'unknown' outside a checkout."""
+    import os
+    import subprocess
+    try:
+        out = subprocess.run(["git", "rev-parse", "--short", "HEAD"], capture_output=True, text=True, timeout=5,
+                             cwd=os.path.dirname(os.path.abspath(__file__)))
+        return out.stdout.strip() or "unknown" if out.returncode == 0 else "unknown"
+    except (OSError, subprocess.SubprocessError):
+        return "unknown"
+
+
 class CudaEngine:
     def __init__(self, device=0):
         self.lib = load()
@@ -100,7 +138,9 @@ class CudaEngine:
         else:
             self.reset_salt = self._pinned_salt
 
-    def _frame(self, width, height, spp, accumulate):
+    def _frame(self, width, height, spp, accumulate, image=None):
+        """A ptr_frame of this engine's state; ``image`` = the full image's (width, height)
+        when the frame is one tile of it (engine.imageSize)."""
         r = self.renderers[self.current]
         fr = abi.Frame()
         fr.width, fr.height = width, height
@@ -108,7 +148,9 @@ class CudaEngine:
         fr.spp = spp
         fr.reset_salt = self.reset_salt & 0xFFFFFFFF
         fr.accumulate = 1 if accumulate else 0
-        fr.camera = r.camera(self.params, width, height)
+        iw, ih = image or (width, height)
+        fr.camera = r.camera(self.params, iw, ih)
+        fr.image_size = (C.c_int32 * 2)(iw, ih)
         return fr
 
     def render_frame(self, width, height, spp=1, sync=False):
@@ -152,11 +194,50 @@ class CudaEngine:
                                              out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
         return out
 
-    # -- differentiation ---------------------------------------------------------------------
+    # -- production outputs ------------------------------------------------------------------
+    def render_tiled(self, width, height, spp, tile_size=None, pictures=("radiance",), scene_id=None):
+        """A tiled production render (TiledRenderer.render, src/app/TiledRenderer.ts:63-143):
+        the image is covered by tiles of ``tile_size`` rounded up to TILE_ALIGN
+        (``plan_tiles``), each rendered at ``spp`` from a fresh accumulation with its
+        pixel offset and the full image size, under one reset salt for the whole job (a
+        salt the caller pinned is kept).  Every pixel therefore computes exactly what it
+        would in one full-size render.  Returns ``(images, stamps)``: per picture a
+        (height, width, 3) float32 array, row 0 = bottom, and its reproducibility stamp
+        with the full image's resolution and spp."""
+        if self.scene is None or self.current is None:
+            raise EngineError(abi.PTR_E_INVALID, "no scene registered or no renderer loaded")
+        if not isinstance(spp, int) or spp < 1:
+            raise ValueError(f"Tiled render: spp must be a positive integer (got {spp})")
+        plan = plan_tiles(width, height, tile_size or DEFAULT_TILE_SIZE)
+        pinned = self._pinned_salt
+        self.pin_reset_salt(pinned if pinned is not None else self.reset_salt + 1)
+        images = {p: np.zeros((height, width, 3), np.float32) for p in pictures}
+        stamps = {}
+        try:
+            for t in plan["tiles"]:
+                self.width, self.height = t["width"], t["height"]
+                self.reset()
+                fr = self._frame(t["width"], t["height"], spp, accumulate=False, image=(width, height))
+                fr.pixel_offset = (C.c_int32 * 2)(t["x"], t["y"])
+                self._check(self.lib.ptr_render(self.programs[self.current], self.scene, C.byref(fr)))
+                self.sample_count = spp
+                for p in pictures:
+                    images[p][t["y"]:t["y"] + t["height"], t["x"]:t["x"] + t["width"]] = self.read_export(p)
+            for p in pictures:
+                stamps[p] = self.render_stamp(p, scene_id=scene_id, resolution=(width, height), spp=spp)
+        finally:
+            if pinned is None:
+                self._pinned_salt = None
+            else:
+                self.pin_reset_salt(pinned)
+        return images, stamps
+
     def render_stamp(self, picture="radiance", scene_id=None, resolution=None, spp=None):
-        """The reproducibility stamp of a saved picture (App.ts buildRenderStamp): the
-        picture, the scene id, the active strategy, the live parameters, the sample count,
-        the resolution and the reset salt, plus this library's ABI version and a UTC date.
+        """The reproducibility stamp of a saved picture (App.buildRenderStamp,
+        src/app/App.ts:821-842; the RenderStamp of src/app/utils/file-export.ts:13-24):
+        the picture, the scene id, the active strategy, its resolved measurement, the live
+        parameters, the sample count, the resolution, the reset salt, the source revision
+        ('unknown' when there is none) and a UTC date; plus this library's ABI version.
         A tiled render passes the full image's resolution and spp."""
         import datetime
         r = self.renderers.get(self.current)
@@ -164,14 +245,17 @@ class CudaEngine:
             "picture": picture,
             "scene": scene_id or "unknown",
             "strategy": r.strategy if r is not None else None,
+            "measurement": r.measurement if r is not None else None,
             "parameters": dict(self.params),
             "spp": int(self.sample_count if spp is None else spp),
             "resolution": list(resolution or (self.width, self.height)),
             "resetSalt": int(self.reset_salt),
-            "abi": int(self.lib.ptr_abi_version()),
+            "git": _source_revision(),
             "date": datetime.datetime.now(datetime.timezone.utc).isoformat(),
+            "abi": int(self.lib.ptr_abi_version()),
         }
 
+    # -- differentiation ---------------------------------------------------------------------
     def backward(self, dl_dimage, width, height, spp, first_sample=0, salt=None):
         """Path-replay adjoint: gradient of a loss whose derivative with respect to the
         current renderer's image is ``dl_dimage`` ((H, W, 3), row 0 = bottom), estimated

@@ -38,6 +38,7 @@ from . import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 SUBSET = os.path.join(HERE, "data", "jh_cie1931_d65_subset.npz")
 RES = 64
+MODEL_VERSION = "jh-cie1931-d65-v1"   # the shipped colour model (color/spectral/data.ts:3)
 LAMBDA_MIN, LAMBDA_MAX, STEP = 360.0, 830.0, 5.0
 PLANCK_Q = 14387768.775039338      # h c / k in nm K (blackbody.glsl:5)
 

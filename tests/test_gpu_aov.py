@@ -77,3 +77,8 @@ def test_render_stamp(engine):
     assert stamp["picture"] == "albedo" and stamp["scene"] == "cornell-c1"
     assert stamp["spp"] == 8 and stamp["resolution"] == [32, 24] and stamp["resetSalt"] == 3
     assert stamp["strategy"]["measurement"]["aovs"] == ["albedo"] and stamp["abi"] >= 3
+    # the resolved measurement (plan/measurement.ts:14-35) and the source revision
+    m = stamp["measurement"]
+    assert m["aovs"] == ["albedo"] and m["color"] == "rgb" and m["sensor"] == "ideal"
+    assert m["maxNullCrossings"] == 32 and m["scattering"] == "full" and m["response"] == "radiance"
+    assert isinstance(stamp["git"], str) and stamp["git"]
