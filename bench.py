@@ -446,14 +446,7 @@ def run_ours(args):
                          "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
                          "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}
         if not args.no_cpu_baseline:
-            if args.workload == "media":   # the CPU restatement has no spectral model: its RGB walk
-                from pathtracerglsl_b200 import scenes as _sc
-                sc_rgb, st_rgb, _ = _sc.media_scene(spectral=False)
-                line["cpu_baseline"] = cpu_baseline(sc_rgb, st_rgb, w, h, spp)
-                line["cpu_baseline"]["sample"] = "RGB walk of the same scene (no spectral model on the CPU): " + \
-                    line["cpu_baseline"]["sample"]
-            else:
-                line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
+            line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
         print(json.dumps(line), flush=True)
     eng.close()
     if dist is not None:

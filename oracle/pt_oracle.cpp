@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <type_traits>
 #include <limits>
 #include <omp.h>
 
@@ -72,6 +73,36 @@ inline float spectrum_max(v3 s) { float m = s[2]; m = fmaxf_(s[1], m); m = fmaxf
 inline bool spectrum_is_black(v3 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f; }
 inline int spectrum_sample_channel(float u) { int c = (int)(u * 3.0f); return c < 2 ? c : 2; }
 
+// The spectral carrier: four wavelength lanes (color/spectral/types.glsl, SPECTRUM_N = 4),
+// with the spectrum helpers of spectrum.glsl:1-24 at N = 4.
+struct s4 {
+    float x, y, z, w;
+    s4() : x(0.f), y(0.f), z(0.f), w(0.f) {}
+    explicit s4(float s) : x(s), y(s), z(s), w(s) {}
+    s4(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+    float operator[](int i) const { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
+    float& operator[](int i) { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
+};
+inline s4 operator+(s4 a, s4 b) { return s4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+inline s4 operator-(s4 a, s4 b) { return s4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+inline s4 operator*(s4 a, s4 b) { return s4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+inline s4 operator/(s4 a, s4 b) { return s4(a.x / b.x, a.y / b.y, a.z / b.z, a.w / b.w); }
+inline s4 operator*(s4 a, float t) { return s4(a.x * t, a.y * t, a.z * t, a.w * t); }
+inline s4 operator*(float t, s4 a) { return s4(t * a.x, t * a.y, t * a.z, t * a.w); }
+inline s4 operator/(s4 a, float t) { return s4(a.x / t, a.y / t, a.z / t, a.w / t); }
+inline s4 operator-(s4 a) { return s4(-a.x, -a.y, -a.z, -a.w); }
+inline s4 vexp(s4 a) { return s4(std::exp(a.x), std::exp(a.y), std::exp(a.z), std::exp(a.w)); }
+inline s4 vmax(s4 a, s4 b) { return s4(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z), fmaxf_(a.w, b.w)); }
+inline float spectrum_average(s4 s) { float sum = s.x; sum += s.y; sum += s.z; sum += s.w; return sum * (1.0f / 4.0f); }
+inline float spectrum_max(s4 s) { float m = s.w; m = fmaxf_(s.z, m); m = fmaxf_(s.y, m); m = fmaxf_(s.x, m); return m; }
+inline bool spectrum_is_zero(v3 s) { return s.x == 0.0f && s.y == 0.0f && s.z == 0.0f; }
+inline bool spectrum_is_zero(s4 s) { return s.x == 0.0f && s.y == 0.0f && s.z == 0.0f && s.w == 0.0f; }
+inline bool spectrum_is_black(s4 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f && s.w <= 0.f; }
+// the channel of the chromatic free-flight draw: one of the carrier's N lanes
+template <class Col> inline int sample_channel(float u);
+template <> inline int sample_channel<v3>(float u) { return spectrum_sample_channel(u); }
+template <> inline int sample_channel<s4>(float u) { int c = (int)(u * 4.0f); return c < 3 ? c : 3; }
+
 // ---------------------------------------------------------------- RNG (pcg4d.glsl:12-40)
 struct Rng {
     uint32_t base, dim;
@@ -116,8 +147,10 @@ struct Hit {
     float alpha = -1.0f;   // per-triangle GGX alpha of a mesh hit, < 0 = the material's
     int prim = -1;         // original triangle index of a mesh hit
 };
-struct LightSample { v3 wi; float distance; v3 radiance; float pdf; uint32_t flags; int light_id; };
-struct ISample { v3 wi; v3 weight; float pdf; uint32_t flags; };
+template <class Col> struct LightSampleT { v3 wi; float distance; Col radiance; float pdf; uint32_t flags; int light_id; };
+template <class Col> struct ISampleT { v3 wi; Col weight; float pdf; uint32_t flags; };
+using LightSample = LightSampleT<v3>;
+using ISample = ISampleT<v3>;
 
 // fp_uncertainty (math.glsl:54-56)
 inline float fp_uncertainty(v3 p) {
@@ -146,7 +179,7 @@ inline float dielectric_fresnel(float cos_i, float eta) {
     return 0.5f * (r_par * r_par + r_perp * r_perp);
 }
 // schlick_fresnel (math.glsl:83-85)
-inline v3 schlick_fresnel(v3 f0, float c) { return f0 + (v3(1.0f) - f0) * std::pow(1.0f - c, 5.0f); }
+template <class Col> inline Col schlick_fresnel(Col f0, float c) { return f0 + (Col(1.0f) - f0) * std::pow(1.0f - c, 5.0f); }
 // ray_spawn (glsl/core/ray.glsl:29-32)
 inline Ray ray_spawn(const Hit& h, v3 wi) {
     float side = dot(wi, h.ng) >= 0.0f ? 1.0f : -1.0f;
@@ -702,19 +735,19 @@ struct Scene {
 
 // ---------------------------------------------------------------- materials
 // lambert (materials/lambert/lambert.glsl:7-37)
-inline v3 lambert_eval(v3 wi, v3 wo, const Hit& h, const ptr_material& m) {
-    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return v3(0.0f);
-    return ld3(m.albedo) * (1.0f / PI);
+template <class Col> inline Col lambert_eval(v3 wi, v3 wo, const Hit& h, Col albedo) {
+    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return Col(0.0f);
+    return albedo * (1.0f / PI);
 }
-inline ISample lambert_sample(v3 wo, const Hit& h, const ptr_material& m, float, float u0, float u1) {
+template <class Col> inline ISampleT<Col> lambert_sample(v3 wo, const Hit& h, Col albedo, float, float u0, float u1) {
     const Frame& f = h.frame;
     v3 n = dot(wo, f.n) < 0.0f ? -f.n : f.n;
     float cos_theta = std::sqrt(u1);
     float sin_theta = std::sqrt(fmaxf_(0.0f, 1.0f - u1));
     float phi = TWO_PI * u0;
-    ISample s;
+    ISampleT<Col> s;
     s.wi = normalize(f.t * (sin_theta * std::cos(phi)) + f.b * (sin_theta * std::sin(phi)) + n * cos_theta);
-    s.weight = ld3(m.albedo);
+    s.weight = albedo;
     s.pdf = cos_theta * (1.0f / PI);
     s.flags = LOBE_REFLECTION;
     return s;
@@ -743,23 +776,23 @@ inline v3 mf_sample_vndf(v3 wol, float a, float u0, float u1) {
     return normalize(v3(a * nh.x, a * nh.y, fmaxf_(1e-6f, nh.z)));
 }
 // ggx conductor (materials/ggx/ggx.glsl:16-64)
-inline v3 ggx_eval(v3 wi, v3 wo, const Hit& h, const ptr_material& m, float a) {
+template <class Col> inline Col ggx_eval(v3 wi, v3 wo, const Hit& h, Col f0, float a) {
     v3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return v3(0.0f);
+    if (wil.z * wol.z <= 0.0f) return Col(0.0f);
     v3 hh = normalize(wil + wol);
-    v3 F = schlick_fresnel(ld3(m.f0), std::fabs(dot(wol, hh)));
+    Col F = schlick_fresnel(f0, std::fabs(dot(wol, hh)));
     return F * (mf_D(hh, a) * mf_G1(wil, a) * mf_G1(wol, a) / (4.0f * std::fabs(wil.z) * std::fabs(wol.z)));
 }
-inline ISample ggx_sample(v3 wo, const Hit& h, const ptr_material& m, float a, float u0, float u1) {
+template <class Col> inline ISampleT<Col> ggx_sample(v3 wo, const Hit& h, Col f0, float a, float u0, float u1) {
     v3 wol = mf_to_local(h.frame, wo);
     float side = wol.z < 0.0f ? -1.0f : 1.0f;
     wol = wol * side;
     v3 hh = mf_sample_vndf(wol, a, u0, u1);
     v3 i = -wol;
     v3 wil = i - 2.0f * dot(hh, i) * hh;   // reflect(-wol, h)
-    ISample s;
-    if (wil.z <= 0.0f) { s.wi = wo; s.weight = v3(0.0f); s.pdf = 0.0f; s.flags = LOBE_REFLECTION; return s; }
-    v3 F = schlick_fresnel(ld3(m.f0), std::fabs(dot(wol, hh)));
+    ISampleT<Col> s;
+    if (wil.z <= 0.0f) { s.wi = wo; s.weight = Col(0.0f); s.pdf = 0.0f; s.flags = LOBE_REFLECTION; return s; }
+    Col F = schlick_fresnel(f0, std::fabs(dot(wol, hh)));
     s.weight = F * mf_G1(wil, a);
     s.pdf = mf_G1(wol, a) * mf_D(hh, a) / (4.0f * std::fabs(wol.z));
     s.flags = LOBE_REFLECTION;
@@ -774,12 +807,12 @@ inline float ggx_pdf(v3 wi, v3 wo, const Hit& h, float a) {
 }
 
 // mirror (materials/mirror/mirror.glsl): one delta lobe weighted by Schlick Fresnel
-inline ISample mirror_sample(v3 wo, const Hit& h, const ptr_material& m) {
+template <class Col> inline ISampleT<Col> mirror_sample(v3 wo, const Hit& h, Col f0) {
     v3 n = h.frame.n;
     float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
-    ISample s;
+    ISampleT<Col> s;
     s.wi = normalize(2.0f * cos_i * n - wo);
-    s.weight = schlick_fresnel(ld3(m.f0), cos_i);
+    s.weight = schlick_fresnel(f0, cos_i);
     s.pdf = 0.0f;
     s.flags = LOBE_REFLECTION | LOBE_DELTA;
     return s;
@@ -795,20 +828,20 @@ inline bool rough_half(v3 wil, v3 wol, float eta, v3& m) {
     if (m.z < 0.0f) m = -m;
     return dot(m, wil) * wil.z >= 0.0f && dot(m, wol) * wol.z >= 0.0f;
 }
-inline v3 rough_dielectric_eval_local(v3 wil, v3 wol, const ptr_material& mt, float a, float n_i, float n_t) {
-    if (wol.z <= 0.0f || wil.z == 0.0f) return v3(0.0f);
-    if (n_i == n_t) return v3(0.0f);
+template <class Col> inline Col rough_dielectric_eval_local(v3 wil, v3 wol, Col tint, float a, float n_i, float n_t) {
+    if (wol.z <= 0.0f || wil.z == 0.0f) return Col(0.0f);
+    if (n_i == n_t) return Col(0.0f);
     float eta = n_i / n_t;
     v3 m;
-    if (!rough_half(wil, wol, eta, m)) return v3(0.0f);
+    if (!rough_half(wil, wol, eta, m)) return Col(0.0f);
     float cos_om = clampf(std::fabs(dot(wol, m)), 1e-6f, 1.0f);
     float F = dielectric_fresnel(cos_om, eta);
     float DG = mf_D(m, a) * mf_G1(wol, a) * mf_G1(wil, a);
-    if (wil.z > 0.0f) return v3(1.0f) * (DG * F / (4.0f * wil.z * wol.z));
+    if (wil.z > 0.0f) return Col(1.0f) * (DG * F / (4.0f * wil.z * wol.z));
     float denom = dot(wil, m) + dot(wol, m) * eta;
     denom *= denom;
     float ft = DG * (1.0f - F) * std::fabs(dot(wil, m) * dot(wol, m) / (wil.z * wol.z * denom));
-    return ld3(mt.transmittance) * (ft * eta * eta);
+    return tint * (ft * eta * eta);
 }
 inline float rough_dielectric_pdf_local(v3 wil, v3 wol, float a, float n_i, float n_t) {
     if (wol.z <= 0.0f || wil.z == 0.0f) return 0.0f;
@@ -824,18 +857,19 @@ inline float rough_dielectric_pdf_local(v3 wil, v3 wol, float a, float n_i, floa
     return (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * std::fabs(dot(wil, m)) / denom;
 }
 // the sampled lobe in the local frame (wil); the caller maps it out of the frame
-inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, float a, float n_i, float n_t,
-                                             float uc, float u0, float u1) {
-    ISample s;
+template <class Col>
+inline ISampleT<Col> rough_dielectric_sample_local(v3 wol, Col tint, float a, float n_i, float n_t, float uc, float u0,
+                                                   float u1) {
+    ISampleT<Col> s;
     s.wi = wol;
-    s.weight = v3(0.0f);
+    s.weight = Col(0.0f);
     s.pdf = 0.0f;
     s.flags = LOBE_REFLECTION;
     if (wol.z <= 0.0f) return s;
     float eta = n_i / n_t;
     if (n_i == n_t) {
         s.wi = -wol;
-        s.weight = ld3(mt.transmittance);
+        s.weight = tint;
         s.flags = LOBE_TRANSMISSION | LOBE_DELTA;
         return s;
     }
@@ -847,7 +881,7 @@ inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, flo
         v3 i = -wol;
         wil = i - 2.0f * dot(m, i) * m;
         if (wil.z <= 0.0f) return s;
-        s.weight = v3(1.0f) * mf_G1(wil, a);
+        s.weight = Col(1.0f) * mf_G1(wil, a);
         s.pdf = F * mf_G1(wol, a) * mf_D(m, a) / (4.0f * wol.z);
         s.flags = LOBE_REFLECTION;
     } else {
@@ -857,7 +891,7 @@ inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, flo
         if (wil.z >= 0.0f) return s;
         float denom = dot(wil, m) + dot(wol, m) * eta;
         denom *= denom;
-        s.weight = ld3(mt.transmittance) * (mf_G1(wil, a) * eta * eta);
+        s.weight = tint * (mf_G1(wil, a) * eta * eta);
         s.pdf = (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * std::fabs(dot(wil, m)) / denom;
         s.flags = LOBE_TRANSMISSION;
     }
@@ -866,7 +900,8 @@ inline ISample rough_dielectric_sample_local(v3 wol, const ptr_material& mt, flo
 }
 
 // ---------------------------------------------------------------- media (transport/volume/analytic)
-struct MediumSample { bool scattered; float t; v3 weight; v3 exit_p, exit_dir; };
+template <class Col> struct MediumSampleT { bool scattered; float t; Col weight; v3 exit_p, exit_dir; };
+using MediumSample = MediumSampleT<v3>;
 
 // ---- heterogeneous media (transport/volume/delta_tracking/delta_tracking.glsl)
 // The coefficient field: the stack program of a GLSL expression of p, interpreted with
@@ -951,22 +986,23 @@ inline v3 field_eval(const uint32_t* code, v3 p) {
     return st[0];
 }
 // medium_sample_analytic (transport/volume/analytic/analytic.glsl:9-43)
-inline MediumSample medium_sample_analytic(const ptr_material& m, const Ray& r, float t_max, float x0, float x1) {
-    v3 sigma_t = ld3(m.sigma_a) + ld3(m.sigma_s);
-    int c = spectrum_sample_channel(x0);
+template <class Col>
+inline MediumSampleT<Col> medium_sample_analytic(Col sigma_a, Col sigma_s, const Ray& r, float t_max, float x0, float x1) {
+    Col sigma_t = sigma_a + sigma_s;
+    int c = sample_channel<Col>(x0);
     float sc = sigma_t[c];
     float t = sc == 0.0f ? t_max : -std::log(1.0f - x1) / sc;
-    MediumSample ms;
+    MediumSampleT<Col> ms;
     if (t < t_max) {
-        v3 tr = vexp(-sigma_t * t);
+        Col tr = vexp(-sigma_t * t);
         float pdf = spectrum_average(sigma_t * tr);
         ms.scattered = true;
         ms.t = t;
         ms.exit_p = r.o + r.d * t;
         ms.exit_dir = r.d;
-        ms.weight = ld3(m.sigma_s) * tr / fmaxf_(pdf, 1e-20f);
+        ms.weight = sigma_s * tr / fmaxf_(pdf, 1e-20f);
     } else {
-        v3 tr = vexp(-sigma_t * t_max);
+        Col tr = vexp(-sigma_t * t_max);
         float pdf = spectrum_average(tr);
         ms.scattered = false;
         ms.t = t_max;
@@ -980,7 +1016,7 @@ inline float hg_eval(v3 wi, v3 wo, float g) {
     float d = 1.0f + g * g - 2.0f * g * c;
     return (1.0f - g * g) / (4.0f * PI * d * std::sqrt(fmaxf_(d, 1e-8f)));
 }
-inline ISample hg_sample(v3 wo, float g, float x0, float x1) {
+template <class Col> inline ISampleT<Col> hg_sample(v3 wo, float g, float x0, float x1) {
     float cos_theta;
     if (std::fabs(g) < 1e-3f) cos_theta = 1.0f - 2.0f * x0;
     else {
@@ -991,10 +1027,10 @@ inline ISample hg_sample(v3 wo, float g, float x0, float x1) {
     float phi = TWO_PI * x1;
     v3 t, b;
     build_basis(-wo, t, b);
-    ISample s;
+    ISampleT<Col> s;
     s.wi = normalize(t * (sin_theta * std::cos(phi)) + b * (sin_theta * std::sin(phi)) + (-wo) * cos_theta);
-    s.weight = v3(1.0f);
-    s.pdf = spectrum_average(v3(hg_eval(s.wi, wo, g)));
+    s.weight = Col(1.0f);
+    s.pdf = spectrum_average(Col(hg_eval(s.wi, wo, g)));
     s.flags = LOBE_MEDIUM;
     return s;
 }
@@ -1065,13 +1101,116 @@ inline Dual fresnel_dual(double cos_i, Dual eta) {
 // ---------------------------------------------------------------- the renderer
 struct Counters { uint64_t closest = 0, shadow = 0; };
 
-struct Tracer {
+// ---------------------------------------------------------------- spectral colour model
+// spectral_curves (color/spectral/lookup.glsl:1-7): row 0 of the curve table, CIE x, y, z
+// and luminance-normalised D65 per 5 nm from 360 nm, linearly interpolated.
+inline void spectral_curves(const ptr_scene_desc& d, float lambda, float out[4]) {
+    float x = (lambda - 360.0f) / 5.0f;
+    int i = (int)x;
+    i = i < 93 ? i : 93;
+    const float* a = d.spectral->curves + 4 * i;
+    const float* b = a + 4;
+    float f = x - (float)i;
+    for (int k = 0; k < 4; ++k) out[k] = a[k] * (1.0f - f) + b[k] * f;
+}
+// One lane of a lifted colour record: the bounded sigmoid of spectral_bounded
+// (lookup.glsl:38-48) over the record's host-fitted coefficients, times its scale
+// (color_lift_coefficient, :52-56); Planck relative to 550 nm (blackbody.glsl:4-10);
+// or a grey constant; then D65 for emission (color_lift_emission, :57-61).
+inline float spectrum_lane(const ptr_scene_desc& d, const ptr_spectrum& sp, float lambda) {
+    float v;
+    if (sp.kind == PTR_SPEC_LIFTED) {
+        float t = (lambda - 360.0f) / 470.0f;
+        float p = (sp.c[0] * t + sp.c[1]) * t + sp.c[2];
+        v = clampf(0.5f + 0.5f * p / std::sqrt(1.0f + p * p), 0.0f, 1.0f);
+        v = sp.scale * v;
+    } else if (sp.kind == PTR_SPEC_BLACKBODY) {
+        float q = 14387768.775039338f / sp.c[0];
+        float ratio = 550.0f / lambda;
+        float ratio2 = ratio * ratio;
+        v = sp.c[1] * (std::exp(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (std::exp(q / lambda) - 1.0f);
+        v = sp.scale * v;
+    } else {
+        v = sp.scale;
+    }
+    if (sp.d65) {
+        float c[4];
+        spectral_curves(d, lambda, c);
+        v = v * c[3];
+    }
+    return v;
+}
+// wavelengths_sample (color/spectral/spectral.glsl:1-10): one number, four cyclic quarter
+// offsets in CDF space, each lane with its own density: the truncated sech^2 of
+// visible.glsl:3-13 or uniform.glsl:1-2, over the program's range.
+inline void wavelengths_sample(const ptr_program_desc& P, float u, float lam[4], float pdf[4]) {
+    for (int k = 0; k < 4; ++k) {
+        float v = u + 0.25f * (float)k;
+        v = v - std::floor(v);
+        if (P.wavelengths == PTR_WAVELENGTHS_UNIFORM) {
+            lam[k] = P.lambda_min + (P.lambda_max - P.lambda_min) * v;
+            pdf[k] = 1.0f / (P.lambda_max - P.lambda_min);
+        } else {
+            float a = std::tanh(0.0072f * (P.lambda_min - 538.0f));
+            float b = std::tanh(0.0072f * (P.lambda_max - 538.0f));
+            lam[k] = 538.0f + std::atanh(a * (1.0f - v) + b * v) / 0.0072f;
+            float c = std::cosh(0.0072f * (lam[k] - 538.0f));
+            pdf[k] = 0.0072f / ((b - a) * c * c);
+        }
+    }
+}
+// color_to_pixel (spectral.glsl:27-33) with the CIE 1931 sensor (sensor/cie1931/cie1931.glsl:3-5):
+// 0.25 * sum_i (M xyz(lambda_i) / int ybar) (L_i / pdf_i).
+inline v3 color_to_pixel(const ptr_scene_desc& d, s4 L, const float lam[4], const float pdf[4]) {
+    const float* M = d.spectral->xyz_to_rgb;
+    v3 pixel(0.0f);
+    for (int k = 0; k < 4; ++k) {
+        float c[4];
+        spectral_curves(d, lam[k], c);
+        v3 rgb(M[0] * c[0] + M[1] * c[1] + M[2] * c[2], M[3] * c[0] + M[4] * c[1] + M[5] * c[2],
+               M[6] * c[0] + M[7] * c[1] + M[8] * c[2]);
+        pixel = pixel + rgb / d.spectral->cie_y_integral * (L[k] / pdf[k]);
+    }
+    return 0.25f * pixel;
+}
+
+// The walk, generic over the colour carrier: v3 (RGB) or s4 (four wavelength lanes of
+// measurement.color 'spectral').  Colours of materials, lights and the environment come
+// from the colour accessors below: the RGB records, or the spectral records evaluated at
+// the path's wavelengths.
+template <class Col>
+struct TracerT {
+    static constexpr bool SPECTRAL = std::is_same<Col, s4>::value;
+    using LS = LightSampleT<Col>;
+    using IS = ISampleT<Col>;
+    using MS = MediumSampleT<Col>;
     const Scene& S;
     const ptr_scene_desc& d;
     const ptr_program_desc& P;
     Rng rng;
     Counters cnt;
-    Tracer(const Scene& s) : S(s), d(*s.d), P(*s.prog) {}
+    float wl[4] = {0.f, 0.f, 0.f, 0.f};   // the path's wavelengths (spectral only)
+    TracerT(const Scene& s) : S(s), d(*s.d), P(*s.prog) {}
+
+    // ---- colour accessors (RGB records; or color/spectral/lookup.glsl:38-59 and
+    // spectra/blackbody/blackbody.glsl:4-10 over the lifted records, per lane)
+    Col spec(const ptr_spectrum& sp) const {
+        if constexpr (SPECTRAL) {
+            return s4(spectrum_lane(d, sp, wl[0]), spectrum_lane(d, sp, wl[1]), spectrum_lane(d, sp, wl[2]),
+                      spectrum_lane(d, sp, wl[3]));
+        } else {
+            return Col(0.0f);
+        }
+    }
+    Col c_albedo(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].albedo); else return ld3(d.materials[mi].albedo); }
+    Col c_emission(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].emission); else return ld3(d.materials[mi].emission); }
+    Col c_tint(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].transmittance); else return ld3(d.materials[mi].transmittance); }
+    Col c_f0(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].f0); else return ld3(d.materials[mi].f0); }
+    Col c_sigma_a(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].sigma_a); else return ld3(d.materials[mi].sigma_a); }
+    Col c_sigma_s(int mi) const { if constexpr (SPECTRAL) return spec(d.spectral->materials[mi].sigma_s); else return ld3(d.materials[mi].sigma_s); }
+    Col c_light(int li) const { if constexpr (SPECTRAL) return spec(d.spectral->lights[li]); else return ld3(d.lights[li].radiance); }
+    Col c_env() const { if constexpr (SPECTRAL) return spec(d.spectral->env); else return ld3(d.env.color); }
+    int mat_index(const ptr_material& m) const { return (int)(&m - d.materials); }
 
     // ---- forward-mode tangents (oracle_forward_tile only; null in the plain renders, whose
     // float32 walk they never touch).  d throughput / d theta_k and d radiance / d theta_k
@@ -1089,7 +1228,7 @@ struct Tracer {
         std::fill(tan->rad.begin(), tan->rad.end(), 0.0);
     }
     // throughput <- throughput * W:  d thr = d thr * W + thr * dW
-    void tan_mul(v3 thr, v3 W, const DW* dw, int n) {
+    void tan_mul(Col thr, Col W, const DW* dw, int n) {
         if (!tan) return;
         for (int k = 0; k < tan->K; ++k)
             for (int c = 0; c < 3; ++c) tan->thr[3 * k + c] *= (double)W[c];
@@ -1097,7 +1236,7 @@ struct Tracer {
             for (int c = 0; c < 3; ++c) tan->thr[3 * dw[j].k + c] += (double)thr[c] * dw[j].d[c];
     }
     // radiance += throughput * X:  d rad += d thr * X + thr * dX
-    void tan_add(v3 thr, v3 X, const DW* dw, int n) {
+    void tan_add(Col thr, Col X, const DW* dw, int n) {
         if (!tan) return;
         for (int k = 0; k < tan->K; ++k)
             for (int c = 0; c < 3; ++c) tan->rad[3 * k + c] += tan->thr[3 * k + c] * (double)X[c];
@@ -1117,7 +1256,7 @@ struct Tracer {
         return (m >= 0 && d.materials[m].model == PTR_MAT_DIELECTRIC) ? slot_k(m, PTR_GRAD_IOR) : -1;
     }
     // the per-parameter derivatives X dlog_k of X from its log-derivatives, appended at n
-    static int dw_from_dlog(v3 X, const std::vector<std::pair<int, double>>& dlog, std::vector<DW>& out, int n) {
+    static int dw_from_dlog(Col X, const std::vector<std::pair<int, double>>& dlog, std::vector<DW>& out, int n) {
         if (out.size() < (size_t)n + dlog.size()) out.resize((size_t)n + dlog.size());
         for (const auto& e : dlog) {
             out[n].k = e.first;
@@ -1144,8 +1283,12 @@ struct Tracer {
         const float* p = d.env.radiance + 4 * ((size_t)j * d.env.width + i);
         return v3(p[0], p[1], p[2]);
     }
-    v3 environment_radiance(v3 dir) const {
-        if (d.env.kind == PTR_ENV_CONSTANT) return ld3(d.env.color) * d.env.intensity;
+    Col environment_radiance(v3 dir) const {
+        if (d.env.kind == PTR_ENV_CONSTANT) return c_env() * d.env.intensity;
+        if constexpr (SPECTRAL) return Col(0.0f);   // spectral programs take constant environments only
+        else return image_radiance(dir);
+    }
+    v3 image_radiance(v3 dir) const {
         if (d.env.kind != PTR_ENV_IMAGE) return v3(0.0f);
         const int W = d.env.width, H = d.env.height;
         float u, v;
@@ -1202,8 +1345,8 @@ struct Tracer {
         float rr = 2.0f * std::sqrt(h * (1.0f - h));
         return v3(rr * std::cos(phi), y, rr * std::sin(phi));
     }
-    LightSample environment_sample(float x0, float x1) const {
-        LightSample ls;
+    LS environment_sample(float x0, float x1) const {
+        LS ls;
         if (d.env.kind == PTR_ENV_IMAGE) {
             float a = uniform_fraction();
             if (x0 < a) {
@@ -1226,7 +1369,7 @@ struct Tracer {
         float phi = TWO_PI * x1;
         ls.wi = v3(r * std::cos(phi), z, r * std::sin(phi));
         ls.distance = MAX_DIST;
-        ls.radiance = ld3(d.env.color) * d.env.intensity;
+        ls.radiance = c_env() * d.env.intensity;
         ls.pdf = 1.0f / (4.0f * PI);
         ls.flags = 0u;
         ls.light_id = -1;
@@ -1258,9 +1401,10 @@ struct Tracer {
         n = normalize(cross(b - a, c - a));
         return a * (1.0f - su) + b * (su * (1.0f - x1)) + c * (su * x1);
     }
-    LightSample light_sample_one(const ptr_light& l, v3 p, float x0, float x1) const {
-        LightSample ls;
-        ls.radiance = ld3(l.radiance);
+    LS light_sample_one(const ptr_light& l, v3 p, float x0, float x1) const {
+        LS ls;
+        const int li = (int)(&l - d.lights);
+        ls.radiance = c_light(li);
         ls.flags = 0u;
         ls.light_id = -1;
         if (l.kind == PTR_LIGHT_MESH) {   // radiance without falloff; one-sided
@@ -1317,7 +1461,7 @@ struct Tracer {
         float d2 = dot(dd, dd);
         ls.wi = dd * (1.0f / std::sqrt(d2));
         ls.distance = std::sqrt(d2);
-        ls.radiance = ld3(l.radiance) / d2;
+        ls.radiance = c_light(li) / d2;
         ls.pdf = 1.0f;
         ls.flags = LIGHT_DELTA;
         return ls;
@@ -1347,8 +1491,8 @@ struct Tracer {
         return 0.0f;
     }
     // lighting_sample_finite: power CDF + cdf_rescale (features/lighting.ts:546-637)
-    LightSample lighting_sample_finite(v3 p, float x0, float x1) const {
-        LightSample ls;
+    LS lighting_sample_finite(v3 p, float x0, float x1) const {
+        LS ls;
         if (d.n_lights == 1) {
             ls = light_sample_one(d.lights[0], p, x0, x1);
             ls.light_id = 0;
@@ -1435,8 +1579,8 @@ struct Tracer {
         }
         return pmf;
     }
-    LightSample lighting_sample_tree(const Query& q, float x0, float x1) {
-        LightSample ls;
+    LS lighting_sample_tree(const Query& q, float x0, float x1) {
+        LS ls;
         float sel;
         int id = tree_pick(q, x0, sel);
         if (id < 0) { ls.pdf = 0.0f; return ls; }
@@ -1448,20 +1592,20 @@ struct Tracer {
     }
 
     // lighting_sample: two-stage env-vs-finite (features/lighting.ts generateLightSampling)
-    LightSample lighting_sample(const Query& q, float x0, float x1) {
+    LS lighting_sample(const Query& q, float x0, float x1) {
         if (d.n_lights == 0) {
             if (S.env_samplable) return environment_sample(x0, x1);
-            LightSample ls; ls.pdf = 0.0f; return ls;
+            LS ls; ls.pdf = 0.0f; return ls;
         }
         if (!S.env_select_live) return S.tree ? lighting_sample_tree(q, x0, x1) : lighting_sample_finite(q.p, x0, x1);
         float pe = d.env.select_prob;
         if (x0 < pe) {
-            LightSample ls = environment_sample(clampf(x0 / pe, 0.0f, 0.9999999f), x1);
+            LS ls = environment_sample(clampf(x0 / pe, 0.0f, 0.9999999f), x1);
             ls.pdf *= pe;
             return ls;
         }
         float fx = clampf((x0 - pe) / (1.0f - pe), 0.0f, 0.9999999f);
-        LightSample ls = S.tree ? lighting_sample_tree(q, fx, x1) : lighting_sample_finite(q.p, fx, x1);
+        LS ls = S.tree ? lighting_sample_tree(q, fx, x1) : lighting_sample_finite(q.p, fx, x1);
         ls.pdf *= (1.0f - pe);
         return ls;
     }
@@ -1485,14 +1629,15 @@ struct Tracer {
     // ---- material dispatch (features/materials.ts:902-954)
     float hit_alpha = -1.0f;   // the current vertex's per-triangle alpha (mesh hits)
     float alpha_of(const ptr_material& m) const { return hit_alpha >= 0.0f ? hit_alpha : m.alpha; }
-    ISample surface_sample(const ptr_material& m, v3 wo, const Hit& h, float uc, float u0, float u1) const {
-        if (m.model == PTR_MAT_LAMBERT) return lambert_sample(wo, h, m, uc, u0, u1);
-        if (m.model == PTR_MAT_GGX) return ggx_sample(wo, h, m, alpha_of(m), u0, u1);
-        if (m.model == PTR_MAT_MIRROR) return mirror_sample(wo, h, m);
+    IS surface_sample(const ptr_material& m, v3 wo, const Hit& h, float uc, float u0, float u1) const {
+        const int mi = mat_index(m);
+        if (m.model == PTR_MAT_LAMBERT) return lambert_sample(wo, h, c_albedo(mi), uc, u0, u1);
+        if (m.model == PTR_MAT_GGX) return ggx_sample(wo, h, c_f0(mi), alpha_of(m), u0, u1);
+        if (m.model == PTR_MAT_MIRROR) return mirror_sample(wo, h, c_f0(mi));
         if (m.model == PTR_MAT_ROUGH_DIELECTRIC) {
-            ISample s = rough_dielectric_sample_local(mf_to_local(h.frame, wo), m, alpha_of(m), S.ior_of(h.region_from),
-                                                      S.ior_of(h.region_to), uc, u0, u1);
-            if (s.weight.x == 0.0f && s.weight.y == 0.0f && s.weight.z == 0.0f && !(s.flags & LOBE_DELTA)) s.wi = wo;
+            IS s = rough_dielectric_sample_local(mf_to_local(h.frame, wo), c_tint(mi), alpha_of(m), S.ior_of(h.region_from),
+                                                 S.ior_of(h.region_to), uc, u0, u1);
+            if (spectrum_is_zero(s.weight) && !(s.flags & LOBE_DELTA)) s.wi = wo;
             else if (s.flags & LOBE_DELTA) s.wi = -wo;
             else s.wi = mf_from_local(h.frame, s.wi);
             return s;
@@ -1503,10 +1648,10 @@ struct Tracer {
         v3 n = h.frame.n;
         float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
         float F = dielectric_fresnel(cos_i, eta);
-        ISample s;
+        IS s;
         if (uc < F) {
             s.wi = normalize(2.0f * cos_i * n - wo);
-            s.weight = v3(1.0f);
+            s.weight = Col(1.0f);
             s.pdf = 0.0f;
             s.flags = LOBE_REFLECTION | LOBE_DELTA;
         } else {
@@ -1514,19 +1659,20 @@ struct Tracer {
             float cos_t = std::sqrt(fmaxf_(0.0f, 1.0f - sin2_t));
             s.wi = normalize(-eta * wo + (eta * cos_i - cos_t) * n);
             float radiance_scale = (n_i * n_i) / (n_t * n_t);
-            s.weight = ld3(m.transmittance) * radiance_scale;
+            s.weight = c_tint(mi) * radiance_scale;
             s.pdf = 0.0f;
             s.flags = LOBE_TRANSMISSION | LOBE_DELTA;
         }
         return s;
     }
-    v3 surface_eval(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
-        if (m.model == PTR_MAT_LAMBERT) return lambert_eval(wi, wo, h, m);
-        if (m.model == PTR_MAT_GGX) return ggx_eval(wi, wo, h, m, alpha_of(m));
+    Col surface_eval(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
+        const int mi = mat_index(m);
+        if (m.model == PTR_MAT_LAMBERT) return lambert_eval(wi, wo, h, c_albedo(mi));
+        if (m.model == PTR_MAT_GGX) return ggx_eval(wi, wo, h, c_f0(mi), alpha_of(m));
         if (m.model == PTR_MAT_ROUGH_DIELECTRIC)
-            return rough_dielectric_eval_local(mf_to_local(h.frame, wi), mf_to_local(h.frame, wo), m, alpha_of(m),
+            return rough_dielectric_eval_local(mf_to_local(h.frame, wi), mf_to_local(h.frame, wo), c_tint(mi), alpha_of(m),
                                                S.ior_of(h.region_from), S.ior_of(h.region_to));
-        return v3(0.0f);
+        return Col(0.0f);
     }
     float surface_pdf(const ptr_material& m, v3 wi, v3 wo, const Hit& h) const {
         if (m.model == PTR_MAT_LAMBERT) return lambert_pdf(wi, wo, h);
@@ -1542,9 +1688,8 @@ struct Tracer {
     bool scatter_live(int med) const { return P.scattering && (d.materials[med].flags & PTR_MATF_SCATTERING); }
     // medium_transmittance (analytic.glsl:49-51): Beer-Lambert over sigma_t; under
     // scattering 'ignored' the medium is absorbing-only (sigma_t = sigma_a)
-    v3 medium_transmittance(int med, float len) const {
-        const ptr_material& m = d.materials[med];
-        v3 st = scatter_live(med) ? ld3(m.sigma_a) + ld3(m.sigma_s) : ld3(m.sigma_a);
+    Col medium_transmittance(int med, float len) const {
+        Col st = scatter_live(med) ? c_sigma_a(med) + c_sigma_s(med) : c_sigma_a(med);
         return vexp(-st * len);
     }
     // ---- heterogeneous media: the D1-clamped fields and the tracking arms
@@ -1619,22 +1764,21 @@ struct Tracer {
     }
     uint32_t shadow_seed = 0;   // the path's sampler dimension at the current NEE site
 
-    v3 medium_survival(int med) const {
-        const ptr_material& m = d.materials[med];
-        v3 sa = ld3(m.sigma_a), ss = ld3(m.sigma_s);
-        return ss / vmax(ss + sa, v3(1e-9f));
+    Col medium_survival(int med) const {
+        Col sa = c_sigma_a(med), ss = c_sigma_s(med);
+        return ss / vmax(ss + sa, Col(1e-9f));
     }
 
     // shadow_transmittance: opaque (transport/shadow/opaque/opaque.glsl:16-19) or the
     // media segment walker (transport/shadow/media/media.glsl:29-62)
     // dlog (forward mode): d log T / d theta_k of every medium segment crossed, appended
-    v3 shadow_transmittance(Ray sr, v3 light_p, int crossings_left, std::vector<std::pair<int, double>>* dlog = nullptr) {
+    Col shadow_transmittance(Ray sr, v3 light_p, int crossings_left, std::vector<std::pair<int, double>>* dlog = nullptr) {
         cnt.shadow++;
         if (!S.has_media) {
             float maxDist = length(light_p - sr.o) - SHADOW_BACKOFF;
-            return S.scene_intersect_any(sr, maxDist) ? v3(0.0f) : v3(1.0f);
+            return S.scene_intersect_any(sr, maxDist) ? Col(0.0f) : Col(1.0f);
         }
-        v3 T(1.0f);
+        Col T(1.0f);
         int medium = S.scene_region_at(sr.o);
         Ray seg = sr;
         Rng srng;
@@ -1646,9 +1790,9 @@ struct Tracer {
             bool hit_boundary = S.scene_intersect(seg, h) && h.t < remaining;
             float seg_len = hit_boundary ? h.t : remaining;
             int med_mat = S.material_of(medium);
-            if (S.material_has_medium(med_mat) && is_het(med_mat)) {
+            if (S.material_has_medium(med_mat) && !SPECTRAL && is_het(med_mat)) {
                 if (!srng_live) { srng = shadow_rng(rng.base, shadow_seed); srng_live = true; }
-                T = T * medium_ratio_track(d.materials[med_mat], seg, seg_len, srng, scatter_live(med_mat));
+                if constexpr (!SPECTRAL) T = T * medium_ratio_track(d.materials[med_mat], seg, seg_len, srng, scatter_live(med_mat));
             } else if (S.material_has_medium(med_mat)) {
                 T = T * medium_transmittance(med_mat, seg_len);
                 if (dlog) {   // T_seg = exp(-sigma len), sigma = st (scattering) or (1 - a) st
@@ -1663,12 +1807,12 @@ struct Tracer {
                 }
             }
             if (!hit_boundary) return T;
-            if (!S.is_null_interface(S.material_of(h.region_owner))) return v3(0.0f);
+            if (!S.is_null_interface(S.material_of(h.region_owner))) return Col(0.0f);
             medium = h.region_to;
             seg = ray_spawn(h, seg.d);
             seg.d = normalize(light_p - seg.o);
         }
-        return v3(0.0f);
+        return Col(0.0f);
     }
 
     static float power_heuristic(float pf, float pg) {
@@ -1684,7 +1828,7 @@ struct Tracer {
     // the reference.  Area lights (quad, sphere) are an extension the reference's
     // Validator rejects: a uniform point on the light's area is drawn first (two more
     // numbers), the estimate then carries Le * cos_l / (d^2 * pdf_area).
-    void equiangular_sample_direct(const Ray& r, int med_mat, float t_max, v3 thr, v3& radiance, int crossings_left) {
+    void equiangular_sample_direct(const Ray& r, int med_mat, float t_max, Col thr, Col& radiance, int crossings_left) {
         const ptr_material& mm = d.materials[med_mat];
         float uc = rng.next();
         int id = d.n_lights - 1;
@@ -1728,27 +1872,27 @@ struct Tracer {
         float t = t_c + h * std::tan(theta);
         float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
         v3 p_evt = r.o + r.d * t;
-        v3 sigma_s = ld3(mm.sigma_s);
+        Col sigma_s = c_sigma_s(med_mat);
         if (spectrum_is_black(sigma_s)) return;
-        v3 T_seg = vexp(-(ld3(mm.sigma_a) + sigma_s) * t);
+        Col T_seg = vexp(-(c_sigma_a(med_mat) + sigma_s) * t);
         v3 to_light = pos - p_evt;
         float d2 = fmaxf_(dot(to_light, to_light), 1e-8f);
         float dist = std::sqrt(d2);
         v3 wi = to_light / dist;
-        v3 Le;
+        Col Le;
         float denom;
         if (area) {
             float cos_l = dot(nl, -wi);
             if (!(cos_l > 0.0f)) return;
-            Le = ld3(l.radiance) * (cos_l / d2);
+            Le = c_light(id) * (cos_l / d2);
             denom = pdf_t * (pdf_area * sel);
         } else {
-            Le = ld3(l.radiance) / d2;
+            Le = c_light(id) / d2;
             denom = pdf_t * sel;
         }
-        v3 vis = shadow_transmittance(Ray{p_evt, wi}, pos, crossings_left);
+        Col vis = shadow_transmittance(Ray{p_evt, wi}, pos, crossings_left);
         if (spectrum_is_black(vis)) return;
-        v3 ph(hg_eval(wi, -r.d, mm.phase_g));
+        Col ph(hg_eval(wi, -r.d, mm.phase_g));
         radiance = radiance + thr * T_seg * sigma_s * ph * Le * vis / denom;
     }
 
@@ -1756,7 +1900,7 @@ struct Tracer {
     // GGX: w = f cos / pdf with the pdf detached, so dw = w d log fs(alpha).  Dielectric:
     // w = F / F_detached (reflection) or T (n_i / n_t)^2 (1 - F) / (1 - F)_detached
     // (refraction), differentiated along the IORs of the two regions the interface joins.
-    void tan_continuation(const ptr_material& m, int mat, v3 wo, const Hit& hit, const ISample& bs, v3 thr, DW* dw) {
+    void tan_continuation(const ptr_material& m, int mat, v3 wo, const Hit& hit, const IS& bs, Col thr, DW* dw) {
         int n = 0;
         if (m.model == PTR_MAT_LAMBERT) {
             for (int c = 0; c < 3; ++c) {
@@ -1797,13 +1941,13 @@ struct Tracer {
     }
 
     // ---- the walk (transport/integrators/pt/pt.ts:299-464, as emitted for media scenes)
-    v3 transport_trace(Ray ray) {
+    Col transport_trace(Ray ray) {
         const bool nee = P.direct != PTR_DIRECT_NONE;
         const bool mis = P.direct == PTR_DIRECT_MIS;
         const bool media = S.has_media;
         const int N = P.max_bounces;
         // path_state_init (pt.ts:147-176)
-        v3 throughput(1.0f), radiance(0.0f);
+        Col throughput(1.0f), radiance(0.0f);
         bool prev_was_delta = true;
         float prev_bsdf_pdf = 0.0f;
         v3 prev_qp = ray.o;
@@ -1824,7 +1968,7 @@ struct Tracer {
             throughput = throughput / p_survive;
             return true;
         };
-        auto roulette_interior = [&](int bounce, v3 survival) -> bool {   // pt.ts:230-283
+        auto roulette_interior = [&](int bounce, Col survival) -> bool {   // pt.ts:230-283
             if (P.rr_start < 0) return true;
             if (bounce < P.rr_start) return true;
             float p_survive = spectrum_max(survival);
@@ -1869,9 +2013,9 @@ struct Tracer {
                     float x0 = rng.next(), x1 = rng.next();
                     float t_max = boundary ? hit.t : MAX_DIST;
                     const ptr_material& mm = d.materials[med_mat];
-                    const bool het = is_het(med_mat);
+                    const bool het = !SPECTRAL && is_het(med_mat);
                     if (het && !scatter_live(med_mat)) {   // ratio-tracked pass-through
-                        throughput = throughput * medium_ratio_track(mm, r, t_max, rng, false);
+                        if constexpr (!SPECTRAL) throughput = throughput * medium_ratio_track(mm, r, t_max, rng, false);
                     } else if (!scatter_live(med_mat)) {
                         // absorbing-only arm (deterministic): weight = exp(-sigma_a t_max)
                         if (tan) {   // exp(-(1 - a) st t_max)
@@ -1881,16 +2025,21 @@ struct Tracer {
                             const Dual w_a = dexp(-(1.0 - Dual{a, 1.0}) * st * (double)t_max);
                             dw[0] = {slot_k(med_mat, PTR_GRAD_SIGMA_T), {w_st.d, w_st.d, w_st.d}};
                             dw[1] = {slot_k(med_mat, PTR_GRAD_MEDIUM_ALBEDO), {w_a.d, w_a.d, w_a.d}};
-                            tan_mul(throughput, vexp(-ld3(mm.sigma_a) * t_max), dw.data(), 2);
+                            tan_mul(throughput, vexp(-c_sigma_a(med_mat) * t_max), dw.data(), 2);
                         }
-                        throughput = throughput * vexp(-ld3(mm.sigma_a) * t_max);
+                        throughput = throughput * vexp(-c_sigma_a(med_mat) * t_max);
                     } else {
-                        MediumSample ms = het ? medium_sample_delta(mm, r, t_max, x0, x1)
-                                              : medium_sample_analytic(mm, r, t_max, x0, x1);
+                        MS ms;
+                        if constexpr (!SPECTRAL) {
+                            ms = het ? medium_sample_delta(mm, r, t_max, x0, x1)
+                                     : medium_sample_analytic(c_sigma_a(med_mat), c_sigma_s(med_mat), r, t_max, x0, x1);
+                        } else {
+                            ms = medium_sample_analytic(c_sigma_a(med_mat), c_sigma_s(med_mat), r, t_max, x0, x1);
+                        }
                         if (tan) {   // free flight with the detached channel-MIS density
                             double st, a;
                             grey_params(med_mat, st, a);
-                            const v3 sigma_t = ld3(mm.sigma_a) + ld3(mm.sigma_s);
+                            const Col sigma_t = c_sigma_a(med_mat) + c_sigma_s(med_mat);
                             if (ms.scattered) {   // a st exp(-st t) / pdf
                                 const float pdf = fmaxf_(spectrum_average(sigma_t * vexp(-sigma_t * ms.t)), 1e-20f);
                                 const Dual w_st = a * Dual{st, 1.0} * dexp(-Dual{st, 1.0} * (double)ms.t) / (double)pdf;
@@ -1914,19 +2063,19 @@ struct Tracer {
                             // the equiangular site replaces it (pt.ts:379)
                             if (nee && !P.equiangular) {
                                 float y0 = rng.next(), y1 = rng.next();
-                                LightSample ls = lighting_sample(Query{p_evt, v3(0.0f), false}, y0, y1);
+                                LS ls = lighting_sample(Query{p_evt, v3(0.0f), false}, y0, y1);
                                 shadow_seed = rng.dim;
                                 if (ls.pdf > 0.0f) {
                                     v3 light_p = p_evt + ls.wi * ls.distance;
                                     dlog_vis.clear();
-                                    v3 vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings,
-                                                                  tan ? &dlog_vis : nullptr);
+                                    Col vis = shadow_transmittance(Ray{p_evt, ls.wi}, light_p, shadow_left_base - null_crossings,
+                                                                   tan ? &dlog_vis : nullptr);
                                     if (!spectrum_is_black(vis)) {
                                         float w = 1.0f;
                                         if (mis && !(ls.flags & LIGHT_DELTA))   // hg_pdf = spectrum_average(hg_eval)
-                                            w = power_heuristic(ls.pdf, spectrum_average(v3(hg_eval(ls.wi, wo_med, mm.phase_g))));
+                                            w = power_heuristic(ls.pdf, spectrum_average(Col(hg_eval(ls.wi, wo_med, mm.phase_g))));
                                         if (tan) {   // X = Le p_HG(g) T w / pdf
-                                            const v3 X = ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
+                                            const Col X = ls.radiance * Col(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
                                             const Dual ph = hg_dual(ls.wi, wo_med, Dual{(double)mm.phase_g, 1.0});
                                             int n = 0;
                                             dw[n].k = slot_k(med_mat, PTR_GRAD_HG_G);
@@ -1935,13 +2084,13 @@ struct Tracer {
                                             n = dw_from_dlog(X, dlog_vis, dw, n + 1);
                                             tan_add(throughput, X, dw.data(), n);
                                         }
-                                        radiance = radiance + throughput * ls.radiance * v3(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
+                                        radiance = radiance + throughput * ls.radiance * Col(hg_eval(ls.wi, wo_med, mm.phase_g)) * vis * w / ls.pdf;
                                     }
                                 }
                             }
                             // kernel_sample_phase (techniques/kernel/kernel_phase.glsl:7-15)
                             float z0 = rng.next(), z1 = rng.next();
-                            ISample ps = hg_sample(wo_med, mm.phase_g, z0, z1);
+                            IS ps = hg_sample<Col>(wo_med, mm.phase_g, z0, z1);
                             if (tan) {   // p_HG(g) / pdf
                                 const Dual ph = hg_dual(ps.wi, wo_med, Dual{(double)mm.phase_g, 1.0});
                                 const double dg = ph.d / (double)ps.pdf;
@@ -1982,29 +2131,29 @@ struct Tracer {
             // kernel_score_emitter_hit (kernel.glsl:16-25)
             int mat_emit = S.material_of(hit.region_to);
             if (S.material_is_emissive(mat_emit)) {
-                if (tan) tan_add(throughput, w_emitter(hit) * ld3(d.materials[mat_emit].emission), nullptr, 0);
-                radiance = radiance + throughput * w_emitter(hit) * ld3(d.materials[mat_emit].emission);
+                if (tan) tan_add(throughput, w_emitter(hit) * c_emission(mat_emit), nullptr, 0);
+                radiance = radiance + throughput * w_emitter(hit) * c_emission(mat_emit);
             }
             if (bounce == N) break;
             const ptr_material& m = d.materials[mat];
             // light_sample_direct (techniques/light/light.glsl:8-28)
             if (nee && S.material_has_nondelta_lobes(mat)) {
                 float y0 = rng.next(), y1 = rng.next();
-                LightSample ls = lighting_sample(Query{hit.p, hit.frame.n, m.model == PTR_MAT_ROUGH_DIELECTRIC}, y0, y1);
+                LS ls = lighting_sample(Query{hit.p, hit.frame.n, m.model == PTR_MAT_ROUGH_DIELECTRIC}, y0, y1);
                 shadow_seed = rng.dim;
                 if (ls.pdf > 0.0f) {
                     v3 light_p = hit.p + ls.wi * ls.distance;
                     Ray sr = ray_spawn(hit, ls.wi);
                     sr.d = normalize(light_p - sr.o);
                     dlog_vis.clear();
-                    v3 vis = shadow_transmittance(sr, light_p, shadow_left_base - null_crossings, tan ? &dlog_vis : nullptr);
+                    Col vis = shadow_transmittance(sr, light_p, shadow_left_base - null_crossings, tan ? &dlog_vis : nullptr);
                     if (!spectrum_is_black(vis)) {
-                        v3 f = surface_eval(m, ls.wi, wo, hit);
+                        Col f = surface_eval(m, ls.wi, wo, hit);
                         float cos_i = std::fabs(dot(ls.wi, hit.frame.n));
                         float w = 1.0f;
                         if (mis && !(ls.flags & LIGHT_DELTA)) w = power_heuristic(ls.pdf, surface_pdf(m, ls.wi, wo, hit));
                         if (tan) {   // X = Le f cos T w / pdf
-                            const v3 X = ls.radiance * f * cos_i * vis * w / ls.pdf;
+                            const Col X = ls.radiance * f * cos_i * vis * w / ls.pdf;
                             int n = 0;
                             if (m.model == PTR_MAT_LAMBERT) {   // f = albedo / pi
                                 for (int c = 0; c < 3; ++c) {
@@ -2031,7 +2180,7 @@ struct Tracer {
             // kernel_sample_continuation (kernel.glsl:27-34)
             float uc = rng.next();
             float u0 = rng.next(), u1 = rng.next();
-            ISample bs = surface_sample(m, wo, hit, uc, u0, u1);
+            IS bs = surface_sample(m, wo, hit, uc, u0, u1);
             if (spectrum_is_black(bs.weight)) break;
             if (tan) tan_continuation(m, mat, wo, hit, bs, throughput, dw.data());
             throughput = throughput * bs.weight;
@@ -2051,6 +2200,7 @@ struct Tracer {
         return radiance;
     }
 };
+using Tracer = TracerT<v3>;
 
 // camera_generateRay (camera/pinhole/pinhole.glsl:4-18) + pixel_sample (pixel/box/box.glsl:5)
 inline Ray camera_ray(const ptr_camera& c, int W, int H, float fx, float fy) {
@@ -2189,8 +2339,14 @@ int oracle_forward_tile(const ptr_scene_desc* sd, const ptr_program_desc* pd, co
     return 0;
 }
 
-static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
-                             double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
+// The RGB walk, or the spectral one: four wavelengths drawn between the film point and
+// the lens draws (accumulation.ts main(): cameraSample, then wavelengths_sample), each
+// sample's lanes projected to linear sRGB by color_to_pixel before the fold.
+}  // extern "C"
+
+template <class Col>
+static int render_tile_scene_t(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
+                               double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
     // engine.imageSize: the full image when this frame is a tile of it (pinhole.glsl:6)
     const int W = fr->image_size[0] > 0 ? fr->image_size[0] : fr->width;
     const int H = fr->image_size[1] > 0 ? fr->image_size[1] : fr->height;
@@ -2198,7 +2354,7 @@ static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0
     if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel reduction(+ : closest, shadow)
     {
-        Tracer T(S);
+        TracerT<Col> T(S);
 #pragma omp for schedule(dynamic, 1)
         for (int ty = 0; ty < th; ++ty) {
             const int y = y0 + ty;
@@ -2214,9 +2370,16 @@ static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0
                     float pyf = (float)y + 0.5f + (float)fr->pixel_offset[1];
                     float a0 = T.rng.next(), a1 = T.rng.next();
                     float fx = pxf + (a0 - 0.5f), fy = pyf + (a1 - 0.5f);
+                    float lam[4], lpdf[4];
+                    if constexpr (std::is_same<Col, s4>::value) {
+                        wavelengths_sample(*S.prog, T.rng.next(), lam, lpdf);
+                        for (int q = 0; q < 4; ++q) T.wl[q] = lam[q];
+                    }
                     T.rng.next(); T.rng.next();   // xiLens (pinhole ignores it)
                     Ray r = camera_ray(fr->camera, W, H, fx, fy);
-                    v3 L = T.transport_trace(r);
+                    v3 L;
+                    if constexpr (std::is_same<Col, s4>::value) L = color_to_pixel(*S.d, T.transport_trace(r), lam, lpdf);
+                    else L = T.transport_trace(r);
                     if (samples_out) {
                         float* o = samples_out + 3 * ((size_t)k * tw * th + pix);
                         o[0] = L.x; o[1] = L.y; o[2] = L.z;
@@ -2237,6 +2400,17 @@ static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0
     return 0;
 }
 
+static int render_tile_scene(const Scene& S, const ptr_frame* fr, int x0, int y0, int tw, int th,
+                             double* sum, double* sumsq, float* samples_out, uint64_t* out_counts, int threads) {
+    if (S.prog->color == PTR_COLOR_SPECTRAL) {
+        if (!S.d->spectral) return -1;
+        return render_tile_scene_t<s4>(S, fr, x0, y0, tw, th, sum, sumsq, samples_out, out_counts, threads);
+    }
+    return render_tile_scene_t<v3>(S, fr, x0, y0, tw, th, sum, sumsq, samples_out, out_counts, threads);
+}
+
+extern "C" {
+
 
 // The rough dielectric in its local frame (n = +z, wo in the upper hemisphere), for the
 // BSDF property tests: eval (rgb) and pdf of n (wi, wo) pairs; n samples for n (uc, u0, u1).
@@ -2246,7 +2420,7 @@ int oracle_rough_dielectric_eval_n(int n, float alpha, float n_i, float n_t, con
     for (int c = 0; c < 3; ++c) m.transmittance[c] = tint[c];
     for (int k = 0; k < n; ++k) {
         v3 wil(wi[3 * k], wi[3 * k + 1], wi[3 * k + 2]), wol(wo[3 * k], wo[3 * k + 1], wo[3 * k + 2]);
-        v3 f = rough_dielectric_eval_local(wil, wol, m, alpha, n_i, n_t);
+        v3 f = rough_dielectric_eval_local(wil, wol, ld3(m.transmittance), alpha, n_i, n_t);
         f_out[3 * k] = f.x; f_out[3 * k + 1] = f.y; f_out[3 * k + 2] = f.z;
         pdf_out[k] = rough_dielectric_pdf_local(wil, wol, alpha, n_i, n_t);
     }
@@ -2257,8 +2431,8 @@ int oracle_rough_dielectric_sample_n(int n, float alpha, float n_i, float n_t, c
     ptr_material m{};
     for (int c = 0; c < 3; ++c) m.transmittance[c] = tint[c];
     for (int k = 0; k < n; ++k) {
-        ISample smp = rough_dielectric_sample_local(v3(wo[3 * k], wo[3 * k + 1], wo[3 * k + 2]), m, alpha, n_i, n_t,
-                                                    u[3 * k], u[3 * k + 1], u[3 * k + 2]);
+        ISample smp = rough_dielectric_sample_local(v3(wo[3 * k], wo[3 * k + 1], wo[3 * k + 2]), ld3(m.transmittance),
+                                                    alpha, n_i, n_t, u[3 * k], u[3 * k + 1], u[3 * k + 2]);
         wi_out[3 * k] = smp.wi.x; wi_out[3 * k + 1] = smp.wi.y; wi_out[3 * k + 2] = smp.wi.z;
         weight_out[3 * k] = smp.weight.x; weight_out[3 * k + 1] = smp.weight.y; weight_out[3 * k + 2] = smp.weight.z;
         pdf_out[k] = smp.pdf;

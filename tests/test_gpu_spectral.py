@@ -145,3 +145,38 @@ def test_media_workload_renders():
         assert eng.counters()["error_flags"] == 0
     finally:
         eng.close()
+
+
+# ---- the device against the oracle's spectral walk, sample for sample ------------------
+# Same packed scene, same counter-based random numbers, same four wavelengths per sample
+# (the oracle restates wavelengths_sample, the lifted-record evaluation and color_to_pixel):
+# the gates of test_gpu_parity.compare.
+
+@pytest.mark.parametrize("spectral", [True, False], ids=["spectral", "rgb"])
+def test_media_workload_matches_oracle(engine, oracle_lib, spectral):
+    """The media + spectral configuration itself: a chromatic medium (sigma_t 0.5, 1, 2)
+    inside an IOR-1.33 boundary, a grey null-interface medium, a 3000 K sphere light under
+    equiangular sampling and a quad at radiance 20, depth 64; and its RGB twin."""
+    from test_gpu_parity import compare
+    sc, st, _ = scenes.media_scene(spectral=spectral)
+    compare(engine, oracle_lib, sc, st, 48, 48, 8, {})
+
+
+@pytest.mark.parametrize("case", ["furnace", "blackbody", "grey-cornell"])
+def test_spectral_witnesses_match_oracle(engine, oracle_lib, case):
+    from test_gpu_parity import compare
+    if case == "furnace":
+        scene = {"id": "furnace", "objects": [{"type": "sphere", "parameters": {"center": [0, 0, 0], "radius": 1.0},
+                                               "material": "grey"}],
+                 "materials": {"grey": {"model": "lambert", "albedo": [0.8, 0.8, 0.8]}}, "lights": [],
+                 "environment": {"type": "constant", "color": [1.0, 1.0, 1.0], "intensity": 1.0}}
+        compare(engine, oracle_lib, scene, _strategy(max_bounces=8), 24, 24, 16,
+                {"camera.position": [0, 0, 3.5], "camera.target": [0, 0, 0], "camera.fov": 0.6})
+    elif case == "blackbody":
+        compare(engine, oracle_lib, _panel({"blackbody": {"kelvin": 3000.0, "scale": 2.0}}),
+                _strategy(lo=380.0, hi=780.0, wavelengths="uniform"), 16, 16, 16, CAM)
+    else:
+        sc, st = scenes.cornell(direct="mis")
+        st_s = dict(st, measurement=dict(st["measurement"], color="spectral"))
+        compare(engine, oracle_lib, sc, st_s, 32, 32, 8,
+                {"camera.position": [0, 1, 4], "camera.target": [0, 1, 0], "camera.fov": 0.698})
