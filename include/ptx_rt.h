@@ -354,10 +354,13 @@ int ptr_get_batch_profile(ptr_ctx* ctx, float* ms_out, int* launches_out, int n)
 int ptr_render_samples(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, float* host_out, size_t n);
 
 /* Nearest-hit queries on an uploaded scene: rays are n x (origin.xyz, direction.xyz);
- * per ray returns the region (-1 = miss), the instance element, the ORIGINAL triangle
- * index of a mesh hit (-1 otherwise) and t (1000 = MAX_DIST on a miss).  accel selects
- * the mesh BLAS walk (PTR_ACCEL_BVH / PTR_ACCEL_CWBVH).  The scene_intersect traversal
- * of the reference (features/intersection.ts:1665-1713) without the region probe. */
+ * per ray returns the region (-1 = miss), the instance (its index among the batch's
+ * placements; 0 for other regions), the ORIGINAL triangle index of a mesh hit (-1
+ * otherwise) and t (1000 = MAX_DIST on a miss).  accel selects the mesh BLAS walk
+ * (PTR_ACCEL_BVH / PTR_ACCEL_CWBVH).  The scene_intersect traversal of the reference
+ * (features/intersection.ts:1665-1713) without the region probe.  Hits at equal t go to
+ * the lower region, then the lower instance, then the lower triangle index, whatever
+ * order the walk visits them in. */
 int ptr_trace_closest(ptr_ctx* ctx, ptr_scene* scene, int accel, const float* rays, int n,
                       int* region, int* element, int* prim, float* t);
 

@@ -48,7 +48,7 @@ def lib():
         _lib.oracle_session_render_tile.restype = ctypes.c_int
         _lib.oracle_session_render_tile.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4 + [ctypes.c_int]
         _lib.oracle_trace_closest.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
-                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_mesh_brute.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         _lib.oracle_rough_dielectric_eval_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 5
         _lib.oracle_rough_dielectric_sample_n.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float] + [ctypes.c_void_p] * 7
@@ -210,16 +210,18 @@ class Session:
 
 
 def trace_closest(packed, renderer, rays):
-    """Nearest hit per ray (rays: n x 6 float32 origin, direction) -> (region, prim, t)."""
+    """Nearest hit per ray (rays: n x 6 float32 origin, direction) -> (region, instance,
+    prim, t); ties at equal t go to the lower region, instance and triangle index."""
     rays = np.ascontiguousarray(rays, np.float32)
     n = len(rays)
     region = np.zeros(n, np.int32)
+    element = np.zeros(n, np.int32)
     prim = np.zeros(n, np.int32)
     t = np.zeros(n, np.float32)
     desc = packed.desc()
     lib().oracle_trace_closest(ctypes.addressof(desc), ctypes.addressof(renderer.program), rays.ctypes.data, n,
-                               region.ctypes.data, prim.ctypes.data, t.ctypes.data)
-    return region, prim, t
+                               region.ctypes.data, element.ctypes.data, prim.ctypes.data, t.ctypes.data)
+    return region, element, prim, t
 
 
 def mesh_brute(packed, mesh_index, rays):

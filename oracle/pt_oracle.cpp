@@ -2442,9 +2442,11 @@ int oracle_rough_dielectric_sample_n(int n, float alpha, float n_i, float n_t, c
 }
 
 // Nearest-hit queries with the oracle's own acceleration: per ray (o.xyz, d.xyz) the
-// region (-1 = miss), the original triangle index (-1 if not a mesh hit) and t.
+// region (-1 = miss), the instance index (element; 0 outside instanced batches), the
+// original triangle index (-1 if not a mesh hit) and t.  Ties at equal t resolve in scan
+// order: the lower region, instance and triangle index.
 int oracle_trace_closest(const ptr_scene_desc* sd, const ptr_program_desc* pd, const float* rays, int n,
-                         int* region, int* prim, float* t_out) {
+                         int* region, int* element, int* prim, float* t_out) {
     Scene S(sd, pd);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int k = 0; k < n; ++k) {
@@ -2454,6 +2456,7 @@ int oracle_trace_closest(const ptr_scene_desc* sd, const ptr_program_desc* pd, c
         h.eps = MARCH_CLEARANCE;
         bool f = S.primitive_intersect(r, h);
         region[k] = f ? h.region_owner : -1;
+        if (element) element[k] = f ? h.element : 0;
         prim[k] = f ? h.prim : -1;
         t_out[k] = h.t;
     }

@@ -63,6 +63,17 @@ __device__ __forceinline__ void load_tri(const float4* tri, int i, f3& a, f3& e1
     float4 t0 = __ldg(tri + 3 * i), t1 = __ldg(tri + 3 * i + 1), t2 = __ldg(tri + 3 * i + 2);
     a = xyz(t0); e1 = xyz(t1); e2 = xyz(t2);
 }
+// The caller's index of the triangle in leaf slot i (stored in the record's first w).
+__device__ __forceinline__ int tri_orig(const float4* tri, int i) { return __float_as_int(__ldg(&tri[3 * (size_t)i].w)); }
+
+// Hits at equal t resolve in one order whatever the traversal visits first: the lower
+// region index, then the lower instance index (the caller's placement order), then the
+// lower triangle index of the caller's mesh.  The oracle's ordered scans give that order,
+// so hit IDs agree at ties too.  Node tests keep boxes entered exactly at the current t
+// (a tied triangle may sit on the box's near face); leaf tests take t == tmax only when
+// it wins the tie.  NoTie: no tie with the incoming tmax is won (a plain mesh region;
+// its incoming tmax belongs to an earlier region).
+struct NoTie { __device__ __forceinline__ bool operator()() const { return false; } };
 
 // ---- binary BVH walk --------------------------------------------------------------------
 __device__ __forceinline__ bool aabb_hit(float4 n0, float4 n1, f3 ro, f3 inv, float tmax) {
@@ -72,7 +83,7 @@ __device__ __forceinline__ bool aabb_hit(float4 n0, float4 n1, f3 ro, f3 inv, fl
     float tn = gmax(gmax(gmin(tx0, tx1), gmin(ty0, ty1)), gmin(tz0, tz1));
     float tf = gmin(gmin(gmax(tx0, tx1), gmax(ty0, ty1)), gmax(tz0, tz1)) * kBvhTfarPad;
     float tenter = gmax(tn, 0.0f);
-    return tf >= tenter && tenter < tmax;
+    return tf >= tenter && tenter <= tmax;
 }
 
 // Leaf(off, cnt) -> for nearest walks updates the caller's tmax itself; returns true to
@@ -229,28 +240,33 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
 }
 
 // ---- one mesh BLAS in a given frame (ro/rd already in the mesh's local frame) --------------
+// tie_in(): whether this walk wins a tie with the incoming tmax (a lower instance index
+// than the hit that set it); ties inside the walk go to the lower triangle index.
+template <class Tie = NoTie>
 __device__ __forceinline__ bool mesh_nearest(const DevScene& S, const DevMesh& m, f3 ro, f3 rd, float& tmax, int& prim,
-                                             Work* w = nullptr) {
+                                             Work* w = nullptr, Tie tie_in = Tie{}) {
     bool found = false;
+    const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
+    auto take = [&](int i, float t) {
+        return t > 0.0f && (t < tmax || (t == tmax && (found ? tri_orig(tri, i) < tri_orig(tri, prim) : tie_in())));
+    };
     if (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) {
-        const float4* tri = m.tri_w;
         walk_wide(S, m.cwbvh, ro, rd, tmax, [&](int i) {
             f3 a, e1, e2;
             if (w) w->tris++;
             load_tri(tri, i, a, e1, e2);
             float t;
-            if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
+            if (tri_test(ro, rd, a, e1, e2, t) && take(i, t)) { tmax = t; prim = i; found = true; }
             return false;
         }, w ? &w->nodes : nullptr);
     } else {
-        const float4* tri = m.tri;
         walk_binary(S, m.bvh, ro, rd, tmax, [&](int off, int cnt) {
             for (int i = off; i < off + cnt; ++i) {
                 f3 a, e1, e2;
                 if (w) w->tris++;
                 load_tri(tri, i, a, e1, e2);
                 float t;
-                if (tri_test(ro, rd, a, e1, e2, t) && t > 0.0f && t < tmax) { tmax = t; prim = i; found = true; }
+                if (tri_test(ro, rd, a, e1, e2, t) && take(i, t)) { tmax = t; prim = i; found = true; }
             }
             return false;
         }, w ? &w->nodes : nullptr);
@@ -400,7 +416,9 @@ struct InstFlat {
                     found = true;
                     return false;
                 }
-            } else if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f && tt < t) {
+            } else if (tri_test(ro, rd, a, e1, e2, tt) && tt > 0.0f &&
+                       (tt < t || (tt == t && (found ? tri_orig(m.tri_w, i) < tri_orig(m.tri_w, prim)
+                                                     : (h.region == region && __ldg(b.inst_id + inst) < __ldg(b.inst_id + h.element)))))) {
                 t = tt;
                 prim = i;
                 found = true;
@@ -456,12 +474,16 @@ __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_regio
     float t_near = h.t;
     const bool wide = S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w;
     const float4* place = wide ? b.place_w : b.place;
+    const int* inst_id = wide ? b.inst_id_w : b.inst_id;
+    // an instance wins a tie with the current hit when that hit is an instance of this
+    // batch with a higher placement index
+    auto wins_tie = [&](int i) { return h.region == region && __ldg(inst_id + i) < __ldg(inst_id + h.element); };
     // one instance: the params-tier sphere, or the mesh prototype in the placement's frame
     auto instance = [&](int i) {
         if (b.proto_shape == PTR_SHAPE_SPHERE) {
             float4 rec = __ldg(place + 2 * i);
             float t;
-            if (sphere_intersect(r, xyz(rec), rec.w, t) && t < t_near) {
+            if (sphere_intersect(r, xyz(rec), rec.w, t) && (t < t_near || (t == t_near && wins_tie(i)))) {
                 t_near = t; h.t = t; h.region = region; h.element = i; h.prim = -1;
             }
         } else {
@@ -472,7 +494,7 @@ __device__ __forceinline__ void accel_closest(const DevScene& S, const ptr_regio
             f3 rd = qrot(q, r.d) / s;
             int prim = -1;
             float t = t_near;
-            if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim, w)) {
+            if (mesh_nearest(S, S.meshes[b.proto_mesh], ro, rd, t, prim, w, [&] { return wins_tie(i); })) {
                 t_near = t; h.t = t; h.region = region; h.element = i; h.prim = prim;
             }
         }

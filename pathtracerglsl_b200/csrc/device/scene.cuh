@@ -39,6 +39,10 @@ struct DevBatch {
     // placement in the binary / wide TLAS leaf order (NULL: the instances are no lights)
     const int* light_of;
     const int* light_of_w;
+    // the caller's index of each placement in the binary / wide TLAS leaf order (the tie
+    // rule between instances, and the element a hit query reports)
+    const int* inst_id;
+    const int* inst_id_w;
 };
 
 struct DevScene {

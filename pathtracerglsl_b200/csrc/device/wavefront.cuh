@@ -1585,8 +1585,13 @@ __global__ void k_trace_rays(DevScene S, const float* rays, int n, int* region, 
             const float4* tri = (S.accel == PTR_ACCEL_CWBVH && m.cwbvh) ? m.tri_w : m.tri;
             orig = __float_as_int(tri[3 * h.prim].w);
         }
+        int el = h.element;
+        if (h.region >= 0 && S.regions[h.region].shape == PTR_SHAPE_INSTANCES) {   // the caller's instance index
+            const DevBatch& b = S.batches[S.regions[h.region].ref];
+            el = ((S.inst_accel == PTR_ACCEL_CWBVH && b.tlas_w) ? b.inst_id_w : b.inst_id)[h.element];
+        }
         region[k] = h.region;
-        element[k] = h.element;
+        element[k] = el;
         prim[k] = orig;
         t_out[k] = h.t;
     }

@@ -690,6 +690,13 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
         }
         if ((rc = dev_copy(ctx, s->allocs, rec_leaf.data(), rec_leaf.size(), &p4))) return rc;
         b.place = p4;
+        {
+            std::vector<int> ids(tl.order.begin(), tl.order.begin() + N);
+            const int* pi = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, ids.data(), ids.size(), &pi))) return rc;
+            b.inst_id = pi;
+        }
+        b.inst_id_w = nullptr;
         if ((rc = dev_copy(ctx, s->allocs, (const float4*)tl.nodes.data(), 2 * (size_t)tl.node_count, &p4))) return rc;
         b.tlas = p4;
         // the compressed wide twin of the TLAS (instanceAccel 'cwbvh', cwbvh.ts:80-372 over
@@ -706,6 +713,10 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
             const uint4* u4 = nullptr;
             if ((rc = dev_copy(ctx, s->allocs, rec_w.data(), rec_w.size(), &p4))) return rc;
             b.place_w = p4;
+            std::vector<int> ids(wt.order.begin(), wt.order.begin() + N);
+            const int* pid = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, ids.data(), ids.size(), &pid))) return rc;
+            b.inst_id_w = pid;
             if (bd.light_base >= 0) {
                 std::vector<int> lo(N);
                 for (int i = 0; i < N; ++i) lo[i] = bd.light_base + (int)wt.order[i];

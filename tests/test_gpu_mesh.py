@@ -49,32 +49,73 @@ def _trace(engine, accel, rays):
     return reg, el, prim, t
 
 
+_BRUTE = {}   # (level, rays seed) -> the brute-force answer, shared by both walks
+
+
+@pytest.mark.parametrize("level", [5, 8])
 @pytest.mark.parametrize("accel", [abi.ACCEL_BVH, abi.ACCEL_CWBVH])
-def test_mesh_hit_ids_bit_exact_vs_brute_force(engine, oracle_lib, accel):
-    sc, st = _plain_mesh_scene(5)
+def test_mesh_hit_ids_bit_exact_vs_brute_force(engine, oracle_lib, accel, level):
+    """20,000 rays against the level-5 icosphere (20,480 triangles) and the level-8 one of
+    the mesh configuration (1,310,720 triangles): triangle and t equal to a brute-force
+    scan, ties included (the lower triangle index wins on both sides)."""
+    sc, st = _plain_mesh_scene(level)
     r, pk = Compiler().compile(sc, st)
     engine.register_scene(pk)
     rays = _rays(20000, 1)
     reg, el, prim, t = _trace(engine, accel, rays)
-    bprim, bt = oracle_lib.mesh_brute(pk, 0, rays)
+    if (level, 1) not in _BRUTE:
+        _BRUTE[level, 1] = oracle_lib.mesh_brute(pk, 0, rays)
+    bprim, bt = _BRUTE[level, 1]
     assert (bprim >= 0).sum() > 5000
     np.testing.assert_array_equal(prim, bprim)
     np.testing.assert_array_equal(t[bprim >= 0], bt[bprim >= 0])
 
 
 @pytest.mark.parametrize("accel", [abi.ACCEL_BVH, abi.ACCEL_CWBVH])
-def test_instanced_mesh_hits_match_oracle(engine, oracle_lib, accel):
+@pytest.mark.parametrize("instance_accel", ["tlas", "cwbvh"])
+def test_instanced_mesh_hits_match_oracle(engine, oracle_lib, accel, instance_accel):
+    """Instanced meshes: region, instance, triangle and t equal to the oracle's ordered scan
+    over the instances, bit for bit, whichever TLAS and BLAS the device walks."""
     sc, st, _ = scenes.mesh_scene(level=4, instances=9, env_size=(64, 32))
+    st = dict(st, estimator=dict(st["estimator"], instanceAccel=instance_accel))
     r, pk = Compiler().compile(sc, st)
     engine.register_scene(pk)
+    engine.load_renderer(r)
     rays = _rays(40000, 2, spread=3.0, dist=10.0)
     reg, el, prim, t = _trace(engine, accel, rays)
-    oreg, oprim, ot = oracle_lib.trace_closest(pk, r, rays)
-    mesh_hits = oprim >= 0
-    assert mesh_hits.sum() > 2000
-    assert (reg == oreg).mean() > 0.9999
-    assert (prim == oprim).mean() > 0.9999
-    np.testing.assert_allclose(t[mesh_hits & (prim == oprim)], ot[mesh_hits & (prim == oprim)], rtol=0, atol=0)
+    oreg, oel, oprim, ot = oracle_lib.trace_closest(pk, r, rays)
+    assert (oprim >= 0).sum() > 2000
+    np.testing.assert_array_equal(reg, oreg)
+    np.testing.assert_array_equal(prim, oprim)
+    inst = oprim >= 0
+    np.testing.assert_array_equal(el[inst], oel[inst])
+    np.testing.assert_array_equal(t[oreg >= 0], ot[oreg >= 0])
+
+
+def test_instanced_ties_resolve_to_the_lower_instance(engine, oracle_lib):
+    """Two placements of one mesh at the same pose: every hit on them is a tie at equal t,
+    which both sides give to the first placement (the reference scans its instances in
+    order with a strict nearer-than test)."""
+    v, f = scenes.icosphere(3)
+    proto = {"kind": "mesh", "positions": v.astype(np.float32).reshape(-1), "indices": f.astype(np.uint32).reshape(-1),
+             "material": "m"}
+    place = [{"position": [0.5, 0.0, 0.0], "scale": 1.0}, {"position": [0.5, 0.0, 0.0], "scale": 1.0},
+             {"position": [-1.5, 0.0, 0.0], "scale": 1.0}]
+    sc = {"id": "ties", "objects": [{"kind": "instanced", "prototype": proto, "placements": place}],
+          "materials": {"m": {"model": "lambert"}}, "lights": []}
+    st = {"id": "s", "measurement": {"camera": {}, "maxBounces": 2},
+          "estimator": {"directLighting": "none", "russianRoulette": None, "meshTraversal": "cwbvh"}}
+    r, pk = Compiler().compile(sc, st)
+    engine.register_scene(pk)
+    rays = _rays(5000, 3, spread=1.5, dist=6.0)
+    for accel in (abi.ACCEL_BVH, abi.ACCEL_CWBVH):
+        reg, el, prim, t = _trace(engine, accel, rays)
+        oreg, oel, oprim, ot = oracle_lib.trace_closest(pk, r, rays)
+        hit = oprim >= 0
+        assert hit.sum() > 500 and not (oel[hit] == 1).any()
+        np.testing.assert_array_equal(reg, oreg)
+        np.testing.assert_array_equal(el[hit], oel[hit])
+        np.testing.assert_array_equal(prim, oprim)
 
 
 @pytest.mark.parametrize("accel", ["bvh", "cwbvh"])
