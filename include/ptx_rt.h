@@ -449,11 +449,19 @@ int ptr_update_params(ptr_scene* scene, const ptr_material* materials, int n_mat
  * lacks fold away, and with at most 16 regions the region loops unroll into one arm per
  * region with its intersection routine fixed, like the reference's generated arms (in
  * place of the region BVH, which returns the same hits).  Later ptr_render calls of the program with this scene use them (samples
- * are bit-identical to the generic kernels); the batch, adjoint replay and counting passes
- * keep the generic kernels.  Modules are cached per occupant census for the process.
+ * are bit-identical to the generic kernels); the adjoint replay and the counting passes keep
+ * the generic kernels (a batch takes ptr_specialize_batch).  Modules are cached per occupant census for the process.
  * seconds_out (may be NULL): compile time (0 for a cached module).  scene = NULL returns
  * the program to the generic kernels.  PTR_E_UNSUPPORTED when NVRTC cannot be loaded. */
 int ptr_specialize(ptr_program* prog, ptr_scene* scene, double* seconds_out);
+
+/* The batched kernels of ptr_render_batch compiled for a job mix (no counterpart in the
+ * reference, which draws one scene per frame): the union of the jobs' occupant censuses
+ * (material models, light kinds, environment kinds, region shapes; no region unrolling),
+ * compiled with NVRTC like ptr_specialize.  Later ptr_render_batch calls on the context
+ * whose jobs have the same union census use them; samples are identical to the generic
+ * batched kernels.  The jobs' frames are not read.  seconds_out as for ptr_specialize. */
+int ptr_specialize_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs, double* seconds_out);
 
 /* ---- launch tuning (no counterpart in the reference: WebGL draws one fragment per pixel) ----
  * capacity: paths in flight per wave (0 = the default 2^24); block: threads per block of the

@@ -29,12 +29,22 @@
 using namespace ptx;
 
 struct ptr_program;
+struct SpecKernels {
+    uint64_t scene_id = 0;
+    const void* closest = nullptr;
+    const void* shade = nullptr;
+    const void* shadow = nullptr;
+};
+
 struct ptr_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
     ptr_program* batch = nullptr;     // path pool + tables of batched renders
     ptr_tuning tune{1 << 24, 256, 1, 0};   // pool capacity, block size, sort buckets, ray sort
+    // batched kernels compiled for a job mix's occupant census (ptr_specialize_batch),
+    // by census key
+    std::map<std::string, SpecKernels> batch_spec;
 };
 
 struct ptr_scene {
@@ -56,13 +66,6 @@ struct ptr_scene {
 };
 
 // Kernels of one program compiled for one scene (ptr_specialize).
-struct SpecKernels {
-    uint64_t scene_id = 0;
-    const void* closest = nullptr;
-    const void* shade = nullptr;
-    const void* shadow = nullptr;
-};
-
 struct ptr_program {
     ptr_ctx* ctx = nullptr;
     ptr_program_desc desc{};
@@ -440,9 +443,10 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
 
 // One wave of a batched render: the same kernel sequence over the concatenated job space;
 // scene, program knobs and frame come from the per-job tables.
+// sk: the mix's compiled batched kernels (ptr_specialize_batch), or null for the generic ones.
 void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchTables& bt, int direct, bool media,
                        bool equiangular, cudaStream_t st, int iters, int n_sm, const ptr_tuning& tune,
-                       std::vector<ProfRec>* prof = nullptr, bool dry = false) {
+                       const SpecKernels* sk, std::vector<ProfRec>* prof = nullptr, bool dry = false) {
     const int block = tune.block;
     int n_launched = 0;
     const Launcher L{block, n_sm, st, dry, &n_launched};
@@ -472,7 +476,8 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
         PathPool pi = pool;
         pi.ray_in = pool.ray_sort && it > 0;
         r = mark(1);
-        L(k_closest<false, true>, 0, S0, pi, in, bt);
+        if (sk) L.raw(sk->closest, 0, S0, pi, in, bt);
+        else L(k_closest<false, true>, 0, S0, pi, in, bt);
         done(r);
         if (pool.sort_buckets > 1) {
             r = mark(5);
@@ -480,7 +485,8 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
             done(r);
         }
         r = mark(2);
-        switch (direct * 2 + (media ? 1 : 0)) {
+        if (sk) L.raw(sk->shade, 0, S0, pi, P0, in, bt, AdjParams{});
+        else switch (direct * 2 + (media ? 1 : 0)) {
             case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
             case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
             case 2: L(k_shade<f3, PTR_DIRECT_NEE, false, true>, 0, S0, pi, P0, in, bt, AdjParams{}); break;
@@ -497,7 +503,8 @@ void launch_batch_wave(const DevScene& S0, const PathPool& pool_in, const BatchT
         if (direct != PTR_DIRECT_NONE) {
             r = mark(3);
             for (int slot = equiangular ? 1 : 0; slot >= 0; --slot) {
-                if (media) L(k_shadow<f3, true, false, true>, 0, S0, pool, P0, bt, slot, AdjParams{});
+                if (sk) L.raw(sk->shadow, 0, S0, pool, P0, bt, slot, AdjParams{});
+                else if (media) L(k_shadow<f3, true, false, true>, 0, S0, pool, P0, bt, slot, AdjParams{});
                 else L(k_shadow<f3, false, false, true>, 0, S0, pool, P0, bt, slot, AdjParams{});
             }
             done(r);
@@ -1100,22 +1107,77 @@ std::string lib_dir() {
     return k == std::string::npos ? std::string(".") : f.substr(0, k);
 }
 struct SpecModule { cudaLibrary_t lib = nullptr; const void* closest = nullptr; const void* shade = nullptr; const void* shadow = nullptr; };
-// Compile (or fetch) the closest-hit, shading and shadow kernels of a program for a scene's
-// occupant census.  The key is the option list, so equal scenes share one module.
-int spec_compile(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* sc, SpecModule& out, bool& compiled) {
+// The occupant census a set of kernels is compiled for: material models, light kinds,
+// environment kinds and region shapes present (bit masks), the regions in order when
+// there are at most 16 (0 otherwise), the light tree, the direct-lighting mode, media,
+// colour model, and whether the kernels are the batched variants.
+struct Census {
+    unsigned mats = 0, lights = 0, envs = 0, shapes = 0;
+    int nregions = 0;
+    unsigned long long shape_code = 0;
+    bool tree = false, media = false, spectral = false, batch = false;
+    int direct = 0;
+};
+Census census_of(const ptr_program* p, const ptr_scene* sc) {
+    Census c;
+    c.mats = sc->spec_mats;
+    c.lights = sc->spec_lights;
+    c.envs = sc->spec_envs;
+    c.shapes = sc->spec_shapes;
+    c.nregions = sc->spec_nregions;
+    c.shape_code = sc->spec_shape_code;
+    c.tree = p->desc.light_tree != 0;
+    c.media = sc->has_media != 0;
+    c.spectral = p->desc.color == PTR_COLOR_SPECTRAL;
+    c.direct = p->desc.direct;
+    return c;
+}
+// The union census of a job mix (the batched kernels serve every job of it): masks OR-ed,
+// no region unrolling (the jobs' region lists differ).
+Census census_of_batch(const ptr_batch_job* jobs, int n) {
+    Census c;
+    c.batch = true;
+    for (int j = 0; j < n; ++j) {
+        const Census k = census_of(jobs[j].prog, jobs[j].scene);
+        c.mats |= k.mats;
+        c.lights |= k.lights;
+        c.envs |= k.envs;
+        c.shapes |= k.shapes;
+        c.tree = c.tree || k.tree;
+        c.media = c.media || k.media;
+        c.direct = k.direct;
+    }
+    return c;
+}
+std::vector<std::string> census_options(const Census& c) {
+    return {"-DPTR_SPEC_MATS=" + std::to_string(c.mats) + "u",
+            "-DPTR_SPEC_LIGHTS=" + std::to_string(c.lights) + "u",
+            "-DPTR_SPEC_ENVS=" + std::to_string(c.envs) + "u",
+            "-DPTR_SPEC_SHAPES=" + std::to_string(c.shapes) + "u",
+            "-DPTR_SPEC_NREGIONS=" + std::to_string(c.nregions),
+            "-DPTR_SPEC_SHAPE_CODE=" + std::to_string(c.shape_code) + "ull",
+            std::string("-DPTR_SPEC_TREE=") + (c.tree ? "1" : "0")};
+}
+std::string census_key(const Census& c) {
+    std::string k;
+    for (const auto& o : census_options(c)) k += o + "\n";
+    return k + std::to_string(c.direct) + (c.media ? "m" : "-") + (c.spectral ? "s" : "-") + (c.batch ? "b" : "-");
+}
+// Compile (or fetch) the closest-hit, shading and shadow kernels for a census.  Modules are
+// cached by census for the process, so equal scenes (and equal mixes) share one module.
+int spec_compile(ptr_ctx* ctx, const Census& c, SpecModule& out, bool& compiled) {
     compiled = false;
     static std::mutex mu;
     static std::map<std::string, SpecModule> cache;
     Nvrtc& nv = nvrtc();
     if (!nv.ok) return fail(ctx, PTR_E_UNSUPPORTED, "ptr_specialize: " + nv.why);
-    const bool spectral = p->desc.color == PTR_COLOR_SPECTRAL;
-    const bool media = sc->has_media != 0;
-    const char* col = spectral ? "ptx::s4" : "ptx::f3";
-    const char* md = media ? "true" : "false";
-    const std::string n_closest = "ptx::k_closest<false, false>";
-    const std::string n_shade = std::string("ptx::k_shade<") + col + ", " + std::to_string(p->desc.direct) + ", " + md +
-                                ", false, false>";
-    const std::string n_shadow = std::string("ptx::k_shadow<") + col + ", " + md + ", false, false, false>";
+    const char* col = c.spectral ? "ptx::s4" : "ptx::f3";
+    const char* md = c.media ? "true" : "false";
+    const char* bt = c.batch ? "true" : "false";
+    const std::string n_closest = std::string("ptx::k_closest<false, ") + bt + ">";
+    const std::string n_shade = std::string("ptx::k_shade<") + col + ", " + std::to_string(c.direct) + ", " + md +
+                                ", " + bt + ", false>";
+    const std::string n_shadow = std::string("ptx::k_shadow<") + col + ", " + md + ", false, " + bt + ", false>";
     const std::string dir = lib_dir();
     const char* dev_env = std::getenv("PTR_DEVICE_SRC");
     const char* inc_env = std::getenv("PTR_INCLUDE");
@@ -1123,17 +1185,11 @@ int spec_compile(ptr_ctx* ctx, const ptr_program* p, const ptr_scene* sc, SpecMo
         "-arch=sm_100a", "-std=c++17", "-fmad=false", "-lineinfo",
         "-default-device",   // the public header's host prototypes, declared only
         std::string("-I") + (dev_env ? dev_env : dir + "/csrc/device"),
-        std::string("-I") + (inc_env ? inc_env : dir + "/../include"),
-        "-DPTR_SPEC_MATS=" + std::to_string(sc->spec_mats) + "u",
-        "-DPTR_SPEC_LIGHTS=" + std::to_string(sc->spec_lights) + "u",
-        "-DPTR_SPEC_ENVS=" + std::to_string(sc->spec_envs) + "u",
-        "-DPTR_SPEC_SHAPES=" + std::to_string(sc->spec_shapes) + "u",
-        "-DPTR_SPEC_NREGIONS=" + std::to_string(sc->spec_nregions),
-        "-DPTR_SPEC_SHAPE_CODE=" + std::to_string(sc->spec_shape_code) + "ull",
-        std::string("-DPTR_SPEC_TREE=") + (p->desc.light_tree ? "1" : "0")};
+        std::string("-I") + (inc_env ? inc_env : dir + "/../include")};
+    for (const auto& o : census_options(c)) opts.push_back(o);
     std::string key;
     for (const auto& o : opts) key += o + "\n";
-    key += n_shade + "\n" + n_shadow;
+    key += n_closest + "\n" + n_shade + "\n" + n_shadow;
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(key);
     if (it != cache.end()) { out = it->second; return PTR_OK; }
@@ -1551,6 +1607,12 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
             if (jobs[k].prog == J.prog)
                 return fail(ctx, PTR_E_INVALID, "ptr_render_batch: jobs " + std::to_string(k) + " and " + std::to_string(j) + " share a program (one film per job)");
     }
+    // the mix's compiled kernels, when ptr_specialize_batch compiled its census
+    const SpecKernels* sk = nullptr;
+    if (!ctx->batch_spec.empty()) {
+        auto it = ctx->batch_spec.find(census_key(census_of_batch(jobs, n_jobs)));
+        if (it != ctx->batch_spec.end()) sk = &it->second;
+    }
     std::vector<DevScene> scenes(n_jobs);
     std::vector<ProgParams> progs(n_jobs);
     std::vector<BatchJob> bjobs(n_jobs);
@@ -1584,8 +1646,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         F.salt = J.frame.reset_salt;
         F.px_off = J.frame.pixel_offset[0];
         F.py_off = J.frame.pixel_offset[1];
-    F.img_w = J.frame.image_size[0] > 0 ? J.frame.image_size[0] : J.frame.width;
-    F.img_h = J.frame.image_size[1] > 0 ? J.frame.image_size[1] : J.frame.height;
+        F.img_w = J.frame.image_size[0] > 0 ? J.frame.image_size[0] : J.frame.width;
+        F.img_h = J.frame.image_size[1] > 0 ? J.frame.image_size[1] : J.frame.height;
         F.total = total_j;
         F.capacity = 0;
         F.cam = J.frame.camera;
@@ -1644,7 +1706,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         std::vector<ProfRec> prof;
         prof.reserve((size_t)waves * (iters * 5 + 2));
         for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, &prof);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk, &prof);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1659,10 +1721,10 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         }
     } else {
         // occupancy queries outside capture, then the captured wave
-        launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, nullptr, true);
+        launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk, nullptr, true);
         if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk);
             e = cudaStreamEndCapture(st, &g);
         }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
@@ -1888,11 +1950,36 @@ int ptr_specialize(ptr_program* p, ptr_scene* s, double* seconds_out) {
     const auto t0 = std::chrono::steady_clock::now();
     SpecModule m;
     bool compiled = false;
-    if (int rc = spec_compile(ctx, p, s, m, compiled)) return rc;
+    if (int rc = spec_compile(ctx, census_of(p, s), m, compiled)) return rc;
     p->spec.scene_id = s->id;
     p->spec.closest = m.closest;
     p->spec.shade = m.shade;
     p->spec.shadow = m.shadow;
+    if (seconds_out && compiled) *seconds_out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return PTR_OK;
+}
+
+int ptr_specialize_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs, double* seconds_out) {
+    if (!ctx || !jobs || n_jobs <= 0) return fail(ctx, PTR_E_INVALID, "ptr_specialize_batch: no jobs");
+    if (seconds_out) *seconds_out = 0.0;
+    for (int j = 0; j < n_jobs; ++j) {
+        const ptr_batch_job& J = jobs[j];
+        if (!J.prog || !J.scene || J.prog->ctx != ctx || J.scene->ctx != ctx)
+            return fail(ctx, PTR_E_INVALID, "ptr_specialize_batch: job " + std::to_string(j) + " has a null or foreign program/scene");
+        if (J.prog->desc.direct != jobs[0].prog->desc.direct || J.prog->desc.color != PTR_COLOR_RGB)
+            return fail(ctx, PTR_E_INVALID, "ptr_specialize_batch: the jobs must share directLighting and render RGB");
+    }
+    CK(ctx, cudaSetDevice(ctx->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    const Census c = census_of_batch(jobs, n_jobs);
+    SpecModule m;
+    bool compiled = false;
+    if (int rc = spec_compile(ctx, c, m, compiled)) return rc;
+    SpecKernels k;
+    k.closest = m.closest;
+    k.shade = m.shade;
+    k.shadow = m.shadow;
+    ctx->batch_spec[census_key(c)] = k;
     if (seconds_out && compiled) *seconds_out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return PTR_OK;
 }

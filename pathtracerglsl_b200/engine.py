@@ -427,11 +427,46 @@ class Batch:
         return {k: (ms[i], n[i]) for i, k in enumerate(CudaEngine.KERNEL_CLASSES)}
 
     def render_plain(self, frames, sync=True):
+        """The same frames one job per launch, each job's whole spp budget in one
+        ptr_render."""
         arr = self._jobs(frames)
         for j in range(len(arr)):
             self.engine._check(self.lib.ptr_render(self.programs[j], self.scenes[j], C.byref(arr[j].frame)))
         if sync:
             self.engine.sync()
+
+    def render_progressive(self, frames, sync=True):
+        """The reference's own plain schedule: one scene per frame and one sample per pixel
+        per frame (Engine.renderFrame, src/engine/Engine.ts:190-204), i.e. spp ptr_render
+        calls of 1 spp per job, each accumulating into the job's film."""
+        arr = self._jobs(frames)
+        for j in range(len(arr)):
+            fr = abi.Frame()
+            C.pointer(fr)[0] = arr[j].frame
+            spp = fr.spp
+            for k in range(spp):
+                fr.spp = 1
+                fr.first_sample = arr[j].frame.first_sample + k
+                fr.accumulate = 1 if (k > 0 or arr[j].frame.accumulate) else 0
+                self.engine._check(self.lib.ptr_render(self.programs[j], self.scenes[j], C.byref(fr)))
+        if sync:
+            self.engine.sync()
+
+    def specialize(self, plain=False):
+        """Compile the batched kernels for this mix's occupant census (ptr_specialize_batch);
+        with plain=True also each job's own per-scene kernels for render_plain /
+        render_progressive (ptr_specialize).  Returns the compile seconds."""
+        sizes = list(self.sizes)
+        arr = self._jobs([(1, 1, 1)] * len(self.programs))
+        self.sizes = sizes
+        secs = C.c_double()
+        self.engine._check(self.lib.ptr_specialize_batch(self.engine.ctx, arr, len(arr), C.byref(secs)))
+        total = secs.value
+        if plain:
+            for j in range(len(arr)):
+                self.engine._check(self.lib.ptr_specialize(self.programs[j], self.scenes[j], C.byref(secs)))
+                total += secs.value
+        return total
 
     def read_export(self, j, name="radiance"):
         w, h = self.sizes[j]

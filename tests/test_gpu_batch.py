@@ -132,3 +132,27 @@ def test_region_bvh_equals_the_linear_scan(engine, monkeypatch):
         engine.reset()
         out.append(engine.render_samples(40, 40, 4))
     np.testing.assert_array_equal(out[1], out[0])
+
+
+def test_specialised_batch_equals_generic_and_plain(engine):
+    """ptr_specialize_batch: the mix's union-census kernels render every job's film equal
+    to the generic batched kernels and to the plain path; the progressive plain (one
+    sample per launch, the reference's frame loop) folds the same samples."""
+    items, frames = _jobs(6, 8, 30, 40, 6)
+    b = engine.batch(items)
+    try:
+        b.render(frames)
+        generic = [b.read_export(j).copy() for j in range(len(b))]
+        secs = b.specialize()
+        assert secs >= 0.0
+        b.render(frames)
+        for j in range(len(b)):
+            np.testing.assert_allclose(b.read_export(j), generic[j], rtol=1e-9, atol=1e-12)
+        b.render_plain(frames)
+        for j in range(len(b)):
+            np.testing.assert_allclose(b.read_export(j), generic[j], rtol=1e-9, atol=1e-12)
+        b.render_progressive(frames)
+        for j in range(len(b)):
+            np.testing.assert_allclose(b.read_export(j), generic[j], rtol=1e-6, atol=1e-9)
+    finally:
+        b.close()

@@ -78,3 +78,35 @@ def test_specialised_kernels_compile(case):
             assert lib.nvrtcGetLoweredName(prog, n, C.byref(low)) == 0 and low.value
     finally:
         lib.nvrtcDestroyProgram(C.byref(prog))
+
+
+@pytest.mark.parametrize("media", ["false", "true"])
+def test_batched_kernels_compile(media):
+    """ptr_specialize_batch's union census of the uneven Cornell-style mix (Lambert,
+    dielectric and GGX; quad lights; quads and spheres; no region unrolling), BATCH = true."""
+    lib = _nvrtc()
+    names = [b"ptx::k_closest<false, true>", f"ptx::k_shade<ptx::f3, 2, {media}, true, false>".encode(),
+             f"ptx::k_shadow<ptx::f3, {media}, false, true, false>".encode()]
+    opts = [b"-arch=sm_100a", b"-std=c++17", b"-fmad=false", b"-default-device",
+            ("-I" + os.path.join(ROOT, "pathtracerglsl_b200", "csrc", "device")).encode(),
+            ("-I" + os.path.join(ROOT, "include")).encode(),
+            b"-DPTR_SPEC_MATS=7u", b"-DPTR_SPEC_LIGHTS=1u", b"-DPTR_SPEC_ENVS=1u",
+            f"-DPTR_SPEC_SHAPES={(1 << 1) | (1 << 2)}u".encode(), b"-DPTR_SPEC_NREGIONS=0",
+            b"-DPTR_SPEC_SHAPE_CODE=0ull", b"-DPTR_SPEC_TREE=0"]
+    prog = C.c_void_p()
+    assert lib.nvrtcCreateProgram(C.byref(prog), PRELUDE, b"ptr_specialize.cu", 0, None, None) == 0
+    try:
+        for n in names:
+            assert lib.nvrtcAddNameExpression(prog, n) == 0
+        arr = (C.c_char_p * len(opts))(*opts)
+        rc = lib.nvrtcCompileProgram(prog, len(opts), arr)
+        size = C.c_size_t()
+        lib.nvrtcGetProgramLogSize(prog, C.byref(size))
+        log = C.create_string_buffer(size.value)
+        lib.nvrtcGetProgramLog(prog, log)
+        assert rc == 0, log.value.decode(errors="replace")[:4000]
+        for n in names:
+            low = C.c_char_p()
+            assert lib.nvrtcGetLoweredName(prog, n, C.byref(low)) == 0 and low.value
+    finally:
+        lib.nvrtcDestroyProgram(C.byref(prog))
