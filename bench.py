@@ -193,10 +193,9 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from pathtracerglsl_b200.compiler import Compiler
-    if args.workload == "batch":
-        jobs, cfg = batch_workload()
-        sc, st, (w, h, spp) = jobs[0]
-    elif args.workload == "adjoint":
+    if args.workload in ("batch", "metric"):
+        return run_reference_batch(args)
+    if args.workload == "adjoint":
         from pathtracerglsl_b200 import scenes
         sc, st, (w, h, _spp_p, spp) = scenes.adjoint_scene(0)
         cfg = {"workload": "adjoint-c5 scene, forward walk only (the CPU restatement has no adjoint)",
@@ -236,11 +235,56 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_batch(args):
+    """The reference arm on the batched mix: the oracle (CPU restatement) on all host threads,
+    each step 1 spp over one 1/16-height band of every job of the 64-job mix."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from pathtracerglsl_b200.compiler import Compiler
+    jobs, cfg = batch_workload()
+    if args.workload == "metric":
+        cfg = dict(cfg, workload="metric: " + cfg["workload"])
+    oracle.build()
+    threads = os.cpu_count() or 1
+    sessions = []
+    for sc, st, (w, h, spp) in jobs:
+        r, pk = Compiler().compile(sc, st)
+        sessions.append((oracle.Session(pk, r), w, h, pk, r))   # set-up (the oracle's BVH) untimed
+
+    def step(k):   # one band of every job of the mix
+        n = 0
+        for sess, w, h, _pk, _r in sessions:
+            band = max(1, h // 16)
+            y0 = (k * band) % h
+            th = min(band, h - y0)
+            sess.render_tile(w, h, (0, y0, w, th), 1, first_sample=0, salt=1, threads=threads)
+            n += w * th
+        return n
+
+    for i in range(args.warmup):
+        step(i)
+    t0 = time.perf_counter()
+    done = 0
+    for i in range(args.steps):
+        done += step(args.warmup + i)
+    el = time.perf_counter() - t0
+    value = done / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
+                             "sample": "per step 1 spp over a 1/16-height band of every job of the 64-job mix, "
+                                       "OpenMP over pixels"},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 # DRAM bytes of the roofline kernel per closest-hit query (a shaded path, for k_shade), from
 # one ncu capture of one whole wave of the workload at 1 spp with the autotuner's pick
 # (dram__bytes_read.sum + dram__bytes_write.sum over the wave's launches / the wave's
-# queries; profiles/k_closest_mesh_full.md, profiles/k_shade_cornell_full.md).  Scaled to a
-# launch of the timed configuration by its queries per launch.
+# queries).  Scaled to a launch of the timed configuration by its queries per launch; the
+# line labels it "ncu capture, scaled" (it is not measured in the timed run).
 NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 392.93}
 # the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
 ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
@@ -272,34 +316,63 @@ def algorithmic_bytes(kernel, c, cw=True):
     return 0
 
 
-def image_error(eng, w, h, spp, salt, budget=5e9):
-    """RMSE of one step's image against an FP64-accumulated reference of the same frame
-    rendered by this build with independent random numbers: 65,536 spp when that is at most
-    `budget` samples, else 4,096 spp (at least 256x the step, so the reference's own noise is
-    under 0.4 % of the step's variance).  Matched RMSE: the measured RMSE equals the one the
-    per-pixel variance predicts (ratio ~1), and ~99.7 % of pixel channels lie within 3 sigma."""
+def error_tiles(w, h, tile=64, n=4):
+    """Crops of the image for the matched-RMSE reference: the whole frame when it is at most
+    n tiles in area, else n tile x tile crops spread over it (engine coordinates)."""
+    if w * h <= n * tile * tile:
+        return [(0, 0, w, h)]
+    fr = [(0.2, 0.3), (0.4, 0.65), (0.6, 0.35), (0.8, 0.7)]
+    out = []
+    for fx, fy in fr[:n]:
+        x = min(max(0, int(fx * w) - tile // 2), w - tile)
+        y = min(max(0, int(fy * h) - tile // 2), h - tile)
+        out.append((x, y, min(tile, w), min(tile, h)))
+    return out
+
+
+def image_error(eng, w, h, spp, salt, ref_spp=65536, chunk=4096):
+    """RMSE of one step's image against an FP64-accumulated 65,536-spp reference of the
+    same frame rendered by this build with independent random numbers (the whole frame for
+    small images, else four 64 x 64 crops rendered as tiles of the full image: each pixel
+    computes exactly what the full render computes there).  sigma^2 per pixel channel =
+    v / spp + v_ref / ref_spp.  'within_3sigma' takes v from the step's own samples (the
+    literal gate, heavy-tailed at 16 spp); 'within_3sigma_ref_var' takes v from the
+    reference's 65,536 samples (the per-sample variance, well estimated).  Matched RMSE:
+    the measured RMSE equals the predicted one (ratio ~1) and ~99.7 % of channels lie
+    within 3 sigma."""
     import numpy as np
-    ref_spp = 65536 if w * h * 65536 <= budget else 4096
-    chunk = 256
-    eng.pin_reset_salt(0x5EED0000 + salt)
-    eng.reset()
-    for _ in range(ref_spp // chunk):
-        eng.render_frame(w, h, chunk)
-    ref = eng.read_export("radiance").astype(np.float64)
-    ref_var = eng.read_export("variance").astype(np.float64)
     eng.pin_reset_salt(salt)
     eng.reset()
     eng.render_frame(w, h, spp)
     img = eng.read_export("radiance").astype(np.float64)
     var = eng.read_export("variance").astype(np.float64)
-    sig2 = var / spp + ref_var / ref_spp
-    d = img - ref
+    d_all, s_lit, s_ref = [], [], []
+    tiles = error_tiles(w, h)
+    for (x, y, tw, th) in tiles:
+        eng.pin_reset_salt(0x5EED0000 + salt)
+        done = 0
+        while done < ref_spp:
+            k = min(chunk, ref_spp - done)
+            eng.render_tile(x, y, tw, th, w, h, k, accumulate=done > 0)
+            done += k
+        ref = eng.read_export("radiance").astype(np.float64)
+        ref_var = eng.read_export("variance").astype(np.float64)
+        d_all.append((img[y:y + th, x:x + tw] - ref).ravel())
+        s_lit.append((var[y:y + th, x:x + tw] / spp + ref_var / ref_spp).ravel())
+        s_ref.append((ref_var / spp + ref_var / ref_spp).ravel())
+    eng.width, eng.height = w, h
+    eng.pin_reset_salt(salt)
+    eng.reset()
+    d, sl, sr = np.concatenate(d_all), np.concatenate(s_lit), np.concatenate(s_ref)
     rmse = float(np.sqrt(np.mean(d * d)))
-    expected = float(np.sqrt(np.mean(sig2)))
-    live = sig2 > 0
-    within = float(np.mean(np.abs(d[live]) <= 3.0 * np.sqrt(sig2[live]))) if live.any() else 1.0
+    expected = float(np.sqrt(np.mean(sr)))
+
+    def within(sig2):
+        live = sig2 > 0
+        return float(np.mean(np.abs(d[live]) <= 3.0 * np.sqrt(sig2[live]))) if live.any() else 1.0
     return {"value": rmse, "expected": expected, "ratio": rmse / expected if expected > 0 else None,
-            "within_3sigma": within, "reference_spp": ref_spp, "step_spp": spp,
+            "within_3sigma": within(sl), "within_3sigma_ref_var": within(sr), "reference_spp": ref_spp,
+            "step_spp": spp, "crops": [list(t) for t in tiles],
             "reference": "FP64-accumulated film of this build, independent random numbers"}
 
 
@@ -316,10 +389,26 @@ def run_ours(args):
     import torch
     rank, local, world, dist = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    line = measure_ours(args, args.workload, rank, local, world, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.close()
+
+
+# the autotuner's pick for the mesh workload on this pool's B200s (recorded from its search
+# over pool capacity x sort buckets x ray order), used where the mesh line rides along the
+# composite metric run
+MESH_PICK = "capacity=33554432,sort_buckets=8,ray_sort=1"
+
+
+def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True):
+    """One plain workload (one ptr_render per step): the JSON line (rank 0; None elsewhere)."""
+    import torch
     from pathtracerglsl_b200.compiler import Compiler
     from pathtracerglsl_b200.engine import CudaEngine
 
-    sc, st, w, h, spp, cfg = workload(args.workload)
+    sc, st, w, h, spp, cfg = workload(name)
     if args.spp:      # a smaller step of the same scene (profiler captures)
         spp = args.spp
         cfg = dict(cfg, spp_per_step=spp)
@@ -351,10 +440,11 @@ def run_ours(args):
     # occupant-sorted shading queue and the ray-coherence queue order for this workload
     # (at least two steps and 0.25 s per candidate, before the warm-up and the timed region)
     from pathtracerglsl_b200 import autotune
-    if args.tuning:   # a recorded pick (e.g. for a profiler run of the same configuration)
-        pick = dict(autotune.DEFAULTS, **parse_tuning(args.tuning))
+    tuning = tuning or args.tuning
+    if tuning:   # a recorded pick (e.g. for a profiler run of the same configuration)
+        pick = dict(autotune.DEFAULTS, **parse_tuning(tuning))
         eng.set_tuning(**pick)
-        cfg = dict(cfg, tuning=pick, tuning_search="given on the command line")
+        cfg = dict(cfg, tuning=pick, tuning_search="a recorded pick of the autotuner")
     else:
         cands = [dict(capacity=c, block=256, sort_buckets=k, ray_sort=r)
                  for c in (0, 1 << 25) for k in (1, 8, 16) for r in (0, 1)]
@@ -416,7 +506,7 @@ def run_ours(args):
     eng.reset()
     eng.profile_render(w, h, spp, _abi.PROFILE_WORK)
     cnt = eng.counters()
-    kernel = ROOFLINE_KERNEL.get(args.workload) or max(prof.items(), key=lambda kv: kv[1][0])[0]
+    kernel = ROOFLINE_KERNEL.get(name) or max(prof.items(), key=lambda kv: kv[1][0])[0]
     kms, klaunch = prof[kernel]
     peak, peak_kind = measured_peaks()
     launch_ms = kms / max(klaunch, 1)
@@ -425,8 +515,10 @@ def run_ours(args):
     total_prof_ms = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "kernel": "k_" + kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (NCU_TRAFFIC_PER_QUERY[(args.workload, kernel)] * cnt["closest_queries"] / max(klaunch, 1)
-                            if (args.workload, kernel) in NCU_TRAFFIC_PER_QUERY else None),
+                "traffic": (NCU_TRAFFIC_PER_QUERY[(name, kernel)] * cnt["closest_queries"] / max(klaunch, 1)
+                            if (name, kernel) in NCU_TRAFFIC_PER_QUERY else None),
+                "traffic_source": ("ncu capture of one wave at 1 spp, scaled by queries per launch"
+                                   if (name, kernel) in NCU_TRAFFIC_PER_QUERY else None),
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                 "share": {k: v[0] / total_prof_ms for k, v in prof.items()}}
     launches = sum(v[1] for v in prof.values()) + 1   # + the frame-parameter kernel
@@ -445,12 +537,10 @@ def run_ours(args):
                 "rays": {"closest_per_sample": cnt["closest_queries"] / cnt["paths"],
                          "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
                          "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}
-        if not args.no_cpu_baseline:
+        if cpu_leg and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
-        print(json.dumps(line), flush=True)
     eng.close()
-    if dist is not None:
-        dist.close()
+    return line if rank == 0 else None
 
 
 # ---------------------------------------------------------------------------------- batch
@@ -468,14 +558,30 @@ def batch_workload():
 
 
 def run_batch(args):
-    """Batched wavefront (one ptr_render_batch over the 64 jobs, CUDA graph per wave)
-    against the plain path (one ptr_render per job) on the same frames: identical
-    per-sample estimators, so the RMSE is matched by construction."""
     import torch
     rank, local, world, dist = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    line = measure_batch(args, rank, local, world, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.close()
+
+
+PROGRESSIVE_SPP = 8   # samples per job of the progressive plain (the reference's frame loop)
+
+
+def measure_batch(args, rank, local, world, dist, cpu_leg=True):
+    """Batched wavefront (one ptr_render_batch over the 64 jobs, CUDA graph per wave, the
+    mix's union-census kernels) against three plain forms on the same frames: one
+    ptr_render per job at its full spp with each job's own per-scene kernels (the
+    strongest plain), the same with the generic kernels, and the reference's own frame
+    loop (one scene per launch, one sample per pixel per launch: Engine.renderFrame).  All
+    forms draw identical per-sample estimators and random streams, so the RMSE is matched
+    by construction (the GPU tests check batched = plain per job)."""
+    import torch
     from pathtracerglsl_b200.compiler import Compiler
-    from pathtracerglsl_b200.engine import CudaEngine
+    from pathtracerglsl_b200.engine import CudaEngine, EngineError
 
     jobs, cfg = batch_workload()
     items = [Compiler().compile(sc, st) for sc, st, _ in jobs]
@@ -483,11 +589,24 @@ def run_batch(args):
     samples_step = cfg["samples_per_step"]
     eng = CudaEngine(local)
     b = eng.batch(items)
+    # batched kernels for the mix's union census and each job's per-scene kernels (NVRTC,
+    # untimed), before the tuning search
+    specialised = not args.generic
+    if specialised:
+        try:
+            secs = b.specialize(plain=True)
+            cfg = dict(cfg, kernels=f"batched: specialised for the mix's union occupant census; plain: each job's "
+                                    f"per-scene kernels (NVRTC, {secs:.1f} s of compiles, untimed)")
+        except EngineError as e:
+            specialised = False
+            cfg = dict(cfg, kernels=f"generic: specialisation unavailable ({e})")
+    if not specialised:
+        cfg = dict(cfg, kernels="generic (precompiled, table-driven)")
     # the project's autotuner picks pool capacity, block size and sort-bucket count on a
-    # reduced copy of the mix (every job at 1/16 of its spp), then both arms use the pick
+    # reduced copy of the mix (every job at 1/16 of its spp), then every arm uses the pick
     from pathtracerglsl_b200 import autotune
     small = [(w, h, max(1, spp // 16), 0, 7) for (w, h, spp, _f, _s) in frames]
-    tuned = autotune.tune(eng, lambda: b.render(small), budget_s=90.0)
+    tuned = autotune.tune(eng, lambda: b.render(small), budget_s=40.0)
     cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
                tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
@@ -497,13 +616,13 @@ def run_batch(args):
     b.render_plain(frames)
     torch.cuda.synchronize()
 
-    def timed(fn):
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    def timed(fn, steps):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         barrier(dist)
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
-            for k in range(args.steps):
+            for k in range(steps):
                 flush.fill_(float(k))
                 starts[k].record(stream)
                 fn()
@@ -516,12 +635,24 @@ def run_batch(args):
     clocks.start()
     time.sleep(0.5)
     t_window = time.time()
-    dev_ms = timed(lambda: b.render(frames))
+    dev_ms = timed(lambda: b.render(frames), args.steps)
     clocks.mark(t_window, time.time())
     clk = clocks.stop()
-    plain_ms = timed(lambda: b.render_plain(frames, sync=False))
     value = samples_step * args.steps * world / (dev_ms / 1000.0)
-    plain = samples_step * args.steps * world / (plain_ms / 1000.0)
+    # the plain forms, a few steps each (the same frames, after the headline's timed region)
+    k_plain = min(args.steps, 3)
+    plain_ms = timed(lambda: b.render_plain(frames, sync=False), k_plain)
+    plain = samples_step * k_plain * world / (plain_ms / 1000.0)
+    plain_generic = None
+    if specialised:
+        b.specialize_off()
+        gen_ms = timed(lambda: b.render_plain(frames, sync=False), k_plain)
+        plain_generic = samples_step * k_plain * world / (gen_ms / 1000.0)
+        b.specialize(plain=True)
+    prog_frames = [(w, h, min(spp, PROGRESSIVE_SPP), 0, salt) for (w, h, spp, _f, salt) in frames]
+    prog_samples = sum(w * h * spp for (w, h, spp, _f, _s) in prog_frames)
+    prog_ms = timed(lambda: b.render_progressive(prog_frames, sync=False), 1)
+    progressive = prog_samples * world / (prog_ms / 1000.0)
 
     # end to end: tables from host memory in, every job's radiance out to host memory
     barrier(dist)
@@ -550,32 +681,83 @@ def run_batch(args):
                 "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                 "share": {k: v[0] / total_prof_ms for k, v in prof.items()}}
     launches = sum(v[1] for v in prof.values())
+    line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": dict(cfg, l2="flushed between steps (256 MiB write, untimed)",
                                parallelism=f"replicas x{world}"),
-                "plain": {"value": plain, "unit": "samples/s", "ms_per_step": plain_ms / args.steps,
+                "plain": {"value": plain, "unit": "samples/s", "ms_per_step": plain_ms / k_plain, "steps": k_plain,
+                          "form": "one ptr_render per job at its full spp" +
+                                  (", each job's per-scene kernels" if specialised else ", generic kernels"),
                           "batched_over_plain": value / plain,
                           "rmse": "matched: identical per-sample estimators and random streams"},
+                "plain_generic": (None if plain_generic is None else
+                                  {"value": plain_generic, "unit": "samples/s", "steps": k_plain,
+                                   "form": "one ptr_render per job at its full spp, generic kernels",
+                                   "batched_over_plain": value / plain_generic}),
+                "plain_progressive": {"value": progressive, "unit": "samples/s", "ms": prog_ms,
+                                      "samples": prog_samples,
+                                      "form": f"the reference's frame loop: one scene and one sample per pixel per "
+                                              f"ptr_render (Engine.renderFrame), the first {PROGRESSIVE_SPP} samples "
+                                              f"of every job",
+                                      "batched_over_plain": value / progressive},
                 "e2e": e2e, "roofline": roofline, "gpu_launches": launches * args.steps, "clocks": clk,
                 "rays": {"closest_per_sample": cnt["closest_queries"] / cnt["paths"],
                          "shadow_per_sample": cnt["shadow_queries"] / cnt["paths"],
                          "mrays_per_s": value * (cnt["closest_queries"] + cnt["shadow_queries"]) / cnt["paths"] / 1e6}}
-        if not args.no_cpu_baseline:
-            sc, st, (w, h, spp) = jobs[0]
-            line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp)
-            line["cpu_baseline"]["sample"] = "job 0 of the batch: " + line["cpu_baseline"]["sample"]
-        print(json.dumps(line), flush=True)
+        if cpu_leg and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_batch(jobs)
     b.close()
     eng.close()
-    if dist is not None:
-        dist.close()
+    return line
+
+
+def cpu_baseline_batch(jobs, seconds=10.0):
+    """The oracle on all host threads over a bounded sample of the mix: 1 spp over one
+    1/16-height band of each job in turn until about `seconds` of host time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from pathtracerglsl_b200.compiler import Compiler
+    oracle.build()
+    threads = os.cpu_count() or 1
+    sessions = []
+    for sc, st, (w, h, spp) in jobs:
+        r, pk = Compiler().compile(sc, st)
+        sessions.append((oracle.Session(pk, r), w, h, pk, r))   # set-up (the oracle's BVH) untimed
+    done = 0
+    k = 0
+    t0 = time.perf_counter()
+    while True:
+        sess, w, h, _pk, _r = sessions[k % len(sessions)]
+        band = max(1, h // 16)
+        y0 = ((k // len(sessions)) * band) % h
+        th = min(band, h - y0)
+        sess.render_tile(w, h, (0, y0, w, th), 1, first_sample=0, salt=1, threads=threads)
+        done += w * th
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": done / el, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{done} samples: 1 spp over {k} bands (1/16 of a job's height each, the jobs in turn) "
+                      f"of the 64-job mix ({el:.1f} s of host time)"}
 
 
 # ---------------------------------------------------------------------------------- adjoint
 def run_adjoint(args):
+    import torch
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    line = measure_adjoint(args, rank, local, world, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.close()
+
+
+def measure_adjoint(args, rank, local, world, dist, cpu_leg=True):
     """The inverse-rendering workload: loss = L2 between the image at the current
     parameters (64 spp primal) and a target rendered at seeded +-10 % perturbed parameters;
     one step = one path-replay adjoint pass at 16 spp (forward walk + replay, gradients of
@@ -583,8 +765,6 @@ def run_adjoint(args):
     same 16 spp (the adjoint's cost ratio) and the 64-spp primal."""
     import torch
     import numpy as np
-    rank, local, world, dist = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
     from pathtracerglsl_b200 import adjoint, scenes
     from pathtracerglsl_b200.compiler import Compiler
     from pathtracerglsl_b200.engine import CudaEngine
@@ -692,11 +872,38 @@ def run_adjoint(args):
                              "traffic": None, "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                              "share": {k: v[0] / total_prof_ms for k, v in prof.items()}},
                 "gpu_launches": args.steps * 2 * sum(v[1] for v in prof.values())}
-        if not args.no_cpu_baseline:
+        if cpu_leg and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(sc, st, w, h, spp_a)
             line["cpu_baseline"]["sample"] = "forward only (the oracle has no adjoint): " + line["cpu_baseline"]["sample"]
-        print(json.dumps(line), flush=True)
     eng.close()
+    return line if rank == 0 else None
+
+
+# ---------------------------------------------------------------------------------- the metric
+def run_metric(args):
+    """The metric's own comparisons in one line: the headline is the batched wavefront on the
+    64-job uneven mix (against its plain forms); beside it the path-replay adjoint against the
+    forward pass on the adjoint scene, and the plain mesh workload (1080p, 1.31 M-triangle
+    instanced CWBVH) with its matched RMSE against a 65,536-spp reference."""
+    import torch
+    rank, local, world, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    line = measure_batch(args, rank, local, world, dist)
+    adj = measure_adjoint(args, rank, local, world, dist, cpu_leg=False)
+    mesh = measure_ours(args, "mesh", rank, local, world, dist, tuning=MESH_PICK, cpu_leg=False)
+    if rank == 0:
+        line["adjoint"] = {"value": adj["value"], "unit": "samples/s", "ms_per_step": adj["ms_per_step"],
+                           "steps": adj["steps"], "config": adj["config"],
+                           "forward": adj["forward"], "adjoint_over_forward_cost": adj["forward"]["adjoint_over_forward_cost"],
+                           "loss": adj["loss"], "gradient_l2": adj["gradient_l2"], "e2e": adj["e2e"],
+                           "roofline": adj["roofline"], "clocks": adj["clocks"]}
+        line["mesh"] = {k: mesh[k] for k in ("value", "unit", "ms_per_step", "steps", "config", "e2e", "roofline",
+                                             "clocks", "rmse", "rays", "traversal")}
+        line["gpu_launches"] = line["gpu_launches"] + adj["gpu_launches"] + mesh["gpu_launches"]
+        line["config"] = dict(line["config"], workload="metric: " + line["config"]["workload"],
+                              also="adjoint-c5 (adjoint vs forward) and mesh-c2 (plain, matched RMSE) in the "
+                                   "'adjoint' and 'mesh' keys")
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.close()
 
@@ -707,7 +914,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mesh")
+    ap.add_argument("--workload", default="metric",
+                    help="metric (default: batch mix + adjoint + mesh), batch, adjoint, mesh, mesh-bvh, cornell, media")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", default="", help="skip the autotuner: e.g. sort_buckets=16,ray_sort=1")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0: the workload's own)")
@@ -718,6 +926,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "metric":
+        run_metric(args)
     elif args.workload == "batch":
         run_batch(args)
     elif args.workload == "adjoint":

@@ -215,12 +215,7 @@ class CudaEngine:
         stamps = {}
         try:
             for t in plan["tiles"]:
-                self.width, self.height = t["width"], t["height"]
-                self.reset()
-                fr = self._frame(t["width"], t["height"], spp, accumulate=False, image=(width, height))
-                fr.pixel_offset = (C.c_int32 * 2)(t["x"], t["y"])
-                self._check(self.lib.ptr_render(self.programs[self.current], self.scene, C.byref(fr)))
-                self.sample_count = spp
+                self.render_tile(t["x"], t["y"], t["width"], t["height"], width, height, spp)
                 for p in pictures:
                     images[p][t["y"]:t["y"] + t["height"], t["x"]:t["x"] + t["width"]] = self.read_export(p)
             for p in pictures:
@@ -231,6 +226,21 @@ class CudaEngine:
             else:
                 self.pin_reset_salt(pinned)
         return images, stamps
+
+    def render_tile(self, x, y, tile_width, tile_height, width, height, spp, accumulate=False):
+        """Render ``spp`` samples per pixel of the tile at (x, y) (y from the bottom) of a
+        width x height image into the current renderer's film (engine.pixelOffset +
+        engine.imageSize): from a fresh accumulation, or with ``accumulate`` onto the
+        samples already folded for the same tile.  The film then holds the tile's pixels."""
+        if self.scene is None or self.current is None:
+            raise EngineError(abi.PTR_E_INVALID, "no scene registered or no renderer loaded")
+        if not accumulate or (self.width, self.height) != (tile_width, tile_height):
+            self.width, self.height = tile_width, tile_height
+            self.reset()
+        fr = self._frame(tile_width, tile_height, spp, accumulate=self.sample_count > 0, image=(width, height))
+        fr.pixel_offset = (C.c_int32 * 2)(x, y)
+        self._check(self.lib.ptr_render(self.programs[self.current], self.scene, C.byref(fr)))
+        self.sample_count += spp
 
     def render_stamp(self, picture="radiance", scene_id=None, resolution=None, spp=None):
         """The reproducibility stamp of a saved picture (App.buildRenderStamp,
@@ -451,6 +461,13 @@ class Batch:
                 self.engine._check(self.lib.ptr_render(self.programs[j], self.scenes[j], C.byref(fr)))
         if sync:
             self.engine.sync()
+
+    def specialize_off(self):
+        """Return every job's plain renders to the generic kernels (the batched kernels of
+        the mix stay compiled)."""
+        secs = C.c_double()
+        for p in self.programs:
+            self.engine._check(self.lib.ptr_specialize(p, None, C.byref(secs)))
 
     def specialize(self, plain=False):
         """Compile the batched kernels for this mix's occupant census (ptr_specialize_batch);
