@@ -416,7 +416,10 @@ int ptr_render_noalloc(const ptr_scene_desc* scene, const ptr_program_desc* prog
  * Media must be grey (sigma_a, sigma_s equal in r, g, b); the medium's parameters are
  * sigma_t = sigma_a + sigma_s and the single-scattering albedo sigma_s / sigma_t. */
 #define PTR_GRAD_SLOTS 8
-#define PTR_GRAD_ALBEDO_R 0        /* Lambert albedo r, g, b: slots 0, 1, 2         */
+#define PTR_GRAD_COLOR_R 0         /* the model's colour r, g, b: slots 0, 1, 2 -
+                                      Lambert albedo, GGX / mirror F0, dielectric
+                                      transmittance                                   */
+#define PTR_GRAD_ALBEDO_R PTR_GRAD_COLOR_R
 #define PTR_GRAD_ALPHA 3           /* GGX alpha (materials without per-triangle alpha) */
 #define PTR_GRAD_IOR 4             /* dielectric IOR (interface terms)               */
 #define PTR_GRAD_SIGMA_T 5         /* grey homogeneous medium sigma_t               */

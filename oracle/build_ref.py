@@ -49,7 +49,13 @@ def _compile(case, src_path):
     return case, r.returncode == 0, r.stderr[-2000:]
 
 
-def build(ref_root="/root/reference", all_cases=False, jobs=None):
+# Where the reference checkout is read from (this build recipe's one default; the
+# PTR_REFERENCE_DIR environment variable or the first argument overrides it).
+REFERENCE_DIR = os.environ.get("PTR_REFERENCE_DIR", "/root/reference")
+
+
+def build(ref_root=None, all_cases=False, jobs=None):
+    ref_root = ref_root or REFERENCE_DIR
     snap = os.path.join(ref_root, extract_snapshots.SNAP_REL)
     if not os.path.exists(snap):
         return None
@@ -82,7 +88,7 @@ def build(ref_root="/root/reference", all_cases=False, jobs=None):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    idx = build(args[0] if args else "/root/reference", all_cases="--all" in sys.argv)
+    idx = build(args[0] if args else None, all_cases="--all" in sys.argv)
     if idx is None:
         print("reference snapshot not found; oracle/_ref not built")
     else:

@@ -1896,20 +1896,45 @@ struct TracerT {
         radiance = radiance + thr * T_seg * sigma_s * ph * Le * vis / denom;
     }
 
+    // d w_c / d F0_c of a weight w_c = F_c(F0_c) x (terms free of F0), Schlick's F at cosine c:
+    // w_c (1 - (1 - c)^5) / F_c, one entry per channel, appended at n.
+    int dw_schlick_f0(int mat, const ptr_material& m, double c, Col w, DW* dw, int n) const {
+        const double s5 = std::pow(1.0 - c, 5.0);
+        for (int ch = 0; ch < 3; ++ch) {
+            const double F = (double)m.f0[ch] + (1.0 - (double)m.f0[ch]) * s5;
+            dw[n].k = slot_k(mat, PTR_GRAD_COLOR_R + ch);
+            dw[n].d[0] = dw[n].d[1] = dw[n].d[2] = 0.0;
+            dw[n].d[ch] = F > 0.0 ? (double)w[ch] * (1.0 - s5) / F : 0.0;
+            ++n;
+        }
+        return n;
+    }
+    // the cosine Schlick's F of the GGX conductor sees for the pair (wi, wo)
+    static double ggx_fresnel_cos(v3 wi, v3 wo, const Hit& h) {
+        v3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+        v3 hh = normalize(wil + wol);
+        return (double)std::fabs(dot(wol, hh));
+    }
+
     // The continuation lobe's weight derivative (forward mode).  Lambert: w = albedo.
-    // GGX: w = f cos / pdf with the pdf detached, so dw = w d log fs(alpha).  Dielectric:
+    // GGX: w = F(F0) fs(alpha) cos / pdf with the pdf detached, so dw = w d log F(F0)
+    // per channel and w d log fs(alpha).  Mirror: w = F(F0).  Dielectric:
     // w = F / F_detached (reflection) or T (n_i / n_t)^2 (1 - F) / (1 - F)_detached
-    // (refraction), differentiated along the IORs of the two regions the interface joins.
+    // (refraction), differentiated along the IORs of the two regions the interface joins,
+    // and along the transmittance T on refraction.
     void tan_continuation(const ptr_material& m, int mat, v3 wo, const Hit& hit, const IS& bs, Col thr, DW* dw) {
         int n = 0;
         if (m.model == PTR_MAT_LAMBERT) {
             for (int c = 0; c < 3; ++c) {
-                dw[n].k = slot_k(mat, PTR_GRAD_ALBEDO_R + c);
+                dw[n].k = slot_k(mat, PTR_GRAD_COLOR_R + c);
                 dw[n].d[0] = dw[n].d[1] = dw[n].d[2] = 0.0;
                 dw[n].d[c] = 1.0;
                 ++n;
             }
+        } else if (m.model == PTR_MAT_MIRROR) {
+            n = dw_schlick_f0(mat, m, (double)clampf(dot(wo, hit.frame.n), 1e-6f, 1.0f), bs.weight, dw, n);
         } else if (m.model == PTR_MAT_GGX) {
+            n = dw_schlick_f0(mat, m, ggx_fresnel_cos(bs.wi, wo, hit), bs.weight, dw, n);
             if (hit_alpha < 0.0f) {
                 const Dual fs = ggx_fs_dual(bs.wi, wo, hit.frame, Dual{(double)m.alpha, 1.0});
                 dw[n].k = slot_k(mat, PTR_GRAD_ALPHA);
@@ -1935,6 +1960,15 @@ struct TracerT {
                     for (int c = 0; c < 3; ++c) dw[n].d[c] = (double)m.transmittance[c] * dd;
                 }
                 ++n;
+            }
+            if (bs.flags & LOBE_TRANSMISSION) {   // d w_c / d T_c = (n_i / n_t)^2
+                const double scale = (double)((n_i * n_i) / (n_t * n_t));
+                for (int c = 0; c < 3; ++c) {
+                    dw[n].k = slot_k(mat, PTR_GRAD_COLOR_R + c);
+                    dw[n].d[0] = dw[n].d[1] = dw[n].d[2] = 0.0;
+                    dw[n].d[c] = scale;
+                    ++n;
+                }
             }
         }
         tan_mul(thr, bs.weight, dw, n);
@@ -2164,11 +2198,14 @@ struct TracerT {
                                                      (double)w / (double)ls.pdf;
                                     ++n;
                                 }
-                            } else if (m.model == PTR_MAT_GGX && hit_alpha < 0.0f) {   // f = F fs(alpha)
-                                const Dual fs = ggx_fs_dual(ls.wi, wo, hit.frame, Dual{(double)m.alpha, 1.0});
-                                dw[n].k = slot_k(mat, PTR_GRAD_ALPHA);
-                                for (int c = 0; c < 3; ++c) dw[n].d[c] = fs.v > 0.0 ? (double)X[c] * fs.d / fs.v : 0.0;
-                                ++n;
+                            } else if (m.model == PTR_MAT_GGX) {   // f = F(F0) fs(alpha)
+                                n = dw_schlick_f0(mat, m, ggx_fresnel_cos(ls.wi, wo, hit), X, dw.data(), n);
+                                if (hit_alpha < 0.0f) {
+                                    const Dual fs = ggx_fs_dual(ls.wi, wo, hit.frame, Dual{(double)m.alpha, 1.0});
+                                    dw[n].k = slot_k(mat, PTR_GRAD_ALPHA);
+                                    for (int c = 0; c < 3; ++c) dw[n].d[c] = fs.v > 0.0 ? (double)X[c] * fs.d / fs.v : 0.0;
+                                    ++n;
+                                }
                             }
                             n = dw_from_dlog(X, dlog_vis, dw, n);
                             tan_add(throughput, X, dw.data(), n);

@@ -27,8 +27,10 @@ ACCEL_BVH, ACCEL_CWBVH = range(2)
 EQUIANGULAR_OFF, EQUIANGULAR_DELTA, EQUIANGULAR_AREA = range(3)
 # adjoint parameter slots per material (include/ptx_rt.h PTR_GRAD_*)
 GRAD_SLOTS = 8
-GRAD_ALBEDO_R, GRAD_ALBEDO_G, GRAD_ALBEDO_B, GRAD_ALPHA, GRAD_IOR, GRAD_SIGMA_T, GRAD_MEDIUM_ALBEDO, GRAD_HG_G = range(8)
-GRAD_NAMES = ("albedo.r", "albedo.g", "albedo.b", "alpha", "ior", "sigma_t", "medium_albedo", "g")
+# slots 0-2: the model's colour (Lambert albedo, GGX / mirror F0, dielectric transmittance)
+GRAD_COLOR_R, GRAD_COLOR_G, GRAD_COLOR_B, GRAD_ALPHA, GRAD_IOR, GRAD_SIGMA_T, GRAD_MEDIUM_ALBEDO, GRAD_HG_G = range(8)
+GRAD_ALBEDO_R, GRAD_ALBEDO_G, GRAD_ALBEDO_B = GRAD_COLOR_R, GRAD_COLOR_G, GRAD_COLOR_B
+GRAD_NAMES = ("color.r", "color.g", "color.b", "alpha", "ior", "sigma_t", "medium_albedo", "g")
 
 F4 = C.c_float * 4
 

@@ -3,7 +3,7 @@
 No counterpart in the reference, which renders only.  Per material there are
 ``abi.GRAD_SLOTS`` parameters, laid out as the C ABI's PTR_GRAD_* slots:
 
-* Lambert albedo r, g, b;
+* the model's colour r, g, b: Lambert albedo, GGX / mirror F0, dielectric transmittance;
 * GGX alpha;
 * dielectric IOR, the IOR of every region the material is attached to;
 * for a grey homogeneous medium: sigma_t = sigma_a + sigma_s, the single-scattering albedo
@@ -29,6 +29,15 @@ def _regions(packed):
     return (abi.Region * len(packed.regions)).from_buffer(packed.regions)
 
 
+def _color(m):
+    """The colour parameter of a material's model (slots 0-2)."""
+    if m.model in (abi.MAT_GGX, abi.MAT_MIRROR):
+        return m.f0
+    if m.model == abi.MAT_DIELECTRIC:
+        return m.transmittance
+    return m.albedo
+
+
 def live_mask(packed):
     """(n_materials, GRAD_SLOTS) bool: the slots each material's model uses."""
     mats = _materials(packed)
@@ -37,10 +46,14 @@ def live_mask(packed):
     mask = np.zeros((len(mats), abi.GRAD_SLOTS), bool)
     for i, m in enumerate(mats):
         if m.model == abi.MAT_LAMBERT and not (m.flags & abi.MATF_EMISSIVE):
-            mask[i, abi.GRAD_ALBEDO_R:abi.GRAD_ALBEDO_B + 1] = True
+            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
         elif m.model == abi.MAT_GGX:
+            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
             mask[i, abi.GRAD_ALPHA] = True
+        elif m.model == abi.MAT_MIRROR:
+            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
         elif m.model == abi.MAT_DIELECTRIC and i in used:
+            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
             mask[i, abi.GRAD_IOR] = True
         if m.flags & abi.MATF_MEDIUM:
             mask[i, abi.GRAD_SIGMA_T] = True
@@ -59,7 +72,7 @@ def param_table(packed):
         ior.setdefault(r.material, r.ior)
     out = np.zeros((len(mats), abi.GRAD_SLOTS), np.float64)
     for i, m in enumerate(mats):
-        out[i, 0:3] = list(m.albedo)[:3]
+        out[i, 0:3] = list(_color(m))[:3]
         out[i, abi.GRAD_ALPHA] = m.alpha
         out[i, abi.GRAD_IOR] = ior.get(i, 1.0)
         st = m.sigma_a[0] + m.sigma_s[0]
@@ -80,7 +93,13 @@ def with_params(packed, table):
     for i, m in enumerate(mats):
         row = table[i]
         if mask[i, 0]:
-            m.albedo = abi.F4(*(list(row[0:3]) + [0.0]))
+            col = abi.F4(*(list(row[0:3]) + [0.0]))
+            if m.model in (abi.MAT_GGX, abi.MAT_MIRROR):
+                m.f0 = col
+            elif m.model == abi.MAT_DIELECTRIC:
+                m.transmittance = col
+            else:
+                m.albedo = col
         if mask[i, abi.GRAD_ALPHA]:
             m.alpha = float(row[abi.GRAD_ALPHA])
         if mask[i, abi.GRAD_SIGMA_T]:

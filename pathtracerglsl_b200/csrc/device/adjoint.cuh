@@ -9,8 +9,9 @@
 // detached too (they sum to one / keep the estimator unbiased for every theta, so their
 // derivatives vanish in expectation).
 //
-// Per material, PTR_GRAD_SLOTS parameters (include/ptx_rt.h): Lambert albedo (rgb), GGX
-// alpha, dielectric IOR, grey homogeneous medium sigma_t, single-scattering albedo and HG g.
+// Per material, PTR_GRAD_SLOTS parameters (include/ptx_rt.h): the model's colour (rgb:
+// Lambert albedo, GGX / mirror F0, dielectric transmittance), GGX alpha, dielectric IOR, grey
+// homogeneous medium sigma_t, single-scattering albedo and HG g.
 // For the IOR only the interface terms (Fresnel lobe choice, the eta^2 radiance factor) are
 // differentiated: the refracted direction's own dependence on the IOR would need an
 // attached derivative of every later vertex.
@@ -36,6 +37,19 @@ __device__ __forceinline__ float ggx_dlog_alpha(f3 wi, f3 wo, const Hit& h, floa
     if (wil.z * wol.z <= 0.0f) return 0.0f;
     f3 hh = normalize(wil + wol);
     return mf_dlogD(hh.z, a) + mf_dlogG1(wil.z, a) + mf_dlogG1(wol.z, a);
+}
+// d log F_c / d F0_c of Schlick's Fresnel F = F0 + (1 - F0) (1 - c)^5, per channel.
+__device__ __forceinline__ f3 schlick_dlog_f0(f3 f0, float c) {
+    const float s5 = powf(1.0f - c, 5.0f);
+    const f3 F = f0 + (f3(1.0f) - f0) * s5;
+    return f3(1.0f - s5) / vmax(F, f3(1e-20f));
+}
+// d log f_c / d F0_c of the GGX conductor for the pair (wi, wo): only Fresnel depends on F0.
+__device__ __forceinline__ f3 ggx_dlog_f0(f3 wi, f3 wo, const Hit& h, f3 f0) {
+    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
+    if (wil.z * wol.z <= 0.0f) return f3(0.0f);
+    f3 hh = normalize(wil + wol);
+    return schlick_dlog_f0(f0, fabsf(dot(wol, hh)));
 }
 // d log p_HG / d g (forward convention, hg.glsl:11-42).
 __device__ __forceinline__ float hg_dlog_g(f3 wi, f3 wo, float g) {
@@ -109,6 +123,7 @@ __device__ __forceinline__ void grad_block_flush(const double* s, int n, double*
 }
 
 // Shadow-record kinds of the per-vertex lobe derivative D = dlog f(wi_light) - dlog w_cont.
-constexpr int kGradKindNone = 0, kGradKindAlbedo = 1, kGradKindAlpha = 2, kGradKindPhase = 3;
+// GGX: the per-channel F0 part in xyz, the alpha part in w.
+constexpr int kGradKindNone = 0, kGradKindAlbedo = 1, kGradKindGGX = 2, kGradKindPhase = 3;
 
 }  // namespace ptx

@@ -876,6 +876,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             GradAcc ga;
             int sh_kind = kGradKindNone, sh_mat = 0;
             f3 sh_dnee(0.0f);   // dlog f at the light direction of this vertex's NEE query
+            float sh_dw = 0.0f; // its scalar part (GGX alpha beside the per-channel F0 part)
             if constexpr (ADJ) {
                 lrem = xyz(pool.l_rem[i]);
                 ga.s = s_grad;
@@ -1121,9 +1122,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         if (m.model == PTR_MAT_LAMBERT) {
                                             sh_kind = kGradKindAlbedo;
                                             sh_dnee = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
-                                        } else if (m.model == PTR_MAT_GGX && hit.alpha < 0.0f) {
-                                            sh_kind = kGradKindAlpha;
-                                            sh_dnee = f3(ggx_dlog_alpha(ls.wi, wo, hit, alpha), 0.0f, 0.0f);
+                                        } else if (m.model == PTR_MAT_GGX) {   // F0 (per channel) and alpha
+                                            sh_kind = kGradKindGGX;
+                                            sh_dnee = ggx_dlog_f0(ls.wi, wo, hit, ld3(m.f0));
+                                            sh_dw = hit.alpha < 0.0f ? ggx_dlog_alpha(ls.wi, wo, hit, alpha) : 0.0f;
                                         }
                                     }
                                 }
@@ -1150,12 +1152,20 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         ga.vec(mat, PTR_GRAD_ALBEDO_R, lrem, dlog);
                                         if (shadow) sh_dnee = sh_dnee - dlog;
                                     } else if (m.model == PTR_MAT_GGX) {
+                                        f3 dF = ggx_dlog_f0(bs.wi, wo, hit, ld3(m.f0));
+                                        ga.vec(mat, PTR_GRAD_COLOR_R, lrem, dF);
+                                        if (shadow) sh_dnee = sh_dnee - dF;
                                         if (hit.alpha < 0.0f) {
                                             float da = ggx_dlog_alpha(bs.wi, wo, hit, alpha);
                                             ga.scl(mat, PTR_GRAD_ALPHA, lrem, da);
-                                            if (shadow) sh_dnee.x -= da;
+                                            if (shadow) sh_dw -= da;
                                         }
+                                    } else if (m.model == PTR_MAT_MIRROR) {   // w = Schlick F(F0, cos_i)
+                                        float ci = clampf(dot(wo, hit.frame.n), 1e-6f, 1.0f);
+                                        ga.vec(mat, PTR_GRAD_COLOR_R, lrem, schlick_dlog_f0(ld3(m.f0), ci));
                                     } else if (m.model == PTR_MAT_DIELECTRIC) {
+                                        if (bs.flags & kLobeTransmission)   // w = T (n_i / n_t)^2: d log w / d T = 1 / T
+                                            ga.vec(mat, PTR_GRAD_COLOR_R, lrem, f3(1.0f) / vmax(ld3(m.transmittance), f3(1e-20f)));
                                         const bool entering = hit.region_to == hit.region_owner;
                                         if (entering || hit.region_from == hit.region_owner) {
                                             float ci = dot(wo, hit.frame.n);
@@ -1206,7 +1216,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if constexpr (ADJ) {
                 pool.l_rem[i] = f4(lrem, 0.0f);
                 if (shadow) {
-                    pool.sh_g[i] = f4(sh_dnee, 0.0f);
+                    pool.sh_g[i] = f4(sh_dnee, sh_dw);
                     pool.sh_gm[i] = sh_mat | (sh_kind << 16);
                 }
             }
@@ -1424,9 +1434,13 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 pool.l_rem[i] = make_float4(lr.x - add.x, lr.y - add.y, lr.z - add.z, 0.f);
                 const int gm = pool.sh_gm[i];
                 const int kind = gm >> 16, vmat = gm & 0xFFFF;
-                const f3 D = xyz(pool.sh_g[i]);
-                if (kind == kGradKindAlbedo) ga.vec(vmat, PTR_GRAD_ALBEDO_R, add, D);
-                else if (kind == kGradKindAlpha) ga.scl(vmat, PTR_GRAD_ALPHA, add, D.x);
+                const float4 Dg = pool.sh_g[i];
+                const f3 D = xyz(Dg);
+                if (kind == kGradKindAlbedo) ga.vec(vmat, PTR_GRAD_COLOR_R, add, D);
+                else if (kind == kGradKindGGX) {
+                    ga.vec(vmat, PTR_GRAD_COLOR_R, add, D);
+                    ga.scl(vmat, PTR_GRAD_ALPHA, add, Dg.w);
+                }
                 else if (kind == kGradKindPhase) ga.scl(vmat, PTR_GRAD_HG_G, add, D.x);
                 for (int e = 0; e < n_mm; ++e) {   // T = exp(-st len) (scattering) or exp(-(1-a) st len)
                     GreyMedium g = grey_medium(S.materials[mm_id[e]]);

@@ -30,7 +30,11 @@ COLOURS = [
 ]
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    """ref_root: the reference checkout (default: the PTR_REFERENCE_DIR environment variable)."""
+    ref_root = ref_root or os.environ.get("PTR_REFERENCE_DIR")
+    if not ref_root:
+        raise SystemExit("usage: make_spectral_subset.py <reference checkout> (or set PTR_REFERENCE_DIR)")
     data_dir = os.path.join(ref_root, "src/components/color/spectral/data")
     model = SpectralModel.from_assets(data_dir)
     idx = set()

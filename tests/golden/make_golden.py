@@ -39,7 +39,7 @@ def camera_params(case):
 
 
 def main():
-    build_ref.build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    build_ref.build(sys.argv[1] if len(sys.argv) > 1 else None)   # default: build_ref.REFERENCE_DIR
     out = {}
     for case in ref_scenes.CASES:
         cam = camera_params(case)

@@ -39,6 +39,42 @@ def test_forward_mode_rides_the_plain_walk(oracle_lib):
     assert not np.any(f["jac"][..., dead])
 
 
+def _check_linear_parameters(r, pk, W, H, spp, salt):
+    """The forward mode against central differences of the oracle for the parameters that
+    move no sampling decision (no roulette): the colour slots and the medium's albedo.
+    Returns the number of parameters checked."""
+    import oracle
+    f = oracle.forward(pk, r, W, H, spp, salt=salt)
+    theta = adjoint.param_table(pk)
+    dl = np.random.RandomState(1).uniform(-1, 1, (H, W, 3))
+    g = np.einsum("hwc,hwck->k", dl, f["jac"]).reshape(-1, abi.GRAD_SLOTS)
+    mask = adjoint.live_mask(pk)
+    checked = 0
+    for i, k in zip(*np.nonzero(mask)):
+        if k not in (abi.GRAD_COLOR_R, abi.GRAD_COLOR_G, abi.GRAD_COLOR_B, abi.GRAD_MEDIUM_ALBEDO):
+            continue
+        eps = 1e-2
+        tp, tm = theta.copy(), theta.copy()
+        tp[i, k] += eps
+        tm[i, k] -= eps
+        ip = oracle.render(adjoint.with_params(pk, tp), r, W, H, spp, salt=salt)["mean"]
+        im = oracle.render(adjoint.with_params(pk, tm), r, W, H, spp, salt=salt)["mean"]
+        fd = float((dl * (ip - im)).sum() / (2 * eps))
+        assert abs(g[i, k] - fd) <= 1e-3 * abs(fd) + 1e-6, (pk.material_names[i], abi.GRAD_NAMES[k], g[i, k], fd)
+        checked += 1
+    return checked
+
+
+def test_forward_mode_colour_slots_on_the_adjoint_scene(oracle_lib):
+    """Lambert albedo, GGX F0 and dielectric transmittance (slots 0-2) of every model the
+    inverse-rendering scene holds, on a reduced copy of it (8 spheres)."""
+    sc, st, _ = scenes.adjoint_scene(0, n_spheres=8)
+    r, pk = Compiler().compile(sc, st)
+    models = {m["model"] for m in sc["materials"].values()}
+    assert {"lambert", "ggx", "dielectric"} <= models
+    assert _check_linear_parameters(r, pk, 12, 12, 8, 5) == 3 * (len(sc["materials"]) - 1) + 1
+
+
 def test_forward_mode_matches_oracle_differences_on_linear_parameters(oracle_lib):
     import oracle
     r, pk = _box()
@@ -50,7 +86,7 @@ def test_forward_mode_matches_oracle_differences_on_linear_parameters(oracle_lib
     mask = adjoint.live_mask(pk)
     checked = 0
     for i, k in zip(*np.nonzero(mask)):
-        if k not in (abi.GRAD_ALBEDO_R, abi.GRAD_ALBEDO_G, abi.GRAD_ALBEDO_B, abi.GRAD_MEDIUM_ALBEDO):
+        if k not in (abi.GRAD_COLOR_R, abi.GRAD_COLOR_G, abi.GRAD_COLOR_B, abi.GRAD_MEDIUM_ALBEDO):
             continue
         eps = 1e-2
         tp, tm = theta.copy(), theta.copy()
@@ -61,7 +97,7 @@ def test_forward_mode_matches_oracle_differences_on_linear_parameters(oracle_lib
         fd = float((dl * (ip - im)).sum() / (2 * eps))
         assert abs(g[i, k] - fd) <= 1e-3 * abs(fd) + 1e-6, (pk.material_names[i], abi.GRAD_NAMES[k], g[i, k], fd)
         checked += 1
-    assert checked == 13   # 4 Lambert albedos x 3 channels + the medium's albedo
+    assert checked == 16   # 4 Lambert albedos x 3 channels + the GGX F0 x 3 + the medium's albedo
 
 
 def test_forward_mode_ior_exact_at_normal_incidence(oracle_lib):
