@@ -466,6 +466,19 @@ int ptr_specialize(ptr_program* prog, ptr_scene* scene, double* seconds_out);
  * batched kernels.  The jobs' frames are not read.  seconds_out as for ptr_specialize. */
 int ptr_specialize_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs, double* seconds_out);
 
+/* ---- where mesh BVHs are built (no counterpart in the reference, which builds on the host:
+ * buildBVHCore / buildCWBVH, src/components/accel/bvh/bvh.ts:132-343 and
+ * src/components/accel/cwbvh/cwbvh.ts:80-372).  PTR_BUILD_HOST (the default): the
+ * reference's binned-SAH binary BVH (leaf 2) and its SAH collapse to the compressed wide
+ * BVH, on the host.  PTR_BUILD_DEVICE: a linear BVH over Morton codes (Karras 2012) and a
+ * greedy eight-wide collapse with the same quantized 80-byte nodes, on the GPU, from the
+ * mesh's vertex and index arrays.  Hits are the same either way (exact nearest hits with
+ * one tie rule); node counts and traversal cost differ.  Applies to later
+ * ptr_upload_scene calls on the context. */
+#define PTR_BUILD_HOST 0
+#define PTR_BUILD_DEVICE 1
+int ptr_set_accel_build(ptr_ctx* ctx, int where);
+
 /* ---- launch tuning (no counterpart in the reference: WebGL draws one fragment per pixel) ----
  * capacity: paths in flight per wave (0 = the default 2^24); block: threads per block of the
  * wavefront kernels (128 or 256; the grid keeps 2048 resident threads per SM);

@@ -42,6 +42,7 @@ SIGNATURES = {
     "ptr_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(abi.Tuning)]),
     "ptr_specialize": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
     "ptr_specialize_batch": (C.c_int, [C.c_void_p, C.POINTER(abi.BatchJob), C.c_int, C.POINTER(C.c_double)]),
+    "ptr_set_accel_build": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(abi.Tuning)]),
     "ptr_sync": (C.c_int, [C.c_void_p, C.c_int]),
     "ptr_read_export": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_float), C.c_size_t]),

@@ -24,6 +24,7 @@ LIGHT_QUAD, LIGHT_SPHERE, LIGHT_POINT, LIGHT_MESH = range(4)
 ENV_NONE, ENV_CONSTANT, ENV_IMAGE = range(3)
 DIRECT_NONE, DIRECT_NEE, DIRECT_MIS = range(3)
 ACCEL_BVH, ACCEL_CWBVH = range(2)
+BUILD_HOST, BUILD_DEVICE = range(2)
 EQUIANGULAR_OFF, EQUIANGULAR_DELTA, EQUIANGULAR_AREA = range(3)
 # adjoint parameter slots per material (include/ptx_rt.h PTR_GRAD_*)
 GRAD_SLOTS = 8

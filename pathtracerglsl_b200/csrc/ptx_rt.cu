@@ -24,6 +24,7 @@
 #include <dlfcn.h>
 
 #include "device/wavefront.cuh"
+#include "device/lbvh.cuh"
 #include "host/accel_build.h"
 
 using namespace ptx;
@@ -45,6 +46,7 @@ struct ptr_ctx {
     // batched kernels compiled for a job mix's occupant census (ptr_specialize_batch),
     // by census key
     std::map<std::string, SpecKernels> batch_spec;
+    int accel_build = PTR_BUILD_HOST;   // where ptr_upload_scene builds mesh BVHs (ptr_set_accel_build)
 };
 
 struct ptr_scene {
@@ -523,6 +525,129 @@ int device_sms(int dev) {
     return n > 0 ? n : 148;
 }
 
+// A mesh's binary BVH and compressed wide BVH built on the device (device/lbvh.cuh) from
+// its vertex and index arrays, with the triangle records of both leaf orders.  The
+// arrays the walks read join the scene's allocations; the build's temporaries are freed.
+int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMesh& m, std::vector<double>& root,
+                      int& n_nodes, int& n_cw_nodes, int& bin_depth) {
+    using namespace lbvh;
+    const int n = md.n_triangles;
+    cudaStream_t st = ctx->stream;
+    const int n_sm = device_sms(ctx->device);
+    const int grid = n_sm * 8, block = 256;
+    int n_pad = kBitonicTile;
+    while (n_pad < n) n_pad <<= 1;
+    std::vector<void*> tmp;
+    auto alloc = [&](size_t bytes, bool keep) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        (keep ? s->allocs : tmp).push_back(p);
+        return p;
+    };
+    auto release = [&]() { for (void* p : tmp) cudaFree(p); tmp.clear(); };
+    const int total = 2 * n - 1;
+    const int n_int = std::max(n - 1, 1);
+    float* d_pos = (float*)alloc(sizeof(float) * 3 * (size_t)md.n_vertices, false);
+    unsigned* d_idx = (unsigned*)alloc(sizeof(unsigned) * 3 * (size_t)n, false);
+    float* d_alpha = md.tri_alpha ? (float*)alloc(sizeof(float) * (size_t)n, false) : nullptr;
+    float4* lo = (float4*)alloc(sizeof(float4) * (size_t)n, false);
+    float4* hi = (float4*)alloc(sizeof(float4) * (size_t)n, false);
+    int* cb = (int*)alloc(sizeof(int) * 8, false);
+    unsigned long long* keys = (unsigned long long*)alloc(sizeof(unsigned long long) * (size_t)n_pad, false);
+    int* child = (int*)alloc(sizeof(int) * 2 * (size_t)n_int, false);
+    int* parent = (int*)alloc(sizeof(int) * (size_t)total, false);
+    int2* range = (int2*)alloc(sizeof(int2) * (size_t)total, false);
+    unsigned* arrivals = (unsigned*)alloc(sizeof(unsigned) * (size_t)n_int, false);
+    float4* nlo = (float4*)alloc(sizeof(float4) * (size_t)total, false);
+    float4* nhi = (float4*)alloc(sizeof(float4) * (size_t)total, false);
+    int2* ta = (int2*)alloc(sizeof(int2) * (size_t)n, false);
+    int2* tb = (int2*)alloc(sizeof(int2) * (size_t)n, false);
+    unsigned* counters = (unsigned*)alloc(sizeof(unsigned) * 8, false);
+    uint32_t* wide_big = (uint32_t*)alloc(sizeof(uint32_t) * 20 * (size_t)n, false);
+    uint32_t* order = (uint32_t*)alloc(sizeof(uint32_t) * (size_t)n, false);
+    float4* bvh = (float4*)alloc(sizeof(float4) * 2 * (size_t)total, true);
+    float4* tri = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
+    float4* tri_w = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
+    if (!d_pos || !d_idx || (md.tri_alpha && !d_alpha) || !lo || !hi || !cb || !keys || !child || !parent || !range ||
+        !arrivals || !nlo || !nhi || !ta || !tb || !counters || !wide_big || !order || !bvh || !tri || !tri_w) {
+        release();
+        return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc");
+    }
+    const int cb_init[8] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, (int)0x80000000, (int)0x80000000, (int)0x80000000, 0, 0};
+    const unsigned cnt_init[8] = {1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    const int2 root_task = make_int2(0, 0);   // binary node 0 (internal root, or the one leaf) -> wide node 0
+    cudaError_t e = cudaMemcpyAsync(d_pos, md.positions, sizeof(float) * 3 * (size_t)md.n_vertices, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, md.indices, sizeof(unsigned) * 3 * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && d_alpha) e = cudaMemcpyAsync(d_alpha, md.tri_alpha, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cb, cb_init, sizeof(cb_init), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counters, cnt_init, sizeof(cnt_init), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ta, &root_task, sizeof(int2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(arrivals, 0, sizeof(unsigned) * (size_t)n_int, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host arrays' copies end before they may go
+    if (e != cudaSuccess) { release(); return cuda_fail(ctx, e, "scene: device BVH build"); }
+    k_boxes<<<grid, block, 0, st>>>(d_pos, d_idx, n, lo, hi, cb);
+    k_keys<<<grid, block, 0, st>>>(lo, hi, n, n_pad, cb, keys);
+    k_bitonic_local<<<n_pad / kBitonicTile, 512, 0, st>>>(keys, 2, kBitonicTile);
+    for (int k = 2 * kBitonicTile; k <= n_pad; k <<= 1) {
+        for (int j = k >> 1; j >= kBitonicTile; j >>= 1) k_bitonic_global<<<grid, block, 0, st>>>(keys, n_pad, k, j);
+        k_bitonic_local<<<n_pad / kBitonicTile, 512, 0, st>>>(keys, k, k);
+    }
+    k_hierarchy<<<grid, block, 0, st>>>(keys, n, child, parent, range);
+    k_refit<<<grid, block, 0, st>>>(keys, lo, hi, n, child, parent, arrivals, nlo, nhi);
+    int* depth_dev = cb + 6;   // the binary layout's deepest level (initialised to 0)
+    k_binary_layout<<<grid, block, 0, st>>>(n, child, parent, range, nlo, nhi, bvh, depth_dev);
+    // the wide nodes, one level of tasks per launch
+    int n_tasks = 1, levels = 0;
+    int2 *tin = ta, *tout = tb;
+    unsigned cnt[4] = {0u, 0u, 0u, 0u};
+    e = cudaGetLastError();
+    while (n_tasks > 0 && e == cudaSuccess) {
+        if (++levels > 64) { cnt[3] |= 2u; break; }
+        e = cudaMemsetAsync(counters + 2, 0, sizeof(unsigned), st);
+        if (e != cudaSuccess) break;
+        k_collapse<<<std::min(grid, (n_tasks + block - 1) / block), block, 0, st>>>(n, child, range, nlo, nhi, keys, tin, n_tasks,
+                                                                                   tout, counters, wide_big, order);
+        e = cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        n_tasks = (int)cnt[2];
+        std::swap(tin, tout);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) { release(); return cuda_fail(ctx, e, "scene: device BVH build"); }
+    if (cnt[3] != 0u || cnt[1] != (unsigned)n || cnt[0] == 0u || cnt[0] > (unsigned)std::max(n, 1)) {
+        release();
+        return fail(ctx, PTR_E_INVALID, "scene: device CWBVH build failed (exponent range, depth or item count)");
+    }
+    if (levels >= ptx_host::kCwbvhStackDepth) {
+        release();
+        return fail(ctx, PTR_E_INVALID, "scene: device CWBVH depth " + std::to_string(levels) + " reaches the walk's stack depth");
+    }
+    uint32_t* wide = (uint32_t*)alloc(sizeof(uint32_t) * 20 * (size_t)cnt[0], true);
+    if (!wide) { release(); return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc"); }
+    e = cudaMemcpyAsync(wide, wide_big, sizeof(uint32_t) * 20 * (size_t)cnt[0], cudaMemcpyDeviceToDevice, st);
+    k_emit_tris<<<grid, block, 0, st>>>(d_pos, d_idx, d_alpha, nullptr, keys, n, tri);
+    k_emit_tris<<<grid, block, 0, st>>>(d_pos, d_idx, d_alpha, order, keys, n, tri_w);
+    float4 rb[2];
+    int depth = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rb, bvh, sizeof(rb), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&depth, depth_dev, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    release();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scene: device BVH build");
+    if (depth >= ptx_host::kBvhStackDepth)
+        return fail(ctx, PTR_E_INVALID, "scene: device BVH depth " + std::to_string(depth) + " reaches the walk's stack depth");
+    m.tri = tri;
+    m.tri_w = tri_w;
+    m.bvh = bvh;
+    m.cwbvh = (const uint4*)wide;
+    n_nodes = total;
+    n_cw_nodes = (int)cnt[0];
+    bin_depth = depth;
+    root = {rb[0].x, rb[0].y, rb[0].z, rb[1].x, rb[1].y, rb[1].z};
+    return PTR_OK;
+}
+
 // Acceleration structures of meshes and instanced batches, built on the host and uploaded
 // once: per mesh the binary SAH BLAS (leaf 2) and the compressed wide BVH, each with the
 // triangles re-emitted in its leaf order as (v0, e1 | alpha, e2); per batch a binary TLAS
@@ -574,23 +699,32 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
             }
             return tri;
         };
-        ptx_host::BinaryBvh bin = ptx_host::build_bvh(boxes.data(), T, ptx_host::kBvhLeafSize, false);
-        if (bin.max_depth >= ptx_host::kBvhStackDepth) std::fprintf(stderr, "ptx_rt: BVH depth %d reaches the walk's stack depth\n", bin.max_depth);
-        ptx_host::WideBvh wide = ptx_host::build_cwbvh(boxes.data(), T, ptx_host::kCwbvhCPrim);
-        if (wide.error) return fail(ctx, PTR_E_INVALID, "scene: CWBVH build failed (exponent range or DP invariant)");
-        std::vector<float4> tri_b = tri_array(bin.order), tri_w = tri_array(wide.order);
         DevMesh& m = meshes[mi];
         const float4* p4 = nullptr;
-        const uint4* u4 = nullptr;
         int rc;
-        if ((rc = dev_copy(ctx, s->allocs, tri_b.data(), tri_b.size(), &p4))) return rc;
-        m.tri = p4;
-        if ((rc = dev_copy(ctx, s->allocs, tri_w.data(), tri_w.size(), &p4))) return rc;
-        m.tri_w = p4;
-        if ((rc = dev_copy(ctx, s->allocs, (const float4*)bin.nodes.data(), 2 * (size_t)bin.node_count, &p4))) return rc;
-        m.bvh = p4;
-        if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wide.nodes.data(), 5 * (size_t)wide.node_count, &u4))) return rc;
-        m.cwbvh = u4;
+        int n_nodes = 0, n_cw_nodes = 0, bin_depth = 0;
+        if (ctx->accel_build == PTR_BUILD_DEVICE) {   // linear BVH + wide collapse on the GPU
+            if ((rc = build_mesh_device(ctx, s, md, m, root_box[mi], n_nodes, n_cw_nodes, bin_depth))) return rc;
+        } else {
+            ptx_host::BinaryBvh bin = ptx_host::build_bvh(boxes.data(), T, ptx_host::kBvhLeafSize, false);
+            if (bin.max_depth >= ptx_host::kBvhStackDepth) std::fprintf(stderr, "ptx_rt: BVH depth %d reaches the walk's stack depth\n", bin.max_depth);
+            ptx_host::WideBvh wide = ptx_host::build_cwbvh(boxes.data(), T, ptx_host::kCwbvhCPrim);
+            if (wide.error) return fail(ctx, PTR_E_INVALID, "scene: CWBVH build failed (exponent range or DP invariant)");
+            std::vector<float4> tri_b = tri_array(bin.order), tri_w = tri_array(wide.order);
+            const uint4* u4 = nullptr;
+            if ((rc = dev_copy(ctx, s->allocs, tri_b.data(), tri_b.size(), &p4))) return rc;
+            m.tri = p4;
+            if ((rc = dev_copy(ctx, s->allocs, tri_w.data(), tri_w.size(), &p4))) return rc;
+            m.tri_w = p4;
+            if ((rc = dev_copy(ctx, s->allocs, (const float4*)bin.nodes.data(), 2 * (size_t)bin.node_count, &p4))) return rc;
+            m.bvh = p4;
+            if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wide.nodes.data(), 5 * (size_t)wide.node_count, &u4))) return rc;
+            m.cwbvh = u4;
+            n_nodes = bin.node_count;
+            n_cw_nodes = wide.node_count;
+            bin_depth = bin.max_depth;
+            root_box[mi] = {bin.nodes[0], bin.nodes[1], bin.nodes[2], bin.nodes[4], bin.nodes[5], bin.nodes[6]};
+        }
         m.light_cdf = nullptr;
         m.light_tri = nullptr;
         if (is_light[mi]) {
@@ -626,11 +760,10 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
             m.light_tri = p4;
         }
         m.n_tris = T;
-        m.n_nodes = bin.node_count;
-        m.n_cw_nodes = wide.node_count;
-        root_box[mi] = {bin.nodes[0], bin.nodes[1], bin.nodes[2], bin.nodes[4], bin.nodes[5], bin.nodes[6]};
+        m.n_nodes = n_nodes;
+        m.n_cw_nodes = n_cw_nodes;
         grow(root_box[mi].data(), root_box[mi].data() + 3);
-        s->max_stack_depth = std::max(s->max_stack_depth, bin.max_depth);
+        s->max_stack_depth = std::max(s->max_stack_depth, bin_depth);
     }
     std::vector<DevBatch> batches(d->n_batches > 0 ? d->n_batches : 0);
     for (int bi = 0; bi < d->n_batches; ++bi) {
@@ -1981,6 +2114,13 @@ int ptr_specialize_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs, do
     k.shadow = m.shadow;
     ctx->batch_spec[census_key(c)] = k;
     if (seconds_out && compiled) *seconds_out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return PTR_OK;
+}
+
+int ptr_set_accel_build(ptr_ctx* ctx, int where) {
+    if (!ctx) return PTR_E_INVALID;
+    if (where != PTR_BUILD_HOST && where != PTR_BUILD_DEVICE) return fail(ctx, PTR_E_INVALID, "ptr_set_accel_build: unknown builder");
+    ctx->accel_build = where;
     return PTR_OK;
 }
 

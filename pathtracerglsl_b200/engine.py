@@ -90,6 +90,12 @@ class CudaEngine:
         return rc
 
     # -- scene data --------------------------------------------------------------------
+    def set_accel_build(self, where):
+        """Where later register_scene calls build mesh BVHs: 'host' (the reference's SAH
+        builders restated, the default) or 'device' (linear BVH + wide collapse on the GPU)."""
+        code = {"host": abi.BUILD_HOST, "device": abi.BUILD_DEVICE}[where]
+        self._check(self.lib.ptr_set_accel_build(self.ctx, code))
+
     def register_scene(self, packed):
         """Upload a packed scene (host arrays are copied; the host keeps ownership)."""
         if self.scene is not None:
