@@ -13,31 +13,39 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
+# the same restatement with its float transcendentals evaluated in double and rounded once
+# (a second binary32 libm; see fm in pt_oracle.cpp)
+LIB_WIDE = os.path.join(BUILD, "liboracle_wide.so")
 SOURCES = [os.path.join(HERE, "pt_oracle.cpp")]
 
 
 def build(force=False):
-    """Compile the restatement with g++ (OpenMP, -O3, binary32 without FMA contraction)."""
+    """Compile the restatement with g++ (OpenMP, -O3, binary32 without FMA contraction),
+    and its wide-transcendental twin."""
     os.makedirs(BUILD, exist_ok=True)
     header = os.path.join(HERE, "..", "include", "ptx_rt.h")
     newest = max(os.path.getmtime(p) for p in SOURCES + [header])
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
-        return LIB
-    cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-           *SOURCES, "-o", LIB]
-    subprocess.run(cmd, check=True)
+    for out, extra in ((LIB, []), (LIB_WIDE, ["-DORACLE_WIDE_MATH"])):
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= newest:
+            continue
+        cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared", *extra,
+               *SOURCES, "-o", out + ".tmp"]
+        subprocess.run(cmd, check=True)
+        os.replace(out + ".tmp", out)
     return LIB
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
+def lib(variant=""):
+    """The oracle library: "" (the host libm's float functions) or "wide"."""
+    if variant not in _libs:
+        path = LIB_WIDE if variant == "wide" else LIB
+        if not os.path.exists(path):
             build()
-        _lib = ctypes.CDLL(LIB)
+        _lib = ctypes.CDLL(path)
+        _libs[variant] = _lib
         _lib.oracle_render.restype = ctypes.c_int
         _lib.oracle_render.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_void_p, ctypes.c_int]
         _lib.oracle_render_tile.restype = ctypes.c_int
@@ -55,14 +63,15 @@ def lib():
         _lib.oracle_field_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         _lib.oracle_forward_tile.restype = ctypes.c_int
         _lib.oracle_forward_tile.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 2 + [ctypes.c_int]
-    return _lib
+    return _libs[variant]
 
 
 def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=None,
-           threads=0, keep_samples=False, pixel_offset=(0, 0), image_size=None):
+           threads=0, keep_samples=False, pixel_offset=(0, 0), image_size=None, variant=""):
     """Render with the oracle.  Returns dict(mean, var, sum, sumsq, samples?, counts).
     ``pixel_offset`` / ``image_size``: the frame is a width x height tile at that offset of
-    an image of that size (engine.pixelOffset / engine.imageSize)."""
+    an image of that size (engine.pixelOffset / engine.imageSize).  ``variant``: "" or
+    "wide" (the twin whose float transcendentals are evaluated in double)."""
     from pathtracerglsl_b200 import abi
     desc = packed.desc()
     fr = abi.Frame()
@@ -77,7 +86,7 @@ def render(packed, renderer, width, height, spp, first_sample=0, salt=0, params=
     q = np.zeros((height, width, 3), np.float64)
     samples = np.zeros((spp, height, width, 3), np.float32) if keep_samples else None
     counts = (ctypes.c_uint64 * 2)()
-    rc = lib().oracle_render(ctypes.addressof(desc), ctypes.addressof(renderer.program), ctypes.addressof(fr),
+    rc = lib(variant).oracle_render(ctypes.addressof(desc), ctypes.addressof(renderer.program), ctypes.addressof(fr),
                              s.ctypes.data, q.ctypes.data,
                              samples.ctypes.data if samples is not None else None,
                              ctypes.addressof(counts), threads)

@@ -23,6 +23,30 @@
 
 #include "../include/ptx_rt.h"
 
+// The float transcendentals of the walk.  By default the host libm's float functions;
+// built with ORACLE_WIDE_MATH they are evaluated in double and rounded once, which gives
+// a second, independent binary32 libm.  Renders with the two differ only where one
+// function result differs by an ulp and a later comparison flips: the rate at which that
+// happens is the rate expected between any two correct libms (the device's included).
+// Double arguments (the forward mode's duals) always take the double functions.
+namespace fm {
+#ifdef ORACLE_WIDE_MATH
+#define FM_F1(name) inline float name(float x) { return (float)std::name((double)x); }
+#define FM_F2(name) inline float name(float x, float y) { return (float)std::name((double)x, (double)y); }
+#else
+#define FM_F1(name) inline float name(float x) { return std::name(x); }
+#define FM_F2(name) inline float name(float x, float y) { return std::name(x, y); }
+#endif
+#define FM_D1(name) inline double name(double x) { return std::name(x); }
+#define FM_D2(name) inline double name(double x, double y) { return std::name(x, y); }
+FM_F1(exp) FM_F1(log) FM_F1(sin) FM_F1(cos) FM_F1(tan) FM_F1(tanh) FM_F1(atanh) FM_F1(cosh) FM_F2(atan2) FM_F2(pow)
+FM_D1(exp) FM_D1(log) FM_D1(sin) FM_D1(cos) FM_D1(tan) FM_D1(tanh) FM_D1(atanh) FM_D1(cosh) FM_D2(atan2) FM_D2(pow)
+#undef FM_F1
+#undef FM_F2
+#undef FM_D1
+#undef FM_D2
+}  // namespace fm
+
 namespace {
 
 // ---------------------------------------------------------------- vector helpers
@@ -50,7 +74,7 @@ inline float fminf_(float a, float b) { return b < a ? b : a; }
 inline float fmaxf_(float a, float b) { return a < b ? b : a; }
 inline v3 vmin(v3 a, v3 b) { return v3(fminf_(a.x, b.x), fminf_(a.y, b.y), fminf_(a.z, b.z)); }
 inline v3 vmax(v3 a, v3 b) { return v3(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z)); }
-inline v3 vexp(v3 a) { return v3(std::exp(a.x), std::exp(a.y), std::exp(a.z)); }
+inline v3 vexp(v3 a) { return v3(fm::exp(a.x), fm::exp(a.y), fm::exp(a.z)); }
 inline v3 ld3(const float* p) { return v3(p[0], p[1], p[2]); }
 inline float clampf(float x, float lo, float hi) { return fminf_(fmaxf_(x, lo), hi); }
 inline float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
@@ -91,7 +115,7 @@ inline s4 operator*(s4 a, float t) { return s4(a.x * t, a.y * t, a.z * t, a.w * 
 inline s4 operator*(float t, s4 a) { return s4(t * a.x, t * a.y, t * a.z, t * a.w); }
 inline s4 operator/(s4 a, float t) { return s4(a.x / t, a.y / t, a.z / t, a.w / t); }
 inline s4 operator-(s4 a) { return s4(-a.x, -a.y, -a.z, -a.w); }
-inline s4 vexp(s4 a) { return s4(std::exp(a.x), std::exp(a.y), std::exp(a.z), std::exp(a.w)); }
+inline s4 vexp(s4 a) { return s4(fm::exp(a.x), fm::exp(a.y), fm::exp(a.z), fm::exp(a.w)); }
 inline s4 vmax(s4 a, s4 b) { return s4(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z), fmaxf_(a.w, b.w)); }
 inline float spectrum_average(s4 s) { float sum = s.x; sum += s.y; sum += s.z; sum += s.w; return sum * (1.0f / 4.0f); }
 inline float spectrum_max(s4 s) { float m = s.w; m = fmaxf_(s.z, m); m = fmaxf_(s.y, m); m = fmaxf_(s.x, m); return m; }
@@ -179,7 +203,7 @@ inline float dielectric_fresnel(float cos_i, float eta) {
     return 0.5f * (r_par * r_par + r_perp * r_perp);
 }
 // schlick_fresnel (math.glsl:83-85)
-template <class Col> inline Col schlick_fresnel(Col f0, float c) { return f0 + (Col(1.0f) - f0) * std::pow(1.0f - c, 5.0f); }
+template <class Col> inline Col schlick_fresnel(Col f0, float c) { return f0 + (Col(1.0f) - f0) * fm::pow(1.0f - c, 5.0f); }
 // ray_spawn (glsl/core/ray.glsl:29-32)
 inline Ray ray_spawn(const Hit& h, v3 wi) {
     float side = dot(wi, h.ng) >= 0.0f ? 1.0f : -1.0f;
@@ -746,7 +770,7 @@ template <class Col> inline ISampleT<Col> lambert_sample(v3 wo, const Hit& h, Co
     float sin_theta = std::sqrt(fmaxf_(0.0f, 1.0f - u1));
     float phi = TWO_PI * u0;
     ISampleT<Col> s;
-    s.wi = normalize(f.t * (sin_theta * std::cos(phi)) + f.b * (sin_theta * std::sin(phi)) + n * cos_theta);
+    s.wi = normalize(f.t * (sin_theta * fm::cos(phi)) + f.b * (sin_theta * fm::sin(phi)) + n * cos_theta);
     s.weight = albedo;
     s.pdf = cos_theta * (1.0f / PI);
     s.flags = LOBE_REFLECTION;
@@ -768,8 +792,8 @@ inline v3 mf_sample_vndf(v3 wol, float a, float u0, float u1) {
     v3 T2 = cross(vh, T1);
     float rr = std::sqrt(u0);
     float phi = TWO_PI * u1;
-    float t1 = rr * std::cos(phi);
-    float t2 = rr * std::sin(phi);
+    float t1 = rr * fm::cos(phi);
+    float t2 = rr * fm::sin(phi);
     float s_ = 0.5f * (1.0f + vh.z);
     t2 = (1.0f - s_) * std::sqrt(fmaxf_(0.0f, 1.0f - t1 * t1)) + s_ * t2;
     v3 nh = t1 * T1 + t2 * T2 + std::sqrt(fmaxf_(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
@@ -929,10 +953,10 @@ inline v3 field_eval(const uint32_t* code, v3 p) {
                 float x = a[k];
                 switch (op) {
                     case PTR_FOP_NEG: x = -x; break;
-                    case PTR_FOP_EXP: x = std::exp(x); break;
-                    case PTR_FOP_LOG: x = std::log(x); break;
-                    case PTR_FOP_SIN: x = std::sin(x); break;
-                    case PTR_FOP_COS: x = std::cos(x); break;
+                    case PTR_FOP_EXP: x = fm::exp(x); break;
+                    case PTR_FOP_LOG: x = fm::log(x); break;
+                    case PTR_FOP_SIN: x = fm::sin(x); break;
+                    case PTR_FOP_COS: x = fm::cos(x); break;
                     case PTR_FOP_SQRT: x = std::sqrt(x); break;
                     case PTR_FOP_ABS: x = std::fabs(x); break;
                     case PTR_FOP_FLOOR: x = std::floor(x); break;
@@ -948,7 +972,7 @@ inline v3 field_eval(const uint32_t* code, v3 p) {
             for (int k = 0; k < 3; ++k) {
                 float x = a[k], y = b[k];
                 switch (op) {
-                    case PTR_FOP_POW: x = std::pow(x, y); break;
+                    case PTR_FOP_POW: x = fm::pow(x, y); break;
                     case PTR_FOP_MIN: x = y < x ? y : x; break;
                     case PTR_FOP_MAX: x = x < y ? y : x; break;
                     case PTR_FOP_MOD: x = x - y * std::floor(x / y); break;
@@ -991,7 +1015,7 @@ inline MediumSampleT<Col> medium_sample_analytic(Col sigma_a, Col sigma_s, const
     Col sigma_t = sigma_a + sigma_s;
     int c = sample_channel<Col>(x0);
     float sc = sigma_t[c];
-    float t = sc == 0.0f ? t_max : -std::log(1.0f - x1) / sc;
+    float t = sc == 0.0f ? t_max : -fm::log(1.0f - x1) / sc;
     MediumSampleT<Col> ms;
     if (t < t_max) {
         Col tr = vexp(-sigma_t * t);
@@ -1028,7 +1052,7 @@ template <class Col> inline ISampleT<Col> hg_sample(v3 wo, float g, float x0, fl
     v3 t, b;
     build_basis(-wo, t, b);
     ISampleT<Col> s;
-    s.wi = normalize(t * (sin_theta * std::cos(phi)) + b * (sin_theta * std::sin(phi)) + (-wo) * cos_theta);
+    s.wi = normalize(t * (sin_theta * fm::cos(phi)) + b * (sin_theta * fm::sin(phi)) + (-wo) * cos_theta);
     s.weight = Col(1.0f);
     s.pdf = spectrum_average(Col(hg_eval(s.wi, wo, g)));
     s.flags = LOBE_MEDIUM;
@@ -1056,7 +1080,7 @@ inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
 inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
 inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
 inline Dual dsqrt(Dual a) { double r = std::sqrt(a.v); return {r, r > 0.0 ? a.d / (2.0 * r) : 0.0}; }
-inline Dual dexp(Dual a) { double e = std::exp(a.v); return {e, e * a.d}; }
+inline Dual dexp(Dual a) { double e = fm::exp(a.v); return {e, e * a.d}; }
 constexpr double PI_D = 3.14159265359;   // the same constant as PI, in float64
 
 // Trowbridge-Reitz D, separable Smith G1 (microfacet.glsl:22-54) with a dual alpha.
@@ -1128,7 +1152,7 @@ inline float spectrum_lane(const ptr_scene_desc& d, const ptr_spectrum& sp, floa
         float q = 14387768.775039338f / sp.c[0];
         float ratio = 550.0f / lambda;
         float ratio2 = ratio * ratio;
-        v = sp.c[1] * (std::exp(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (std::exp(q / lambda) - 1.0f);
+        v = sp.c[1] * (fm::exp(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (fm::exp(q / lambda) - 1.0f);
         v = sp.scale * v;
     } else {
         v = sp.scale;
@@ -1151,10 +1175,10 @@ inline void wavelengths_sample(const ptr_program_desc& P, float u, float lam[4],
             lam[k] = P.lambda_min + (P.lambda_max - P.lambda_min) * v;
             pdf[k] = 1.0f / (P.lambda_max - P.lambda_min);
         } else {
-            float a = std::tanh(0.0072f * (P.lambda_min - 538.0f));
-            float b = std::tanh(0.0072f * (P.lambda_max - 538.0f));
-            lam[k] = 538.0f + std::atanh(a * (1.0f - v) + b * v) / 0.0072f;
-            float c = std::cosh(0.0072f * (lam[k] - 538.0f));
+            float a = fm::tanh(0.0072f * (P.lambda_min - 538.0f));
+            float b = fm::tanh(0.0072f * (P.lambda_max - 538.0f));
+            lam[k] = 538.0f + fm::atanh(a * (1.0f - v) + b * v) / 0.0072f;
+            float c = fm::cosh(0.0072f * (lam[k] - 538.0f));
             pdf[k] = 0.0072f / ((b - a) * c * c);
         }
     }
@@ -1273,8 +1297,8 @@ struct TracerT {
     // bilinear, wrap u, clamp v) and sampled by env/sampler_cdf.glsl:13-84.
     void equirect_uv(v3 dir, float& u, float& v) const {
         v3 n = normalize(dir);
-        float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : std::atan2(n.z, n.x)) + d.env.rotation;
-        float theta = std::atan2(std::sqrt(n.x * n.x + n.z * n.z), n.y);
+        float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : fm::atan2(n.z, n.x)) + d.env.rotation;
+        float theta = fm::atan2(std::sqrt(n.x * n.x + n.z * n.z), n.y);
         u = phi * (1.0f / TWO_PI) + 0.5f;
         u = u - std::floor(u);
         v = theta * (1.0f / PI);
@@ -1317,7 +1341,7 @@ struct TracerT {
         float dm = marg(j) - (j > 0 ? marg(j - 1) : 0.0f);
         float dc = cond(j, i) - (i > 0 ? cond(j, i - 1) : 0.0f);
         float theta = PI * ((float)j + 0.5f) / (float)H;
-        float domega = (TWO_PI / (float)W) * 2.0f * std::sin(theta) * std::sin(0.5f * PI / (float)H);
+        float domega = (TWO_PI / (float)W) * 2.0f * fm::sin(theta) * fm::sin(0.5f * PI / (float)H);
         return (dc * dm) / domega;
     }
     v3 sample_table(float x0, float x1) const {
@@ -1337,13 +1361,13 @@ struct TracerT {
         float phi = (((float)i + uf) / (float)W - 0.5f) * TWO_PI - d.env.rotation;
         bool north = 2 * j < H;
         float row = north ? (float)j : (float)(H - j - 1);
-        float a = std::sin(0.5f * PI * row / (float)H);
-        float b = std::sin(0.5f * PI * (row + 1.0f) / (float)H);
+        float a = fm::sin(0.5f * PI * row / (float)H);
+        float b = fm::sin(0.5f * PI * (row + 1.0f) / (float)H);
         float tt = north ? vf : 1.0f - vf;
         float h = (a * a) * (1.0f - tt) + (b * b) * tt;
         float y = (north ? 1.0f : -1.0f) * (1.0f - 2.0f * h);
         float rr = 2.0f * std::sqrt(h * (1.0f - h));
-        return v3(rr * std::cos(phi), y, rr * std::sin(phi));
+        return v3(rr * fm::cos(phi), y, rr * fm::sin(phi));
     }
     LS environment_sample(float x0, float x1) const {
         LS ls;
@@ -1353,7 +1377,7 @@ struct TracerT {
                 float y = 1.0f - 2.0f * (x0 / a);
                 float r = std::sqrt(fmaxf_(0.0f, 1.0f - y * y));
                 float phi = TWO_PI * x1;
-                ls.wi = v3(r * std::cos(phi), y, r * std::sin(phi));
+                ls.wi = v3(r * fm::cos(phi), y, r * fm::sin(phi));
             } else {
                 ls.wi = sample_table((x0 - a) / (1.0f - a), x1);
             }
@@ -1367,7 +1391,7 @@ struct TracerT {
         float z = 1.0f - 2.0f * x0;
         float r = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
         float phi = TWO_PI * x1;
-        ls.wi = v3(r * std::cos(phi), z, r * std::sin(phi));
+        ls.wi = v3(r * fm::cos(phi), z, r * fm::sin(phi));
         ls.distance = MAX_DIST;
         ls.radiance = c_env() * d.env.intensity;
         ls.pdf = 1.0f / (4.0f * PI);
@@ -1447,7 +1471,7 @@ struct TracerT {
             v3 w = to_c * (1.0f / std::sqrt(dc2));
             v3 t, b;
             build_basis(w, t, b);
-            ls.wi = normalize(t * (sin_t * std::cos(phi)) + b * (sin_t * std::sin(phi)) + w * cos_t);
+            ls.wi = normalize(t * (sin_t * fm::cos(phi)) + b * (sin_t * fm::sin(phi)) + w * cos_t);
             ls.pdf = 1.0f / (TWO_PI * omc_max);
             float proj = dot(to_c, ls.wi);
             v3 perp = to_c - proj * ls.wi;
@@ -1714,7 +1738,7 @@ struct TracerT {
         float t = 0.0f, xd = x0, xe = x1;
         const int cap = tracking_cap(sbar * t_max);
         for (int i = 0; i < cap; ++i) {
-            t += -std::log(1.0f - xd) / sbar;
+            t += -fm::log(1.0f - xd) / sbar;
             if (t >= t_max) { ms.weight = w; return ms; }
             v3 p = r.o + r.d * t;
             v3 sa, ss;
@@ -1750,7 +1774,7 @@ struct TracerT {
         float t = 0.0f;
         const int cap = tracking_cap(sbar * len);
         for (int i = 0; i < cap; ++i) {
-            t += -std::log(1.0f - g.next()) / sbar;
+            t += -fm::log(1.0f - g.next()) / sbar;
             if (t >= len) return T;
             v3 sa, ss;
             het_props(m, r.o + r.d * t, sa, ss);
@@ -1853,7 +1877,7 @@ struct TracerT {
                 float z = 1.0f - 2.0f * y0;
                 float rr = std::sqrt(fmaxf_(0.0f, 1.0f - z * z));
                 float phi = TWO_PI * y1;
-                nl = v3(rr * std::cos(phi), z, rr * std::sin(phi));
+                nl = v3(rr * fm::cos(phi), z, rr * fm::sin(phi));
                 pos = ld3(l.p) + nl * l.p[3];
                 pdf_area = 1.0f / (4.0f * PI * l.p[3] * l.p[3]);
             }
@@ -1865,11 +1889,11 @@ struct TracerT {
         float t_c = dot(D, r.d);
         float h2 = fmaxf_(dot(D, D) - t_c * t_c, 1e-8f);
         float h = std::sqrt(h2);
-        float theta_a = std::atan2(0.0f - t_c, h);
-        float theta_b = std::atan2(t_max - t_c, h);
+        float theta_a = fm::atan2(0.0f - t_c, h);
+        float theta_b = fm::atan2(t_max - t_c, h);
         float u = rng.next();
         float theta = theta_a * (1.0f - u) + theta_b * u;
-        float t = t_c + h * std::tan(theta);
+        float t = t_c + h * fm::tan(theta);
         float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
         v3 p_evt = r.o + r.d * t;
         Col sigma_s = c_sigma_s(med_mat);
@@ -1899,7 +1923,7 @@ struct TracerT {
     // d w_c / d F0_c of a weight w_c = F_c(F0_c) x (terms free of F0), Schlick's F at cosine c:
     // w_c (1 - (1 - c)^5) / F_c, one entry per channel, appended at n.
     int dw_schlick_f0(int mat, const ptr_material& m, double c, Col w, DW* dw, int n) const {
-        const double s5 = std::pow(1.0 - c, 5.0);
+        const double s5 = fm::pow(1.0 - c, 5.0);
         for (int ch = 0; ch < 3; ++ch) {
             const double F = (double)m.f0[ch] + (1.0 - (double)m.f0[ch]) * s5;
             dw[n].k = slot_k(mat, PTR_GRAD_COLOR_R + ch);
@@ -2077,7 +2101,7 @@ struct TracerT {
                             if (ms.scattered) {   // a st exp(-st t) / pdf
                                 const float pdf = fmaxf_(spectrum_average(sigma_t * vexp(-sigma_t * ms.t)), 1e-20f);
                                 const Dual w_st = a * Dual{st, 1.0} * dexp(-Dual{st, 1.0} * (double)ms.t) / (double)pdf;
-                                const Dual w_a = Dual{a, 1.0} * st * std::exp(-st * (double)ms.t) / (double)pdf;
+                                const Dual w_a = Dual{a, 1.0} * st * fm::exp(-st * (double)ms.t) / (double)pdf;
                                 dw[0] = {slot_k(med_mat, PTR_GRAD_SIGMA_T), {w_st.d, w_st.d, w_st.d}};
                                 dw[1] = {slot_k(med_mat, PTR_GRAD_MEDIUM_ALBEDO), {w_a.d, w_a.d, w_a.d}};
                                 tan_mul(throughput, ms.weight, dw.data(), 2);

@@ -40,7 +40,7 @@ __device__ __forceinline__ float ggx_dlog_alpha(f3 wi, f3 wo, const Hit& h, floa
 }
 // d log F_c / d F0_c of Schlick's Fresnel F = F0 + (1 - F0) (1 - c)^5, per channel.
 __device__ __forceinline__ f3 schlick_dlog_f0(f3 f0, float c) {
-    const float s5 = powf(1.0f - c, 5.0f);
+    const float s5 = m_pow(1.0f - c, 5.0f);
     const f3 F = f0 + (f3(1.0f) - f0) * s5;
     return f3(1.0f - s5) / vmax(F, f3(1e-20f));
 }

@@ -12,6 +12,22 @@
 
 namespace ptx {
 
+// The walk's float transcendentals.  By default CUDA's single-precision functions; a
+// build with PTR_WIDE_MATH (ptr_specialize with that define) evaluates them in double and
+// rounds once, the same functions as the oracle's wide twin, so that samples can be
+// compared without the two libms' last-ulp differences.
+#ifdef PTR_WIDE_MATH
+#define PTR_M1(name, fn) __device__ __forceinline__ float name(float x) { return (float)fn((double)x); }
+#define PTR_M2(name, fn) __device__ __forceinline__ float name(float x, float y) { return (float)fn((double)x, (double)y); }
+#else
+#define PTR_M1(name, fn) __device__ __forceinline__ float name(float x) { return fn##f(x); }
+#define PTR_M2(name, fn) __device__ __forceinline__ float name(float x, float y) { return fn##f(x, y); }
+#endif
+PTR_M1(m_exp, exp) PTR_M1(m_log, log) PTR_M1(m_sin, sin) PTR_M1(m_cos, cos) PTR_M1(m_tan, tan)
+PTR_M1(m_tanh, tanh) PTR_M1(m_atanh, atanh) PTR_M1(m_cosh, cosh) PTR_M2(m_atan2, atan2) PTR_M2(m_pow, pow)
+#undef PTR_M1
+#undef PTR_M2
+
 // ---- scene specialisation.  The generic library keeps every occupant (all masks on, the
 // region list read from the scene).  A build for one scene x strategy defines the masks of
 // the occupants it holds and, optionally, its region count and region shapes as
@@ -76,7 +92,7 @@ __device__ __forceinline__ float gmin(float a, float b) { return b < a ? b : a; 
 __device__ __forceinline__ float gmax(float a, float b) { return a < b ? b : a; }
 __device__ __forceinline__ f3 vmin(f3 a, f3 b) { return f3(gmin(a.x, b.x), gmin(a.y, b.y), gmin(a.z, b.z)); }
 __device__ __forceinline__ f3 vmax(f3 a, f3 b) { return f3(gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z)); }
-__device__ __forceinline__ f3 vexp(f3 a) { return f3(expf(a.x), expf(a.y), expf(a.z)); }
+__device__ __forceinline__ f3 vexp(f3 a) { return f3(m_exp(a.x), m_exp(a.y), m_exp(a.z)); }
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return gmin(gmax(x, lo), hi); }
 __device__ __forceinline__ float signf(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
 __device__ __forceinline__ f3 ld3(const float* p) { return f3(p[0], p[1], p[2]); }
@@ -122,7 +138,7 @@ __device__ __forceinline__ int spectrum_sample_channel(float u) { int c = (int)(
 __device__ __forceinline__ float spectrum_average(s4 s) { float a = s.x; a += s.y; a += s.z; a += s.w; return a * (1.0f / 4.0f); }
 __device__ __forceinline__ float spectrum_max(s4 s) { float m = s.w; m = gmax(s.z, m); m = gmax(s.y, m); m = gmax(s.x, m); return m; }
 __device__ __forceinline__ bool spectrum_is_black(s4 s) { return s.x <= 0.f && s.y <= 0.f && s.z <= 0.f && s.w <= 0.f; }
-__device__ __forceinline__ s4 vexp(s4 a) { return s4(expf(a.x), expf(a.y), expf(a.z), expf(a.w)); }
+__device__ __forceinline__ s4 vexp(s4 a) { return s4(m_exp(a.x), m_exp(a.y), m_exp(a.z), m_exp(a.w)); }
 __device__ __forceinline__ s4 vmax(s4 a, s4 b) { return s4(gmax(a.x, b.x), gmax(a.y, b.y), gmax(a.z, b.z), gmax(a.w, b.w)); }
 // Uniform lane choice for channel-MIS: min(int(u * N), N - 1).
 template <class Col> __device__ __forceinline__ int sample_channel(float u);
@@ -195,7 +211,7 @@ __device__ __forceinline__ float dielectric_fresnel(float cos_i, float eta) {
 }
 template <class Col>
 __device__ __forceinline__ Col schlick_fresnel(Col f0, float c) {
-    return f0 + (Col(1.0f) - f0) * powf(1.0f - c, 5.0f);
+    return f0 + (Col(1.0f) - f0) * m_pow(1.0f - c, 5.0f);
 }
 __device__ __forceinline__ float power_heuristic(float pf, float pg) {
     float f2 = pf * pf;

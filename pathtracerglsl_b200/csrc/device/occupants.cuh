@@ -37,7 +37,7 @@ __device__ __forceinline__ float spec_lane(const DevScene& S, const ptr_spectrum
         float q = 14387768.775039338f / sp.c[0];
         float ratio = 550.0f / lambda;
         float ratio2 = ratio * ratio;
-        v = sp.c[1] * (expf(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (expf(q / lambda) - 1.0f);
+        v = sp.c[1] * (m_exp(q / 550.0f) - 1.0f) * ratio2 * ratio2 * ratio / (m_exp(q / lambda) - 1.0f);
         v = sp.scale * v;
     } else {
         v = sp.scale;
@@ -85,8 +85,8 @@ __device__ __forceinline__ ISample<Col> lambert_sample(f3 wo, const Hit& h, Col 
     float sin_theta = sqrtf(gmax(0.0f, 1.0f - u1));
     float phi = kTwoPi * u0;
     float sp, cp;
-    sp = sinf(phi);
-    cp = cosf(phi);
+    sp = m_sin(phi);
+    cp = m_cos(phi);
     ISample<Col> s;
     s.wi = normalize(h.frame.t * (sin_theta * cp) + h.frame.b * (sin_theta * sp) + n * cos_theta);
     s.weight = albedo;
@@ -119,8 +119,8 @@ __device__ __forceinline__ f3 mf_sample_vndf(f3 wol, float a, float u0, float u1
     f3 T2 = cross(vh, T1);
     float rr = sqrtf(u0);
     float phi = kTwoPi * u1;
-    float t1 = rr * cosf(phi);
-    float t2 = rr * sinf(phi);
+    float t1 = rr * m_cos(phi);
+    float t2 = rr * m_sin(phi);
     float s_ = 0.5f * (1.0f + vh.z);
     t2 = (1.0f - s_) * sqrtf(gmax(0.0f, 1.0f - t1 * t1)) + s_ * t2;
     f3 nh = t1 * T1 + t2 * T2 + sqrtf(gmax(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
@@ -305,7 +305,7 @@ __device__ __forceinline__ ISample<Col> hg_sample(f3 wo, float g, float x0, floa
     f3 t, b;
     build_basis(-wo, t, b);
     ISample<Col> s;
-    s.wi = normalize(t * (sin_theta * cosf(phi)) + b * (sin_theta * sinf(phi)) + (-wo) * cos_theta);
+    s.wi = normalize(t * (sin_theta * m_cos(phi)) + b * (sin_theta * m_sin(phi)) + (-wo) * cos_theta);
     s.weight = Col(1.0f);
     float e = hg_eval(s.wi, wo, g);
     s.pdf = spectrum_average(Col(e));
@@ -320,8 +320,8 @@ __device__ __forceinline__ ISample<Col> hg_sample(f3 wo, float g, float x0, floa
 // env/sampler_cdf.glsl:13-84 mixed with 1/16 uniform-sphere probability.
 __device__ __forceinline__ float2 equirect_uv(const DevScene& S, f3 dir) {
     f3 n = normalize(dir);
-    float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : atan2f(n.z, n.x)) + S.env_rotation;
-    float theta = atan2f(sqrtf(n.x * n.x + n.z * n.z), n.y);
+    float phi = (n.x == 0.0f && n.z == 0.0f ? 0.0f : m_atan2(n.z, n.x)) + S.env_rotation;
+    float theta = m_atan2(sqrtf(n.x * n.x + n.z * n.z), n.y);
     float u = phi * (1.0f / kTwoPi) + 0.5f;
     u = u - floorf(u);
     return make_float2(u, theta * (1.0f / kPi));
@@ -358,7 +358,7 @@ __device__ __forceinline__ float env_marg(const DevScene& S, int j) { return __l
 __device__ __forceinline__ float env_cond(const DevScene& S, int j, int i) { return __ldg(S.env_cond + (size_t)j * S.env_w + i); }
 __device__ __forceinline__ float env_texel_domega(int j, int W, int H) {
     float theta = kPi * ((float)j + 0.5f) / (float)H;
-    return (kTwoPi / (float)W) * 2.0f * sinf(theta) * sinf(0.5f * kPi / (float)H);
+    return (kTwoPi / (float)W) * 2.0f * m_sin(theta) * m_sin(0.5f * kPi / (float)H);
 }
 __device__ __forceinline__ float env_uniform_fraction(const DevScene& S) {
     return env_marg(S, S.env_h - 1) > 0.0f ? 0.0625f : 1.0f;
@@ -379,13 +379,13 @@ __device__ __forceinline__ f3 env_chart_sample(const DevScene& S, int ci, int cj
     float phi = (((float)ci + ux) / (float)W - 0.5f) * kTwoPi - S.env_rotation;
     bool north = 2 * cj < H;
     float row = north ? (float)cj : (float)(H - cj - 1);
-    float a = sinf(0.5f * kPi * row / (float)H);
-    float b = sinf(0.5f * kPi * (row + 1.0f) / (float)H);
+    float a = m_sin(0.5f * kPi * row / (float)H);
+    float b = m_sin(0.5f * kPi * (row + 1.0f) / (float)H);
     float t = north ? uy : 1.0f - uy;
     float h = (a * a) * (1.0f - t) + (b * b) * t;
     float y = (north ? 1.0f : -1.0f) * (1.0f - 2.0f * h);
     float r = 2.0f * sqrtf(h * (1.0f - h));
-    return f3(r * cosf(phi), y, r * sinf(phi));
+    return f3(r * m_cos(phi), y, r * m_sin(phi));
 }
 __device__ __forceinline__ f3 env_sample_table(const DevScene& S, float x0, float x1) {
     const int W = S.env_w, H = S.env_h;
@@ -425,7 +425,7 @@ __device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float 
             float y = 1.0f - 2.0f * (x0 / a);
             float r = sqrtf(gmax(0.0f, 1.0f - y * y));
             float phi = kTwoPi * x1;
-            ls.wi = f3(r * cosf(phi), y, r * sinf(phi));
+            ls.wi = f3(r * m_cos(phi), y, r * m_sin(phi));
         } else {
             ls.wi = env_sample_table(S, (x0 - a) / (1.0f - a), x1);
         }
@@ -439,7 +439,7 @@ __device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float 
     float z = 1.0f - 2.0f * x0;
     float r = sqrtf(gmax(0.0f, 1.0f - z * z));
     float phi = kTwoPi * x1;
-    ls.wi = f3(r * cosf(phi), z, r * sinf(phi));
+    ls.wi = f3(r * m_cos(phi), z, r * m_sin(phi));
     ls.distance = kMaxDist;
     ls.radiance = Colors<Col>::env_color(S, wl) * S.env_intensity;
     ls.pdf = 1.0f / (4.0f * kPi);
@@ -518,7 +518,7 @@ __device__ LightSample<Col> light_sample_one(const DevScene& S, const ptr_light&
         f3 w = to_c * (1.0f / sqrtf(dc2));
         f3 t, b;
         build_basis(w, t, b);
-        ls.wi = normalize(t * (sin_t * cosf(phi)) + b * (sin_t * sinf(phi)) + w * cos_t);
+        ls.wi = normalize(t * (sin_t * m_cos(phi)) + b * (sin_t * m_sin(phi)) + w * cos_t);
         ls.pdf = 1.0f / (kTwoPi * omc);
         float proj = dot(to_c, ls.wi);
         f3 perp = to_c - proj * ls.wi;
@@ -772,10 +772,10 @@ __device__ f3 field_eval(const uint32_t* code, f3 p) {
                 float x = r[k];
                 switch (op) {
                     case PTR_FOP_NEG: x = -x; break;
-                    case PTR_FOP_EXP: x = expf(x); break;
-                    case PTR_FOP_LOG: x = logf(x); break;
-                    case PTR_FOP_SIN: x = sinf(x); break;
-                    case PTR_FOP_COS: x = cosf(x); break;
+                    case PTR_FOP_EXP: x = m_exp(x); break;
+                    case PTR_FOP_LOG: x = m_log(x); break;
+                    case PTR_FOP_SIN: x = m_sin(x); break;
+                    case PTR_FOP_COS: x = m_cos(x); break;
                     case PTR_FOP_SQRT: x = sqrtf(x); break;
                     case PTR_FOP_ABS: x = fabsf(x); break;
                     case PTR_FOP_FLOOR: x = floorf(x); break;
@@ -792,7 +792,7 @@ __device__ f3 field_eval(const uint32_t* code, f3 p) {
             for (int k = 0; k < 3; ++k) {
                 float x = ra[k], y = rb[k];
                 switch (op) {
-                    case PTR_FOP_POW: x = powf(x, y); break;
+                    case PTR_FOP_POW: x = m_pow(x, y); break;
                     case PTR_FOP_MIN: x = y < x ? y : x; break;
                     case PTR_FOP_MAX: x = x < y ? y : x; break;
                     case PTR_FOP_MOD: x = x - y * floorf(x / y); break;
@@ -873,7 +873,7 @@ __device__ MediumSample<f3> medium_sample_delta(const DevScene& S, const ptr_mat
     float t = 0.0f, xd = x0, xe = x1;
     const int cap = tracking_cap(sbar * t_max);
     for (int i = 0; i < cap; ++i) {
-        t += -logf(1.0f - xd) / sbar;
+        t += -m_log(1.0f - xd) / sbar;
         if (t >= t_max) { ms.weight = w; return ms; }
         f3 p = r.o + r.d * t;
         HetProps h = het_props(S, m, p);
@@ -909,7 +909,7 @@ __device__ f3 medium_ratio_track(const DevScene& S, const ptr_material& m, const
     float t = 0.0f;
     const int cap = tracking_cap(sbar * len);
     for (int i = 0; i < cap; ++i) {
-        t += -logf(1.0f - rng.next()) / sbar;
+        t += -m_log(1.0f - rng.next()) / sbar;
         if (t >= len) return T;
         HetProps h = het_props(S, m, r.o + r.d * t);
         T = T * (vmax(f3(sbar) - (extinction ? h.sa + h.ss : h.sa), f3(0.0f)) / sbar);
@@ -934,7 +934,7 @@ __device__ __forceinline__ MediumSample<Col> medium_sample_analytic(Col sigma_a,
     Col sigma_t = sigma_a + sigma_s;
     int c = sample_channel<Col>(x0);
     float sc = sigma_t[c];
-    float t = sc == 0.0f ? t_max : -logf(1.0f - x1) / sc;
+    float t = sc == 0.0f ? t_max : -m_log(1.0f - x1) / sc;
     MediumSample<Col> ms;
     if (t < t_max) {
         Col tr = vexp(-sigma_t * t);
@@ -989,7 +989,7 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat,
             float z = 1.0f - 2.0f * y0;
             float rr = sqrtf(gmax(0.0f, 1.0f - z * z));
             float phi = kTwoPi * y1;
-            nl = f3(rr * cosf(phi), z, rr * sinf(phi));
+            nl = f3(rr * m_cos(phi), z, rr * m_sin(phi));
             pos = ld3(l.p) + nl * l.p[3];
             pdf_area = 1.0f / (4.0f * kPi * l.p[3] * l.p[3]);
         }
@@ -1000,11 +1000,11 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat,
     float t_c = dot(D, r.d);
     float h2 = gmax(dot(D, D) - t_c * t_c, 1e-8f);
     float h = sqrtf(h2);
-    float theta_a = atan2f(0.0f - t_c, h);
-    float theta_b = atan2f(t_max - t_c, h);
+    float theta_a = m_atan2(0.0f - t_c, h);
+    float theta_b = m_atan2(t_max - t_c, h);
     float u = rng.next();
     float theta = theta_a * (1.0f - u) + theta_b * u;
-    float t = t_c + h * tanf(theta);
+    float t = t_c + h * m_tan(theta);
     float pdf_t = h / ((theta_b - theta_a) * (h2 + (t - t_c) * (t - t_c)));
     q.p_evt = r.o + r.d * t;
     Col sigma_s = Colors<Col>::sigma_s(S, med_mat, wl);

@@ -398,10 +398,10 @@ __device__ __forceinline__ void wavelengths_sample(const FrameParams& F, float u
             l[k] = F.lambda_min + (F.lambda_max - F.lambda_min) * v;
             p[k] = 1.0f / (F.lambda_max - F.lambda_min);
         } else {
-            float a = tanhf(0.0072f * (F.lambda_min - 538.0f));
-            float b = tanhf(0.0072f * (F.lambda_max - 538.0f));
-            l[k] = 538.0f + atanhf(a * (1.0f - v) + b * v) / 0.0072f;
-            float c = coshf(0.0072f * (l[k] - 538.0f));
+            float a = m_tanh(0.0072f * (F.lambda_min - 538.0f));
+            float b = m_tanh(0.0072f * (F.lambda_max - 538.0f));
+            l[k] = 538.0f + m_atanh(a * (1.0f - v) + b * v) / 0.0072f;
+            float c = m_cosh(0.0072f * (l[k] - 538.0f));
             p[k] = 0.0072f / ((b - a) * c * c);
         }
     }

@@ -1320,6 +1320,19 @@ int spec_compile(ptr_ctx* ctx, const Census& c, SpecModule& out, bool& compiled)
         std::string("-I") + (dev_env ? dev_env : dir + "/csrc/device"),
         std::string("-I") + (inc_env ? inc_env : dir + "/../include")};
     for (const auto& o : census_options(c)) opts.push_back(o);
+    // PTR_SPEC_DEFINES: extra space-separated -D options (the wide-math parity build)
+    if (const char* extra = std::getenv("PTR_SPEC_DEFINES")) {
+        std::string tok;
+        for (const char* q = extra;; ++q) {
+            if (*q == ' ' || *q == '\0') {
+                if (tok.rfind("-D", 0) == 0) opts.push_back(tok);
+                tok.clear();
+                if (*q == '\0') break;
+            } else {
+                tok += *q;
+            }
+        }
+    }
     std::string key;
     for (const auto& o : opts) key += o + "\n";
     key += n_closest + "\n" + n_shade + "\n" + n_shadow;

@@ -110,3 +110,28 @@ def test_batched_kernels_compile(media):
             assert lib.nvrtcGetLoweredName(prog, n, C.byref(low)) == 0 and low.value
     finally:
         lib.nvrtcDestroyProgram(C.byref(prog))
+
+
+def test_wide_math_kernels_compile():
+    """The per-scene kernels with PTR_WIDE_MATH (double-rounded float transcendentals, the
+    parity build of tests/test_gpu_math_parity.py)."""
+    lib = _nvrtc()
+    names = [b"ptx::k_closest<false, false>", b"ptx::k_shade<ptx::f3, 2, true, false, false>",
+             b"ptx::k_shadow<ptx::f3, true, false, false, false>"]
+    opts = [b"-arch=sm_100a", b"-std=c++17", b"-fmad=false", b"-default-device", b"-DPTR_WIDE_MATH",
+            ("-I" + os.path.join(ROOT, "pathtracerglsl_b200", "csrc", "device")).encode(),
+            ("-I" + os.path.join(ROOT, "include")).encode()]
+    prog = C.c_void_p()
+    assert lib.nvrtcCreateProgram(C.byref(prog), PRELUDE, b"ptr_specialize.cu", 0, None, None) == 0
+    try:
+        for n in names:
+            assert lib.nvrtcAddNameExpression(prog, n) == 0
+        arr = (C.c_char_p * len(opts))(*opts)
+        rc = lib.nvrtcCompileProgram(prog, len(opts), arr)
+        size = C.c_size_t()
+        lib.nvrtcGetProgramLogSize(prog, C.byref(size))
+        log = C.create_string_buffer(size.value)
+        lib.nvrtcGetProgramLog(prog, log)
+        assert rc == 0, log.value.decode(errors="replace")[:4000]
+    finally:
+        lib.nvrtcDestroyProgram(C.byref(prog))
