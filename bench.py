@@ -402,8 +402,10 @@ def run_ours(args):
 MESH_PICK = "capacity=33554432,sort_buckets=8,ray_sort=1"
 
 
-def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True):
-    """One plain workload (one ptr_render per step): the JSON line (rank 0; None elsewhere)."""
+def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True, accel_build=None, rmse_leg=True):
+    """One plain workload (one ptr_render per step): the JSON line (rank 0; None elsewhere).
+    accel_build: where mesh BVHs are built at upload ('host' or 'device'; the upload's wall
+    time is reported)."""
     import torch
     from pathtracerglsl_b200.compiler import Compiler
     from pathtracerglsl_b200.engine import CudaEngine
@@ -414,7 +416,12 @@ def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True
         cfg = dict(cfg, spp_per_step=spp)
     renderer, packed = Compiler().compile(sc, st)
     eng = CudaEngine(local)
+    accel_build = accel_build or args.accel_build
+    eng.set_accel_build(accel_build)
+    t_up = time.perf_counter()
     eng.register_scene(packed)
+    eng.sync()
+    cfg = dict(cfg, accel_build=accel_build, upload_s=time.perf_counter() - t_up)
     eng.load_renderer(renderer)
     eng.pin_reset_salt(1 + rank)      # each replica renders its own sample stream
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
@@ -496,7 +503,7 @@ def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True
            "h2d_bytes_per_step": 160, "d2h_bytes_per_step": int(img.nbytes)}
 
     # ---- image error of a step against a high-spp reference of the same frame (untimed)
-    rmse = image_error(eng, w, h, spp, 1 + rank) if not args.no_rmse else None
+    rmse = image_error(eng, w, h, spp, 1 + rank) if (rmse_leg and not args.no_rmse) else None
 
     # ---- instrumented passes (not part of the timed region): per-kernel-class device
     # time with CUDA events, then the traversal tallies of the counting kernels
@@ -891,6 +898,8 @@ def run_metric(args):
     line = measure_batch(args, rank, local, world, dist)
     adj = measure_adjoint(args, rank, local, world, dist, cpu_leg=False)
     mesh = measure_ours(args, "mesh", rank, local, world, dist, tuning=MESH_PICK, cpu_leg=False)
+    mesh_dev = measure_ours(args, "mesh", rank, local, world, dist, tuning=MESH_PICK, cpu_leg=False,
+                            accel_build="device", rmse_leg=False)
     if rank == 0:
         line["adjoint"] = {"value": adj["value"], "unit": "samples/s", "ms_per_step": adj["ms_per_step"],
                            "steps": adj["steps"], "config": adj["config"],
@@ -899,7 +908,14 @@ def run_metric(args):
                            "roofline": adj["roofline"], "clocks": adj["clocks"]}
         line["mesh"] = {k: mesh[k] for k in ("value", "unit", "ms_per_step", "steps", "config", "e2e", "roofline",
                                              "clocks", "rmse", "rays", "traversal")}
-        line["gpu_launches"] = line["gpu_launches"] + adj["gpu_launches"] + mesh["gpu_launches"]
+        line["mesh"]["device_built"] = {
+            "value": mesh_dev["value"], "unit": "samples/s", "ms_per_step": mesh_dev["ms_per_step"],
+            "upload_s": mesh_dev["config"]["upload_s"], "host_built_upload_s": mesh["config"]["upload_s"],
+            "over_host_built": mesh_dev["value"] / mesh["value"], "traversal": mesh_dev["traversal"],
+            "clocks": mesh_dev["clocks"],
+            "form": "the same workload with its 1.31 M-triangle BLAS built on the device (linear BVH + greedy "
+                    "eight-wide collapse) instead of the host's SAH builders"}
+        line["gpu_launches"] = line["gpu_launches"] + adj["gpu_launches"] + mesh["gpu_launches"] + mesh_dev["gpu_launches"]
         line["config"] = dict(line["config"], workload="metric: " + line["config"]["workload"],
                               also="adjoint-c5 (adjoint vs forward) and mesh-c2 (plain, matched RMSE) in the "
                                    "'adjoint' and 'mesh' keys")
@@ -921,6 +937,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0: the workload's own)")
     ap.add_argument("--no-rmse", action="store_true", help="skip the high-spp image-error reference")
     ap.add_argument("--generic", action="store_true", help="keep the generic kernels (no ptr_specialize)")
+    ap.add_argument("--accel-build", default="host", choices=["host", "device"],
+                    help="where mesh BVHs are built at upload (plain workloads)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
