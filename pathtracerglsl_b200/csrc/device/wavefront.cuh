@@ -25,12 +25,22 @@
 namespace ptx {
 
 // Path pool (indexed by path slot).
+// One field of a two-field path record: path i's value at p[2 i] and the partner field's
+// at p[2 i + 1], so the two 16-byte fields a kernel reads and writes together fill one
+// 32-byte sector (a surviving path's store never half-fills a sector that the L2 would
+// first have to read back from DRAM).
+template <class T> struct Pair {
+    T* p;
+    __host__ __device__ __forceinline__ T& operator[](long long i) const { return p[2 * i]; }
+    __host__ __device__ __forceinline__ explicit operator bool() const { return p != nullptr; }
+};
+
 struct PathPool {
-    float4* ray_o;     // origin.xyz, prev_bsdf_pdf
-    float4* ray_d;     // direction.xyz, eta_scale
-    float4* thr;       // throughput.xyz, -
-    float4* rad;       // radiance.xyz, -
-    float4* prev_q;    // stored light-query point (prev_query.p)
+    Pair<float4> ray_o;  // origin.xyz, prev_bsdf_pdf          } one record
+    Pair<float4> ray_d;  // direction.xyz, eta_scale           }
+    Pair<float4> thr;    // throughput.xyz, -                  } one record
+    Pair<float4> rad;    // radiance.xyz, -                    }
+    Pair<float4> prev_q; // stored light-query point (prev_query.p)  } one record, with st
     float4* prev_n;    // stored light-query normal and two-sidedness (light-tree selection)
     unsigned* sh_seed; // the shadow query's sampler dimension at its NEE site (heterogeneous media)
     // first-hit pictures (programs with measurement.aovs; NULL otherwise): per path its
@@ -38,21 +48,21 @@ struct PathPool {
     // doubles per pixel, then the normal block)
     float4* aov;
     double* aov_sum;
-    int4* st;          // bounce, current_medium, null_crossings, prev_was_delta
+    Pair<int4> st;       // bounce, current_medium, null_crossings, prev_was_delta
     uint2* rng;        // sampler base, dimension
-    float4* hit;       // t, u, v, - ; (region, element, prim) in hit_i
-    int4* hit_i;       // region_owner, element, prim, -
+    Pair<float4> hit;    // t, u, v, - ; (region, element, prim) in hit_i    } one record
+    Pair<int4> hit_i;    // region_owner, element, prim, -                   }
     // shadow queries (one per path and iteration at most)
-    float4* sh_o;      // origin.xyz, max distance (opaque form)
-    float4* sh_d;      // direction.xyz, crossings left (as int)
-    float4* sh_lp;     // light point.xyz, MIS weight
-    float4* sh_c;      // contribution prefix throughput*Le*f*cos (xyz), pdf
+    Pair<float4> sh_o;   // origin.xyz, max distance (opaque form)     } one record
+    Pair<float4> sh_d;   // direction.xyz, crossings left (as int)     }
+    Pair<float4> sh_lp;  // light point.xyz, MIS weight                } one record
+    Pair<float4> sh_c;   // contribution prefix throughput*Le*f*cos (xyz), pdf  }
     // second shadow slot: the per-segment equiangular query of the same iteration (a path
     // may issue it and a surface NEE query in one walk iteration); NULL when unused
-    float4* sh2_o;
-    float4* sh2_d;
-    float4* sh2_lp;
-    float4* sh2_c;
+    Pair<float4> sh2_o;
+    Pair<float4> sh2_d;
+    Pair<float4> sh2_lp;
+    Pair<float4> sh2_c;
     int* q[2];         // live-path queues (ping-pong)
     int* shq;          // shadow queue
     int* shq2;         // second-slot shadow queue (count in cnt[4])
@@ -1213,6 +1223,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                 }
             }
             pool.rad[i] = col_st(rad, 0.0f);
+            pool.thr[i] = col_st(thr, 0.0f);   // with rad: the whole record, for a dying path too
             if constexpr (ADJ) {
                 pool.l_rem[i] = f4(lrem, 0.0f);
                 if (shadow) {
@@ -1223,7 +1234,6 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if (alive) {
                 pool.ray_o[i] = f4(r.o, prev_bsdf_pdf);
                 pool.ray_d[i] = f4(r.d, eta_scale);
-                pool.thr[i] = col_st(thr, 0.0f);
                 pool.prev_q[i] = f4(prev_qp, 0.0f);
                 pool.st[i] = make_int4(bounce, cur_med, nulls, prev_delta ? 1 : 0);
                 pool.rng[i] = make_uint2(rng.base, rng.dim);
@@ -1260,8 +1270,8 @@ constexpr unsigned kErrAdjMedia = 8u;      // ... more were crossed (their terms
 // order of scene_any); an unoccluded query adds its stored contribution as k_shadow does.
 template <class Col, bool COUNT>
 __device__ __forceinline__ void shadow_refill(const DevScene& S, const PathPool& pool, const int* shq, unsigned n, int slot,
-                                              const float4* a_o, const float4* a_d, const float4* a_lp, const float4* a_c,
-                                              unsigned* ticket, Work* w) {
+                                              const Pair<float4> a_o, const Pair<float4> a_d, const Pair<float4> a_lp,
+                                              const Pair<float4> a_c, unsigned* ticket, Work* w) {
     constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     const int fr = S.flat_region;
     const DevBatch& b = S.batches[S.regions[fr].ref];
@@ -1341,10 +1351,10 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     const unsigned n = pool.cnt[slot ? 4 : 2];
     if (blockIdx.x == 0 && threadIdx.x == 0) pool.stats[1] += n;
     const int* shq = slot ? pool.shq2 : (pool.ray_sort ? sorted_queue(pool.shq_s, pool.shq, n) : pool.shq);
-    const float4* a_o = slot ? pool.sh2_o : pool.sh_o;
-    const float4* a_d = slot ? pool.sh2_d : pool.sh_d;
-    const float4* a_lp = slot ? pool.sh2_lp : pool.sh_lp;
-    const float4* a_c = slot ? pool.sh2_c : pool.sh_c;
+    const Pair<float4> a_o = slot ? pool.sh2_o : pool.sh_o;
+    const Pair<float4> a_d = slot ? pool.sh2_d : pool.sh_d;
+    const Pair<float4> a_lp = slot ? pool.sh2_lp : pool.sh_lp;
+    const Pair<float4> a_c = slot ? pool.sh2_c : pool.sh_c;
     Work wk{0u, 0u, 0u, 0u};
     if (PTR_REFILL && !MEDIA && !BATCH && !ADJ && pool.fetch && S0.flat_region >= 0 &&
         inst_mesh_flat_ok(S0, S0.batches[S0.regions[S0.flat_region].ref])) {

@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -209,13 +210,18 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
     size_t c = (size_t)capacity;
     PathPool& q = p->pool;
     int rc = PTR_OK;
-    if ((rc = get(c * 16, (void**)&q.ray_o)) || (rc = get(c * 16, (void**)&q.ray_d)) ||
-        (rc = get(c * 16, (void**)&q.thr)) || (rc = get(c * 16, (void**)&q.rad)) ||
-        (rc = get(c * 16, (void**)&q.prev_q)) || (rc = get(c * 16, (void**)&q.prev_n)) || (rc = get(c * 4, (void**)&q.sh_seed)) || (rc = get(c * 16, (void**)&q.st)) ||
-        (rc = get(c * 8, (void**)&q.rng)) || (rc = get(c * 16, (void**)&q.hit)) ||
-        (rc = get(c * 16, (void**)&q.hit_i)) || (rc = get(c * 16, (void**)&q.sh_o)) ||
-        (rc = get(c * 16, (void**)&q.sh_d)) || (rc = get(c * 16, (void**)&q.sh_lp)) ||
-        (rc = get(c * 16, (void**)&q.sh_c)) || (rc = get(c * 4, (void**)&q.q[0])) ||
+    // a two-field record: 32 bytes per path, the first field at +0, the second at +16
+    auto pair = [&](auto& a, auto& b) -> int {
+        void* base = nullptr;
+        if (int r = get(c * 32, &base)) return r;
+        a.p = (std::remove_reference_t<decltype(*a.p)>*)base;
+        b.p = (std::remove_reference_t<decltype(*b.p)>*)((char*)base + 16);
+        return PTR_OK;
+    };
+    if ((rc = pair(q.ray_o, q.ray_d)) || (rc = pair(q.thr, q.rad)) ||
+        (rc = pair(q.prev_q, q.st)) || (rc = get(c * 16, (void**)&q.prev_n)) || (rc = get(c * 4, (void**)&q.sh_seed)) ||
+        (rc = get(c * 8, (void**)&q.rng)) || (rc = pair(q.hit, q.hit_i)) ||
+        (rc = pair(q.sh_o, q.sh_d)) || (rc = pair(q.sh_lp, q.sh_c)) || (rc = get(c * 4, (void**)&q.q[0])) ||
         (rc = get(c * 4, (void**)&q.q[1])) || (rc = get(c * 4, (void**)&q.shq)) ||
         (rc = get(c * 4, (void**)&q.job)) ||
         (rc = get(64, (void**)&q.cnt)) || (rc = get(64, (void**)&q.stats)) ||
@@ -232,8 +238,7 @@ int alloc_pool(ptr_program* p, int capacity, bool slot2, bool adj = false, bool 
         return fail(ctx, PTR_E_CUDA, "path pool: clearing the work tickets failed");
     }
     // the second shadow slot only for programs with the per-segment equiangular site
-    if (slot2 && ((rc = get(c * 16, (void**)&q.sh2_o)) || (rc = get(c * 16, (void**)&q.sh2_d)) ||
-                  (rc = get(c * 16, (void**)&q.sh2_lp)) || (rc = get(c * 16, (void**)&q.sh2_c)) ||
+    if (slot2 && ((rc = pair(q.sh2_o, q.sh2_d)) || (rc = pair(q.sh2_lp, q.sh2_c)) ||
                   (rc = get(c * 4, (void**)&q.shq2)))) {
         free_pool(p);
         return rc;
@@ -1992,7 +1997,7 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     long long cap = (long long)npix <= cap_max ? (cap_max / (long long)npix) * (long long)npix : cap_max;
     if (cap > total) cap = total;
     if (p->capacity < cap || !p->pool.l_rem) {
-        int rc = alloc_pool(p, (int)std::max<long long>(cap, p->capacity), p->pool.sh2_o != nullptr, true);
+        int rc = alloc_pool(p, (int)std::max<long long>(cap, p->capacity), p->pool.sh2_o.p != nullptr, true);
         if (rc) return rc;
     }
     if (!p->fp_dev) CK(ctx, cudaMalloc(&p->fp_dev, sizeof(FrameParams)));
@@ -2324,10 +2329,13 @@ PathPool na_pool(unsigned char* base) {
     size_t c = kNoAllocMaxPaths;
     unsigned char* p = base + kNaPool;
     auto take = [&](size_t bytes) { unsigned char* r = p; p += bytes * c; return (void*)r; };
-    q.ray_o = (float4*)take(16); q.ray_d = (float4*)take(16); q.thr = (float4*)take(16);
-    q.rad = (float4*)take(16); q.prev_q = (float4*)take(16); q.prev_n = nullptr; q.sh_seed = nullptr; q.st = (int4*)take(16);
-    q.hit = (float4*)take(16); q.hit_i = (int4*)take(16); q.sh_o = (float4*)take(16);
-    q.sh_d = (float4*)take(16); q.sh_lp = (float4*)take(16); q.sh_c = (float4*)take(16);
+    auto pair = [&](auto& a, auto& b) {   // a two-field record of 32 bytes per path
+        unsigned char* base = (unsigned char*)take(32);
+        a.p = (std::remove_reference_t<decltype(*a.p)>*)base;
+        b.p = (std::remove_reference_t<decltype(*b.p)>*)(base + 16);
+    };
+    pair(q.ray_o, q.ray_d); pair(q.thr, q.rad); pair(q.prev_q, q.st); q.prev_n = nullptr; q.sh_seed = nullptr;
+    pair(q.hit, q.hit_i); pair(q.sh_o, q.sh_d); pair(q.sh_lp, q.sh_c);
     q.rng = (uint2*)take(8); q.q[0] = (int*)take(4); q.q[1] = (int*)take(4); q.shq = (int*)take(4);
     q.cnt = (unsigned*)(base + kNaCnt);
     q.stats = (unsigned long long*)(base + kNaStats);
