@@ -612,10 +612,15 @@ def measure_batch(args, rank, local, world, dist, cpu_leg=True):
     # the project's autotuner picks pool capacity, block size and sort-bucket count on a
     # reduced copy of the mix (every job at 1/16 of its spp), then every arm uses the pick
     from pathtracerglsl_b200 import autotune
-    small = [(w, h, max(1, spp // 16), 0, 7) for (w, h, spp, _f, _s) in frames]
-    tuned = autotune.tune(eng, lambda: b.render(small), budget_s=40.0)
-    cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
-               tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
+    if args.tuning:   # a recorded pick (e.g. for a profiler run of the same configuration)
+        pick = dict(autotune.DEFAULTS, **parse_tuning(args.tuning))
+        eng.set_tuning(**pick)
+        cfg = dict(cfg, tuning=pick, tuning_search="a recorded pick of the autotuner")
+    else:
+        small = [(w, h, max(1, spp // 16), 0, 7) for (w, h, spp, _f, _s) in frames]
+        tuned = autotune.tune(eng, lambda: b.render(small), budget_s=40.0)
+        cfg = dict(cfg, tuning={k: tuned["best"][k] for k in autotune.KNOBS},
+                   tuning_search=[{k: r[k] for k in autotune.KNOBS + ("ms",)} for r in tuned["results"]])
     stream = torch.cuda.ExternalStream(eng.stream_handle(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     for _ in range(args.warmup):
