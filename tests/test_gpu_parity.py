@@ -2,8 +2,11 @@
 
 Both consume the same packed scene and draw the same counter-based random numbers, so
 samples agree exactly except where a transcendental (sinf/expf/powf/...) differs by an
-ulp between CUDA and the host libm and a later branch flips.  Tolerances:
-  * per sample: |cuda - oracle| <= 1e-4 * max(1, |oracle|) for >= 99% of samples;
+ulp between CUDA and the host libm and a later branch flips.  Measured over every case
+of the GPU suite: 51 of 52 cases have no sample outside the per-sample tolerance, the
+equiangular haze case 2 of 9,600; with the same (double-rounded) transcendentals on both
+sides no case has any (test_gpu_math_parity).  Tolerances:
+  * per sample: |cuda - oracle| <= 1e-4 * max(1, |oracle|) for >= 99.9% of samples;
   * per pixel: |mean_cuda - mean_oracle| <= 3 * combined standard error + 1e-6 for
     >= 99.7% of pixels (the 3-sigma gate of the per-pixel Monte Carlo error).
 """
@@ -37,7 +40,7 @@ def _cam(case):
     return {}
 
 
-def compare(engine, oracle_lib, scene, st, W, H, spp, params, salt=11, frac_samples=0.99, frac_pixels=0.997):
+def compare(engine, oracle_lib, scene, st, W, H, spp, params, salt=11, frac_samples=0.999, frac_pixels=0.997):
     r, pk = Compiler().compile(scene, st)
     engine.register_scene(pk)
     engine.load_renderer(r)
@@ -119,7 +122,7 @@ def test_heterogeneous_media_match_oracle(engine, oracle_lib, kind, direct):
     queries' own streams, against the oracle sample by sample.  The fields' exp/sin run on
     CUDA's and the host's libm, so a rare lottery may fall differently: 98 % of samples."""
     sc, st = scenes.het_fog(direct=direct, kind=kind)
-    compare(engine, oracle_lib, sc, st, 40, 40, 8, CASE_CAMERAS["cornell"], frac_samples=0.98)
+    compare(engine, oracle_lib, sc, st, 40, 40, 8, CASE_CAMERAS["cornell"])
 
 
 def test_upload_rejects_malformed_field_programs(engine):

@@ -60,4 +60,4 @@ def test_tile_matches_the_oracle_tile(engine, oracle_lib):
     assert rc == abi.PTR_OK
     o = oracle_lib.render(pk, r, tw, th, spp, salt=salt, keep_samples=True, pixel_offset=(tx, ty), image_size=(W, H))
     close = np.abs(out - o["samples"]) <= 1e-4 * np.maximum(1.0, np.abs(o["samples"]))
-    assert close.all(axis=-1).mean() >= 0.99
+    assert close.all(axis=-1).mean() >= 0.999
