@@ -663,7 +663,8 @@ def measure_batch(args, rank, local, world, dist, cpu_leg=True):
         b.specialize(plain=True)
     prog_frames = [(w, h, min(spp, PROGRESSIVE_SPP), 0, salt) for (w, h, spp, _f, salt) in frames]
     prog_samples = sum(w * h * spp for (w, h, spp, _f, _s) in prog_frames)
-    prog_ms = timed(lambda: b.render_progressive(prog_frames, sync=False), 1)
+    b.render_progressive([(w, h, 2, 0, salt) for (w, h, _s, _f, salt) in prog_frames])   # untimed warm-up
+    prog_ms = timed(lambda: b.render_progressive(prog_frames, sync=False), 2) / 2.0
     progressive = prog_samples * world / (prog_ms / 1000.0)
 
     # end to end: tables from host memory in, every job's radiance out to host memory
