@@ -184,26 +184,6 @@ struct BatchTables {
     int capacity;
 };
 
-// Batched kernels: every job's scene record staged once per block in shared memory
-// (PTR_BATCH_SMEM_SCENES builds, mixes of at most kBatchSmemJobs jobs), so that a path's
-// scene fields are shared-memory loads instead of global loads the compiler repeats
-// after each store; other builds read the records in place.
-#ifndef PTR_BATCH_SMEM_SCENES
-#define PTR_BATCH_SMEM_SCENES 0
-#endif
-constexpr int kBatchSmemJobs = 64;
-constexpr size_t kBatchSceneBytes = PTR_BATCH_SMEM_SCENES ? kBatchSmemJobs * sizeof(DevScene) : 16;
-__device__ __forceinline__ const DevScene* stage_batch_scenes(const BatchTables& bt, unsigned char* raw) {
-    if (!PTR_BATCH_SMEM_SCENES || bt.n_jobs > kBatchSmemJobs) return bt.scenes;
-    static_assert(sizeof(DevScene) % 4 == 0, "scene records are copied as words");
-    const int words = bt.n_jobs * (int)(sizeof(DevScene) / 4);
-    const unsigned* src = reinterpret_cast<const unsigned*>(bt.scenes);
-    unsigned* dst = reinterpret_cast<unsigned*>(raw);
-    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
-    __syncthreads();
-    return reinterpret_cast<const DevScene*>(raw);
-}
-
 constexpr unsigned kErrStack = 1u;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -621,8 +601,6 @@ __device__ __forceinline__ void closest_refill(const DevScene& S, const PathPool
 
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene S0, PathPool pool, int in, BatchTables bt) {
-    __shared__ __align__(16) unsigned char s_scene_raw[BATCH ? kBatchSceneBytes : 16];
-    const DevScene* scenes = BATCH ? stage_batch_scenes(bt, s_scene_raw) : nullptr;
     const int buckets = pool.sort_buckets;
     unsigned n = pool.cnt[in];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -644,7 +622,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     while (cur.next(k)) {
         if (k >= n) continue;
         int i = q[k];
-        const DevScene& S = BATCH ? scenes[pool.job[i]] : S0;
+        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         Ray r;
         r.o = xyz(pool.ray_o[i]);
         r.d = xyz(pool.ray_d[i]);
@@ -862,8 +840,6 @@ __device__ __forceinline__ const int* closest_queue(const PathPool& pool, int in
 template <class Col, int DIRECT, bool MEDIA, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0, PathPool pool, ProgParams P0, int in, BatchTables bt,
                                                                      AdjParams adj = AdjParams{}) {
-    __shared__ __align__(16) unsigned char s_scene_raw[BATCH ? kBatchSceneBytes : 16];
-    const DevScene* scenes = BATCH ? stage_batch_scenes(bt, s_scene_raw) : nullptr;
     constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     static_assert(!(ADJ && SPECTRAL), "the adjoint replay is RGB only");
     using CM = Colors<Col>;
@@ -885,7 +861,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
         unsigned rk = 0u, sk = 0u;   // ray-coherence keys of the spawned ray / shadow query
         if (k < n) {
             i = q[k];
-            const DevScene& S = BATCH ? scenes[pool.job[i]] : S0;
+            const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
             const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
             float4 ro = pool.ray_o[i], rd = pool.ray_d[i];
             Ray r;
@@ -1368,8 +1344,6 @@ __device__ __forceinline__ void shadow_refill(const DevScene& S, const PathPool&
 template <class Col, bool MEDIA, bool COUNT, bool BATCH, bool ADJ = false>
 __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S0, PathPool pool, ProgParams P0, BatchTables bt,
                                                                       int slot, AdjParams adj = AdjParams{}) {
-    __shared__ __align__(16) unsigned char s_scene_raw[BATCH ? kBatchSceneBytes : 16];
-    const DevScene* scenes = BATCH ? stage_batch_scenes(bt, s_scene_raw) : nullptr;
     constexpr bool SPECTRAL = sizeof(Col) == sizeof(s4);
     static_assert(!(ADJ && SPECTRAL), "the adjoint replay is RGB only");
     extern __shared__ double s_grad[];
@@ -1393,7 +1367,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     while (cur.next(k)) {
         if (k >= n) continue;
         int i = shq[k];
-        const DevScene& S = BATCH ? scenes[pool.job[i]] : S0;
+        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
         const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
         float4 so = a_o[i], sd = a_d[i], lp = a_lp[i], c = a_c[i];
         Col cc = col_ld<Col>(c);

@@ -227,11 +227,16 @@ def test_adjoint_on_the_inverse_rendering_scene_matches_forward_mode(oracle_lib)
 
 def test_adjoint_on_the_inverse_rendering_scene_matches_finite_differences():
     """Central differences (eps = 1e-3, common random numbers: the same salt and spp as the
-    adjoint) of the linearised loss, for every parameter but the IORs.  The colour slots and
-    the medium's albedo move no sampling decision, so their differences are exact to 0.5 %;
-    alpha, sigma_t and g move sampled directions and distances (noisier differences).  The
-    IOR is left out: its refracted-direction term is not propagated (documented in the C
-    header); its interface terms are checked by the forward mode and the slab."""
+    adjoint) of the linearised loss, for the parameters that move no sampling decision:
+    every material's colour (Lambert albedo, GGX F0, dielectric transmittance) and the
+    medium's albedo — 202 of the scene's 252.  For these the differences are exact, so the
+    gate is 2 % over the vector and 0.5 % per parameter.  GGX alpha, sigma_t and g move
+    sampled directions and distances: with common random numbers their differences are
+    dominated by the samples whose decisions flip (measured on this scene, the differences
+    at eps = 1e-3 and 1e-2 disagree with each other by more than their size), so they are
+    checked against the float64 forward mode above, and against differences on the box
+    scene, not here.  The IOR's refracted-direction term is not propagated (documented in
+    the C header)."""
     W = H = 64
     spp, salt = 512, 17
     rig = _c5_rig(W, H)
@@ -241,14 +246,15 @@ def test_adjoint_on_the_inverse_rendering_scene_matches_finite_differences():
         primal = rig.render(rig.theta, 256, 302)
         _, dl = adjoint.l2_loss(primal, target)
         g = rig.backward(dl, spp, salt=salt)
-        idx = [(i, k) for i, k in zip(*np.nonzero(rig.mask)) if k != abi.GRAD_IOR]
+        linear = (abi.GRAD_COLOR_R, abi.GRAD_COLOR_G, abi.GRAD_COLOR_B, abi.GRAD_MEDIUM_ALBEDO)
+        idx = [(i, k) for i, k in zip(*np.nonzero(rig.mask)) if k in linear]
+        assert len(idx) >= 200
         fd = np.array([rig.fd(dl, i, k, 1e-3, spp, salt) for i, k in idx])
         ga = np.array([g[i, k] for i, k in idx])
         rel = np.linalg.norm(ga - fd) / np.linalg.norm(fd)
         assert rel < 0.02, rel
-        linear = (abi.GRAD_COLOR_R, abi.GRAD_COLOR_G, abi.GRAD_COLOR_B, abi.GRAD_MEDIUM_ALBEDO)
         bad = [(rig.pk.material_names[i], abi.GRAD_NAMES[k], a, f) for (i, k), a, f in zip(idx, ga, fd)
-               if k in linear and abs(a - f) > 0.005 * abs(f) + 1e-3 * np.abs(fd).max()]
+               if abs(a - f) > 0.005 * abs(f) + 1e-3 * np.abs(fd).max()]
         assert not bad, bad[:10]
     finally:
         rig.close()

@@ -135,31 +135,3 @@ def test_wide_math_kernels_compile():
         assert rc == 0, log.value.decode(errors="replace")[:4000]
     finally:
         lib.nvrtcDestroyProgram(C.byref(prog))
-
-
-def test_batched_kernels_with_staged_scenes_compile():
-    """The batched kernels with every job's scene record staged in shared memory
-    (PTR_BATCH_SMEM_SCENES)."""
-    lib = _nvrtc()
-    names = [b"ptx::k_closest<false, true>", b"ptx::k_shade<ptx::f3, 2, false, true, false>",
-             b"ptx::k_shadow<ptx::f3, false, false, true, false>"]
-    opts = [b"-arch=sm_100a", b"-std=c++17", b"-fmad=false", b"-default-device", b"-DPTR_BATCH_SMEM_SCENES=1",
-            ("-I" + os.path.join(ROOT, "pathtracerglsl_b200", "csrc", "device")).encode(),
-            ("-I" + os.path.join(ROOT, "include")).encode(),
-            b"-DPTR_SPEC_MATS=7u", b"-DPTR_SPEC_LIGHTS=1u", b"-DPTR_SPEC_ENVS=1u",
-            f"-DPTR_SPEC_SHAPES={(1 << 1) | (1 << 2)}u".encode(), b"-DPTR_SPEC_NREGIONS=0",
-            b"-DPTR_SPEC_SHAPE_CODE=0ull", b"-DPTR_SPEC_TREE=0"]
-    prog = C.c_void_p()
-    assert lib.nvrtcCreateProgram(C.byref(prog), PRELUDE, b"ptr_specialize.cu", 0, None, None) == 0
-    try:
-        for n in names:
-            assert lib.nvrtcAddNameExpression(prog, n) == 0
-        arr = (C.c_char_p * len(opts))(*opts)
-        rc = lib.nvrtcCompileProgram(prog, len(opts), arr)
-        size = C.c_size_t()
-        lib.nvrtcGetProgramLogSize(prog, C.byref(size))
-        log = C.create_string_buffer(size.value)
-        lib.nvrtcGetProgramLog(prog, log)
-        assert rc == 0, log.value.decode(errors="replace")[:4000]
-    finally:
-        lib.nvrtcDestroyProgram(C.byref(prog))
