@@ -285,7 +285,7 @@ def run_reference_batch(args):
 # (dram__bytes_read.sum + dram__bytes_write.sum over the wave's launches / the wave's
 # queries).  Scaled to a launch of the timed configuration by its queries per launch; the
 # line labels it "ncu capture, scaled" (it is not measured in the timed run).
-NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 392.93}
+NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 311.37}
 # the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
 ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
 
