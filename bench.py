@@ -285,7 +285,7 @@ def run_reference_batch(args):
 # (dram__bytes_read.sum + dram__bytes_write.sum over the wave's launches / the wave's
 # queries).  Scaled to a launch of the timed configuration by its queries per launch; the
 # line labels it "ncu capture, scaled" (it is not measured in the timed run).
-NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 207.25, ("cornell", "shade"): 311.37}
+NCU_TRAFFIC_PER_QUERY = {("mesh", "closest"): 216.18, ("cornell", "shade"): 311.37}
 # the kernel each workload's roofline is reported for (its dominant traversal / shading kernel)
 ROOFLINE_KERNEL = {"mesh": "closest", "mesh-bvh": "closest", "cornell": "shade", "media": "shade"}
 
@@ -538,6 +538,7 @@ def measure_ours(args, name, rank, local, world, dist, tuning=None, cpu_leg=True
                                parallelism=f"replicas x{world}"),
                 "e2e": e2e, "roofline": roofline, "gpu_launches": launches * args.steps,
                 "clocks": clk, "rmse": rmse,
+                "error_flags": cnt["error_flags"],   # walk stack / guard errors of the counting pass (0 = none)
                 "traversal": {k: cnt[k] for k in ("blas_nodes", "triangles", "tlas_nodes", "instances",
                                                    "shadow_blas_nodes", "shadow_triangles", "shadow_tlas_nodes",
                                                    "shadow_instances")},

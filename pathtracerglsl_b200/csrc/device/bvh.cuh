@@ -210,14 +210,13 @@ __device__ __forceinline__ bool walk_wide(const DevScene& S, const uint4* nodes,
     int ptr = -1;
     unsigned g_base = 0u, g_hits = 1u << (cr.octinv & 7u), g_imask = 1u;
     for (int guard = 0; guard < 65536; guard++) {
-        if (g_hits == 0u) {
+        if (g_hits == 0u) {   // pop a group and go on to its next node in the same iteration
             if (ptr < 0) return false;
             const uint2 top = stack[ptr];
             g_base = top.x;
             g_hits = top.y & 0xFFu;
             g_imask = top.y >> 8;
             ptr--;
-            continue;
         }
         const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
         if (g_hits != 0u) {
@@ -306,6 +305,10 @@ __device__ __forceinline__ bool mesh_any(const DevScene& S, const DevMesh& m, f3
 // lane the sequence of node visits, leaf tests and tmax updates is that of the nested
 // walks, so hits (and the work tallies) are identical.  ANY: stop at the first triangle hit.
 // The walk as a resumable state: init() for one ray, then step() until it reports the end.
+// A step runs the bookkeeping transitions in line instead of spending a loop iteration on
+// each: a TLAS leaf enters its first instance and that instance's BLAS root in the same
+// step, a group pop goes straight on to the popped node, and a finished BLAS walk hands
+// over to the next instance or TLAS node at the start of the next step.
 struct InstFlat {
     f3 winv;                               // TLAS: world-ray reciprocal, node stack, leaf range
     int tstack[kBvhStack];
@@ -334,6 +337,16 @@ struct InstFlat {
     template <bool ANY>
     __device__ __forceinline__ bool step(const DevScene& S, const DevBatch& b, const DevMesh& m, int region, const Ray& r,
                                          HitRec& h, float max_dist, Work* w) {
+        if (phase == 2 && g_hits == 0u && ptr < 0) {   // the BLAS walk is done
+            if (!ANY && found) {
+                t_near = t;
+                h.t = t;
+                h.region = region;
+                h.element = inst;
+                h.prim = prim;
+            }
+            phase = li < lend ? 1 : 0;
+        }
         if (phase == 0) {
             if (tptr < 0) return false;
             const int ni = tstack[tptr--];
@@ -343,7 +356,7 @@ struct InstFlat {
             if (n0.w >= 0.0f) {
                 li = (int)n1.w;
                 lend = li + (int)n0.w;
-                phase = 1;
+                phase = 1;                 // enter its first instance in this step
             } else {
                 const int axis = (int)(-n0.w - 1.0f);
                 const int L = ni + 1, R = (int)n1.w;
@@ -354,8 +367,8 @@ struct InstFlat {
                 } else {
                     flag_error(S, kErrBvhStack);
                 }
+                return true;
             }
-            return true;
         }
         if (phase == 1) {
             if (li >= lend) { phase = 0; return true; }
@@ -373,27 +386,14 @@ struct InstFlat {
             t = t_near;
             prim = -1;
             found = false;
-            phase = 2;
-            return true;
+            phase = 2;                     // and walk its BLAS root in this step
         }
-        if (g_hits == 0u) {
-            if (ptr < 0) {                 // this instance's BLAS walk is done
-                if (!ANY && found) {
-                    t_near = t;
-                    h.t = t;
-                    h.region = region;
-                    h.element = inst;
-                    h.prim = prim;
-                }
-                phase = 1;
-                return true;
-            }
+        if (g_hits == 0u) {                // pop a group (the stack is not empty here)
             const uint2 top = stack[ptr];
             g_base = top.x;
             g_hits = top.y & 0xFFu;
             g_imask = top.y >> 8;
             ptr--;
-            return true;
         }
         const unsigned child = cw_next_child(g_hits, g_base, g_imask, cr.octinv);
         if (g_hits != 0u) {
