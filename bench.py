@@ -789,6 +789,15 @@ def measure_adjoint(args, rank, local, world, dist, cpu_leg=True):
     eng = CudaEngine(local)
     eng.register_scene(packed)
     eng.load_renderer(renderer)
+    # per-scene kernels for the forward walk and (compiled at the first backward pass, in
+    # the warm-up) the replay, untimed
+    kernels = "generic (precompiled, table-driven)"
+    if not args.generic:
+        from pathtracerglsl_b200.engine import EngineError
+        try:
+            kernels = f"specialised for this scene x strategy (NVRTC, {eng.specialize():.1f} s compile, untimed)"
+        except EngineError as e:
+            kernels = f"generic: specialisation unavailable ({e})"
     theta = adjoint.param_table(packed)
     mask = adjoint.live_mask(packed)
     rng = np.random.RandomState(11)
@@ -875,7 +884,7 @@ def measure_adjoint(args, rank, local, world, dist, cpu_leg=True):
                                        "GGX alpha / dielectric IOR) + one grey-medium sphere (sigma_t 2, albedo 0.9, g 0.6); "
                                        "loss = L2 to a target at seeded +-10 % parameters; path-replay adjoint",
                            "width": w, "height": h, "spp_primal": spp_p, "spp_adjoint": spp_a, "max_depth": 8,
-                           "parameters": int(mask.sum()), "color": "rgb",
+                           "parameters": int(mask.sum()), "color": "rgb", "kernels": kernels,
                            "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
                            "step": "one adjoint pass (forward walk + replay + float64 gradient scatter) at 16 spp"},
                 "forward": {"value": samples / (fwd_ms / 1000.0), "unit": "samples/s", "ms_per_step": fwd_ms / args.steps,

@@ -36,6 +36,8 @@ struct SpecKernels {
     const void* closest = nullptr;
     const void* shade = nullptr;
     const void* shadow = nullptr;
+    const void* shade_adj = nullptr;    // the adjoint replay's shading and shadow kernels
+    const void* shadow_adj = nullptr;   // (compiled at the first ptr_backward)
 };
 
 struct ptr_ctx {
@@ -428,9 +430,17 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     const size_t smem = sizeof(double) * PTR_GRAD_SLOTS * (size_t)S.n_materials;
     const BatchTables nob{};
     const bool media = s->has_media != 0;
+    // the per-scene replay kernels (ptr_specialize, then the first ptr_backward), if any
+    const SpecKernels* sk = (p->spec.scene_id == s->id && p->spec.shade_adj) ? &p->spec : nullptr;
     L(k_generate<true>, 0, S, pool, p->fp_dev, adj);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
+        if (sk) {
+            L.raw(sk->closest, 0, S, pool, in, nob);
+            L.raw(sk->shade_adj, smem, S, pool, P, in, nob, adj);
+            if (P.direct != PTR_DIRECT_NONE) L.raw(sk->shadow_adj, smem, S, pool, P, nob, 0, adj);
+            continue;
+        }
         L(k_closest<false, false>, 0, S, pool, in, nob);
         switch (P.direct * 2 + (media ? 1 : 0)) {
             case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, false, true>, smem, S, pool, P, in, nob, adj); break;
@@ -1254,6 +1264,7 @@ struct Census {
     int nregions = 0;
     unsigned long long shape_code = 0;
     bool tree = false, media = false, spectral = false, batch = false;
+    bool adj = false;                  // the replay's kernels (ADJ = true) instead of the forward's
     int direct = 0;
 };
 Census census_of(const ptr_program* p, const ptr_scene* sc) {
@@ -1299,7 +1310,8 @@ std::vector<std::string> census_options(const Census& c) {
 std::string census_key(const Census& c) {
     std::string k;
     for (const auto& o : census_options(c)) k += o + "\n";
-    return k + std::to_string(c.direct) + (c.media ? "m" : "-") + (c.spectral ? "s" : "-") + (c.batch ? "b" : "-");
+    return k + std::to_string(c.direct) + (c.media ? "m" : "-") + (c.spectral ? "s" : "-") + (c.batch ? "b" : "-") +
+           (c.adj ? "a" : "-");
 }
 // Compile (or fetch) the closest-hit, shading and shadow kernels for a census.  Modules are
 // cached by census for the process, so equal scenes (and equal mixes) share one module.
@@ -1313,9 +1325,10 @@ int spec_compile(ptr_ctx* ctx, const Census& c, SpecModule& out, bool& compiled)
     const char* md = c.media ? "true" : "false";
     const char* bt = c.batch ? "true" : "false";
     const std::string n_closest = std::string("ptx::k_closest<false, ") + bt + ">";
+    const char* adj = c.adj ? "true" : "false";
     const std::string n_shade = std::string("ptx::k_shade<") + col + ", " + std::to_string(c.direct) + ", " + md +
-                                ", " + bt + ", false>";
-    const std::string n_shadow = std::string("ptx::k_shadow<") + col + ", " + md + ", false, " + bt + ", false>";
+                                ", " + bt + ", " + adj + ">";
+    const std::string n_shadow = std::string("ptx::k_shadow<") + col + ", " + md + ", false, " + bt + ", " + adj + ">";
     const std::string dir = lib_dir();
     const char* dev_env = std::getenv("PTR_DEVICE_SRC");
     const char* inc_env = std::getenv("PTR_INCLUDE");
@@ -2042,6 +2055,16 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
     const int iters = wave_iterations(p, s);
     const long long waves = (total + cap - 1) / cap;
     const int n_sm = device_sms(ctx->device);
+    // a specialised program: the replay's kernels for the same census (NVRTC, once)
+    if (p->spec.scene_id == s->id && p->spec.shade && !p->spec.shade_adj) {
+        Census c = census_of(p, s);
+        c.adj = true;
+        SpecModule m;
+        bool compiled = false;
+        if (int rc = spec_compile(ctx, c, m, compiled)) return rc;
+        p->spec.shade_adj = m.shade;
+        p->spec.shadow_adj = m.shadow;
+    }
     const int saved_profile = p->profile_next;
     p->profile_next = 0;
     for (long long w = 0; w < waves; ++w) {
@@ -2102,6 +2125,7 @@ int ptr_specialize(ptr_program* p, ptr_scene* s, double* seconds_out) {
     SpecModule m;
     bool compiled = false;
     if (int rc = spec_compile(ctx, census_of(p, s), m, compiled)) return rc;
+    p->spec = SpecKernels{};                       // the replay's kernels follow at the first ptr_backward
     p->spec.scene_id = s->id;
     p->spec.closest = m.closest;
     p->spec.shade = m.shade;

@@ -79,3 +79,33 @@ def test_specialisation_is_cached_and_scene_bound(engine):
     engine.register_scene(pk)
     engine.reset()
     np.testing.assert_array_equal(engine.render_samples(32, 24, 2), ref)
+
+
+def test_specialised_replay_matches_generic_gradients(engine):
+    """ptr_backward of a specialised program runs the replay (ADJ) kernels compiled for the
+    same census: the forward walk is bit-identical and every gradient equals the generic
+    kernels' up to the order of the float64 atomic sums."""
+    from pathtracerglsl_b200 import adjoint
+    sc, st, (w, h, _, _) = scenes.adjoint_scene(0, n_spheres=8, width=48, height=48)
+    r, pk = Compiler().compile(sc, st)
+    engine.register_scene(pk)
+    engine.load_renderer(r)
+    engine.select_renderer(r.id)
+    engine.params = {}
+    rng = np.random.RandomState(4)
+    dl = rng.uniform(-1.0, 1.0, (h, w, 3)).astype(np.float32)
+    engine.specialize(False)
+    g_generic = engine.backward(dl, w, h, 4, salt=9)
+    engine.pin_reset_salt(9)
+    engine.reset()
+    f_generic = engine.render_samples(w, h, 4)
+    engine.specialize()
+    g_special = engine.backward(dl, w, h, 4, salt=9)
+    engine.pin_reset_salt(9)
+    engine.reset()
+    np.testing.assert_array_equal(engine.render_samples(w, h, 4), f_generic)
+    live = adjoint.live_mask(pk)
+    assert np.abs(g_generic[live]).max() > 0.0
+    scale = np.abs(g_generic).max()
+    np.testing.assert_allclose(g_special, g_generic, rtol=1e-9, atol=1e-12 * scale)
+    engine.specialize(False)

@@ -135,3 +135,36 @@ def test_wide_math_kernels_compile():
         assert rc == 0, log.value.decode(errors="replace")[:4000]
     finally:
         lib.nvrtcDestroyProgram(C.byref(prog))
+
+
+@pytest.mark.parametrize("media", ["false", "true"])
+def test_replay_kernels_compile(media):
+    """The adjoint replay's kernels (ADJ = true) for the inverse-rendering scene's census:
+    Lambert, dielectric, GGX and the null interface; one quad light; quads and spheres; 70
+    regions (too many to unroll)."""
+    lib = _nvrtc()
+    names = [b"ptx::k_closest<false, false>", f"ptx::k_shade<ptx::f3, 2, {media}, false, true>".encode(),
+             f"ptx::k_shadow<ptx::f3, {media}, false, false, true>".encode()]
+    opts = [b"-arch=sm_100a", b"-std=c++17", b"-fmad=false", b"-default-device",
+            ("-I" + os.path.join(ROOT, "pathtracerglsl_b200", "csrc", "device")).encode(),
+            ("-I" + os.path.join(ROOT, "include")).encode(),
+            b"-DPTR_SPEC_MATS=23u", b"-DPTR_SPEC_LIGHTS=1u", b"-DPTR_SPEC_ENVS=1u",
+            f"-DPTR_SPEC_SHAPES={(1 << 1) | (1 << 2)}u".encode(), b"-DPTR_SPEC_NREGIONS=0",
+            b"-DPTR_SPEC_SHAPE_CODE=0ull", b"-DPTR_SPEC_TREE=0"]
+    prog = C.c_void_p()
+    assert lib.nvrtcCreateProgram(C.byref(prog), PRELUDE, b"ptr_specialize.cu", 0, None, None) == 0
+    try:
+        for n in names:
+            assert lib.nvrtcAddNameExpression(prog, n) == 0
+        arr = (C.c_char_p * len(opts))(*opts)
+        rc = lib.nvrtcCompileProgram(prog, len(opts), arr)
+        size = C.c_size_t()
+        lib.nvrtcGetProgramLogSize(prog, C.byref(size))
+        log = C.create_string_buffer(size.value)
+        lib.nvrtcGetProgramLog(prog, log)
+        assert rc == 0, log.value.decode(errors="replace")[:4000]
+        for n in names:
+            low = C.c_char_p()
+            assert lib.nvrtcGetLoweredName(prog, n, C.byref(low)) == 0 and low.value
+    finally:
+        lib.nvrtcDestroyProgram(C.byref(prog))
