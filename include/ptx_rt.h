@@ -451,9 +451,12 @@ int ptr_update_params(ptr_scene* scene, const ptr_material* materials, int n_mat
  * (sm_100a): material models, light kinds, environment kind and region shapes the scene
  * lacks fold away, and with at most 16 regions the region loops unroll into one arm per
  * region with its intersection routine fixed, like the reference's generated arms (in
- * place of the region BVH, which returns the same hits).  Later ptr_render calls of the program with this scene use them (samples
- * are bit-identical to the generic kernels); the adjoint replay and the counting passes keep
- * the generic kernels (a batch takes ptr_specialize_batch).  Modules are cached per occupant census for the process.
+ * place of the region BVH, which returns the same hits).  Later ptr_render calls of the
+ * program with this scene use them (samples are bit-identical to the generic kernels), and
+ * so does ptr_backward's forward walk; its replay kernels (shading and shadow with the
+ * adjoint terms) are compiled for the same census at the first ptr_backward that follows.
+ * The counting passes keep the generic kernels (a batch takes ptr_specialize_batch).
+ * Modules are cached per occupant census for the process.
  * seconds_out (may be NULL): compile time (0 for a cached module).  scene = NULL returns
  * the program to the generic kernels.  PTR_E_UNSUPPORTED when NVRTC cannot be loaded. */
 int ptr_specialize(ptr_program* prog, ptr_scene* scene, double* seconds_out);
