@@ -19,6 +19,7 @@ import copy
 import numpy as np
 
 from . import abi
+from . import occupants
 
 
 def _materials(packed):
@@ -29,13 +30,16 @@ def _regions(packed):
     return (abi.Region * len(packed.regions)).from_buffer(packed.regions)
 
 
+def _color_field(m):
+    """The ptr_material field of a material's colour parameter (slots 0-2): its model's
+    registry row names it (albedo where the model differentiates no colour)."""
+    row = occupants.MATERIAL_BY_ID.get(m.model)
+    return (row.grad_color if row is not None else None) or "albedo"
+
+
 def _color(m):
     """The colour parameter of a material's model (slots 0-2)."""
-    if m.model in (abi.MAT_GGX, abi.MAT_MIRROR):
-        return m.f0
-    if m.model == abi.MAT_DIELECTRIC:
-        return m.transmittance
-    return m.albedo
+    return getattr(m, _color_field(m))
 
 
 def live_mask(packed):
@@ -45,16 +49,16 @@ def live_mask(packed):
     used = {r.material for r in regs}
     mask = np.zeros((len(mats), abi.GRAD_SLOTS), bool)
     for i, m in enumerate(mats):
-        if m.model == abi.MAT_LAMBERT and not (m.flags & abi.MATF_EMISSIVE):
-            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
-        elif m.model == abi.MAT_GGX:
-            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
-            mask[i, abi.GRAD_ALPHA] = True
-        elif m.model == abi.MAT_MIRROR:
-            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
-        elif m.model == abi.MAT_DIELECTRIC and i in used:
-            mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
-            mask[i, abi.GRAD_IOR] = True
+        row = occupants.MATERIAL_BY_ID.get(m.model)
+        # an emitter's record is a light's; a model with an IOR parameter is live only
+        # where a region uses it (the IOR is a region row)
+        if row is not None and not (m.flags & abi.MATF_EMISSIVE) and not (row.grad_ior and i not in used):
+            if row.grad_color:
+                mask[i, abi.GRAD_COLOR_R:abi.GRAD_COLOR_B + 1] = True
+            if row.grad_alpha:
+                mask[i, abi.GRAD_ALPHA] = True
+            if row.grad_ior:
+                mask[i, abi.GRAD_IOR] = True
         if m.flags & abi.MATF_MEDIUM:
             mask[i, abi.GRAD_SIGMA_T] = True
             mask[i, abi.GRAD_MEDIUM_ALBEDO] = True
@@ -93,13 +97,7 @@ def with_params(packed, table):
     for i, m in enumerate(mats):
         row = table[i]
         if mask[i, 0]:
-            col = abi.F4(*(list(row[0:3]) + [0.0]))
-            if m.model in (abi.MAT_GGX, abi.MAT_MIRROR):
-                m.f0 = col
-            elif m.model == abi.MAT_DIELECTRIC:
-                m.transmittance = col
-            else:
-                m.albedo = col
+            setattr(m, _color_field(m), abi.F4(*(list(row[0:3]) + [0.0])))
         if mask[i, abi.GRAD_ALPHA]:
             m.alpha = float(row[abi.GRAD_ALPHA])
         if mask[i, abi.GRAD_SIGMA_T]:

@@ -31,7 +31,8 @@ def build(force=False, verbose=False):
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
     units = [os.path.join(CSRC, "ptx_rt.cu")] + sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp")))
-    cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), *units, "-o", LIB + ".tmp"]
+    cmd = [NVCC, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-I", os.path.join(CSRC, "device"), *units,
+           "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

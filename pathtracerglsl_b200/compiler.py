@@ -19,6 +19,7 @@ import numpy as np
 
 from . import abi
 from . import field as medium_field
+from . import occupants
 
 # ----------------------------------------------------------------------------- diagnostics
 
@@ -144,14 +145,11 @@ def camera_basis(position, target):
 
 
 # ----------------------------------------------------------------------------- registries
-# The occupant registries this build implements (one row per occupant, like the
-# reference's MATERIAL_MODELS / LIGHT_KINDS / PRIMITIVES registries).
-MATERIAL_MODELS = {"lambert": abi.MAT_LAMBERT, "dielectric": abi.MAT_DIELECTRIC,
-                   "ggx": abi.MAT_GGX, "mirror": abi.MAT_MIRROR, "rough_dielectric": abi.MAT_ROUGH_DIELECTRIC,
-                   "none": abi.MAT_NONE}
-PRIMITIVES = {"plane": abi.SHAPE_PLANE, "sphere": abi.SHAPE_SPHERE, "quad": abi.SHAPE_QUAD,
-              "box": abi.SHAPE_BOX}
-LIGHT_KINDS = {"quad": abi.LIGHT_QUAD, "sphere": abi.LIGHT_SPHERE, "point": abi.LIGHT_POINT}
+# The occupant registries (one row per occupant, like the reference's MATERIAL_MODELS /
+# LIGHT_KINDS / PRIMITIVES registries) live in occupants.py.
+MATERIAL_MODELS = occupants.MATERIAL_MODELS
+PRIMITIVES = occupants.PRIMITIVES
+LIGHT_KINDS = occupants.LIGHT_KINDS
 DIRECT = {"none": abi.DIRECT_NONE, "nee": abi.DIRECT_NEE, "mis": abi.DIRECT_MIS}
 # meshTraversal 'bvh' / 'cwbvh'; instanceAccel 'tlas' / 'cwbvh' ('linear', the reference's
 # scan over every instance, returns the same nearest hit: it walks the binary TLAS here)
@@ -524,7 +522,7 @@ class Compiler:
             if o.get("kind") not in (None, "mesh"):
                 continue
             m = mats_src[o["material"]]
-            if m.get("sampleAsLight") is False or m.get("model") != "lambert":
+            if m.get("sampleAsLight") is False or not getattr(MATERIAL_MODELS.get(m.get("model")), "emitter", False):
                 continue
             e = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
             if max(e) <= 0.0 or (o.get("kind") is None and o["type"] not in ("sphere", "quad")):
@@ -576,7 +574,7 @@ class Compiler:
                 m = mats_src[proto["material"]]
                 if proto.get("kind") == "mesh" or proto.get("type") != "sphere":
                     continue
-                if m.get("sampleAsLight") is False or m.get("model") != "lambert":
+                if m.get("sampleAsLight") is False or not getattr(MATERIAL_MODELS.get(m.get("model")), "emitter", False):
                     continue
                 e = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
                 if max(e) <= 0.0:
@@ -717,7 +715,8 @@ class Compiler:
         albedo 0.8, emission 0, transmittance 1, f0 0.9, roughness 0.5."""
         rec = abi.Material()
         model = m["model"]
-        rec.model = MATERIAL_MODELS[model]
+        row = MATERIAL_MODELS[model]
+        rec.model = row.model
         alb = rgb(m.get("albedo"), params, [0.8, 0.8, 0.8])
         emi = rgb(m.get("emission"), params, [0.0, 0.0, 0.0])
         rec.albedo = abi.F4(*(alb + [0.0]))
@@ -727,7 +726,7 @@ class Compiler:
         rough = float(resolve(m.get("roughness"), params, 0.5))
         rec.alpha = max(1e-3, rough * rough)          # ggx.glsl:7-9 derived row
         flags = 0
-        if model == "lambert" and max(emi) > 0.0:
+        if row.emitter and max(emi) > 0.0:
             flags |= abi.MATF_EMISSIVE
         med = m.get("medium")
         if med is not None:
@@ -768,7 +767,8 @@ class Compiler:
 
     @staticmethod
     def _ior(m, params):
-        if m.get("model") in ("dielectric", "rough_dielectric"):   # the region-table ior row
+        row = MATERIAL_MODELS.get(m.get("model"))
+        if row is not None and row.ior:   # the region-table ior row
             return float(resolve(m.get("ior"), params, 1.5))
         return 1.0
 

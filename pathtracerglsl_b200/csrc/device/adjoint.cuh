@@ -20,68 +20,15 @@
 
 namespace ptx {
 
-// d log D / d alpha of the Trowbridge-Reitz distribution at half-vector cosine hz.
-__device__ __forceinline__ float mf_dlogD(float hz, float a) {
-    float t = hz * hz * (a * a - 1.0f) + 1.0f;
-    return 2.0f / a - 4.0f * a * hz * hz / t;
-}
-// d log G1 / d alpha of the separable Smith term at cosine c.
-__device__ __forceinline__ float mf_dlogG1(float c, float a) {
-    c = fabsf(c);
-    float s = sqrtf(a * a + (1.0f - a * a) * c * c);
-    return -(a * (1.0f - c * c) / s) / (c + s);
-}
-// d log f / d alpha of the GGX conductor for the pair (wi, wo) (Fresnel does not depend on alpha).
-__device__ __forceinline__ float ggx_dlog_alpha(f3 wi, f3 wo, const Hit& h, float a) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return 0.0f;
-    f3 hh = normalize(wil + wol);
-    return mf_dlogD(hh.z, a) + mf_dlogG1(wil.z, a) + mf_dlogG1(wol.z, a);
-}
-// d log F_c / d F0_c of Schlick's Fresnel F = F0 + (1 - F0) (1 - c)^5, per channel.
-__device__ __forceinline__ f3 schlick_dlog_f0(f3 f0, float c) {
-    const float s5 = m_pow(1.0f - c, 5.0f);
-    const f3 F = f0 + (f3(1.0f) - f0) * s5;
-    return f3(1.0f - s5) / vmax(F, f3(1e-20f));
-}
-// d log f_c / d F0_c of the GGX conductor for the pair (wi, wo): only Fresnel depends on F0.
-__device__ __forceinline__ f3 ggx_dlog_f0(f3 wi, f3 wo, const Hit& h, f3 f0) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return f3(0.0f);
-    f3 hh = normalize(wil + wol);
-    return schlick_dlog_f0(f0, fabsf(dot(wol, hh)));
-}
+// The surface models' own derivative terms live beside them (materials/*.cuh: nee_grad,
+// cont_grad); here are the medium's and the accumulators.
+
 // d log p_HG / d g (forward convention, hg.glsl:11-42).
 __device__ __forceinline__ float hg_dlog_g(f3 wi, f3 wo, float g) {
     float c = dot(wi, -wo);
     float d = gmax(1.0f + g * g - 2.0f * g * c, 1e-8f);
     return -2.0f * g / (1.0f - g * g) - 1.5f * (2.0f * g - 2.0f * c) / d;
 }
-// Exact unpolarised Fresnel in float64 (the derivative below differences it).
-__device__ __forceinline__ double fresnel_d(double cos_i, double eta) {
-    double sin2_t = eta * eta * (1.0 - cos_i * cos_i);
-    if (sin2_t >= 1.0) return 1.0;
-    double cos_t = sqrt(1.0 - sin2_t);
-    double rp = (cos_i - eta * cos_t) / (cos_i + eta * cos_t);
-    double rs = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
-    return 0.5 * (rp * rp + rs * rs);
-}
-// d log w / d ior of the smooth dielectric's sampled lobe, where ior is the IOR of the
-// region the interface belongs to (n_t on entry, n_i on exit).  Reflection: w = F / F_detached;
-// refraction: w = T (n_i/n_t)^2 (1-F) / (1-F)_detached.
-__device__ __forceinline__ float dielectric_dlog_ior(float cos_i, float n_i, float n_t, bool entering, bool refracted) {
-    const double eta = (double)n_i / (double)n_t;
-    const double deta = entering ? -(double)n_i / ((double)n_t * (double)n_t) : 1.0 / (double)n_t;
-    const double c = (double)fminf(fmaxf(cos_i, 1e-6f), 1.0f);
-    const double h = 1e-6 * eta;
-    const double F = fresnel_d(c, eta);
-    const double dF = (fresnel_d(c, eta + h) - fresnel_d(c, eta - h)) / (2.0 * h) * deta;
-    if (!refracted) return F > 0.0 ? (float)(dF / F) : 0.0f;
-    const double own = entering ? (double)n_t : (double)n_i;
-    const double dscale = (entering ? -2.0 : 2.0) / own;
-    return (float)(dscale - (F < 1.0 ? dF / (1.0 - F) : 0.0));
-}
-
 // Grey homogeneous medium: sigma_t and the single-scattering albedo a
 // (sigma_s = a sigma_t, sigma_a = (1 - a) sigma_t), read from channel 0.
 struct GreyMedium { float st, a; };

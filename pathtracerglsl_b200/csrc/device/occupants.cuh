@@ -1,8 +1,10 @@
-// occupants.cuh — materials, lights, environment and media of the transport loop.
+// occupants.cuh — lights, environment and media of the transport loop, and the colour
+// models every occupant reads through.
 //
-// One function family per occupant, selected by the material/light record's kind (the
-// device counterpart of the reference's generated dispatch over its registries,
-// src/compiler/generate/features/materials.ts:902-954 and lighting.ts:546-693).
+// One function family per occupant, selected by the light record's kind (the device
+// counterpart of the reference's generated dispatch over its registries,
+// src/compiler/generate/features/lighting.ts:546-693).  Surface material models live in
+// materials/, one header each, listed in materials/registry.cuh.
 #pragma once
 #include "scene.cuh"
 
@@ -72,218 +74,7 @@ template <> struct Colors<s4> {
     __device__ static s4 env_color(const DevScene& S, const Wl& w) { return spec_eval(S, S.spec_env, w); }
 };
 
-// ---- Lambert (materials/lambert/lambert.glsl:7-37) --------------------------------------
-template <class Col>
-__device__ __forceinline__ Col lambert_eval(f3 wi, f3 wo, const Hit& h, Col albedo) {
-    if (dot(wi, h.frame.n) * dot(wo, h.frame.n) <= 0.0f) return Col(0.0f);
-    return albedo * (1.0f / kPi);
-}
-template <class Col>
-__device__ __forceinline__ ISample<Col> lambert_sample(f3 wo, const Hit& h, Col albedo, float u0, float u1) {
-    f3 n = dot(wo, h.frame.n) < 0.0f ? -h.frame.n : h.frame.n;
-    float cos_theta = sqrtf(u1);
-    float sin_theta = sqrtf(gmax(0.0f, 1.0f - u1));
-    float phi = kTwoPi * u0;
-    float sp, cp;
-    sp = m_sin(phi);
-    cp = m_cos(phi);
-    ISample<Col> s;
-    s.wi = normalize(h.frame.t * (sin_theta * cp) + h.frame.b * (sin_theta * sp) + n * cos_theta);
-    s.weight = albedo;
-    s.pdf = cos_theta * (1.0f / kPi);
-    s.flags = kLobeReflection;
-    return s;
-}
-__device__ __forceinline__ float lambert_pdf(f3 wi, f3 wo, const Hit& h) {
-    float c = dot(wi, h.frame.n) * signf(dot(wo, h.frame.n));
-    return gmax(0.0f, c) * (1.0f / kPi);
-}
-
-// ---- GGX conductor + microfacet machinery (glsl/core/microfacet.glsl:22-54,
-// materials/ggx/ggx.glsl:16-64): Trowbridge-Reitz D, separable Smith G1, Heitz 2018
-// visible-normal sampling, Schlick Fresnel. ----------------------------------------------
-__device__ __forceinline__ f3 mf_to_local(const Frame& f, f3 v) { return f3(dot(v, f.t), dot(v, f.b), dot(v, f.n)); }
-__device__ __forceinline__ f3 mf_from_local(const Frame& f, f3 v) { return normalize(f.t * v.x + f.b * v.y + f.n * v.z); }
-__device__ __forceinline__ float mf_D(f3 h, float a) {
-    float t = h.z * h.z * (a * a - 1.0f) + 1.0f;
-    return a * a / (kPi * t * t);
-}
-__device__ __forceinline__ float mf_G1(f3 v, float a) {
-    float c = fabsf(v.z);
-    return 2.0f * c / (c + sqrtf(a * a + (1.0f - a * a) * c * c));
-}
-__device__ __forceinline__ f3 mf_sample_vndf(f3 wol, float a, float u0, float u1) {
-    f3 vh = normalize(f3(a * wol.x, a * wol.y, wol.z));
-    float lensq = vh.x * vh.x + vh.y * vh.y;
-    f3 T1 = lensq > 0.0f ? f3(-vh.y, vh.x, 0.0f) * (1.0f / sqrtf(lensq)) : f3(1.f, 0.f, 0.f);
-    f3 T2 = cross(vh, T1);
-    float rr = sqrtf(u0);
-    float phi = kTwoPi * u1;
-    float t1 = rr * m_cos(phi);
-    float t2 = rr * m_sin(phi);
-    float s_ = 0.5f * (1.0f + vh.z);
-    t2 = (1.0f - s_) * sqrtf(gmax(0.0f, 1.0f - t1 * t1)) + s_ * t2;
-    f3 nh = t1 * T1 + t2 * T2 + sqrtf(gmax(0.0f, 1.0f - t1 * t1 - t2 * t2)) * vh;
-    return normalize(f3(a * nh.x, a * nh.y, gmax(1e-6f, nh.z)));
-}
-template <class Col>
-__device__ __forceinline__ Col ggx_eval(f3 wi, f3 wo, const Hit& h, Col f0, float a) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return Col(0.0f);
-    f3 hh = normalize(wil + wol);
-    Col F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
-    return F * (mf_D(hh, a) * mf_G1(wil, a) * mf_G1(wol, a) / (4.0f * fabsf(wil.z) * fabsf(wol.z)));
-}
-template <class Col>
-__device__ __forceinline__ ISample<Col> ggx_sample(f3 wo, const Hit& h, Col f0, float a, float u0, float u1) {
-    f3 wol = mf_to_local(h.frame, wo);
-    float side = wol.z < 0.0f ? -1.0f : 1.0f;
-    wol = wol * side;
-    f3 hh = mf_sample_vndf(wol, a, u0, u1);
-    f3 i = -wol;
-    f3 wil = i - 2.0f * dot(hh, i) * hh;
-    ISample<Col> s;
-    if (wil.z <= 0.0f) { s.wi = wo; s.weight = Col(0.0f); s.pdf = 0.0f; s.flags = kLobeReflection; return s; }
-    Col F = schlick_fresnel(f0, fabsf(dot(wol, hh)));
-    s.weight = F * mf_G1(wil, a);
-    s.pdf = mf_G1(wol, a) * mf_D(hh, a) / (4.0f * fabsf(wol.z));
-    s.flags = kLobeReflection;
-    s.wi = mf_from_local(h.frame, wil * side);
-    return s;
-}
-__device__ __forceinline__ float ggx_pdf(f3 wi, f3 wo, const Hit& h, float a) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wil.z * wol.z <= 0.0f) return 0.0f;
-    f3 hh = normalize(wil + wol);
-    return mf_G1(wol, a) * mf_D(hh, a) / (4.0f * fabsf(wol.z));
-}
-
-// ---- smooth dielectric with the eta^2 radiance factor (dielectric.glsl:14-52) ----------
-template <class Col>
-__device__ __forceinline__ ISample<Col> dielectric_sample(f3 wo, const Hit& h, Col tint, float n_i, float n_t, float uc) {
-    float eta = n_i / n_t;
-    f3 n = h.frame.n;
-    float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
-    float F = dielectric_fresnel(cos_i, eta);
-    ISample<Col> s;
-    if (uc < F) {
-        s.wi = normalize(2.0f * cos_i * n - wo);
-        s.weight = Col(1.0f);
-        s.pdf = 0.0f;
-        s.flags = kLobeReflection | kLobeDelta;
-    } else {
-        float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
-        float cos_t = sqrtf(gmax(0.0f, 1.0f - sin2_t));
-        s.wi = normalize(-eta * wo + (eta * cos_i - cos_t) * n);
-        float radiance_scale = (n_i * n_i) / (n_t * n_t);
-        s.weight = tint * radiance_scale;
-        s.pdf = 0.0f;
-        s.flags = kLobeTransmission | kLobeDelta;
-    }
-    return s;
-}
-
-// ---- mirror: one delta lobe weighted by Schlick Fresnel (materials/mirror/mirror.glsl) ----
-template <class Col>
-__device__ __forceinline__ ISample<Col> mirror_sample(f3 wo, const Hit& h, Col f0) {
-    f3 n = h.frame.n;
-    float cos_i = clampf(dot(wo, n), 1e-6f, 1.0f);
-    ISample<Col> s;
-    s.wi = normalize(2.0f * cos_i * n - wo);
-    s.weight = schlick_fresnel(f0, cos_i);
-    s.pdf = 0.0f;
-    s.flags = kLobeReflection | kLobeDelta;
-    return s;
-}
-
-// ---- rough dielectric: the two-lobe microfacet BSDF of Walter et al. 2007 with visible-
-// normal sampling, exact Fresnel and the eta^2 radiance factor on the transmission lobe
-// (materials/rough_dielectric/rough_dielectric.glsl).  wo lies in the frame's upper
-// hemisphere (the frame faces region_from); eta = n_i / n_t; equal indices make the
-// interface a delta pass-through. ----------------------------------------------------------
-// generalised half vector of a (wi, wo) pair, faced upward; false for a degenerate pair or
-// a back-facing microfacet (shared by eval and pdf)
-__device__ __forceinline__ bool rough_half(f3 wil, f3 wol, float eta, f3& m) {
-    float etap = wil.z > 0.0f ? 1.0f : 1.0f / eta;
-    m = wil * etap + wol;
-    if (dot(m, m) <= 0.0f) return false;
-    m = normalize(m);
-    if (m.z < 0.0f) m = -m;
-    return dot(m, wil) * wil.z >= 0.0f && dot(m, wol) * wol.z >= 0.0f;
-}
-template <class Col>
-__device__ __forceinline__ Col rough_dielectric_eval(f3 wi, f3 wo, const Hit& h, Col tint, float a, float n_i, float n_t) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wol.z <= 0.0f || wil.z == 0.0f) return Col(0.0f);
-    if (n_i == n_t) return Col(0.0f);
-    float eta = n_i / n_t;
-    f3 m;
-    if (!rough_half(wil, wol, eta, m)) return Col(0.0f);
-    float cos_om = clampf(fabsf(dot(wol, m)), 1e-6f, 1.0f);
-    float F = dielectric_fresnel(cos_om, eta);
-    float DG = mf_D(m, a) * mf_G1(wol, a) * mf_G1(wil, a);
-    if (wil.z > 0.0f) return Col(1.0f) * (DG * F / (4.0f * wil.z * wol.z));
-    float denom = dot(wil, m) + dot(wol, m) * eta;
-    denom *= denom;
-    float ft = DG * (1.0f - F) * fabsf(dot(wil, m) * dot(wol, m) / (wil.z * wol.z * denom));
-    return tint * (ft * eta * eta);
-}
-__device__ __forceinline__ float rough_dielectric_pdf(f3 wi, f3 wo, const Hit& h, float a, float n_i, float n_t) {
-    f3 wil = mf_to_local(h.frame, wi), wol = mf_to_local(h.frame, wo);
-    if (wol.z <= 0.0f || wil.z == 0.0f) return 0.0f;
-    if (n_i == n_t) return 0.0f;
-    float eta = n_i / n_t;
-    f3 m;
-    if (!rough_half(wil, wol, eta, m)) return 0.0f;
-    float cos_om = clampf(fabsf(dot(wol, m)), 1e-6f, 1.0f);
-    float F = dielectric_fresnel(cos_om, eta);
-    if (wil.z > 0.0f) return F * mf_G1(wol, a) * mf_D(m, a) / (4.0f * wol.z);
-    float denom = dot(wil, m) + dot(wol, m) * eta;
-    denom *= denom;
-    return (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * fabsf(dot(wil, m)) / denom;
-}
-template <class Col>
-__device__ __forceinline__ ISample<Col> rough_dielectric_sample(f3 wo, const Hit& h, Col tint, float a, float n_i, float n_t,
-                                                                float uc, float u0, float u1) {
-    f3 wol = mf_to_local(h.frame, wo);
-    ISample<Col> s;
-    s.wi = wo;
-    s.weight = Col(0.0f);
-    s.pdf = 0.0f;
-    s.flags = kLobeReflection;
-    if (wol.z <= 0.0f) return s;
-    float eta = n_i / n_t;
-    if (n_i == n_t) {   // index-matched: the delta pass-through
-        s.wi = -wo;
-        s.weight = tint;
-        s.flags = kLobeTransmission | kLobeDelta;
-        return s;
-    }
-    f3 m = mf_sample_vndf(wol, a, u0, u1);
-    float cos_om = clampf(dot(wol, m), 1e-6f, 1.0f);
-    float F = dielectric_fresnel(cos_om, eta);
-    f3 wil;
-    if (uc < F) {
-        f3 i = -wol;
-        wil = i - 2.0f * dot(m, i) * m;
-        if (wil.z <= 0.0f) return s;
-        s.weight = Col(1.0f) * mf_G1(wil, a);
-        s.pdf = F * mf_G1(wol, a) * mf_D(m, a) / (4.0f * wol.z);
-        s.flags = kLobeReflection;
-    } else {
-        float sin2_t = eta * eta * (1.0f - cos_om * cos_om);
-        float cos_t = sqrtf(gmax(0.0f, 1.0f - sin2_t));
-        wil = normalize(-eta * wol + (eta * cos_om - cos_t) * m);
-        if (wil.z >= 0.0f) return s;
-        float denom = dot(wil, m) + dot(wol, m) * eta;
-        denom *= denom;
-        s.weight = tint * (mf_G1(wil, a) * eta * eta);
-        s.pdf = (1.0f - F) * mf_G1(wol, a) * mf_D(m, a) * cos_om / wol.z * fabsf(dot(wil, m)) / denom;
-        s.flags = kLobeTransmission;
-    }
-    s.wi = mf_from_local(h.frame, wil);
-    return s;
-}
+// ---- surface material models: one header each under materials/ (registry.cuh) ---------
 
 // ---- HG phase, forward convention (volume_scattering/hg/hg.glsl:11-42) -----------------
 __device__ __forceinline__ float hg_eval(f3 wi, f3 wo, float g) {

@@ -21,6 +21,7 @@
 #include "occupants.cuh"
 #include "bvh.cuh"
 #include "adjoint.cuh"
+#include "materials/registry.cuh"
 
 namespace ptx {
 
@@ -884,9 +885,10 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             rng.dim = rs.y;
             Col lrem(0.0f);
             GradAcc ga;
-            int sh_kind = kGradKindNone, sh_mat = 0;
-            f3 sh_dnee(0.0f);   // dlog f at the light direction of this vertex's NEE query
-            float sh_dw = 0.0f; // its scalar part (GGX alpha beside the per-channel F0 part)
+            int sh_mat = 0;
+            // the NEE query's lobe derivative: dlog f toward the light (per channel) and its
+            // scalar part (GGX alpha beside the per-channel F0 part)
+            NeeGrad sg{kGradKindNone, f3(0.0f), 0.0f};
             if constexpr (ADJ) {
                 lrem = xyz(pool.l_rem[i]);
                 ga.s = s_grad;
@@ -985,9 +987,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         if constexpr (SPECTRAL) pool.sh_pdf[i] = ls.pdf;
                                         shadow = true;
                                         if constexpr (ADJ) {
-                                            sh_kind = kGradKindPhase;
+                                            sg.kind = kGradKindPhase;
                                             sh_mat = med_mat;
-                                            sh_dnee = f3(hg_dlog_g(ls.wi, wo_med, mm.phase_g), 0.0f, 0.0f);
+                                            sg.dnee = f3(hg_dlog_g(ls.wi, wo_med, mm.phase_g), 0.0f, 0.0f);
                                         }
                                     }
                                 }
@@ -998,7 +1000,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                 if constexpr (ADJ) {   // phase continuation: w = p_HG / pdf_detached
                                     float dg = hg_dlog_g(ps.wi, wo_med, mm.phase_g);
                                     ga.scl(med_mat, PTR_GRAD_HG_G, lrem, dg);
-                                    if (shadow) sh_dnee.x -= dg;
+                                    if (shadow) sg.dnee.x -= dg;
                                 }
                                 prev_delta = false;
                                 prev_bsdf_pdf = ps.pdf;
@@ -1055,9 +1057,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                         // any event, weighted by the arrival throughput
                         if constexpr (!SPECTRAL) {
                             if (bounce == 0 && pool.aov) {
-                                f3 fact = PTR_IS_MAT(m, PTR_MAT_LAMBERT) ? ld3(m.albedo)
-                                        : (PTR_IS_MAT(m, PTR_MAT_GGX) || PTR_IS_MAT(m, PTR_MAT_MIRROR)) ? ld3(m.f0)
-                                                                                                        : ld3(m.transmittance);
+                                f3 fact = ld3(m.transmittance);
+                                auto aov = [&](auto M) { fact = decltype(M)::aov(m); };
+                                dispatch_model<false>(m.model, aov, MaterialModels{});
                                 fact = vmin(vmax(fact, f3(0.0f)), f3(1.0f));
                                 f3 nf = dot(hit.frame.n, wo) < 0.0f ? -hit.frame.n : hit.frame.n;
                                 pool.aov[2 * i] = f4(fact * thr, 0.0f);
@@ -1093,12 +1095,11 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             done = true;
                         } else {
                             const float alpha = hit.alpha >= 0.0f ? hit.alpha : m.alpha;
-                            const bool rough = PTR_IS_MAT(m, PTR_MAT_ROUGH_DIELECTRIC);
-                            const bool nondelta = PTR_IS_MAT(m, PTR_MAT_LAMBERT) || PTR_IS_MAT(m, PTR_MAT_GGX) || rough;
-                            // of the non-delta models, Lambert (folded when the build holds it alone)
-                            const bool lam = has_mat(PTR_MAT_LAMBERT) &&
-                                             ((!has_mat(PTR_MAT_GGX) && !has_mat(PTR_MAT_ROUGH_DIELECTRIC)) || m.model == PTR_MAT_LAMBERT);
+                            // light queries with sphere support (a transmissive non-delta lobe)
+                            const bool rough = model_has<IsSphereQuery>(m.model, MaterialModels{});
+                            const bool nondelta = model_has<IsNonDelta>(m.model, MaterialModels{});
                             const float n_from = ior_of(S, hit.region_from), n_to = ior_of(S, hit.region_to);
+                            const MatSite<Col> site{S, mat, m, hit, wl, alpha, n_from, n_to};
                             // light_sample_direct (light.glsl:8-28)
                             if (nee && nondelta) {
                                 float y0 = rng.next();
@@ -1110,16 +1111,17 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     f3 light_p = hit.p + ls.wi * ls.distance;
                                     Ray sr = ray_spawn(hit, ls.wi);
                                     sr.d = normalize(light_p - sr.o);
-                                    Col f = rough ? rough_dielectric_eval(ls.wi, wo, hit, CM::tint(S, mat, wl), alpha, n_from, n_to)
-                                          : lam ? lambert_eval(ls.wi, wo, hit, CM::albedo(S, mat, wl))
-                                                : ggx_eval(ls.wi, wo, hit, CM::f0(S, mat, wl), alpha);
+                                    Col f(0.0f);
+                                    float bp = 0.0f;
+                                    const bool want_pdf = mis && !(ls.flags & kLightDelta);
+                                    auto lobe = [&](auto M) {
+                                        f = decltype(M)::eval(site, ls.wi, wo);
+                                        if (want_pdf) bp = decltype(M)::pdf(site, ls.wi, wo);
+                                    };
+                                    dispatch_model<true>(m.model, lobe, MaterialModels{});
                                     float cos_i = fabsf(dot(ls.wi, hit.frame.n));
                                     float w = 1.0f;
-                                    if (mis && !(ls.flags & kLightDelta)) {
-                                        float bp = rough ? rough_dielectric_pdf(ls.wi, wo, hit, alpha, n_from, n_to)
-                                                   : lam ? lambert_pdf(ls.wi, wo, hit) : ggx_pdf(ls.wi, wo, hit, alpha);
-                                        w = power_heuristic(ls.pdf, bp);
-                                    }
+                                    if (want_pdf) w = power_heuristic(ls.pdf, bp);
                                     float maxd = length(light_p - sr.o) - kShadowBackoff;
                                     pool.sh_o[i] = f4(sr.o, maxd);
                                     pool.sh_d[i] = f4(sr.d, __int_as_float(P.max_null - nulls));
@@ -1129,14 +1131,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     shadow = true;
                                     if constexpr (ADJ) {
                                         sh_mat = mat;
-                                        if (m.model == PTR_MAT_LAMBERT) {
-                                            sh_kind = kGradKindAlbedo;
-                                            sh_dnee = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
-                                        } else if (m.model == PTR_MAT_GGX) {   // F0 (per channel) and alpha
-                                            sh_kind = kGradKindGGX;
-                                            sh_dnee = ggx_dlog_f0(ls.wi, wo, hit, ld3(m.f0));
-                                            sh_dw = hit.alpha < 0.0f ? ggx_dlog_alpha(ls.wi, wo, hit, alpha) : 0.0f;
-                                        }
+                                        auto ng = [&](auto M) { decltype(M)::nee_grad(site, ls.wi, wo, sg); };
+                                        dispatch_model<true>(m.model, ng, MaterialModels{});
                                     }
                                 }
                             }
@@ -1145,45 +1141,16 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             float u0 = rng.next();
                             float u1 = rng.next();
                             ISample<Col> bs;
-                            if (PTR_IS_MAT(m, PTR_MAT_LAMBERT)) bs = lambert_sample(wo, hit, CM::albedo(S, mat, wl), u0, u1);
-                            else if (PTR_IS_MAT(m, PTR_MAT_GGX)) bs = ggx_sample(wo, hit, CM::f0(S, mat, wl), alpha, u0, u1);
-                            else if (rough) bs = rough_dielectric_sample(wo, hit, CM::tint(S, mat, wl), alpha, n_from, n_to, uc, u0, u1);
-                            else if (PTR_IS_MAT(m, PTR_MAT_MIRROR)) bs = mirror_sample(wo, hit, CM::f0(S, mat, wl));
-                            else if (has_mat(PTR_MAT_DIELECTRIC) || has_mat(PTR_MAT_NONE))
-                                bs = dielectric_sample(wo, hit, CM::tint(S, mat, wl), n_from, n_to, uc);
-                            else bs.weight = Col(0.0f);   // unreachable in a build that holds the scene's models
+                            bs.weight = Col(0.0f);   // stays black only in a build without the scene's models
+                            auto cont = [&](auto M) { bs = decltype(M)::sample(site, wo, uc, u0, u1); };
+                            dispatch_model<false>(m.model, cont, MaterialModels{});
                             if (spectrum_is_black(bs.weight)) {
                                 done = true;
                             } else {
                                 thr = thr * bs.weight;
                                 if constexpr (ADJ) {   // the continuation lobe: d log w_cont
-                                    if (m.model == PTR_MAT_LAMBERT) {
-                                        f3 dlog = f3(1.0f) / vmax(ld3(m.albedo), f3(1e-20f));
-                                        ga.vec(mat, PTR_GRAD_ALBEDO_R, lrem, dlog);
-                                        if (shadow) sh_dnee = sh_dnee - dlog;
-                                    } else if (m.model == PTR_MAT_GGX) {
-                                        f3 dF = ggx_dlog_f0(bs.wi, wo, hit, ld3(m.f0));
-                                        ga.vec(mat, PTR_GRAD_COLOR_R, lrem, dF);
-                                        if (shadow) sh_dnee = sh_dnee - dF;
-                                        if (hit.alpha < 0.0f) {
-                                            float da = ggx_dlog_alpha(bs.wi, wo, hit, alpha);
-                                            ga.scl(mat, PTR_GRAD_ALPHA, lrem, da);
-                                            if (shadow) sh_dw -= da;
-                                        }
-                                    } else if (m.model == PTR_MAT_MIRROR) {   // w = Schlick F(F0, cos_i)
-                                        float ci = clampf(dot(wo, hit.frame.n), 1e-6f, 1.0f);
-                                        ga.vec(mat, PTR_GRAD_COLOR_R, lrem, schlick_dlog_f0(ld3(m.f0), ci));
-                                    } else if (m.model == PTR_MAT_DIELECTRIC) {
-                                        if (bs.flags & kLobeTransmission)   // w = T (n_i / n_t)^2: d log w / d T = 1 / T
-                                            ga.vec(mat, PTR_GRAD_COLOR_R, lrem, f3(1.0f) / vmax(ld3(m.transmittance), f3(1e-20f)));
-                                        const bool entering = hit.region_to == hit.region_owner;
-                                        if (entering || hit.region_from == hit.region_owner) {
-                                            float ci = dot(wo, hit.frame.n);
-                                            float d = dielectric_dlog_ior(ci, ior_of(S, hit.region_from), ior_of(S, hit.region_to),
-                                                                          entering, (bs.flags & kLobeTransmission) != 0u);
-                                            ga.scl(mat, PTR_GRAD_IOR, lrem, d);
-                                        }
-                                    }
+                                    auto cg = [&](auto M) { decltype(M)::cont_grad(site, bs, wo, ga, lrem, shadow, sg); };
+                                    dispatch_model<false>(m.model, cg, MaterialModels{});
                                 }
                                 prev_delta = (bs.flags & kLobeDelta) != 0u;
                                 prev_bsdf_pdf = bs.pdf;
@@ -1227,8 +1194,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
             if constexpr (ADJ) {
                 pool.l_rem[i] = f4(lrem, 0.0f);
                 if (shadow) {
-                    pool.sh_g[i] = f4(sh_dnee, sh_dw);
-                    pool.sh_gm[i] = sh_mat | (sh_kind << 16);
+                    pool.sh_g[i] = f4(sg.dnee, sg.dw);
+                    pool.sh_gm[i] = sh_mat | (sg.kind << 16);
                 }
             }
             if (alive) {
