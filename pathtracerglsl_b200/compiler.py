@@ -479,44 +479,21 @@ class Compiler:
             rec.kind = LIGHT_KINDS[kind]
             rec.radiance = abi.F4(*(e + [0.0]))
             rec.region = -1
-            if kind == "quad":
-                corner, e1, e2 = l["corner"], l["edge1"], l["edge2"]
-                c = _cross(e1, e2)
-                area = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
-                nrm = [c[0] / area, c[1] / area, c[2] / area]
-                vals = list(corner) + list(e1) + list(e2) + nrm + [area]
-                rec.p = (abi.C.c_float * 16)(*vals)
+            row = occupants.LIGHT_KIND_ROWS[kind]
+            vals, region_p, geom = row.record(l)
+            rec.p = (abi.C.c_float * 16)(*vals)
+            if row.region_shape is not None:
                 materials.append(self._light_material(e))
                 spec_src.append(("light", l.get("emission", 1.0)))
                 reg = abi.Region()
-                reg.shape = abi.SHAPE_QUAD
-                reg.thin = 1
+                reg.shape = row.region_shape
+                reg.thin = row.thin
                 reg.material = len(materials) - 1
                 reg.ior = 1.0
-                reg.p = (abi.C.c_float * 15)(*(list(corner) + list(e1) + list(e2) + nrm))
+                reg.p = (abi.C.c_float * 15)(*region_p)
                 rec.region = len(regions)
                 regions.append(reg)
                 region_names.append(f"light_{li}")
-                geom = area
-            elif kind == "sphere":
-                center = l.get("position", l.get("center"))
-                rad = l["radius"]
-                rec.p = (abi.C.c_float * 16)(*(list(center) + [rad]))
-                materials.append(self._light_material(e))
-                spec_src.append(("light", l.get("emission", 1.0)))
-                reg = abi.Region()
-                reg.shape = abi.SHAPE_SPHERE
-                reg.thin = 0
-                reg.material = len(materials) - 1
-                reg.ior = 1.0
-                reg.p = (abi.C.c_float * 15)(*(list(center) + [rad]))
-                rec.region = len(regions)
-                regions.append(reg)
-                region_names.append(f"light_{li}")
-                geom = float(rad)
-            else:   # point: delta, registry entry only
-                rec.p = (abi.C.c_float * 16)(*list(l["position"]))
-                geom = None
             lights.append((rec, kind, e, geom, l.get("emission", 1.0)))
         for i, o in enumerate(scene.get("objects", [])):
             if o.get("kind") not in (None, "mesh"):

@@ -56,10 +56,7 @@ __host__ __device__ constexpr bool has_mat(int m) { return ((PTR_SPEC_MATS) >> m
 __host__ __device__ constexpr bool has_light(int k) { return ((PTR_SPEC_LIGHTS) >> k) & 1u; }
 __host__ __device__ constexpr bool has_env(int k) { return ((PTR_SPEC_ENVS) >> k) & 1u; }
 __host__ __device__ constexpr bool has_shape(int k) { return ((PTR_SPEC_SHAPES) >> k) & 1u; }
-// kind k present, and the only one of the four light kinds / of the surface models
-__host__ __device__ constexpr bool only_light(int k) { return ((PTR_SPEC_LIGHTS) & 15u) == (1u << k); }
-#define PTR_IS_LIGHT(l, K) (has_light(K) && (only_light(K) || (l).kind == (K)))
-#define PTR_IS_MAT(m, M) (has_mat(M) && (m).model == (M))
+// (material models and light kinds are dispatched through their registries, occupant.cuh)
 #if PTR_SPEC_NREGIONS > 0
 static_assert(PTR_SPEC_NREGIONS <= 16, "the shape code holds 16 regions");
 // region k's PTR_SHAPE_* in bits [4k, 4k + 4) of PTR_SPEC_SHAPE_CODE

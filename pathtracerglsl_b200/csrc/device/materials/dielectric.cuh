@@ -56,7 +56,7 @@ __device__ __forceinline__ float dielectric_dlog_ior(float cos_i, float n_i, flo
 }
 
 struct Dielectric : MaterialModel {
-    static constexpr int kModel = PTR_MAT_DIELECTRIC;
+    static constexpr int kId = PTR_MAT_DIELECTRIC;
     template <class Col>
     __device__ static ISample<Col> sample(const MatSite<Col>& s, f3 wo, float uc, float, float) {
         return dielectric_sample(wo, s.hit, Colors<Col>::tint(s.S, s.mat, s.wl), s.n_from, s.n_to, uc);

@@ -53,7 +53,7 @@ __device__ __forceinline__ f3 ggx_dlog_f0(f3 wi, f3 wo, const Hit& h, f3 f0) {
 }
 
 struct GGX : MaterialModel {
-    static constexpr int kModel = PTR_MAT_GGX;
+    static constexpr int kId = PTR_MAT_GGX;
     static constexpr bool kNonDelta = true;
     __device__ static f3 aov(const ptr_material& m) { return ld3(m.f0); }
     template <class Col>

@@ -33,7 +33,7 @@ __device__ __forceinline__ float lambert_pdf(f3 wi, f3 wo, const Hit& h) {
 }
 
 struct Lambert : MaterialModel {
-    static constexpr int kModel = PTR_MAT_LAMBERT;
+    static constexpr int kId = PTR_MAT_LAMBERT;
     static constexpr bool kNonDelta = true;
     __device__ static f3 aov(const ptr_material& m) { return ld3(m.albedo); }
     template <class Col>

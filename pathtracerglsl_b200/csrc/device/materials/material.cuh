@@ -4,9 +4,9 @@
 // MaterialModel, plus one line in registry.cuh (the device counterpart of the reference's
 // MATERIAL_MODELS registry, src/components/materials/index.ts, and of its generated dispatch
 // over it, src/compiler/generate/features/materials.ts:902-954).  The per-scene kernels
-// pick models up through the census mask (has_mat(kModel)): absent models fold away.
+// pick models up through the census mask (has_mat(kId)): absent models fold away.
 //
-//   kModel        its ptr_material.model value (PTR_MAT_*, a C ABI constant)
+//   kId           its ptr_material.model value (PTR_MAT_*, a C ABI constant)
 //   kNonDelta     it has a non-delta lobe: NEE and MIS evaluate eval() / pdf() toward lights
 //   kSphereQuery  light selection queries a sphere of directions around the point (a
 //                 transmissive non-delta lobe sees lights on both sides)
@@ -18,6 +18,7 @@
 #pragma once
 #include "occupants.cuh"
 #include "adjoint.cuh"
+#include "occupant.cuh"
 
 namespace ptx {
 
@@ -49,48 +50,10 @@ struct MaterialModel {
     __device__ static void cont_grad(const MatSite<f3>&, const ISample<f3>&, f3, const GradAcc&, f3, bool, NeeGrad&) {}
 };
 
-template <class... M> struct ModelList {};
-
-// A model takes part in a dispatch when the build holds it and, for a non-delta dispatch,
-// when it has a non-delta lobe.
-template <bool NONDELTA, class M>
-__host__ __device__ constexpr bool model_present() { return has_mat(M::kModel) && (!NONDELTA || M::kNonDelta); }
-template <bool NONDELTA, class... M>
-__host__ __device__ constexpr bool any_present(ModelList<M...>) { return (false || ... || model_present<NONDELTA, M>()); }
-
-// Calls f(M{}) for the registered model M of `model`.  Models the build lacks are not
-// instantiated; the last present model in registry order takes whatever was not matched
-// before it without a comparison (the final else of a generated if-chain), so a build
-// holding one model calls it directly.  False when the build holds no candidate.
-template <bool NONDELTA, class F>
-__device__ __forceinline__ bool dispatch_model(int, F&, ModelList<>) { return false; }
-template <bool NONDELTA, class F, class M0, class... Ms>
-__device__ __forceinline__ bool dispatch_model(int model, F& f, ModelList<M0, Ms...>) {
-    if constexpr (model_present<NONDELTA, M0>()) {
-        if constexpr (!any_present<NONDELTA>(ModelList<Ms...>{})) {
-            f(M0{});
-            return true;
-        } else {
-            if (model == M0::kModel) {
-                f(M0{});
-                return true;
-            }
-        }
-    }
-    return dispatch_model<NONDELTA>(model, f, ModelList<Ms...>{});
-}
-
-// True when `model` is a present model whose trait P holds (compared only where needed).
-template <template <class> class P>
-__device__ __forceinline__ bool model_has(int, ModelList<>) { return false; }
-template <template <class> class P, class M0, class... Ms>
-__device__ __forceinline__ bool model_has(int model, ModelList<M0, Ms...>) {
-    if constexpr (has_mat(M0::kModel) && P<M0>::value) {
-        if (model == M0::kModel) return true;
-    }
-    return model_has<P>(model, ModelList<Ms...>{});
-}
-template <class M> struct IsNonDelta { static constexpr bool value = M::kNonDelta; };
-template <class M> struct IsSphereQuery { static constexpr bool value = M::kSphereQuery; };
+// Family predicates of material dispatches (occupant.cuh): the build holds the model, and
+// it has a non-delta lobe / queries lights over the sphere.
+template <class M> struct MatPresent { static constexpr bool value = has_mat(M::kId); };
+template <class M> struct MatNonDelta { static constexpr bool value = has_mat(M::kId) && M::kNonDelta; };
+template <class M> struct MatSphereQuery { static constexpr bool value = has_mat(M::kId) && M::kSphereQuery; };
 
 }  // namespace ptx

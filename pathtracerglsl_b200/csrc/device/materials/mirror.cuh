@@ -18,7 +18,7 @@ __device__ __forceinline__ ISample<Col> mirror_sample(f3 wo, const Hit& h, Col f
 }
 
 struct Mirror : MaterialModel {
-    static constexpr int kModel = PTR_MAT_MIRROR;
+    static constexpr int kId = PTR_MAT_MIRROR;
     __device__ static f3 aov(const ptr_material& m) { return ld3(m.f0); }
     template <class Col>
     __device__ static ISample<Col> sample(const MatSite<Col>& s, f3 wo, float, float, float) {

@@ -8,7 +8,7 @@
 namespace ptx {
 
 struct Null : MaterialModel {
-    static constexpr int kModel = PTR_MAT_NONE;
+    static constexpr int kId = PTR_MAT_NONE;
     template <class Col>
     __device__ static ISample<Col> sample(const MatSite<Col>& s, f3 wo, float uc, float, float) {
         return dielectric_sample(wo, s.hit, Colors<Col>::tint(s.S, s.mat, s.wl), s.n_from, s.n_to, uc);

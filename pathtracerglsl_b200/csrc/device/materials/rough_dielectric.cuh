@@ -94,7 +94,7 @@ __device__ __forceinline__ ISample<Col> rough_dielectric_sample(f3 wo, const Hit
 }
 
 struct RoughDielectric : MaterialModel {
-    static constexpr int kModel = PTR_MAT_ROUGH_DIELECTRIC;
+    static constexpr int kId = PTR_MAT_ROUGH_DIELECTRIC;
     static constexpr bool kNonDelta = true;
     static constexpr bool kSphereQuery = true;
     template <class Col>

@@ -7,11 +7,10 @@
 // materials/, one header each, listed in materials/registry.cuh.
 #pragma once
 #include "scene.cuh"
+#include "sample.cuh"
+#include "lights/registry.cuh"
 
 namespace ptx {
-
-template <class Col = f3> struct ISample { f3 wi; Col weight; float pdf; uint32_t flags; };
-template <class Col = f3> struct LightSample { f3 wi; float distance; Col radiance; float pdf; uint32_t flags; int light_id; };
 
 // ---- colour models ---------------------------------------------------------------------
 // RGB reads the material/light records' rgb directly; the spectral model evaluates the
@@ -239,122 +238,28 @@ __device__ __forceinline__ LightSample<Col> env_sample(const DevScene& S, float 
     return ls;
 }
 
-// ---- lights: quad (area -> solid angle), sphere (visible cone), point (delta), mesh ------
-// (lights/quad/quad.glsl:14-41, lights/sphere/sphere.glsl:21-71, lights/point/point.glsl,
-// lights/mesh/mesh.glsl:18-75)
-__device__ __forceinline__ float sphere_omc_max(float r, float dc2) {
-    float sin2_max = r * r / dc2;
-    return sin2_max / (1.0f + sqrtf(gmax(0.0f, 1.0f - sin2_max)));
-}
-// Mesh light point (lights/mesh/mesh.glsl:18-42): the smallest triangle whose cumulative
-// area exceeds x0 (a zero-area triangle is never picked), x0 rescaled within its span, a
-// uniform point by the square-root map; n is the unit winding normal cross(b-a, c-a),
-// NaN for a triangle degenerate in float32.
-__device__ __noinline__ f3 mesh_light_point(const DevScene& S, const ptr_light& l, float x0, float x1, f3& n) {
-    const DevMesh& m = S.meshes[(int)l.p[0]];
-    const float* cdf = m.light_cdf;
-    int lo = 0, hi = m.n_tris - 1;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(cdf + mid) <= x0) lo = mid + 1;
-        else hi = mid;
-    }
-    float c0 = lo > 0 ? __ldg(cdf + lo - 1) : 0.0f;
-    float c1 = __ldg(cdf + lo);
-    float xr = clampf((x0 - c0) / gmax(c1 - c0, 1.0e-12f), 0.0f, 0.9999999f);
-    f3 a = xyz(__ldg(m.light_tri + 3 * lo)), b = xyz(__ldg(m.light_tri + 3 * lo + 1)), c = xyz(__ldg(m.light_tri + 3 * lo + 2));
-    float su = sqrtf(xr);
-    n = normalize(cross(b - a, c - a));
-    return a * (1.0f - su) + b * (su * (1.0f - x1)) + c * (su * x1);
-}
+// ---- lights: one header per kind under lights/ (registry.cuh) ----------------------------
+// One light of the roster: a direction toward it, its distance, radiance and density.
 template <class Col>
 __device__ LightSample<Col> light_sample_one(const DevScene& S, const ptr_light& l, Col le, f3 p, float x0, float x1) {
-    LightSample<Col> ls;
+    LightSample<Col> ls;   // a kind the build lacks samples nothing
+    ls.wi = f3(0.f, 1.f, 0.f);
+    ls.distance = 1.0f;
     ls.radiance = le;
+    ls.pdf = 0.0f;
     ls.flags = 0u;
     ls.light_id = -1;
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_MESH)) {   // no distance falloff; one-sided
-        f3 n;
-        f3 q = mesh_light_point(S, l, x0, x1, n);
-        f3 dd = q - p;
-        float d2 = dot(dd, dd);
-        ls.wi = dd * (1.0f / sqrtf(d2));
-        ls.distance = sqrtf(d2);
-        float cos_l = dot(n, -ls.wi);
-        if (!(cos_l > 0.0f)) { ls.pdf = 0.0f; return ls; }
-        ls.pdf = d2 / (l.p[12] * cos_l);
-        return ls;
-    }
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
-        f3 q = ld3(l.p) + x0 * ld3(l.p + 3) + x1 * ld3(l.p + 6);
-        f3 dd = q - p;
-        float d2 = dot(dd, dd);
-        ls.wi = dd * (1.0f / sqrtf(d2));
-        ls.distance = sqrtf(d2);
-        float cos_l = dot(ld3(l.p + 9), -ls.wi);
-        if (cos_l <= 0.0f) { ls.pdf = 0.0f; return ls; }
-        ls.pdf = d2 / (l.p[12] * cos_l);
-        return ls;
-    }
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_SPHERE)) {
-        f3 to_c = ld3(l.p) - p;
-        float r = l.p[3];
-        float dc2 = dot(to_c, to_c);
-        if (dc2 <= r * r) { ls.wi = f3(0.f, 1.f, 0.f); ls.distance = 1.0f; ls.pdf = 0.0f; return ls; }
-        float omc = sphere_omc_max(r, dc2);
-        float w_t = x0 * omc;
-        float cos_t = 1.0f - w_t;
-        float sin_t = sqrtf(gmax(0.0f, w_t * (2.0f - w_t)));
-        float phi = kTwoPi * x1;
-        f3 w = to_c * (1.0f / sqrtf(dc2));
-        f3 t, b;
-        build_basis(w, t, b);
-        ls.wi = normalize(t * (sin_t * m_cos(phi)) + b * (sin_t * m_sin(phi)) + w * cos_t);
-        ls.pdf = 1.0f / (kTwoPi * omc);
-        float proj = dot(to_c, ls.wi);
-        f3 perp = to_c - proj * ls.wi;
-        float disc = gmax(0.0f, r * r - dot(perp, perp));
-        ls.distance = (dc2 - r * r) / (proj + sqrtf(disc));
-        return ls;
-    }
-    if (!has_light(PTR_LIGHT_POINT)) {   // unreachable in a build that holds the scene's kinds
-        ls.wi = f3(0.f, 1.f, 0.f);
-        ls.distance = 1.0f;
-        ls.pdf = 0.0f;
-        return ls;
-    }
-    f3 dd = ld3(l.p) - p;
-    float d2 = dot(dd, dd);
-    ls.wi = dd * (1.0f / sqrtf(d2));
-    ls.distance = sqrtf(d2);
-    ls.radiance = le / d2;
-    ls.pdf = 1.0f;
-    ls.flags = kLightDelta;
+    auto one = [&](auto K) { ls = decltype(K)::template sample<Col>(S, l, le, p, x0, x1); };
+    dispatch_light<LightPresent>(l.kind, one);
     return ls;
 }
-// light_n: the hit's geometric normal (mesh lights; mesh.glsl:70-75: uniform area over the
-// whole mesh makes the density d^2 / (A cos_l) whichever triangle was hit)
+// The solid-angle density of an area light's point light_p (normal light_n: the hit's
+// geometric normal) along wi from p; 0 for a delta light.
 __device__ __forceinline__ float light_pdf_one(const ptr_light& l, f3 p, f3 light_p, f3 light_n, f3 wi) {
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_MESH)) {
-        float cos_l = dot(light_n, -wi);
-        if (cos_l <= 0.0f) return 0.0f;
-        f3 dd = light_p - p;
-        return dot(dd, dd) / (l.p[12] * cos_l);
-    }
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_QUAD)) {
-        float cos_l = dot(ld3(l.p + 9), -wi);
-        if (cos_l <= 0.0f) return 0.0f;
-        f3 dd = light_p - p;
-        return dot(dd, dd) / (l.p[12] * cos_l);
-    }
-    if (PTR_IS_LIGHT(l, PTR_LIGHT_SPHERE)) {
-        f3 to_c = ld3(l.p) - p;
-        float dc2 = dot(to_c, to_c);
-        float r = l.p[3];
-        if (dc2 <= r * r) return 0.0f;
-        return 1.0f / (kTwoPi * sphere_omc_max(r, dc2));
-    }
-    return 0.0f;
+    float pdf = 0.0f;
+    auto one = [&](auto K) { pdf = decltype(K)::pdf(l, p, light_p, light_n, wi); };
+    dispatch_light<LightArea>(l.kind, one);
+    return pdf;
 }
 // ---- light-tree selection (accel/light_tree/light_tree.glsl:28-77; the walk pair of
 // features/lighting.ts:767-824) ----------------------------------------------------------
@@ -765,25 +670,12 @@ __device__ __forceinline__ bool equiangular_site(const DevScene& S, int med_mat,
     const float sel = S.n_lights == 1 ? 1.0f : l.select_pdf;
     f3 pos, nl(0.0f);
     float pdf_area = 1.0f;
-    const bool area = l.kind != PTR_LIGHT_POINT;
+    const bool area = light_in<LightArea>(l.kind);
     if (area) {
         float y0 = rng.next();
         float y1 = rng.next();
-        if (l.kind == PTR_LIGHT_QUAD) {
-            pos = ld3(l.p) + y0 * ld3(l.p + 3) + y1 * ld3(l.p + 6);
-            nl = ld3(l.p + 9);
-            pdf_area = 1.0f / l.p[12];
-        } else if (has_light(PTR_LIGHT_MESH) && l.kind == PTR_LIGHT_MESH) {
-            pos = mesh_light_point(S, l, y0, y1, nl);
-            pdf_area = 1.0f / l.p[12];
-        } else {
-            float z = 1.0f - 2.0f * y0;
-            float rr = sqrtf(gmax(0.0f, 1.0f - z * z));
-            float phi = kTwoPi * y1;
-            nl = f3(rr * m_cos(phi), z, rr * m_sin(phi));
-            pos = ld3(l.p) + nl * l.p[3];
-            pdf_area = 1.0f / (4.0f * kPi * l.p[3] * l.p[3]);
-        }
+        auto ap = [&](auto K) { decltype(K)::area_point(S, l, y0, y1, pos, nl, pdf_area); };
+        dispatch_light<LightArea, true>(l.kind, ap);
     } else {
         pos = ld3(l.p);
     }

@@ -1059,7 +1059,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             if (bounce == 0 && pool.aov) {
                                 f3 fact = ld3(m.transmittance);
                                 auto aov = [&](auto M) { fact = decltype(M)::aov(m); };
-                                dispatch_model<false>(m.model, aov, MaterialModels{});
+                                dispatch_material<MatPresent>(m.model, aov);
                                 fact = vmin(vmax(fact, f3(0.0f)), f3(1.0f));
                                 f3 nf = dot(hit.frame.n, wo) < 0.0f ? -hit.frame.n : hit.frame.n;
                                 pool.aov[2 * i] = f4(fact * thr, 0.0f);
@@ -1096,8 +1096,8 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                         } else {
                             const float alpha = hit.alpha >= 0.0f ? hit.alpha : m.alpha;
                             // light queries with sphere support (a transmissive non-delta lobe)
-                            const bool rough = model_has<IsSphereQuery>(m.model, MaterialModels{});
-                            const bool nondelta = model_has<IsNonDelta>(m.model, MaterialModels{});
+                            const bool rough = material_in<MatSphereQuery>(m.model);
+                            const bool nondelta = material_in<MatNonDelta>(m.model);
                             const float n_from = ior_of(S, hit.region_from), n_to = ior_of(S, hit.region_to);
                             const MatSite<Col> site{S, mat, m, hit, wl, alpha, n_from, n_to};
                             // light_sample_direct (light.glsl:8-28)
@@ -1118,7 +1118,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                         f = decltype(M)::eval(site, ls.wi, wo);
                                         if (want_pdf) bp = decltype(M)::pdf(site, ls.wi, wo);
                                     };
-                                    dispatch_model<true>(m.model, lobe, MaterialModels{});
+                                    dispatch_material<MatNonDelta, true>(m.model, lobe);   // nondelta holds here
                                     float cos_i = fabsf(dot(ls.wi, hit.frame.n));
                                     float w = 1.0f;
                                     if (want_pdf) w = power_heuristic(ls.pdf, bp);
@@ -1132,7 +1132,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                                     if constexpr (ADJ) {
                                         sh_mat = mat;
                                         auto ng = [&](auto M) { decltype(M)::nee_grad(site, ls.wi, wo, sg); };
-                                        dispatch_model<true>(m.model, ng, MaterialModels{});
+                                        dispatch_material<MatNonDelta, true>(m.model, ng);
                                     }
                                 }
                             }
@@ -1143,14 +1143,14 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
                             ISample<Col> bs;
                             bs.weight = Col(0.0f);   // stays black only in a build without the scene's models
                             auto cont = [&](auto M) { bs = decltype(M)::sample(site, wo, uc, u0, u1); };
-                            dispatch_model<false>(m.model, cont, MaterialModels{});
+                            dispatch_material<MatPresent>(m.model, cont);
                             if (spectrum_is_black(bs.weight)) {
                                 done = true;
                             } else {
                                 thr = thr * bs.weight;
                                 if constexpr (ADJ) {   // the continuation lobe: d log w_cont
                                     auto cg = [&](auto M) { decltype(M)::cont_grad(site, bs, wo, ga, lrem, shadow, sg); };
-                                    dispatch_model<false>(m.model, cg, MaterialModels{});
+                                    dispatch_material<MatPresent>(m.model, cg);
                                 }
                                 prev_delta = (bs.flags & kLobeDelta) != 0u;
                                 prev_bsdf_pdf = bs.pdf;
