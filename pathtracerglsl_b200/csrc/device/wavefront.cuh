@@ -185,6 +185,35 @@ struct BatchTables {
     int capacity;
 };
 
+// The job of global path index g: the last j with offsets[j] <= g.  A batched wave's pool
+// slot i holds path base + i for the whole wave (base = pool.wave[0]), so the kernels find a
+// path's job from its slot by this search over the small, cached offsets table instead of
+// a per-path load from HBM that every scene-table read would wait for.
+__device__ __forceinline__ int job_of(const BatchTables& bt, long long g) {
+    int lo = 0, hi = bt.n_jobs - 1;   // last j with offsets[j] <= g
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (bt.offsets[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The jobs of a batched wave's slots.  A wave that lies inside one job (every wave of a
+// large job but its last) needs no search at all: its job is found once per thread.
+struct WaveJobs {
+    long long base = 0;
+    int single = 0;   // >= 0: every slot of the wave belongs to this job
+    WaveJobs() = default;
+    __device__ __forceinline__ WaveJobs(const PathPool& pool, const BatchTables& bt) {
+        base = pool.wave[0];
+        const int j = job_of(bt, base);
+        single = bt.offsets[j + 1] >= base + pool.wave[1] ? j : -1;
+    }
+    __device__ __forceinline__ int of(const BatchTables& bt, int slot) const {
+        return single >= 0 ? single : job_of(bt, base + slot);
+    }
+};
+
 constexpr unsigned kErrStack = 1u;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -618,12 +647,13 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         if (COUNT) flush_work(S0, w);
         return;
     }
+    const WaveJobs wj = BATCH ? WaveJobs(pool, bt) : WaveJobs{};
     QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
     unsigned k;
     while (cur.next(k)) {
         if (k >= n) continue;
         int i = q[k];
-        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
+        const DevScene& S = BATCH ? bt.scenes[wj.of(bt, i)] : S0;
         Ray r;
         r.o = xyz(pool.ray_o[i]);
         r.d = xyz(pool.ray_d[i]);
@@ -854,6 +884,7 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
     const bool nee = DIRECT != PTR_DIRECT_NONE;
     const bool mis = DIRECT == PTR_DIRECT_MIS;
     if (blockIdx.x == 0 && threadIdx.x == 0 && pool.fetch) pool.fetch[0] = 0u;   // the next k_closest's ticket
+    const WaveJobs wj = BATCH ? WaveJobs(pool, bt) : WaveJobs{};
     QueueCursor cur(n, pool.fetch ? pool.fetch + 3 : nullptr);
     unsigned k;
     while (cur.next(k)) {
@@ -862,8 +893,9 @@ __global__ void __launch_bounds__(256, PTR_SHADE_MIN_BLOCKS) k_shade(DevScene S0
         unsigned rk = 0u, sk = 0u;   // ray-coherence keys of the spawned ray / shadow query
         if (k < n) {
             i = q[k];
-            const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
-            const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
+            const int job = BATCH ? wj.of(bt, i) : 0;
+            const DevScene& S = BATCH ? bt.scenes[job] : S0;
+            const ProgParams& P = BATCH ? bt.progs[job] : P0;
             float4 ro = pool.ray_o[i], rd = pool.ray_d[i];
             Ray r;
             r.o = xyz(ro);
@@ -1329,13 +1361,15 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
         if (COUNT) flush_work(S0, wk);
         return;
     }
+    const WaveJobs wj = BATCH ? WaveJobs(pool, bt) : WaveJobs{};
     QueueCursor cur(n, pool.fetch ? pool.fetch + 1 + slot : nullptr);
     unsigned k;
     while (cur.next(k)) {
         if (k >= n) continue;
         int i = shq[k];
-        const DevScene& S = BATCH ? bt.scenes[pool.job[i]] : S0;
-        const ProgParams& P = BATCH ? bt.progs[pool.job[i]] : P0;
+        const int job = BATCH ? wj.of(bt, i) : 0;
+        const DevScene& S = BATCH ? bt.scenes[job] : S0;
+        const ProgParams& P = BATCH ? bt.progs[job] : P0;
         float4 so = a_o[i], sd = a_d[i], lp = a_lp[i], c = a_c[i];
         Col cc = col_ld<Col>(c);
         float cpdf = c.w;
@@ -1481,14 +1515,6 @@ __global__ void k_film(PathPool pool, const FrameParams* fp, double* sum, double
 }
 
 // ---- batched renders ------------------------------------------------------------------
-__device__ __forceinline__ int job_of(const BatchTables& bt, long long g) {
-    int lo = 0, hi = bt.n_jobs - 1;   // last j with offsets[j] <= g
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (bt.offsets[mid] <= g) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
 
 // Camera rays for one wave of the concatenated job space.
 __global__ void k_generate_batch(PathPool pool, BatchTables bt) {
@@ -1539,25 +1565,35 @@ __global__ void k_generate_batch(PathPool pool, BatchTables bt) {
     }
 }
 
-// Fold the wave's radiance into each job's film (FP64 atomics: the order of samples of
-// one pixel within a wave is not fixed, which moves the sum by float64 rounding only).
+// Fold the wave's radiance into each job's film.  Within a wave the paths of job j are the
+// contiguous range [s, e) of the concatenated index space, and one pixel's samples lie npix
+// apart in it.  The first npix paths of the range (one per pixel the wave touches) each add
+// their pixel's samples to the film in sample order, like k_film: the film is the sequential
+// FP64 sum of every pixel's samples in sample order, so a batched film equals the job's plain
+// film bit for bit, however the waves split the jobs.
 __global__ void k_film_batch(PathPool pool, BatchTables bt) {
     const long long base = pool.wave[0];
     const long long n = pool.wave[1];
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int j = pool.job[i];
+        const int j = pool.job[i];
         const BatchJob& J = bt.jobs[j];
         const long long npix = (long long)J.frame.width * J.frame.height;
-        long long pix = (base + i - bt.offsets[j]) % npix;
-        float4 L = pool.rad[i];
+        const long long off = bt.offsets[j];
+        const long long g = base + i;
+        if (g - (off > base ? off : base) >= npix) continue;   // not the first visit of its pixel in this wave
+        const long long job_end = j + 1 < bt.n_jobs ? bt.offsets[j + 1] : bt.total;
+        const long long end = job_end < base + n ? job_end : base + n;
+        const long long pix = (g - off) % npix;
         double* su = J.sum + 3 * pix;
         double* sq = J.sumsq + 3 * pix;
-        atomicAdd(su + 0, (double)L.x);
-        atomicAdd(su + 1, (double)L.y);
-        atomicAdd(su + 2, (double)L.z);
-        atomicAdd(sq + 0, (double)L.x * (double)L.x);
-        atomicAdd(sq + 1, (double)L.y * (double)L.y);
-        atomicAdd(sq + 2, (double)L.z * (double)L.z);
+        double s0 = su[0], s1 = su[1], s2 = su[2], q0 = sq[0], q1 = sq[1], q2 = sq[2];
+        for (long long k = g; k < end; k += npix) {
+            const float4 L = pool.rad[k - base];
+            s0 += (double)L.x; s1 += (double)L.y; s2 += (double)L.z;
+            q0 += (double)L.x * (double)L.x; q1 += (double)L.y * (double)L.y; q2 += (double)L.z * (double)L.z;
+        }
+        su[0] = s0; su[1] = s1; su[2] = s2;
+        sq[0] = q0; sq[1] = q1; sq[2] = q2;
     }
 }
 
