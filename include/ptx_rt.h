@@ -320,6 +320,59 @@ int ptr_abi_version(void);
 int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* desc, ptr_scene** out);
 int ptr_free_scene(ptr_scene* scene);
 
+/* ---- scene data in the reference's packed channel format (rail v2) ----------------------
+ * The reference's App packs a scene's array data into RGBA32F channels, one texel = 4
+ * floats, each tenant at the base texel the ledger assigns (planDataLayout,
+ * src/components/data/ledger.ts:121; writers src/components/data/pack.ts; executed by
+ * packSceneData, src/app/sceneData.ts:27):
+ *   vertices  one vec3 texel per vertex (mesh geometry; mesh-light world positions)
+ *   indices   one texel per triangle: its three vertex ids as exact floats, in BVH leaf order
+ *   nodes     two texels per binary BVH node: (min.xyz, A) (max.xyz, B), A >= 1 a leaf of A
+ *             items from offset B, A < 0 an internal node (axis -A-1, right child B)
+ *   records   instance placements in TLAS leaf order (frame tier: two texels, q_inv and
+ *             (t_rigid, s); params tier: one texel, the folded (centre, radius)), mesh-light
+ *             area CDFs (.x per texel)
+ * ptr_upload_scene_rails takes those channels as the App packed them (host memory, row-major
+ * texels, copied to the device once each) and uses the reference's mesh BVHs, instance
+ * TLASes and placement records in place: no re-packing and no host BVH build.  The
+ * scene description still carries the regions, materials, lights and environment, and its
+ * mesh and batch entries their roles (mesh positions/indices and batch placements may be
+ * NULL): mesh i and batch i of the description take rail slot i.  The compressed wide
+ * BVH of each mesh (meshTraversal 'cwbvh') and the wide twin of each TLAS are built from
+ * the rail data (the mesh's on the device).  Hit ids: a rail triangle or instance is its
+ * caller's index when tri_order / inst_order give it (buildBVH's and the TLAS build's leaf
+ * permutations), else its leaf index.  A mesh light samples its triangles by the rail's
+ * CDF, in leaf order as the reference does.  Every base, count, index, node link and
+ * permutation is checked before anything runs (PTR_E_INVALID). */
+typedef struct ptr_rail_mesh {         /* one geometry slot (ledger MeshSlot)            */
+    int64_t vbase, tbase, nbase;       /* vertices / indices / nodes base texels          */
+    int32_t vertex_count, tri_count;
+    int32_t node_count, pad;           /* BVH nodes (2 texels each)                       */
+    const uint32_t* tri_order;         /* caller index of each leaf triangle, or NULL     */
+    const float* tri_alpha;            /* per-triangle GGX alpha by caller index, or NULL */
+} ptr_rail_mesh;
+typedef struct ptr_rail_batch {        /* one instance batch (ledger BatchSlot)           */
+    int64_t placements_base, tlas_base;   /* records / nodes base texels                  */
+    int32_t instance_count, node_count;
+    int32_t placement_texels, pad;     /* 2: frame tier (mesh prototypes), 1: params tier (spheres) */
+    const uint32_t* inst_order;        /* caller index of each leaf placement, or NULL   */
+} ptr_rail_batch;
+typedef struct ptr_rail_mesh_light {   /* a samplable mesh emitter (ledger MeshLightSlot) */
+    int32_t mesh, pad;
+    int64_t wpos_base, cdf_base;       /* vertices / records base texels                  */
+} ptr_rail_mesh_light;
+typedef struct ptr_rails {
+    const float* vertices; int64_t vertices_texels;
+    const float* indices;  int64_t indices_texels;
+    const float* nodes;    int64_t nodes_texels;
+    const float* records;  int64_t records_texels;
+    int32_t n_meshes, n_batches, n_mesh_lights, pad;
+    const ptr_rail_mesh* meshes;
+    const ptr_rail_batch* batches;
+    const ptr_rail_mesh_light* mesh_lights;
+} ptr_rails;
+int ptr_upload_scene_rails(ptr_ctx* ctx, const ptr_scene_desc* desc, const ptr_rails* rails, ptr_scene** out);
+
 /* Program per scene x strategy (Engine.loadRenderer, Engine.ts:147). */
 int ptr_compile(ptr_ctx* ctx, const ptr_program_desc* desc, ptr_program** out);
 int ptr_free_program(ptr_program* prog);

@@ -18,6 +18,7 @@ SIGNATURES = {
     "ptr_last_error": (C.c_char_p, [C.c_void_p]),
     "ptr_upload_scene": (C.c_int, [C.c_void_p, C.POINTER(abi.SceneDesc), C.POINTER(C.c_void_p)]),
     "ptr_free_scene": (C.c_int, [C.c_void_p]),
+    "ptr_upload_scene_rails": (C.c_int, [C.c_void_p, C.POINTER(abi.SceneDesc), C.POINTER(abi.Rails), C.POINTER(C.c_void_p)]),
     "ptr_compile": (C.c_int, [C.c_void_p, C.POINTER(abi.ProgramDesc), C.POINTER(C.c_void_p)]),
     "ptr_free_program": (C.c_int, [C.c_void_p]),
     "ptr_render": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(abi.Frame)]),

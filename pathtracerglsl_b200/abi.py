@@ -73,6 +73,33 @@ class BatchDesc(C.Structure):
                 ("placements", C.POINTER(C.c_float))]
 
 
+class RailMesh(C.Structure):
+    _fields_ = [("vbase", C.c_int64), ("tbase", C.c_int64), ("nbase", C.c_int64),
+                ("vertex_count", C.c_int32), ("tri_count", C.c_int32), ("node_count", C.c_int32), ("pad", C.c_int32),
+                ("tri_order", C.POINTER(C.c_uint32)), ("tri_alpha", C.POINTER(C.c_float))]
+
+
+class RailBatch(C.Structure):
+    _fields_ = [("placements_base", C.c_int64), ("tlas_base", C.c_int64),
+                ("instance_count", C.c_int32), ("node_count", C.c_int32),
+                ("placement_texels", C.c_int32), ("pad", C.c_int32),
+                ("inst_order", C.POINTER(C.c_uint32))]
+
+
+class RailMeshLight(C.Structure):
+    _fields_ = [("mesh", C.c_int32), ("pad", C.c_int32), ("wpos_base", C.c_int64), ("cdf_base", C.c_int64)]
+
+
+class Rails(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_float)), ("vertices_texels", C.c_int64),
+                ("indices", C.POINTER(C.c_float)), ("indices_texels", C.c_int64),
+                ("nodes", C.POINTER(C.c_float)), ("nodes_texels", C.c_int64),
+                ("records", C.POINTER(C.c_float)), ("records_texels", C.c_int64),
+                ("n_meshes", C.c_int32), ("n_batches", C.c_int32), ("n_mesh_lights", C.c_int32), ("pad", C.c_int32),
+                ("meshes", C.POINTER(RailMesh)), ("batches", C.POINTER(RailBatch)),
+                ("mesh_lights", C.POINTER(RailMeshLight))]
+
+
 COLOR_RGB, COLOR_SPECTRAL = range(2)
 WAVELENGTHS_VISIBLE, WAVELENGTHS_UNIFORM = range(2)
 SPEC_GREY, SPEC_LIFTED, SPEC_BLACKBODY = range(3)
@@ -149,4 +176,4 @@ class Tuning(C.Structure):
 
 # Sizes the header documents (checked by the CPU tests).
 EXPECTED_SIZES = {"Region": 80, "Material": 128, "Light": 96, "Spectrum": 32, "SpectralMaterial": 192,
-                  "ProgramDesc": 64}
+                  "ProgramDesc": 64, "RailMesh": 56, "RailBatch": 40, "RailMeshLight": 24, "Rails": 104}

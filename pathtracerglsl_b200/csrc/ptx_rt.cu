@@ -26,6 +26,7 @@
 
 #include "device/wavefront.cuh"
 #include "device/lbvh.cuh"
+#include "device/rails.cuh"
 #include "host/accel_build.h"
 
 using namespace ptx;
@@ -543,10 +544,11 @@ int device_sms(int dev) {
 // A mesh's binary BVH and compressed wide BVH built on the device (device/lbvh.cuh) from
 // its vertex and index arrays, with the triangle records of both leaf orders.  The
 // arrays the walks read join the scene's allocations; the build's temporaries are freed.
-int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMesh& m, std::vector<double>& root,
-                      int& n_nodes, int& n_cw_nodes, int& bin_depth) {
+// The build proper over device-resident inputs: positions (3 floats per vertex), the index
+// triples and the optional per-triangle alpha, all in the caller's triangle order.
+int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const unsigned* d_idx, const float* d_alpha,
+                           int n, DevMesh& m, std::vector<double>& root, int& n_nodes, int& n_cw_nodes, int& bin_depth) {
     using namespace lbvh;
-    const int n = md.n_triangles;
     cudaStream_t st = ctx->stream;
     const int n_sm = device_sms(ctx->device);
     const int grid = n_sm * 8, block = 256;
@@ -562,9 +564,6 @@ int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMe
     auto release = [&]() { for (void* p : tmp) cudaFree(p); tmp.clear(); };
     const int total = 2 * n - 1;
     const int n_int = std::max(n - 1, 1);
-    float* d_pos = (float*)alloc(sizeof(float) * 3 * (size_t)md.n_vertices, false);
-    unsigned* d_idx = (unsigned*)alloc(sizeof(unsigned) * 3 * (size_t)n, false);
-    float* d_alpha = md.tri_alpha ? (float*)alloc(sizeof(float) * (size_t)n, false) : nullptr;
     float4* lo = (float4*)alloc(sizeof(float4) * (size_t)n, false);
     float4* hi = (float4*)alloc(sizeof(float4) * (size_t)n, false);
     int* cb = (int*)alloc(sizeof(int) * 8, false);
@@ -583,7 +582,7 @@ int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMe
     float4* bvh = (float4*)alloc(sizeof(float4) * 2 * (size_t)total, true);
     float4* tri = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
     float4* tri_w = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
-    if (!d_pos || !d_idx || (md.tri_alpha && !d_alpha) || !lo || !hi || !cb || !keys || !child || !parent || !range ||
+    if (!lo || !hi || !cb || !keys || !child || !parent || !range ||
         !arrivals || !nlo || !nhi || !ta || !tb || !counters || !wide_big || !order || !bvh || !tri || !tri_w) {
         release();
         return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc");
@@ -591,14 +590,11 @@ int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMe
     const int cb_init[8] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, (int)0x80000000, (int)0x80000000, (int)0x80000000, 0, 0};
     const unsigned cnt_init[8] = {1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
     const int2 root_task = make_int2(0, 0);   // binary node 0 (internal root, or the one leaf) -> wide node 0
-    cudaError_t e = cudaMemcpyAsync(d_pos, md.positions, sizeof(float) * 3 * (size_t)md.n_vertices, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, md.indices, sizeof(unsigned) * 3 * (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && d_alpha) e = cudaMemcpyAsync(d_alpha, md.tri_alpha, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(cb, cb_init, sizeof(cb_init), cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyAsync(cb, cb_init, sizeof(cb_init), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counters, cnt_init, sizeof(cnt_init), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ta, &root_task, sizeof(int2), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(arrivals, 0, sizeof(unsigned) * (size_t)n_int, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the host arrays' copies end before they may go
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // the small host tables are copied before the launches
     if (e != cudaSuccess) { release(); return cuda_fail(ctx, e, "scene: device BVH build"); }
     k_boxes<<<grid, block, 0, st>>>(d_pos, d_idx, n, lo, hi, cb);
     k_keys<<<grid, block, 0, st>>>(lo, hi, n, n_pad, cb, keys);
@@ -663,12 +659,308 @@ int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMe
     return PTR_OK;
 }
 
+// The device build of a mesh given in host memory (ptr_set_accel_build(PTR_BUILD_DEVICE)).
+int build_mesh_device(ptr_ctx* ctx, ptr_scene* s, const ptr_mesh_desc& md, DevMesh& m, std::vector<double>& root,
+                      int& n_nodes, int& n_cw_nodes, int& bin_depth) {
+    const int n = md.n_triangles;
+    cudaStream_t st = ctx->stream;
+    float* d_pos = nullptr;
+    unsigned* d_idx = nullptr;
+    float* d_alpha = nullptr;
+    auto release = [&]() { cudaFree(d_pos); cudaFree(d_idx); cudaFree(d_alpha); };
+    if (cudaMalloc(&d_pos, sizeof(float) * 3 * (size_t)md.n_vertices) != cudaSuccess ||
+        cudaMalloc(&d_idx, sizeof(unsigned) * 3 * (size_t)n) != cudaSuccess ||
+        (md.tri_alpha && cudaMalloc(&d_alpha, sizeof(float) * (size_t)n) != cudaSuccess)) {
+        release();
+        return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc");
+    }
+    cudaError_t e = cudaMemcpyAsync(d_pos, md.positions, sizeof(float) * 3 * (size_t)md.n_vertices, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, md.indices, sizeof(unsigned) * 3 * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && d_alpha) e = cudaMemcpyAsync(d_alpha, md.tri_alpha, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { release(); return cuda_fail(ctx, e, "scene: device BVH build"); }
+    const int rc = build_mesh_device_core(ctx, s, d_pos, d_idx, d_alpha, n, m, root, n_nodes, n_cw_nodes, bin_depth);
+    release();   // the core synchronised the stream before it returned
+    return rc;
+}
+
+// ---- scene data from the reference's packed channels (rail v2) ----------------------------
+static_assert(sizeof(ptr_rail_mesh) == 56 && sizeof(ptr_rail_batch) == 40 && sizeof(ptr_rail_mesh_light) == 24 &&
+              sizeof(ptr_rails) == 104, "rail records: the layouts the ctypes mirror declares");
+// The channels on the device: flat float4 texel arrays, copied once each.
+struct RailDev {
+    const float4* v = nullptr;
+    const float4* idx = nullptr;
+    const float4* nodes = nullptr;
+    const float4* rec = nullptr;
+};
+
+bool rail_span(int64_t base, int64_t count, int64_t total) {
+    return base >= 0 && count >= 0 && base <= total && count <= total - base;
+}
+bool exact_id(float f, int64_t bound) { return f >= 0.0f && f == std::floor(f) && (int64_t)f < bound; }
+
+// A binary BVH of the nodes channel (the bvh.ts node layout) over n_items leaf items:
+// every box finite, every leaf range inside [0, n_items), every internal node's axis in
+// 0..2 and both children after it inside the tree (so every walk moves forward and stays
+// in the region).  Returns the tree's depth, or -1.
+int rail_tree_depth(const float* nodes, int64_t nbase, int node_count, int n_items) {
+    if (node_count < 1 || (int64_t)node_count > 2 * (int64_t)n_items - 1) return -1;
+    std::vector<int> depth((size_t)node_count, 0);
+    int max_depth = 0;
+    for (int i = 0; i < node_count; ++i) {
+        const float* q = nodes + 4 * (nbase + 2 * (int64_t)i);
+        for (int k = 0; k < 8; ++k)
+            if (k != 3 && k != 7 && !std::isfinite(q[k])) return -1;
+        const float A = q[3], B = q[7];
+        if (A >= 1.0f) {
+            if (A != std::floor(A) || !exact_id(B, n_items) || (int64_t)B + (int64_t)A > n_items) return -1;
+        } else if (A == -1.0f || A == -2.0f || A == -3.0f) {
+            if (B != std::floor(B) || !(B > (float)(i + 1)) || !(B < (float)node_count)) return -1;
+            const int d = depth[(size_t)i] + 1;
+            depth[(size_t)i + 1] = std::max(depth[(size_t)i + 1], d);
+            depth[(size_t)B] = std::max(depth[(size_t)B], d);
+        } else {
+            return -1;
+        }
+        max_depth = std::max(max_depth, depth[(size_t)i]);
+    }
+    return max_depth;
+}
+
+// A permutation of [0, n), or NULL.
+bool rail_permutation(const uint32_t* order, int n) {
+    if (!order) return true;
+    std::vector<char> seen((size_t)n, 0);
+    for (int i = 0; i < n; ++i)
+        if (order[i] >= (uint32_t)n || seen[order[i]]++) return false;
+    return true;
+}
+
+// Mesh mi from its rail slot: triangles gathered into the binary walk's leaf-order records,
+// the rail's BVH nodes used in place, the wide BVH built on the device over the same
+// triangles, and (for a mesh light) its world triangles and area CDF from the rail.
+int rail_mesh(ptr_ctx* ctx, ptr_scene* s, const ptr_rails& R, const RailDev& D, int mi, bool is_light, DevMesh& m,
+              std::vector<double>& root, int& bin_depth) {
+    const ptr_rail_mesh& rm = R.meshes[mi];
+    const int V = rm.vertex_count, T = rm.tri_count, NC = rm.node_count;
+    const std::string who = "rails: mesh " + std::to_string(mi);
+    if (V <= 0 || T <= 0 || !rail_span(rm.vbase, V, R.vertices_texels) || !rail_span(rm.tbase, T, R.indices_texels) ||
+        !rail_span(rm.nbase, 2 * (int64_t)NC, R.nodes_texels))
+        return fail(ctx, PTR_E_INVALID, who + ": empty, or a region outside its channel");
+    for (int i = 0; i < V; ++i) {
+        const float* p = R.vertices + 4 * (rm.vbase + i);
+        if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return fail(ctx, PTR_E_INVALID, who + ": non-finite vertex");
+    }
+    for (int i = 0; i < T; ++i) {
+        const float* t = R.indices + 4 * (rm.tbase + i);
+        if (!exact_id(t[0], V) || !exact_id(t[1], V) || !exact_id(t[2], V)) return fail(ctx, PTR_E_INVALID, who + ": vertex id out of range");
+    }
+    if (!rail_permutation(rm.tri_order, T)) return fail(ctx, PTR_E_INVALID, who + ": tri_order is not a permutation");
+    const int depth = rail_tree_depth(R.nodes, rm.nbase, NC, T);
+    if (depth < 0) return fail(ctx, PTR_E_INVALID, who + ": malformed BVH nodes");
+    if (depth >= ptx_host::kBvhStackDepth) std::fprintf(stderr, "ptx_rt: BVH depth %d reaches the walk's stack depth\n", depth);
+    const ptr_rail_mesh_light* ml = nullptr;
+    for (int k = 0; k < R.n_mesh_lights; ++k)
+        if (R.mesh_lights[k].mesh == mi) ml = &R.mesh_lights[k];
+    if (is_light != (ml != nullptr)) return fail(ctx, PTR_E_INVALID, who + ": a mesh light needs exactly its rail light slot");
+    if (ml) {
+        if (!rail_span(ml->wpos_base, V, R.vertices_texels) || !rail_span(ml->cdf_base, T, R.records_texels))
+            return fail(ctx, PTR_E_INVALID, who + ": light tables outside their channels");
+        for (int i = 0; i < V; ++i) {
+            const float* p = R.vertices + 4 * (ml->wpos_base + i);
+            if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return fail(ctx, PTR_E_INVALID, who + ": non-finite light vertex");
+        }
+        for (int i = 0; i < T; ++i)
+            if (!std::isfinite(R.records[4 * (ml->cdf_base + i)])) return fail(ctx, PTR_E_INVALID, who + ": non-finite light CDF");
+    }
+    cudaStream_t st = ctx->stream;
+    float* d_pos = nullptr;
+    unsigned* d_idx = nullptr;
+    uint32_t* d_order = nullptr;
+    float* d_alpha = nullptr;
+    auto release = [&]() { cudaFree(d_pos); cudaFree(d_idx); cudaFree(d_order); cudaFree(d_alpha); };
+    float4* tri = nullptr;
+    if (cudaMalloc(&d_pos, sizeof(float) * 3 * (size_t)V) != cudaSuccess ||
+        cudaMalloc(&d_idx, sizeof(unsigned) * 3 * (size_t)T) != cudaSuccess ||
+        (rm.tri_order && cudaMalloc(&d_order, sizeof(uint32_t) * (size_t)T) != cudaSuccess) ||
+        (rm.tri_alpha && cudaMalloc(&d_alpha, sizeof(float) * (size_t)T) != cudaSuccess) ||
+        cudaMalloc(&tri, sizeof(float4) * 3 * (size_t)T) != cudaSuccess) {
+        if (tri) cudaFree(tri);
+        release();
+        return fail(ctx, PTR_E_NOMEM, who + ": cudaMalloc");
+    }
+    s->allocs.push_back(tri);
+    const int n_sm = device_sms(ctx->device);
+    cudaError_t e = cudaSuccess;
+    if (d_order) e = cudaMemcpyAsync(d_order, rm.tri_order, sizeof(uint32_t) * (size_t)T, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && d_alpha) e = cudaMemcpyAsync(d_alpha, rm.tri_alpha, sizeof(float) * (size_t)T, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { release(); return cuda_fail(ctx, e, who.c_str()); }
+    rails::k_positions<<<n_sm * 4, 256, 0, st>>>(D.v, rm.vbase, V, d_pos);
+    rails::k_caller_indices<<<n_sm * 4, 256, 0, st>>>(D.idx, rm.tbase, T, d_order, d_idx);
+    rails::k_leaf_tris<<<n_sm * 4, 256, 0, st>>>(d_pos, D.idx, rm.tbase, T, d_order, d_alpha, tri);
+    if ((e = cudaGetLastError()) != cudaSuccess) { release(); return cuda_fail(ctx, e, who.c_str()); }
+    // the wide BVH (meshTraversal 'cwbvh') over the same triangles, built on the device
+    DevMesh wide{};
+    std::vector<double> wide_root;
+    int wn = 0, wcw = 0, wdepth = 0;
+    int rc = build_mesh_device_core(ctx, s, d_pos, d_idx, d_alpha, T, wide, wide_root, wn, wcw, wdepth);
+    release();
+    if (rc) return rc;
+    m.tri = tri;
+    m.bvh = D.nodes + rm.nbase;
+    m.tri_w = wide.tri_w;
+    m.cwbvh = wide.cwbvh;
+    m.n_tris = T;
+    m.n_nodes = NC;
+    m.n_cw_nodes = wcw;
+    m.light_cdf = nullptr;
+    m.light_tri = nullptr;
+    if (ml) {
+        float4* lt = nullptr;
+        float* cdf = nullptr;
+        if (cudaMalloc(&lt, sizeof(float4) * 3 * (size_t)T) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, who + ": cudaMalloc");
+        s->allocs.push_back(lt);
+        if (cudaMalloc(&cdf, sizeof(float) * (size_t)T) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, who + ": cudaMalloc");
+        s->allocs.push_back(cdf);
+        rails::k_light_tris<<<n_sm * 4, 256, 0, st>>>(D.v, ml->wpos_base, D.idx, rm.tbase, T, lt);
+        rails::k_scalars<<<n_sm * 4, 256, 0, st>>>(D.rec, ml->cdf_base, T, cdf);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(ctx, e, who.c_str());
+        m.light_cdf = cdf;
+        m.light_tri = lt;
+    }
+    const float* n0 = R.nodes + 4 * rm.nbase;
+    root = {n0[0], n0[1], n0[2], n0[4], n0[5], n0[6]};
+    bin_depth = depth;
+    return PTR_OK;
+}
+
+// Batch bi from its rail slot: the TLAS nodes and (frame tier) the placement records used
+// in place, params-tier records re-strided, caller instance ids and instance lights per
+// leaf slot, and the wide TLAS twin built on the host over the same instance boxes.
+int rail_batch(ptr_ctx* ctx, ptr_scene* s, const ptr_rails& R, const RailDev& D, int bi, const ptr_batch_desc& bd,
+               const std::vector<std::vector<double>>& root_box, DevBatch& b, std::vector<double>& boxes) {
+    const ptr_rail_batch& rb = R.batches[bi];
+    const int N = rb.instance_count, NC = rb.node_count, PT = rb.placement_texels;
+    const std::string who = "rails: batch " + std::to_string(bi);
+    const bool mesh = bd.prototype_shape == PTR_SHAPE_MESH;
+    if (bd.prototype_shape != PTR_SHAPE_MESH && bd.prototype_shape != PTR_SHAPE_SPHERE)
+        return fail(ctx, PTR_E_INVALID, who + ": prototype must be a mesh or a sphere");
+    if (mesh && (bd.prototype_ref < 0 || bd.prototype_ref >= (int)root_box.size()))
+        return fail(ctx, PTR_E_INVALID, who + ": prototype mesh out of range");
+    if (N <= 0 || N != bd.n_instances || PT != (mesh ? 2 : 1) || !rail_span(rb.placements_base, (int64_t)PT * N, R.records_texels) ||
+        !rail_span(rb.tlas_base, 2 * (int64_t)NC, R.nodes_texels))
+        return fail(ctx, PTR_E_INVALID, who + ": empty, a count that differs from the description, the wrong tier, or a region outside its channel");
+    if (rail_tree_depth(R.nodes, rb.tlas_base, NC, N) < 0) return fail(ctx, PTR_E_INVALID, who + ": malformed TLAS nodes");
+    if (!rail_permutation(rb.inst_order, N)) return fail(ctx, PTR_E_INVALID, who + ": inst_order is not a permutation");
+    // the records at two texels per instance, and each leaf slot's world box
+    std::vector<float4> rec(2 * (size_t)N);
+    boxes.assign(6 * (size_t)N, 0.0);
+    for (int i = 0; i < N; ++i) {
+        const float* r = R.records + 4 * (rb.placements_base + (int64_t)PT * i);
+        for (int k = 0; k < 4 * PT; ++k)
+            if (!std::isfinite(r[k])) return fail(ctx, PTR_E_INVALID, who + ": non-finite placement");
+        double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+        if (mesh) {
+            const double qx = r[0], qy = r[1], qz = r[2], qw = r[3], tx = r[4], ty = r[5], tz = r[6], sc = r[7];
+            if (!(sc > 0.0)) return fail(ctx, PTR_E_INVALID, who + ": placement scale must be positive");
+            const std::vector<double>& rb0 = root_box[bd.prototype_ref];
+            for (int k = 0; k < 8; ++k) {   // world = rotate(conj(q), s * local - t_rigid)
+                const double x = (k & 1) ? rb0[3] : rb0[0], y = (k & 2) ? rb0[4] : rb0[1], z = (k & 4) ? rb0[5] : rb0[2];
+                const double vx = sc * x - tx, vy = sc * y - ty, vz = sc * z - tz;
+                const double cx = -qx, cy = -qy, cz = -qz;
+                const double c1x = cy * vz - cz * vy + qw * vx, c1y = cz * vx - cx * vz + qw * vy, c1z = cx * vy - cy * vx + qw * vz;
+                const double c2x = cy * c1z - cz * c1y, c2y = cz * c1x - cx * c1z, c2z = cx * c1y - cy * c1x;
+                const double w[3] = {vx + 2.0 * c2x, vy + 2.0 * c2y, vz + 2.0 * c2z};
+                for (int a = 0; a < 3; ++a) { mn[a] = std::min(mn[a], w[a]); mx[a] = std::max(mx[a], w[a]); }
+            }
+            rec[2 * (size_t)i] = make_float4(r[0], r[1], r[2], r[3]);
+            rec[2 * (size_t)i + 1] = make_float4(r[4], r[5], r[6], r[7]);
+        } else {
+            if (!(r[3] >= 0.0f)) return fail(ctx, PTR_E_INVALID, who + ": negative sphere radius");
+            for (int a = 0; a < 3; ++a) { mn[a] = (double)r[a] - r[3]; mx[a] = (double)r[a] + r[3]; }
+            rec[2 * (size_t)i] = make_float4(r[0], r[1], r[2], r[3]);
+            rec[2 * (size_t)i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        for (int a = 0; a < 3; ++a) { boxes[6 * (size_t)i + a] = mn[a]; boxes[6 * (size_t)i + 3 + a] = mx[a]; }
+    }
+    std::vector<int> ids((size_t)N);
+    for (int i = 0; i < N; ++i) ids[(size_t)i] = rb.inst_order ? (int)rb.inst_order[i] : i;
+    int rc;
+    const int n_sm = device_sms(ctx->device);
+    if (mesh) {
+        b.place = D.rec + rb.placements_base;
+    } else {
+        float4* place = nullptr;
+        if (cudaMalloc(&place, sizeof(float4) * 2 * (size_t)N) != cudaSuccess) return fail(ctx, PTR_E_NOMEM, who + ": cudaMalloc");
+        s->allocs.push_back(place);
+        rails::k_restride<<<n_sm * 4, 256, 0, ctx->stream>>>(D.rec, rb.placements_base, N, place);
+        if (cudaError_t e = cudaGetLastError()) return cuda_fail(ctx, e, who.c_str());
+        b.place = place;
+    }
+    b.tlas = D.nodes + rb.tlas_base;
+    const int* pi = nullptr;
+    if ((rc = dev_copy(ctx, s->allocs, ids.data(), ids.size(), &pi))) return rc;
+    b.inst_id = pi;
+    b.light_of = nullptr;
+    b.light_of_w = nullptr;
+    if (bd.light_base >= 0) {
+        std::vector<int> lo((size_t)N);
+        for (int i = 0; i < N; ++i) lo[(size_t)i] = bd.light_base + ids[(size_t)i];
+        if ((rc = dev_copy(ctx, s->allocs, lo.data(), lo.size(), &pi))) return rc;
+        b.light_of = pi;
+    }
+    // the wide twin over the leaf slots' boxes; its leaves index leaf slots
+    b.tlas_w = nullptr;
+    b.place_w = nullptr;
+    b.inst_id_w = nullptr;
+    ptx_host::WideBvh wt = ptx_host::build_cwbvh(boxes.data(), N, ptx_host::kCwbvhCPrim);
+    if (!wt.error && wt.node_count > 0) {
+        std::vector<float4> rec_w(2 * (size_t)N);
+        std::vector<int> ids_w((size_t)N), lo_w((size_t)N);
+        for (int i = 0; i < N; ++i) {
+            const uint32_t k = wt.order[(size_t)i];
+            rec_w[2 * (size_t)i] = rec[2 * (size_t)k];
+            rec_w[2 * (size_t)i + 1] = rec[2 * (size_t)k + 1];
+            ids_w[(size_t)i] = ids[k];
+            lo_w[(size_t)i] = bd.light_base + ids[k];
+        }
+        const float4* p4 = nullptr;
+        const uint4* u4 = nullptr;
+        if ((rc = dev_copy(ctx, s->allocs, rec_w.data(), rec_w.size(), &p4))) return rc;
+        b.place_w = p4;
+        if ((rc = dev_copy(ctx, s->allocs, ids_w.data(), ids_w.size(), &pi))) return rc;
+        b.inst_id_w = pi;
+        if (bd.light_base >= 0) {
+            if ((rc = dev_copy(ctx, s->allocs, lo_w.data(), lo_w.size(), &pi))) return rc;
+            b.light_of_w = pi;
+        }
+        if ((rc = dev_copy(ctx, s->allocs, (const uint4*)wt.nodes.data(), 5 * (size_t)wt.node_count, &u4))) return rc;
+        b.tlas_w = u4;
+    }
+    b.n_inst = N;
+    b.proto_shape = bd.prototype_shape;
+    b.proto_mesh = bd.prototype_ref;
+    b.n_tlas = NC;
+    return PTR_OK;
+}
+
 // Acceleration structures of meshes and instanced batches, built on the host and uploaded
 // once: per mesh the binary SAH BLAS (leaf 2) and the compressed wide BVH, each with the
 // triangles re-emitted in its leaf order as (v0, e1 | alpha, e2); per batch a binary TLAS
 // (leaf 2) over the instances' world boxes with the placements in leaf order.
-int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
+// With rails, mesh i and batch i come from their rail slots instead (rail_mesh, rail_batch).
+int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d, const ptr_rails* rails = nullptr) {
     DevScene& S = s->dev;
+    RailDev rd;
+    if (rails) {   // each channel to the device once, as the App packed it
+        int rc0;
+        if ((rails->vertices_texels > 0 && (rc0 = dev_copy(ctx, s->allocs, (const float4*)rails->vertices, (size_t)rails->vertices_texels, &rd.v))) ||
+            (rails->indices_texels > 0 && (rc0 = dev_copy(ctx, s->allocs, (const float4*)rails->indices, (size_t)rails->indices_texels, &rd.idx))) ||
+            (rails->nodes_texels > 0 && (rc0 = dev_copy(ctx, s->allocs, (const float4*)rails->nodes, (size_t)rails->nodes_texels, &rd.nodes))) ||
+            (rails->records_texels > 0 && (rc0 = dev_copy(ctx, s->allocs, (const float4*)rails->records, (size_t)rails->records_texels, &rd.rec))))
+            return rc0;
+    }
     // the bounded geometry's box: its centre splits ray origins into octants for the
     // ray-coherence queue keys
     double world_lo[3] = {1e300, 1e300, 1e300}, world_hi[3] = {-1e300, -1e300, -1e300};
@@ -681,6 +973,13 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     for (int i = 0; i < d->n_lights; ++i)
         if (d->lights[i].kind == PTR_LIGHT_MESH) is_light[(int)d->lights[i].p[0]] = 1;
     for (int mi = 0; mi < d->n_meshes; ++mi) {
+        if (rails) {
+            int depth = 0;
+            if (int rc0 = rail_mesh(ctx, s, *rails, rd, mi, is_light[mi] != 0, meshes[mi], root_box[mi], depth)) return rc0;
+            grow(root_box[mi].data(), root_box[mi].data() + 3);
+            s->max_stack_depth = std::max(s->max_stack_depth, depth);
+            continue;
+        }
         const ptr_mesh_desc& md = d->meshes[mi];
         if (md.n_triangles <= 0 || md.n_vertices <= 0 || !md.positions || !md.indices)
             return fail(ctx, PTR_E_INVALID, "scene: mesh " + std::to_string(mi) + " is empty");
@@ -783,6 +1082,12 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     std::vector<DevBatch> batches(d->n_batches > 0 ? d->n_batches : 0);
     for (int bi = 0; bi < d->n_batches; ++bi) {
         const ptr_batch_desc& bd = d->batches[bi];
+        if (rails) {
+            std::vector<double> boxes;
+            if (int rc0 = rail_batch(ctx, s, *rails, rd, bi, bd, root_box, batches[bi], boxes)) return rc0;
+            for (int i = 0; i < bd.n_instances; ++i) grow(&boxes[6 * (size_t)i], &boxes[6 * (size_t)i + 3]);
+            continue;
+        }
         const int N = bd.n_instances;
         if (N <= 0 || !bd.placements) return fail(ctx, PTR_E_INVALID, "scene: instanced batch " + std::to_string(bi) + " is empty");
         if (bd.prototype_shape == PTR_SHAPE_MESH && (bd.prototype_ref < 0 || bd.prototype_ref >= d->n_meshes))
@@ -1557,7 +1862,23 @@ int check_scene_desc(const ptr_scene_desc* d, std::string& why) {
 }
 }  // namespace
 
-int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
+static int upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, const ptr_rails* rails, ptr_scene** out);
+
+int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) { return upload_scene(ctx, d, nullptr, out); }
+
+int ptr_upload_scene_rails(ptr_ctx* ctx, const ptr_scene_desc* d, const ptr_rails* r, ptr_scene** out) {
+    if (!ctx || !d || !r || !out) return fail(ctx, PTR_E_INVALID, "null argument");
+    if (r->n_meshes != d->n_meshes || r->n_batches != d->n_batches || r->n_mesh_lights < 0 ||
+        (r->n_meshes > 0 && !r->meshes) || (r->n_batches > 0 && !r->batches) || (r->n_mesh_lights > 0 && !r->mesh_lights))
+        return fail(ctx, PTR_E_INVALID, "rails: one rail slot per mesh and per batch of the description");
+    if (r->vertices_texels < 0 || r->indices_texels < 0 || r->nodes_texels < 0 || r->records_texels < 0 ||
+        (r->vertices_texels > 0 && !r->vertices) || (r->indices_texels > 0 && !r->indices) ||
+        (r->nodes_texels > 0 && !r->nodes) || (r->records_texels > 0 && !r->records))
+        return fail(ctx, PTR_E_INVALID, "rails: a channel with texels has a null pointer");
+    return upload_scene(ctx, d, r, out);
+}
+
+static int upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, const ptr_rails* rails, ptr_scene** out) {
     if (!ctx || !d || !out) return fail(ctx, PTR_E_INVALID, "null argument");
     *out = nullptr;
     std::string why;
@@ -1648,7 +1969,7 @@ int ptr_upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, ptr_scene** out) {
         }
         S.env_cond = m;
     }
-    rc = upload_accels(ctx, s, d);
+    rc = upload_accels(ctx, s, d, rails);
     if (!rc) rc = upload_region_bvh(ctx, s, d);
     if (!rc) {
         // the refilling closest-hit loop's scene form: analytic regions and exactly one

@@ -108,6 +108,30 @@ class CudaEngine:
         self._scene_data = packed
         self.reset()
 
+    def register_scene_rails(self, packed, rails, with_orders=True, bare=True):
+        """Upload a packed scene whose array data comes as the reference's packed channels
+        (``rails.pack``: rail v2) through ptr_upload_scene_rails.  bare: the description's
+        mesh positions/indices and batch placements are left NULL, so everything of the
+        meshes and batches comes from the rails.  with_orders: pass the leaf permutations
+        (hit ids are the caller's), else hit ids are leaf indices."""
+        if self.scene is not None:
+            self.lib.ptr_free_scene(self.scene)
+            self.scene = None
+        desc = packed.desc()
+        if bare:
+            for i in range(desc.n_meshes):
+                desc.meshes[i].positions = None
+                desc.meshes[i].indices = None
+                desc.meshes[i].tri_alpha = None
+            for i in range(desc.n_batches):
+                desc.batches[i].placements = None
+        st = rails.struct(with_orders)
+        h = C.c_void_p()
+        self._check(self.lib.ptr_upload_scene_rails(self.ctx, C.byref(desc), C.byref(st), C.byref(h)))
+        self.scene = h
+        self._scene_data = packed
+        self.reset()
+
     # -- renderers ----------------------------------------------------------------------
     def load_renderer(self, renderer):
         h = C.c_void_p()
