@@ -903,6 +903,28 @@ def measure_adjoint(args, rank, local, world, dist, cpu_leg=True):
     return line if rank == 0 else None
 
 
+def rails_upload_seconds(local):
+    """The mesh workload's scene uploaded from the reference's packed channels
+    (ptr_upload_scene_rails): the channels are packed first, untimed (the App's work, whose
+    BVH builds the reference already does on the host); timed is the upload call, which
+    copies the channels, checks them, gathers the triangles and builds the wide BLAS on the
+    device."""
+    from pathtracerglsl_b200 import _native, rails
+    from pathtracerglsl_b200.compiler import Compiler
+    from pathtracerglsl_b200.engine import CudaEngine
+    sc, st, *_ = workload("mesh")
+    _, packed = Compiler().compile(sc, st)
+    pr = rails.pack(packed, _native.load())
+    eng = CudaEngine(local)
+    try:
+        t0 = time.perf_counter()
+        eng.register_scene_rails(packed, pr)
+        eng.sync()
+        return time.perf_counter() - t0
+    finally:
+        eng.close()
+
+
 # ---------------------------------------------------------------------------------- the metric
 def run_metric(args):
     """The metric's own comparisons in one line: the headline is the batched wavefront on the
@@ -917,6 +939,7 @@ def run_metric(args):
     mesh = measure_ours(args, "mesh", rank, local, world, dist, tuning=MESH_PICK, cpu_leg=False)
     mesh_dev = measure_ours(args, "mesh", rank, local, world, dist, tuning=MESH_PICK, cpu_leg=False,
                             accel_build="device", rmse_leg=False)
+    rails_s = rails_upload_seconds(local)
     if rank == 0:
         line["adjoint"] = {"value": adj["value"], "unit": "samples/s", "ms_per_step": adj["ms_per_step"],
                            "steps": adj["steps"], "config": adj["config"],
@@ -932,6 +955,7 @@ def run_metric(args):
             "clocks": mesh_dev["clocks"],
             "form": "the same workload with its 1.31 M-triangle BLAS built on the device (linear BVH + greedy "
                     "eight-wide collapse) instead of the host's SAH builders"}
+        line["mesh"]["rails_upload_s"] = rails_s   # the scene from the reference's packed channels
         line["gpu_launches"] = line["gpu_launches"] + adj["gpu_launches"] + mesh["gpu_launches"] + mesh_dev["gpu_launches"]
         line["config"] = dict(line["config"], workload="metric: " + line["config"]["workload"],
                               also="adjoint-c5 (adjoint vs forward) and mesh-c2 (plain, matched RMSE) in the "
