@@ -60,7 +60,10 @@ struct DevScene {
     const float4* region_bvh;     // 2 float4 per node, leaf items index region_items
     const int* region_items;      // leaf order -> region index
     const int* linear_regions;    // regions outside the BVH (planes, meshes, batches), in order
-    int n_linear, n_region_nodes, pad_r0, pad_r1;
+    // Without a region BVH: the region list as runs of one shape, (shape, first, count, 0)
+    // in region order, so the scan dispatches once per run (NULL: per region)
+    const int4* region_runs;
+    int n_linear, n_region_nodes, n_runs, pad_r1;
     int n_regions, n_materials, n_lights, ambient_material;
     int has_media, accel, n_meshes, n_batches;
     int inst_accel;           // PTR_ACCEL_* of the instanced batches' TLAS

@@ -237,6 +237,21 @@ __device__ __forceinline__ int warp_append(unsigned* counter, bool pred) {
 // ---- scene queries -------------------------------------------------------------------
 // Nearest hit over every arm; returns region (or -1), element, primitive and t.
 
+template <int V> struct ShapeC { static constexpr int value = V; };
+// Calls f(ShapeC<shape>{}, first, end) for each same-shape run of the region list, the
+// shape a compile-time constant for the analytic shapes the build holds (one dispatch per
+// run instead of one per region); other runs get f(ShapeC<-1>{}, ...).
+template <class F>
+__device__ __forceinline__ void for_region_runs(const DevScene& S, F&& f) {
+    for (int q = 0; q < S.n_runs; ++q) {
+        const int4 run = __ldg(S.region_runs + q);
+        const int a = run.y, b = run.y + run.z;
+        if (has_shape(PTR_SHAPE_SPHERE) && run.x == PTR_SHAPE_SPHERE) f(ShapeC<PTR_SHAPE_SPHERE>{}, a, b);
+        else if (has_shape(PTR_SHAPE_QUAD) && run.x == PTR_SHAPE_QUAD) f(ShapeC<PTR_SHAPE_QUAD>{}, a, b);
+        else f(ShapeC<-1>{}, a, b);
+    }
+}
+
 __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r, Work* w = nullptr) {
     HitRec h;
     h.t = kMaxDist;
@@ -263,10 +278,17 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
     for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) arm(k, S.regions[k], spec_shape(k));
 #else
     const bool tabled = S.region_bvh != nullptr;
-    const int n = tabled ? S.n_linear : S.n_regions;
-    for (int k = 0; k < n; ++k) {
-        const int i = tabled ? S.linear_regions[k] : k;
-        arm(i, S.regions[i], S.regions[i].shape);
+    if (!tabled && S.region_runs) {
+        for_region_runs(S, [&](auto sc, int a, int b) {
+            constexpr int SH = decltype(sc)::value;
+            for (int i = a; i < b; ++i) arm(i, S.regions[i], SH >= 0 ? SH : S.regions[i].shape);
+        });
+    } else {
+        const int n = tabled ? S.n_linear : S.n_regions;
+        for (int k = 0; k < n; ++k) {
+            const int i = tabled ? S.linear_regions[k] : k;
+            arm(i, S.regions[i], S.regions[i].shape);
+        }
     }
 #endif
     if (tabled) {
@@ -304,10 +326,26 @@ __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float
         if (arm(S.regions[k], spec_shape(k))) return true;
 #else
     const bool tabled = S.region_bvh != nullptr;
-    const int n = tabled ? S.n_linear : S.n_regions;
-    for (int k = 0; k < n; ++k) {
-        const int i = tabled ? S.linear_regions[k] : k;
-        if (arm(S.regions[i], S.regions[i].shape)) return true;
+    if (!tabled && S.region_runs) {
+        bool hit = false;
+        for (int q = 0; q < S.n_runs && !hit; ++q) {
+            const int4 run = __ldg(S.region_runs + q);
+            const int a = run.y, b = run.y + run.z;
+            if (has_shape(PTR_SHAPE_SPHERE) && run.x == PTR_SHAPE_SPHERE) {
+                for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], PTR_SHAPE_SPHERE);
+            } else if (has_shape(PTR_SHAPE_QUAD) && run.x == PTR_SHAPE_QUAD) {
+                for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], PTR_SHAPE_QUAD);
+            } else {
+                for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], S.regions[i].shape);
+            }
+        }
+        if (hit) return true;
+    } else {
+        const int n = tabled ? S.n_linear : S.n_regions;
+        for (int k = 0; k < n; ++k) {
+            const int i = tabled ? S.linear_regions[k] : k;
+            if (arm(S.regions[i], S.regions[i].shape)) return true;
+        }
     }
 #endif
     if (tabled) {

@@ -1971,6 +1971,15 @@ static int upload_scene(ptr_ctx* ctx, const ptr_scene_desc* d, const ptr_rails* 
     }
     rc = upload_accels(ctx, s, d, rails);
     if (!rc) rc = upload_region_bvh(ctx, s, d);
+    if (!rc && !S.region_bvh && d->n_regions > 0) {   // the scan's same-shape runs
+        std::vector<int4> runs;
+        for (int i = 0; i < d->n_regions; ++i) {
+            const int sh = d->regions[i].shape;
+            if (!runs.empty() && runs.back().x == sh) runs.back().z++;
+            else runs.push_back(make_int4(sh, i, 1, 0));
+        }
+        if ((rc = dev_copy(ctx, s->allocs, runs.data(), runs.size(), &S.region_runs)) == PTR_OK) S.n_runs = (int)runs.size();
+    }
     if (!rc) {
         // the refilling closest-hit loop's scene form: analytic regions and exactly one
         // acceleration region, an instanced mesh batch, with no region BVH
