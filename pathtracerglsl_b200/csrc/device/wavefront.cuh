@@ -252,6 +252,27 @@ __device__ __forceinline__ void for_region_runs(const DevScene& S, F&& f) {
     }
 }
 
+// The root of region i inside a run of one analytic shape, its parameters fetched as
+// aligned float4s: an uploaded region table is 256-byte aligned and its records 80 bytes,
+// so a record's bytes 16..79 are four float4s (ior, p[0..2]), (p[3..6]), (p[7..10]),
+// (p[11..14]).  Same operands as analytic_root_shape, fewer load instructions.
+template <int SH>
+__device__ __forceinline__ bool run_root(const DevScene& S, int i, const Ray& r, float& t) {
+    const float4* g4 = reinterpret_cast<const float4*>(S.regions + i);
+    if constexpr (SH == PTR_SHAPE_SPHERE) {
+        const float4 a = __ldg(g4 + 1), b = __ldg(g4 + 2);
+        return sphere_intersect(r, f3(a.y, a.z, a.w), b.x, t);
+    } else if constexpr (SH == PTR_SHAPE_QUAD) {
+        const float4 a = __ldg(g4 + 1), b = __ldg(g4 + 2), c = __ldg(g4 + 3), d = __ldg(g4 + 4);
+        return quad_intersect(r, f3(a.y, a.z, a.w), f3(b.x, b.y, b.z), f3(b.w, c.x, c.y), f3(c.z, c.w, d.x), t);
+    } else {
+        return analytic_root(S.regions[i], r, t);
+    }
+}
+#ifndef __CUDACC_RTC__   // (NVRTC has no offsetof; the library build checks the layout)
+static_assert(sizeof(ptr_region) == 80 && __builtin_offsetof(ptr_region, p) == 20, "run_root's float4 view of a region record");
+#endif
+
 __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r, Work* w = nullptr) {
     HitRec h;
     h.t = kMaxDist;
@@ -281,7 +302,19 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
     if (!tabled && S.region_runs) {
         for_region_runs(S, [&](auto sc, int a, int b) {
             constexpr int SH = decltype(sc)::value;
-            for (int i = a; i < b; ++i) arm(i, S.regions[i], SH >= 0 ? SH : S.regions[i].shape);
+            for (int i = a; i < b; ++i) {
+                if constexpr (SH >= 0) {
+                    float t;
+                    if (run_root<SH>(S, i, r, t) && t < h.t) {
+                        h.t = t;
+                        h.region = i;
+                        h.element = 0;
+                        h.prim = -1;
+                    }
+                } else {
+                    arm(i, S.regions[i], S.regions[i].shape);
+                }
+            }
         });
     } else {
         const int n = tabled ? S.n_linear : S.n_regions;
@@ -331,10 +364,11 @@ __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float
         for (int q = 0; q < S.n_runs && !hit; ++q) {
             const int4 run = __ldg(S.region_runs + q);
             const int a = run.y, b = run.y + run.z;
+            float t;
             if (has_shape(PTR_SHAPE_SPHERE) && run.x == PTR_SHAPE_SPHERE) {
-                for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], PTR_SHAPE_SPHERE);
+                for (int i = a; i < b && !hit; ++i) hit = run_root<PTR_SHAPE_SPHERE>(S, i, r, t) && t < max_dist;
             } else if (has_shape(PTR_SHAPE_QUAD) && run.x == PTR_SHAPE_QUAD) {
-                for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], PTR_SHAPE_QUAD);
+                for (int i = a; i < b && !hit; ++i) hit = run_root<PTR_SHAPE_QUAD>(S, i, r, t) && t < max_dist;
             } else {
                 for (int i = a; i < b && !hit; ++i) hit = arm(S.regions[i], S.regions[i].shape);
             }
@@ -375,10 +409,26 @@ __device__ __forceinline__ int scene_region_at(const DevScene& S, f3 p) {
     for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) arm(k, S.regions[k], spec_shape(k));
 #else
     const bool tabled = S.region_bvh != nullptr;
-    const int n = tabled ? S.n_linear : S.n_regions;
-    for (int k = 0; k < n; ++k) {
-        const int i = tabled ? S.linear_regions[k] : k;
-        arm(i, S.regions[i], S.regions[i].shape);
+    if (!tabled && S.region_runs) {
+        for_region_runs(S, [&](auto sc, int a, int b) {
+            constexpr int SH = decltype(sc)::value;
+            for (int i = a; i < b; ++i) {
+                if constexpr (SH == PTR_SHAPE_SPHERE) {   // the sphere's centre and radius as two float4 loads
+                    const float4* g4 = reinterpret_cast<const float4*>(S.regions + i);
+                    const float4 c = __ldg(g4 + 1), rr = __ldg(g4 + 2);
+                    const float d = length(p - f3(c.y, c.z, c.w)) - rr.x;
+                    if (d < 0.0f && (d > best || (d == best && i < region))) { best = d; region = i; }
+                } else {
+                    arm(i, S.regions[i], SH >= 0 ? SH : S.regions[i].shape);
+                }
+            }
+        });
+    } else {
+        const int n = tabled ? S.n_linear : S.n_regions;
+        for (int k = 0; k < n; ++k) {
+            const int i = tabled ? S.linear_regions[k] : k;
+            arm(i, S.regions[i], S.regions[i].shape);
+        }
     }
 #endif
     if (tabled) {
