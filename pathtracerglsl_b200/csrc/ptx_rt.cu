@@ -1231,13 +1231,13 @@ int upload_accels(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d, const ptr
 }
 
 // Region BVH over the bounded analytic regions (spheres, boxes, quads) when there are at
-// least PTR_REGION_BVH_MIN of them (default 129; the reference tests every non-instanced
-// primitive as one unrolled arm, and on B200 the linear scan of the regions measured
-// faster than this BVH up to ~200 spheres).  Planes, meshes and instanced batches stay in
+// least PTR_REGION_BVH_MIN of them (default 257; the reference tests every non-instanced
+// primitive as one unrolled arm, and on B200 the linear scan by same-shape runs measured
+// faster than this BVH beyond 200 spheres).  Planes, meshes and instanced batches stay in
 // the ordered linear list.  Hits equal the linear scan's (same tie rule).
 int upload_region_bvh(ptr_ctx* ctx, ptr_scene* s, const ptr_scene_desc* d) {
     DevScene& S = s->dev;
-    int min_items = 129;
+    int min_items = 257;
     if (const char* env = std::getenv("PTR_REGION_BVH_MIN")) min_items = std::atoi(env);
     std::vector<int> bounded, linear;
     std::vector<double> boxes;
