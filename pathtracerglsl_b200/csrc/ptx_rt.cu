@@ -2112,6 +2112,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     std::vector<BatchJob> bjobs(n_jobs);
     std::vector<long long> offsets(n_jobs + 1, 0);
     int iters = 0;
+    std::vector<int> job_iters(n_jobs);
     for (int j = 0; j < n_jobs; ++j) {
         const ptr_batch_job& J = jobs[j];
         ptr_program* p = J.prog;
@@ -2148,7 +2149,8 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         bjobs[j].sum = p->sum;
         bjobs[j].sumsq = p->sumsq;
         offsets[j + 1] = offsets[j] + total_j;
-        iters = std::max(iters, p->desc.max_bounces + 1 + (J.scene->has_media ? p->desc.max_null_crossings : 0));
+        job_iters[j] = p->desc.max_bounces + 1 + (J.scene->has_media ? p->desc.max_null_crossings : 0);
+        iters = std::max(iters, job_iters[j]);
     }
     const long long total = offsets[n_jobs];
     if (!ctx->batch) {
@@ -2185,6 +2187,13 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
     bt.total = total;
     bt.capacity = (int)cap;
     const long long waves = (total + cap - 1) / cap;
+    // each wave walks only as many iterations as the deepest job it holds
+    std::vector<int> wave_iters((size_t)waves, 0);
+    for (long long w = 0, j = 0; w < waves; ++w) {
+        const long long lo = w * cap, hi = std::min(total, lo + cap);
+        while (j < n_jobs && offsets[j + 1] <= lo) ++j;
+        for (long long k = j; k < n_jobs && offsets[k] < hi; ++k) wave_iters[(size_t)w] = std::max(wave_iters[(size_t)w], job_iters[(size_t)k]);
+    }
     const int n_sm = device_sms(ctx->device);
     cudaError_t e = cudaMemcpyAsync(d_scenes, scenes.data(), sizeof(DevScene) * n_jobs, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_progs, progs.data(), sizeof(ProgParams) * n_jobs, cudaMemcpyHostToDevice, st);
@@ -2200,7 +2209,7 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
         std::vector<ProfRec> prof;
         prof.reserve((size_t)waves * (iters * 5 + 2));
         for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk, &prof);
+            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, wave_iters[(size_t)w], n_sm, ctx->tune, sk, &prof);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -2214,16 +2223,32 @@ int ptr_render_batch(ptr_ctx* ctx, const ptr_batch_job* jobs, int n_jobs) {
             cudaEventDestroy(pr.b);
         }
     } else {
-        // occupancy queries outside capture, then the captured wave
+        // occupancy queries outside capture, then one captured wave per iteration count the
+        // waves need
         launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk, nullptr, true);
-        if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, iters, n_sm, ctx->tune, sk);
-            e = cudaStreamEndCapture(st, &g);
+        std::map<int, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+        for (long long w = 0; e == cudaSuccess && w < waves; ++w) {
+            const int it = wave_iters[(size_t)w];
+            auto gi = graphs.find(it);
+            if (gi == graphs.end()) {
+                cudaGraph_t gw = nullptr;
+                cudaGraphExec_t gew = nullptr;
+                e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    launch_batch_wave(jobs[0].scene->dev, bp->pool, bt, direct, media, equi, st, it, n_sm, ctx->tune, sk);
+                    e = cudaStreamEndCapture(st, &gw);
+                }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&gew, gw, 0);
+                gi = graphs.emplace(it, std::make_pair(gw, gew)).first;
+                if (e != cudaSuccess) break;
+            }
+            e = cudaGraphLaunch(gi->second.second, st);
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
-        for (long long w = 0; e == cudaSuccess && w < waves; ++w) e = cudaGraphLaunch(ge, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        for (auto& kv : graphs) {
+            if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
+            if (kv.second.first) cudaGraphDestroy(kv.second.first);
+        }
     }
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "ptr_render_batch");
     if (ge) cudaGraphExecDestroy(ge);
