@@ -545,9 +545,12 @@ int device_sms(int dev) {
 // its vertex and index arrays, with the triangle records of both leaf orders.  The
 // arrays the walks read join the scene's allocations; the build's temporaries are freed.
 // The build proper over device-resident inputs: positions (3 floats per vertex), the index
-// triples and the optional per-triangle alpha, all in the caller's triangle order.
+// triples and the optional per-triangle alpha, all in the caller's triangle order.  binary:
+// also emit the preorder binary BVH and its triangle records (a caller with its own binary
+// tree, the rail upload, takes the wide BVH only; root and bin_depth are then not set).
 int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const unsigned* d_idx, const float* d_alpha,
-                           int n, DevMesh& m, std::vector<double>& root, int& n_nodes, int& n_cw_nodes, int& bin_depth) {
+                           int n, DevMesh& m, std::vector<double>& root, int& n_nodes, int& n_cw_nodes, int& bin_depth,
+                           bool binary = true) {
     using namespace lbvh;
     cudaStream_t st = ctx->stream;
     const int n_sm = device_sms(ctx->device);
@@ -579,11 +582,11 @@ int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const
     unsigned* counters = (unsigned*)alloc(sizeof(unsigned) * 8, false);
     uint32_t* wide_big = (uint32_t*)alloc(sizeof(uint32_t) * 20 * (size_t)n, false);
     uint32_t* order = (uint32_t*)alloc(sizeof(uint32_t) * (size_t)n, false);
-    float4* bvh = (float4*)alloc(sizeof(float4) * 2 * (size_t)total, true);
-    float4* tri = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
+    float4* bvh = binary ? (float4*)alloc(sizeof(float4) * 2 * (size_t)total, true) : nullptr;
+    float4* tri = binary ? (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true) : nullptr;
     float4* tri_w = (float4*)alloc(sizeof(float4) * 3 * (size_t)n, true);
     if (!lo || !hi || !cb || !keys || !child || !parent || !range ||
-        !arrivals || !nlo || !nhi || !ta || !tb || !counters || !wide_big || !order || !bvh || !tri || !tri_w) {
+        !arrivals || !nlo || !nhi || !ta || !tb || !counters || !wide_big || !order || (binary && (!bvh || !tri)) || !tri_w) {
         release();
         return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc");
     }
@@ -606,7 +609,7 @@ int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const
     k_hierarchy<<<grid, block, 0, st>>>(keys, n, child, parent, range);
     k_refit<<<grid, block, 0, st>>>(keys, lo, hi, n, child, parent, arrivals, nlo, nhi);
     int* depth_dev = cb + 6;   // the binary layout's deepest level (initialised to 0)
-    k_binary_layout<<<grid, block, 0, st>>>(n, child, parent, range, nlo, nhi, bvh, depth_dev);
+    if (binary) k_binary_layout<<<grid, block, 0, st>>>(n, child, parent, range, nlo, nhi, bvh, depth_dev);
     // the wide nodes, one level of tasks per launch
     int n_tasks = 1, levels = 0;
     int2 *tin = ta, *tout = tb;
@@ -636,11 +639,11 @@ int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const
     uint32_t* wide = (uint32_t*)alloc(sizeof(uint32_t) * 20 * (size_t)cnt[0], true);
     if (!wide) { release(); return fail(ctx, PTR_E_NOMEM, "scene: device BVH build: cudaMalloc"); }
     e = cudaMemcpyAsync(wide, wide_big, sizeof(uint32_t) * 20 * (size_t)cnt[0], cudaMemcpyDeviceToDevice, st);
-    k_emit_tris<<<grid, block, 0, st>>>(d_pos, d_idx, d_alpha, nullptr, keys, n, tri);
+    if (binary) k_emit_tris<<<grid, block, 0, st>>>(d_pos, d_idx, d_alpha, nullptr, keys, n, tri);
     k_emit_tris<<<grid, block, 0, st>>>(d_pos, d_idx, d_alpha, order, keys, n, tri_w);
     float4 rb[2];
     int depth = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(rb, bvh, sizeof(rb), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && binary) e = cudaMemcpyAsync(rb, bvh, sizeof(rb), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&depth, depth_dev, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -654,8 +657,10 @@ int build_mesh_device_core(ptr_ctx* ctx, ptr_scene* s, const float* d_pos, const
     m.cwbvh = (const uint4*)wide;
     n_nodes = total;
     n_cw_nodes = (int)cnt[0];
-    bin_depth = depth;
-    root = {rb[0].x, rb[0].y, rb[0].z, rb[1].x, rb[1].y, rb[1].z};
+    if (binary) {
+        bin_depth = depth;
+        root = {rb[0].x, rb[0].y, rb[0].z, rb[1].x, rb[1].y, rb[1].z};
+    }
     return PTR_OK;
 }
 
@@ -804,7 +809,7 @@ int rail_mesh(ptr_ctx* ctx, ptr_scene* s, const ptr_rails& R, const RailDev& D, 
     DevMesh wide{};
     std::vector<double> wide_root;
     int wn = 0, wcw = 0, wdepth = 0;
-    int rc = build_mesh_device_core(ctx, s, d_pos, d_idx, d_alpha, T, wide, wide_root, wn, wcw, wdepth);
+    int rc = build_mesh_device_core(ctx, s, d_pos, d_idx, d_alpha, T, wide, wide_root, wn, wcw, wdepth, false);
     release();
     if (rc) return rc;
     m.tri = tri;
