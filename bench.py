@@ -832,7 +832,10 @@ def measure_adjoint(args, rank, local, world, dist, cpu_leg=True):
         return reduce_max(dist, sum(a.elapsed_time(b) for a, b in zip(starts, ends)))
 
     def adj_step(k):
-        return eng.backward(dl, w, h, spp_a, salt=3000 + 17 * k + rank)
+        torch.cuda.nvtx.range_push("adjoint_step")   # names the step's launches for a profiler
+        g = eng.backward(dl, w, h, spp_a, salt=3000 + 17 * k + rank)
+        torch.cuda.nvtx.range_pop()
+        return g
 
     def fwd_step(k):
         eng.pin_reset_salt(3000 + 17 * k + rank)
