@@ -1511,10 +1511,12 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                     }
                 }
                 if (!hit_boundary) { finished = true; break; }
+                // an optical surface blocks the query: decided from the hit region alone,
+                // before the hit's frame and its region classification
+                const int om = material_of(S, hr.region);
+                if (!(om >= 0 && S.materials[om].model == PTR_MAT_NONE)) { T = Col(0.0f); finished = true; break; }
                 Hit h;
                 fill_hit(S, seg, hr, h);
-                int om = material_of(S, h.region_owner);
-                if (!(om >= 0 && S.materials[om].model == PTR_MAT_NONE)) { T = Col(0.0f); finished = true; break; }
                 medium = h.region_to;
                 seg = ray_spawn(h, seg.d);
                 seg.d = normalize(light_p - seg.o);
