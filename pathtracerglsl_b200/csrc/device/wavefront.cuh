@@ -104,6 +104,13 @@ struct PathPool {
     unsigned char* skey;      // key per position of the shadow queue
     int* q_ray;
     int* shq_s;
+    // the adjoint's hit log (ptr_backward; NULL otherwise): the forward walk records every
+    // closest hit of walk iterations below hit_log_iters at [iter * hit_log_stride + path]
+    // (hit, hit_i as two float4), and the replay of the same paths reads them back instead of
+    // walking the scene again.  iter and hit_log_mode (1 record, 2 replay) are set per launch.
+    float4* hit_log;
+    long long hit_log_stride;
+    int hit_log_iters, hit_log_mode, iter, pad_log;
 };
 
 constexpr int kRayBuckets = 64;   // ray_key values
@@ -237,6 +244,12 @@ __device__ __forceinline__ int warp_append(unsigned* counter, bool pred) {
 // ---- scene queries -------------------------------------------------------------------
 // Nearest hit over every arm; returns region (or -1), element, primitive and t.
 
+__device__ __forceinline__ float4 int4_as_float4(int4 v) {
+    return make_float4(__int_as_float(v.x), __int_as_float(v.y), __int_as_float(v.z), __int_as_float(v.w));
+}
+__device__ __forceinline__ int4 float4_as_int4(float4 v) {
+    return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z), __float_as_int(v.w));
+}
 template <int V> struct ShapeC { static constexpr int value = V; };
 // Calls f(ShapeC<shape>{}, first, end) for each same-shape run of the region list, the
 // shape a compile-time constant for the analytic shapes the build holds (one dispatch per
@@ -736,19 +749,35 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         return;
     }
     const WaveJobs wj = BATCH ? WaveJobs(pool, bt) : WaveJobs{};
+    // the adjoint's hit log: this launch's slice, when its iteration is logged
+    float4* log = (!BATCH && pool.hit_log && pool.iter < pool.hit_log_iters)
+                      ? pool.hit_log + 2 * (size_t)pool.iter * (size_t)pool.hit_log_stride : nullptr;
     QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
     unsigned k;
     while (cur.next(k)) {
         if (k >= n) continue;
         int i = q[k];
         const DevScene& S = BATCH ? bt.scenes[wj.of(bt, i)] : S0;
-        Ray r;
-        r.o = xyz(pool.ray_o[i]);
-        r.d = xyz(pool.ray_d[i]);
-        HitRec h = scene_closest(S, r, COUNT ? &w : nullptr);
-        pool.hit[i] = make_float4(h.t, h.u, h.v, 0.f);
-        pool.hit_i[i] = make_int4(h.region, h.element, h.prim, 0);
-        if (buckets > 1) pool.sort_key[i] = (unsigned char)shade_key(S, h.region, pool.st[i].y, buckets);
+        float4 hf;
+        int4 hi;
+        if (log && pool.hit_log_mode == 2) {   // the replay: the forward walk's hit of this path
+            hf = log[2 * (size_t)i];
+            hi = float4_as_int4(log[2 * (size_t)i + 1]);
+        } else {
+            Ray r;
+            r.o = xyz(pool.ray_o[i]);
+            r.d = xyz(pool.ray_d[i]);
+            HitRec h = scene_closest(S, r, COUNT ? &w : nullptr);
+            hf = make_float4(h.t, h.u, h.v, 0.f);
+            hi = make_int4(h.region, h.element, h.prim, 0);
+            if (log && pool.hit_log_mode == 1) {
+                log[2 * (size_t)i] = hf;
+                log[2 * (size_t)i + 1] = int4_as_float4(hi);
+            }
+        }
+        pool.hit[i] = hf;
+        pool.hit_i[i] = hi;
+        if (buckets > 1) pool.sort_key[i] = (unsigned char)shade_key(S, hi.x, pool.st[i].y, buckets);
     }
     if (COUNT) flush_work(S0, w);
 }

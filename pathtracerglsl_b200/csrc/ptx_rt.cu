@@ -111,6 +111,8 @@ struct ptr_program {
     size_t adj_dl_n = 0;
     double* adj_grads = nullptr;      // PTR_GRAD_SLOTS per material
     size_t adj_grads_n = 0;
+    float4* hit_log = nullptr;        // the adjoint's hit log (PathPool::hit_log)
+    size_t hit_log_bytes = 0;
 };
 
 namespace {
@@ -348,6 +350,7 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         int in = it & 1;
         PathPool pi = pool;   // camera rays keep their generation order; later queues are key-sorted
         pi.ray_in = pool.ray_sort && it > 0;
+        pi.iter = it;
         r = mark(1);
         if (S.work) L(k_closest<true, false>, 0, S, pi, in, nob);
         else if (sk) L.raw(sk->closest, 0, S, pi, in, nob);
@@ -436,13 +439,15 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
     L(k_generate<true>, 0, S, pool, p->fp_dev, adj);
     for (int it = 0; it < iters; ++it) {
         int in = it & 1;
+        PathPool pi = pool;
+        pi.iter = it;
         if (sk) {
-            L.raw(sk->closest, 0, S, pool, in, nob);
+            L.raw(sk->closest, 0, S, pi, in, nob);
             L.raw(sk->shade_adj, smem, S, pool, P, in, nob, adj);
             if (P.direct != PTR_DIRECT_NONE) L.raw(sk->shadow_adj, smem, S, pool, P, nob, 0, adj);
             continue;
         }
-        L(k_closest<false, false>, 0, S, pool, in, nob);
+        L(k_closest<false, false>, 0, S, pi, in, nob);
         switch (P.direct * 2 + (media ? 1 : 0)) {
             case 0: L(k_shade<f3, PTR_DIRECT_NONE, false, false, true>, smem, S, pool, P, in, nob, adj); break;
             case 1: L(k_shade<f3, PTR_DIRECT_NONE, true, false, true>, smem, S, pool, P, in, nob, adj); break;
@@ -2074,6 +2079,7 @@ int ptr_free_program(ptr_program* p) {
     if (p->work_dev) cudaFree(p->work_dev);
     if (p->adj_dl) cudaFree(p->adj_dl);
     if (p->adj_grads) cudaFree(p->adj_grads);
+    if (p->hit_log) cudaFree(p->hit_log);
     delete p;
     return PTR_OK;
 }
@@ -2425,12 +2431,31 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
         p->spec.shade_adj = m.shade;
         p->spec.shadow_adj = m.shadow;
     }
+    // the forward walk logs its closest hits for the replay, as many walk iterations as 1 GiB
+    // holds (32 bytes per path slot and iteration); later iterations are walked again
+    const long long per_iter = 32ll * p->capacity;
+    int log_iters = (int)std::min<long long>(iters, (1ll << 30) / std::max<long long>(per_iter, 1));
+    if (log_iters > 0 && p->hit_log_bytes < (size_t)(per_iter * log_iters)) {
+        if (p->hit_log) cudaFree(p->hit_log);
+        p->hit_log = nullptr;
+        p->hit_log_bytes = 0;
+        if (cudaMalloc(&p->hit_log, (size_t)(per_iter * log_iters)) == cudaSuccess) p->hit_log_bytes = (size_t)(per_iter * log_iters);
+        else { cudaGetLastError(); log_iters = 0; }   // no log: the replay walks every query
+    }
     const int saved_profile = p->profile_next;
     p->profile_next = 0;
+    p->pool.hit_log = log_iters > 0 ? p->hit_log : nullptr;
+    p->pool.hit_log_stride = p->capacity;
+    p->pool.hit_log_iters = log_iters;
     for (long long w = 0; w < waves; ++w) {
+        p->pool.hit_log_mode = 1;
         launch_wave(p, s, st, iters, nullptr, n_sm, nullptr, false);
+        p->pool.hit_log_mode = 2;
         launch_replay(p, s, st, iters, n_sm, adj);
     }
+    p->pool.hit_log = nullptr;
+    p->pool.hit_log_iters = 0;
+    p->pool.hit_log_mode = 0;
     p->profile_next = saved_profile;
     CK(ctx, cudaGetLastError());
     CK(ctx, cudaMemcpyAsync(grads, p->adj_grads, ng * sizeof(double), cudaMemcpyDeviceToHost, st));
