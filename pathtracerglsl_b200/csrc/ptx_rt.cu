@@ -2432,9 +2432,12 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
         p->spec.shadow_adj = m.shadow;
     }
     // the forward walk logs its closest hits for the replay, as many walk iterations as 1 GiB
-    // holds (32 bytes per path slot and iteration); later iterations are walked again
+    // holds (32 bytes per path slot and iteration; PTR_HIT_LOG_BYTES overrides the bound);
+    // later iterations are walked again
     const long long per_iter = 32ll * p->capacity;
-    int log_iters = (int)std::min<long long>(iters, (1ll << 30) / std::max<long long>(per_iter, 1));
+    long long log_budget = 1ll << 30;
+    if (const char* env = std::getenv("PTR_HIT_LOG_BYTES")) log_budget = std::max(0ll, (long long)std::atoll(env));
+    int log_iters = (int)std::min<long long>(iters, log_budget / std::max<long long>(per_iter, 1));
     if (log_iters > 0 && p->hit_log_bytes < (size_t)(per_iter * log_iters)) {
         if (p->hit_log) cudaFree(p->hit_log);
         p->hit_log = nullptr;

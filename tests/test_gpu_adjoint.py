@@ -258,3 +258,26 @@ def test_adjoint_on_the_inverse_rendering_scene_matches_finite_differences():
         assert not bad, bad[:10]
     finally:
         rig.close()
+
+
+@pytest.mark.parametrize("log_bytes, capacity", [("0", None), ("600000", None), (None, "4096")])
+def test_hit_log_bounds_and_waves_leave_gradients_unchanged(monkeypatch, log_bytes, capacity):
+    """The replay reads the forward walk's logged hits where the log holds their walk
+    iteration and walks the scene again elsewhere: with no log, a log holding only the first
+    iterations, or a pool of several waves (the log rewritten per wave), every gradient is
+    the default run's up to the order of the float64 atomic sums."""
+    W = H = 48
+    rig = _c5_rig(W, H)
+    try:
+        rng = np.random.RandomState(5)
+        dl = rng.uniform(-1.0, 1.0, (H, W, 3)) / (H * W * 3)
+        ref = rig.backward(dl, 4, salt=21)
+        if log_bytes is not None:
+            monkeypatch.setenv("PTR_HIT_LOG_BYTES", log_bytes)
+        if capacity is not None:
+            monkeypatch.setenv("PTR_CAPACITY", capacity)
+        g = rig.backward(dl, 4, salt=21)
+        assert np.abs(ref[rig.mask]).max() > 0.0
+        np.testing.assert_allclose(g, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
+    finally:
+        rig.close()
