@@ -309,7 +309,20 @@ __device__ __forceinline__ HitRec scene_closest(const DevScene& S, const Ray& r,
 #if PTR_SPEC_NREGIONS > 0
     constexpr bool tabled = false;
 #pragma unroll
-    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) arm(k, S.regions[k], spec_shape(k));
+    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) {
+        const int sh = spec_shape(k);   // folds to a constant in each unrolled arm
+        float t;
+        bool hit = false;
+        if (sh == PTR_SHAPE_SPHERE) hit = run_root<PTR_SHAPE_SPHERE>(S, k, r, t);
+        else if (sh == PTR_SHAPE_QUAD) hit = run_root<PTR_SHAPE_QUAD>(S, k, r, t);
+        else arm(k, S.regions[k], sh);
+        if (hit && t < h.t) {
+            h.t = t;
+            h.region = k;
+            h.element = 0;
+            h.prim = -1;
+        }
+    }
 #else
     const bool tabled = S.region_bvh != nullptr;
     if (!tabled && S.region_runs) {
@@ -368,8 +381,17 @@ __device__ __forceinline__ bool scene_any(const DevScene& S, const Ray& r, float
 #if PTR_SPEC_NREGIONS > 0
     constexpr bool tabled = false;
 #pragma unroll
-    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k)
-        if (arm(S.regions[k], spec_shape(k))) return true;
+    for (int k = 0; k < PTR_SPEC_NREGIONS; ++k) {
+        const int sh = spec_shape(k);   // folds to a constant in each unrolled arm
+        float t;
+        if (sh == PTR_SHAPE_SPHERE) {
+            if (run_root<PTR_SHAPE_SPHERE>(S, k, r, t) && t < max_dist) return true;
+        } else if (sh == PTR_SHAPE_QUAD) {
+            if (run_root<PTR_SHAPE_QUAD>(S, k, r, t) && t < max_dist) return true;
+        } else if (arm(S.regions[k], sh)) {
+            return true;
+        }
+    }
 #else
     const bool tabled = S.region_bvh != nullptr;
     if (!tabled && S.region_runs) {
