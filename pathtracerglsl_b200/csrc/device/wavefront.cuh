@@ -104,10 +104,12 @@ struct PathPool {
     unsigned char* skey;      // key per position of the shadow queue
     int* q_ray;
     int* shq_s;
-    // the adjoint's hit log (ptr_backward; NULL otherwise): the forward walk records every
-    // closest hit of walk iterations below hit_log_iters at [iter * hit_log_stride + path]
-    // (hit, hit_i as two float4), and the replay of the same paths reads them back instead of
-    // walking the scene again.  iter and hit_log_mode (1 record, 2 replay) are set per launch.
+    // the adjoint's walk log (ptr_backward; NULL otherwise): for walk iterations below
+    // hit_log_iters the forward walk records, per path, four float4 at
+    // [4 * (iter * hit_log_stride + path)]: its closest hit (hit, hit_i), then its slot-0
+    // shadow query's visibility and media (ShadowLog).  The replay of the same paths reads
+    // them back instead of walking the scene again.  iter and hit_log_mode (1 record,
+    // 2 replay) are set per launch.
     float4* hit_log;
     long long hit_log_stride;
     int hit_log_iters, hit_log_mode, iter, pad_log;
@@ -773,7 +775,7 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
     const WaveJobs wj = BATCH ? WaveJobs(pool, bt) : WaveJobs{};
     // the adjoint's hit log: this launch's slice, when its iteration is logged
     float4* log = (!BATCH && pool.hit_log && pool.iter < pool.hit_log_iters)
-                      ? pool.hit_log + 2 * (size_t)pool.iter * (size_t)pool.hit_log_stride : nullptr;
+                      ? pool.hit_log + 4 * (size_t)pool.iter * (size_t)pool.hit_log_stride : nullptr;
     QueueCursor cur(n, pool.fetch ? pool.fetch + 0 : nullptr);
     unsigned k;
     while (cur.next(k)) {
@@ -783,8 +785,8 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
         float4 hf;
         int4 hi;
         if (log && pool.hit_log_mode == 2) {   // the replay: the forward walk's hit of this path
-            hf = log[2 * (size_t)i];
-            hi = float4_as_int4(log[2 * (size_t)i + 1]);
+            hf = log[4 * (size_t)i];
+            hi = float4_as_int4(log[4 * (size_t)i + 1]);
         } else {
             Ray r;
             r.o = xyz(pool.ray_o[i]);
@@ -793,8 +795,8 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_closest(DevScene 
             hf = make_float4(h.t, h.u, h.v, 0.f);
             hi = make_int4(h.region, h.element, h.prim, 0);
             if (log && pool.hit_log_mode == 1) {
-                log[2 * (size_t)i] = hf;
-                log[2 * (size_t)i + 1] = int4_as_float4(hi);
+                log[4 * (size_t)i] = hf;
+                log[4 * (size_t)i + 1] = int4_as_float4(hi);
             }
         }
         pool.hit[i] = hf;
@@ -1494,7 +1496,16 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
     const Pair<float4> a_lp = slot ? pool.sh2_lp : pool.sh_lp;
     const Pair<float4> a_c = slot ? pool.sh2_c : pool.sh_c;
     Work wk{0u, 0u, 0u, 0u};
-    if (PTR_REFILL && !MEDIA && !BATCH && !ADJ && pool.fetch && S0.flat_region >= 0 &&
+    // the adjoint's walk log: this launch's slot-0 shadow records (two float4 per path after
+    // its closest hit: visibility rgb and the media count, then up to two (medium, length)
+    // pairs; a count of -1 marks a query the replay walks again)
+    float4* slog = nullptr;
+    if constexpr (!BATCH && !SPECTRAL)
+        if (slot == 0 && pool.hit_log && pool.iter < pool.hit_log_iters)
+            slog = pool.hit_log + 4 * (size_t)pool.iter * (size_t)pool.hit_log_stride + 2;
+    const bool rec = !ADJ && slog && pool.hit_log_mode == 1;
+    const bool rep = ADJ && slog && pool.hit_log_mode == 2;
+    if (PTR_REFILL && !MEDIA && !BATCH && !ADJ && !rec && pool.fetch && S0.flat_region >= 0 &&
         inst_mesh_flat_ok(S0, S0.batches[S0.regions[S0.flat_region].ref])) {
         shadow_refill<Col, COUNT>(S0, pool, shq, n, slot, a_o, a_d, a_lp, a_c, pool.fetch + 1 + slot, &wk);
         if (COUNT) flush_work(S0, wk);
@@ -1524,7 +1535,25 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
         int mm_id[kAdjMaxMedia];
         float mm_len[kAdjMaxMedia];
         int n_mm = 0;
-        if (!MEDIA) {
+        bool logged = false;
+        if constexpr (ADJ) {
+            if (rep) {   // the forward walk's visibility and media of this same query
+                const float4 a = slog[4 * (size_t)i], b = slog[4 * (size_t)i + 1];
+                n_mm = __float_as_int(a.w);
+                logged = n_mm >= 0;
+                if (logged) {
+                    vis = Col(a.x, a.y, a.z);
+                    mm_id[0] = __float_as_int(b.x);
+                    mm_len[0] = b.y;
+                    mm_id[1] = __float_as_int(b.z);
+                    mm_len[1] = b.w;
+                } else {
+                    n_mm = 0;
+                }
+            }
+        }
+        if (logged) {
+        } else if (!MEDIA) {
             vis = scene_any(S, sr, so.w, COUNT ? &wk : nullptr) ? Col(0.0f) : Col(1.0f);
         } else {
             f3 light_p = xyz(lp);
@@ -1553,12 +1582,12 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                         }
                     }
                     if (!het) T = T * medium_transmittance<Col>(S, P, med_mat, seg_len, wl);
-                    if constexpr (ADJ) {
+                    if (ADJ || rec) {
                         int e = 0;
                         while (e < n_mm && mm_id[e] != med_mat) e++;
                         if (e < n_mm) mm_len[e] += seg_len;
                         else if (n_mm < kAdjMaxMedia) { mm_id[n_mm] = med_mat; mm_len[n_mm] = seg_len; n_mm++; }
-                        else flag_error(S, kErrAdjMedia);
+                        else if (ADJ) flag_error(S, kErrAdjMedia);   // (a recording walk logs -1 here)
                     }
                 }
                 if (!hit_boundary) { finished = true; break; }
@@ -1573,6 +1602,14 @@ __global__ void __launch_bounds__(256, PTR_TRACE_MIN_BLOCKS) k_shadow(DevScene S
                 seg.d = normalize(light_p - seg.o);
             }
             vis = finished ? T : Col(0.0f);
+        }
+        if constexpr (!ADJ && !SPECTRAL) {
+            if (rec) {
+                const bool fits = n_mm <= 2;
+                slog[4 * (size_t)i] = make_float4(vis.x, vis.y, vis.z, __int_as_float(fits ? n_mm : -1));
+                slog[4 * (size_t)i + 1] = make_float4(__int_as_float(n_mm > 0 ? mm_id[0] : -1), n_mm > 0 ? mm_len[0] : 0.0f,
+                                                      __int_as_float(n_mm > 1 ? mm_id[1] : -1), n_mm > 1 ? mm_len[1] : 0.0f);
+            }
         }
         if (!spectrum_is_black(vis)) {
             float w = lp.w;

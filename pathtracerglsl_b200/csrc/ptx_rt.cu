@@ -380,18 +380,20 @@ void launch_wave_t(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         }
         if (P.direct != PTR_DIRECT_NONE) {
             r = mark(3);
+            PathPool ps = pool;
+            ps.iter = it;
             // slot 1 (equiangular segment queries) before slot 0 (surface / vertex NEE)
             for (int slot = P.equiangular ? 1 : 0; slot >= 0; --slot) {
                 if (S.work) {
                     DevScene Sq = S;
                     Sq.work = S.work + 4;   // the shadow queries' own tallies
-                    if (media) L(k_shadow<Col, true, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
-                    else L(k_shadow<Col, false, true, false>, 0, Sq, pool, P, nob, slot, AdjParams{});
+                    if (media) L(k_shadow<Col, true, true, false>, 0, Sq, ps, P, nob, slot, AdjParams{});
+                    else L(k_shadow<Col, false, true, false>, 0, Sq, ps, P, nob, slot, AdjParams{});
                 } else if (sk) {
-                    L.raw(sk->shadow, 0, S, pool, P, nob, slot, AdjParams{});
+                    L.raw(sk->shadow, 0, S, ps, P, nob, slot, AdjParams{});
                 } else {
-                    if (media) L(k_shadow<Col, true, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
-                    else L(k_shadow<Col, false, false, false>, 0, S, pool, P, nob, slot, AdjParams{});
+                    if (media) L(k_shadow<Col, true, false, false>, 0, S, ps, P, nob, slot, AdjParams{});
+                    else L(k_shadow<Col, false, false, false>, 0, S, ps, P, nob, slot, AdjParams{});
                 }
             }
             done(r);
@@ -444,7 +446,7 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
         if (sk) {
             L.raw(sk->closest, 0, S, pi, in, nob);
             L.raw(sk->shade_adj, smem, S, pool, P, in, nob, adj);
-            if (P.direct != PTR_DIRECT_NONE) L.raw(sk->shadow_adj, smem, S, pool, P, nob, 0, adj);
+            if (P.direct != PTR_DIRECT_NONE) L.raw(sk->shadow_adj, smem, S, pi, P, nob, 0, adj);
             continue;
         }
         L(k_closest<false, false>, 0, S, pi, in, nob);
@@ -457,8 +459,8 @@ void launch_replay(ptr_program* p, const ptr_scene* s, cudaStream_t st, int iter
             default: L(k_shade<f3, PTR_DIRECT_MIS, true, false, true>, smem, S, pool, P, in, nob, adj); break;
         }
         if (P.direct != PTR_DIRECT_NONE) {
-            if (media) L(k_shadow<f3, true, false, false, true>, smem, S, pool, P, nob, 0, adj);
-            else L(k_shadow<f3, false, false, false, true>, smem, S, pool, P, nob, 0, adj);
+            if (media) L(k_shadow<f3, true, false, false, true>, smem, S, pi, P, nob, 0, adj);
+            else L(k_shadow<f3, false, false, false, true>, smem, S, pi, P, nob, 0, adj);
         }
     }
     k_advance<<<1, 32, 0, st>>>(pool);
@@ -2431,11 +2433,11 @@ int ptr_backward(ptr_program* p, ptr_scene* s, const ptr_frame* f, const float* 
         p->spec.shade_adj = m.shade;
         p->spec.shadow_adj = m.shadow;
     }
-    // the forward walk logs its closest hits for the replay, as many walk iterations as 1 GiB
-    // holds (32 bytes per path slot and iteration; PTR_HIT_LOG_BYTES overrides the bound);
-    // later iterations are walked again
-    const long long per_iter = 32ll * p->capacity;
-    long long log_budget = 1ll << 30;
+    // the forward walk logs its closest hits and slot-0 shadow queries for the replay, as many
+    // walk iterations as 4 GiB holds (64 bytes per path slot and iteration; PTR_HIT_LOG_BYTES
+    // overrides the bound); later iterations are walked again
+    const long long per_iter = 64ll * p->capacity;
+    long long log_budget = 4ll << 30;
     if (const char* env = std::getenv("PTR_HIT_LOG_BYTES")) log_budget = std::max(0ll, (long long)std::atoll(env));
     int log_iters = (int)std::min<long long>(iters, log_budget / std::max<long long>(per_iter, 1));
     if (log_iters > 0 && p->hit_log_bytes < (size_t)(per_iter * log_iters)) {

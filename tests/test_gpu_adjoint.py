@@ -260,12 +260,14 @@ def test_adjoint_on_the_inverse_rendering_scene_matches_finite_differences():
         rig.close()
 
 
-@pytest.mark.parametrize("log_bytes, capacity", [("0", None), ("600000", None), (None, "4096")])
+@pytest.mark.parametrize("log_bytes, capacity", [("0", None), ("1200000", None), (None, "4096")])
 def test_hit_log_bounds_and_waves_leave_gradients_unchanged(monkeypatch, log_bytes, capacity):
-    """The replay reads the forward walk's logged hits where the log holds their walk
-    iteration and walks the scene again elsewhere: with no log, a log holding only the first
-    iterations, or a pool of several waves (the log rewritten per wave), every gradient is
-    the default run's up to the order of the float64 atomic sums."""
+    """The replay reads the forward walk's logged closest hits and shadow-query results
+    (visibility, media lengths) where the log holds their walk iteration and walks the scene
+    again elsewhere: with no log, a log holding only the first iterations (1.2 MB: two
+    iterations of the 9216-path pool at 64 bytes a path), or a pool of several waves (the log
+    rewritten per wave), every gradient is the default run's up to the order of the float64
+    atomic sums."""
     W = H = 48
     rig = _c5_rig(W, H)
     try:
