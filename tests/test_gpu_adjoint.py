@@ -283,3 +283,35 @@ def test_hit_log_bounds_and_waves_leave_gradients_unchanged(monkeypatch, log_byt
         np.testing.assert_allclose(g, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
     finally:
         rig.close()
+
+
+def test_walk_log_walks_again_queries_through_more_than_two_media(monkeypatch):
+    """A shadow record holds at most two (medium, length) pairs.  Three disjoint grey-medium
+    spheres stacked under the ceiling light make the floor's shadow queries cross three
+    distinct media, so the forward walk marks them and the replay walks them again: the
+    gradients equal those of a run with no log, and every medium's sigma_t is live."""
+    sc, st = scenes.adjoint_box_scene()
+    sc = dict(sc)
+    objects = list(sc["objects"][:5])
+    materials = dict(sc["materials"])
+    for j, (y, s) in enumerate([(0.45, 1.0), (0.95, 2.0), (1.45, 3.0)]):
+        materials[f"fog{j}"] = {"model": "none", "medium": {"sigma_a": [0.1 * s] * 3, "sigma_s": [0.9 * s] * 3,
+                                                            "phase_g": 0.3}}
+        objects.append({"type": "sphere", "parameters": {"center": [0.0, y, -0.2], "radius": 0.2},
+                        "material": f"fog{j}"})
+    sc["objects"] = objects
+    sc["materials"] = materials
+    W = H = 48
+    rig = Rig(sc, st, W, H)
+    try:
+        rng = np.random.RandomState(37)
+        dl = rng.uniform(-1.0, 1.0, (H, W, 3)) / (H * W * 3)
+        ref = rig.backward(dl, 4, salt=31)
+        monkeypatch.setenv("PTR_HIT_LOG_BYTES", "0")
+        g = rig.backward(dl, 4, salt=31)
+        np.testing.assert_allclose(ref, g, rtol=1e-9, atol=1e-12 * np.abs(g).max())
+        for j in range(3):
+            i = rig.pk.material_names.index(f"fog{j}")
+            assert ref[i, abi.GRAD_SIGMA_T] != 0.0, j
+    finally:
+        rig.close()
