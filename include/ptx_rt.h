@@ -486,7 +486,9 @@ int ptr_render_noalloc(const ptr_scene_desc* scene, const ptr_program_desc* prog
  * (n >= PTR_GRAD_SLOTS * n_materials doubles, host memory).  dL_dimage is host memory,
  * 3 floats per pixel (row 0 at the bottom), typically 2 (I - target) / n for an L2 loss on
  * an image I rendered with ptr_render.  The program's film is left untouched.  Synchronises.
- * Not available for equiangular programs.  The program keeps a log of the forward walk's
+ * Returns PTR_E_INVALID, before any device work, for spectral programs, chromatic or
+ * heterogeneous media, equiangular or light-tree programs, programs with AOVs and more
+ * than 512 materials.  The program keeps a log of the forward walk's
  * closest hits and shadow-query results for its replay (64 bytes per path and walk
  * iteration, at most 4 GiB of device memory, freed with the program). */
 int ptr_backward(ptr_program* prog, ptr_scene* scene, const ptr_frame* frame, const float* dL_dimage,
